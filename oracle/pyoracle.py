@@ -1,0 +1,278 @@
+"""ctypes binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Imported by tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg, where
+it is the checker, never the thing measured on the GPU path.  Two libraries share one
+API shape:
+
+* ``liboracle.so`` (prefix ``orc_``): the project's restatement of the reference's
+  arithmetic (oracle_math.hpp, oracle_system.hpp), in float (the reference's FP32
+  semantics) or double (the FP64 oracle);
+* ``_ref/libclothref.so`` (prefix ``ref_``): the reference's own force, Jacobian,
+  material and face code (PhysicsHelper.cu, Material.cu, Face.cu, Edge.cu, ...)
+  compiled from its sources, with the oracle's assembly and solver around it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_ORACLE = os.path.join(HERE, "liboracle.so")
+LIB_REF = os.path.join(HERE, "_ref", "libclothref.so")
+REFERENCE_SRC = "/root/reference/src"
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+
+METHOD_LLT = 0      # LL^T in the cloth's precision: the reference CPU path
+METHOD_LLT64 = 1    # LL^T in double of the same assembled system
+METHOD_PCG64 = 2    # FP64 block-Jacobi PCG to a relative residual
+
+
+def build(ref: bool = True) -> None:
+    """Builds liboracle.so and, when the reference checkout is present, _ref/libclothref.so."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if ref and os.path.isdir(REFERENCE_SRC):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REFSRC={REFERENCE_SRC}"], check=True)
+
+
+def _d(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+class Lib:
+    def __init__(self, which: str = "oracle"):
+        self.which = which
+        path = LIB_ORACLE if which == "oracle" else LIB_REF
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (run oracle/pyoracle.build())")
+        self.lib = ctypes.CDLL(path)
+        self.p = "orc_" if which == "oracle" else "ref_"
+        L = self.lib
+        f = self.fn
+        f("material_free", None, [_vp])
+        f("material_density", ctypes.c_double, [_vp])
+        f("material_stretching", None, [_vp, ctypes.c_int, _dp, _dp])
+        f("material_bending", None, [_vp, ctypes.c_int, _dp, _dp])
+        f("cloth_new", _vp, [_vp, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip])
+        f("cloth_free", None, [_vp])
+        f("cloth_num_edges", ctypes.c_int, [_vp])
+        f("cloth_num_nodes", ctypes.c_int, [_vp])
+        f("cloth_num_interior_edges", ctypes.c_int, [_vp])
+        f("cloth_interior_edges", None, [_vp, _ip, _ip])
+        f("cloth_face_forces", None, [_vp, _dp, _dp])
+        f("cloth_edge_forces", None, [_vp, _dp, _dp, _dp])
+        f("cloth_set_handles", None, [_vp, ctypes.c_int, _ip, _dp])
+        f("cloth_assemble", ctypes.c_int, [_vp, _dp])
+        f("cloth_system", None, [_vp, _ip, _ip, _dp, _dp])
+        f("cloth_solve", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _dp])
+        f("cloth_advance", None, [_vp, _dp, ctypes.c_double])
+        f("cloth_state", None, [_vp, _dp, _dp])
+        f("cloth_set_state", None, [_vp, _dp, _dp])
+        f("cloth_masses", None, [_vp, _dp])
+        f("cloth_normals", None, [_vp, _dp])
+        f("cloth_step", ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _dp])
+        f("cloth_factor_nnz", ctypes.c_longlong, [_vp])
+        f("run_cloths", ctypes.c_double, [ctypes.POINTER(_vp), ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, _ip])
+        if which == "oracle":
+            f("material_new", _vp, [ctypes.c_int, ctypes.c_double, _dp, _dp, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double])
+            f("material_table", None, [_vp, _dp])
+        else:
+            f("material_new", _vp, [ctypes.c_char_p])
+            f("cloth_topology_mismatches", ctypes.c_int, [_vp])
+
+    def fn(self, name, restype, argtypes):
+        fobj = getattr(self.lib, self.p + name)
+        fobj.restype = restype
+        fobj.argtypes = argtypes
+        setattr(self, name, fobj)
+
+
+_LIBS: dict = {}
+
+
+def lib(which: str = "oracle") -> Lib:
+    if which not in _LIBS:
+        _LIBS[which] = Lib(which)
+    return _LIBS[which]
+
+
+class Material:
+    """A material of the restated oracle (real='float' or 'double') or, with which='ref',
+    the reference's own Material built from a written data file."""
+
+    def __init__(self, spec: dict, real: str = "float", which: str = "oracle", workdir: str | None = None):
+        self.L = lib(which)
+        self.which = which
+        self.spec = spec
+        if which == "oracle":
+            st = _d(np.array(spec["stretching"], np.float64).reshape(24))
+            be = _d(np.array(spec["bending"], np.float64).reshape(15))
+            self.h = self.L.material_new(0 if real == "float" else 1, spec["density"], _ptr(st, _dp), _ptr(be, _dp),
+                                         spec.get("thicken", 1.0), spec.get("density_mult", 1.0),
+                                         spec.get("stretching_mult", 1.0), spec.get("bending_mult", 1.0))
+        else:
+            import json
+            wd = workdir or tempfile.mkdtemp(prefix="clothref_")
+            path = os.path.join(wd, "material_%d.json" % id(self))
+            with open(path, "w") as fh:
+                json.dump({k: spec[k] for k in ("density", "stretching", "bending")}, fh)
+            text = json.dumps({"data": path, "thicken": spec.get("thicken", 1.0),
+                               "density_mult": spec.get("density_mult", 1.0),
+                               "stretching_mult": spec.get("stretching_mult", 1.0),
+                               "bending_mult": spec.get("bending_mult", 1.0)})
+            self.h = self.L.material_new(text.encode())
+
+    @property
+    def density(self) -> float:
+        return self.L.material_density(self.h)
+
+    def stretching(self, G3) -> np.ndarray:
+        G3 = _d(G3).reshape(-1, 3)
+        out = np.zeros((G3.shape[0], 4))
+        self.L.material_stretching(self.h, G3.shape[0], _ptr(G3, _dp), _ptr(out, _dp))
+        return out
+
+    def bending(self, q5) -> np.ndarray:
+        q5 = _d(q5).reshape(-1, 5)
+        out = np.zeros(q5.shape[0])
+        self.L.material_bending(self.h, q5.shape[0], _ptr(q5, _dp), _ptr(out, _dp))
+        return out
+
+    def table(self) -> np.ndarray:
+        out = np.zeros(30 * 30 * 30 * 4)
+        self.L.material_table(self.h, _ptr(out, _dp))
+        return out.reshape(30, 30, 30, 4)
+
+    def __del__(self):
+        try:
+            self.L.material_free(self.h)
+        except Exception:
+            pass
+
+
+class Cloth:
+    def __init__(self, sheet: dict, material: Material):
+        self.L = material.L
+        self.material = material
+        x, v, u = _d(sheet["x"]), _d(sheet["v"]), _d(sheet["uv"])
+        fx, fu = _i(sheet["fx"]), _i(sheet["fu"])
+        self.n = x.shape[0]
+        self.nf = fx.shape[0]
+        self.h = self.L.cloth_new(material.h, self.n, _ptr(x, _dp), _ptr(v, _dp), u.shape[0], _ptr(u, _dp),
+                                  self.nf, _ptr(fx, _ip), _ptr(fu, _ip))
+        hn = sheet.get("handles", np.zeros(0, np.int32))
+        if len(hn):
+            hn = _i(hn)
+            pos = _d(x.reshape(-1, 3)[hn])
+            self.L.cloth_set_handles(self.h, len(hn), _ptr(hn, _ip), _ptr(pos, _dp))
+
+    def __del__(self):
+        try:
+            self.L.cloth_free(self.h)
+        except Exception:
+            pass
+
+    @property
+    def n_interior(self) -> int:
+        return self.L.cloth_num_interior_edges(self.h)
+
+    def interior_edges(self):
+        k = self.n_interior
+        nodes = np.zeros((k, 4), np.int32)
+        faces = np.zeros((k, 2), np.int32)
+        self.L.cloth_interior_edges(self.h, _ptr(nodes, _ip), _ptr(faces, _ip))
+        return nodes, faces
+
+    def face_forces(self):
+        f = np.zeros((self.nf, 9))
+        J = np.zeros((self.nf, 9, 9))
+        self.L.cloth_face_forces(self.h, _ptr(f, _dp), _ptr(J, _dp))
+        return f, J
+
+    def edge_forces(self):
+        k = self.n_interior
+        f = np.zeros((k, 12))
+        J = np.zeros((k, 12, 12))
+        th = np.zeros(k)
+        self.L.cloth_edge_forces(self.h, _ptr(f, _dp), _ptr(J, _dp), _ptr(th, _dp))
+        return f, J, th
+
+    def assemble(self, params):
+        p = _d(params)
+        nnzb = self.L.cloth_assemble(self.h, _ptr(p, _dp))
+        rp = np.zeros(self.n + 1, np.int32)
+        ci = np.zeros(nnzb, np.int32)
+        val = np.zeros((nnzb, 3, 3))
+        b = np.zeros(3 * self.n)
+        self.L.cloth_system(self.h, _ptr(rp, _ip), _ptr(ci, _ip), _ptr(val, _dp), _ptr(b, _dp))
+        return rp, ci, val, b
+
+    def solve(self, method=METHOD_LLT, tol=1e-12, max_iter=100000):
+        dv = np.zeros(3 * self.n)
+        rr = ctypes.c_double(0)
+        st = self.L.cloth_solve(self.h, method, tol, max_iter, _ptr(dv, _dp), ctypes.byref(rr))
+        if st < -1:
+            raise RuntimeError("oracle solve failed (matrix not positive definite)")
+        return dv, rr.value
+
+    def step(self, params, method=METHOD_LLT, tol=1e-12, max_iter=100000):
+        p = _d(params)
+        dv = np.zeros(3 * self.n)
+        rr = ctypes.c_double(0)
+        st = self.L.cloth_step(self.h, _ptr(p, _dp), method, tol, max_iter, _ptr(dv, _dp), ctypes.byref(rr))
+        if st < -1:
+            raise RuntimeError("oracle step failed (matrix not positive definite)")
+        return dv, rr.value
+
+    def advance(self, dv, dt):
+        d = _d(dv)
+        self.L.cloth_advance(self.h, _ptr(d, _dp), dt)
+
+    def state(self):
+        x = np.zeros(3 * self.n)
+        v = np.zeros(3 * self.n)
+        self.L.cloth_state(self.h, _ptr(x, _dp), _ptr(v, _dp))
+        return x.reshape(-1, 3), v.reshape(-1, 3)
+
+    def set_state(self, x, v):
+        x, v = _d(x), _d(v)
+        self.L.cloth_set_state(self.h, _ptr(x, _dp), _ptr(v, _dp))
+
+    def masses(self):
+        m = np.zeros(self.n)
+        self.L.cloth_masses(self.h, _ptr(m, _dp))
+        return m
+
+    def normals(self):
+        m = np.zeros(3 * self.nf)
+        self.L.cloth_normals(self.h, _ptr(m, _dp))
+        return m.reshape(-1, 3)
+
+    def topology_mismatches(self) -> int:
+        return self.L.cloth_topology_mismatches(self.h)
+
+
+def run_cloths(cloths, params_list, steps: int, method: int = METHOD_LLT, threads: int = 1):
+    """Steps independent cloths on `threads` host threads; returns (seconds, status)."""
+    L = cloths[0].L
+    arr = (_vp * len(cloths))(*[c.h for c in cloths])
+    p = _d(np.array(params_list, np.float64).reshape(-1))
+    st = np.zeros(len(cloths), np.int32)
+    sec = L.run_cloths(arr, len(cloths), _ptr(p, _dp), steps, method, threads, _ptr(st, _ip))
+    return sec, st

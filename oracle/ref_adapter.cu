@@ -1,0 +1,204 @@
+// Reference adapter (oracle/_ref/libclothref.so).  TEST INFRASTRUCTURE ONLY.
+//
+// Compiled together with the reference's own sources, read in place from the reference
+// checkout (Node.cu, Vertex.cu, Face.cu, Edge.cu, Material.cu, MathHelper.cu,
+// JsonHelper.cu, PhysicsHelper.cu, ...; see oracle/Makefile).  It builds the reference's
+// Node/Vertex/Face/Edge objects the way Mesh::load does on the CPU (Mesh.cu:360-399) and
+// evaluates forces and Jacobians with the reference's stretchingForce
+// (PhysicsHelper.cu:264-291) and bendingForce (PhysicsHelper.cu:327-353), face rest data
+// with Face::initialize (Face.cu:12-20), normals with Face::update (Face.cu:124-132) and
+// stiffness with Material (Material.cu:3-156).  Assembly and the FP32 sparse Cholesky
+// around them are the oracle's restatement of Cloth.cu:42-169 and of SimplicialLLT.
+// The exported names mirror liboracle.so's with the prefix ref_.
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <sstream>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "Edge.cuh"
+#include "Face.cuh"
+#include "Material.cuh"
+#include "Node.cuh"
+#include "PhysicsHelper.cuh"
+#include "Vertex.cuh"
+
+#include "oracle_system.hpp"
+
+#define ORC_API(name) ref_##name
+#define ORC_NO_DEFAULT_FACTORIES 1
+#include "oracle_capi.inc"
+
+namespace {
+
+struct RefCloth {
+    std::vector<Node> nodes;
+    std::vector<Vertex> verts;
+    std::vector<Face> faces;
+    std::vector<Edge> edges;
+    const ::Material* mat = nullptr;
+};
+
+struct RefClothImpl : ClothImpl<float> {
+    RefCloth rc;
+};
+
+}  // namespace
+
+extern "C" {
+
+// json_text: the cloth's "materials" object, e.g. {"data": "path.json", "thicken": 1}.
+void* ref_material_new(const char* json_text) {
+    Json::Value v;
+    std::istringstream in(json_text);
+    in >> v;
+    return new ::Material(v);
+}
+
+void ref_material_free(void* m) { delete static_cast<::Material*>(m); }
+
+double ref_material_density(void* m) { return static_cast<::Material*>(m)->getDensity(); }
+
+void ref_material_stretching(void* m, int n, const double* G3, double* out) {
+    auto* mat = static_cast<::Material*>(m);
+    for (int i = 0; i < n; i++) {
+        Matrix2x2f G;
+        G(0, 0) = (float)G3[3 * i];
+        G(0, 1) = G(1, 0) = (float)G3[3 * i + 1];
+        G(1, 1) = (float)G3[3 * i + 2];
+        Vector4f k = mat->stretchingStiffness(G);
+        for (int c = 0; c < 4; c++) out[4 * i + c] = k(c);
+    }
+}
+
+void ref_material_bending(void* m, int n, const double* in5, double* out) {
+    auto* mat = static_cast<::Material*>(m);
+    for (int i = 0; i < n; i++) {
+        const double* q = in5 + 5 * i;
+        out[i] = mat->bendingStiffness((float)q[0], (float)q[1], (float)q[2], Vector2f((float)q[3], (float)q[4]));
+    }
+}
+
+void* ref_cloth_new(void* mat, int nn, const double* x, const double* v, int nv, const double* u, int nf,
+                    const int* fx, const int* fu) {
+    auto* c = new RefClothImpl();
+    RefCloth& rc = c->rc;
+    rc.mat = static_cast<::Material*>(mat);
+    rc.nodes.resize(nn);
+    for (int i = 0; i < nn; i++) {
+        rc.nodes[i] = Node(Vector3f((float)x[3 * i], (float)x[3 * i + 1], (float)x[3 * i + 2]), true);
+        rc.nodes[i].v = Vector3f((float)v[3 * i], (float)v[3 * i + 1], (float)v[3 * i + 2]);
+        rc.nodes[i].index = i;
+    }
+    rc.verts.resize(nv);
+    for (int i = 0; i < nv; i++) {
+        rc.verts[i] = Vertex(Vector2f((float)u[2 * i], (float)u[2 * i + 1]));
+        rc.verts[i].index = i;
+    }
+    // Topology numbering (edge order) comes from the oracle's restatement; the sides are
+    // then set by the reference's own Edge::initialize, in Mesh::load's call order.
+    orc::Topology topo;
+    topo.build(nn, nv, nf, fx, fu);
+    std::unordered_map<uint64_t, int> emap;
+    for (int e = 0; e < topo.nEdges(); e++)
+        emap[(uint64_t)(uint32_t)topo.eNodes[2 * e] << 32 | (uint32_t)topo.eNodes[2 * e + 1]] = e;
+    auto eid = [&](int a, int b) {
+        if (a > b) std::swap(a, b);
+        return emap[(uint64_t)(uint32_t)a << 32 | (uint32_t)b];
+    };
+    rc.edges.resize(topo.nEdges());
+    for (int e = 0; e < topo.nEdges(); e++)
+        rc.edges[e] = Edge(&rc.nodes[topo.eNodes[2 * e]], &rc.nodes[topo.eNodes[2 * e + 1]]);
+    rc.faces.resize(nf);
+    for (int f = 0; f < nf; f++) {
+        Vertex* v0 = &rc.verts[fu[3 * f]];
+        Vertex* v1 = &rc.verts[fu[3 * f + 1]];
+        Vertex* v2 = &rc.verts[fu[3 * f + 2]];
+        v0->node = &rc.nodes[fx[3 * f]];
+        v1->node = &rc.nodes[fx[3 * f + 1]];
+        v2->node = &rc.nodes[fx[3 * f + 2]];
+        rc.faces[f] = Face(v0, v1, v2, rc.mat);
+        Edge* e0 = &rc.edges[eid(fx[3 * f], fx[3 * f + 1])];
+        Edge* e1 = &rc.edges[eid(fx[3 * f + 1], fx[3 * f + 2])];
+        Edge* e2 = &rc.edges[eid(fx[3 * f + 2], fx[3 * f])];
+        e0->initialize(v2, &rc.faces[f]);
+        e1->initialize(v0, &rc.faces[f]);
+        e2->initialize(v1, &rc.faces[f]);
+        rc.faces[f].setEdges(e0, e1, e2);
+    }
+    for (int f = 0; f < nf; f++) rc.faces[f].update();
+
+    std::vector<float> xf(x, x + 3 * nn), vf(v, v + 3 * nn), uf(u, u + 2 * nv);
+    c->c.init(nn, xf.data(), vf.data(), nv, uf.data(), nf, fx, fu, nullptr, rc.mat->getDensity());
+    // rest data from the reference's Face objects
+    for (int f = 0; f < nf; f++) {
+        const Face& F = rc.faces[f];
+        c->c.finv[4 * f + 0] = F.inverse(0, 0);
+        c->c.finv[4 * f + 1] = F.inverse(0, 1);
+        c->c.finv[4 * f + 2] = F.inverse(1, 0);
+        c->c.finv[4 * f + 3] = F.inverse(1, 1);
+        c->c.farea[f] = F.area;
+        c->c.fmass[f] = F.mass;
+    }
+    c->c.updateGeometry();
+    RefClothImpl* self = c;
+    c->c.syncHook = [self](orc::Cloth<float>& cl) {
+        RefCloth& r = self->rc;
+        for (size_t i = 0; i < r.nodes.size(); i++) {
+            r.nodes[i].x = Vector3f(cl.x[3 * i], cl.x[3 * i + 1], cl.x[3 * i + 2]);
+            r.nodes[i].v = Vector3f(cl.v[3 * i], cl.v[3 * i + 1], cl.v[3 * i + 2]);
+        }
+        for (size_t f = 0; f < r.faces.size(); f++) {
+            r.faces[f].update();
+            for (int k = 0; k < 3; k++) cl.fn[3 * f + k] = r.faces[f].n(k);
+        }
+    };
+    c->c.faceHook = [self](int f, float* fo, float* J) {
+        Vector9f ff;
+        Matrix9x9f JJ;
+        stretchingForce(&self->rc.faces[f], self->rc.mat, ff, JJ);
+        for (int p = 0; p < 9; p++) {
+            fo[p] = ff(p);
+            for (int q = 0; q < 9; q++) J[9 * p + q] = JJ(p, q);
+        }
+    };
+    c->c.edgeHook = [self](int e, float* fo, float* J, float* theta) {
+        Vector12f ff;
+        Matrix12x12f JJ;
+        bendingForce(&self->rc.edges[e], self->rc.mat, ff, JJ);
+        for (int p = 0; p < 12; p++) {
+            fo[p] = ff(p);
+            for (int q = 0; q < 12; q++) J[12 * p + q] = JJ(p, q);
+        }
+        if (theta) *theta = self->rc.edges[e].angle();
+    };
+    c->c.syncHook(c->c);
+    return static_cast<ClothBase*>(c);
+}
+
+// Number of edges whose sides as set by the reference's Edge::initialize disagree with
+// the oracle's restated topology (0 when the restatement is faithful).
+int ref_cloth_topology_mismatches(void* cb) {
+    auto* c = static_cast<RefClothImpl*>(static_cast<ClothBase*>(cb));
+    const RefCloth& r = c->rc;
+    const orc::Topology& t = c->c.topo;
+    int bad = 0;
+    for (int e = 0; e < t.nEdges(); e++) {
+        const Edge& E = r.edges[e];
+        for (int s = 0; s < 2; s++) {
+            int face = E.adjacents[s] ? (int)(E.adjacents[s] - r.faces.data()) : -1;
+            int opp = E.opposites[s] ? (int)(E.opposites[s] - r.verts.data()) : -1;
+            int v0 = E.vertices[s][0] ? (int)(E.vertices[s][0] - r.verts.data()) : -1;
+            int v1 = E.vertices[s][1] ? (int)(E.vertices[s][1] - r.verts.data()) : -1;
+            if (face != t.eFace[2 * e + s] || opp != t.eOpp[2 * e + s] || v0 != t.eVert[4 * e + 2 * s] ||
+                v1 != t.eVert[4 * e + 2 * s + 1])
+                bad++;
+        }
+    }
+    return bad;
+}
+
+}  // extern "C"
