@@ -1,0 +1,146 @@
+// Internal data layout of the B200 implicit cloth step.  Not part of the C ABI.
+//
+// HBM layout (one batch of independent sheets = "instances"):
+//   nodes   : x, v, dv as 3N floats (xyz interleaved), mass N, handle float4 N (xyz target,
+//             w = handle count), FP64 solution accumulator dv64 3N.
+//   faces   : int4 {n0, n1, n2, sheet} (global node ids), float4 inverse rest matrix
+//             (Face::inverse, Face.cu:16), rest area; one 128-byte element record per face.
+//   edges   : interior edges only (the reference skips boundary edges, Cloth.cu:142):
+//             int4 {n0, n1, opposite0, opposite1}, int meta (face-vertex rotations), sheet,
+//             float4 {area0 + area1, bias weight side 0, side 1, 0}; one 128-byte record.
+//   system  : SELL-32 block layout.  Rows (nodes) of a sheet are cut into slices of 32
+//             consecutive rows; slice s has `width` block slots per row (padded with zero
+//             blocks).  Slot (slice, k, lane) stores its 3x3 block in a "panel" of 32 lanes:
+//             entries 0-3 as float4[32], entries 4-7 as float4[32], entry 8 as float[32]
+//             (1152 bytes per panel, 128-bit coalesced loads).  Slot k = 0 is the diagonal.
+//             Column indices and the assembly contributor lists are per *topology* (shared
+//             by all sheets with identical connectivity) and hold sheet-local node ids.
+#ifndef CLOTHSTEP_CS_INTERNAL_H
+#define CLOTHSTEP_CS_INTERNAL_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define CS_SLICE 32
+#define CS_PANEL_FLOATS 288  // 32 lanes x 9 entries
+#define CS_TABLE_N 30
+#define CS_TABLE_ENTRIES (CS_TABLE_N * CS_TABLE_N * CS_TABLE_N)
+#define CS_FACE_REC 32
+#define CS_EDGE_REC 32
+
+// Contributor code: bit 31 = edge (1) / face (0); bits 4..30 = sheet-local element id;
+// bits 2..3 = local row corner a; bits 0..1 = local column corner b.
+#define CS_CODE_EDGE 0x80000000u
+__host__ __device__ inline uint32_t cs_code(int is_edge, int elem, int a, int b) {
+    return (is_edge ? CS_CODE_EDGE : 0u) | ((uint32_t)elem << 4) | ((uint32_t)a << 2) | (uint32_t)b;
+}
+
+struct SheetDesc {
+    int node_off, n_nodes;
+    int face_off, n_faces;
+    int edge_off, n_edges;      // interior edges
+    int slice_off, n_slices;    // global slices
+    int topo;                   // shared topology id
+    int table;                  // stretching table id
+    float bending[15];          // scaled bending samples, 3x5 (Material.cu:38-40)
+    float wind_density, wind_drag, wind_v[3];
+};
+
+struct SliceDesc {
+    int sheet;
+    int topo_slice;  // index into the per-topology slice arrays
+    int row0;        // first global row (node)
+    int rows;        // rows in this slice (<= 32)
+    int width;       // block slots per row
+    int panel0;      // first global value panel
+    int tpanel0;     // first per-topology panel (columns, contributor lists)
+    int pad;
+};
+
+// Solver phases of one instance (one sheet's system) inside the batched loop.
+enum InstPhase : int {
+    PH_CG = 0,        // one preconditioned CG iteration on the FP32 correction system
+    PH_RES = 1,       // FP64 residual b - A (dv64 + e) and its norm
+    PH_INIT = 2,      // start a CG sweep: dv64 += e, e = 0, z = P r, p = z
+    PH_FINISH = 3,    // dv64 += e, then done
+    PH_DONE = 4,
+};
+
+// Instance flags
+#define CS_IF_CONVERGED 1
+#define CS_IF_WARM_REJECTED 2
+#define CS_IF_BREAKDOWN 4
+#define CS_IF_CAPPED 8
+
+struct InstState {
+    double bnorm2;      // ||b||^2 (FP64)
+    double rz;          // r.z of the current iteration
+    double rz_new;
+    double pq;
+    double rr;          // ||r||^2 of the recursive residual
+    double res0;        // FP64 true residual norm at the start of the current sweep
+    double resnorm;     // last FP64 true residual norm
+    double first_res;   // FP64 residual of the initial guess
+    float alpha, beta;
+    int phase;
+    int sweep_iters;
+    int iters;          // total CG iterations this step
+    int sweeps;         // FP64 residual evaluations this step
+    int flags;
+    int resumes;        // plain FP32 solver: failed FP64 checks after which CG resumed
+};
+
+// Step parameters in device memory (read by every kernel of the captured step graph).
+struct DevParams {
+    float dt;
+    float gravity[3];
+    float handle_stiffness;
+    double tol;            // FP64-checked relative residual target
+    double inner_tol;      // relative reduction per CG sweep (mixed precision)
+    int max_iters;         // CG iterations per instance per step
+    int sweep_cap;         // CG iterations per sweep
+    int mixed;             // 1: FP32 CG + FP64 refinement; 0: plain FP32 CG (FP32 dots)
+    int warm;              // 0 zero guess, 1 warm start from dv64 as preloaded
+    int loop_cap;          // hard bound on loop trips per step
+    int advance;           // 1: v += dv, x += dt v at the end of the step
+};
+
+struct Batch {
+    int N = 0, F = 0, E = 0, S = 0;
+    int n_slices = 0, n_panels = 0, n_tpanels = 0, n_tables = 0;
+    // nodes
+    float *x = nullptr, *v = nullptr, *dv = nullptr, *mass = nullptr;
+    float4* handle = nullptr;
+    double* dv64 = nullptr;
+    float* warm = nullptr;   // warm-start vector (previous dv or learned prediction)
+    // faces
+    int4* face_nodes = nullptr;
+    float4* face_inv = nullptr;
+    float* face_area = nullptr;
+    float* face_rec = nullptr;
+    // edges
+    int4* edge_nodes = nullptr;
+    int* edge_meta = nullptr;
+    int* edge_sheet = nullptr;
+    float4* edge_par = nullptr;
+    float* edge_rec = nullptr;
+    // sheets, materials, topology
+    SheetDesc* sheets = nullptr;
+    float4* tables = nullptr;
+    SliceDesc* slices = nullptr;
+    int* tcol = nullptr;         // per topology panel: 32 local column ids
+    int* tcptr = nullptr;        // per topology slot: contributor range start (n_tpanels*32 + 1)
+    uint32_t* tcontrib = nullptr;
+    // system
+    float* A = nullptr;          // n_panels * 288
+    float* b = nullptr;          // 3N
+    float* Pinv = nullptr;       // 9N
+    // PCG
+    float *e = nullptr, *r = nullptr, *z = nullptr, *pA = nullptr, *pB = nullptr, *q = nullptr;
+    double* part = nullptr;      // 2 per slice
+    InstState* inst = nullptr;
+    DevParams* params = nullptr;
+    int* loop = nullptr;         // [0] loop trip counter, [1] instances not done
+};
+
+#endif

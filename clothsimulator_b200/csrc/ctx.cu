@@ -1,0 +1,1077 @@
+// Host runtime of the B200 implicit cloth step and its C ABI (include/clothstep.h).
+//
+// cs_load_batch turns a batch of cloths into the HBM layout of cs_internal.h:
+//   * edges in the reference's numbering (first appearance while walking the faces'
+//     corners, Mesh.cu:56-68, 385-395) with sides as Edge::initialize sets them
+//     (Edge.cu:13-31); only interior edges carry bending (Cloth.cu:140-154);
+//   * face rest data exactly as Face::initialize computes it (Face.cu:12-20), lumped node
+//     masses as Mesh::updateNodeGeometries sums them (Mesh.cu:190-200);
+//   * the fixed 3x3-block pattern of A (diagonal + face pairs + bending stencils) in SELL-32
+//     slices, and for every block its contributors in the reference's accumulation order,
+//     so the gather kernel reproduces Cloth::addMatrixAndVector's sums (Cloth.cu:42-76)
+//     without atomics.  Pattern, columns and contributor lists are built once per distinct
+//     topology and shared by every sheet that has it;
+//   * the 30^3 stretching tables (Material.cu:28-36) per distinct material and multiplier.
+// cs_step runs the whole step as one CUDA graph whose solve loop is a device-driven
+// conditional while node (no host round trip per iteration, unlike Cloth.cu:784-809).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/clothstep.h"
+#include "cs_internal.h"
+
+// kernels (forces.cu, pcg.cu)
+__global__ void cs_face_kernel(Batch B);
+__global__ void cs_edge_kernel(Batch B);
+__global__ void cs_gather_kernel(Batch B);
+__global__ void cs_expand_kernel(Batch B, float* face_f, float* face_J, float* edge_f, float* edge_J);
+__global__ void cs_spmv_kernel(Batch B);
+__global__ void cs_reduce1_kernel(Batch B);
+__global__ void cs_vector_kernel(Batch B);
+__global__ void cs_reduce2_kernel(Batch B, cudaGraphConditionalHandle handle);
+__global__ void cs_solve_prologue_kernel(Batch B);
+__global__ void cs_solve_setup_kernel(Batch B);
+__global__ void cs_advance_kernel(Batch B);
+__global__ void cs_spmv_plain_kernel(Batch B, const float* x, float* y);
+
+namespace {
+
+// ---------------------------------------------------------------------------------------
+// Material tables (Material.cu:3-85), host side, float arithmetic in the reference's order.
+
+void eigen2(float a, float b, float d, float Q[2][2], float l[2]) {  // MathHelper.cu:3-36
+    float amd = a - d, apd = a + d, b2 = b * b;
+    float det = std::sqrt(4.0f * b2 + amd * amd);
+    float l1 = 0.5f * (apd + det), l2 = 0.5f * (apd - det);
+    l[0] = l1;
+    l[1] = l2;
+    if (b != 0.0f) {
+        float v0 = l1 - d, v1 = b, vn = std::sqrt(v0 * v0 + b2);
+        Q[0][0] = v0 / vn;
+        Q[1][0] = v1 / vn;
+        v0 = l2 - d;
+        vn = std::sqrt(v0 * v0 + b2);
+        Q[0][1] = v0 / vn;
+        Q[1][1] = v1 / vn;
+    } else if (a >= d) {
+        Q[0][0] = 1.0f; Q[1][0] = 0.0f; Q[0][1] = 0.0f; Q[1][1] = 1.0f;
+    } else {
+        Q[0][0] = 0.0f; Q[1][0] = 1.0f; Q[0][1] = 1.0f; Q[1][1] = 0.0f;
+    }
+}
+
+float clampf(float x, float a, float b) { return x < a ? a : (x > b ? b : x); }
+
+// calculateStretchingSample (Material.cu:45-85); data[2][5][4] as built at Material.cu:20-27.
+void stretchingSample(float G00, float G01, float G11, const float data[2][5][4], float out[4]) {
+    float Q[2][2], l[2];
+    eigen2(2.0f * G00, 2.0f * G01, 2.0f * G11, Q, l);
+    if (l[0] == l[1] && Q[0][0] == 0.0f && Q[1][1] == 0.0f) {
+        Q[0][0] = 1.0f; Q[0][1] = 0.0f; Q[1][0] = 0.0f; Q[1][1] = 1.0f;
+    }
+    if (Q[0][0] < 0.0f) { Q[0][0] = -Q[0][0]; Q[1][0] = -Q[1][0]; }
+    if (Q[1][1] < 0.0f) { Q[0][1] = -Q[0][1]; Q[1][1] = -Q[1][1]; }
+    float strainWeight = (std::sqrt(l[0] + 1.0f) - 1.0f) * 6.0f;
+    strainWeight = clampf(strainWeight, 0.0f, 1.0f - 1e-6f);
+    int strainId = (int)strainWeight;
+    strainWeight -= strainId;
+    float q10 = Q[1][0], q00 = Q[0][0];
+    float at = std::atan2(q10, q00);
+    float angleWeight = (float)((double)(at < 0.0f ? -at : at) / M_PI * 8.0f);
+    angleWeight = clampf(angleWeight, 0.0f, 4.0f - 1e-6f);
+    int angleId = (int)angleWeight;
+    angleWeight -= angleId;
+    float w[2][2] = {{(1.0f - strainWeight) * (1.0f - angleWeight), (1.0f - strainWeight) * angleWeight},
+                     {strainWeight * (1.0f - angleWeight), strainWeight * angleWeight}};
+    float ans[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++)
+            for (int c = 0; c < 4; c++) ans[c] += data[strainId + i][angleId + j][c] * w[i][j];
+    for (int c = 0; c < 4; c++) out[c] = (ans[c] > 0.0f ? ans[c] : 0.0f) * 2.0f;
+}
+
+// Unscaled 30^3 samples of one material's stretching rows.
+std::vector<float> stretchingSamples(const float rows[6][4]) {
+    float data[2][5][4];
+    for (int c = 0; c < 4; c++) data[0][0][c] = rows[0][c];
+    for (int i = 1; i < 5; i++)
+        for (int c = 0; c < 4; c++) data[0][i][c] = data[0][0][c];
+    for (int i = 0; i < 5; i++)
+        for (int c = 0; c < 4; c++) data[1][i][c] = rows[i + 1][c];
+    std::vector<float> out(4 * CS_TABLE_ENTRIES);
+    for (int i = 0; i < CS_TABLE_N; i++)
+        for (int j = 0; j < CS_TABLE_N; j++)
+            for (int k = 0; k < CS_TABLE_N; k++) {
+                float G00 = (float)i / CS_TABLE_N - 0.25f;
+                float G11 = (float)j / CS_TABLE_N - 0.25f;
+                float G01 = (float)k / CS_TABLE_N;
+                stretchingSample(G00, G01, G11, data, &out[4 * ((i * CS_TABLE_N + j) * CS_TABLE_N + k)]);
+            }
+    return out;
+}
+
+// Bias weight of one uv edge after the fold and clamp of Material.cu:130-133.
+float biasWeight(float d0, float d1) {
+    float at = std::atan2(d1, d0);
+    float w = (float)((double)((at < 0.0f ? -at : at) * 4.0f) / M_PI);
+    if (w > 2.0f) w = 4.0f - w;
+    return clampf(w, 0.0f, 2.0f - 1e-6f);
+}
+
+// ---------------------------------------------------------------------------------------
+// Topology and pattern of one distinct mesh connectivity.
+
+struct Topo {
+    int n_nodes = 0, n_verts = 0, n_faces = 0;
+    std::vector<int> fx, fu;
+    // interior edges in reference order
+    std::vector<int> ie_nodes;  // 4 per: n0, n1, opposite node side 0, side 1
+    std::vector<int> ie_faces;  // 2 per
+    std::vector<int> ie_meta;   // rotations of the adjacent faces' vertex order
+    std::vector<int> ie_verts;  // 4 per: uv vertices [side][0..1]
+    // SELL-32 pattern
+    int n_slices = 0, n_tpanels = 0;
+    std::vector<int> slice_rows, slice_width, slice_tpanel0;
+    std::vector<int> tcol;                 // n_tpanels * 32 (local node ids)
+    std::vector<int> tcptr;                // n_tpanels * 32 + 1
+    std::vector<uint32_t> tcontrib;
+    // block-CSR view for cs_get_system: per row, columns sorted, and the SELL slot of each
+    std::vector<int> csr_ptr, csr_col, csr_slot;
+    long long nnzb = 0;
+};
+
+struct TopoKey {
+    int nn, nv, nf;
+    uint64_t h;
+    bool operator<(const TopoKey& o) const {
+        if (nn != o.nn) return nn < o.nn;
+        if (nv != o.nv) return nv < o.nv;
+        if (nf != o.nf) return nf < o.nf;
+        return h < o.h;
+    }
+};
+
+uint64_t hashInts(const int32_t* a, size_t n, uint64_t h) {
+    for (size_t i = 0; i < n; i++) {
+        h ^= (uint64_t)(uint32_t)a[i] + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2);
+    }
+    return h;
+}
+
+std::shared_ptr<Topo> buildTopo(const cs_sheet_desc& s, std::string& err) {
+    auto t = std::make_shared<Topo>();
+    const int nn = s.n_nodes, nv = s.n_verts, nf = s.n_faces;
+    t->n_nodes = nn;
+    t->n_verts = nv;
+    t->n_faces = nf;
+    t->fx.assign(s.face_nodes, s.face_nodes + 3 * nf);
+    t->fu.assign(s.face_verts, s.face_verts + 3 * nf);
+    for (int i = 0; i < 3 * nf; i++) {
+        if (t->fx[i] < 0 || t->fx[i] >= nn || t->fu[i] < 0 || t->fu[i] >= nv) {
+            err = "face index out of range";
+            return nullptr;
+        }
+    }
+    // Edges: first appearance order, nodes[0] < nodes[1]; sides per Edge::initialize.
+    std::unordered_map<uint64_t, int> map;
+    map.reserve(3 * (size_t)nf);
+    std::vector<int> eN, eF, eV, eO;
+    auto find = [&](int a, int b) {
+        if (a > b) std::swap(a, b);
+        uint64_t key = (uint64_t)(uint32_t)a << 32 | (uint32_t)b;
+        auto it = map.find(key);
+        if (it != map.end()) return it->second;
+        int id = (int)eN.size() / 2;
+        map.emplace(key, id);
+        eN.push_back(a); eN.push_back(b);
+        eF.push_back(-1); eF.push_back(-1);
+        for (int i = 0; i < 4; i++) eV.push_back(-1);
+        eO.push_back(-1); eO.push_back(-1);
+        return id;
+    };
+    auto init = [&](int e, int oppCorner, int f) {
+        for (int i = 0; i < 3; i++) {
+            int c0 = i, c1 = (i + 1) % 3;
+            int n0 = t->fx[3 * f + c0], n1 = t->fx[3 * f + c1];
+            if (eN[2 * e] == n0 && eN[2 * e + 1] == n1) {
+                eV[4 * e] = t->fu[3 * f + c0];
+                eV[4 * e + 1] = t->fu[3 * f + c1];
+                eO[2 * e] = 3 * f + oppCorner;
+                eF[2 * e] = f;
+                return;
+            } else if (eN[2 * e + 1] == n0 && eN[2 * e] == n1) {
+                eV[4 * e + 2] = t->fu[3 * f + c1];
+                eV[4 * e + 3] = t->fu[3 * f + c0];
+                eO[2 * e + 1] = 3 * f + oppCorner;
+                eF[2 * e + 1] = f;
+                return;
+            }
+        }
+    };
+    for (int f = 0; f < nf; f++) {
+        int a = t->fx[3 * f], b = t->fx[3 * f + 1], c = t->fx[3 * f + 2];
+        if (a == b || b == c || a == c) {
+            err = "degenerate face (repeated node)";
+            return nullptr;
+        }
+        int e0 = find(a, b), e1 = find(b, c), e2 = find(c, a);
+        init(e0, 2, f);
+        init(e1, 0, f);
+        init(e2, 1, f);
+    }
+    const int ne = (int)eN.size() / 2;
+    for (int e = 0; e < ne; e++) {
+        if (eF[2 * e] < 0 || eF[2 * e + 1] < 0) continue;
+        int n0 = eN[2 * e], n1 = eN[2 * e + 1];
+        int o0 = t->fx[eO[2 * e]], o1 = t->fx[eO[2 * e + 1]];
+        int f0 = eF[2 * e], f1 = eF[2 * e + 1];
+        // rotation r with fx[f][0] = (n0, n1, o0)[r] for face 0 and (n1, n0, o1)[r] for face 1
+        int ta[3] = {n0, n1, o0}, tb[3] = {n1, n0, o1};
+        int r0 = -1, r1 = -1;
+        for (int r = 0; r < 3; r++) {
+            if (ta[r] == t->fx[3 * f0] && ta[(r + 1) % 3] == t->fx[3 * f0 + 1]) r0 = r;
+            if (tb[r] == t->fx[3 * f1] && tb[(r + 1) % 3] == t->fx[3 * f1 + 1]) r1 = r;
+        }
+        if (r0 < 0 || r1 < 0) {
+            err = "inconsistent face orientation";
+            return nullptr;
+        }
+        t->ie_nodes.insert(t->ie_nodes.end(), {n0, n1, o0, o1});
+        t->ie_faces.insert(t->ie_faces.end(), {f0, f1});
+        t->ie_meta.push_back(r0 | (r1 << 2));
+        t->ie_verts.insert(t->ie_verts.end(), {eV[4 * e], eV[4 * e + 1], eV[4 * e + 2], eV[4 * e + 3]});
+    }
+    const int nie = (int)t->ie_meta.size();
+    if (nie >= (1 << 27) || nf >= (1 << 27)) {
+        err = "sheet too large for the contributor encoding";
+        return nullptr;
+    }
+
+    // Contributions per row in the reference's order: faces by index, then interior edges.
+    std::vector<int> cnt(nn + 1, 0);
+    for (int f = 0; f < nf; f++)
+        for (int a = 0; a < 3; a++) cnt[t->fx[3 * f + a] + 1] += 3;
+    for (int e = 0; e < nie; e++)
+        for (int a = 0; a < 4; a++) cnt[t->ie_nodes[4 * e + a] + 1] += 4;
+    for (int i = 0; i < nn; i++) cnt[i + 1] += cnt[i];
+    std::vector<uint64_t> rc(cnt[nn]);  // (col << 32) | code, per row, stable-sorted by col
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    for (int f = 0; f < nf; f++)
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                int i = t->fx[3 * f + a], j = t->fx[3 * f + b];
+                rc[fill[i]++] = ((uint64_t)(uint32_t)j << 32) | cs_code(0, f, a, b);
+            }
+    for (int e = 0; e < nie; e++)
+        for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) {
+                int i = t->ie_nodes[4 * e + a], j = t->ie_nodes[4 * e + b];
+                rc[fill[i]++] = ((uint64_t)(uint32_t)j << 32) | cs_code(1, e, a, b);
+            }
+    // per row: columns (diagonal first, then ascending) and contributor ranges
+    std::vector<std::vector<int>> rowCols(nn);
+    std::vector<std::vector<std::pair<int, int>>> rowRanges(nn);
+    for (int i = 0; i < nn; i++) {
+        auto beg = rc.begin() + cnt[i], end = rc.begin() + cnt[i + 1];
+        std::stable_sort(beg, end, [](uint64_t a, uint64_t b) { return (a >> 32) < (b >> 32); });
+        std::vector<int> cols;
+        std::vector<std::pair<int, int>> ranges;
+        cols.push_back(i);
+        ranges.push_back({0, 0});
+        for (int p = cnt[i]; p < cnt[i + 1];) {
+            int j = (int)(rc[p] >> 32);
+            int q = p;
+            while (q < cnt[i + 1] && (int)(rc[q] >> 32) == j) q++;
+            if (j == i)
+                ranges[0] = {p, q};
+            else {
+                cols.push_back(j);
+                ranges.push_back({p, q});
+            }
+            p = q;
+        }
+        rowCols[i] = std::move(cols);
+        rowRanges[i] = std::move(ranges);
+    }
+    // SELL-32 slices
+    t->n_slices = (nn + CS_SLICE - 1) / CS_SLICE;
+    int tp = 0;
+    for (int s = 0; s < t->n_slices; s++) {
+        int r0 = s * CS_SLICE, rows = std::min(CS_SLICE, nn - r0);
+        int w = 1;
+        for (int l = 0; l < rows; l++) w = std::max(w, (int)rowCols[r0 + l].size());
+        t->slice_rows.push_back(rows);
+        t->slice_width.push_back(w);
+        t->slice_tpanel0.push_back(tp);
+        tp += w;
+    }
+    t->n_tpanels = tp;
+    t->tcol.assign((size_t)tp * CS_SLICE, 0);
+    t->tcptr.assign((size_t)tp * CS_SLICE + 1, 0);
+    t->tcontrib.clear();
+    t->tcontrib.reserve(rc.size());
+    std::vector<int> slotOf;  // per (row, column position)
+    std::vector<int> rowSlotBase(nn + 1, 0);
+    for (int i = 0; i < nn; i++) rowSlotBase[i + 1] = rowSlotBase[i] + (int)rowCols[i].size();
+    slotOf.assign(rowSlotBase[nn], -1);
+    for (int s = 0; s < t->n_slices; s++) {
+        int r0 = s * CS_SLICE;
+        for (int k = 0; k < t->slice_width[s]; k++)
+            for (int l = 0; l < CS_SLICE; l++) {
+                size_t slot = (size_t)(t->slice_tpanel0[s] + k) * CS_SLICE + l;
+                t->tcptr[slot] = (int)t->tcontrib.size();
+                if (l < t->slice_rows[s]) {
+                    int i = r0 + l;
+                    if (k < (int)rowCols[i].size()) {
+                        t->tcol[slot] = rowCols[i][k];
+                        auto rg = rowRanges[i][k];
+                        for (int p = rg.first; p < rg.second; p++) t->tcontrib.push_back((uint32_t)(rc[p] & 0xffffffffu));
+                        slotOf[rowSlotBase[i] + k] = (int)slot;
+                    } else {
+                        t->tcol[slot] = i;  // padding: zero block on the diagonal column
+                    }
+                }
+            }
+    }
+    t->tcptr[(size_t)tp * CS_SLICE] = (int)t->tcontrib.size();
+    // block-CSR view
+    t->csr_ptr.assign(nn + 1, 0);
+    t->csr_col.clear();
+    t->csr_slot.clear();
+    for (int i = 0; i < nn; i++) {
+        std::vector<std::pair<int, int>> cs;
+        for (size_t k = 0; k < rowCols[i].size(); k++) cs.push_back({rowCols[i][k], slotOf[rowSlotBase[i] + k]});
+        std::sort(cs.begin(), cs.end());
+        for (auto& c : cs) {
+            t->csr_col.push_back(c.first);
+            t->csr_slot.push_back(c.second);
+        }
+        t->csr_ptr[i + 1] = (int)t->csr_col.size();
+    }
+    t->nnzb = (long long)t->csr_col.size();
+    return t;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+
+struct cs_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    Batch B;
+    bool loaded = false;
+    std::vector<void*> allocs;
+    // host copies needed by the inspection entry points
+    std::vector<SheetDesc> sheets;
+    std::vector<SliceDesc> slices;
+    std::vector<std::shared_ptr<Topo>> sheetTopo;
+    long long nnzb_pattern = 0;
+    // graph
+    cudaGraphExec_t graphExec = nullptr;
+    cudaGraph_t graph = nullptr;
+    DevParams hostParams{};
+    bool lastStepValid = false;
+};
+
+namespace {
+
+cs_status fail(cs_ctx* c, cs_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return st;
+}
+
+#define CS_CUDA(call)                                                                              \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail(c, CS_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+cs_status dalloc(cs_ctx* c, T** p, size_t count) {
+    if (count == 0) count = 1;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if (e != cudaSuccess) return fail(c, CS_ERR_CUDA, "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+    c->allocs.push_back(q);
+    *p = (T*)q;
+    return CS_OK;
+}
+
+template <class T>
+cs_status upload(cs_ctx* c, T** p, const std::vector<T>& h) {
+    cs_status st = dalloc(c, p, h.size());
+    if (st != CS_OK) return st;
+    if (!h.empty()) CS_CUDA(cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return CS_OK;
+}
+
+void freeBatch(cs_ctx* c) {
+    if (c->graphExec) cudaGraphExecDestroy(c->graphExec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graphExec = nullptr;
+    c->graph = nullptr;
+    for (void* p : c->allocs) cudaFree(p);
+    c->allocs.clear();
+    c->B = Batch();
+    c->loaded = false;
+    c->lastStepValid = false;
+}
+
+inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+void launchAssembly(cs_ctx* c) {
+    Batch& B = c->B;
+    if (B.F) cs_face_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B);
+    if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B);
+    cs_gather_kernel<<<nblk((long long)B.n_slices * 32, 128), 128, 0, c->stream>>>(B);
+}
+
+void launchSolvePrologue(cs_ctx* c) {
+    Batch& B = c->B;
+    cs_solve_setup_kernel<<<B.S, 128, 0, c->stream>>>(B);
+    cs_solve_prologue_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B);
+}
+
+void launchTrip(cs_ctx* c, cudaGraphConditionalHandle h) {
+    Batch& B = c->B;
+    int g = nblk((long long)B.n_slices * 32, 128);
+    cs_spmv_kernel<<<g, 128, 0, c->stream>>>(B);
+    cs_reduce1_kernel<<<B.S, 128, 0, c->stream>>>(B);
+    cs_vector_kernel<<<g, 128, 0, c->stream>>>(B);
+    cs_reduce2_kernel<<<B.S, 128, 0, c->stream>>>(B, h);
+}
+
+cs_status buildGraph(cs_ctx* c) {
+    if (c->graphExec) return CS_OK;
+    cudaGraph_t graph;
+    CS_CUDA(cudaGraphCreate(&graph, 0));
+    c->graph = graph;
+    // prelude: assembly + solve setup, captured into the graph
+    CS_CUDA(cudaStreamBeginCaptureToGraph(c->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    launchAssembly(c);
+    launchSolvePrologue(c);
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    CS_CUDA(cudaStreamGetCaptureInfo(c->stream, &cst, nullptr, nullptr, &deps, &ndeps));
+    std::vector<cudaGraphNode_t> prelude(deps, deps + ndeps);
+    CS_CUDA(cudaStreamEndCapture(c->stream, &graph));
+    // while loop over solve trips
+    cudaGraphConditionalHandle handle;
+    CS_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t loopNode;
+    CS_CUDA(cudaGraphAddNode(&loopNode, graph, prelude.data(), prelude.size(), &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CS_CUDA(cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    launchTrip(c, handle);
+    CS_CUDA(cudaStreamEndCapture(c->stream, &body));
+    // epilogue
+    CS_CUDA(cudaStreamBeginCaptureToGraph(c->stream, graph, &loopNode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
+    cs_advance_kernel<<<nblk(3LL * c->B.N, 256), 256, 0, c->stream>>>(c->B);
+    CS_CUDA(cudaStreamEndCapture(c->stream, &graph));
+    CS_CUDA(cudaGraphInstantiate(&c->graphExec, graph, 0));
+    return CS_OK;
+}
+
+DevParams toDev(const cs_step_params* p) {
+    DevParams d{};
+    d.dt = p->dt;
+    for (int i = 0; i < 3; i++) d.gravity[i] = p->gravity[i];
+    d.handle_stiffness = p->handle_stiffness;
+    d.tol = p->tol > 0 ? p->tol : 1e-6;
+    d.inner_tol = p->inner_tol > 0 ? p->inner_tol : 1e-4;
+    d.max_iters = p->max_iters > 0 ? p->max_iters : 2000;
+    d.sweep_cap = p->sweep_cap > 0 ? p->sweep_cap : (p->precision == CS_PREC_MIXED ? 1000000 : 20);
+    d.mixed = p->precision == CS_PREC_MIXED;
+    d.warm = p->warm_start != CS_WARM_ZERO;
+    d.loop_cap = 2 * d.max_iters + 256;
+    d.advance = p->advance;
+    return d;
+}
+
+}  // namespace
+
+extern "C" {
+
+cs_status cs_create(cs_ctx** out, int device) {
+    if (!out) return CS_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return CS_ERR_NO_DEVICE;
+    if (device < 0 || device >= n) return CS_ERR_INVALID_ARG;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return CS_ERR_NO_DEVICE;
+    if (prop.major != 10) return CS_ERR_NO_DEVICE;  // built for sm_100a only
+    auto* c = new cs_ctx();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        delete c;
+        return CS_ERR_CUDA;
+    }
+    *out = c;
+    return CS_OK;
+}
+
+cs_status cs_destroy(cs_ctx* c) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    freeBatch(c);
+    cudaEventDestroy(c->ev0);
+    cudaEventDestroy(c->ev1);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return CS_OK;
+}
+
+const char* cs_last_error(const cs_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, const cs_sheet_desc* sheets,
+                        int n_sheets) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!mats || n_mats <= 0 || !sheets || n_sheets <= 0) return fail(c, CS_ERR_INVALID_ARG, "empty batch");
+    CS_CUDA(cudaSetDevice(c->device));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    freeBatch(c);
+    // validate
+    long long N = 0, F = 0;
+    for (int s = 0; s < n_sheets; s++) {
+        const cs_sheet_desc& d = sheets[s];
+        if (d.n_nodes <= 0 || d.n_faces <= 0 || d.n_verts <= 0 || !d.x || !d.uv || !d.face_nodes || !d.face_verts)
+            return fail(c, CS_ERR_INVALID_ARG, "sheet %d: empty or missing arrays", s);
+        if (d.material < 0 || d.material >= n_mats) return fail(c, CS_ERR_INVALID_ARG, "sheet %d: bad material", s);
+        if (d.n_handles < 0 || (d.n_handles > 0 && !d.handle_nodes))
+            return fail(c, CS_ERR_INVALID_ARG, "sheet %d: bad handles", s);
+        for (int h = 0; h < d.n_handles; h++)
+            if (d.handle_nodes[h] < 0 || d.handle_nodes[h] >= d.n_nodes)
+                return fail(c, CS_ERR_INVALID_ARG, "sheet %d: handle node %d out of range", s, d.handle_nodes[h]);
+        for (int i = 0; i < 3 * d.n_nodes; i++)
+            if (!std::isfinite(d.x[i]) || (d.v && !std::isfinite(d.v[i])))
+                return fail(c, CS_ERR_INVALID_ARG, "sheet %d: non-finite node state", s);
+        N += d.n_nodes;
+        F += d.n_faces;
+    }
+    if (N >= (1LL << 31) / 9 || F >= (1LL << 31) / 32) return fail(c, CS_ERR_INVALID_ARG, "batch too large");
+
+    // topologies (shared)
+    std::map<TopoKey, int> topoIndex;
+    std::vector<std::shared_ptr<Topo>> topos;
+    c->sheetTopo.assign(n_sheets, nullptr);
+    std::vector<int> sheetTopoId(n_sheets);
+    for (int s = 0; s < n_sheets; s++) {
+        const cs_sheet_desc& d = sheets[s];
+        TopoKey k{d.n_nodes, d.n_verts, d.n_faces, 0};
+        k.h = hashInts(d.face_nodes, 3 * (size_t)d.n_faces, 1469598103934665603ULL);
+        k.h = hashInts(d.face_verts, 3 * (size_t)d.n_faces, k.h);
+        auto it = topoIndex.find(k);
+        if (it != topoIndex.end() &&
+            std::equal(d.face_nodes, d.face_nodes + 3 * d.n_faces, topos[it->second]->fx.begin()) &&
+            std::equal(d.face_verts, d.face_verts + 3 * d.n_faces, topos[it->second]->fu.begin())) {
+            sheetTopoId[s] = it->second;
+        } else {
+            std::string err;
+            auto t = buildTopo(d, err);
+            if (!t) return fail(c, CS_ERR_INVALID_ARG, "sheet %d: %s", s, err.c_str());
+            sheetTopoId[s] = (int)topos.size();
+            topoIndex[k] = (int)topos.size();
+            topos.push_back(t);
+        }
+        c->sheetTopo[s] = topos[sheetTopoId[s]];
+    }
+    // materials: scaled stretching tables per distinct (rows, multiplier)
+    std::map<std::vector<float>, std::vector<float>> baseSamples;
+    std::map<std::vector<float>, int> tableIndex;
+    std::vector<float4> tables;
+    std::vector<int> sheetTable(n_sheets);
+    for (int s = 0; s < n_sheets; s++) {
+        const cs_material_desc& m = mats[sheets[s].material];
+        std::vector<float> rows(&m.stretching[0][0], &m.stretching[0][0] + 24);
+        float smult = m.stretching_mult * m.thicken;
+        std::vector<float> key = rows;
+        key.push_back(smult);
+        auto it = tableIndex.find(key);
+        if (it != tableIndex.end()) {
+            sheetTable[s] = it->second;
+            continue;
+        }
+        auto bt = baseSamples.find(rows);
+        if (bt == baseSamples.end()) bt = baseSamples.emplace(rows, stretchingSamples(m.stretching)).first;
+        int id = (int)(tables.size() / CS_TABLE_ENTRIES);
+        tableIndex[key] = id;
+        sheetTable[s] = id;
+        const std::vector<float>& b = bt->second;
+        for (int i = 0; i < CS_TABLE_ENTRIES; i++)
+            tables.push_back(make_float4(b[4 * i] * smult, b[4 * i + 1] * smult, b[4 * i + 2] * smult, b[4 * i + 3] * smult));
+    }
+
+    // per-sheet arrays
+    Batch& B = c->B;
+    std::vector<float> hx, hv, hmass;
+    std::vector<float4> hhandle, hface_inv, hedge_par;
+    std::vector<int4> hface_nodes, hedge_nodes;
+    std::vector<float> hface_area;
+    std::vector<int> hedge_meta, hedge_sheet;
+    std::vector<SheetDesc> hs(n_sheets);
+    std::vector<SliceDesc> hslices;
+    // per-topology arrays, concatenated
+    std::vector<int> htcol, htcptr;
+    std::vector<uint32_t> htcontrib;
+    std::vector<int> topoPanel0(topos.size()), topoSlice0(topos.size());
+    {
+        int tp = 0, ts = 0;
+        for (size_t t = 0; t < topos.size(); t++) {
+            topoPanel0[t] = tp;
+            topoSlice0[t] = ts;
+            const Topo& T = *topos[t];
+            int cbase = (int)htcontrib.size();
+            htcol.insert(htcol.end(), T.tcol.begin(), T.tcol.end());
+            for (size_t i = 0; i + 1 < T.tcptr.size(); i++) htcptr.push_back(T.tcptr[i] + cbase);
+            htcontrib.insert(htcontrib.end(), T.tcontrib.begin(), T.tcontrib.end());
+            tp += T.n_tpanels;
+            ts += T.n_slices;
+        }
+        htcptr.push_back((int)htcontrib.size());
+    }
+    int node_off = 0, face_off = 0, edge_off = 0, slice_off = 0, panel_off = 0;
+    long long nnzb = 0;
+    for (int s = 0; s < n_sheets; s++) {
+        const cs_sheet_desc& d = sheets[s];
+        const cs_material_desc& m = mats[d.material];
+        const Topo& T = *topos[sheetTopoId[s]];
+        SheetDesc& sd = hs[s];
+        sd.node_off = node_off;
+        sd.n_nodes = d.n_nodes;
+        sd.face_off = face_off;
+        sd.n_faces = d.n_faces;
+        sd.edge_off = edge_off;
+        sd.n_edges = (int)T.ie_meta.size();
+        sd.slice_off = slice_off;
+        sd.n_slices = T.n_slices;
+        sd.topo = sheetTopoId[s];
+        sd.table = sheetTable[s];
+        float bmult = m.bending_mult * m.thicken;
+        for (int i = 0; i < 15; i++) sd.bending[i] = m.bending[i / 5][i % 5] * bmult;
+        sd.wind_density = d.wind_density;
+        sd.wind_drag = d.wind_drag;
+        for (int i = 0; i < 3; i++) sd.wind_v[i] = d.wind_velocity[i];
+        float density = m.density * (m.density_mult * m.thicken);
+        // nodes
+        for (int i = 0; i < 3 * d.n_nodes; i++) {
+            hx.push_back(d.x[i]);
+            hv.push_back(d.v ? d.v[i] : 0.0f);
+        }
+        // faces: Face::initialize (Face.cu:12-20)
+        std::vector<float> fmass(d.n_faces);
+        for (int f = 0; f < d.n_faces; f++) {
+            const float* u0 = d.uv + 2 * d.face_verts[3 * f];
+            const float* u1 = d.uv + 2 * d.face_verts[3 * f + 1];
+            const float* u2 = d.uv + 2 * d.face_verts[3 * f + 2];
+            float d1x = u1[0] - u0[0], d1y = u1[1] - u0[1], d2x = u2[0] - u0[0], d2y = u2[1] - u0[1];
+            float a = d1x, b = d2x, cc = d1y, dd = d2y;
+            float invDet = 1.0f / (a * dd - b * cc);
+            float4 inv = make_float4(dd * invDet, -b * invDet, -cc * invDet, a * invDet);
+            float cr = d1x * d2y - d1y * d2x;
+            float area = 0.5f * (cr < 0.0f ? -cr : cr);
+            if (!(area > 0.0f)) return fail(c, CS_ERR_INVALID_ARG, "sheet %d face %d: zero rest area", s, f);
+            hface_inv.push_back(inv);
+            hface_area.push_back(area);
+            fmass[f] = area * density;
+            hface_nodes.push_back(make_int4(node_off + d.face_nodes[3 * f], node_off + d.face_nodes[3 * f + 1],
+                                            node_off + d.face_nodes[3 * f + 2], s));
+        }
+        // lumped mass (Mesh.cu:190-200)
+        std::vector<float> mass(d.n_nodes, 0.0f);
+        for (int f = 0; f < d.n_faces; f++) {
+            float mm = fmass[f] / 3.0f;
+            for (int k = 0; k < 3; k++) mass[d.face_nodes[3 * f + k]] += mm;
+        }
+        hmass.insert(hmass.end(), mass.begin(), mass.end());
+        // handles
+        std::vector<float4> hd(d.n_nodes, make_float4(0.f, 0.f, 0.f, 0.f));
+        for (int h = 0; h < d.n_handles; h++) {
+            int i = d.handle_nodes[h];
+            const float* p = d.handle_pos ? d.handle_pos + 3 * h : d.x + 3 * i;
+            hd[i] = make_float4(p[0], p[1], p[2], hd[i].w + 1.0f);
+        }
+        hhandle.insert(hhandle.end(), hd.begin(), hd.end());
+        // interior edges
+        for (size_t e = 0; e < T.ie_meta.size(); e++) {
+            const int* n4 = &T.ie_nodes[4 * e];
+            hedge_nodes.push_back(make_int4(node_off + n4[0], node_off + n4[1], node_off + n4[2], node_off + n4[3]));
+            hedge_meta.push_back(T.ie_meta[e]);
+            hedge_sheet.push_back(s);
+            int f0 = T.ie_faces[2 * e], f1 = T.ie_faces[2 * e + 1];
+            float area = hface_area[face_off + f0] + hface_area[face_off + f1];
+            const int* ev = &T.ie_verts[4 * e];
+            float b0 = biasWeight(d.uv[2 * ev[1]] - d.uv[2 * ev[0]], d.uv[2 * ev[1] + 1] - d.uv[2 * ev[0] + 1]);
+            float b1 = biasWeight(d.uv[2 * ev[3]] - d.uv[2 * ev[2]], d.uv[2 * ev[3] + 1] - d.uv[2 * ev[2] + 1]);
+            hedge_par.push_back(make_float4(area, b0, b1, 0.0f));
+        }
+        // slices
+        for (int t = 0; t < T.n_slices; t++) {
+            SliceDesc sl{};
+            sl.sheet = s;
+            sl.topo_slice = topoSlice0[sheetTopoId[s]] + t;
+            sl.row0 = node_off + t * CS_SLICE;
+            sl.rows = T.slice_rows[t];
+            sl.width = T.slice_width[t];
+            sl.panel0 = panel_off + T.slice_tpanel0[t];
+            sl.tpanel0 = topoPanel0[sheetTopoId[s]] + T.slice_tpanel0[t];
+            hslices.push_back(sl);
+        }
+        node_off += d.n_nodes;
+        face_off += d.n_faces;
+        edge_off += (int)T.ie_meta.size();
+        slice_off += T.n_slices;
+        panel_off += T.n_tpanels;
+        nnzb += T.nnzb;
+    }
+    B.N = node_off;
+    B.F = face_off;
+    B.E = edge_off;
+    B.S = n_sheets;
+    B.n_slices = slice_off;
+    B.n_panels = panel_off;
+    B.n_tpanels = (int)(htcol.size() / CS_SLICE);
+    B.n_tables = (int)(tables.size() / CS_TABLE_ENTRIES);
+    c->nnzb_pattern = nnzb;
+    c->sheets = hs;
+    c->slices = hslices;
+
+    cs_status st;
+#define UP(field, vec) \
+    if ((st = upload(c, &B.field, vec)) != CS_OK) return st;
+    UP(x, hx);
+    UP(v, hv);
+    UP(mass, hmass);
+    UP(handle, hhandle);
+    UP(face_nodes, hface_nodes);
+    UP(face_inv, hface_inv);
+    UP(face_area, hface_area);
+    UP(edge_nodes, hedge_nodes);
+    UP(edge_meta, hedge_meta);
+    UP(edge_sheet, hedge_sheet);
+    UP(edge_par, hedge_par);
+    UP(sheets, hs);
+    UP(tables, tables);
+    UP(slices, hslices);
+    UP(tcol, htcol);
+    UP(tcptr, htcptr);
+    UP(tcontrib, htcontrib);
+#undef UP
+#define AL(field, n) \
+    if ((st = dalloc(c, &B.field, (size_t)(n))) != CS_OK) return st;
+    AL(dv, 3LL * B.N);
+    AL(dv64, 3LL * B.N);
+    AL(warm, 3LL * B.N);
+    AL(face_rec, (long long)B.F * CS_FACE_REC);
+    AL(edge_rec, (long long)std::max(B.E, 1) * CS_EDGE_REC);
+    AL(A, (long long)B.n_panels * CS_PANEL_FLOATS);
+    AL(b, 3LL * B.N);
+    AL(Pinv, 9LL * B.N);
+    AL(e, 3LL * B.N);
+    AL(r, 3LL * B.N);
+    AL(z, 3LL * B.N);
+    AL(pA, 3LL * B.N);
+    AL(pB, 3LL * B.N);
+    AL(q, 3LL * B.N);
+    AL(part, 2LL * B.n_slices);
+    AL(inst, B.S);
+    AL(params, 1);
+    AL(loop, 4);
+#undef AL
+    CS_CUDA(cudaMemset(B.dv, 0, 3LL * B.N * sizeof(float)));
+    CS_CUDA(cudaMemset(B.warm, 0, 3LL * B.N * sizeof(float)));
+    CS_CUDA(cudaMemset(B.A, 0, (size_t)B.n_panels * CS_PANEL_FLOATS * sizeof(float)));
+    CS_CUDA(cudaMemset(B.inst, 0, B.S * sizeof(InstState)));
+    CS_CUDA(cudaMemset(B.loop, 0, 4 * sizeof(int)));
+    CS_CUDA(cudaDeviceSynchronize());
+    c->loaded = true;
+    return CS_OK;
+}
+
+cs_status cs_get_sizes(const cs_ctx* c, long long* sizes) {
+    if (!c || !sizes) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return CS_ERR_STATE;
+    sizes[0] = c->B.N;
+    sizes[1] = c->B.F;
+    sizes[2] = c->B.E;
+    sizes[3] = (long long)c->B.n_panels * CS_SLICE;
+    sizes[4] = c->B.n_slices;
+    sizes[5] = c->B.S;
+    sizes[6] = c->nnzb_pattern;
+    return CS_OK;
+}
+
+cs_status cs_set_state(cs_ctx* c, const float* x, const float* v) {
+    if (!c || (!x && !v)) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    size_t n = 3 * (size_t)c->B.N * sizeof(float);
+    if (x) CS_CUDA(cudaMemcpyAsync(c->B.x, x, n, cudaMemcpyHostToDevice, c->stream));
+    if (v) CS_CUDA(cudaMemcpyAsync(c->B.v, v, n, cudaMemcpyHostToDevice, c->stream));
+    return CS_OK;
+}
+
+cs_status cs_get_state(cs_ctx* c, float* x, float* v) {
+    if (!c || (!x && !v)) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    size_t n = 3 * (size_t)c->B.N * sizeof(float);
+    if (x) CS_CUDA(cudaMemcpyAsync(x, c->B.x, n, cudaMemcpyDeviceToHost, c->stream));
+    if (v) CS_CUDA(cudaMemcpyAsync(v, c->B.v, n, cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+cs_status cs_set_state_device(cs_ctx* c, const float* x, const float* v) {
+    if (!c || (!x && !v)) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    size_t n = 3 * (size_t)c->B.N * sizeof(float);
+    if (x) CS_CUDA(cudaMemcpyAsync(c->B.x, x, n, cudaMemcpyDeviceToDevice, c->stream));
+    if (v) CS_CUDA(cudaMemcpyAsync(c->B.v, v, n, cudaMemcpyDeviceToDevice, c->stream));
+    return CS_OK;
+}
+
+cs_status cs_get_state_device(cs_ctx* c, float* x, float* v) {
+    if (!c || (!x && !v)) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    size_t n = 3 * (size_t)c->B.N * sizeof(float);
+    if (x) CS_CUDA(cudaMemcpyAsync(x, c->B.x, n, cudaMemcpyDeviceToDevice, c->stream));
+    if (v) CS_CUDA(cudaMemcpyAsync(v, c->B.v, n, cudaMemcpyDeviceToDevice, c->stream));
+    return CS_OK;
+}
+
+cs_status cs_device_pointers(cs_ctx* c, float** x, float** v, float** dv) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    if (x) *x = c->B.x;
+    if (v) *v = c->B.v;
+    if (dv) *dv = c->B.dv;
+    return CS_OK;
+}
+
+static cs_status validateParams(cs_ctx* c, const cs_step_params* p) {
+    if (!p) return fail(c, CS_ERR_INVALID_ARG, "null params");
+    if (!(p->dt > 0.0f) || !std::isfinite(p->dt)) return fail(c, CS_ERR_INVALID_ARG, "dt must be positive");
+    if (!std::isfinite(p->handle_stiffness) || p->handle_stiffness < 0) return fail(c, CS_ERR_INVALID_ARG, "bad handle stiffness");
+    for (int i = 0; i < 3; i++)
+        if (!std::isfinite(p->gravity[i])) return fail(c, CS_ERR_INVALID_ARG, "bad gravity");
+    if (p->precision != CS_PREC_PLAIN_FP32 && p->precision != CS_PREC_MIXED) return fail(c, CS_ERR_INVALID_ARG, "bad precision");
+    if (p->warm_start < CS_WARM_ZERO || p->warm_start > CS_WARM_GIVEN) return fail(c, CS_ERR_INVALID_ARG, "bad warm start");
+    if (p->warm_start == CS_WARM_LEARNED) return fail(c, CS_ERR_NOT_TRAINED, "learned warm start: no trained network");
+    return CS_OK;
+}
+
+cs_status cs_assemble(cs_ctx* c, const cs_step_params* p) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    cs_status st = validateParams(c, p);
+    if (st != CS_OK) return st;
+    CS_CUDA(cudaSetDevice(c->device));
+    DevParams d = toDev(p);
+    CS_CUDA(cudaMemcpyAsync(c->B.params, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
+    launchAssembly(c);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    cs_status st = validateParams(c, p);
+    if (st != CS_OK) return st;
+    CS_CUDA(cudaSetDevice(c->device));
+    DevParams d = toDev(p);
+    c->hostParams = d;
+    CS_CUDA(cudaMemcpyAsync(c->B.params, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
+    CS_CUDA(cudaEventRecord(c->ev0, c->stream));
+    if (p->use_graph) {
+        if ((st = buildGraph(c)) != CS_OK) return st;
+        CS_CUDA(cudaGraphLaunch(c->graphExec, c->stream));
+    } else {
+        launchAssembly(c);
+        launchSolvePrologue(c);
+        int go = 1;
+        int trips = 0;
+        while (go) {
+            for (int t = 0; t < 8; t++) launchTrip(c, 0);
+            trips += 8;
+            CS_CUDA(cudaMemcpyAsync(&go, c->B.loop + 3, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            CS_CUDA(cudaStreamSynchronize(c->stream));
+            if (trips > d.loop_cap + 16) break;
+        }
+        cs_advance_kernel<<<nblk(3LL * c->B.N, 256), 256, 0, c->stream>>>(c->B);
+    }
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaEventRecord(c->ev1, c->stream));
+    c->lastStepValid = true;
+    if (!stats) return CS_OK;
+    std::vector<InstState> inst(c->B.S);
+    int loopv[4];
+    CS_CUDA(cudaMemcpyAsync(inst.data(), c->B.inst, c->B.S * sizeof(InstState), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaMemcpyAsync(loopv, c->B.loop, sizeof(loopv), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    memset(stats, 0, sizeof(*stats));
+    stats->n_instances = c->B.S;
+    stats->loop_trips = loopv[0];
+    bool capped = false, breakdown = false;
+    for (int s = 0; s < c->B.S; s++) {
+        const InstState& I = inst[s];
+        stats->converged += (I.flags & CS_IF_CONVERGED) ? 1 : 0;
+        stats->max_iters = std::max(stats->max_iters, I.iters);
+        stats->total_iters += I.iters;
+        stats->max_sweeps = std::max(stats->max_sweeps, I.sweeps);
+        stats->warm_rejected += (I.flags & CS_IF_WARM_REJECTED) ? 1 : 0;
+        double bn = std::sqrt(I.bnorm2);
+        double rel = bn > 0 ? I.resnorm / bn : 0.0;
+        stats->max_rel_residual = std::max(stats->max_rel_residual, rel);
+        if (!(I.flags & CS_IF_CONVERGED)) capped = true;
+        if (I.flags & CS_IF_BREAKDOWN) breakdown = true;
+    }
+    float ms = 0.f;
+    CS_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    stats->ms = ms;
+    if (loopv[0] >= d.loop_cap) return fail(c, CS_ERR_TIMEOUT, "solve loop hit its trip bound (%d)", d.loop_cap);
+    if (capped) return fail(c, breakdown ? CS_ERR_NON_SPD : CS_ERR_NOT_CONVERGED, "%d of %d sheets did not converge",
+                            c->B.S - stats->converged, c->B.S);
+    return CS_OK;
+}
+
+cs_status cs_sync(cs_ctx* c) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+cs_status cs_set_warm_start(cs_ctx* c, const float* dv) {
+    if (!c || !dv) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    CS_CUDA(cudaMemcpyAsync(c->B.warm, dv, 3 * (size_t)c->B.N * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    return CS_OK;
+}
+
+cs_status cs_get_dv(cs_ctx* c, float* dv) {
+    if (!c || !dv) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    CS_CUDA(cudaMemcpyAsync(dv, c->B.dv, 3 * (size_t)c->B.N * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
+cs_status cs_get_instance_stats(cs_ctx* c, int* iters, double* rel, int* flags) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->loaded || !c->lastStepValid) return fail(c, CS_ERR_STATE, "no step run");
+    std::vector<InstState> inst(c->B.S);
+    CS_CUDA(cudaMemcpyAsync(inst.data(), c->B.inst, c->B.S * sizeof(InstState), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    for (int s = 0; s < c->B.S; s++) {
+        if (iters) iters[s] = inst[s].iters;
+        double bn = std::sqrt(inst[s].bnorm2);
+        if (rel) rel[s] = bn > 0 ? inst[s].resnorm / bn : 0.0;
+        if (flags) flags[s] = inst[s].flags;
+    }
+    return CS_OK;
+}
+
+cs_status cs_get_system(cs_ctx* c, int32_t* row_ptr, int32_t* col, float* val, float* b) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    const Batch& B = c->B;
+    std::vector<float> A((size_t)B.n_panels * CS_PANEL_FLOATS);
+    CS_CUDA(cudaMemcpy(A.data(), B.A, A.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    if (b) CS_CUDA(cudaMemcpy(b, B.b, 3 * (size_t)B.N * sizeof(float), cudaMemcpyDeviceToHost));
+    long long pos = 0;
+    int rowBase = 0;
+    if (row_ptr) row_ptr[0] = 0;
+    for (int s = 0; s < B.S; s++) {
+        const Topo& T = *c->sheetTopo[s];
+        const SheetDesc& sd = c->sheets[s];
+        int panelBase = c->slices[sd.slice_off].panel0 - T.slice_tpanel0[0];
+        for (int i = 0; i < T.n_nodes; i++) {
+            for (int p = T.csr_ptr[i]; p < T.csr_ptr[i + 1]; p++) {
+                int slot = T.csr_slot[p];
+                int lane = slot % CS_SLICE, panel = panelBase + slot / CS_SLICE;
+                const float* P = A.data() + (size_t)panel * CS_PANEL_FLOATS;
+                if (col) col[pos] = rowBase + T.csr_col[p];
+                if (val) {
+                    float* o = val + 9 * pos;
+                    for (int t = 0; t < 4; t++) o[t] = P[4 * lane + t];
+                    for (int t = 0; t < 4; t++) o[4 + t] = P[128 + 4 * lane + t];
+                    o[8] = P[256 + lane];
+                }
+                pos++;
+            }
+            if (row_ptr) row_ptr[rowBase + i + 1] = (int32_t)pos;
+        }
+        rowBase += T.n_nodes;
+    }
+    return CS_OK;
+}
+
+cs_status cs_get_element_forces(cs_ctx* c, float* face_f, float* face_J, float* edge_f, float* edge_J,
+                                int32_t* edge_nodes) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    const Batch& B = c->B;
+    float *dff = nullptr, *dfJ = nullptr, *def = nullptr, *deJ = nullptr;
+    CS_CUDA(cudaMalloc(&dff, 9 * (size_t)B.F * sizeof(float)));
+    CS_CUDA(cudaMalloc(&dfJ, 81 * (size_t)B.F * sizeof(float)));
+    CS_CUDA(cudaMalloc(&def, 12 * (size_t)std::max(B.E, 1) * sizeof(float)));
+    CS_CUDA(cudaMalloc(&deJ, 144 * (size_t)std::max(B.E, 1) * sizeof(float)));
+    cs_expand_kernel<<<nblk(std::max(B.F, B.E), 128), 128, 0, c->stream>>>(B, dff, dfJ, def, deJ);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess && face_f) e = cudaMemcpy(face_f, dff, 9 * (size_t)B.F * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && face_J) e = cudaMemcpy(face_J, dfJ, 81 * (size_t)B.F * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && edge_f) e = cudaMemcpy(edge_f, def, 12 * (size_t)B.E * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && edge_J) e = cudaMemcpy(edge_J, deJ, 144 * (size_t)B.E * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && edge_nodes) e = cudaMemcpy(edge_nodes, B.edge_nodes, 16 * (size_t)B.E, cudaMemcpyDeviceToHost);
+    cudaFree(dff);
+    cudaFree(dfJ);
+    cudaFree(def);
+    cudaFree(deJ);
+    if (e != cudaSuccess) return fail(c, CS_ERR_CUDA, "element force readback: %s", cudaGetErrorString(e));
+    return CS_OK;
+}
+
+cs_status cs_spmv(cs_ctx* c, const float* x, float* y) {
+    if (!c || !x || !y) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    size_t n = 3 * (size_t)c->B.N * sizeof(float);
+    float *dx = nullptr, *dy = nullptr;
+    CS_CUDA(cudaMalloc(&dx, n));
+    CS_CUDA(cudaMalloc(&dy, n));
+    cudaError_t e = cudaMemcpy(dx, x, n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        cs_spmv_plain_kernel<<<nblk((long long)c->B.n_slices * 32, 128), 128, 0, c->stream>>>(c->B, dx, dy);
+        e = cudaStreamSynchronize(c->stream);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(y, dy, n, cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(dy);
+    if (e != cudaSuccess) return fail(c, CS_ERR_CUDA, "spmv: %s", cudaGetErrorString(e));
+    return CS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,517 @@
+// Element kernels of the implicit step and the deterministic block assembly.
+//
+// Compiled with -fmad=false: every expression below follows the reference's FP32 operation
+// order (PhysicsHelper.cu:264-353, Material.cu:91-156, Face.cu:109-132, Edge.cu:101-111,
+// Cloth.cu:42-169) without fused multiply-adds, so the assembled system matches the
+// reference's CPU assembly entry by entry.
+//
+// Kernels:
+//   cs_face_kernel   one thread per face: normal, wind drag, stretching force and the data
+//                    that determines its 9x9 Jacobian, and the face's right-hand-side terms.
+//   cs_edge_kernel   one thread per interior edge: dihedral bending force, the rank-one
+//                    Jacobian factors (dtheta, coefficient) and the edge's right-hand side.
+//   cs_gather_kernel one warp per 32-row slice: every block (i, j) of A sums its
+//                    contributors in the reference's order (mass, faces by index, edges by
+//                    index, handles) from a precomputed per-topology list: no atomics, no
+//                    sort, bit-reproducible.  Diagonal slots also produce b, the 3x3
+//                    block-Jacobi inverse and the slice's ||b||^2.
+#include "cs_internal.h"
+
+namespace {
+
+struct f3 {
+    float x, y, z;
+};
+__device__ __forceinline__ f3 mk(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ f3 ld3(const float* p, int i) { return mk(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+__device__ __forceinline__ f3 sub(f3 a, f3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ f3 add(f3 a, f3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ f3 scl(float s, f3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ f3 mulv(f3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+// Vector.cuh operator/ multiplies by the reciprocal.
+__device__ __forceinline__ f3 dvd(f3 a, float s) {
+    float inv = 1.0f / s;
+    return mk(a.x * inv, a.y * inv, a.z * inv);
+}
+__device__ __forceinline__ float dot(f3 a, f3 b) {
+    float s = a.x * b.x;
+    s += a.y * b.y;
+    s += a.z * b.z;
+    return s;
+}
+__device__ __forceinline__ float nrm(f3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ f3 normalized(f3 a) { return dvd(a, nrm(a)); }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float clampf_(float x, float a, float b) { return x < a ? a : (x > b ? b : x); }
+__device__ __forceinline__ float maxf_(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float minf_(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float absf_(float a) { return a < 0.0f ? -a : a; }
+
+// Material::stretchingStiffness (Material.cu:91-124): trilinear lookup on the 30^3 table.
+__device__ __forceinline__ float4 stretch_stiffness(const float4* __restrict__ T, float G00, float G01, float G11) {
+    const float hi = (float)(CS_TABLE_N - 1) - 1e-6f;
+    float x = (G00 + 0.25f) * (float)CS_TABLE_N;
+    x = clampf_(x, 0.0f, hi);
+    int xi = (int)x;
+    x -= xi;
+    float y = (G11 + 0.25f) * (float)CS_TABLE_N;
+    y = clampf_(y, 0.0f, hi);
+    int yi = (int)y;
+    y -= yi;
+    float z = absf_(G01) * (float)CS_TABLE_N;
+    z = clampf_(z, 0.0f, hi);
+    int zi = (int)z;
+    z -= zi;
+    float w[8];
+    w[0] = (1.0f - x) * (1.0f - y) * (1.0f - z);
+    w[1] = (1.0f - x) * (1.0f - y) * z;
+    w[2] = (1.0f - x) * y * (1.0f - z);
+    w[3] = (1.0f - x) * y * z;
+    w[4] = x * (1.0f - y) * (1.0f - z);
+    w[5] = x * (1.0f - y) * z;
+    w[6] = x * y * (1.0f - z);
+    w[7] = x * y * z;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+        int i = t >> 2, j = (t >> 1) & 1, k = t & 1;
+        float4 s = __ldg(&T[((xi + i) * CS_TABLE_N + (yi + j)) * CS_TABLE_N + (zi + k)]);
+        a.x += s.x * w[t];
+        a.y += s.y * w[t];
+        a.z += s.z * w[t];
+        a.w += s.w * w[t];
+    }
+    return a;
+}
+
+// Material::bendingStiffness (Material.cu:126-156).  bias is the side's bias weight after
+// the fold and clamp of Material.cu:130-133, precomputed from the rest uv edge.
+__device__ __forceinline__ float bend_stiffness(const float* __restrict__ samples, float length, float angle,
+                                                float area, float bias) {
+    float curv = length * angle / area;
+    float alpha = 0.5f * curv;
+    float biasWeight = bias;
+    int biasId = (int)biasWeight;
+    biasWeight -= biasId;
+    float valueWeight = 0.2f * alpha;
+    valueWeight = minf_(valueWeight, 4.0f - 1e-6f);
+    int valueId = (int)valueWeight;
+    valueId = valueId > 0 ? valueId : 0;
+    valueWeight -= valueId;
+    float w00 = (1.0f - biasWeight) * (1.0f - valueWeight);
+    float w01 = (1.0f - biasWeight) * valueWeight;
+    float w10 = biasWeight * (1.0f - valueWeight);
+    float w11 = biasWeight * valueWeight;
+    float ans = 0.0f;
+    ans += samples[biasId * 5 + valueId] * w00;
+    ans += samples[biasId * 5 + valueId + 1] * w01;
+    ans += samples[(biasId + 1) * 5 + valueId] * w10;
+    ans += samples[(biasId + 1) * 5 + valueId + 1] * w11;
+    return maxf_(ans, 0.0f);
+}
+
+// One entry h(p, q) of the stretching Hessian (PhysicsHelper.cu:283-286) with the
+// reference's expression order.  p = 3a + kp, q = 3b + kq; fu_p = fu[kp], fv_p = fv[kp],
+// D0a = D(0, a), D1a = D(1, a) and likewise for q; same = (kp == kq).
+__device__ __forceinline__ float stretch_h(float fu_p, float fv_p, float fu_q, float fv_q, float D0a, float D1a,
+                                           float D0b, float D1b, float k0, float k1, float k2, float k3, float gu,
+                                           float gv, bool same) {
+    float fuu_p = D0a * fu_p, fvv_p = D1a * fv_p, fuv_p = 0.5f * (D0a * fv_p + D1a * fu_p);
+    float fuu_q = D0b * fu_q, fvv_q = D1b * fv_q, fuv_q = 0.5f * (D0b * fv_q + D1b * fu_q);
+    float guDuu = same ? (gu * D0a) * D0b : 0.0f;
+    float gvDvv = same ? (gv * D1a) * D1b : 0.0f;
+    float guDvv = same ? (gu * D1a) * D1b : 0.0f;
+    float gvDuu = same ? (gv * D0a) * D0b : 0.0f;
+    float h = k0 * (fuu_p * fuu_q + guDuu);
+    h += k2 * (fvv_p * fvv_q + gvDvv);
+    h += k1 * (fuu_p * fvv_q + guDvv + fvv_p * fuu_q + gvDuu);
+    h += 2.0f * k3 * (fuv_p * fuv_q);
+    return h;
+}
+
+__device__ __forceinline__ float sel3(float a, float b, float c, int i) { return i == 0 ? a : (i == 1 ? b : c); }
+
+}  // namespace
+
+// Face record (32 floats): [0..2] fu, [3..5] fv, [6..8] D row 0, [9..11] D row 1,
+// [12..15] stiffness k, [16] max(G00,0), [17] max(G11,0), [18] rest area,
+// [20..28] dt*(f + dt*J*v) of the stretching term, [29..31] dt * wind force per node.
+__global__ void __launch_bounds__(128) cs_face_kernel(Batch B) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= B.F) return;
+    const DevParams& P = *B.params;
+    const float dt = P.dt;
+    int4 fn = B.face_nodes[f];
+    const SheetDesc& sh = B.sheets[fn.w];
+    f3 x0 = ld3(B.x, fn.x), x1 = ld3(B.x, fn.y), x2 = ld3(B.x, fn.z);
+    f3 v0 = ld3(B.v, fn.x), v1 = ld3(B.v, fn.y), v2 = ld3(B.v, fn.z);
+    float area = B.face_area[f];
+    float4 inv = B.face_inv[f];  // (00, 01, 10, 11)
+
+    // Face::update (Face.cu:124-127): normal from the current positions.
+    f3 e1 = sub(x1, x0), e2 = sub(x2, x0);
+    f3 n = normalized(cross(e1, e2));
+
+    // Wind drag (Cloth.cu:105-122), on the rest area of a free face.
+    f3 avg = dvd(add(add(v0, v1), v2), 3.0f);
+    f3 rel = sub(mk(sh.wind_v[0], sh.wind_v[1], sh.wind_v[2]), avg);
+    float vn = dot(n, rel);
+    f3 vt = sub(rel, scl(vn, n));
+    f3 force = dvd(scl(area, add(scl(sh.wind_density * absf_(vn) * vn, n), scl(sh.wind_drag, vt))), 3.0f);
+    f3 fw = scl(dt, force);
+
+    // stretchingForce (PhysicsHelper.cu:264-291)
+    float F[3][2];
+    {
+        float e1a[3] = {e1.x, e1.y, e1.z}, e2a[3] = {e2.x, e2.y, e2.z};
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            float s0 = e1a[i] * inv.x;
+            s0 += e2a[i] * inv.z;
+            float s1 = e1a[i] * inv.y;
+            s1 += e2a[i] * inv.w;
+            F[i][0] = s0;
+            F[i][1] = s1;
+        }
+    }
+    float FtF00 = F[0][0] * F[0][0], FtF01 = F[0][0] * F[0][1], FtF11 = F[0][1] * F[0][1];
+    FtF00 += F[1][0] * F[1][0];
+    FtF01 += F[1][0] * F[1][1];
+    FtF11 += F[1][1] * F[1][1];
+    FtF00 += F[2][0] * F[2][0];
+    FtF01 += F[2][0] * F[2][1];
+    FtF11 += F[2][1] * F[2][1];
+    float G00 = 0.5f * (FtF00 - 1.0f), G01 = 0.5f * (FtF01 - 0.0f), G11 = 0.5f * (FtF11 - 1.0f);
+    float4 k = stretch_stiffness(B.tables + (size_t)sh.table * CS_TABLE_ENTRIES, G00, G01, G11);
+
+    float rec[20];
+    rec[0] = F[0][0]; rec[1] = F[1][0]; rec[2] = F[2][0];
+    rec[3] = F[0][1]; rec[4] = F[1][1]; rec[5] = F[2][1];
+    rec[6] = -inv.x - inv.z;  // D(0,0) = -Y00 - Y10
+    rec[7] = inv.x;           // D(0,1) = Y00
+    rec[8] = inv.z;           // D(0,2) = Y10
+    rec[9] = -inv.y - inv.w;  // D(1,0) = -Y01 - Y11
+    rec[10] = inv.y;          // D(1,1) = Y01
+    rec[11] = inv.w;          // D(1,2) = Y11
+    rec[12] = k.x; rec[13] = k.y; rec[14] = k.z; rec[15] = k.w;
+    rec[16] = maxf_(G00, 0.0f);
+    rec[17] = maxf_(G11, 0.0f);
+    rec[18] = area;
+    rec[19] = 0.0f;
+
+    // f = -area * grad, grad with the expression order of PhysicsHelper.cu:282.
+    const float vel[9] = {v0.x, v0.y, v0.z, v1.x, v1.y, v1.z, v2.x, v2.y, v2.z};
+    float bs[9];
+#pragma unroll
+    for (int p = 0; p < 9; p++) {
+        const int a = p / 3, kp = p % 3;
+        const float D0a = rec[6 + a], D1a = rec[9 + a];
+        const float fu_p = rec[kp], fv_p = rec[3 + kp];
+        float fuu = D0a * fu_p, fvv = D1a * fv_p, fuv = 0.5f * (D0a * fv_p + D1a * fu_p);
+        float g = k.x * G00 * fuu;
+        g += k.z * G11 * fvv;
+        g += k.y * (G00 * fvv + G11 * fuu);
+        g += 2.0f * k.w * G01 * fuv;
+        float fp = -area * g;
+        float jv = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            const int b = q / 3, kq = q % 3;
+            float h = stretch_h(fu_p, fv_p, rec[kq], rec[3 + kq], D0a, D1a, rec[6 + b], rec[9 + b], k.x, k.y, k.z,
+                                k.w, rec[16], rec[17], kp == kq);
+            float J = -area * h;
+            jv += (dt * J) * vel[q];
+        }
+        bs[p] = dt * (fp + jv);
+    }
+    float4* out = reinterpret_cast<float4*>(B.face_rec + (size_t)f * CS_FACE_REC);
+    out[0] = make_float4(rec[0], rec[1], rec[2], rec[3]);
+    out[1] = make_float4(rec[4], rec[5], rec[6], rec[7]);
+    out[2] = make_float4(rec[8], rec[9], rec[10], rec[11]);
+    out[3] = make_float4(rec[12], rec[13], rec[14], rec[15]);
+    out[4] = make_float4(rec[16], rec[17], rec[18], 0.0f);
+    out[5] = make_float4(bs[0], bs[1], bs[2], bs[3]);
+    out[6] = make_float4(bs[4], bs[5], bs[6], bs[7]);
+    out[7] = make_float4(bs[8], fw.x, fw.y, fw.z);
+}
+
+// Edge record (32 floats): [0..11] dtheta, [12] coefficient, [13] theta, [16..27]
+// dt*(f + dt*J*v) of the bending term.
+__global__ void __launch_bounds__(128) cs_edge_kernel(Batch B) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= B.E) return;
+    const DevParams& P = *B.params;
+    const float dt = P.dt;
+    int4 en = B.edge_nodes[e];
+    int meta = B.edge_meta[e];
+    const SheetDesc& sh = B.sheets[B.edge_sheet[e]];
+    float4 par = B.edge_par[e];
+    f3 x0 = ld3(B.x, en.x), x1 = ld3(B.x, en.y), x2 = ld3(B.x, en.z), x3 = ld3(B.x, en.w);
+
+    // Adjacent face normals with each face's own vertex order (Face.cu:124-127).
+    // Face 0's cyclic vertex order is a rotation of (x0, x1, opposite0), face 1's of
+    // (x1, x0, opposite1); meta holds the two rotations.
+    f3 n0, n1;
+    {
+        int r = meta & 3;
+        f3 a = r == 0 ? x0 : (r == 1 ? x1 : x2);
+        f3 b = r == 0 ? x1 : (r == 1 ? x2 : x0);
+        f3 c = r == 0 ? x2 : (r == 1 ? x0 : x1);
+        n0 = normalized(cross(sub(b, a), sub(c, a)));
+        r = (meta >> 2) & 3;
+        a = r == 0 ? x1 : (r == 1 ? x0 : x3);
+        b = r == 0 ? x0 : (r == 1 ? x3 : x1);
+        c = r == 0 ? x3 : (r == 1 ? x1 : x0);
+        n1 = normalized(cross(sub(b, a), sub(c, a)));
+    }
+    // bendingForce (PhysicsHelper.cu:327-353)
+    float length = nrm(sub(x1, x0));
+    float angle;
+    {
+        f3 ee = normalized(sub(x0, x1));
+        float sine = dot(ee, cross(n0, n1));
+        float cosine = dot(n0, n1);
+        angle = (float)atan2((double)sine, (double)cosine);
+    }
+    float area = par.x;
+    f3 ed = sub(x1, x0);
+    float en2 = dot(ed, ed);
+    float h0, h1, w00, w01, w10, w11;
+    {
+        f3 t = sub(x2, x0);
+        f3 rr = dvd(mulv(ed, dot(ed, t)), en2);
+        h0 = nrm(sub(t, rr));
+        float tt = dot(ed, sub(x2, x0)) / en2;
+        w00 = 1.0f - tt;
+        w01 = tt;
+    }
+    {
+        f3 t = sub(x3, x0);
+        f3 rr = dvd(mulv(ed, dot(ed, t)), en2);
+        h1 = nrm(sub(t, rr));
+        float tt = dot(ed, sub(x3, x0)) / en2;
+        w10 = 1.0f - tt;
+        w11 = tt;
+    }
+    f3 a0 = sub(dvd(scl(-w00, n0), h0), dvd(scl(w10, n1), h1));
+    f3 a1 = sub(dvd(scl(-w01, n0), h0), dvd(scl(w11, n1), h1));
+    f3 a2 = dvd(n0, h0);
+    f3 a3 = dvd(n1, h1);
+    float dth[12] = {a0.x, a0.y, a0.z, a1.x, a1.y, a1.z, a2.x, a2.y, a2.z, a3.x, a3.y, a3.z};
+    float k0 = bend_stiffness(sh.bending, length, angle, area, par.y);
+    float k1 = bend_stiffness(sh.bending, length, angle, area, par.z);
+    float coef = -0.25f * minf_(k0, k1) * (length * length) / area;
+    float ca = coef * angle;
+
+    f3 v0 = ld3(B.v, en.x), v1 = ld3(B.v, en.y), v2 = ld3(B.v, en.z), v3 = ld3(B.v, en.w);
+    float vel[12] = {v0.x, v0.y, v0.z, v1.x, v1.y, v1.z, v2.x, v2.y, v2.z, v3.x, v3.y, v3.z};
+    float bb[12];
+#pragma unroll
+    for (int p = 0; p < 12; p++) {
+        float jv = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 12; q++) jv += (dt * (coef * (dth[p] * dth[q]))) * vel[q];
+        bb[p] = dt * (ca * dth[p] + jv);
+    }
+    float4* out = reinterpret_cast<float4*>(B.edge_rec + (size_t)e * CS_EDGE_REC);
+    out[0] = make_float4(dth[0], dth[1], dth[2], dth[3]);
+    out[1] = make_float4(dth[4], dth[5], dth[6], dth[7]);
+    out[2] = make_float4(dth[8], dth[9], dth[10], dth[11]);
+    out[3] = make_float4(coef, angle, 0.0f, 0.0f);
+    out[4] = make_float4(bb[0], bb[1], bb[2], bb[3]);
+    out[5] = make_float4(bb[4], bb[5], bb[6], bb[7]);
+    out[6] = make_float4(bb[8], bb[9], bb[10], bb[11]);
+}
+
+// One warp per slice; lane = row.  Writes A's panels, and for the diagonal slot b, the
+// block-Jacobi inverse and the slice's ||b||^2 (part[2*slice]).
+__global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
+    int slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (slice >= B.n_slices) return;
+    const SliceDesc sd = B.slices[slice];
+    const SheetDesc& sh = B.sheets[sd.sheet];
+    const DevParams& P = *B.params;
+    const float dt = P.dt;
+    const float s = -dt * dt;
+    const bool live = lane < sd.rows;
+    const int row = sd.row0 + lane;
+    double bsq = 0.0;
+    for (int k = 0; k < sd.width; k++) {
+        const int tslot = (sd.tpanel0 + k) * CS_SLICE + lane;
+        float a[9];
+#pragma unroll
+        for (int t = 0; t < 9; t++) a[t] = 0.0f;
+        if (live) {
+            if (k == 0) {
+                float m = B.mass[row];
+                a[0] = m; a[4] = m; a[8] = m;
+            }
+            int c0 = B.tcptr[tslot], c1 = B.tcptr[tslot + 1];
+            for (int c = c0; c < c1; c++) {
+                uint32_t code = B.tcontrib[c];
+                int elem = (int)((code >> 4) & 0x7FFFFFFu);
+                int ca = (code >> 2) & 3, cb = code & 3;
+                if (!(code & CS_CODE_EDGE)) {
+                    const float* rec = B.face_rec + (size_t)(sh.face_off + elem) * CS_FACE_REC;
+                    float r[20];
+                    const float4* r4 = reinterpret_cast<const float4*>(rec);
+#pragma unroll
+                    for (int t = 0; t < 5; t++) {
+                        float4 v = r4[t];
+                        r[4 * t] = v.x; r[4 * t + 1] = v.y; r[4 * t + 2] = v.z; r[4 * t + 3] = v.w;
+                    }
+                    const float ar = r[18];
+                    const float D0a = sel3(r[6], r[7], r[8], ca), D1a = sel3(r[9], r[10], r[11], ca);
+                    const float D0b = sel3(r[6], r[7], r[8], cb), D1b = sel3(r[9], r[10], r[11], cb);
+#pragma unroll
+                    for (int kk = 0; kk < 3; kk++)
+#pragma unroll
+                        for (int hh = 0; hh < 3; hh++) {
+                            float h = stretch_h(r[kk], r[3 + kk], r[hh], r[3 + hh], D0a, D1a, D0b, D1b, r[12], r[13],
+                                                r[14], r[15], r[16], r[17], kk == hh);
+                            float J = -ar * h;
+                            a[3 * kk + hh] += s * J;
+                        }
+                } else {
+                    const float* rec = B.edge_rec + (size_t)(sh.edge_off + elem) * CS_EDGE_REC;
+                    float coef = rec[12];
+#pragma unroll
+                    for (int kk = 0; kk < 3; kk++)
+#pragma unroll
+                        for (int hh = 0; hh < 3; hh++) {
+                            float J = coef * (rec[3 * ca + kk] * rec[3 * cb + hh]);
+                            a[3 * kk + hh] += s * J;
+                        }
+                }
+            }
+            if (k == 0) {
+                float4 hd = B.handle[row];
+                int hc = (int)hd.w;
+                for (int t = 0; t < hc; t++) {
+                    float add_ = dt * dt * P.handle_stiffness;
+                    a[0] += add_; a[4] += add_; a[8] += add_;
+                }
+            }
+        }
+        float* panel = B.A + (size_t)(sd.panel0 + k) * CS_PANEL_FLOATS;
+        reinterpret_cast<float4*>(panel)[lane] = make_float4(a[0], a[1], a[2], a[3]);
+        reinterpret_cast<float4*>(panel + 128)[lane] = make_float4(a[4], a[5], a[6], a[7]);
+        panel[256 + lane] = a[8];
+
+        if (k == 0 && live) {
+            // Right-hand side in the reference's order: gravity, wind (faces), stretching
+            // (faces), bending (edges), handles (Cloth.cu:94-169).
+            float m = B.mass[row];
+            float g0 = (dt * m) * P.gravity[0], g1 = (dt * m) * P.gravity[1], g2 = (dt * m) * P.gravity[2];
+            float b0 = 0.0f + g0, b1 = 0.0f + g1, b2 = 0.0f + g2;
+            int c0 = B.tcptr[tslot], c1 = B.tcptr[tslot + 1];
+            for (int c = c0; c < c1; c++) {
+                uint32_t code = B.tcontrib[c];
+                if (code & CS_CODE_EDGE) continue;
+                int elem = (int)((code >> 4) & 0x7FFFFFFu);
+                const float* rec = B.face_rec + (size_t)(sh.face_off + elem) * CS_FACE_REC;
+                b0 += rec[29]; b1 += rec[30]; b2 += rec[31];
+            }
+            for (int c = c0; c < c1; c++) {
+                uint32_t code = B.tcontrib[c];
+                if (code & CS_CODE_EDGE) continue;
+                int elem = (int)((code >> 4) & 0x7FFFFFFu);
+                int ca = (code >> 2) & 3;
+                const float* rec = B.face_rec + (size_t)(sh.face_off + elem) * CS_FACE_REC;
+                b0 += rec[20 + 3 * ca]; b1 += rec[21 + 3 * ca]; b2 += rec[22 + 3 * ca];
+            }
+            for (int c = c0; c < c1; c++) {
+                uint32_t code = B.tcontrib[c];
+                if (!(code & CS_CODE_EDGE)) continue;
+                int elem = (int)((code >> 4) & 0x7FFFFFFu);
+                int ca = (code >> 2) & 3;
+                const float* rec = B.edge_rec + (size_t)(sh.edge_off + elem) * CS_EDGE_REC;
+                b0 += rec[16 + 3 * ca]; b1 += rec[17 + 3 * ca]; b2 += rec[18 + 3 * ca];
+            }
+            float4 hd = B.handle[row];
+            int hc = (int)hd.w;
+            if (hc > 0) {
+                f3 xr = ld3(B.x, row), vr = ld3(B.v, row);
+                f3 fh = mulv(scl(dt, sub(sub(mk(hd.x, hd.y, hd.z), xr), scl(dt, vr))), P.handle_stiffness);
+                for (int t = 0; t < hc; t++) {
+                    b0 += fh.x; b1 += fh.y; b2 += fh.z;
+                }
+            }
+            B.b[3 * row] = b0;
+            B.b[3 * row + 1] = b1;
+            B.b[3 * row + 2] = b2;
+            bsq = (double)b0 * b0 + (double)b1 * b1 + (double)b2 * b2;
+            // 3x3 block-Jacobi inverse in double, stored in float.
+            double m00 = a[0], m01 = a[1], m02 = a[2], m10 = a[3], m11 = a[4], m12 = a[5], m20 = a[6], m21 = a[7],
+                   m22 = a[8];
+            double c00 = m11 * m22 - m12 * m21, c01 = m12 * m20 - m10 * m22, c02 = m10 * m21 - m11 * m20;
+            double det = m00 * c00 + m01 * c01 + m02 * c02;
+            double id = det != 0.0 ? 1.0 / det : 0.0;
+            float* Pi = B.Pinv + 9 * (size_t)row;
+            Pi[0] = (float)(c00 * id);
+            Pi[1] = (float)((m02 * m21 - m01 * m22) * id);
+            Pi[2] = (float)((m01 * m12 - m02 * m11) * id);
+            Pi[3] = (float)(c01 * id);
+            Pi[4] = (float)((m00 * m22 - m02 * m20) * id);
+            Pi[5] = (float)((m02 * m10 - m00 * m12) * id);
+            Pi[6] = (float)(c02 * id);
+            Pi[7] = (float)((m01 * m20 - m00 * m21) * id);
+            Pi[8] = (float)((m00 * m11 - m01 * m10) * id);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bsq += __shfl_xor_sync(0xffffffffu, bsq, o);
+    if (lane == 0) B.part[2 * slice] = bsq;
+}
+
+// Expands the element records of the last assembly into the reference's per-element
+// outputs (f, J) for inspection: faces as stretchingForce returns them
+// (PhysicsHelper.cu:288-290), interior edges as bendingForce does (PhysicsHelper.cu:351-352).
+__global__ void __launch_bounds__(128) cs_expand_kernel(Batch B, float* face_f, float* face_J, float* edge_f,
+                                                        float* edge_J) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < B.F) {
+        const float* r = B.face_rec + (size_t)i * CS_FACE_REC;
+        const float area = r[18];
+        for (int p = 0; p < 9; p++) {
+            const int a = p / 3, kp = p % 3;
+            const float D0a = r[6 + a], D1a = r[9 + a];
+            const float fu_p = r[kp], fv_p = r[3 + kp];
+            // G is re-derived from the stored deformation gradient F (rec[0..5]) with the face
+            // kernel's arithmetic, so f is the value the face kernel used.
+            float F00 = r[0], F10 = r[1], F20 = r[2], F01 = r[3], F11 = r[4], F21 = r[5];
+            float FtF00 = F00 * F00, FtF01 = F00 * F01, FtF11 = F01 * F01;
+            FtF00 += F10 * F10;
+            FtF01 += F10 * F11;
+            FtF11 += F11 * F11;
+            FtF00 += F20 * F20;
+            FtF01 += F20 * F21;
+            FtF11 += F21 * F21;
+            float G00 = 0.5f * (FtF00 - 1.0f), G01 = 0.5f * (FtF01 - 0.0f), G11 = 0.5f * (FtF11 - 1.0f);
+            float fuu = D0a * fu_p, fvv = D1a * fv_p, fuv = 0.5f * (D0a * fv_p + D1a * fu_p);
+            float g = r[12] * G00 * fuu;
+            g += r[14] * G11 * fvv;
+            g += r[13] * (G00 * fvv + G11 * fuu);
+            g += 2.0f * r[15] * G01 * fuv;
+            face_f[9 * (size_t)i + p] = -area * g;
+            for (int q = 0; q < 9; q++) {
+                const int b = q / 3, kq = q % 3;
+                float h = stretch_h(fu_p, fv_p, r[kq], r[3 + kq], D0a, D1a, r[6 + b], r[9 + b], r[12], r[13], r[14],
+                                    r[15], r[16], r[17], kp == kq);
+                face_J[81 * (size_t)i + 9 * p + q] = -area * h;
+            }
+        }
+    }
+    if (i < B.E) {
+        const float* r = B.edge_rec + (size_t)i * CS_EDGE_REC;
+        const float coef = r[12], angle = r[13];
+        const float ca = coef * angle;
+        for (int p = 0; p < 12; p++) {
+            edge_f[12 * (size_t)i + p] = ca * r[p];
+            for (int q = 0; q < 12; q++) edge_J[144 * (size_t)i + 12 * p + q] = coef * (r[p] * r[q]);
+        }
+    }
+}

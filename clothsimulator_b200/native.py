@@ -1,0 +1,320 @@
+"""ctypes binding of libclothstep.so (the C ABI in include/clothstep.h).
+
+This is plumbing for Python callers (tests, bench.py); it adds no computation.  The library
+must be built in-tree (``python -c "import __graft_entry__; __graft_entry__.build()"`` or
+``make -C clothsimulator_b200/csrc``); importing this module without it raises, and there is
+no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libclothstep.so")
+
+CS_OK = 0
+CS_ERR_INVALID_ARG = 1
+CS_ERR_CUDA = 2
+CS_ERR_NOT_CONVERGED = 3
+CS_ERR_NON_SPD = 4
+CS_ERR_TIMEOUT = 5
+CS_ERR_STATE = 6
+CS_ERR_NO_DEVICE = 7
+CS_ERR_NOT_TRAINED = 8
+
+PREC_PLAIN_FP32 = 0
+PREC_MIXED = 1
+WARM_ZERO, WARM_PREVIOUS, WARM_LEARNED, WARM_GIVEN = 0, 1, 2, 3
+
+EXPORTED = [
+    "cs_create", "cs_destroy", "cs_last_error", "cs_load_batch", "cs_get_sizes", "cs_set_state", "cs_get_state",
+    "cs_set_state_device", "cs_get_state_device", "cs_step", "cs_sync", "cs_set_warm_start", "cs_get_dv",
+    "cs_get_instance_stats", "cs_assemble", "cs_get_system", "cs_get_element_forces", "cs_spmv",
+    "cs_device_pointers",
+]
+
+
+class MaterialDesc(ctypes.Structure):
+    _fields_ = [
+        ("density", ctypes.c_float),
+        ("stretching", ctypes.c_float * 24),
+        ("bending", ctypes.c_float * 15),
+        ("thicken", ctypes.c_float),
+        ("density_mult", ctypes.c_float),
+        ("stretching_mult", ctypes.c_float),
+        ("bending_mult", ctypes.c_float),
+    ]
+
+
+_fp = ctypes.POINTER(ctypes.c_float)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class SheetDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_nodes", ctypes.c_int), ("n_verts", ctypes.c_int), ("n_faces", ctypes.c_int), ("n_handles", ctypes.c_int),
+        ("x", _fp), ("v", _fp), ("uv", _fp), ("face_nodes", _ip), ("face_verts", _ip),
+        ("handle_nodes", _ip), ("handle_pos", _fp), ("material", ctypes.c_int),
+        ("wind_density", ctypes.c_float), ("wind_drag", ctypes.c_float), ("wind_velocity", ctypes.c_float * 3),
+    ]
+
+
+class StepParams(ctypes.Structure):
+    _fields_ = [
+        ("dt", ctypes.c_float), ("gravity", ctypes.c_float * 3), ("handle_stiffness", ctypes.c_float),
+        ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double), ("max_iters", ctypes.c_int),
+        ("sweep_cap", ctypes.c_int), ("precision", ctypes.c_int), ("warm_start", ctypes.c_int),
+        ("advance", ctypes.c_int), ("use_graph", ctypes.c_int),
+    ]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [
+        ("n_instances", ctypes.c_int), ("converged", ctypes.c_int), ("max_iters", ctypes.c_int),
+        ("total_iters", ctypes.c_longlong), ("max_sweeps", ctypes.c_int), ("warm_rejected", ctypes.c_int),
+        ("loop_trips", ctypes.c_int), ("max_rel_residual", ctypes.c_double), ("ms", ctypes.c_float),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_LIB = None
+
+
+def load_library() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run __graft_entry__.build()")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    sig = {
+        "cs_create": [ctypes.POINTER(vp), ctypes.c_int],
+        "cs_destroy": [vp],
+        "cs_load_batch": [vp, ctypes.POINTER(MaterialDesc), ctypes.c_int, ctypes.POINTER(SheetDesc), ctypes.c_int],
+        "cs_get_sizes": [vp, ctypes.POINTER(ctypes.c_longlong)],
+        "cs_set_state": [vp, _fp, _fp],
+        "cs_get_state": [vp, _fp, _fp],
+        "cs_set_state_device": [vp, vp, vp],
+        "cs_get_state_device": [vp, vp, vp],
+        "cs_step": [vp, ctypes.POINTER(StepParams), ctypes.POINTER(StepStats)],
+        "cs_sync": [vp],
+        "cs_set_warm_start": [vp, _fp],
+        "cs_get_dv": [vp, _fp],
+        "cs_get_instance_stats": [vp, _ip, _dp, _ip],
+        "cs_assemble": [vp, ctypes.POINTER(StepParams)],
+        "cs_get_system": [vp, _ip, _ip, _fp, _fp],
+        "cs_get_element_forces": [vp, _fp, _fp, _fp, _fp, _ip],
+        "cs_spmv": [vp, _fp, _fp],
+        "cs_device_pointers": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    lib.cs_last_error.argtypes = [vp]
+    lib.cs_last_error.restype = ctypes.c_char_p
+    _LIB = lib
+    return lib
+
+
+class ClothStepError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"status {status}: {message}")
+        self.status = status
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def material_desc(spec: dict) -> MaterialDesc:
+    m = MaterialDesc()
+    m.density = spec["density"]
+    st = np.asarray(spec["stretching"], np.float32).reshape(24)
+    be = np.asarray(spec["bending"], np.float32).reshape(15)
+    for i in range(24):
+        m.stretching[i] = st[i]
+    for i in range(15):
+        m.bending[i] = be[i]
+    m.thicken = spec.get("thicken", 1.0)
+    m.density_mult = spec.get("density_mult", 1.0)
+    m.stretching_mult = spec.get("stretching_mult", 1.0)
+    m.bending_mult = spec.get("bending_mult", 1.0)
+    return m
+
+
+def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, inner_tol=1e-4, max_iters=2000,
+                sweep_cap=0, precision=PREC_MIXED, warm_start=WARM_ZERO, advance=1, use_graph=1) -> StepParams:
+    p = StepParams()
+    p.dt = dt
+    for i in range(3):
+        p.gravity[i] = gravity[i]
+    p.handle_stiffness = handle_stiffness
+    p.tol = tol
+    p.inner_tol = inner_tol
+    p.max_iters = max_iters
+    p.sweep_cap = sweep_cap
+    p.precision = precision
+    p.warm_start = warm_start
+    p.advance = advance
+    p.use_graph = use_graph
+    return p
+
+
+class Context:
+    """Owns one cs_ctx.  `sheets` are dicts as produced by clothsimulator_b200.scenes."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        st = self.lib.cs_create(ctypes.byref(h), device)
+        if st != CS_OK:
+            raise ClothStepError(st, "cs_create failed (no usable sm_100 CUDA device)")
+        self.h = h
+        self._keep = []
+        self.n = 0
+
+    def check(self, st: int, allow=(CS_OK,)):
+        if st not in allow:
+            raise ClothStepError(st, self.lib.cs_last_error(self.h).decode())
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load(self, sheets):
+        mats = (MaterialDesc * len(sheets))()
+        descs = (SheetDesc * len(sheets))()
+        keep = []
+        for i, s in enumerate(sheets):
+            mats[i] = material_desc(s["material"])
+            d = descs[i]
+            x, v, uv = _f32(s["x"]), _f32(s["v"]), _f32(s["uv"])
+            fx, fu = _i32(s["fx"]), _i32(s["fu"])
+            hn = _i32(s.get("handles", np.zeros(0, np.int32)))
+            keep += [x, v, uv, fx, fu, hn]
+            d.n_nodes = x.shape[0]
+            d.n_verts = uv.shape[0]
+            d.n_faces = fx.shape[0]
+            d.n_handles = hn.shape[0]
+            d.x = x.ctypes.data_as(_fp)
+            d.v = v.ctypes.data_as(_fp)
+            d.uv = uv.ctypes.data_as(_fp)
+            d.face_nodes = fx.ctypes.data_as(_ip)
+            d.face_verts = fu.ctypes.data_as(_ip)
+            d.handle_nodes = hn.ctypes.data_as(_ip)
+            d.handle_pos = None
+            d.material = i
+            w = s["wind"]
+            d.wind_density = w["density"]
+            d.wind_drag = w["drag"]
+            for k in range(3):
+                d.wind_velocity[k] = w["velocity"][k]
+        self.check(self.lib.cs_load_batch(self.h, mats, len(sheets), descs, len(sheets)))
+        self.sizes = self.get_sizes()
+        self.n = int(self.sizes[0])
+        self.n_sheets = len(sheets)
+        return self
+
+    def get_sizes(self):
+        s = (ctypes.c_longlong * 7)()
+        self.check(self.lib.cs_get_sizes(self.h, s))
+        return [int(v) for v in s]
+
+    def set_state(self, x=None, v=None):
+        xa = _f32(x) if x is not None else None
+        va = _f32(v) if v is not None else None
+        self.check(self.lib.cs_set_state(self.h, xa.ctypes.data_as(_fp) if xa is not None else None,
+                                         va.ctypes.data_as(_fp) if va is not None else None))
+        self.check(self.lib.cs_sync(self.h))
+
+    def get_state(self):
+        x = np.zeros((self.n, 3), np.float32)
+        v = np.zeros((self.n, 3), np.float32)
+        self.check(self.lib.cs_get_state(self.h, x.ctypes.data_as(_fp), v.ctypes.data_as(_fp)))
+        return x, v
+
+    def step(self, params: StepParams, allow_unconverged: bool = False):
+        stats = StepStats()
+        allow = (CS_OK, CS_ERR_NOT_CONVERGED) if allow_unconverged else (CS_OK,)
+        st = self.check(self.lib.cs_step(self.h, ctypes.byref(params), ctypes.byref(stats)), allow)
+        return stats, st
+
+    def step_async(self, params: StepParams):
+        self.check(self.lib.cs_step(self.h, ctypes.byref(params), None))
+
+    def sync(self):
+        self.check(self.lib.cs_sync(self.h))
+
+    def set_warm_start(self, dv):
+        a = _f32(dv)
+        self.check(self.lib.cs_set_warm_start(self.h, a.ctypes.data_as(_fp)))
+
+    def get_dv(self):
+        dv = np.zeros((self.n, 3), np.float32)
+        self.check(self.lib.cs_get_dv(self.h, dv.ctypes.data_as(_fp)))
+        return dv
+
+    def instance_stats(self):
+        S = self.n_sheets
+        it = np.zeros(S, np.int32)
+        rr = np.zeros(S, np.float64)
+        fl = np.zeros(S, np.int32)
+        self.check(self.lib.cs_get_instance_stats(self.h, it.ctypes.data_as(_ip), rr.ctypes.data_as(_dp),
+                                                  fl.ctypes.data_as(_ip)))
+        return it, rr, fl
+
+    def assemble(self, params: StepParams):
+        self.check(self.lib.cs_assemble(self.h, ctypes.byref(params)))
+
+    def system(self):
+        nnzb = self.sizes[6]
+        rp = np.zeros(self.n + 1, np.int32)
+        ci = np.zeros(nnzb, np.int32)
+        val = np.zeros((nnzb, 3, 3), np.float32)
+        b = np.zeros(3 * self.n, np.float32)
+        self.check(self.lib.cs_get_system(self.h, rp.ctypes.data_as(_ip), ci.ctypes.data_as(_ip),
+                                          val.ctypes.data_as(_fp), b.ctypes.data_as(_fp)))
+        return rp, ci, val, b
+
+    def element_forces(self):
+        F, E = self.sizes[1], self.sizes[2]
+        ff = np.zeros((F, 9), np.float32)
+        fJ = np.zeros((F, 9, 9), np.float32)
+        ef = np.zeros((E, 12), np.float32)
+        eJ = np.zeros((E, 12, 12), np.float32)
+        en = np.zeros((E, 4), np.int32)
+        self.check(self.lib.cs_get_element_forces(self.h, ff.ctypes.data_as(_fp), fJ.ctypes.data_as(_fp),
+                                                  ef.ctypes.data_as(_fp), eJ.ctypes.data_as(_fp),
+                                                  en.ctypes.data_as(_ip)))
+        return ff, fJ, ef, eJ, en
+
+    def spmv(self, x):
+        xa = _f32(x).reshape(-1)
+        y = np.zeros_like(xa)
+        self.check(self.lib.cs_spmv(self.h, xa.ctypes.data_as(_fp), y.ctypes.data_as(_fp)))
+        return y
+
+    def device_pointers(self):
+        x, v, dv = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        self.check(self.lib.cs_device_pointers(self.h, ctypes.byref(x), ctypes.byref(v), ctypes.byref(dv)))
+        return x.value, v.value, dv.value

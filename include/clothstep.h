@@ -1,0 +1,160 @@
+/* clothstep: a B200 (sm_100a) implementation of ClothSimulator's implicit cloth step.
+ *
+ * The reference has no C ABI: its implicit step is the C++ overload pair
+ * Cloth::physicsStep(dt, gravity, wind, transformations, handleStiffness, proximities,
+ * repulsionThickness) -- CPU (Cloth.cu:676-693, src/Cloth.cuh:91) and GPU (Cloth.cu:695-813,
+ * src/Cloth.cuh:92) -- chosen by the global `gpu` flag set from `--gpu` (main.cu:7-29) and
+ * called once per cloth from Simulator::physicsStep (Simulator.cu:578-586).  This header is the
+ * seam that replaces the GPU overload: a context holds a batch of cloths ("sheets") resident in
+ * HBM and advances all of them by one implicit step per call.
+ *
+ * Conventions: every function returns a cs_status; host arrays are owned by the caller and
+ * copied in or out; device memory is owned by the context; one context per host thread.
+ * cs_step is asynchronous on the context's stream (cs_sync waits).  No function falls back to
+ * a CPU implementation: without a usable CUDA device cs_create returns CS_ERR_NO_DEVICE.
+ */
+#ifndef CLOTHSTEP_H
+#define CLOTHSTEP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cs_status {
+    CS_OK = 0,
+    CS_ERR_INVALID_ARG = 1,   /* bad sizes, indices out of range, NULL where required */
+    CS_ERR_CUDA = 2,          /* a CUDA runtime call failed; see cs_last_error */
+    CS_ERR_NOT_CONVERGED = 3, /* some instance stopped at its iteration cap (stats tell which) */
+    CS_ERR_NON_SPD = 4,       /* a diagonal block is singular or a CG breakdown occurred */
+    CS_ERR_TIMEOUT = 5,       /* the solve loop hit its trip bound */
+    CS_ERR_STATE = 6,         /* call out of order (e.g. cs_step before cs_load_batch) */
+    CS_ERR_NO_DEVICE = 7,     /* no CUDA device, or not an sm_100 device */
+    CS_ERR_NOT_TRAINED = 8    /* learned warm start requested without a trained network */
+} cs_status;
+
+typedef struct cs_ctx cs_ctx;
+
+/* Material as read by Material::Material (Material.cu:3-41): the data file's density, six
+ * stretching rows of four values and 3x5 bending samples, and the cloth's multipliers. */
+typedef struct cs_material_desc {
+    float density;
+    float stretching[6][4];
+    float bending[3][5];
+    float thicken, density_mult, stretching_mult, bending_mult;
+} cs_material_desc;
+
+/* One cloth.  Arrays follow Mesh::load's CPU branch (Mesh.cu:306-404): node positions and
+ * velocities, uv vertices, and triangles as (node, uv-vertex) index triples.  Handles follow
+ * Cloth::addHandles (Cloth.cu:653-664): the node's position at load is the target unless
+ * handle_pos is given.  Wind follows Wind.cu:3-7; the reference has one global wind
+ * (Simulator.cu:28), here each sheet has its own. */
+typedef struct cs_sheet_desc {
+    int n_nodes, n_verts, n_faces, n_handles;
+    const float* x;            /* 3*n_nodes */
+    const float* v;            /* 3*n_nodes, or NULL for zero velocity */
+    const float* uv;           /* 2*n_verts */
+    const int32_t* face_nodes; /* 3*n_faces */
+    const int32_t* face_verts; /* 3*n_faces */
+    const int32_t* handle_nodes; /* n_handles */
+    const float* handle_pos;   /* 3*n_handles, or NULL */
+    int material;              /* index into the materials passed to cs_load_batch */
+    float wind_density, wind_drag, wind_velocity[3];
+} cs_sheet_desc;
+
+enum { CS_PREC_PLAIN_FP32 = 0, CS_PREC_MIXED = 1 };
+enum { CS_WARM_ZERO = 0, CS_WARM_PREVIOUS = 1, CS_WARM_LEARNED = 2, CS_WARM_GIVEN = 3 };
+
+/* Parameters of one step (Cloth::physicsStep's dt, gravity, handleStiffness) plus solver
+ * controls.  The reference's GPU solve stops at an absolute ||r|| < 1e-6 or 400 iterations
+ * (Cloth.cuh:43-44); here the target is an FP64-checked relative residual. */
+typedef struct cs_step_params {
+    float dt;
+    float gravity[3];
+    float handle_stiffness;   /* Magic::handleStiffness, default 1e3 (Magic.cu:6) */
+    double tol;               /* relative residual ||b - A dv|| / ||b||, checked in FP64 */
+    double inner_tol;         /* mixed precision: residual reduction per CG sweep */
+    int max_iters;            /* CG iterations per sheet per step */
+    int sweep_cap;            /* CG iterations per sweep (mixed) / between FP64 checks (plain) */
+    int precision;            /* CS_PREC_* */
+    int warm_start;           /* CS_WARM_* */
+    int advance;              /* 1: v += dv and x += dt v (a full step); 0: solve only */
+    int use_graph;            /* 1: run the captured CUDA graph; 0: host-driven launches */
+} cs_step_params;
+
+typedef struct cs_step_stats {
+    int n_instances;
+    int converged;            /* instances that met tol */
+    int max_iters;            /* max CG iterations over instances */
+    long long total_iters;    /* sum of CG iterations over instances */
+    int max_sweeps;           /* max FP64 residual evaluations */
+    int warm_rejected;        /* instances whose warm start was discarded */
+    int loop_trips;           /* trips of the batched solve loop */
+    double max_rel_residual;  /* max over instances of the final FP64 relative residual */
+    float ms;                 /* device time of the step (CUDA events) */
+} cs_step_stats;
+
+/* Context lifetime (replaces the per-cloth cuBLAS/cuSPARSE handles, Cloth.cu:19-20). */
+cs_status cs_create(cs_ctx** ctx, int device);
+cs_status cs_destroy(cs_ctx* ctx);
+const char* cs_last_error(const cs_ctx* ctx);
+
+/* Uploads a batch of cloths: topology (Mesh::load, Mesh.cu:306-452), face rest data
+ * (Face::initialize, Face.cu:12-20), lumped masses (Mesh.cu:182-203), material tables
+ * (Material.cu:3-41), handles, and the fixed block-sparse pattern of the system. */
+cs_status cs_load_batch(cs_ctx* ctx, const cs_material_desc* materials, int n_materials,
+                        const cs_sheet_desc* sheets, int n_sheets);
+
+/* sizes[0..6] = nodes, faces, interior edges, stored 3x3 blocks (incl. padding), slices,
+ * sheets, nonzero blocks of the pattern. */
+cs_status cs_get_sizes(const cs_ctx* ctx, long long* sizes);
+
+/* Node state of the whole batch, sheets concatenated in load order (3 floats per node). */
+cs_status cs_set_state(cs_ctx* ctx, const float* x, const float* v);
+cs_status cs_get_state(cs_ctx* ctx, float* x, float* v);
+/* Same with device pointers (no host copy). */
+cs_status cs_set_state_device(cs_ctx* ctx, const float* x, const float* v);
+cs_status cs_get_state_device(cs_ctx* ctx, float* x, float* v);
+
+/* One implicit step of every sheet: assemble (M - dt^2 df/dx) dv = dt (f + dt df/dx v)
+ * (Cloth.cu:676-684), solve with batched PCG, and (if params->advance) v += dv, x += dt v
+ * (Cloth.cu:690-692, Mesh.cu:226-231).  stats may be NULL.  Returns CS_ERR_NOT_CONVERGED if any
+ * sheet stopped at its cap (the step is still applied). */
+cs_status cs_step(cs_ctx* ctx, const cs_step_params* params, cs_step_stats* stats);
+cs_status cs_sync(cs_ctx* ctx);
+
+/* Warm start for CS_WARM_GIVEN: 3 floats per node (host). */
+cs_status cs_set_warm_start(cs_ctx* ctx, const float* dv);
+/* The last step's dv (3 floats per node, host). */
+cs_status cs_get_dv(cs_ctx* ctx, float* dv);
+/* Per-instance results of the last step: iterations, FP64 relative residual, flags
+ * (1 converged, 2 warm start rejected, 4 breakdown, 8 iteration cap), each n_sheets long. */
+cs_status cs_get_instance_stats(cs_ctx* ctx, int* iters, double* rel_residual, int* flags);
+
+/* --- Inspection entry points used by the parity tests ------------------------------------ */
+
+/* Assembles the system for the current state without solving (params->dt, gravity,
+ * handle_stiffness are used). */
+cs_status cs_assemble(cs_ctx* ctx, const cs_step_params* params);
+/* The assembled system in block-CSR, rows = nodes in load order, columns sorted:
+ * row_ptr (N+1), col (nnzb), val (9*nnzb, row-major blocks), b (3N), each may be NULL.
+ * nnzb = sizes[6] of cs_get_sizes. */
+cs_status cs_get_system(cs_ctx* ctx, int32_t* row_ptr, int32_t* col, float* val, float* b);
+/* Per-element forces and Jacobians of the last assembly, expanded from the element records:
+ * faces (9 and 81 floats each, PhysicsHelper.cu:264-291) and interior edges in the
+ * reference's edge order (12 and 144 floats each, PhysicsHelper.cu:327-353); any may be NULL.
+ * edge_nodes receives 4 node ids per interior edge. */
+cs_status cs_get_element_forces(cs_ctx* ctx, float* face_f, float* face_J, float* edge_f, float* edge_J,
+                                int32_t* edge_nodes);
+/* y = A x with the assembled system (host vectors of 3N floats). */
+cs_status cs_spmv(cs_ctx* ctx, const float* x, float* y);
+/* Device pointers of the batch state, for zero-copy callers: x, v, dv (3N floats each). */
+cs_status cs_device_pointers(cs_ctx* ctx, float** x, float** v, float** dv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLOTHSTEP_H */

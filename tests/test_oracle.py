@@ -1,0 +1,163 @@
+"""The CPU oracle pinned against the reference's own code, and its own consistency checks.
+
+* Golden fixtures (tests/golden/*.npz, made by tests/golden/make_golden.py from the reference's
+  compiled Material/stretchingForce/bendingForce/Face code) must be reproduced bit for bit by
+  the restated FP32 oracle.
+* Where the reference adapter is built, it is compared live on more random inputs.
+* FP64 oracle: Jacobians against central finite differences where the reference's Jacobian
+  is exact (constant stiffness, stretched faces; dihedral angle 0), zero forces at rest, and
+  the sparse Cholesky and FP64 PCG against SciPy's direct solve.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import pyoracle
+from clothsimulator_b200 import scenes
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def golden_sheet(g):
+    mult = g["material_mults"]
+    mat = {"density": float(g["material_density"]), "stretching": g["material_stretching"].tolist(),
+           "bending": g["material_bending"].tolist(), "thicken": float(mult[0]), "density_mult": float(mult[1]),
+           "stretching_mult": float(mult[2]), "bending_mult": float(mult[3])}
+    sheet = {k: g[k] for k in ("x", "v", "uv", "fx", "fu", "handles")}
+    sheet["material"] = mat
+    return sheet, mat
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_oracle_reproduces_reference_golden(path):
+    g = np.load(path)
+    sheet, mat = golden_sheet(g)
+    m = pyoracle.Material(mat, "float")
+    assert np.array_equal(m.stretching(g["G"]), g["k"])
+    assert np.array_equal(m.bending(g["bend_query"]), g["bend_k"])
+    c = pyoracle.Cloth(sheet, m)
+    ff, fJ = c.face_forces()
+    assert np.array_equal(ff.astype(np.float32), g["face_f"]) and np.array_equal(fJ.astype(np.float32), g["face_J"])
+    en, _ = c.interior_edges()
+    ef, eJ, th = c.edge_forces()
+    assert np.array_equal(en, g["edge_nodes"])
+    assert np.array_equal(ef.astype(np.float32), g["edge_f"]) and np.array_equal(eJ.astype(np.float32), g["edge_J"])
+    assert np.array_equal(th.astype(np.float32), g["edge_theta"])
+    rp, ci, val, b = c.assemble(g["params"])
+    assert np.array_equal(rp, g["row_ptr"]) and np.array_equal(ci, g["col"])
+    assert np.array_equal(val.astype(np.float32), g["val"]) and np.array_equal(b.astype(np.float32), g["b"])
+    dv, _ = c.step(g["params"], pyoracle.METHOD_LLT)
+    x1, v1 = c.state()
+    assert np.array_equal(dv.astype(np.float32), g["dv"])
+    assert np.array_equal(x1.astype(np.float32), g["x1"]) and np.array_equal(v1.astype(np.float32), g["v1"])
+
+
+@pytest.mark.ref
+def test_oracle_matches_reference_adapter_live():
+    if not os.path.exists(pyoracle.LIB_REF):
+        pytest.skip("reference adapter not built")
+    rng = np.random.default_rng(42)
+    for trial in range(3):
+        scene = scenes.uneven_batch(1, seed=trial, nq_range=(5, 12))
+        s = scene.sheets[0]
+        s["x"] = (s["x"] + rng.normal(0, 0.02, s["x"].shape)).astype(np.float32)
+        s["v"] = rng.normal(0, 0.2, s["v"].shape).astype(np.float32)
+        mo, mr = pyoracle.Material(s["material"]), pyoracle.Material(s["material"], which="ref")
+        co, cr = pyoracle.Cloth(s, mo), pyoracle.Cloth(s, mr)
+        assert cr.topology_mismatches() == 0
+        p = scenes.step_params(scene, s)
+        a, b = co.assemble(p), cr.assemble(p)
+        for u, w in zip(a, b):
+            assert np.array_equal(u, w)
+        d1, _ = co.step(p)
+        d2, _ = cr.step(p)
+        assert np.array_equal(d1, d2)
+
+
+def _fd_check(sheet, which, eps=1e-6):
+    m = pyoracle.Material(sheet["material"], "double")
+    c = pyoracle.Cloth(sheet, m)
+    x0, v0 = c.state()
+    if which == "face":
+        f0, J0 = c.face_forces()
+        nodes = sheet["fx"]
+    else:
+        f0, J0, _ = c.edge_forces()
+        nodes, _ = c.interior_edges()
+    worst = 0.0
+    for e in range(min(len(nodes), 6)):
+        K = nodes.shape[1]
+        Jfd = np.zeros((3 * K, 3 * K))
+        for a in range(K):
+            for d in range(3):
+                xp = x0.copy()
+                xm = x0.copy()
+                xp[nodes[e, a], d] += eps
+                xm[nodes[e, a], d] -= eps
+                c.set_state(xp.reshape(-1), v0.reshape(-1))
+                fp = (c.face_forces()[0] if which == "face" else c.edge_forces()[0])[e]
+                c.set_state(xm.reshape(-1), v0.reshape(-1))
+                fm = (c.face_forces()[0] if which == "face" else c.edge_forces()[0])[e]
+                Jfd[:, 3 * a + d] = (fp - fm) / (2 * eps)
+        c.set_state(x0.reshape(-1), v0.reshape(-1))
+        worst = max(worst, np.abs(Jfd - J0[e]).max() / np.abs(J0[e]).max())
+    return worst
+
+
+def test_fp64_stretching_jacobian_matches_finite_differences():
+    s = scenes.hang(4, seed=1).sheets[0]
+    s["x"] = (s["x"] * np.array([1.05, 1.08, 1.0])).astype(np.float64)  # stretched: G > 0, exact Hessian
+    s["x"][:, 2] = 0.0
+    assert _fd_check(s, "face") < 1e-6
+
+
+def test_fp64_bending_jacobian_matches_finite_differences_at_zero_angle():
+    s = scenes.hang(4, seed=1).sheets[0]
+    s["x"] = s["x"].astype(np.float64)
+    s["x"][:, 2] = 0.0  # flat: theta = 0, where the Gauss-Newton Jacobian is exact
+    s["x"][:, :2] += np.random.default_rng(0).normal(0, 0.01, (s["x"].shape[0], 2))
+    assert _fd_check(s, "edge") < 1e-5
+
+
+def test_flat_sheet_at_rest_has_no_internal_force():
+    s = scenes.hang(6, seed=0).sheets[0]
+    s["x"][:, 2] = 0.0
+    c = pyoracle.Cloth(s, pyoracle.Material(s["material"], "double"))
+    ff, _ = c.face_forces()
+    ef, _, th = c.edge_forces()
+    assert np.abs(ff).max() < 1e-12 and np.abs(ef).max() < 1e-12 and np.abs(th).max() < 1e-12
+
+
+def _scipy_system(rp, ci, val, n):
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    I = (3 * rows[:, None, None] + np.arange(3)[None, :, None]).repeat(3, 2)
+    J = (3 * ci[:, None, None] + np.arange(3)[None, None, :]).repeat(3, 1)
+    return sp.csr_matrix((val.reshape(-1), (I.reshape(-1), J.reshape(-1))), shape=(3 * n, 3 * n))
+
+
+def test_sparse_cholesky_and_pcg_match_scipy():
+    scene = scenes.hang(10, seed=4)
+    s = scene.sheets[0]
+    c = pyoracle.Cloth(s, pyoracle.Material(s["material"], "float"))
+    rp, ci, val, b = c.assemble(scenes.step_params(scene, s))
+    A = _scipy_system(rp, ci, val, c.n)
+    ref = spla.spsolve(A.tocsc(), b)
+    d64, r64 = c.solve(pyoracle.METHOD_LLT64)
+    assert np.linalg.norm(d64 - ref) / np.linalg.norm(ref) < 1e-12 and r64 < 1e-13
+    d32, r32 = c.solve(pyoracle.METHOD_LLT)
+    assert np.linalg.norm(d32 - ref) / np.linalg.norm(ref) < 1e-3
+    dp, rr = c.solve(pyoracle.METHOD_PCG64, tol=1e-13)
+    assert np.linalg.norm(dp - ref) / np.linalg.norm(ref) < 1e-9 and rr < 1e-12
+
+
+def test_topology_counts_for_grid():
+    for nq in (1, 2, 5, 16):
+        s = scenes.hang(nq, seed=0).sheets[0]
+        c = pyoracle.Cloth(s, pyoracle.Material(s["material"]))
+        # a grid of nq x nq quads has 3nq^2 + 2nq edges, of which 4nq lie on the boundary
+        assert c.L.cloth_num_edges(c.h) == 3 * nq * nq + 2 * nq
+        assert c.n_interior == 3 * nq * nq - 2 * nq
