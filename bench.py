@@ -1,0 +1,378 @@
+"""Benchmark of the implicit cloth step on B200.
+
+Workload (default): 1,024 sheets of 64x64 quads (4,325,376 nodes), top edge pinned, per-sheet
+horizontal wind, stretching log-U[10, 500] N/m and bending log-U[1e-6, 1e-3] N m through the
+material multipliers, dt = 1/100 s: the learned-warm-start configuration, which fits one GPU.
+One step = assembly + batched PCG to an FP64-checked relative residual of 1e-6 for every sheet
++ v += dv, x += dt v, with the state resident in HBM.
+
+Metric: node-steps/s (sum over sheets of nodes x steps / device time).  The line reports the
+mixed-precision solver with its warm start (`value`) and the plain FP32 PCG from a zero guess
+on the same GPU (`plain_fp32`).  `--impl reference` times the reference's CPU path for this
+workload (the reference's own force code compiled from its sources + FP32 sparse Cholesky).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+       torchrun --nproc-per-node N bench.py --gpus N   (one rank per GPU, sheets per rank fixed)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "node-steps/s @ rel.res 1e-6: learned+mixed-prec batched PCG vs plain FP32 PCG"
+UNIT = "node-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--sheets", type=int, default=1024)
+    ap.add_argument("--nq", type=int, default=64)
+    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--warm", default="previous", choices=["previous", "zero", "learned"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 arm")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--host-loop", action="store_true",
+                    help="launch the solve loop from the host instead of the CUDA graph (profilers cannot "
+                         "see kernels inside a graph with conditional nodes)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [t.strip() for t in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        except FileNotFoundError:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def workload(args, rank):
+    from clothsimulator_b200 import scenes
+
+    return scenes.windy_batch(args.sheets, args.nq, seed=1000 + rank)
+
+
+def cpu_baseline(scene, seconds: float, which: str = "ref", threads: int = 1, n_steps: int = 1):
+    """Times the reference CPU path (FP32 assembly + FP32 sparse Cholesky, one sheet after
+    another as Simulator.cu:584-585 does) on a bounded sample of the workload's sheets."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from clothsimulator_b200 import scenes
+
+    if which == "ref" and not os.path.exists(pyoracle.LIB_REF):
+        which = "oracle"
+    kind = "reference" if which == "ref" else "port"
+    sheets = scene.sheets
+    # calibrate on one sheet (first step includes the symbolic analysis, as SimplicialLLT does)
+    mk = (lambda s: pyoracle.Cloth(s, pyoracle.Material(s["material"], which=which))) if which == "ref" else \
+        (lambda s: pyoracle.Cloth(s, pyoracle.Material(s["material"], "float")))
+    c0 = mk(sheets[0])
+    t0 = time.perf_counter()
+    c0.step(scenes.step_params(scene, sheets[0]), pyoracle.METHOD_LLT)
+    one = max(time.perf_counter() - t0, 1e-4)
+    count = int(max(threads, min(len(sheets), math.ceil(seconds * threads / (one * n_steps)))))
+    cloths = [mk(s) for s in sheets[:count]]
+    params = [scenes.step_params(scene, s) for s in sheets[:count]]
+    sec, status = pyoracle.run_cloths(cloths, params, n_steps, pyoracle.METHOD_LLT, threads)
+    nodes = sum(s["x"].shape[0] for s in sheets[:count])
+    return {
+        "value": nodes * n_steps / sec,
+        "unit": UNIT,
+        "cores": threads,
+        "kind": kind,
+        "sample": f"{count} of {len(sheets)} sheets ({scene.name}), {n_steps} step(s) each, "
+                  f"{'reference force code' if kind == 'reference' else 'restated force code'} + FP32 sparse LL^T, "
+                  f"{sec:.1f} s on {threads} thread(s)",
+        "failed_solves": int((status < -1).sum()),
+    }
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    scene = workload(args, 0)
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(max(1, args.warmup)):
+        cpu_baseline(scene, 2.0, "ref", threads)
+    samples = []
+    for _ in range(args.steps):
+        r = cpu_baseline(scene, args.cpu_seconds / max(1, args.steps) * 4, "ref", threads)
+        vals.append(r["value"])
+        samples.append(r["sample"])
+    value = statistics.median(vals)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": scene.name, "sheets": len(scene.sheets), "nodes": scene.n_nodes, "tol": args.tol},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": r["kind"], "sample": samples[-1]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from clothsimulator_b200 import native
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("gloo", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    scene = workload(args, rank)
+    ctx = native.Context(local)
+    ctx.load(scene.sheets)
+    sizes = ctx.sizes
+    N = sizes[0]
+    x0 = np.concatenate([s["x"] for s in scene.sheets])
+    v0 = np.concatenate([s["v"] for s in scene.sheets])
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    warm_mode = {"previous": native.WARM_PREVIOUS, "zero": native.WARM_ZERO, "learned": native.WARM_LEARNED}[args.warm]
+
+    def timed_arm(precision, warm, clocks=None):
+        ctx.set_state(x0, v0)
+        p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol, max_iters=4000,
+                               precision=precision, warm_start=native.WARM_ZERO, use_graph=0 if args.host_loop else 1)
+        stats_w = []
+        for i in range(args.warmup):
+            st, _ = ctx.step(p, allow_unconverged=True)
+            stats_w.append(st.as_dict())
+            p.warm_start = warm
+        c0 = ctx.counters()
+        barrier()
+        torch.cuda.synchronize()
+        ctx.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(local) if clocks is not None else None
+        if sampler:
+            sampler.__enter__()
+        e0.record(stream)
+        for i in range(args.steps):
+            ctx.step_async(p)
+        e1.record(stream)
+        e1.synchronize()
+        if sampler:
+            sampler.__exit__()
+            clocks.update(sampler.summary())
+        torch.cuda.synchronize()
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        c1 = ctx.counters()
+        # one untimed step with statistics for the report
+        st, _ = ctx.step(p, allow_unconverged=True)
+        it, rr, fl = ctx.instance_stats()
+        return {
+            "ms": ms,
+            "launches": c1["launches"] - c0["launches"],
+            "trips": c1["trips"] - c0["trips"],
+            "after": st.as_dict(),
+            "iters_mean": float(it.mean()),
+            "iters_max": int(it.max()),
+            "converged_frac": float(np.mean((fl & 1) > 0)),
+            "max_relres": float(rr.max()),
+        }
+
+    clocks = {}
+    best = timed_arm(native.PREC_MIXED, warm_mode if warm_mode != native.WARM_LEARNED else native.WARM_PREVIOUS,
+                     clocks)
+    node_steps = N * args.steps * world
+    value = node_steps / (best["ms"] / 1e3)
+    plain = None
+    if not args.no_plain:
+        pr = timed_arm(native.PREC_PLAIN_FP32, native.WARM_ZERO)
+        plain = {"value": node_steps / (pr["ms"] / 1e3), "ms_per_step": pr["ms"] / args.steps,
+                 "iters_mean": pr["iters_mean"], "iters_max": pr["iters_max"],
+                 "converged_frac": pr["converged_frac"], "max_relres": pr["max_relres"]}
+
+    # dominant kernel roofline (SpMV of a CG iteration), timed live on the context's stream
+    prof = ctx.profile_kernels(native.step_params(scene.dt, scene.gravity, scene.handle_stiffness), reps=20)
+    nnzb = sizes[6]
+    spmv_bytes = nnzb * 40 + N * 48
+    achieved = spmv_bytes / (prof["spmv"] * 1e-3) / 1e9
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+    if os.path.exists(tr_path):
+        t = json.load(open(tr_path))
+        if t.get("nodes") and t.get("dram_bytes"):
+            traffic = t["dram_bytes"] * N / t["nodes"]
+
+    # end to end through the C ABI with pinned host buffers: H2D of x, v, step, D2H of x, v
+    hx = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
+    hv = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
+    hx.numpy()[:] = x0
+    hv.numpy()[:] = v0
+    fp = native._fp
+    import ctypes as C
+
+    px = C.cast(hx.data_ptr(), fp)
+    pv = C.cast(hv.data_ptr(), fp)
+    p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol, max_iters=4000,
+                           precision=native.PREC_MIXED, warm_start=native.WARM_ZERO, use_graph=0 if args.host_loop else 1)
+    ctx.set_state(x0, v0)
+    for i in range(args.warmup):
+        ctx.check(ctx.lib.cs_set_state(ctx.h, px, pv))
+        ctx.step(p, allow_unconverged=True)
+        ctx.check(ctx.lib.cs_get_state(ctx.h, px, pv))
+        p.warm_start = native.WARM_PREVIOUS
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for i in range(args.steps):
+        ctx.check(ctx.lib.cs_set_state(ctx.h, px, pv))
+        ctx.step_async(p)
+        ctx.check(ctx.lib.cs_get_state(ctx.h, px, pv))
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), wall * 1e3))
+    e2e = {"value": node_steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 2 * 12 * N,
+           "d2h_bytes_per_step": 2 * 12 * N}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(scene, args.cpu_seconds, "ref", 1)
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": best["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {
+                "workload": scene.name, "sheets": len(scene.sheets), "nq": args.nq, "nodes_per_gpu": N,
+                "nnzb_per_gpu": nnzb, "tol": args.tol, "solver": "mixed FP32 PCG + FP64 refinement",
+                "warm_start": "previous dv" if args.warm != "zero" else "zero",
+                "l2": "inputs larger than L2 (system matrix %.2f GB per GPU)" % (sizes[3] * 36 / 1e9),
+                "parallelism": f"sheets x{world} (no collective on the data path)",
+                "launch": "host loop" if args.host_loop else "CUDA graph with a device-driven while loop",
+            },
+            "iters_mean": best["iters_mean"], "iters_max": best["iters_max"],
+            "converged_frac": best["converged_frac"], "max_relres": best["max_relres"],
+            "plain_fp32": plain,
+            "speedup_vs_plain_fp32": (value / plain["value"]) if plain else None,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": "cs_spmv_kernel",
+                         "bytes_per_launch": spmv_bytes, "ms_per_launch": prof["spmv"],
+                         "peak_source": "measured" if peaks else "fallback"},
+            "kernel_ms": prof,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": best["launches"],
+            "clocks": clocks,
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

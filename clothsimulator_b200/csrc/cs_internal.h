@@ -87,7 +87,7 @@ struct InstState {
     int iters;          // total CG iterations this step
     int sweeps;         // FP64 residual evaluations this step
     int flags;
-    int resumes;        // plain FP32 solver: failed FP64 checks after which CG resumed
+    int pad;
 };
 
 // Step parameters in device memory (read by every kernel of the captured step graph).

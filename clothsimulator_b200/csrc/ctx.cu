@@ -41,6 +41,7 @@ __global__ void cs_solve_prologue_kernel(Batch B);
 __global__ void cs_solve_setup_kernel(Batch B);
 __global__ void cs_advance_kernel(Batch B);
 __global__ void cs_spmv_plain_kernel(Batch B, const float* x, float* y);
+__global__ void cs_profile_setup_kernel(Batch B, int phase);
 
 namespace {
 
@@ -382,6 +383,8 @@ struct cs_ctx {
     cudaGraph_t graph = nullptr;
     DevParams hostParams{};
     bool lastStepValid = false;
+    long long steps = 0, hostLaunches = 0, graphSteps = 0;
+    int launchesPerStepFixed = 0;
 };
 
 namespace {
@@ -435,11 +438,13 @@ void freeBatch(cs_ctx* c) {
 
 inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
-void launchAssembly(cs_ctx* c) {
+int launchAssembly(cs_ctx* c) {
     Batch& B = c->B;
-    if (B.F) cs_face_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B);
-    if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B);
+    int n = 1;
+    if (B.F) cs_face_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B), n++;
+    if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B), n++;
     cs_gather_kernel<<<nblk((long long)B.n_slices * 32, 128), 128, 0, c->stream>>>(B);
+    return n;
 }
 
 void launchSolvePrologue(cs_ctx* c) {
@@ -502,7 +507,7 @@ DevParams toDev(const cs_step_params* p) {
     d.tol = p->tol > 0 ? p->tol : 1e-6;
     d.inner_tol = p->inner_tol > 0 ? p->inner_tol : 1e-4;
     d.max_iters = p->max_iters > 0 ? p->max_iters : 2000;
-    d.sweep_cap = p->sweep_cap > 0 ? p->sweep_cap : (p->precision == CS_PREC_MIXED ? 1000000 : 20);
+    d.sweep_cap = p->sweep_cap > 0 ? p->sweep_cap : 1000000;
     d.mixed = p->precision == CS_PREC_MIXED;
     d.warm = p->warm_start != CS_WARM_ZERO;
     d.loop_cap = 2 * d.max_iters + 256;
@@ -800,13 +805,13 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     AL(part, 2LL * B.n_slices);
     AL(inst, B.S);
     AL(params, 1);
-    AL(loop, 4);
+    AL(loop, 8);
 #undef AL
     CS_CUDA(cudaMemset(B.dv, 0, 3LL * B.N * sizeof(float)));
     CS_CUDA(cudaMemset(B.warm, 0, 3LL * B.N * sizeof(float)));
     CS_CUDA(cudaMemset(B.A, 0, (size_t)B.n_panels * CS_PANEL_FLOATS * sizeof(float)));
     CS_CUDA(cudaMemset(B.inst, 0, B.S * sizeof(InstState)));
-    CS_CUDA(cudaMemset(B.loop, 0, 4 * sizeof(int)));
+    CS_CUDA(cudaMemset(B.loop, 0, 8 * sizeof(int)));
     CS_CUDA(cudaDeviceSynchronize());
     c->loaded = true;
     return CS_OK;
@@ -911,13 +916,14 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
         if ((st = buildGraph(c)) != CS_OK) return st;
         CS_CUDA(cudaGraphLaunch(c->graphExec, c->stream));
     } else {
-        launchAssembly(c);
+        c->hostLaunches += launchAssembly(c) + 3;
         launchSolvePrologue(c);
         int go = 1;
         int trips = 0;
         while (go) {
             for (int t = 0; t < 8; t++) launchTrip(c, 0);
             trips += 8;
+            c->hostLaunches += 32;
             CS_CUDA(cudaMemcpyAsync(&go, c->B.loop + 3, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
             CS_CUDA(cudaStreamSynchronize(c->stream));
             if (trips > d.loop_cap + 16) break;
@@ -927,9 +933,14 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
     CS_CUDA(cudaGetLastError());
     CS_CUDA(cudaEventRecord(c->ev1, c->stream));
     c->lastStepValid = true;
+    c->steps++;
+    if (p->use_graph) {
+        c->graphSteps++;
+        c->launchesPerStepFixed = (c->B.F ? 1 : 0) + (c->B.E ? 1 : 0) + 1 + 3;
+    }
     if (!stats) return CS_OK;
     std::vector<InstState> inst(c->B.S);
-    int loopv[4];
+    int loopv[8];
     CS_CUDA(cudaMemcpyAsync(inst.data(), c->B.inst, c->B.S * sizeof(InstState), cudaMemcpyDeviceToHost, c->stream));
     CS_CUDA(cudaMemcpyAsync(loopv, c->B.loop, sizeof(loopv), cudaMemcpyDeviceToHost, c->stream));
     CS_CUDA(cudaStreamSynchronize(c->stream));
@@ -1071,6 +1082,72 @@ cs_status cs_spmv(cs_ctx* c, const float* x, float* y) {
     cudaFree(dx);
     cudaFree(dy);
     if (e != cudaSuccess) return fail(c, CS_ERR_CUDA, "spmv: %s", cudaGetErrorString(e));
+    return CS_OK;
+}
+
+cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float* ms) {
+    if (!c || !ms || reps <= 0) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    cs_status st = validateParams(c, p);
+    if (st != CS_OK) return st;
+    CS_CUDA(cudaSetDevice(c->device));
+    Batch& B = c->B;
+    DevParams d = toDev(p);
+    CS_CUDA(cudaMemcpyAsync(B.params, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
+    launchAssembly(c);
+    const int g = nblk((long long)B.n_slices * 32, 128);
+    auto timeIt = [&](int which) -> float {
+        cudaEventRecord(c->ev0, c->stream);
+        for (int r = 0; r < reps; r++) {
+            switch (which) {
+                case 0: if (B.F) cs_face_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B); break;
+                case 1: if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B); break;
+                case 2: cs_gather_kernel<<<g, 128, 0, c->stream>>>(B); break;
+                case 3: cs_spmv_kernel<<<g, 128, 0, c->stream>>>(B); break;
+                case 4: cs_vector_kernel<<<g, 128, 0, c->stream>>>(B); break;
+                case 5: cs_reduce1_kernel<<<B.S, 128, 0, c->stream>>>(B); break;
+                case 6: cs_spmv_kernel<<<g, 128, 0, c->stream>>>(B); break;
+            }
+        }
+        cudaEventRecord(c->ev1, c->stream);
+        cudaEventSynchronize(c->ev1);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, c->ev0, c->ev1);
+        return t / reps;
+    };
+    for (int k = 0; k < 3; k++) ms[k] = timeIt(k);
+    // solver kernels with every instance held in one phase
+    cs_solve_setup_kernel<<<B.S, 128, 0, c->stream>>>(B);
+    cs_solve_prologue_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B);
+    cs_profile_setup_kernel<<<nblk(B.S, 128), 128, 0, c->stream>>>(B, PH_CG);
+    ms[3] = timeIt(3);
+    ms[4] = timeIt(4);
+    ms[5] = timeIt(5);
+    cs_profile_setup_kernel<<<nblk(B.S, 128), 128, 0, c->stream>>>(B, PH_RES);
+    ms[6] = timeIt(6);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    c->lastStepValid = false;
+    return CS_OK;
+}
+
+cs_status cs_get_counters(cs_ctx* c, long long* out) {
+    if (!c || !out) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    int loopv[8];
+    CS_CUDA(cudaMemcpyAsync(loopv, c->B.loop, sizeof(loopv), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    long long trips = (long long)(unsigned)loopv[4];
+    out[0] = c->steps;
+    out[1] = trips;
+    // graph steps: fixed kernels plus four per loop trip; host-driven steps are counted directly
+    out[2] = c->hostLaunches + c->graphSteps * c->launchesPerStepFixed + 4 * trips;
+    return CS_OK;
+}
+
+cs_status cs_get_stream(cs_ctx* c, void** stream) {
+    if (!c || !stream) return CS_ERR_INVALID_ARG;
+    *stream = (void*)c->stream;
     return CS_OK;
 }
 

@@ -9,7 +9,7 @@
 //   cs_spmv_kernel    PH_CG : p_new = z + beta p_old (fused), q = A p_new, partial p.q
 //                     PH_RES: r = b - A (dv64 + e) in FP64, partial ||r||^2
 //   cs_reduce1_kernel PH_CG : alpha = rz / pq
-//                     PH_RES: accept (PH_FINISH), restart (PH_INIT) or resume (plain FP32)
+//                     PH_RES: accept (PH_FINISH) or restart a sweep (PH_INIT)
 //   cs_vector_kernel  PH_CG : e += alpha p, r -= alpha q, z = P^-1 r, partials r.z, r.r
 //                     PH_INIT / PH_FINISH: dv64 += e, e = 0 (and z, r.z for a new sweep)
 //   cs_reduce2_kernel PH_CG : beta, inner stopping test; the last block counts unfinished
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(128) cs_reduce1_kernel(Batch B) {
     if (res <= P.tol * bn || bn == 0.0) {
         I.flags |= CS_IF_CONVERGED;
         I.phase = PH_FINISH;
-    } else if (I.iters >= P.max_iters || (I.flags & CS_IF_BREAKDOWN) && !mixed) {
+    } else if (I.iters >= P.max_iters) {
         I.flags |= CS_IF_CAPPED;
         I.phase = PH_FINISH;
     } else if (mixed || I.rz == 0.0) {
@@ -204,8 +204,10 @@ __global__ void __launch_bounds__(128) cs_reduce1_kernel(Batch B) {
         I.res0 = res;
         I.phase = PH_INIT;
     } else {
-        I.resumes += 1;
-        I.phase = PH_RES + 100;  // plain FP32: resume the same Krylov sequence (cs_reduce2_kernel)
+        // Plain FP32 PCG stopped on its own recursive residual; the FP64 check above measured
+        // its true residual, which FP32 rounding can keep above tol.  It ends here, unconverged.
+        I.flags |= CS_IF_CAPPED;
+        I.phase = PH_FINISH;
     }
 }
 
@@ -314,7 +316,7 @@ __global__ void __launch_bounds__(128) cs_reduce2_kernel(Batch B, cudaGraphCondi
                 if (mixed)
                     stop = rn <= P.inner_tol * I.res0 || rn <= 0.5 * P.tol * bn || I.sweep_iters >= P.sweep_cap;
                 else
-                    stop = (I.resumes == 0) ? (rn <= P.tol * bn) : (I.sweep_iters >= P.sweep_cap);
+                    stop = rn <= P.tol * bn;
                 if (!finite_d((double)beta) || !(rz > 0.0) || (I.flags & CS_IF_BREAKDOWN)) {
                     beta = 0.f;
                     stop = true;
@@ -325,12 +327,7 @@ __global__ void __launch_bounds__(128) cs_reduce2_kernel(Batch B, cudaGraphCondi
             }
         }
     } else if (threadIdx.x == 0) {
-        if (ph == PH_RES + 100) {
-            I.phase = PH_CG;
-            I.sweep_iters = 0;
-        } else if (ph == PH_FINISH) {
-            I.phase = PH_DONE;
-        }
+        if (ph == PH_FINISH) I.phase = PH_DONE;
     }
     if (threadIdx.x == 0) {
         if (I.phase != PH_DONE) atomicAdd(&B.loop[1], 1);
@@ -341,6 +338,7 @@ __global__ void __launch_bounds__(128) cs_reduce2_kernel(Batch B, cudaGraphCondi
             int remaining = atomicAdd(&B.loop[1], 0);
             int trips = B.loop[0] + 1;
             B.loop[0] = trips;
+            B.loop[4] += 1;  // cumulative trips since load
             int go = (remaining > 0 && trips < P.loop_cap) ? 1 : 0;
             B.loop[3] = go;
             if (handle) cudaGraphSetConditional(handle, go);
@@ -375,7 +373,7 @@ __global__ void __launch_bounds__(128) cs_solve_setup_kernel(Batch B) {
         I.res0 = sqrt(acc);
         I.resnorm = I.first_res = -1.0;
         I.alpha = I.beta = 0.f;
-        I.sweep_iters = I.iters = I.sweeps = I.flags = I.resumes = 0;
+        I.sweep_iters = I.iters = I.sweeps = I.flags = 0;
         I.phase = B.params->warm ? PH_RES : PH_INIT;
         if (s == 0) {
             B.loop[0] = 0;
@@ -425,4 +423,16 @@ __global__ void __launch_bounds__(128) cs_spmv_plain_kernel(Batch B, const float
     y[3 * row] = y0;
     y[3 * row + 1] = y1;
     y[3 * row + 2] = y2;
+}
+
+// Measurement only: holds every instance in one phase with finite solver scalars so that a
+// single solver kernel can be timed in isolation (cs_profile_kernels).
+__global__ void cs_profile_setup_kernel(Batch B, int phase) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= B.S) return;
+    InstState& I = B.inst[s];
+    I.phase = phase;
+    I.alpha = 0.25f;
+    I.beta = 0.5f;
+    I.rz = 1.0;
 }

@@ -33,7 +33,7 @@ EXPORTED = [
     "cs_create", "cs_destroy", "cs_last_error", "cs_load_batch", "cs_get_sizes", "cs_set_state", "cs_get_state",
     "cs_set_state_device", "cs_get_state_device", "cs_step", "cs_sync", "cs_set_warm_start", "cs_get_dv",
     "cs_get_instance_stats", "cs_assemble", "cs_get_system", "cs_get_element_forces", "cs_spmv",
-    "cs_device_pointers",
+    "cs_device_pointers", "cs_profile_kernels", "cs_get_counters", "cs_get_stream",
 ]
 
 
@@ -113,6 +113,9 @@ def load_library() -> ctypes.CDLL:
         "cs_get_element_forces": [vp, _fp, _fp, _fp, _fp, _ip],
         "cs_spmv": [vp, _fp, _fp],
         "cs_device_pointers": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)],
+        "cs_profile_kernels": [vp, ctypes.POINTER(StepParams), ctypes.c_int, _fp],
+        "cs_get_counters": [vp, ctypes.POINTER(ctypes.c_longlong)],
+        "cs_get_stream": [vp, ctypes.POINTER(vp)],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -255,7 +258,7 @@ class Context:
 
     def step(self, params: StepParams, allow_unconverged: bool = False):
         stats = StepStats()
-        allow = (CS_OK, CS_ERR_NOT_CONVERGED) if allow_unconverged else (CS_OK,)
+        allow = (CS_OK, CS_ERR_NOT_CONVERGED, CS_ERR_NON_SPD) if allow_unconverged else (CS_OK,)
         st = self.check(self.lib.cs_step(self.h, ctypes.byref(params), ctypes.byref(stats)), allow)
         return stats, st
 
@@ -318,3 +321,20 @@ class Context:
         x, v, dv = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
         self.check(self.lib.cs_device_pointers(self.h, ctypes.byref(x), ctypes.byref(v), ctypes.byref(dv)))
         return x.value, v.value, dv.value
+
+    KERNELS = ["face", "edge", "gather", "spmv", "vector", "reduce", "spmv_fp64"]
+
+    def profile_kernels(self, params: StepParams, reps: int = 20) -> dict:
+        ms = (ctypes.c_float * 8)()
+        self.check(self.lib.cs_profile_kernels(self.h, ctypes.byref(params), reps, ms))
+        return {k: float(ms[i]) for i, k in enumerate(self.KERNELS)}
+
+    def counters(self):
+        out = (ctypes.c_longlong * 3)()
+        self.check(self.lib.cs_get_counters(self.h, out))
+        return {"steps": int(out[0]), "trips": int(out[1]), "launches": int(out[2])}
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self.check(self.lib.cs_get_stream(self.h, ctypes.byref(s)))
+        return s.value or 0

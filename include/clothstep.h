@@ -64,6 +64,11 @@ typedef struct cs_sheet_desc {
     float wind_density, wind_drag, wind_velocity[3];
 } cs_sheet_desc;
 
+/* CS_PREC_PLAIN_FP32: FP32 PCG with FP32 dot products from the guess, stopping when its own
+ * recursive residual meets tol (as the reference's solve does, Cloth.cu:784-788); its true
+ * residual is then checked in FP64 and reported, and the sheet counts as converged only if that
+ * meets tol.  CS_PREC_MIXED: FP32 PCG sweeps with FP64 dot products inside FP64 iterative
+ * refinement (outer residual b - A dv in FP64) until the FP64 residual meets tol. */
 enum { CS_PREC_PLAIN_FP32 = 0, CS_PREC_MIXED = 1 };
 enum { CS_WARM_ZERO = 0, CS_WARM_PREVIOUS = 1, CS_WARM_LEARNED = 2, CS_WARM_GIVEN = 3 };
 
@@ -77,7 +82,7 @@ typedef struct cs_step_params {
     double tol;               /* relative residual ||b - A dv|| / ||b||, checked in FP64 */
     double inner_tol;         /* mixed precision: residual reduction per CG sweep */
     int max_iters;            /* CG iterations per sheet per step */
-    int sweep_cap;            /* CG iterations per sweep (mixed) / between FP64 checks (plain) */
+    int sweep_cap;            /* mixed precision: CG iterations per sweep (0: no cap) */
     int precision;            /* CS_PREC_* */
     int warm_start;           /* CS_WARM_* */
     int advance;              /* 1: v += dv and x += dt v (a full step); 0: solve only */
@@ -152,6 +157,20 @@ cs_status cs_get_element_forces(cs_ctx* ctx, float* face_f, float* face_J, float
 cs_status cs_spmv(cs_ctx* ctx, const float* x, float* y);
 /* Device pointers of the batch state, for zero-copy callers: x, v, dv (3N floats each). */
 cs_status cs_device_pointers(cs_ctx* ctx, float** x, float** v, float** dv);
+
+/* --- Measurement entry points --------------------------------------------------------------
+ * The reference's only instrumentation is per-phase wall clock after cudaDeviceSynchronize
+ * (Simulator.cu:845-855); these time on the device instead. */
+
+/* Times each kernel of the step in isolation with CUDA events on the context's stream, `reps`
+ * launches each, on the current batch: ms[0] face, [1] edge, [2] gather (assembly),
+ * [3] SpMV of a CG iteration, [4] vector update of a CG iteration, [5] per-instance reduction,
+ * [6] FP64 residual SpMV.  Overwrites the solver's scratch vectors (not x, v or dv). */
+cs_status cs_profile_kernels(cs_ctx* ctx, const cs_step_params* params, int reps, float* ms);
+/* Cumulative counts since cs_load_batch: [0] steps, [1] solve-loop trips, [2] kernel launches. */
+cs_status cs_get_counters(cs_ctx* ctx, long long* counters);
+/* The cudaStream_t the context launches on (for callers that record events on it). */
+cs_status cs_get_stream(cs_ctx* ctx, void** stream);
 
 #ifdef __cplusplus
 }
