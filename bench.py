@@ -288,7 +288,7 @@ def run_ours(args):
     peaks = measured_peaks()
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     traffic = None
-    tr_path = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+    tr_path = os.path.join(ROOT, "profiles", "cs_spmv_kernel_windy128x64_traffic.json")
     if os.path.exists(tr_path):
         t = json.load(open(tr_path))
         if t.get("nodes") and t.get("dram_bytes"):
