@@ -34,6 +34,7 @@ EXPORTED = [
     "cs_set_state_device", "cs_get_state_device", "cs_step", "cs_sync", "cs_set_warm_start", "cs_get_dv",
     "cs_get_instance_stats", "cs_assemble", "cs_get_system", "cs_get_element_forces", "cs_spmv",
     "cs_device_pointers", "cs_profile_kernels", "cs_get_counters", "cs_get_stream",
+    "cs_solve_block_csr_noalloc",
 ]
 
 
@@ -116,6 +117,8 @@ def load_library() -> ctypes.CDLL:
         "cs_profile_kernels": [vp, ctypes.POINTER(StepParams), ctypes.c_int, _fp],
         "cs_get_counters": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "cs_get_stream": [vp, ctypes.POINTER(vp)],
+        "cs_solve_block_csr_noalloc": [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int,
+                                       vp, _ip, _dp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

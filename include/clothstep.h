@@ -172,6 +172,25 @@ cs_status cs_get_counters(cs_ctx* ctx, long long* counters);
 /* The cudaStream_t the context launches on (for callers that record events on it). */
 cs_status cs_get_stream(cs_ctx* ctx, void** stream);
 
+/* --- Allocation-free solve ------------------------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory (a host
+ * whose own allocator owns all device memory, real-time loops that must not allocate, plugins
+ * that may not grow the device footprint): solves one 3x3-block CSR system A x = b with the
+ * batched solver's scheme (FP32 block-Jacobi PCG, FP64 dots, FP64 iterative refinement to the
+ * relative residual tol), using a fixed 2 MiB static device array as scratch instead of
+ * allocating.  row_ptr (n_rows+1), col (nnzb), val (9*nnzb, row-major blocks), b and x (3*n_rows)
+ * are device pointers owned by the caller; stream is a cudaStream_t (NULL = default stream).
+ * n_rows above CS_NOALLOC_MAX_ROWS is rejected with CS_ERR_INVALID_ARG, as are out-of-range
+ * row pointers or columns.  Every call on a device shares the one scratch array: calls that
+ * overlap on the GPU race and must be serialised.  The first call on each device looks up the
+ * array's address (cudaGetSymbolAddress) with that device current; make it before any stream
+ * capture.  If iters or rel_residual (host pointers) are given, the call waits for the stream
+ * and returns CS_OK or CS_ERR_NOT_CONVERGED; otherwise it returns after the launch. */
+#define CS_NOALLOC_MAX_ROWS 16384
+cs_status cs_solve_block_csr_noalloc(int n_rows, int nnzb, const int32_t* row_ptr, const int32_t* col,
+                                     const float* val, const float* b, float* x, double tol, int max_iters,
+                                     void* stream, int* iters, double* rel_residual);
+
 #ifdef __cplusplus
 }
 #endif
