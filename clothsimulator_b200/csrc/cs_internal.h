@@ -4,7 +4,7 @@
 //   nodes   : x, v, dv as 3N floats (xyz interleaved), mass N, handle float4 N (xyz target,
 //             w = handle count), FP64 solution accumulator dv64 3N.
 //   faces   : int4 {n0, n1, n2, sheet} (global node ids), float4 inverse rest matrix
-//             (Face::inverse, Face.cu:16), rest area; one 128-byte element record per face.
+//             (Face::inverse, Face.cu:16), rest area; one 384-byte element record per face.
 //   edges   : interior edges only (the reference skips boundary edges, Cloth.cu:142):
 //             int4 {n0, n1, opposite0, opposite1}, int meta (face-vertex rotations), sheet,
 //             float4 {area0 + area1, bias weight side 0, side 1, 0}; one 128-byte record.
@@ -25,7 +25,7 @@
 #define CS_PANEL_FLOATS 288  // 32 lanes x 9 entries
 #define CS_TABLE_N 30
 #define CS_TABLE_ENTRIES (CS_TABLE_N * CS_TABLE_N * CS_TABLE_N)
-#define CS_FACE_REC 32
+#define CS_FACE_REC 96
 #define CS_EDGE_REC 32
 
 // Contributor code: bit 31 = edge (1) / face (0); bits 4..30 = sheet-local element id;
@@ -44,6 +44,7 @@ struct SheetDesc {
     int table;                  // stretching table id
     float bending[15];          // scaled bending samples, 3x5 (Material.cu:38-40)
     float wind_density, wind_drag, wind_v[3];
+    int nbr_ptr_off, nbr_off;   // this sheet's topology in the one-ring neighbour arrays
 };
 
 struct SliceDesc {
@@ -131,6 +132,9 @@ struct Batch {
     int* tcol = nullptr;         // per topology panel: 32 local column ids
     int* tcptr = nullptr;        // per topology slot: contributor range start (n_tpanels*32 + 1)
     uint32_t* tcontrib = nullptr;
+    int* nbr_ptr = nullptr;      // per topology: one-ring neighbour CSR (sheet-local ids)
+    int* nbr = nullptr;
+    int* node_sheet = nullptr;   // sheet of every node
     // system
     float* A = nullptr;          // n_panels * 288
     float* b = nullptr;          // 3N

@@ -27,6 +27,7 @@
 
 #include "../../include/clothstep.h"
 #include "cs_internal.h"
+#include "mlp.h"
 
 // kernels (forces.cu, pcg.cu)
 __global__ void cs_face_kernel(Batch B);
@@ -147,6 +148,8 @@ struct Topo {
     // block-CSR view for cs_get_system: per row, columns sorted, and the SELL slot of each
     std::vector<int> csr_ptr, csr_col, csr_slot;
     long long nnzb = 0;
+    // one-ring mesh neighbours (nodes sharing a face edge), sorted, for the learned warm start
+    std::vector<int> nbr_ptr, nbr;
 };
 
 struct TopoKey {
@@ -358,6 +361,21 @@ std::shared_ptr<Topo> buildTopo(const cs_sheet_desc& s, std::string& err) {
         t->csr_ptr[i + 1] = (int)t->csr_col.size();
     }
     t->nnzb = (long long)t->csr_col.size();
+    // one-ring neighbours
+    {
+        std::vector<std::vector<int>> nb(nn);
+        for (int f = 0; f < nf; f++)
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++)
+                    if (a != b) nb[t->fx[3 * f + a]].push_back(t->fx[3 * f + b]);
+        t->nbr_ptr.assign(nn + 1, 0);
+        for (int i = 0; i < nn; i++) {
+            std::sort(nb[i].begin(), nb[i].end());
+            nb[i].erase(std::unique(nb[i].begin(), nb[i].end()), nb[i].end());
+            t->nbr_ptr[i + 1] = t->nbr_ptr[i] + (int)nb[i].size();
+            t->nbr.insert(t->nbr.end(), nb[i].begin(), nb[i].end());
+        }
+    }
     return t;
 }
 
@@ -383,8 +401,15 @@ struct cs_ctx {
     cudaGraph_t graph = nullptr;
     DevParams hostParams{};
     bool lastStepValid = false;
-    long long steps = 0, hostLaunches = 0, graphSteps = 0;
-    int launchesPerStepFixed = 0;
+    long long steps = 0, hostLaunches = 0, graphSteps = 0, graphLaunchesFixed = 0;
+    // learned warm start
+    MlpDev mlp;
+    bool mlpInit = false;
+    int mlpGridTile = 0, mlpGridTrain = 0;
+    long long adamStep = 0;
+    float* mlpScratch = nullptr;  // per-epoch loss accumulators, gradient output
+    cudaGraphExec_t graphExecLearned = nullptr;
+    cudaGraph_t graphLearned = nullptr;
 };
 
 namespace {
@@ -427,8 +452,16 @@ cs_status upload(cs_ctx* c, T** p, const std::vector<T>& h) {
 void freeBatch(cs_ctx* c) {
     if (c->graphExec) cudaGraphExecDestroy(c->graphExec);
     if (c->graph) cudaGraphDestroy(c->graph);
+    if (c->graphExecLearned) cudaGraphExecDestroy(c->graphExecLearned);
+    if (c->graphLearned) cudaGraphDestroy(c->graphLearned);
     c->graphExec = nullptr;
     c->graph = nullptr;
+    c->graphExecLearned = nullptr;
+    c->graphLearned = nullptr;
+    c->mlp = MlpDev();
+    c->mlpInit = false;
+    c->adamStep = 0;
+    c->mlpScratch = nullptr;
     for (void* p : c->allocs) cudaFree(p);
     c->allocs.clear();
     c->B = Batch();
@@ -441,7 +474,7 @@ inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 int launchAssembly(cs_ctx* c) {
     Batch& B = c->B;
     int n = 1;
-    if (B.F) cs_face_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B), n++;
+    if (B.F) cs_face_kernel<<<nblk(B.F, 64), 64, 0, c->stream>>>(B), n++;
     if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B), n++;
     cs_gather_kernel<<<nblk((long long)B.n_slices * 32, 128), 128, 0, c->stream>>>(B);
     return n;
@@ -453,6 +486,17 @@ void launchSolvePrologue(cs_ctx* c) {
     cs_solve_prologue_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B);
 }
 
+// Learned warm start: features of the assembled system, layer 1, layers 2-3 + output; the
+// prediction replaces the previous dv in B.warm (the solve then starts from it).
+int launchMlpInference(cs_ctx* c, float* pred) {
+    Batch& B = c->B;
+    MlpDev& M = c->mlp;
+    cs_mlp_features_kernel<<<nblk(B.N, 256), 256, 0, c->stream>>>(B, M, M.feat);
+    cs_mlp_l1_kernel<<<c->mlpGridTile, 128, MLP_SMEM_L1, c->stream>>>(B, M, M.feat, 0, B.N, nullptr);
+    cs_mlp_l23_kernel<<<c->mlpGridTile, 128, MLP_SMEM_L23, c->stream>>>(B, M, 0, B.N, nullptr, nullptr, nullptr, pred);
+    return 3;
+}
+
 void launchTrip(cs_ctx* c, cudaGraphConditionalHandle h) {
     Batch& B = c->B;
     int g = nblk((long long)B.n_slices * 32, 128);
@@ -462,14 +506,16 @@ void launchTrip(cs_ctx* c, cudaGraphConditionalHandle h) {
     cs_reduce2_kernel<<<B.S, 128, 0, c->stream>>>(B, h);
 }
 
-cs_status buildGraph(cs_ctx* c) {
-    if (c->graphExec) return CS_OK;
+cs_status buildGraph(cs_ctx* c, bool learned) {
+    cudaGraphExec_t& exec = learned ? c->graphExecLearned : c->graphExec;
+    if (exec) return CS_OK;
     cudaGraph_t graph;
     CS_CUDA(cudaGraphCreate(&graph, 0));
-    c->graph = graph;
-    // prelude: assembly + solve setup, captured into the graph
+    (learned ? c->graphLearned : c->graph) = graph;
+    // prelude: assembly (+ learned warm start) + solve setup, captured into the graph
     CS_CUDA(cudaStreamBeginCaptureToGraph(c->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     launchAssembly(c);
+    if (learned) launchMlpInference(c, c->B.warm);
     launchSolvePrologue(c);
     cudaStreamCaptureStatus cst;
     const cudaGraphNode_t* deps = nullptr;
@@ -495,7 +541,7 @@ cs_status buildGraph(cs_ctx* c) {
     CS_CUDA(cudaStreamBeginCaptureToGraph(c->stream, graph, &loopNode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
     cs_advance_kernel<<<nblk(3LL * c->B.N, 256), 256, 0, c->stream>>>(c->B);
     CS_CUDA(cudaStreamEndCapture(c->stream, &graph));
-    CS_CUDA(cudaGraphInstantiate(&c->graphExec, graph, 0));
+    CS_CUDA(cudaGraphInstantiate(&exec, graph, 0));
     return CS_OK;
 }
 
@@ -643,6 +689,8 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     // per-topology arrays, concatenated
     std::vector<int> htcol, htcptr;
     std::vector<uint32_t> htcontrib;
+    std::vector<int> hnbr_ptr, hnbr, hnode_sheet;
+    std::vector<int> topoNbrPtr0(topos.size()), topoNbr0(topos.size());
     std::vector<int> topoPanel0(topos.size()), topoSlice0(topos.size());
     {
         int tp = 0, ts = 0;
@@ -654,6 +702,10 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             htcol.insert(htcol.end(), T.tcol.begin(), T.tcol.end());
             for (size_t i = 0; i + 1 < T.tcptr.size(); i++) htcptr.push_back(T.tcptr[i] + cbase);
             htcontrib.insert(htcontrib.end(), T.tcontrib.begin(), T.tcontrib.end());
+            topoNbrPtr0[t] = (int)hnbr_ptr.size();
+            topoNbr0[t] = (int)hnbr.size();
+            hnbr_ptr.insert(hnbr_ptr.end(), T.nbr_ptr.begin(), T.nbr_ptr.end());
+            hnbr.insert(hnbr.end(), T.nbr.begin(), T.nbr.end());
             tp += T.n_tpanels;
             ts += T.n_slices;
         }
@@ -676,6 +728,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         sd.n_slices = T.n_slices;
         sd.topo = sheetTopoId[s];
         sd.table = sheetTable[s];
+        sd.nbr_ptr_off = topoNbrPtr0[sheetTopoId[s]];
+        sd.nbr_off = topoNbr0[sheetTopoId[s]];
+        hnode_sheet.insert(hnode_sheet.end(), d.n_nodes, s);
         float bmult = m.bending_mult * m.thicken;
         for (int i = 0; i < 15; i++) sd.bending[i] = m.bending[i / 5][i % 5] * bmult;
         sd.wind_density = d.wind_density;
@@ -785,6 +840,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     UP(tcol, htcol);
     UP(tcptr, htcptr);
     UP(tcontrib, htcontrib);
+    UP(nbr_ptr, hnbr_ptr);
+    UP(nbr, hnbr);
+    UP(node_sheet, hnode_sheet);
 #undef UP
 #define AL(field, n) \
     if ((st = dalloc(c, &B.field, (size_t)(n))) != CS_OK) return st;
@@ -884,7 +942,8 @@ static cs_status validateParams(cs_ctx* c, const cs_step_params* p) {
         if (!std::isfinite(p->gravity[i])) return fail(c, CS_ERR_INVALID_ARG, "bad gravity");
     if (p->precision != CS_PREC_PLAIN_FP32 && p->precision != CS_PREC_MIXED) return fail(c, CS_ERR_INVALID_ARG, "bad precision");
     if (p->warm_start < CS_WARM_ZERO || p->warm_start > CS_WARM_GIVEN) return fail(c, CS_ERR_INVALID_ARG, "bad warm start");
-    if (p->warm_start == CS_WARM_LEARNED) return fail(c, CS_ERR_NOT_TRAINED, "learned warm start: no trained network");
+    if (p->warm_start == CS_WARM_LEARNED && !c->mlpInit)
+        return fail(c, CS_ERR_NOT_TRAINED, "learned warm start: no network (cs_mlp_init / cs_mlp_set_weights)");
     return CS_OK;
 }
 
@@ -912,18 +971,19 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
     c->hostParams = d;
     CS_CUDA(cudaMemcpyAsync(c->B.params, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
     CS_CUDA(cudaEventRecord(c->ev0, c->stream));
+    const bool learned = p->warm_start == CS_WARM_LEARNED;
     if (p->use_graph) {
-        if ((st = buildGraph(c)) != CS_OK) return st;
-        CS_CUDA(cudaGraphLaunch(c->graphExec, c->stream));
+        if ((st = buildGraph(c, learned)) != CS_OK) return st;
+        CS_CUDA(cudaGraphLaunch(learned ? c->graphExecLearned : c->graphExec, c->stream));
     } else {
         c->hostLaunches += launchAssembly(c) + 3;
+        if (learned) c->hostLaunches += launchMlpInference(c, c->B.warm);
         launchSolvePrologue(c);
         int go = 1;
         int trips = 0;
         while (go) {
             for (int t = 0; t < 8; t++) launchTrip(c, 0);
             trips += 8;
-            c->hostLaunches += 32;
             CS_CUDA(cudaMemcpyAsync(&go, c->B.loop + 3, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
             CS_CUDA(cudaStreamSynchronize(c->stream));
             if (trips > d.loop_cap + 16) break;
@@ -936,7 +996,7 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
     c->steps++;
     if (p->use_graph) {
         c->graphSteps++;
-        c->launchesPerStepFixed = (c->B.F ? 1 : 0) + (c->B.E ? 1 : 0) + 1 + 3;
+        c->graphLaunchesFixed += (c->B.F ? 1 : 0) + (c->B.E ? 1 : 0) + 1 + 3 + (learned ? 3 : 0);
     }
     if (!stats) return CS_OK;
     std::vector<InstState> inst(c->B.S);
@@ -1100,7 +1160,7 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
         cudaEventRecord(c->ev0, c->stream);
         for (int r = 0; r < reps; r++) {
             switch (which) {
-                case 0: if (B.F) cs_face_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B); break;
+                case 0: if (B.F) cs_face_kernel<<<nblk(B.F, 64), 64, 0, c->stream>>>(B); break;
                 case 1: if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B); break;
                 case 2: cs_gather_kernel<<<g, 128, 0, c->stream>>>(B); break;
                 case 3: cs_spmv_kernel<<<g, 128, 0, c->stream>>>(B); break;
@@ -1141,13 +1201,265 @@ cs_status cs_get_counters(cs_ctx* c, long long* out) {
     out[0] = c->steps;
     out[1] = trips;
     // graph steps: fixed kernels plus four per loop trip; host-driven steps are counted directly
-    out[2] = c->hostLaunches + c->graphSteps * c->launchesPerStepFixed + 4 * trips;
+    out[2] = c->hostLaunches + c->graphLaunchesFixed + 4 * trips;
     return CS_OK;
 }
 
 cs_status cs_get_stream(cs_ctx* c, void** stream) {
     if (!c || !stream) return CS_ERR_INVALID_ARG;
     *stream = (void*)c->stream;
+    return CS_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Learned warm start (no reference counterpart; network in mlp.cu).
+
+namespace {
+
+uint64_t splitmix(uint64_t& x) {
+    uint64_t z = (x += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+uint16_t to_bf16_bits(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+cs_status mlpUploadWeights(cs_ctx* c, const std::vector<float>& w) {
+    std::vector<uint16_t> wb(MLP_P);
+    for (int i = 0; i < MLP_P; i++) wb[i] = to_bf16_bits(w[i]);
+    CS_CUDA(cudaMemcpy(c->mlp.w, w.data(), MLP_P * sizeof(float), cudaMemcpyHostToDevice));
+    CS_CUDA(cudaMemcpy(c->mlp.wb, wb.data(), MLP_P * 2, cudaMemcpyHostToDevice));
+    CS_CUDA(cudaMemset(c->mlp.m, 0, MLP_P * sizeof(float)));
+    CS_CUDA(cudaMemset(c->mlp.v, 0, MLP_P * sizeof(float)));
+    c->adamStep = 0;
+    return CS_OK;
+}
+
+cs_status mlpCheckErr(cs_ctx* c) {
+    int e = 0;
+    CS_CUDA(cudaMemcpy(&e, c->mlp.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return fail(c, CS_ERR_TIMEOUT, "a tensor-core completion wait gave up");
+    return CS_OK;
+}
+
+// One forward + backward pass over sheets [s0, s1) of dataset slot `slot`; leaves the
+// per-CTA gradient partials and loss partials in place.
+void mlpForwardBackward(cs_ctx* c, int slot, int s0, int s1) {
+    Batch& B = c->B;
+    MlpDev& M = c->mlp;
+    const int n0 = c->sheets[s0].node_off;
+    const int n1 = c->sheets[s1 - 1].node_off + c->sheets[s1 - 1].n_nodes;
+    const float* f = M.dfeat + (size_t)slot * B.N * 16;
+    const float* tg = M.dtarget + (size_t)slot * B.N * 3;
+    cs_mlp_l1_kernel<<<c->mlpGridTile, 128, MLP_SMEM_L1, c->stream>>>(B, M, f, n0, n1, M.z1);
+    cs_mlp_l23_kernel<<<c->mlpGridTile, 128, MLP_SMEM_L23, c->stream>>>(B, M, n0, n1, M.z2, M.z3, M.y, nullptr);
+    cs_mlp_bwd23_kernel<<<c->mlpGridTrain, 128, MLP_SMEM_BWD23, c->stream>>>(B, M, n0, n1, tg);
+    cs_mlp_bwd1_kernel<<<c->mlpGridTrain, 128, MLP_SMEM_BWD1, c->stream>>>(B, M, f, n0, n1);
+}
+
+}  // namespace
+
+cs_status cs_mlp_init(cs_ctx* c, int slots, unsigned long long seed) {
+    if (!c || slots < 0) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    if (c->mlpInit) return fail(c, CS_ERR_STATE, "network already initialised for this batch");
+    CS_CUDA(cudaSetDevice(c->device));
+    cudaDeviceProp prop;
+    CS_CUDA(cudaGetDeviceProperties(&prop, c->device));
+    c->mlpGridTile = 2 * prop.multiProcessorCount;
+    c->mlpGridTrain = prop.multiProcessorCount;
+    CS_CUDA(cudaFuncSetAttribute(cs_mlp_l1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_SMEM_L1));
+    CS_CUDA(cudaFuncSetAttribute(cs_mlp_l23_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_SMEM_L23));
+    CS_CUDA(cudaFuncSetAttribute(cs_mlp_bwd23_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_SMEM_BWD23));
+    CS_CUDA(cudaFuncSetAttribute(cs_mlp_bwd1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_SMEM_BWD1));
+    MlpDev& M = c->mlp;
+    const long long N = c->B.N;
+    cs_status st;
+#define MA(field, n) \
+    if ((st = dalloc(c, &M.field, (size_t)(n))) != CS_OK) return st;
+    MA(w, MLP_P);
+    MA(wb, MLP_P);
+    MA(m, MLP_P);
+    MA(v, MLP_P);
+    MA(gpart, (long long)c->mlpGridTrain * MLP_P);
+    MA(loss_part, c->mlpGridTrain);
+    MA(stats, MLP_NSTAT);
+    MA(feat, N * 16);
+    MA(h1, N * 64);
+    MA(z1, N * 64);
+    MA(z2, N * 64);
+    MA(z3, N * 64);
+    MA(y, N * 3);
+    MA(du2, N * 128);
+    MA(dfeat, std::max(1LL, (long long)slots * N * 16));
+    MA(dtarget, std::max(1LL, (long long)slots * N * 3));
+    MA(err, 1);
+#undef MA
+    if ((st = dalloc(c, &c->mlpScratch, 4096 + MLP_P)) != CS_OK) return st;
+    M.slots = slots;
+    M.grid = c->mlpGridTrain;
+    CS_CUDA(cudaMemset(M.err, 0, sizeof(int)));
+    // initial weights: U(-1/sqrt(fan_in), 1/sqrt(fan_in)), output layer x0.1, zero biases
+    std::vector<float> w(MLP_P, 0.0f);
+    uint64_t rs = seed;
+    auto uni = [&](float a) { return a * (2.0f * (float)((splitmix(rs) >> 11) * (1.0 / 9007199254740992.0)) - 1.0f); };
+    for (int i = 0; i < 64 * 32; i++) w[MLP_W1 + i] = uni(1.0f / std::sqrt(32.0f));
+    for (int i = 0; i < 64 * 128; i++) w[MLP_W2 + i] = uni(1.0f / std::sqrt(128.0f));
+    for (int i = 0; i < 64 * 64; i++) w[MLP_W3 + i] = uni(1.0f / std::sqrt(64.0f));
+    for (int i = 0; i < 3 * 64; i++) w[MLP_W4 + i] = 0.1f * uni(1.0f / std::sqrt(64.0f));
+    if ((st = mlpUploadWeights(c, w)) != CS_OK) return st;
+    std::vector<float> stats(MLP_NSTAT, 0.0f);
+    for (int i = 0; i < 16; i++) stats[16 + i] = 1.0f;
+    for (int i = 0; i < 3; i++) stats[35 + i] = 1.0f;
+    CS_CUDA(cudaMemcpy(M.stats, stats.data(), MLP_NSTAT * sizeof(float), cudaMemcpyHostToDevice));
+    c->mlpInit = true;
+    return CS_OK;
+}
+
+cs_status cs_mlp_record(cs_ctx* c, int slot, int what) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    if (slot < 0 || slot >= c->mlp.slots || (what != 0 && what != 1)) return fail(c, CS_ERR_INVALID_ARG, "bad slot");
+    Batch& B = c->B;
+    float* f = c->mlp.dfeat + (size_t)slot * B.N * 16;
+    if (what == 0)
+        cs_mlp_features_kernel<<<nblk(B.N, 256), 256, 0, c->stream>>>(B, c->mlp, f);
+    else
+        cs_mlp_target_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B, f, c->mlp.dtarget + (size_t)slot * B.N * 3);
+    CS_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
+cs_status cs_mlp_fit_normalization(cs_ctx* c, int n_slots) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    if (n_slots <= 0 || n_slots > c->mlp.slots) return fail(c, CS_ERR_INVALID_ARG, "bad slot count");
+    const int blocks = 296;
+    double* part = nullptr;
+    CS_CUDA(cudaMalloc(&part, (size_t)blocks * 38 * sizeof(double)));
+    const long long n = (long long)n_slots * c->B.N;
+    cs_mlp_moments_kernel<<<blocks, 128, 0, c->stream>>>(c->mlp.dfeat, c->mlp.dtarget, n, part);
+    std::vector<double> h((size_t)blocks * 38);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(h.data(), part, h.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(part);
+    if (e != cudaSuccess) return fail(c, CS_ERR_CUDA, "moments: %s", cudaGetErrorString(e));
+    double sum[38] = {0};
+    for (int b = 0; b < blocks; b++)
+        for (int k = 0; k < 38; k++) sum[k] += h[38 * b + k];
+    std::vector<float> stats(MLP_NSTAT);
+    for (int k = 0; k < 16; k++) {
+        double mu = sum[k] / n, var = sum[19 + k] / n - mu * mu;
+        stats[k] = (float)mu;
+        stats[16 + k] = (float)std::max(std::sqrt(std::max(var, 0.0)), 1e-6 * std::max(std::fabs(mu), 1e-30) + 1e-30);
+    }
+    for (int k = 0; k < 3; k++) {
+        double mu = sum[16 + k] / n, var = sum[35 + k] / n - mu * mu;
+        stats[32 + k] = (float)mu;
+        stats[35 + k] = (float)std::max(std::sqrt(std::max(var, 0.0)), 1e-12);
+    }
+    CS_CUDA(cudaMemcpy(c->mlp.stats, stats.data(), MLP_NSTAT * sizeof(float), cudaMemcpyHostToDevice));
+    return CS_OK;
+}
+
+cs_status cs_mlp_gradient(cs_ctx* c, int slot, int s0, int s1, float* grad, float* loss) {
+    if (!c || !grad) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    if (slot < 0 || slot >= c->mlp.slots || s0 < 0 || s1 <= s0 || s1 > c->B.S)
+        return fail(c, CS_ERR_INVALID_ARG, "bad slot or sheet range");
+    float* acc = c->mlpScratch;
+    float* gout = c->mlpScratch + 4096;
+    CS_CUDA(cudaMemsetAsync(acc, 0, sizeof(float), c->stream));
+    mlpForwardBackward(c, slot, s0, s1);
+    cs_mlp_adam_kernel<<<nblk(MLP_P, 256), 256, 0, c->stream>>>(c->mlp, c->mlpGridTrain, 0.f, 0.f, 0.f, 0.f, 1, gout);
+    cs_mlp_loss_acc_kernel<<<1, 32, 0, c->stream>>>(c->mlp, c->mlpGridTrain, acc);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    CS_CUDA(cudaMemcpy(grad, gout, MLP_P * sizeof(float), cudaMemcpyDeviceToHost));
+    if (loss) CS_CUDA(cudaMemcpy(loss, acc, sizeof(float), cudaMemcpyDeviceToHost));
+    return mlpCheckErr(c);
+}
+
+cs_status cs_mlp_train(cs_ctx* c, int n_slots, int epochs, float lr, int sheets_per_batch, unsigned long long seed,
+                       float* epoch_loss) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    if (n_slots <= 0 || n_slots > c->mlp.slots || epochs <= 0 || epochs > 4096 || !(lr > 0) || sheets_per_batch <= 0)
+        return fail(c, CS_ERR_INVALID_ARG, "bad training arguments");
+    CS_CUDA(cudaSetDevice(c->device));
+    const int S = c->B.S;
+    const int groups = (S + sheets_per_batch - 1) / sheets_per_batch;
+    std::vector<std::pair<int, int>> order;
+    for (int sl = 0; sl < n_slots; sl++)
+        for (int g = 0; g < groups; g++) order.push_back({sl, g});
+    uint64_t rs = seed;
+    float* acc = c->mlpScratch;
+    CS_CUDA(cudaMemsetAsync(acc, 0, epochs * sizeof(float), c->stream));
+    for (int ep = 0; ep < epochs; ep++) {
+        for (size_t i = order.size(); i > 1; i--) std::swap(order[i - 1], order[splitmix(rs) % i]);
+        for (auto& o : order) {
+            const int s0 = o.second * sheets_per_batch, s1 = std::min(S, s0 + sheets_per_batch);
+            mlpForwardBackward(c, o.first, s0, s1);
+            c->adamStep++;
+            cs_mlp_adam_kernel<<<nblk(MLP_P, 256), 256, 0, c->stream>>>(c->mlp, c->mlpGridTrain, lr, 0.9f, 0.999f,
+                                                                       1e-8f, (int)c->adamStep, nullptr);
+            cs_mlp_loss_acc_kernel<<<1, 32, 0, c->stream>>>(c->mlp, c->mlpGridTrain, acc + ep);
+        }
+    }
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    if (epoch_loss) {
+        std::vector<float> h(epochs);
+        CS_CUDA(cudaMemcpy(h.data(), acc, epochs * sizeof(float), cudaMemcpyDeviceToHost));
+        for (int ep = 0; ep < epochs; ep++) epoch_loss[ep] = h[ep] / (float)order.size();
+    }
+    return mlpCheckErr(c);
+}
+
+cs_status cs_mlp_predict(cs_ctx* c, float* pred) {
+    if (!c || !pred) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    float* d = c->B.z;  // solver scratch, free between steps
+    launchMlpInference(c, d);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaMemcpyAsync(pred, d, 3 * (size_t)c->B.N * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    return mlpCheckErr(c);
+}
+
+cs_status cs_mlp_get_record(cs_ctx* c, int slot, float* feat, float* target) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    if (slot < 0 || slot >= c->mlp.slots) return fail(c, CS_ERR_INVALID_ARG, "bad slot");
+    const size_t N = c->B.N;
+    if (feat) CS_CUDA(cudaMemcpy(feat, c->mlp.dfeat + slot * N * 16, N * 16 * sizeof(float), cudaMemcpyDeviceToHost));
+    if (target) CS_CUDA(cudaMemcpy(target, c->mlp.dtarget + slot * N * 3, N * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+    return CS_OK;
+}
+
+cs_status cs_mlp_get_weights(cs_ctx* c, float* out, int n) {
+    if (!c || !out || n != CS_MLP_PARAMS) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    CS_CUDA(cudaMemcpy(out, c->mlp.w, MLP_P * sizeof(float), cudaMemcpyDeviceToHost));
+    CS_CUDA(cudaMemcpy(out + MLP_P, c->mlp.stats, MLP_NSTAT * sizeof(float), cudaMemcpyDeviceToHost));
+    return CS_OK;
+}
+
+cs_status cs_mlp_set_weights(cs_ctx* c, const float* in, int n) {
+    if (!c || !in || n != CS_MLP_PARAMS) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    for (int i = 0; i < n; i++)
+        if (!std::isfinite(in[i])) return fail(c, CS_ERR_INVALID_ARG, "non-finite weight");
+    std::vector<float> w(in, in + MLP_P);
+    cs_status st = mlpUploadWeights(c, w);
+    if (st != CS_OK) return st;
+    CS_CUDA(cudaMemcpy(c->mlp.stats, in + MLP_P, MLP_NSTAT * sizeof(float), cudaMemcpyHostToDevice));
     return CS_OK;
 }
 

@@ -6,8 +6,8 @@
 // reference's CPU assembly entry by entry.
 //
 // Kernels:
-//   cs_face_kernel   one thread per face: normal, wind drag, stretching force and the data
-//                    that determines its 9x9 Jacobian, and the face's right-hand-side terms.
+//   cs_face_kernel   one thread per face: normal, wind drag, stretching force, its 9x9
+//                    contribution -dt^2 J to A and the face's right-hand-side terms.
 //   cs_edge_kernel   one thread per interior edge: dihedral bending force, the rank-one
 //                    Jacobian factors (dtheta, coefficient) and the edge's right-hand side.
 //   cs_gather_kernel one warp per 32-row slice: every block (i, j) of A sums its
@@ -131,18 +131,21 @@ __device__ __forceinline__ float stretch_h(float fu_p, float fv_p, float fu_q, f
     return h;
 }
 
-__device__ __forceinline__ float sel3(float a, float b, float c, int i) { return i == 0 ? a : (i == 1 ? b : c); }
-
 }  // namespace
 
-// Face record (32 floats): [0..2] fu, [3..5] fv, [6..8] D row 0, [9..11] D row 1,
-// [12..15] stiffness k, [16] max(G00,0), [17] max(G11,0), [18] rest area,
-// [20..28] dt*(f + dt*J*v) of the stretching term, [29..31] dt * wind force per node.
-__global__ void __launch_bounds__(128) cs_face_kernel(Batch B) {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= B.F) return;
+// Face record (CS_FACE_REC = 96 floats): [0..80] the face's 9x9 contribution to A,
+// -dt*dt*J (row-major, block (a, b) at rows 3a..3a+2, columns 3b..3b+2), [81..89]
+// dt*(f + dt*J*v) of the stretching term, [90..92] dt * wind force added to each node.
+//
+// face_eval evaluates one face exactly as Face::update (normal), the wind loop of
+// Cloth::addExternalForces and stretchingForce (PhysicsHelper.cu:264-291) do.  With
+// rec != nullptr it writes the face record; with fo/Jo it writes f and J as stretchingForce
+// returns them (the inspection path).
+__device__ __forceinline__ void face_eval(const Batch& B, int f, float* __restrict__ rec, float* __restrict__ fo,
+                                          float* __restrict__ Jo) {
     const DevParams& P = *B.params;
     const float dt = P.dt;
+    const float s = -dt * dt;
     int4 fn = B.face_nodes[f];
     const SheetDesc& sh = B.sheets[fn.w];
     f3 x0 = ld3(B.x, fn.x), x1 = ld3(B.x, fn.y), x2 = ld3(B.x, fn.z);
@@ -162,7 +165,7 @@ __global__ void __launch_bounds__(128) cs_face_kernel(Batch B) {
     f3 force = dvd(scl(area, add(scl(sh.wind_density * absf_(vn) * vn, n), scl(sh.wind_drag, vt))), 3.0f);
     f3 fw = scl(dt, force);
 
-    // stretchingForce (PhysicsHelper.cu:264-291)
+    // F = [x1 - x0, x2 - x0] * inverse (Face.cu:109-111), G = (F^T F - I) / 2
     float F[3][2];
     {
         float e1a[3] = {e1.x, e1.y, e1.z}, e2a[3] = {e2.x, e2.y, e2.z};
@@ -185,56 +188,57 @@ __global__ void __launch_bounds__(128) cs_face_kernel(Batch B) {
     FtF11 += F[2][1] * F[2][1];
     float G00 = 0.5f * (FtF00 - 1.0f), G01 = 0.5f * (FtF01 - 0.0f), G11 = 0.5f * (FtF11 - 1.0f);
     float4 k = stretch_stiffness(B.tables + (size_t)sh.table * CS_TABLE_ENTRIES, G00, G01, G11);
-
-    float rec[20];
-    rec[0] = F[0][0]; rec[1] = F[1][0]; rec[2] = F[2][0];
-    rec[3] = F[0][1]; rec[4] = F[1][1]; rec[5] = F[2][1];
-    rec[6] = -inv.x - inv.z;  // D(0,0) = -Y00 - Y10
-    rec[7] = inv.x;           // D(0,1) = Y00
-    rec[8] = inv.z;           // D(0,2) = Y10
-    rec[9] = -inv.y - inv.w;  // D(1,0) = -Y01 - Y11
-    rec[10] = inv.y;          // D(1,1) = Y01
-    rec[11] = inv.w;          // D(1,2) = Y11
-    rec[12] = k.x; rec[13] = k.y; rec[14] = k.z; rec[15] = k.w;
-    rec[16] = maxf_(G00, 0.0f);
-    rec[17] = maxf_(G11, 0.0f);
-    rec[18] = area;
-    rec[19] = 0.0f;
-
-    // f = -area * grad, grad with the expression order of PhysicsHelper.cu:282.
+    const float gu = maxf_(G00, 0.0f), gv = maxf_(G11, 0.0f);
+    // D = [-Y.row0 - Y.row1, Y.row0, Y.row1] as columns (PhysicsHelper.cu:268-271)
+    const float D0[3] = {-inv.x - inv.z, inv.x, inv.z};
+    const float D1[3] = {-inv.y - inv.w, inv.y, inv.w};
+    const float fu[3] = {F[0][0], F[1][0], F[2][0]};
+    const float fv[3] = {F[0][1], F[1][1], F[2][1]};
     const float vel[9] = {v0.x, v0.y, v0.z, v1.x, v1.y, v1.z, v2.x, v2.y, v2.z};
-    float bs[9];
 #pragma unroll
     for (int p = 0; p < 9; p++) {
         const int a = p / 3, kp = p % 3;
-        const float D0a = rec[6 + a], D1a = rec[9 + a];
-        const float fu_p = rec[kp], fv_p = rec[3 + kp];
-        float fuu = D0a * fu_p, fvv = D1a * fv_p, fuv = 0.5f * (D0a * fv_p + D1a * fu_p);
+        const float fuu = D0[a] * fu[kp], fvv = D1[a] * fv[kp], fuv = 0.5f * (D0[a] * fv[kp] + D1[a] * fu[kp]);
+        // grad with the expression order of PhysicsHelper.cu:282; f = -area * grad
         float g = k.x * G00 * fuu;
         g += k.z * G11 * fvv;
         g += k.y * (G00 * fvv + G11 * fuu);
         g += 2.0f * k.w * G01 * fuv;
-        float fp = -area * g;
+        const float fp = -area * g;
         float jv = 0.0f;
 #pragma unroll
         for (int q = 0; q < 9; q++) {
             const int b = q / 3, kq = q % 3;
-            float h = stretch_h(fu_p, fv_p, rec[kq], rec[3 + kq], D0a, D1a, rec[6 + b], rec[9 + b], k.x, k.y, k.z,
-                                k.w, rec[16], rec[17], kp == kq);
-            float J = -area * h;
+            const float h = stretch_h(fu[kp], fv[kp], fu[kq], fv[kq], D0[a], D1[a], D0[b], D1[b], k.x, k.y, k.z, k.w,
+                                      gu, gv, kp == kq);
+            const float J = -area * h;
             jv += (dt * J) * vel[q];
+            if (rec) rec[9 * p + q] = s * J;
+            if (Jo) Jo[9 * p + q] = J;
         }
-        bs[p] = dt * (fp + jv);
+        if (rec) rec[81 + p] = dt * (fp + jv);
+        if (fo) fo[p] = fp;
     }
-    float4* out = reinterpret_cast<float4*>(B.face_rec + (size_t)f * CS_FACE_REC);
-    out[0] = make_float4(rec[0], rec[1], rec[2], rec[3]);
-    out[1] = make_float4(rec[4], rec[5], rec[6], rec[7]);
-    out[2] = make_float4(rec[8], rec[9], rec[10], rec[11]);
-    out[3] = make_float4(rec[12], rec[13], rec[14], rec[15]);
-    out[4] = make_float4(rec[16], rec[17], rec[18], 0.0f);
-    out[5] = make_float4(bs[0], bs[1], bs[2], bs[3]);
-    out[6] = make_float4(bs[4], bs[5], bs[6], bs[7]);
-    out[7] = make_float4(bs[8], fw.x, fw.y, fw.z);
+    if (rec) {
+        rec[90] = fw.x;
+        rec[91] = fw.y;
+        rec[92] = fw.z;
+    }
+}
+
+// One thread per face; the block's records are staged in shared memory (row stride 97 floats,
+// conflict-free) and written out as one contiguous, coalesced range.
+__global__ void __launch_bounds__(64) cs_face_kernel(Batch B) {
+    constexpr int kStride = CS_FACE_REC + 1;
+    __shared__ float stage[64 * kStride];
+    const int f0 = blockIdx.x * blockDim.x;
+    const int f = f0 + threadIdx.x;
+    if (f < B.F) face_eval(B, f, stage + threadIdx.x * kStride, nullptr, nullptr);
+    __syncthreads();
+    const int nf = min((int)blockDim.x, B.F - f0);
+    float* out = B.face_rec + (size_t)f0 * CS_FACE_REC;
+    for (int e = threadIdx.x; e < nf * CS_FACE_REC; e += blockDim.x)
+        out[e] = stage[(e / CS_FACE_REC) * kStride + e % CS_FACE_REC];
 }
 
 // Edge record (32 floats): [0..11] dtheta, [12] coefficient, [13] theta, [16..27]
@@ -355,26 +359,11 @@ __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
                 int elem = (int)((code >> 4) & 0x7FFFFFFu);
                 int ca = (code >> 2) & 3, cb = code & 3;
                 if (!(code & CS_CODE_EDGE)) {
-                    const float* rec = B.face_rec + (size_t)(sh.face_off + elem) * CS_FACE_REC;
-                    float r[20];
-                    const float4* r4 = reinterpret_cast<const float4*>(rec);
-#pragma unroll
-                    for (int t = 0; t < 5; t++) {
-                        float4 v = r4[t];
-                        r[4 * t] = v.x; r[4 * t + 1] = v.y; r[4 * t + 2] = v.z; r[4 * t + 3] = v.w;
-                    }
-                    const float ar = r[18];
-                    const float D0a = sel3(r[6], r[7], r[8], ca), D1a = sel3(r[9], r[10], r[11], ca);
-                    const float D0b = sel3(r[6], r[7], r[8], cb), D1b = sel3(r[9], r[10], r[11], cb);
+                    const float* rec = B.face_rec + (size_t)(sh.face_off + elem) * CS_FACE_REC + 27 * ca + 3 * cb;
 #pragma unroll
                     for (int kk = 0; kk < 3; kk++)
 #pragma unroll
-                        for (int hh = 0; hh < 3; hh++) {
-                            float h = stretch_h(r[kk], r[3 + kk], r[hh], r[3 + hh], D0a, D1a, D0b, D1b, r[12], r[13],
-                                                r[14], r[15], r[16], r[17], kk == hh);
-                            float J = -ar * h;
-                            a[3 * kk + hh] += s * J;
-                        }
+                        for (int hh = 0; hh < 3; hh++) a[3 * kk + hh] += rec[9 * kk + hh];
                 } else {
                     const float* rec = B.edge_rec + (size_t)(sh.edge_off + elem) * CS_EDGE_REC;
                     float coef = rec[12];
@@ -413,7 +402,7 @@ __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
                 if (code & CS_CODE_EDGE) continue;
                 int elem = (int)((code >> 4) & 0x7FFFFFFu);
                 const float* rec = B.face_rec + (size_t)(sh.face_off + elem) * CS_FACE_REC;
-                b0 += rec[29]; b1 += rec[30]; b2 += rec[31];
+                b0 += rec[90]; b1 += rec[91]; b2 += rec[92];
             }
             for (int c = c0; c < c1; c++) {
                 uint32_t code = B.tcontrib[c];
@@ -421,7 +410,7 @@ __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
                 int elem = (int)((code >> 4) & 0x7FFFFFFu);
                 int ca = (code >> 2) & 3;
                 const float* rec = B.face_rec + (size_t)(sh.face_off + elem) * CS_FACE_REC;
-                b0 += rec[20 + 3 * ca]; b1 += rec[21 + 3 * ca]; b2 += rec[22 + 3 * ca];
+                b0 += rec[81 + 3 * ca]; b1 += rec[82 + 3 * ca]; b2 += rec[83 + 3 * ca];
             }
             for (int c = c0; c < c1; c++) {
                 uint32_t code = B.tcontrib[c];
@@ -467,44 +456,14 @@ __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
     if (lane == 0) B.part[2 * slice] = bsq;
 }
 
-// Expands the element records of the last assembly into the reference's per-element
-// outputs (f, J) for inspection: faces as stretchingForce returns them
-// (PhysicsHelper.cu:288-290), interior edges as bendingForce does (PhysicsHelper.cu:351-352).
+// The reference's per-element outputs (f, J) for inspection: faces re-evaluated from the
+// current state as stretchingForce returns them (PhysicsHelper.cu:288-290), interior edges
+// expanded from the last assembly's records as bendingForce returns them
+// (PhysicsHelper.cu:351-352).
 __global__ void __launch_bounds__(128) cs_expand_kernel(Batch B, float* face_f, float* face_J, float* edge_f,
                                                         float* edge_J) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < B.F) {
-        const float* r = B.face_rec + (size_t)i * CS_FACE_REC;
-        const float area = r[18];
-        for (int p = 0; p < 9; p++) {
-            const int a = p / 3, kp = p % 3;
-            const float D0a = r[6 + a], D1a = r[9 + a];
-            const float fu_p = r[kp], fv_p = r[3 + kp];
-            // G is re-derived from the stored deformation gradient F (rec[0..5]) with the face
-            // kernel's arithmetic, so f is the value the face kernel used.
-            float F00 = r[0], F10 = r[1], F20 = r[2], F01 = r[3], F11 = r[4], F21 = r[5];
-            float FtF00 = F00 * F00, FtF01 = F00 * F01, FtF11 = F01 * F01;
-            FtF00 += F10 * F10;
-            FtF01 += F10 * F11;
-            FtF11 += F11 * F11;
-            FtF00 += F20 * F20;
-            FtF01 += F20 * F21;
-            FtF11 += F21 * F21;
-            float G00 = 0.5f * (FtF00 - 1.0f), G01 = 0.5f * (FtF01 - 0.0f), G11 = 0.5f * (FtF11 - 1.0f);
-            float fuu = D0a * fu_p, fvv = D1a * fv_p, fuv = 0.5f * (D0a * fv_p + D1a * fu_p);
-            float g = r[12] * G00 * fuu;
-            g += r[14] * G11 * fvv;
-            g += r[13] * (G00 * fvv + G11 * fuu);
-            g += 2.0f * r[15] * G01 * fuv;
-            face_f[9 * (size_t)i + p] = -area * g;
-            for (int q = 0; q < 9; q++) {
-                const int b = q / 3, kq = q % 3;
-                float h = stretch_h(fu_p, fv_p, r[kq], r[3 + kq], D0a, D1a, r[6 + b], r[9 + b], r[12], r[13], r[14],
-                                    r[15], r[16], r[17], kp == kq);
-                face_J[81 * (size_t)i + 9 * p + q] = -area * h;
-            }
-        }
-    }
+    if (i < B.F) face_eval(B, i, nullptr, face_f + 9 * (size_t)i, face_J + 81 * (size_t)i);
     if (i < B.E) {
         const float* r = B.edge_rec + (size_t)i * CS_EDGE_REC;
         const float coef = r[12], angle = r[13];

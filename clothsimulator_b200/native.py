@@ -34,8 +34,12 @@ EXPORTED = [
     "cs_set_state_device", "cs_get_state_device", "cs_step", "cs_sync", "cs_set_warm_start", "cs_get_dv",
     "cs_get_instance_stats", "cs_assemble", "cs_get_system", "cs_get_element_forces", "cs_spmv",
     "cs_device_pointers", "cs_profile_kernels", "cs_get_counters", "cs_get_stream",
-    "cs_solve_block_csr_noalloc",
+    "cs_solve_block_csr_noalloc", "cs_tc_gemm_check", "cs_mlp_init", "cs_mlp_record", "cs_mlp_fit_normalization",
+    "cs_mlp_train", "cs_mlp_gradient", "cs_mlp_predict", "cs_mlp_get_record", "cs_mlp_get_weights",
+    "cs_mlp_set_weights",
 ]
+MLP_PARAMS = 14761
+MLP_TRAINED = 14723
 
 
 class MaterialDesc(ctypes.Structure):
@@ -119,6 +123,16 @@ def load_library() -> ctypes.CDLL:
         "cs_get_stream": [vp, ctypes.POINTER(vp)],
         "cs_solve_block_csr_noalloc": [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int,
                                        vp, _ip, _dp],
+        "cs_tc_gemm_check": [vp, vp, _fp, ctypes.c_int, ctypes.c_int],
+        "cs_mlp_init": [vp, ctypes.c_int, ctypes.c_ulonglong],
+        "cs_mlp_record": [vp, ctypes.c_int, ctypes.c_int],
+        "cs_mlp_fit_normalization": [vp, ctypes.c_int],
+        "cs_mlp_train": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_ulonglong, _fp],
+        "cs_mlp_gradient": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _fp, _fp],
+        "cs_mlp_predict": [vp, _fp],
+        "cs_mlp_get_record": [vp, ctypes.c_int, _fp, _fp],
+        "cs_mlp_get_weights": [vp, _fp, ctypes.c_int],
+        "cs_mlp_set_weights": [vp, _fp, ctypes.c_int],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -341,3 +355,45 @@ class Context:
         s = ctypes.c_void_p()
         self.check(self.lib.cs_get_stream(self.h, ctypes.byref(s)))
         return s.value or 0
+
+    # --- learned warm start -------------------------------------------------------------
+    def mlp_init(self, slots: int, seed: int = 0):
+        self.check(self.lib.cs_mlp_init(self.h, slots, seed))
+
+    def mlp_record(self, slot: int, what: int):
+        self.check(self.lib.cs_mlp_record(self.h, slot, what))
+
+    def mlp_fit_normalization(self, n_slots: int):
+        self.check(self.lib.cs_mlp_fit_normalization(self.h, n_slots))
+
+    def mlp_train(self, n_slots: int, epochs: int, lr: float = 1e-3, sheets_per_batch: int = 64, seed: int = 0):
+        losses = np.zeros(epochs, np.float32)
+        self.check(self.lib.cs_mlp_train(self.h, n_slots, epochs, lr, sheets_per_batch, seed,
+                                         losses.ctypes.data_as(_fp)))
+        return losses
+
+    def mlp_gradient(self, slot: int, s0: int, s1: int):
+        g = np.zeros(MLP_TRAINED, np.float32)
+        loss = ctypes.c_float(0)
+        self.check(self.lib.cs_mlp_gradient(self.h, slot, s0, s1, g.ctypes.data_as(_fp), ctypes.byref(loss)))
+        return g, loss.value
+
+    def mlp_predict(self):
+        p = np.zeros((self.n, 3), np.float32)
+        self.check(self.lib.cs_mlp_predict(self.h, p.ctypes.data_as(_fp)))
+        return p
+
+    def mlp_get_record(self, slot: int):
+        f = np.zeros((self.n, 16), np.float32)
+        t = np.zeros((self.n, 3), np.float32)
+        self.check(self.lib.cs_mlp_get_record(self.h, slot, f.ctypes.data_as(_fp), t.ctypes.data_as(_fp)))
+        return f, t
+
+    def mlp_get_weights(self):
+        w = np.zeros(MLP_PARAMS, np.float32)
+        self.check(self.lib.cs_mlp_get_weights(self.h, w.ctypes.data_as(_fp), MLP_PARAMS))
+        return w
+
+    def mlp_set_weights(self, w):
+        a = _f32(w)
+        self.check(self.lib.cs_mlp_set_weights(self.h, a.ctypes.data_as(_fp), MLP_PARAMS))

@@ -255,3 +255,36 @@ def step_params(scene: Scene, sheet: dict) -> list:
     """Packed parameters [dt, g(3), wind density, drag, wind velocity(3), handle stiffness]."""
     w = sheet["wind"]
     return [scene.dt, *scene.gravity, w["density"], w["drag"], *w["velocity"], scene.handle_stiffness]
+
+
+def write_scene(scene: Scene, directory: str, frames: int = 2, solver: dict | None = None) -> str:
+    """Writes a scene in the reference's format: one OBJ per sheet, its material data file,
+    and a config JSON with the reference's keys (frame_time, frame_steps, end_frame, gravity,
+    wind, magic, cloths[mesh, materials], handles[cloth, nodes], disable) -- plus the
+    per-cloth "wind" and the "solver" object, extensions the reference ignores.  Returns the
+    config path."""
+    os.makedirs(directory, exist_ok=True)
+    cloths, handles = [], []
+    for i, s in enumerate(scene.sheets):
+        mesh = os.path.join(directory, f"sheet{i}.obj")
+        write_obj(s, mesh)
+        data = write_material_file(s["material"], directory, f"material{i}")
+        m = s["material"]
+        cloths.append({"mesh": mesh, "materials": {"data": data, "thicken": m.get("thicken", 1.0),
+                                                   "density_mult": m.get("density_mult", 1.0),
+                                                   "stretching_mult": m.get("stretching_mult", 1.0),
+                                                   "bending_mult": m.get("bending_mult", 1.0)},
+                       "wind": s["wind"]})
+        if len(s.get("handles", [])):
+            handles.append({"cloth": i, "nodes": [int(n) for n in s["handles"]]})
+    config = {
+        "frame_time": scene.dt * 4, "frame_steps": 4, "end_frame": frames,
+        "gravity": list(scene.gravity), "magic": {"handle_stiffness": scene.handle_stiffness},
+        "cloths": cloths, "handles": handles, "disable": ["remeshing"],
+    }
+    if solver:
+        config["solver"] = solver
+    path = os.path.join(directory, "config.json")
+    with open(path, "w") as fh:
+        fh.write("// generated scene\n" + json.dumps(config, indent=2))
+    return path

@@ -171,6 +171,37 @@ cs_status cs_profile_kernels(cs_ctx* ctx, const cs_step_params* params, int reps
 cs_status cs_get_counters(cs_ctx* ctx, long long* counters);
 /* The cudaStream_t the context launches on (for callers that record events on it). */
 cs_status cs_get_stream(cs_ctx* ctx, void** stream);
+/* Check of the tcgen05 tile GEMM the learned warm start is built on (no reference counterpart):
+ * D[128 x N] = A[128 x K] * B[N x K]^T with BF16 inputs (raw 16-bit patterns, row-major host
+ * arrays) and FP32 accumulation in tensor memory; K and N multiples of 16 in [16, 128]. */
+cs_status cs_tc_gemm_check(const uint16_t* A, const uint16_t* B, float* D, int K, int N);
+
+/* --- Learned warm start ---------------------------------------------------------------------
+ * No counterpart in the reference.  A one-ring message-passing MLP predicts each step's dv
+ * from per-node features of the assembled system (b, the diagonal block, v, the previous dv,
+ * the mass); the batched solver starts from the prediction (cs_step with CS_WARM_LEARNED) and
+ * discards it, per sheet, when its FP64 residual exceeds the zero guess's.  The layers run on
+ * tcgen05 tensor cores (BF16 operands, FP32 accumulation).  Training is on the device:
+ *   for each step of a trajectory: cs_assemble; cs_mlp_record(slot, 0); cs_step;
+ *   cs_mlp_record(slot, 1); then cs_mlp_fit_normalization and cs_mlp_train. */
+#define CS_MLP_PARAMS 14761  /* weights and biases (14723) + input/output normalisation (38) */
+cs_status cs_mlp_init(cs_ctx* ctx, int dataset_slots, unsigned long long seed);
+/* what = 0: features of the system assembled by the last cs_assemble (with the previous dv);
+ * what = 1: the target (the last cs_step's dv minus that previous dv). */
+cs_status cs_mlp_record(cs_ctx* ctx, int slot, int what);
+cs_status cs_mlp_fit_normalization(cs_ctx* ctx, int n_slots);
+/* Adam over minibatches of sheets_per_batch whole sheets of each recorded slot, shuffled per
+ * epoch; epoch_loss (optional, epochs floats) receives the mean minibatch loss. */
+cs_status cs_mlp_train(cs_ctx* ctx, int n_slots, int epochs, float lr, int sheets_per_batch,
+                       unsigned long long seed, float* epoch_loss);
+/* Gradient (CS_MLP_PARAMS - 38 floats) and loss of one minibatch, without updating. */
+cs_status cs_mlp_gradient(cs_ctx* ctx, int slot, int sheet_begin, int sheet_end, float* grad, float* loss);
+/* The prediction for the system assembled by the last cs_assemble (3 floats per node). */
+cs_status cs_mlp_predict(cs_ctx* ctx, float* pred);
+/* A recorded training pair: 16 raw features and 3 target values per node (host arrays). */
+cs_status cs_mlp_get_record(cs_ctx* ctx, int slot, float* feat, float* target);
+cs_status cs_mlp_get_weights(cs_ctx* ctx, float* out, int n);
+cs_status cs_mlp_set_weights(cs_ctx* ctx, const float* in, int n);
 
 /* --- Allocation-free solve ------------------------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device memory (a host
