@@ -8,8 +8,9 @@
 //   edges   : interior edges only (the reference skips boundary edges, Cloth.cu:142):
 //             int4 {n0, n1, opposite0, opposite1}, int meta (face-vertex rotations), sheet,
 //             float4 {area0 + area1, bias weight side 0, side 1, 0}; one 128-byte record.
-//   system  : SELL-32 block layout.  Rows (nodes) of a sheet are cut into slices of 32
-//             consecutive rows; slice s has `width` block slots per row (padded with zero
+//   system  : SELL-32 block layout.  A sheet's rows (nodes), sorted by block count within
+//             windows of sigma rows (sigma chosen per topology to minimise padding), are cut
+//             into slices of 32; slice s has `width` block slots per row (padded with zero
 //             blocks).  Slot (slice, k, lane) stores its 3x3 block in a "panel" of 32 lanes:
 //             entries 0-3 as float4[32], entries 4-7 as float4[32], entry 8 as float[32]
 //             (1152 bytes per panel, 128-bit coalesced loads).  Slot k = 0 is the diagonal.
@@ -45,12 +46,13 @@ struct SheetDesc {
     float bending[15];          // scaled bending samples, 3x5 (Material.cu:38-40)
     float wind_density, wind_drag, wind_v[3];
     int nbr_ptr_off, nbr_off;   // this sheet's topology in the one-ring neighbour arrays
+    int row2slot_off;           // this sheet's topology in the row -> slot map
 };
 
 struct SliceDesc {
     int sheet;
     int topo_slice;  // index into the per-topology slice arrays
-    int row0;        // first global row (node)
+    int row0;        // the sheet's first node; lane l holds row row0 + rowmap[topo_slice * 32 + l]
     int rows;        // rows in this slice (<= 32)
     int width;       // block slots per row
     int panel0;      // first global value panel
@@ -135,6 +137,8 @@ struct Batch {
     int* nbr_ptr = nullptr;      // per topology: one-ring neighbour CSR (sheet-local ids)
     int* nbr = nullptr;
     int* node_sheet = nullptr;   // sheet of every node
+    int* rowmap = nullptr;       // per topology slice lane: sheet-local row
+    int* row2slot = nullptr;     // per topology row: slice * 32 + lane
     // system
     float* A = nullptr;          // n_panels * 288
     float* b = nullptr;          // 3N

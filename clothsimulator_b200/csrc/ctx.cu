@@ -139,9 +139,11 @@ struct Topo {
     std::vector<int> ie_faces;  // 2 per
     std::vector<int> ie_meta;   // rotations of the adjacent faces' vertex order
     std::vector<int> ie_verts;  // 4 per: uv vertices [side][0..1]
-    // SELL-32 pattern
-    int n_slices = 0, n_tpanels = 0;
+    // SELL-32 pattern over rows sorted by length within windows of `sigma` rows
+    int n_slices = 0, n_tpanels = 0, sigma = 32;
     std::vector<int> slice_rows, slice_width, slice_tpanel0;
+    std::vector<int> rowmap;    // n_slices * 32: local row of (slice, lane)
+    std::vector<int> row2slot;  // n_nodes: slice * 32 + lane of each local row
     std::vector<int> tcol;                 // n_tpanels * 32 (local node ids)
     std::vector<int> tcptr;                // n_tpanels * 32 + 1
     std::vector<uint32_t> tcontrib;
@@ -305,13 +307,54 @@ std::shared_ptr<Topo> buildTopo(const cs_sheet_desc& s, std::string& err) {
         rowCols[i] = std::move(cols);
         rowRanges[i] = std::move(ranges);
     }
-    // SELL-32 slices
+    // SELL-32 slices.  Rows are sorted by block count (descending, stable) within windows of
+    // sigma rows; sigma is chosen from {32, 64, 128, 256} to minimise the padded slots (the
+    // SpMV reads every slot of a slice's width), the smaller window on ties to keep locality.
+    std::vector<int> len(nn);
+    for (int i = 0; i < nn; i++) len[i] = (int)rowCols[i].size();
+    auto orderFor = [&](int sigma) {
+        std::vector<int> order(nn);
+        for (int i = 0; i < nn; i++) order[i] = i;
+        if (sigma > CS_SLICE)
+            for (int w0 = 0; w0 < nn; w0 += sigma) {
+                int w1 = std::min(nn, w0 + sigma);
+                std::stable_sort(order.begin() + w0, order.begin() + w1, [&](int a, int b) { return len[a] > len[b]; });
+            }
+        return order;
+    };
+    auto padded = [&](const std::vector<int>& order) {
+        long long tot = 0;
+        for (int r0 = 0; r0 < nn; r0 += CS_SLICE) {
+            int r1 = std::min(nn, r0 + CS_SLICE), w = 1;
+            for (int r = r0; r < r1; r++) w = std::max(w, len[order[r]]);
+            tot += (long long)w * (r1 - r0);
+        }
+        return tot;
+    };
+    std::vector<int> order = orderFor(CS_SLICE);
+    long long best = padded(order);
+    t->sigma = CS_SLICE;
+    for (int sigma : {64, 128, 256}) {
+        std::vector<int> o = orderFor(sigma);
+        long long p = padded(o);
+        if (p < best) {
+            best = p;
+            order = o;
+            t->sigma = sigma;
+        }
+    }
     t->n_slices = (nn + CS_SLICE - 1) / CS_SLICE;
+    t->rowmap.assign((size_t)t->n_slices * CS_SLICE, 0);
+    t->row2slot.assign(nn, 0);
+    for (int r = 0; r < nn; r++) {
+        t->rowmap[r] = order[r];
+        t->row2slot[order[r]] = r;
+    }
     int tp = 0;
     for (int s = 0; s < t->n_slices; s++) {
         int r0 = s * CS_SLICE, rows = std::min(CS_SLICE, nn - r0);
         int w = 1;
-        for (int l = 0; l < rows; l++) w = std::max(w, (int)rowCols[r0 + l].size());
+        for (int l = 0; l < rows; l++) w = std::max(w, (int)rowCols[order[r0 + l]].size());
         t->slice_rows.push_back(rows);
         t->slice_width.push_back(w);
         t->slice_tpanel0.push_back(tp);
@@ -333,7 +376,7 @@ std::shared_ptr<Topo> buildTopo(const cs_sheet_desc& s, std::string& err) {
                 size_t slot = (size_t)(t->slice_tpanel0[s] + k) * CS_SLICE + l;
                 t->tcptr[slot] = (int)t->tcontrib.size();
                 if (l < t->slice_rows[s]) {
-                    int i = r0 + l;
+                    int i = order[r0 + l];
                     if (k < (int)rowCols[i].size()) {
                         t->tcol[slot] = rowCols[i][k];
                         auto rg = rowRanges[i][k];
@@ -402,6 +445,7 @@ struct cs_ctx {
     DevParams hostParams{};
     bool lastStepValid = false;
     long long steps = 0, hostLaunches = 0, graphSteps = 0, graphLaunchesFixed = 0;
+    int gatherGrid = 1;  // persistent assembly gather: a few warps per SM walk the slices
     // learned warm start
     MlpDev mlp;
     bool mlpInit = false;
@@ -476,7 +520,7 @@ int launchAssembly(cs_ctx* c) {
     int n = 1;
     if (B.F) cs_face_kernel<<<nblk(B.F, 64), 64, 0, c->stream>>>(B), n++;
     if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B), n++;
-    cs_gather_kernel<<<nblk((long long)B.n_slices * 32, 128), 128, 0, c->stream>>>(B);
+    cs_gather_kernel<<<c->gatherGrid, 128, 0, c->stream>>>(B);
     return n;
 }
 
@@ -689,7 +733,8 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     // per-topology arrays, concatenated
     std::vector<int> htcol, htcptr;
     std::vector<uint32_t> htcontrib;
-    std::vector<int> hnbr_ptr, hnbr, hnode_sheet;
+    std::vector<int> hnbr_ptr, hnbr, hnode_sheet, hrowmap, hrow2slot;
+    std::vector<int> topoRow2Slot0(topos.size());
     std::vector<int> topoNbrPtr0(topos.size()), topoNbr0(topos.size());
     std::vector<int> topoPanel0(topos.size()), topoSlice0(topos.size());
     {
@@ -702,6 +747,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             htcol.insert(htcol.end(), T.tcol.begin(), T.tcol.end());
             for (size_t i = 0; i + 1 < T.tcptr.size(); i++) htcptr.push_back(T.tcptr[i] + cbase);
             htcontrib.insert(htcontrib.end(), T.tcontrib.begin(), T.tcontrib.end());
+            hrowmap.insert(hrowmap.end(), T.rowmap.begin(), T.rowmap.end());
+            topoRow2Slot0[t] = (int)hrow2slot.size();
+            hrow2slot.insert(hrow2slot.end(), T.row2slot.begin(), T.row2slot.end());
             topoNbrPtr0[t] = (int)hnbr_ptr.size();
             topoNbr0[t] = (int)hnbr.size();
             hnbr_ptr.insert(hnbr_ptr.end(), T.nbr_ptr.begin(), T.nbr_ptr.end());
@@ -729,6 +777,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         sd.topo = sheetTopoId[s];
         sd.table = sheetTable[s];
         sd.nbr_ptr_off = topoNbrPtr0[sheetTopoId[s]];
+        sd.row2slot_off = topoRow2Slot0[sheetTopoId[s]];
         sd.nbr_off = topoNbr0[sheetTopoId[s]];
         hnode_sheet.insert(hnode_sheet.end(), d.n_nodes, s);
         float bmult = m.bending_mult * m.thicken;
@@ -794,7 +843,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             SliceDesc sl{};
             sl.sheet = s;
             sl.topo_slice = topoSlice0[sheetTopoId[s]] + t;
-            sl.row0 = node_off + t * CS_SLICE;
+            sl.row0 = node_off;  // rows: row0 + rowmap[topo_slice * 32 + lane]
             sl.rows = T.slice_rows[t];
             sl.width = T.slice_width[t];
             sl.panel0 = panel_off + T.slice_tpanel0[t];
@@ -843,6 +892,8 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     UP(nbr_ptr, hnbr_ptr);
     UP(nbr, hnbr);
     UP(node_sheet, hnode_sheet);
+    UP(rowmap, hrowmap);
+    UP(row2slot, hrow2slot);
 #undef UP
 #define AL(field, n) \
     if ((st = dalloc(c, &B.field, (size_t)(n))) != CS_OK) return st;
@@ -871,6 +922,11 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     CS_CUDA(cudaMemset(B.inst, 0, B.S * sizeof(InstState)));
     CS_CUDA(cudaMemset(B.loop, 0, 8 * sizeof(int)));
     CS_CUDA(cudaDeviceSynchronize());
+    {
+        cudaDeviceProp prop;
+        CS_CUDA(cudaGetDeviceProperties(&prop, c->device));
+        c->gatherGrid = std::max(1, std::min(nblk((long long)B.n_slices * 32, 128), 2 * prop.multiProcessorCount));
+    }
     c->loaded = true;
     return CS_OK;
 }
@@ -1162,7 +1218,7 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
             switch (which) {
                 case 0: if (B.F) cs_face_kernel<<<nblk(B.F, 64), 64, 0, c->stream>>>(B); break;
                 case 1: if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B); break;
-                case 2: cs_gather_kernel<<<g, 128, 0, c->stream>>>(B); break;
+                case 2: cs_gather_kernel<<<c->gatherGrid, 128, 0, c->stream>>>(B); break;
                 case 3: cs_spmv_kernel<<<g, 128, 0, c->stream>>>(B); break;
                 case 4: cs_vector_kernel<<<g, 128, 0, c->stream>>>(B); break;
                 case 5: cs_reduce1_kernel<<<B.S, 128, 0, c->stream>>>(B); break;

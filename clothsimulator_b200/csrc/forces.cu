@@ -134,7 +134,7 @@ __device__ __forceinline__ float stretch_h(float fu_p, float fv_p, float fu_q, f
 }  // namespace
 
 // Face record (CS_FACE_REC = 96 floats): [0..80] the face's 9x9 contribution to A,
-// -dt*dt*J (row-major, block (a, b) at rows 3a..3a+2, columns 3b..3b+2), [81..89]
+// -dt*dt*J, as nine contiguous row-major 3x3 blocks (block (a, b) at 9 (3a + b)), [81..89]
 // dt*(f + dt*J*v) of the stretching term, [90..92] dt * wind force added to each node.
 //
 // face_eval evaluates one face exactly as Face::update (normal), the wind loop of
@@ -213,7 +213,7 @@ __device__ __forceinline__ void face_eval(const Batch& B, int f, float* __restri
                                       gu, gv, kp == kq);
             const float J = -area * h;
             jv += (dt * J) * vel[q];
-            if (rec) rec[9 * p + q] = s * J;
+            if (rec) rec[9 * (3 * a + b) + 3 * kp + kq] = s * J;  // block (a, b) contiguous
             if (Jo) Jo[9 * p + q] = J;
         }
         if (rec) rec[81 + p] = dt * (fp + jv);
@@ -329,131 +329,155 @@ __global__ void __launch_bounds__(128) cs_edge_kernel(Batch B) {
     out[6] = make_float4(bb[8], bb[9], bb[10], bb[11]);
 }
 
-// One warp per slice; lane = row.  Writes A's panels, and for the diagonal slot b, the
-// block-Jacobi inverse and the slice's ||b||^2 (part[2*slice]).
+// Assembly gather.  Warps walk the slices grid-stride (a persistent launch of a few warps per
+// SM), so the slices in flight at any moment cover a few sheets and their element records
+// stay in L2.  Lane = row.  For every block slot the contributors are summed in the
+// reference's order; their codes and record values are fetched four at a time so several
+// loads are in flight before the ordered additions.  Writes A's panels, and for the
+// diagonal slot b, the block-Jacobi inverse and the slice's ||b||^2 (part[2*slice]).
 __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
-    int slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    if (slice >= B.n_slices) return;
-    const SliceDesc sd = B.slices[slice];
-    const SheetDesc& sh = B.sheets[sd.sheet];
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
     const DevParams& P = *B.params;
     const float dt = P.dt;
     const float s = -dt * dt;
-    const bool live = lane < sd.rows;
-    const int row = sd.row0 + lane;
-    double bsq = 0.0;
-    for (int k = 0; k < sd.width; k++) {
-        const int tslot = (sd.tpanel0 + k) * CS_SLICE + lane;
-        float a[9];
+    for (int slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; slice < B.n_slices; slice += warps) {
+        const SliceDesc sd = B.slices[slice];
+        const SheetDesc& sh = B.sheets[sd.sheet];
+        const bool live = lane < sd.rows;
+        const int row = sd.row0 + (live ? B.rowmap[sd.topo_slice * CS_SLICE + lane] : 0);
+        const float* __restrict__ frec = B.face_rec + (size_t)sh.face_off * CS_FACE_REC;
+        const float* __restrict__ erec = B.edge_rec + (size_t)sh.edge_off * CS_EDGE_REC;
+        double bsq = 0.0;
+        for (int k = 0; k < sd.width; k++) {
+            const int tslot = (sd.tpanel0 + k) * CS_SLICE + lane;
+            float a[9];
 #pragma unroll
-        for (int t = 0; t < 9; t++) a[t] = 0.0f;
-        if (live) {
-            if (k == 0) {
-                float m = B.mass[row];
-                a[0] = m; a[4] = m; a[8] = m;
-            }
-            int c0 = B.tcptr[tslot], c1 = B.tcptr[tslot + 1];
-            for (int c = c0; c < c1; c++) {
-                uint32_t code = B.tcontrib[c];
-                int elem = (int)((code >> 4) & 0x7FFFFFFu);
-                int ca = (code >> 2) & 3, cb = code & 3;
-                if (!(code & CS_CODE_EDGE)) {
-                    const float* rec = B.face_rec + (size_t)(sh.face_off + elem) * CS_FACE_REC + 27 * ca + 3 * cb;
+            for (int t = 0; t < 9; t++) a[t] = 0.0f;
+            int c0 = 0, c1 = 0;
+            if (live) {
+                if (k == 0) {
+                    const float m = B.mass[row];
+                    a[0] = m; a[4] = m; a[8] = m;
+                }
+                c0 = __ldg(&B.tcptr[tslot]);
+                c1 = __ldg(&B.tcptr[tslot + 1]);
+                for (int c = c0; c < c1; c += 4) {
+                    uint32_t code[4];
+                    float v[4][9];
 #pragma unroll
-                    for (int kk = 0; kk < 3; kk++)
+                    for (int j = 0; j < 4; j++) code[j] = (c + j < c1) ? __ldg(&B.tcontrib[c + j]) : 0u;
 #pragma unroll
-                        for (int hh = 0; hh < 3; hh++) a[3 * kk + hh] += rec[9 * kk + hh];
-                } else {
-                    const float* rec = B.edge_rec + (size_t)(sh.edge_off + elem) * CS_EDGE_REC;
-                    float coef = rec[12];
+                    for (int j = 0; j < 4; j++) {
+                        if (c + j >= c1) continue;
+                        const int elem = (int)((code[j] >> 4) & 0x7FFFFFFu);
+                        const int ca = (code[j] >> 2) & 3, cb = code[j] & 3;
+                        if (!(code[j] & CS_CODE_EDGE)) {
+                            const float* r = frec + (size_t)elem * CS_FACE_REC + 9 * (3 * ca + cb);
 #pragma unroll
-                    for (int kk = 0; kk < 3; kk++)
+                            for (int e = 0; e < 9; e++) v[j][e] = __ldg(r + e);
+                        } else {
+                            const float* r = erec + (size_t)elem * CS_EDGE_REC;
+                            const float coef = __ldg(r + 12);
+                            const float d0 = __ldg(r + 3 * ca), d1 = __ldg(r + 3 * ca + 1), d2 = __ldg(r + 3 * ca + 2);
+                            const float e0 = __ldg(r + 3 * cb), e1 = __ldg(r + 3 * cb + 1), e2 = __ldg(r + 3 * cb + 2);
+                            const float da[3] = {d0, d1, d2}, db[3] = {e0, e1, e2};
 #pragma unroll
-                        for (int hh = 0; hh < 3; hh++) {
-                            float J = coef * (rec[3 * ca + kk] * rec[3 * cb + hh]);
-                            a[3 * kk + hh] += s * J;
+                            for (int kk = 0; kk < 3; kk++)
+#pragma unroll
+                                for (int hh = 0; hh < 3; hh++) v[j][3 * kk + hh] = s * (coef * (da[kk] * db[hh]));
                         }
-                }
-            }
-            if (k == 0) {
-                float4 hd = B.handle[row];
-                int hc = (int)hd.w;
-                for (int t = 0; t < hc; t++) {
-                    float add_ = dt * dt * P.handle_stiffness;
-                    a[0] += add_; a[4] += add_; a[8] += add_;
-                }
-            }
-        }
-        float* panel = B.A + (size_t)(sd.panel0 + k) * CS_PANEL_FLOATS;
-        reinterpret_cast<float4*>(panel)[lane] = make_float4(a[0], a[1], a[2], a[3]);
-        reinterpret_cast<float4*>(panel + 128)[lane] = make_float4(a[4], a[5], a[6], a[7]);
-        panel[256 + lane] = a[8];
-
-        if (k == 0 && live) {
-            // Right-hand side in the reference's order: gravity, wind (faces), stretching
-            // (faces), bending (edges), handles (Cloth.cu:94-169).
-            float m = B.mass[row];
-            float g0 = (dt * m) * P.gravity[0], g1 = (dt * m) * P.gravity[1], g2 = (dt * m) * P.gravity[2];
-            float b0 = 0.0f + g0, b1 = 0.0f + g1, b2 = 0.0f + g2;
-            int c0 = B.tcptr[tslot], c1 = B.tcptr[tslot + 1];
-            for (int c = c0; c < c1; c++) {
-                uint32_t code = B.tcontrib[c];
-                if (code & CS_CODE_EDGE) continue;
-                int elem = (int)((code >> 4) & 0x7FFFFFFu);
-                const float* rec = B.face_rec + (size_t)(sh.face_off + elem) * CS_FACE_REC;
-                b0 += rec[90]; b1 += rec[91]; b2 += rec[92];
-            }
-            for (int c = c0; c < c1; c++) {
-                uint32_t code = B.tcontrib[c];
-                if (code & CS_CODE_EDGE) continue;
-                int elem = (int)((code >> 4) & 0x7FFFFFFu);
-                int ca = (code >> 2) & 3;
-                const float* rec = B.face_rec + (size_t)(sh.face_off + elem) * CS_FACE_REC;
-                b0 += rec[81 + 3 * ca]; b1 += rec[82 + 3 * ca]; b2 += rec[83 + 3 * ca];
-            }
-            for (int c = c0; c < c1; c++) {
-                uint32_t code = B.tcontrib[c];
-                if (!(code & CS_CODE_EDGE)) continue;
-                int elem = (int)((code >> 4) & 0x7FFFFFFu);
-                int ca = (code >> 2) & 3;
-                const float* rec = B.edge_rec + (size_t)(sh.edge_off + elem) * CS_EDGE_REC;
-                b0 += rec[16 + 3 * ca]; b1 += rec[17 + 3 * ca]; b2 += rec[18 + 3 * ca];
-            }
-            float4 hd = B.handle[row];
-            int hc = (int)hd.w;
-            if (hc > 0) {
-                f3 xr = ld3(B.x, row), vr = ld3(B.v, row);
-                f3 fh = mulv(scl(dt, sub(sub(mk(hd.x, hd.y, hd.z), xr), scl(dt, vr))), P.handle_stiffness);
-                for (int t = 0; t < hc; t++) {
-                    b0 += fh.x; b1 += fh.y; b2 += fh.z;
-                }
-            }
-            B.b[3 * row] = b0;
-            B.b[3 * row + 1] = b1;
-            B.b[3 * row + 2] = b2;
-            bsq = (double)b0 * b0 + (double)b1 * b1 + (double)b2 * b2;
-            // 3x3 block-Jacobi inverse in double, stored in float.
-            double m00 = a[0], m01 = a[1], m02 = a[2], m10 = a[3], m11 = a[4], m12 = a[5], m20 = a[6], m21 = a[7],
-                   m22 = a[8];
-            double c00 = m11 * m22 - m12 * m21, c01 = m12 * m20 - m10 * m22, c02 = m10 * m21 - m11 * m20;
-            double det = m00 * c00 + m01 * c01 + m02 * c02;
-            double id = det != 0.0 ? 1.0 / det : 0.0;
-            float* Pi = B.Pinv + 9 * (size_t)row;
-            Pi[0] = (float)(c00 * id);
-            Pi[1] = (float)((m02 * m21 - m01 * m22) * id);
-            Pi[2] = (float)((m01 * m12 - m02 * m11) * id);
-            Pi[3] = (float)(c01 * id);
-            Pi[4] = (float)((m00 * m22 - m02 * m20) * id);
-            Pi[5] = (float)((m02 * m10 - m00 * m12) * id);
-            Pi[6] = (float)(c02 * id);
-            Pi[7] = (float)((m01 * m20 - m00 * m21) * id);
-            Pi[8] = (float)((m00 * m11 - m01 * m10) * id);
-        }
-    }
+                    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) bsq += __shfl_xor_sync(0xffffffffu, bsq, o);
-    if (lane == 0) B.part[2 * slice] = bsq;
+                    for (int j = 0; j < 4; j++)
+                        if (c + j < c1)
+#pragma unroll
+                            for (int e = 0; e < 9; e++) a[e] += v[j][e];
+                }
+                if (k == 0) {
+                    const int hc = (int)B.handle[row].w;
+                    for (int t = 0; t < hc; t++) {
+                        const float add_ = dt * dt * P.handle_stiffness;
+                        a[0] += add_; a[4] += add_; a[8] += add_;
+                    }
+                }
+            }
+            float* panel = B.A + (size_t)(sd.panel0 + k) * CS_PANEL_FLOATS;
+            reinterpret_cast<float4*>(panel)[lane] = make_float4(a[0], a[1], a[2], a[3]);
+            reinterpret_cast<float4*>(panel + 128)[lane] = make_float4(a[4], a[5], a[6], a[7]);
+            panel[256 + lane] = a[8];
+
+            if (k == 0 && live) {
+                // Right-hand side in the reference's order: gravity, wind (faces), stretching
+                // (faces), bending (edges), handles (Cloth.cu:94-169).
+                const float m = B.mass[row];
+                const float g0 = (dt * m) * P.gravity[0], g1 = (dt * m) * P.gravity[1], g2 = (dt * m) * P.gravity[2];
+                float b0 = 0.0f + g0, b1 = 0.0f + g1, b2 = 0.0f + g2;
+                for (int pass = 0; pass < 3; pass++) {
+                    for (int c = c0; c < c1; c += 4) {
+                        float w[4][3];
+                        bool use[4];
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            use[j] = false;
+                            if (c + j >= c1) continue;
+                            const uint32_t code = __ldg(&B.tcontrib[c + j]);
+                            const bool edge = (code & CS_CODE_EDGE) != 0;
+                            if (edge != (pass == 2)) continue;
+                            const int elem = (int)((code >> 4) & 0x7FFFFFFu);
+                            const int ca = (code >> 2) & 3;
+                            const float* r = pass == 0 ? frec + (size_t)elem * CS_FACE_REC + 90
+                                           : pass == 1 ? frec + (size_t)elem * CS_FACE_REC + 81 + 3 * ca
+                                                       : erec + (size_t)elem * CS_EDGE_REC + 16 + 3 * ca;
+                            w[j][0] = __ldg(r);
+                            w[j][1] = __ldg(r + 1);
+                            w[j][2] = __ldg(r + 2);
+                            use[j] = true;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            if (use[j]) {
+                                b0 += w[j][0];
+                                b1 += w[j][1];
+                                b2 += w[j][2];
+                            }
+                    }
+                }
+                const float4 hd = B.handle[row];
+                const int hc = (int)hd.w;
+                if (hc > 0) {
+                    const f3 xr = ld3(B.x, row), vr = ld3(B.v, row);
+                    const f3 fh = mulv(scl(dt, sub(sub(mk(hd.x, hd.y, hd.z), xr), scl(dt, vr))), P.handle_stiffness);
+                    for (int t = 0; t < hc; t++) {
+                        b0 += fh.x; b1 += fh.y; b2 += fh.z;
+                    }
+                }
+                B.b[3 * row] = b0;
+                B.b[3 * row + 1] = b1;
+                B.b[3 * row + 2] = b2;
+                bsq = (double)b0 * b0 + (double)b1 * b1 + (double)b2 * b2;
+                // 3x3 block-Jacobi inverse in double, stored in float.
+                const double m00 = a[0], m01 = a[1], m02 = a[2], m10 = a[3], m11 = a[4], m12 = a[5], m20 = a[6],
+                             m21 = a[7], m22 = a[8];
+                const double c00 = m11 * m22 - m12 * m21, c01 = m12 * m20 - m10 * m22, c02 = m10 * m21 - m11 * m20;
+                const double det = m00 * c00 + m01 * c01 + m02 * c02;
+                const double id = det != 0.0 ? 1.0 / det : 0.0;
+                float* Pi = B.Pinv + 9 * (size_t)row;
+                Pi[0] = (float)(c00 * id);
+                Pi[1] = (float)((m02 * m21 - m01 * m22) * id);
+                Pi[2] = (float)((m01 * m12 - m02 * m11) * id);
+                Pi[3] = (float)(c01 * id);
+                Pi[4] = (float)((m00 * m22 - m02 * m20) * id);
+                Pi[5] = (float)((m02 * m10 - m00 * m12) * id);
+                Pi[6] = (float)(c02 * id);
+                Pi[7] = (float)((m01 * m20 - m00 * m21) * id);
+                Pi[8] = (float)((m00 * m11 - m01 * m10) * id);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) bsq += __shfl_xor_sync(0xffffffffu, bsq, o);
+        if (lane == 0) B.part[2 * slice] = bsq;
+    }
 }
 
 // The reference's per-element outputs (f, J) for inspection: faces re-evaluated from the

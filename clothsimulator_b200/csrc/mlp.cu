@@ -144,8 +144,9 @@ __global__ void cs_mlp_features_kernel(Batch B, MlpDev M, float* __restrict__ ou
     if (i >= B.N) return;
     const SheetDesc& sh = B.sheets[B.node_sheet[i]];
     const int local = i - sh.node_off;
-    const SliceDesc& sd = B.slices[sh.slice_off + local / CS_SLICE];
-    const int lane = local % CS_SLICE;
+    const int ts = B.row2slot[sh.row2slot_off + local];
+    const SliceDesc& sd = B.slices[sh.slice_off + ts / CS_SLICE];
+    const int lane = ts % CS_SLICE;
     const float* panel = B.A + (size_t)sd.panel0 * CS_PANEL_FLOATS;
     const float4 a0 = reinterpret_cast<const float4*>(panel)[lane];
     const float4 a1 = reinterpret_cast<const float4*>(panel + 128)[lane];

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(128) cs_spmv_kernel(Batch B) {
     const bool mixed = B.params->mixed != 0;
     const int node_off = B.sheets[sd.sheet].node_off;
     const bool live = lane < sd.rows;
-    const int row = sd.row0 + lane;
+    const int row = sd.row0 + (live ? B.rowmap[sd.topo_slice * CS_SLICE + lane] : 0);
     if (ph == PH_CG) {
         const float beta = I.beta;
         const int par = B.loop[0] & 1;
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(128) cs_vector_kernel(Batch B) {
     if (ph != PH_CG && ph != PH_INIT && ph != PH_FINISH) return;
     const bool mixed = B.params->mixed != 0;
     const bool live = lane < sd.rows;
-    const int row = sd.row0 + lane;
+    const int row = sd.row0 + (live ? B.rowmap[sd.topo_slice * CS_SLICE + lane] : 0);
     double rz = 0.0, rr = 0.0;
     float rzf = 0.f, rrf = 0.f;
     if (live) {
@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(128) cs_spmv_plain_kernel(Batch B, const float
     const SliceDesc sd = B.slices[slice];
     if (lane >= sd.rows) return;
     const int node_off = B.sheets[sd.sheet].node_off;
-    const int row = sd.row0 + lane;
+    const int row = sd.row0 + B.rowmap[sd.topo_slice * CS_SLICE + lane];
     float y0 = 0.f, y1 = 0.f, y2 = 0.f;
     for (int k = 0; k < sd.width; k++) {
         const int col = B.tcol[(sd.tpanel0 + k) * CS_SLICE + lane] + node_off;
