@@ -47,6 +47,7 @@ struct SheetDesc {
     float wind_density, wind_drag, wind_v[3];
     int nbr_ptr_off, nbr_off;   // this sheet's topology in the one-ring neighbour arrays
     int row2slot_off;           // this sheet's topology in the row -> slot map
+    int resident;               // 1: solved by the cluster-resident kernel (resident.cu)
 };
 
 struct SliceDesc {
@@ -67,7 +68,14 @@ enum InstPhase : int {
     PH_INIT = 2,      // start a CG sweep: dv64 += e, e = 0, z = P r, p = z
     PH_FINISH = 3,    // dv64 += e, then done
     PH_DONE = 4,
+    PH_RESIDENT = 5,  // owned by the cluster-resident kernel this step (skipped by the loop)
 };
+
+// Cluster-resident solver limits: CTAs per cluster, warps (slices) per CTA.
+#define CS_RES_MAX_CL 16
+#define CS_RES_MAX_WARPS 24
+#define CS_SOLVER_AUTO_DEV 0
+#define CS_SOLVER_BATCHED_DEV 1
 
 // Instance flags
 #define CS_IF_CONVERGED 1
@@ -106,6 +114,7 @@ struct DevParams {
     int warm;              // 0 zero guess, 1 warm start from dv64 as preloaded
     int loop_cap;          // hard bound on loop trips per step
     int advance;           // 1: v += dv, x += dt v at the end of the step
+    int solver;            // CS_SOLVER_AUTO_DEV: resident sheets on the cluster kernel; BATCHED: loop only
 };
 
 struct Batch {
@@ -148,7 +157,13 @@ struct Batch {
     double* part = nullptr;      // 2 per slice
     InstState* inst = nullptr;
     DevParams* params = nullptr;
-    int* loop = nullptr;         // [0] loop trip counter, [1] instances not done
+    int* loop = nullptr;         // [0] loop trip counter, [1] instances not done, [5] resident work counter
+    // cluster-resident solver (resident.cu)
+    int n_resident = 0;          // sheets listed in rlist
+    int res_cap = 0;             // panels per CTA held in shared memory
+    int* rlist = nullptr;        // resident sheets, largest first
+    int* rsplit = nullptr;       // per topology: CS_RES_MAX_CL + 1 sheet-relative slice bounds per CTA rank
+    int* rcode = nullptr;        // per topology panel slot: (owner rank << 16) | owner-local row slot
 };
 
 #endif

@@ -43,6 +43,7 @@ __global__ void cs_solve_setup_kernel(Batch B);
 __global__ void cs_advance_kernel(Batch B);
 __global__ void cs_spmv_plain_kernel(Batch B, const float* x, float* y);
 __global__ void cs_profile_setup_kernel(Batch B, int phase);
+__global__ void cs_resident_pcg_kernel(Batch B);
 
 namespace {
 
@@ -422,6 +423,36 @@ std::shared_ptr<Topo> buildTopo(const cs_sheet_desc& s, std::string& err) {
     return t;
 }
 
+// Cluster-resident solve plan for one topology: contiguous slice ranges per CTA rank with
+// balanced panel counts.  Returns the largest number of slices a rank gets.
+int residentSplit(const Topo& T, int ncta, std::vector<int>& split) {
+    split.assign(CS_RES_MAX_CL + 1, T.n_slices);
+    std::vector<long long> pre(T.n_slices + 1, 0);
+    for (int i = 0; i < T.n_slices; i++) pre[i + 1] = pre[i] + T.slice_width[i];
+    split[0] = 0;
+    for (int c = 1; c < ncta; c++) {
+        const double target = (double)pre[T.n_slices] * c / ncta;
+        int sl = (int)(std::lower_bound(pre.begin(), pre.end(), (long long)std::ceil(target)) - pre.begin());
+        if (sl > 0 && target - pre[sl - 1] < pre[sl] - target) sl--;
+        split[c] = std::max(split[c - 1], std::min(sl, T.n_slices));
+    }
+    int w = 0;
+    for (int c = 0; c < ncta; c++) w = std::max(w, split[c + 1] - split[c]);
+    return w;
+}
+
+// Owner-rank code of every panel slot of a topology: (rank << 16) | rank-local row slot.
+std::vector<int> residentCodes(const Topo& T, const std::vector<int>& split, int ncta) {
+    std::vector<int> nodeCode(T.n_nodes, 0);
+    for (int c = 0; c < ncta; c++)
+        for (int sl = split[c]; sl < split[c + 1]; sl++)
+            for (int l = 0; l < T.slice_rows[sl]; l++)
+                nodeCode[T.rowmap[sl * CS_SLICE + l]] = (c << 16) | ((sl - split[c]) * CS_SLICE + l);
+    std::vector<int> code(T.tcol.size(), 0);
+    for (size_t i = 0; i < T.tcol.size(); i++) code[i] = nodeCode[T.tcol[i]];
+    return code;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------------------
@@ -454,6 +485,10 @@ struct cs_ctx {
     float* mlpScratch = nullptr;  // per-epoch loss accumulators, gradient output
     cudaGraphExec_t graphExecLearned = nullptr;
     cudaGraph_t graphLearned = nullptr;
+    // cluster-resident solver launch (resident.cu): CTAs per cluster, threads per CTA,
+    // clusters in the persistent grid, dynamic shared memory per CTA
+    int resCL = 0, resThreads = 0, resClusters = 0;
+    size_t resSmem = 0;
 };
 
 namespace {
@@ -530,6 +565,24 @@ void launchSolvePrologue(cs_ctx* c) {
     cs_solve_prologue_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B);
 }
 
+// Sheets that fit a cluster's shared memory: one persistent cluster per sheet at a time.
+void launchResident(cs_ctx* c) {
+    if (c->resClusters <= 0) return;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = c->resCL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(c->resClusters * c->resCL);
+    cfg.blockDim = dim3(c->resThreads);
+    cfg.dynamicSmemBytes = c->resSmem;
+    cfg.stream = c->stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, cs_resident_pcg_kernel, c->B);
+}
+
 // Learned warm start: features of the assembled system, layer 1, layers 2-3 + output; the
 // prediction replaces the previous dv in B.warm (the solve then starts from it).
 int launchMlpInference(cs_ctx* c, float* pred) {
@@ -561,6 +614,7 @@ cs_status buildGraph(cs_ctx* c, bool learned) {
     launchAssembly(c);
     if (learned) launchMlpInference(c, c->B.warm);
     launchSolvePrologue(c);
+    launchResident(c);
     cudaStreamCaptureStatus cst;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
@@ -602,6 +656,7 @@ DevParams toDev(const cs_step_params* p) {
     d.warm = p->warm_start != CS_WARM_ZERO;
     d.loop_cap = 2 * d.max_iters + 256;
     d.advance = p->advance;
+    d.solver = p->solver == CS_SOLVER_BATCHED ? CS_SOLVER_BATCHED_DEV : CS_SOLVER_AUTO_DEV;
     return d;
 }
 
@@ -737,6 +792,71 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     std::vector<int> topoRow2Slot0(topos.size());
     std::vector<int> topoNbrPtr0(topos.size()), topoNbr0(topos.size());
     std::vector<int> topoPanel0(topos.size()), topoSlice0(topos.size());
+    // Cluster-resident solve plan (resident.cu).  CS_RESIDENT_CL sets the CTAs per cluster
+    // (2, 4, 8 or 16; 0 solves every sheet in the batched loop); default 8, the portable size.
+    int resCL = 8;
+    if (const char* ev = std::getenv("CS_RESIDENT_CL")) resCL = std::atoi(ev);
+    if (resCL != 0 && resCL != 2 && resCL != 4 && resCL != 8 && resCL != 16)
+        return fail(c, CS_ERR_INVALID_ARG, "CS_RESIDENT_CL must be 0, 2, 4, 8 or 16");
+    std::vector<int> hrsplit(topos.size() * (CS_RES_MAX_CL + 1), 0), hrcode;
+    std::vector<char> topoResident(topos.size(), 0);
+    int resW = 0, resPanels = 0;
+    for (size_t t = 0; t < topos.size() && resCL > 0; t++) {
+        const Topo& T = *topos[t];
+        std::vector<int> split;
+        const int w = residentSplit(T, resCL, split);
+        if (w > CS_RES_MAX_WARPS) continue;
+        topoResident[t] = 1;
+        resW = std::max(resW, w);
+        for (int k = 0; k < resCL; k++) {
+            int np = 0;
+            for (int sl = split[k]; sl < split[k + 1]; sl++) np += T.slice_width[sl];
+            resPanels = std::max(resPanels, np);
+        }
+        std::copy(split.begin(), split.end(), hrsplit.begin() + t * (CS_RES_MAX_CL + 1));
+    }
+    c->resCL = c->resThreads = c->resClusters = 0;
+    c->resSmem = 0;
+    int resCap = 0;
+    if (resW > 0) {
+        cudaDeviceProp prop;
+        CS_CUDA(cudaGetDeviceProperties(&prop, c->device));
+        cudaFuncAttributes fa;
+        CS_CUDA(cudaFuncGetAttributes(&fa, cs_resident_pcg_kernel));
+        const size_t pbytes = (size_t)resW * CS_SLICE * sizeof(float4);
+        const size_t budget = prop.sharedMemPerBlockOptin > fa.sharedSizeBytes + pbytes
+                                  ? prop.sharedMemPerBlockOptin - fa.sharedSizeBytes - pbytes : 0;
+        resCap = (int)std::min<size_t>((size_t)resPanels, budget / (CS_PANEL_FLOATS * sizeof(float)));
+        const size_t smem = (size_t)resCap * CS_PANEL_FLOATS * sizeof(float) + pbytes;
+        int nclusters = 0;
+        if (budget > 0) {
+            CS_CUDA(cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            if (resCL > 8) CS_CUDA(cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = resCL;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(resCL);
+            cfg.blockDim = dim3(resW * CS_SLICE);
+            cfg.dynamicSmemBytes = smem;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, cs_resident_pcg_kernel, &cfg) != cudaSuccess) {
+                cudaGetLastError();
+                nclusters = 0;
+            }
+        }
+        if (nclusters > 0) {
+            c->resCL = resCL;
+            c->resThreads = resW * CS_SLICE;
+            c->resClusters = nclusters;
+            c->resSmem = smem;
+        } else {
+            std::fill(topoResident.begin(), topoResident.end(), 0);
+        }
+    }
     {
         int tp = 0, ts = 0;
         for (size_t t = 0; t < topos.size(); t++) {
@@ -745,6 +865,14 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             const Topo& T = *topos[t];
             int cbase = (int)htcontrib.size();
             htcol.insert(htcol.end(), T.tcol.begin(), T.tcol.end());
+            if (topoResident[t]) {
+                std::vector<int> code = residentCodes(T, std::vector<int>(hrsplit.begin() + t * (CS_RES_MAX_CL + 1),
+                                                                          hrsplit.begin() + (t + 1) * (CS_RES_MAX_CL + 1)),
+                                                      c->resCL);
+                hrcode.insert(hrcode.end(), code.begin(), code.end());
+            } else {
+                hrcode.insert(hrcode.end(), T.tcol.size(), 0);
+            }
             for (size_t i = 0; i + 1 < T.tcptr.size(); i++) htcptr.push_back(T.tcptr[i] + cbase);
             htcontrib.insert(htcontrib.end(), T.tcontrib.begin(), T.tcontrib.end());
             hrowmap.insert(hrowmap.end(), T.rowmap.begin(), T.rowmap.end());
@@ -779,6 +907,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         sd.nbr_ptr_off = topoNbrPtr0[sheetTopoId[s]];
         sd.row2slot_off = topoRow2Slot0[sheetTopoId[s]];
         sd.nbr_off = topoNbr0[sheetTopoId[s]];
+        sd.resident = topoResident[sheetTopoId[s]];
         hnode_sheet.insert(hnode_sheet.end(), d.n_nodes, s);
         float bmult = m.bending_mult * m.thicken;
         for (int i = 0; i < 15; i++) sd.bending[i] = m.bending[i / 5][i % 5] * bmult;
@@ -866,6 +995,14 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     B.n_tpanels = (int)(htcol.size() / CS_SLICE);
     B.n_tables = (int)(tables.size() / CS_TABLE_ENTRIES);
     c->nnzb_pattern = nnzb;
+    // resident sheets, largest first (the persistent clusters take them in this order)
+    std::vector<int> hrlist;
+    for (int s = 0; s < n_sheets; s++)
+        if (hs[s].resident) hrlist.push_back(s);
+    std::stable_sort(hrlist.begin(), hrlist.end(), [&](int a, int b) { return hs[a].n_slices > hs[b].n_slices; });
+    B.n_resident = (int)hrlist.size();
+    B.res_cap = resCap;
+    c->resClusters = std::min(c->resClusters, B.n_resident);
     c->sheets = hs;
     c->slices = hslices;
 
@@ -894,6 +1031,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     UP(node_sheet, hnode_sheet);
     UP(rowmap, hrowmap);
     UP(row2slot, hrow2slot);
+    UP(rlist, hrlist);
+    UP(rsplit, hrsplit);
+    UP(rcode, hrcode);
 #undef UP
 #define AL(field, n) \
     if ((st = dalloc(c, &B.field, (size_t)(n))) != CS_OK) return st;
@@ -928,6 +1068,18 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         c->gatherGrid = std::max(1, std::min(nblk((long long)B.n_slices * 32, 128), 2 * prop.multiProcessorCount));
     }
     c->loaded = true;
+    return CS_OK;
+}
+
+cs_status cs_get_solver_info(const cs_ctx* c, int* info) {
+    if (!c || !info) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return CS_ERR_STATE;
+    info[0] = c->B.n_resident;
+    info[1] = c->resCL;
+    info[2] = c->resThreads;
+    info[3] = c->resClusters;
+    info[4] = c->B.res_cap;
+    info[5] = (int)c->resSmem;
     return CS_OK;
 }
 
@@ -998,6 +1150,7 @@ static cs_status validateParams(cs_ctx* c, const cs_step_params* p) {
         if (!std::isfinite(p->gravity[i])) return fail(c, CS_ERR_INVALID_ARG, "bad gravity");
     if (p->precision != CS_PREC_PLAIN_FP32 && p->precision != CS_PREC_MIXED) return fail(c, CS_ERR_INVALID_ARG, "bad precision");
     if (p->warm_start < CS_WARM_ZERO || p->warm_start > CS_WARM_GIVEN) return fail(c, CS_ERR_INVALID_ARG, "bad warm start");
+    if (p->solver != CS_SOLVER_AUTO && p->solver != CS_SOLVER_BATCHED) return fail(c, CS_ERR_INVALID_ARG, "bad solver");
     if (p->warm_start == CS_WARM_LEARNED && !c->mlpInit)
         return fail(c, CS_ERR_NOT_TRAINED, "learned warm start: no network (cs_mlp_init / cs_mlp_set_weights)");
     return CS_OK;
@@ -1032,9 +1185,10 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
         if ((st = buildGraph(c, learned)) != CS_OK) return st;
         CS_CUDA(cudaGraphLaunch(learned ? c->graphExecLearned : c->graphExec, c->stream));
     } else {
-        c->hostLaunches += launchAssembly(c) + 3;
+        c->hostLaunches += launchAssembly(c) + 3 + (c->resClusters > 0 ? 1 : 0);
         if (learned) c->hostLaunches += launchMlpInference(c, c->B.warm);
         launchSolvePrologue(c);
+        launchResident(c);
         int go = 1;
         int trips = 0;
         while (go) {
@@ -1052,7 +1206,8 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
     c->steps++;
     if (p->use_graph) {
         c->graphSteps++;
-        c->graphLaunchesFixed += (c->B.F ? 1 : 0) + (c->B.E ? 1 : 0) + 1 + 3 + (learned ? 3 : 0);
+        c->graphLaunchesFixed += (c->B.F ? 1 : 0) + (c->B.E ? 1 : 0) + 1 + 3 + (learned ? 3 : 0) +
+                                 (c->resClusters > 0 ? 1 : 0);
     }
     if (!stats) return CS_OK;
     std::vector<InstState> inst(c->B.S);

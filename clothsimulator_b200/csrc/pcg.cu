@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(128) cs_reduce2_kernel(Batch B, cudaGraphCondi
         if (ph == PH_FINISH) I.phase = PH_DONE;
     }
     if (threadIdx.x == 0) {
-        if (I.phase != PH_DONE) atomicAdd(&B.loop[1], 1);
+        if (I.phase != PH_DONE && I.phase != PH_RESIDENT) atomicAdd(&B.loop[1], 1);
         __threadfence();
         int ticket = atomicAdd(&B.loop[2], 1);
         if (ticket == (int)gridDim.x - 1) {
@@ -374,12 +374,16 @@ __global__ void __launch_bounds__(128) cs_solve_setup_kernel(Batch B) {
         I.resnorm = I.first_res = -1.0;
         I.alpha = I.beta = 0.f;
         I.sweep_iters = I.iters = I.sweeps = I.flags = 0;
-        I.phase = B.params->warm ? PH_RES : PH_INIT;
+        if (sh.resident && B.params->solver == CS_SOLVER_AUTO_DEV)
+            I.phase = PH_RESIDENT;  // solved by cs_resident_pcg_kernel before the loop runs
+        else
+            I.phase = B.params->warm ? PH_RES : PH_INIT;
         if (s == 0) {
             B.loop[0] = 0;
             B.loop[1] = 0;
             B.loop[2] = 0;
             B.loop[3] = 1;
+            B.loop[5] = 0;
         }
     }
 }

@@ -28,6 +28,7 @@ CS_ERR_NOT_TRAINED = 8
 PREC_PLAIN_FP32 = 0
 PREC_MIXED = 1
 WARM_ZERO, WARM_PREVIOUS, WARM_LEARNED, WARM_GIVEN = 0, 1, 2, 3
+SOLVER_AUTO, SOLVER_BATCHED = 0, 1
 
 EXPORTED = [
     "cs_create", "cs_destroy", "cs_last_error", "cs_load_batch", "cs_get_sizes", "cs_set_state", "cs_get_state",
@@ -36,7 +37,7 @@ EXPORTED = [
     "cs_device_pointers", "cs_profile_kernels", "cs_get_counters", "cs_get_stream",
     "cs_solve_block_csr_noalloc", "cs_tc_gemm_check", "cs_mlp_init", "cs_mlp_record", "cs_mlp_fit_normalization",
     "cs_mlp_train", "cs_mlp_gradient", "cs_mlp_predict", "cs_mlp_get_record", "cs_mlp_get_weights",
-    "cs_mlp_set_weights",
+    "cs_mlp_set_weights", "cs_get_solver_info",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -73,7 +74,7 @@ class StepParams(ctypes.Structure):
         ("dt", ctypes.c_float), ("gravity", ctypes.c_float * 3), ("handle_stiffness", ctypes.c_float),
         ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double), ("max_iters", ctypes.c_int),
         ("sweep_cap", ctypes.c_int), ("precision", ctypes.c_int), ("warm_start", ctypes.c_int),
-        ("advance", ctypes.c_int), ("use_graph", ctypes.c_int),
+        ("advance", ctypes.c_int), ("use_graph", ctypes.c_int), ("solver", ctypes.c_int),
     ]
 
 
@@ -104,6 +105,7 @@ def load_library() -> ctypes.CDLL:
         "cs_destroy": [vp],
         "cs_load_batch": [vp, ctypes.POINTER(MaterialDesc), ctypes.c_int, ctypes.POINTER(SheetDesc), ctypes.c_int],
         "cs_get_sizes": [vp, ctypes.POINTER(ctypes.c_longlong)],
+        "cs_get_solver_info": [vp, ctypes.POINTER(ctypes.c_int)],
         "cs_set_state": [vp, _fp, _fp],
         "cs_get_state": [vp, _fp, _fp],
         "cs_set_state_device": [vp, vp, vp],
@@ -175,7 +177,8 @@ def material_desc(spec: dict) -> MaterialDesc:
 
 
 def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, inner_tol=1e-4, max_iters=2000,
-                sweep_cap=0, precision=PREC_MIXED, warm_start=WARM_ZERO, advance=1, use_graph=1) -> StepParams:
+                sweep_cap=0, precision=PREC_MIXED, warm_start=WARM_ZERO, advance=1, use_graph=1,
+                solver=0) -> StepParams:
     p = StepParams()
     p.dt = dt
     for i in range(3):
@@ -189,6 +192,7 @@ def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, in
     p.warm_start = warm_start
     p.advance = advance
     p.use_graph = use_graph
+    p.solver = solver
     return p
 
 
@@ -259,6 +263,13 @@ class Context:
         s = (ctypes.c_longlong * 7)()
         self.check(self.lib.cs_get_sizes(self.h, s))
         return [int(v) for v in s]
+
+    def solver_info(self) -> dict:
+        """Cluster-resident solve plan of the loaded batch."""
+        s = (ctypes.c_int * 6)()
+        self.check(self.lib.cs_get_solver_info(self.h, s))
+        keys = ("resident_sheets", "ctas_per_cluster", "threads_per_cta", "clusters", "panels_in_smem", "smem_bytes")
+        return dict(zip(keys, [int(v) for v in s]))
 
     def set_state(self, x=None, v=None):
         xa = _f32(x) if x is not None else None

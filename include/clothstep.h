@@ -87,7 +87,16 @@ typedef struct cs_step_params {
     int warm_start;           /* CS_WARM_* */
     int advance;              /* 1: v += dv and x += dt v (a full step); 0: solve only */
     int use_graph;            /* 1: run the captured CUDA graph; 0: host-driven launches */
+    int solver;               /* CS_SOLVER_*: which PCG kernels solve the sheets */
 } cs_step_params;
+
+/* CS_SOLVER_AUTO: sheets whose system fits one thread-block cluster's shared memory are
+ * solved by a cluster each, the system resident on chip for the whole solve; the others by
+ * the batched loop.  CS_SOLVER_BATCHED: every sheet by the batched loop (the system streamed
+ * from HBM every iteration).  Both run the same mixed/plain PCG to the same FP64-checked
+ * tolerance. */
+#define CS_SOLVER_AUTO 0
+#define CS_SOLVER_BATCHED 1
 
 typedef struct cs_step_stats {
     int n_instances;
@@ -115,6 +124,11 @@ cs_status cs_load_batch(cs_ctx* ctx, const cs_material_desc* materials, int n_ma
 /* sizes[0..6] = nodes, faces, interior edges, stored 3x3 blocks (incl. padding), slices,
  * sheets, nonzero blocks of the pattern. */
 cs_status cs_get_sizes(const cs_ctx* ctx, long long* sizes);
+
+/* info[0..5] = sheets solved cluster-resident, CTAs per cluster, threads per CTA, clusters
+ * in the persistent grid, SELL panels per CTA in shared memory, dynamic shared memory bytes
+ * per CTA.  No counterpart in the reference (its solver has no such plan). */
+cs_status cs_get_solver_info(const cs_ctx* ctx, int* info);
 
 /* Node state of the whole batch, sheets concatenated in load order (3 floats per node). */
 cs_status cs_set_state(cs_ctx* ctx, const float* x, const float* v);

@@ -1,0 +1,161 @@
+"""Cluster-resident PCG (one thread-block cluster per sheet, the system in distributed shared
+memory) against the CPU oracle and against the batched loop on the same state.
+
+Tolerances (norm-wise relative):
+  * dv of a solve to an FP64-checked relative residual of 1e-10 against an FP64 direct solve
+    of the same FP32 system: 1e-6 (as for the batched loop);
+  * plain FP32 PCG: the FP64-checked residual of the resident and batched solvers within a
+    factor 10 of each other (FP32 rounding differs with the summation order);
+  * iteration counts of the resident and batched solvers on identical systems: within 10 %
+    (same iteration, different summation order of the dot products).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+import pyoracle
+from clothsimulator_b200 import native, scenes
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64).reshape(-1)
+    b = np.asarray(b, np.float64).reshape(-1)
+    den = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))
+
+
+def params_for(scene, **kw):
+    kw.setdefault("tol", 1e-10)
+    kw.setdefault("max_iters", 20000)
+    kw.setdefault("advance", 0)
+    return native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, **kw)
+
+
+def oracle_dv(scene, sheet):
+    c = pyoracle.Cloth(sheet, pyoracle.Material(sheet["material"], "float"))
+    c.assemble(scenes.step_params(scene, sheet))
+    dv, _ = c.solve(pyoracle.METHOD_LLT64)
+    return dv
+
+
+def split_dv(ctx, scene):
+    dv = ctx.get_dv().reshape(-1, 3)
+    out, o = [], 0
+    for s in scene.sheets:
+        n = s["x"].shape[0]
+        out.append(dv[o:o + n].reshape(-1))
+        o += n
+    return out
+
+
+def initial_state(scene):
+    return (np.concatenate([s["x"] for s in scene.sheets]), np.concatenate([s["v"] for s in scene.sheets]))
+
+
+def test_plan_covers_sheets_that_fit(ctx_factory):
+    scene = scenes.windy_batch(6, 64, seed=11)
+    ctx = ctx_factory(scene.sheets)
+    info = ctx.solver_info()
+    assert info["resident_sheets"] == 6
+    assert info["ctas_per_cluster"] == 8 and info["clusters"] >= 1
+    assert info["threads_per_cta"] % 32 == 0 and info["threads_per_cta"] <= 768
+    # a 128x128 sheet needs more than 24 slices per CTA: it stays in the batched loop
+    big = scenes.windy_batch(1, 128, seed=12).sheets + scenes.windy_batch(2, 32, seed=13).sheets
+    ctx2 = ctx_factory(big)
+    assert ctx2.solver_info()["resident_sheets"] == 2
+
+
+def test_resident_solve_matches_oracle(ctx_factory):
+    scene = scenes.windy_batch(3, 32, seed=21)
+    scene.sheets += scenes.windy_batch(1, 64, seed=22).sheets
+    ctx = ctx_factory(scene.sheets)
+    assert ctx.solver_info()["resident_sheets"] == 4
+    stats, _ = ctx.step(params_for(scene))
+    assert stats.converged == 4
+    for s, dv in zip(scene.sheets, split_dv(ctx, scene)):
+        assert rel(dv, oracle_dv(scene, s)) < 1e-6
+
+
+def test_resident_and_batched_agree(ctx_factory):
+    scene = scenes.windy_batch(4, 32, seed=31)
+    ctx = ctx_factory(scene.sheets)
+    x0, v0 = initial_state(scene)
+    res = {}
+    for solver in (native.SOLVER_AUTO, native.SOLVER_BATCHED):
+        ctx.set_state(x0, v0)
+        stats, _ = ctx.step(params_for(scene, solver=solver))
+        it, rr, fl = ctx.instance_stats()
+        res[solver] = (ctx.get_dv().copy(), it.copy(), rr.copy(), fl.copy(), stats.loop_trips)
+    dva, ita, rra, fla, tripa = res[native.SOLVER_AUTO]
+    dvb, itb, rrb, flb, tripb = res[native.SOLVER_BATCHED]
+    assert np.all(fla & 1) and np.all(flb & 1)
+    assert np.all(rra <= 1e-10) and np.all(rrb <= 1e-10)
+    assert rel(dva, dvb) < 1e-6
+    assert np.all(np.abs(ita - itb) <= 0.1 * itb + 2)
+    # every sheet resident: the batched loop only runs its closing trip
+    assert tripa <= 1 < tripb
+
+
+def test_resident_plain_fp32_matches_batched_plain(ctx_factory):
+    scene = scenes.windy_batch(4, 32, seed=41)
+    ctx = ctx_factory(scene.sheets)
+    x0, v0 = initial_state(scene)
+    res = {}
+    for solver in (native.SOLVER_AUTO, native.SOLVER_BATCHED):
+        ctx.set_state(x0, v0)
+        ctx.step(params_for(scene, tol=1e-6, precision=native.PREC_PLAIN_FP32, solver=solver), allow_unconverged=True)
+        res[solver] = ctx.instance_stats()
+    ita, rra, fla = res[native.SOLVER_AUTO]
+    itb, rrb, flb = res[native.SOLVER_BATCHED]
+    assert np.all(ita > 0) and np.all(np.abs(ita - itb) <= 0.1 * itb + 2)
+    # the FP64 check of the plain solver's answer: converged exactly when it met tol
+    assert np.array_equal((fla & 1) > 0, rra <= 1e-6)
+    assert np.all(rra < 1e-3) and np.all(np.abs(np.log10(rra / rrb)) < 1.0)
+
+
+def test_resident_warm_start_and_guard(ctx_factory):
+    scene = scenes.windy_batch(4, 32, seed=51)
+    ctx = ctx_factory(scene.sheets)
+    p = params_for(scene, tol=1e-8, advance=1)
+    ctx.step(p)
+    p.warm_start = native.WARM_PREVIOUS
+    stats, _ = ctx.step(p)
+    assert stats.converged == 4
+    # a warm start far worse than zero must be discarded, and the solve still converges
+    ctx.set_warm_start(np.full((ctx.n, 3), 1e3, np.float32))
+    p.warm_start = native.WARM_GIVEN
+    stats, _ = ctx.step(p)
+    assert stats.converged == 4 and stats.warm_rejected == 4
+
+
+def test_resident_iteration_cap_returns(ctx_factory):
+    scene = scenes.windy_batch(3, 32, seed=61)
+    ctx = ctx_factory(scene.sheets)
+    stats, st = ctx.step(params_for(scene, max_iters=5), allow_unconverged=True)
+    it, rr, fl = ctx.instance_stats()
+    assert st == native.CS_ERR_NOT_CONVERGED
+    assert np.all(it <= 5) and np.all(fl & 8) and not np.any(fl & 1)
+
+
+def test_resident_is_deterministic(ctx_factory):
+    scene = scenes.windy_batch(3, 32, seed=71)
+    ctx = ctx_factory(scene.sheets)
+    x0, v0 = initial_state(scene)
+    out = []
+    for _ in range(2):
+        ctx.set_state(x0, v0)
+        ctx.step(params_for(scene, tol=1e-6))
+        out.append(ctx.get_dv().copy())
+    assert np.array_equal(out[0], out[1])
+
+
+def test_mixed_resident_and_batched_batch(ctx_factory):
+    sheets = scenes.windy_batch(1, 128, seed=81).sheets + scenes.windy_batch(2, 32, seed=82).sheets
+    scene = scenes.Scene("mixed", sheets, dt=1.0 / 100, steps=1)
+    ctx = ctx_factory(scene.sheets)
+    assert ctx.solver_info()["resident_sheets"] == 2
+    stats, _ = ctx.step(params_for(scene))
+    assert stats.converged == 3
+    for s, dv in zip(scene.sheets, split_dv(ctx, scene)):
+        assert rel(dv, oracle_dv(scene, s)) < 1e-6
