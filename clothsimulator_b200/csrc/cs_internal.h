@@ -71,9 +71,11 @@ enum InstPhase : int {
     PH_RESIDENT = 5,  // owned by the cluster-resident kernel this step (skipped by the loop)
 };
 
-// Cluster-resident solver limits: CTAs per cluster, warps (slices) per CTA.
+// Cluster-resident solver limits: CTAs per cluster, warps (slices) per CTA, block slots per
+// row (the SpMV over a row is fully unrolled to this width; column codes live in registers).
 #define CS_RES_MAX_CL 16
-#define CS_RES_MAX_WARPS 24
+#define CS_RES_MAX_WARPS 18
+#define CS_RES_MAX_WIDTH 16
 #define CS_SOLVER_AUTO_DEV 0
 #define CS_SOLVER_BATCHED_DEV 1
 
@@ -163,7 +165,11 @@ struct Batch {
     int res_cap = 0;             // panels per CTA held in shared memory
     int* rlist = nullptr;        // resident sheets, largest first
     int* rsplit = nullptr;       // per topology: CS_RES_MAX_CL + 1 sheet-relative slice bounds per CTA rank
-    int* rcode = nullptr;        // per topology panel slot: (owner rank << 16) | owner-local row slot
+    int* rcode = nullptr;        // per topology panel slot: index of its column in the reading CTA's p array
+    int* rsendptr = nullptr;     // per topology: CS_RES_MAX_CL + 1 offsets into rsend per owner rank
+    uint32_t* rsend = nullptr;   // halo sends: src slot | dst rank << 12 | dst halo index << 16
+    int* rhalo = nullptr;        // per topology: CS_RES_MAX_CL + 1 halo slot counts per rank
+    int res_halo0 = 0;           // first halo slot of every CTA's p array (= own slots per CTA)
 };
 
 #endif

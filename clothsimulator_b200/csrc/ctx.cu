@@ -441,16 +441,75 @@ int residentSplit(const Topo& T, int ncta, std::vector<int>& split) {
     return w;
 }
 
-// Owner-rank code of every panel slot of a topology: (rank << 16) | rank-local row slot.
-std::vector<int> residentCodes(const Topo& T, const std::vector<int>& split, int ncta) {
-    std::vector<int> nodeCode(T.n_nodes, 0);
+// Halo plan of one topology on a cluster of `ncta` CTAs.  CTA c owns the rows of slices
+// [split[c], split[c+1]) at local slots (slice - split[c]) * 32 + lane.  Every column a CTA's
+// rows reference that another CTA owns gets a halo slot in the reading CTA, numbered by
+// (owner rank, owner slot).  code: per panel slot, the local p index of its column (own slot,
+// or CS_RES_HALO_BIT | halo index, rebased once the batch's own-slot count is known).  send:
+// per owner CTA (sendptr), the entries src slot | dst rank << 12 | dst halo index << 16.
+struct ResidentPlan {
+    std::vector<int> split, code, sendptr, halo_count;
+    std::vector<uint32_t> send;
+    int w = 0, max_halo = 0, max_panels = 0, max_width = 0;
+};
+
+#define CS_RES_HALO_BIT 0x40000000
+
+ResidentPlan residentPlan(const Topo& T, int ncta) {
+    ResidentPlan P;
+    P.w = residentSplit(T, ncta, P.split);
+    const int nn = T.n_nodes;
+    std::vector<int> owner(nn, 0), oslot(nn, 0);
     for (int c = 0; c < ncta; c++)
-        for (int sl = split[c]; sl < split[c + 1]; sl++)
-            for (int l = 0; l < T.slice_rows[sl]; l++)
-                nodeCode[T.rowmap[sl * CS_SLICE + l]] = (c << 16) | ((sl - split[c]) * CS_SLICE + l);
-    std::vector<int> code(T.tcol.size(), 0);
-    for (size_t i = 0; i < T.tcol.size(); i++) code[i] = nodeCode[T.tcol[i]];
-    return code;
+        for (int sl = P.split[c]; sl < P.split[c + 1]; sl++)
+            for (int l = 0; l < T.slice_rows[sl]; l++) {
+                owner[T.rowmap[sl * CS_SLICE + l]] = c;
+                oslot[T.rowmap[sl * CS_SLICE + l]] = (sl - P.split[c]) * CS_SLICE + l;
+            }
+    P.code.assign(T.tcol.size(), 0);
+    P.halo_count.assign(CS_RES_MAX_CL + 1, 0);
+    std::vector<std::vector<std::pair<int, int>>> halo(ncta);  // per reader: (owner, owner slot) sorted
+    for (int c = 0; c < ncta; c++) {
+        std::vector<std::pair<int, int>> need;
+        int np = 0;
+        for (int sl = P.split[c]; sl < P.split[c + 1]; sl++) {
+            np += T.slice_width[sl];
+            P.max_width = std::max(P.max_width, T.slice_width[sl]);
+            for (int k = 0; k < T.slice_width[sl]; k++)
+                for (int l = 0; l < T.slice_rows[sl]; l++) {
+                    const int col = T.tcol[(size_t)(T.slice_tpanel0[sl] + k) * CS_SLICE + l];
+                    if (owner[col] != c) need.push_back({owner[col], oslot[col]});
+                }
+        }
+        P.max_panels = std::max(P.max_panels, np);
+        std::sort(need.begin(), need.end());
+        need.erase(std::unique(need.begin(), need.end()), need.end());
+        halo[c] = need;
+        P.max_halo = std::max(P.max_halo, (int)need.size());
+        P.halo_count[c] = (int)need.size();
+        for (int sl = P.split[c]; sl < P.split[c + 1]; sl++)
+            for (int k = 0; k < T.slice_width[sl]; k++)
+                for (int l = 0; l < T.slice_rows[sl]; l++) {
+                    const size_t slot = (size_t)(T.slice_tpanel0[sl] + k) * CS_SLICE + l;
+                    const int col = T.tcol[slot];
+                    if (owner[col] == c) {
+                        P.code[slot] = oslot[col];
+                    } else {
+                        auto it = std::lower_bound(need.begin(), need.end(), std::make_pair(owner[col], oslot[col]));
+                        P.code[slot] = CS_RES_HALO_BIT | (int)(it - need.begin());
+                    }
+                }
+    }
+    P.sendptr.assign(CS_RES_MAX_CL + 1, 0);
+    for (int c = 0; c < ncta; c++) {
+        P.sendptr[c] = (int)P.send.size();
+        for (int d = 0; d < ncta; d++)
+            for (size_t h = 0; h < halo[d].size(); h++)
+                if (halo[d][h].first == c)
+                    P.send.push_back((uint32_t)halo[d][h].second | ((uint32_t)d << 12) | ((uint32_t)h << 16));
+    }
+    for (int c = ncta; c <= CS_RES_MAX_CL; c++) P.sendptr[c] = (int)P.send.size();
+    return P;
 }
 
 }  // namespace
@@ -799,21 +858,24 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     if (resCL != 0 && resCL != 2 && resCL != 4 && resCL != 8 && resCL != 16)
         return fail(c, CS_ERR_INVALID_ARG, "CS_RESIDENT_CL must be 0, 2, 4, 8 or 16");
     std::vector<int> hrsplit(topos.size() * (CS_RES_MAX_CL + 1), 0), hrcode;
+    std::vector<int> hrsendptr(topos.size() * (CS_RES_MAX_CL + 1), 0);
+    std::vector<int> hrhalo(topos.size() * (CS_RES_MAX_CL + 1), 0);
+    std::vector<uint32_t> hrsend;
     std::vector<char> topoResident(topos.size(), 0);
-    int resW = 0, resPanels = 0;
+    std::vector<ResidentPlan> plans(topos.size());
+    int resW = 0, resPanels = 0, resHalo = 0;
     for (size_t t = 0; t < topos.size() && resCL > 0; t++) {
-        const Topo& T = *topos[t];
-        std::vector<int> split;
-        const int w = residentSplit(T, resCL, split);
-        if (w > CS_RES_MAX_WARPS) continue;
+        plans[t] = residentPlan(*topos[t], resCL);
+        const ResidentPlan& P = plans[t];
+        // p indices (own slots + halo) are 12-bit in the kernel's packed column codes
+        if (P.w > CS_RES_MAX_WARPS || P.max_width > CS_RES_MAX_WIDTH || P.max_halo + CS_RES_MAX_WARPS * CS_SLICE >= 4096)
+            continue;
         topoResident[t] = 1;
-        resW = std::max(resW, w);
-        for (int k = 0; k < resCL; k++) {
-            int np = 0;
-            for (int sl = split[k]; sl < split[k + 1]; sl++) np += T.slice_width[sl];
-            resPanels = std::max(resPanels, np);
-        }
-        std::copy(split.begin(), split.end(), hrsplit.begin() + t * (CS_RES_MAX_CL + 1));
+        resW = std::max(resW, P.w);
+        resPanels = std::max(resPanels, P.max_panels);
+        resHalo = std::max(resHalo, P.max_halo);
+        std::copy(P.split.begin(), P.split.end(), hrsplit.begin() + t * (CS_RES_MAX_CL + 1));
+        std::copy(P.halo_count.begin(), P.halo_count.end(), hrhalo.begin() + t * (CS_RES_MAX_CL + 1));
     }
     c->resCL = c->resThreads = c->resClusters = 0;
     c->resSmem = 0;
@@ -823,7 +885,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         CS_CUDA(cudaGetDeviceProperties(&prop, c->device));
         cudaFuncAttributes fa;
         CS_CUDA(cudaFuncGetAttributes(&fa, cs_resident_pcg_kernel));
-        const size_t pbytes = (size_t)resW * CS_SLICE * sizeof(float4);
+        const size_t pbytes = ((size_t)resW * CS_SLICE + resHalo) * sizeof(float4);
         const size_t budget = prop.sharedMemPerBlockOptin > fa.sharedSizeBytes + pbytes
                                   ? prop.sharedMemPerBlockOptin - fa.sharedSizeBytes - pbytes : 0;
         resCap = (int)std::min<size_t>((size_t)resPanels, budget / (CS_PANEL_FLOATS * sizeof(float)));
@@ -866,10 +928,12 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             int cbase = (int)htcontrib.size();
             htcol.insert(htcol.end(), T.tcol.begin(), T.tcol.end());
             if (topoResident[t]) {
-                std::vector<int> code = residentCodes(T, std::vector<int>(hrsplit.begin() + t * (CS_RES_MAX_CL + 1),
-                                                                          hrsplit.begin() + (t + 1) * (CS_RES_MAX_CL + 1)),
-                                                      c->resCL);
-                hrcode.insert(hrcode.end(), code.begin(), code.end());
+                // halo slots follow the batch's own slots in every CTA's p array
+                for (int code : plans[t].code)
+                    hrcode.push_back(code & CS_RES_HALO_BIT ? resW * CS_SLICE + (code & ~CS_RES_HALO_BIT) : code);
+                const int base = (int)hrsend.size();
+                for (int k = 0; k <= CS_RES_MAX_CL; k++) hrsendptr[t * (CS_RES_MAX_CL + 1) + k] = base + plans[t].sendptr[k];
+                hrsend.insert(hrsend.end(), plans[t].send.begin(), plans[t].send.end());
             } else {
                 hrcode.insert(hrcode.end(), T.tcol.size(), 0);
             }
@@ -1002,6 +1066,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     std::stable_sort(hrlist.begin(), hrlist.end(), [&](int a, int b) { return hs[a].n_slices > hs[b].n_slices; });
     B.n_resident = (int)hrlist.size();
     B.res_cap = resCap;
+    B.res_halo0 = resW * CS_SLICE;
     c->resClusters = std::min(c->resClusters, B.n_resident);
     c->sheets = hs;
     c->slices = hslices;
@@ -1034,6 +1099,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     UP(rlist, hrlist);
     UP(rsplit, hrsplit);
     UP(rcode, hrcode);
+    UP(rsendptr, hrsendptr);
+    UP(rsend, hrsend);
+    UP(rhalo, hrhalo);
 #undef UP
 #define AL(field, n) \
     if ((st = dalloc(c, &B.field, (size_t)(n))) != CS_OK) return st;
@@ -1236,6 +1304,7 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
     CS_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     stats->ms = ms;
     if (loopv[0] >= d.loop_cap) return fail(c, CS_ERR_TIMEOUT, "solve loop hit its trip bound (%d)", d.loop_cap);
+    if (loopv[6]) return fail(c, CS_ERR_TIMEOUT, "cluster-resident solve: a wait on another CTA ran out");
     if (capped) return fail(c, breakdown ? CS_ERR_NON_SPD : CS_ERR_NOT_CONVERGED, "%d of %d sheets did not converge",
                             c->B.S - stats->converged, c->B.S);
     return CS_OK;

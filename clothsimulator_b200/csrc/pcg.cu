@@ -384,6 +384,7 @@ __global__ void __launch_bounds__(128) cs_solve_setup_kernel(Batch B) {
             B.loop[2] = 0;
             B.loop[3] = 1;
             B.loop[5] = 0;
+            B.loop[6] = 0;
         }
     }
 }

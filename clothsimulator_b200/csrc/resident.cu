@@ -2,25 +2,34 @@
 // held in the cluster's distributed shared memory for the whole solve.
 //
 // The batched loop of pcg.cu streams every sheet's matrix from HBM once per CG iteration
-// (about 1.7 MB per 64x64 sheet, ~340 iterations per step).  A sheet of that size fits in
+// (about 1.7 MB per 64x64 sheet, ~330 iterations per step).  A sheet of that size fits in
 // the shared memory of an 8-CTA cluster (8 x 227 KB), so here each cluster
 //   * takes the next sheet from a device work counter (persistent clusters; a sheet that
 //     converges early frees its cluster at once, there is no batch-wide tail),
-//   * copies its share of the sheet's SELL-32 panels into shared memory once,
-//   * runs the same per-instance state machine as the batched loop (FP32 CG on the
-//     correction system, FP64 dot products and norms, FP64 outer residual b - A dv64,
-//     warm-start guard, inner and outer stopping tests) with the FP32 vectors in registers
-//     (one thread per row) and the search direction p in shared memory, where the other
-//     CTAs of the cluster read it through distributed shared memory (DSMEM),
-//   * reduces dot products deterministically: warps by shuffle tree, warps of a CTA in
-//     index order, CTAs of the cluster in rank order, every CTA summing the same partials
-//     in the same order, so all CTAs take identical control decisions.
-// Rows of a slice that does not fit the shared-memory panel budget are read from global
-// memory (L2-resident at this working-set size) instead.
+//   * copies its share of the sheet's SELL-32 panels (a contiguous strip of slices) into
+//     shared memory once per solve,
+//   * runs the per-instance state machine of the batched loop (FP32 CG on the correction
+//     system, FP64 dot products and norms, FP64 outer residual b - A dv64, warm-start
+//     guard, inner and outer stopping tests) with the FP32 vectors in registers, one thread
+//     per row.  The CG recurrence is the Chronopoulos-Gear form: per iteration one SpMV
+//     w = A u and ONE fused reduction of (r.u, w.u, r.r), instead of two reductions;
+//   * exchanges data without cluster barriers: after u = P^-1 r each CTA pushes the values
+//     of its strip's boundary rows into the halo slots of the CTAs that read them with
+//     st.async remote stores, which complete bytes on the receiver's mbarrier; reduction
+//     partials travel the same way.  A CTA waits only on its own mbarriers.  Sends for step
+//     k+1 depend on every CTA's step-k partial, so one halo buffer and two reduction buffers
+//     suffice (a sender is never two steps ahead of a receiver);
+//   * sums deterministically: butterflies within warps, over warp partials, over CTA
+//     partials (IEEE addition is commutative, so every lane of a butterfly ends with the same
+//     bits), every CTA summing the same partials: all CTAs take identical decisions.
+// Every wait is bounded.  A CTA whose wait runs out raises an abort flag in all CTAs and an
+// error word for the host, and all CTAs leave through the kernel's final cluster barrier (the
+// only one after start-up), so no CTA exits while another may still address its memory.
+// Rows of a slice beyond the shared-memory panel budget are read from global memory.
 //
 // Replaces the reference's per-cloth GPU solve (Cloth.cu:766-809) like pcg.cu does; the
-// iteration is the same Jacobi-preconditioned CG (PhysicsHelper.cu:479-485 builds the
-// scalar Jacobi preconditioner; here the 3x3 block inverse from the gather kernel).
+// preconditioner is the 3x3 block inverse from the gather kernel (the reference builds the
+// scalar Jacobi one, PhysicsHelper.cu:479-485).
 #include <cooperative_groups.h>
 
 #include "cs_internal.h"
@@ -29,7 +38,57 @@ namespace cg = cooperative_groups;
 
 namespace {
 
-constexpr int RES_NBUF = 3;  // rotating reduction buffers: a buffer is rewritten two syncs later
+constexpr uint32_t RES_WAIT_TRIES = 1u << 20;
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint32_t mapa(uint32_t a, int rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void rbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void rbar_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool rbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Remote arrive on another CTA's mbarrier, releasing this thread's prior writes cluster-wide.
+__device__ __forceinline__ void rbar_arrive_remote(uint32_t cbar) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cbar) : "memory");
+}
+
+__device__ __forceinline__ void st_async_f4(uint32_t caddr, float4 v, uint32_t cbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(caddr),
+                 "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "r"(cbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void st_async_d2(uint32_t caddr, double a, double b, uint32_t cbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(caddr), "d"(a),
+                 "d"(b), "r"(cbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void st_async_u32(uint32_t caddr, uint32_t v, uint32_t cbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];" ::"r"(caddr), "r"(v), "r"(cbar)
+                 : "memory");
+}
 
 __device__ __forceinline__ double rwarp_sum(double v) {
 #pragma unroll
@@ -45,56 +104,98 @@ __device__ __forceinline__ float rwarp_sum(float v) {
 
 __device__ __forceinline__ bool rfinite(double x) { return x == x && x < 1e300 && x > -1e300; }
 
-// Cluster-wide sum of NV values.  fp32: partials and sums in float (the plain FP32 solver);
-// otherwise double.  Ends with a cluster barrier; every thread of every CTA returns the
-// same sums.  `red` holds RES_NBUF x CS_RES_MAX_CL x 2 doubles, `wsum` 32 x 2 doubles.
-template <int NV>
-__device__ __forceinline__ void cluster_sum(const cg::cluster_group& cl, int rank, int ncta, double* red, double* wsum,
-                                            int& buf, double (&v)[NV], bool fp32) {
+// Shared control block of one CTA.
+struct __align__(16) ResShared {
+    double red[2][CS_RES_MAX_CL][4];   // reduction partials by sender rank, two buffers
+    double wsum[CS_RES_MAX_WARPS][4];  // warp partials
+    uint64_t bar[5];                   // 0 halo, 1-2 reduction buffers, 3 residual signal, 4 work item
+    int next;                          // work item sent by rank 0
+    int abort_flag;                    // raised by any CTA whose wait ran out
+};
+
+// Waits for `parity` of `bar` on every thread, at most RES_WAIT_TRIES polls, giving up early
+// once another CTA raised the abort flag.  Returns true on every thread only if the whole
+// CTA saw the phase complete.
+__device__ __forceinline__ bool res_wait(ResShared& S, uint32_t bar, uint32_t parity) {
+    bool ok = false;
+    for (uint32_t t = 0; t < RES_WAIT_TRIES; t++) {
+        if (rbar_try(bar, parity)) {
+            ok = true;
+            break;
+        }
+        if (*(volatile int*)&S.abort_flag) break;
+    }
+    return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+
+// Raises the abort flag in every CTA of the cluster and the error word for the host.
+__device__ __forceinline__ void res_abort(const cg::cluster_group& cl, ResShared& S, int ncta, int* err) {
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < ncta; c++) *(volatile int*)cl.map_shared_rank(&S.abort_flag, c) = 1;
+        atomicExch(err, 1);
+    }
+}
+
+// Cluster-wide sum of three values (fp32: in float, the plain FP32 solver; else double).
+// Partials travel by st.async into buffer `nred & 1` of every CTA.  Returns false if the
+// wait gave up (the caller aborts).
+__device__ __forceinline__ bool cluster_sum3(ResShared& S, int rank, int ncta, uint32_t& nred, double (&v)[3], bool fp32) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int b = (int)(nred & 1u);
 #pragma unroll
-    for (int i = 0; i < NV; i++) v[i] = fp32 ? (double)rwarp_sum((float)v[i]) : rwarp_sum(v[i]);
+    for (int i = 0; i < 3; i++) v[i] = fp32 ? (double)rwarp_sum((float)v[i]) : rwarp_sum(v[i]);
     if (lane == 0) {
 #pragma unroll
-        for (int i = 0; i < NV; i++) wsum[2 * w + i] = v[i];
+        for (int i = 0; i < 3; i++) S.wsum[w][i] = v[i];
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double t[NV];
+    if (w == 0) {
+        double t[3];
 #pragma unroll
-        for (int i = 0; i < NV; i++) {
-            if (fp32) {
-                float a = 0.f;
-                for (int j = 0; j < nw; j++) a += (float)wsum[2 * j + i];
-                t[i] = (double)a;
-            } else {
-                double a = 0.0;
-                for (int j = 0; j < nw; j++) a += wsum[2 * j + i];
-                t[i] = a;
-            }
+        for (int i = 0; i < 3; i++) {
+            const double x = lane < nw ? S.wsum[lane][i] : 0.0;
+            t[i] = fp32 ? (double)rwarp_sum((float)x) : rwarp_sum(x);
         }
-        double* slot = red + 2 * (buf * CS_RES_MAX_CL + rank);
-        for (int c = 0; c < ncta; c++) {
-            double* dst = cl.map_shared_rank(slot, c);
-#pragma unroll
-            for (int i = 0; i < NV; i++) dst[i] = t[i];
+        const uint32_t bar = saddr(&S.bar[1 + b]);
+        if (lane == 0) rbar_expect(bar, (uint32_t)ncta * 32u);
+        __syncwarp();
+        if (lane < ncta) {
+            const uint32_t dst = mapa(saddr(&S.red[b][rank][0]), lane);
+            const uint32_t dbar = mapa(bar, lane);
+            st_async_d2(dst, t[0], t[1], dbar);
+            st_async_d2(dst + 16, t[2], 0.0, dbar);
         }
     }
-    cl.sync();
-    const double* src = red + 2 * buf * CS_RES_MAX_CL;
+    const bool ok = res_wait(S, saddr(&S.bar[1 + b]), (nred >> 1) & 1u);
+    nred++;
 #pragma unroll
-    for (int i = 0; i < NV; i++) {
-        if (fp32) {
-            float a = 0.f;
-            for (int c = 0; c < ncta; c++) a += (float)src[2 * c + i];
-            v[i] = (double)a;
-        } else {
-            double a = 0.0;
-            for (int c = 0; c < ncta; c++) a += src[2 * c + i];
-            v[i] = a;
+    for (int i = 0; i < 3; i++) {
+        const double x = lane < ncta ? S.red[b][lane][i] : 0.0;
+        v[i] = fp32 ? (double)rwarp_sum((float)x) : rwarp_sum(x);
+    }
+    return ok;
+}
+
+// w = (row of A) u over a row's block slots, fully unrolled so that every slot's panel and u
+// loads are in flight together.  `cw` holds the slots' indices into this CTA's u array (own
+// rows, then halo copies of other CTAs' rows), two 16-bit indices per word.  `pn` points at
+// the row's first panel, in shared memory or (beyond the shared-memory budget) global memory.
+__device__ __forceinline__ void row_times_u(const float* __restrict__ pn, int width, const uint32_t (&cw)[CS_RES_MAX_WIDTH / 2],
+                                            const float4* su, int lane, float& q0, float& q1, float& q2) {
+#pragma unroll
+    for (int k = 0; k < CS_RES_MAX_WIDTH; k++) {
+        if (k < width) {
+            const int idx = (int)((cw[k >> 1] >> ((k & 1) * 16)) & 0xffffu);
+            const float* pk = pn + k * CS_PANEL_FLOATS;
+            const float4 a0 = reinterpret_cast<const float4*>(pk)[lane];
+            const float4 a1 = reinterpret_cast<const float4*>(pk + 128)[lane];
+            const float a8 = pk[256 + lane];
+            const float4 pv = su[idx];
+            q0 += a0.x * pv.x + a0.y * pv.y + a0.z * pv.z;
+            q1 += a0.w * pv.x + a1.x * pv.y + a1.y * pv.z;
+            q2 += a1.z * pv.x + a1.w * pv.y + a8 * pv.z;
         }
     }
-    buf = (buf + 1) % RES_NBUF;
 }
 
 }  // namespace
@@ -102,42 +203,56 @@ __device__ __forceinline__ void cluster_sum(const cg::cluster_group& cl, int ran
 extern __shared__ __align__(16) unsigned char cs_res_smem[];
 
 // Launch: cluster dimension (CL, 1, 1), blockDim = 32 x (slices per CTA, at most
-// CS_RES_MAX_WARPS), dynamic shared memory = res_cap panels + one float4 per row slot.
-// Grid: any number of whole clusters (persistent; each takes sheets until none is left).
+// CS_RES_MAX_WARPS), dynamic shared memory = res_cap panels + the u array (res_halo0 own row
+// slots, then the halo slots).  Grid: whole clusters, persistent (each takes sheets until
+// none is left).  B.loop[5] is the work counter (zeroed by the solve setup), B.loop[6] the
+// error word (set when a wait ran out).
 __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kernel(Batch B) {
     const DevParams P = *B.params;
     if (P.solver != CS_SOLVER_AUTO_DEV || B.n_resident == 0) return;  // uniform over the grid
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
     const int ncta = (int)cl.num_blocks();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int cap = B.res_cap;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int cap = B.res_cap, halo0 = B.res_halo0;
     const float* sm_panels = reinterpret_cast<const float*>(cs_res_smem);
-    float4* sm_p = reinterpret_cast<float4*>(cs_res_smem + (size_t)cap * CS_PANEL_FLOATS * sizeof(float));
-    __shared__ double red[RES_NBUF * CS_RES_MAX_CL * 2];
-    __shared__ double wsum[64];
-    __shared__ int sh_next;
-    __shared__ const float4* prank[CS_RES_MAX_CL];
-    if (threadIdx.x < ncta) prank[threadIdx.x] = cl.map_shared_rank(sm_p, (int)threadIdx.x);
-    int buf = 0;
-    const bool mixed = P.mixed != 0;
-    const bool fp32 = !mixed;
+    float4* su = reinterpret_cast<float4*>(cs_res_smem + (size_t)cap * CS_PANEL_FLOATS * sizeof(float));
+    __shared__ ResShared S;
+    if (tid == 0) {
+        rbar_init(saddr(&S.bar[0]), 1);
+        rbar_init(saddr(&S.bar[1]), 1);
+        rbar_init(saddr(&S.bar[2]), 1);
+        rbar_init(saddr(&S.bar[3]), (uint32_t)ncta);
+        rbar_init(saddr(&S.bar[4]), 1);
+        S.abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    cl.sync();  // every CTA's barriers exist before any remote arrive or st.async
+    const uint32_t hbar = saddr(&S.bar[0]), sbar = saddr(&S.bar[3]), ibar = saddr(&S.bar[4]);
+    uint32_t nhalo = 0, nred = 0, nres = 0, nitem = 0;
+    const bool mixed = P.mixed != 0, fp32 = !mixed;
     const int myslot = w * CS_SLICE + lane;
-    __syncthreads();
+    int* err = B.loop + 6;
 
     for (;;) {
-        if (rank == 0 && threadIdx.x == 0) {
-            const int idx = atomicAdd(&B.loop[5], 1);
-            for (int c = 0; c < ncta; c++) *cl.map_shared_rank(&sh_next, c) = idx;
+        // work item: rank 0 takes the next sheet and sends its index to every CTA
+        if (tid == 0) rbar_expect(ibar, 4u);
+        if (rank == 0 && tid == 0) {
+            const int nx = atomicAdd(&B.loop[5], 1);
+            for (int c = 0; c < ncta; c++) st_async_u32(mapa(saddr(&S.next), c), (uint32_t)nx, mapa(ibar, c));
         }
-        cl.sync();
-        const int idx = sh_next;
+        if (!res_wait(S, ibar, nitem & 1u)) {
+            res_abort(cl, S, ncta, err);
+            break;
+        }
+        nitem++;
+        const int idx = S.next;
         if (idx >= B.n_resident) break;
 
         const int s = B.rlist[idx];
         const SheetDesc sh = B.sheets[s];
-        const int* split = B.rsplit + sh.topo * (CS_RES_MAX_CL + 1);
-        const int lo = split[rank], hi = split[rank + 1];
+        const int tb = sh.topo * (CS_RES_MAX_CL + 1);
+        const int lo = B.rsplit[tb + rank], hi = B.rsplit[tb + rank + 1];
         int cta_p0 = 0, cta_p1 = 0;
         if (hi > lo) {
             cta_p0 = B.slices[sh.slice_off + lo].panel0;
@@ -149,7 +264,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
             const int ncopy = min(cta_p1 - cta_p0, cap) * (CS_PANEL_FLOATS / 4);
             const float4* src = reinterpret_cast<const float4*>(B.A + (size_t)cta_p0 * CS_PANEL_FLOATS);
             float4* dst = reinterpret_cast<float4*>(cs_res_smem);
-            for (int i = threadIdx.x; i < ncopy; i += blockDim.x) dst[i] = __ldg(src + i);
+            for (int i = tid; i < ncopy; i += blockDim.x) dst[i] = __ldg(src + i);
         }
         // this thread's row: slice lo + w, lane
         bool live = false;
@@ -165,10 +280,24 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
         }
         if (!live) width = 0;
         const bool in_smem = lp + width <= cap;
-        const float* panels = in_smem ? sm_panels + (size_t)lp * CS_PANEL_FLOATS : B.A + (size_t)gp * CS_PANEL_FLOATS;
         const int g = sh.node_off + row;
+        // u-array indices of the row's slots, packed 16-bit, for the whole solve
+        uint32_t cw[CS_RES_MAX_WIDTH / 2];
+#pragma unroll
+        for (int j = 0; j < CS_RES_MAX_WIDTH / 2; j++) {
+            uint32_t lo16 = 0, hi16 = 0;
+            if (2 * j < width) lo16 = (uint32_t)__ldg(&B.rcode[(tp + 2 * j) * CS_SLICE + lane]) & 0xfffu;
+            if (2 * j + 1 < width) hi16 = (uint32_t)__ldg(&B.rcode[(tp + 2 * j + 1) * CS_SLICE + lane]) & 0xfffu;
+            cw[j] = lo16 | (hi16 << 16);
+        }
+        // halo sends of this CTA (the first one per thread in a register) and bytes it receives
+        const int snd0 = B.rsendptr[tb + rank], snd1 = B.rsendptr[tb + rank + 1];
+        const uint32_t my_send = snd0 + tid < snd1 ? __ldg(&B.rsend[snd0 + tid]) : 0u;
+        const uint32_t halo_bytes = (uint32_t)B.rhalo[tb + rank] * 16u;
+
         float Pi[9];
-        float e[3] = {0.f, 0.f, 0.f}, r[3] = {0.f, 0.f, 0.f}, z[3] = {0.f, 0.f, 0.f};
+        float e[3] = {0.f, 0.f, 0.f}, r[3] = {0.f, 0.f, 0.f}, u[3], wv[3], p[3] = {0.f, 0.f, 0.f},
+              sv3[3] = {0.f, 0.f, 0.f};
         if (live) {
 #pragma unroll
             for (int k = 0; k < 9; k++) Pi[k] = B.Pinv[9 * (size_t)g + k];
@@ -179,10 +308,11 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
             for (int k = 0; k < 9; k++) Pi[k] = 0.f;
         }
         const double bn = sqrt(B.inst[s].bnorm2);
-        double rz = 0.0, rr = 0.0, pq = 0.0, res0 = bn, resnorm = -1.0, first_res = -1.0;
+        double gam = 0.0, rr = 0.0, delta = 0.0, alpha_d = 0.0, res0 = bn, resnorm = -1.0, first_res = -1.0;
         float alpha = 0.f, beta = 0.f;
         int iters = 0, sweeps = 0, sweep_iters = 0, flags = 0, trips = 0;
         int phase = P.warm ? PH_RES : PH_INIT;
+        bool ok = true;
 
         while (phase != PH_FINISH) {
             if (++trips > P.loop_cap) {
@@ -190,7 +320,8 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                 break;
             }
             if (phase == PH_RES) {
-                // fold the FP32 correction into the FP64 solution, then r = b - A dv64 in FP64
+                // fold the FP32 correction into the FP64 solution; every CTA signals that its
+                // rows are written; then r = b - A dv64 in FP64 over global dv64
                 if (live) {
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
@@ -198,17 +329,26 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                         e[c] = 0.f;
                     }
                 }
-                cl.sync();
-                double v[1] = {0.0};
+                __syncthreads();
+                if (tid == 0) {
+                    asm volatile("fence.acq_rel.cluster;" ::: "memory");
+                    for (int c = 0; c < ncta; c++) rbar_arrive_remote(mapa(sbar, c));
+                }
+                ok = res_wait(S, sbar, nres & 1u);
+                nres++;
+                if (!ok) break;
+                double v[3] = {0.0, 0.0, 0.0};
                 if (live) {
+                    const float* pn = in_smem ? sm_panels + (size_t)lp * CS_PANEL_FLOATS : B.A + (size_t)gp * CS_PANEL_FLOATS;
                     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
                     for (int k = 0; k < width; k++) {
                         const int col = __ldg(&B.tcol[(tp + k) * CS_SLICE + lane]) + sh.node_off;
-                        const float* pn = panels + (size_t)k * CS_PANEL_FLOATS;
-                        const float4 a0 = reinterpret_cast<const float4*>(pn)[lane];
-                        const float4 a1 = reinterpret_cast<const float4*>(pn + 128)[lane];
-                        const float a8 = pn[256 + lane];
-                        const double d0 = B.dv64[3 * col], d1 = B.dv64[3 * col + 1], d2 = B.dv64[3 * col + 2];
+                        const float* pk = pn + (size_t)k * CS_PANEL_FLOATS;
+                        const float4 a0 = reinterpret_cast<const float4*>(pk)[lane];
+                        const float4 a1 = reinterpret_cast<const float4*>(pk + 128)[lane];
+                        const float a8 = pk[256 + lane];
+                        const double d0 = __ldcg(&B.dv64[3 * col]), d1 = __ldcg(&B.dv64[3 * col + 1]),
+                                     d2 = __ldcg(&B.dv64[3 * col + 2]);
                         y0 += (double)a0.x * d0 + (double)a0.y * d1 + (double)a0.z * d2;
                         y1 += (double)a0.w * d0 + (double)a1.x * d1 + (double)a1.y * d2;
                         y2 += (double)a1.z * d0 + (double)a1.w * d1 + (double)a8 * d2;
@@ -220,7 +360,8 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     r[2] = (float)r2;
                     v[0] = r0 * r0 + r1 * r1 + r2 * r2;
                 }
-                cluster_sum<1>(cl, rank, ncta, red, wsum, buf, v, false);
+                ok = cluster_sum3(S, rank, ncta, nred, v, false);
+                if (!ok) break;
                 const double res = sqrt(v[0]);
                 resnorm = res;
                 sweeps += 1;
@@ -240,7 +381,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                 } else if (iters >= P.max_iters) {
                     flags |= CS_IF_CAPPED;
                     phase = PH_FINISH;
-                } else if (mixed || rz == 0.0) {
+                } else if (mixed || gam == 0.0) {
                     res0 = res;
                     phase = PH_INIT;
                 } else {
@@ -248,117 +389,141 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     flags |= CS_IF_CAPPED;
                     phase = PH_FINISH;
                 }
-            } else if (phase == PH_INIT) {
-                if ((flags & CS_IF_WARM_REJECTED) && sweeps == 1 && live) {
+                continue;
+            }
+            // PH_INIT (start of a sweep) or PH_CG: u = P^-1 r, halo exchange, w = A u, and
+            // one reduction of (r.u, w.u, r.r)
+            if (phase == PH_INIT && (flags & CS_IF_WARM_REJECTED) && sweeps == 1 && live) {
 #pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        B.dv64[3 * g + c] = 0.0;
-                        r[c] = B.b[3 * g + c];
-                    }
+                for (int c = 0; c < 3; c++) {
+                    B.dv64[3 * g + c] = 0.0;
+                    r[c] = B.b[3 * g + c];
                 }
-                z[0] = Pi[0] * r[0] + Pi[1] * r[1] + Pi[2] * r[2];
-                z[1] = Pi[3] * r[0] + Pi[4] * r[1] + Pi[5] * r[2];
-                z[2] = Pi[6] * r[0] + Pi[7] * r[1] + Pi[8] * r[2];
-                double v[2];
+            }
+            if (phase == PH_CG) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    e[c] = __fmaf_rn(alpha, p[c], e[c]);
+                    r[c] = __fmaf_rn(-alpha, sv3[c], r[c]);
+                }
+            }
+            u[0] = Pi[0] * r[0] + Pi[1] * r[1] + Pi[2] * r[2];
+            u[1] = Pi[3] * r[0] + Pi[4] * r[1] + Pi[5] * r[2];
+            u[2] = Pi[6] * r[0] + Pi[7] * r[1] + Pi[8] * r[2];
+            if (live) su[myslot] = make_float4(u[0], u[1], u[2], 0.f);
+            __syncthreads();
+            if (tid == 0) rbar_expect(hbar, halo_bytes);
+            for (int i = snd0 + tid; i < snd1; i += blockDim.x) {
+                const uint32_t m = i == snd0 + tid ? my_send : __ldg(&B.rsend[i]);
+                const int d = (int)((m >> 12) & 0xfu);
+                st_async_f4(mapa(saddr(&su[halo0 + (int)(m >> 16)]), d), su[m & 0xfffu], mapa(hbar, d));
+            }
+            ok = res_wait(S, hbar, nhalo & 1u);
+            nhalo++;
+            if (!ok) break;
+            wv[0] = wv[1] = wv[2] = 0.f;
+            if (in_smem)
+                row_times_u(sm_panels + (size_t)lp * CS_PANEL_FLOATS, width, cw, su, lane, wv[0], wv[1], wv[2]);
+            else
+                row_times_u(B.A + (size_t)gp * CS_PANEL_FLOATS, width, cw, su, lane, wv[0], wv[1], wv[2]);
+            double v[3] = {0.0, 0.0, 0.0};
+            if (live) {
                 if (mixed) {
-                    v[0] = (double)r[0] * z[0] + (double)r[1] * z[1] + (double)r[2] * z[2];
-                    v[1] = (double)r[0] * r[0] + (double)r[1] * r[1] + (double)r[2] * r[2];
+                    v[0] = (double)r[0] * u[0] + (double)r[1] * u[1] + (double)r[2] * u[2];
+                    v[1] = (double)wv[0] * u[0] + (double)wv[1] * u[1] + (double)wv[2] * u[2];
+                    v[2] = (double)r[0] * r[0] + (double)r[1] * r[1] + (double)r[2] * r[2];
                 } else {
-                    v[0] = (double)(r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
-                    v[1] = (double)(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                    v[0] = (double)(r[0] * u[0] + r[1] * u[1] + r[2] * u[2]);
+                    v[1] = (double)(wv[0] * u[0] + wv[1] * u[1] + wv[2] * u[2]);
+                    v[2] = (double)(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
                 }
-                cluster_sum<2>(cl, rank, ncta, red, wsum, buf, v, fp32);
-                rz = v[0];
-                rr = v[1];
-                beta = 0.f;
+            }
+            ok = cluster_sum3(S, rank, ncta, nred, v, fp32);
+            if (!ok) break;
+            const double gnew = v[0], dnew = v[1];
+            rr = v[2];
+            if (phase == PH_INIT) {
+                gam = gnew;
+                delta = dnew;
                 sweep_iters = 0;
-                phase = (rz > 0.0 && rfinite(rz)) ? PH_CG : PH_RES;
-            } else {
-                // PH_CG: p = z + beta p, q = A p, alpha, e += alpha p, r -= alpha q, z = P^-1 r, beta
-                float p[3] = {z[0], z[1], z[2]};
-                if (beta != 0.f) {
-                    const float4 po = sm_p[myslot];
-                    p[0] = __fmaf_rn(beta, po.x, p[0]);
-                    p[1] = __fmaf_rn(beta, po.y, p[1]);
-                    p[2] = __fmaf_rn(beta, po.z, p[2]);
+                beta = 0.f;
+                if (!(gam > 0.0 && rfinite(gam))) {
+                    phase = PH_RES;
+                    continue;
                 }
-                if (live) sm_p[myslot] = make_float4(p[0], p[1], p[2], 0.f);
-                cl.sync();
-                float q0 = 0.f, q1 = 0.f, q2 = 0.f;
-                for (int k = 0; k < width; k++) {
-                    const uint32_t code = __ldg(reinterpret_cast<const uint32_t*>(B.rcode) + (tp + k) * CS_SLICE + lane);
-                    const float* pn = panels + (size_t)k * CS_PANEL_FLOATS;
-                    const float4 a0 = reinterpret_cast<const float4*>(pn)[lane];
-                    const float4 a1 = reinterpret_cast<const float4*>(pn + 128)[lane];
-                    const float a8 = pn[256 + lane];
-                    const int ork = (int)(code >> 16), osl = (int)(code & 0xffffu);
-                    const float4 pv = (ork == rank) ? sm_p[osl] : prank[ork][osl];
-                    q0 += a0.x * pv.x + a0.y * pv.y + a0.z * pv.z;
-                    q1 += a0.w * pv.x + a1.x * pv.y + a1.y * pv.z;
-                    q2 += a1.z * pv.x + a1.w * pv.y + a8 * pv.z;
-                }
-                double v1[1];
-                if (mixed)
-                    v1[0] = (double)p[0] * q0 + (double)p[1] * q1 + (double)p[2] * q2;
-                else
-                    v1[0] = (double)(p[0] * q0 + p[1] * q1 + p[2] * q2);
-                if (!live) v1[0] = 0.0;
-                cluster_sum<1>(cl, rank, ncta, red, wsum, buf, v1, fp32);
-                const double sum = v1[0];
-                alpha = mixed ? (float)(rz / sum) : (float)rz / (float)sum;
-                if (!(sum > 0.0) || !rfinite((double)alpha)) {
-                    alpha = 0.f;
-                    flags |= CS_IF_BREAKDOWN;
-                }
-                pq = sum;
-                e[0] = __fmaf_rn(alpha, p[0], e[0]);
-                e[1] = __fmaf_rn(alpha, p[1], e[1]);
-                e[2] = __fmaf_rn(alpha, p[2], e[2]);
-                r[0] = __fmaf_rn(-alpha, q0, r[0]);
-                r[1] = __fmaf_rn(-alpha, q1, r[1]);
-                r[2] = __fmaf_rn(-alpha, q2, r[2]);
-                z[0] = Pi[0] * r[0] + Pi[1] * r[1] + Pi[2] * r[2];
-                z[1] = Pi[3] * r[0] + Pi[4] * r[1] + Pi[5] * r[2];
-                z[2] = Pi[6] * r[0] + Pi[7] * r[1] + Pi[8] * r[2];
-                double v[2];
                 if (mixed) {
-                    v[0] = (double)r[0] * z[0] + (double)r[1] * z[1] + (double)r[2] * z[2];
-                    v[1] = (double)r[0] * r[0] + (double)r[1] * r[1] + (double)r[2] * r[2];
+                    alpha_d = gam / delta;
+                    alpha = (float)alpha_d;
                 } else {
-                    v[0] = (double)(r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
-                    v[1] = (double)(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                    alpha = (float)gam / (float)delta;
+                    alpha_d = (double)alpha;
                 }
-                if (!live) v[0] = v[1] = 0.0;
-                cluster_sum<2>(cl, rank, ncta, red, wsum, buf, v, fp32);
-                float nb = mixed ? (float)(v[0] / rz) : (float)v[0] / (float)rz;
-                rz = v[0];
-                rr = v[1];
-                iters += 1;
-                sweep_iters += 1;
-                const double rn = sqrt(rr);
-                bool stop;
-                if (mixed)
-                    stop = rn <= P.inner_tol * res0 || rn <= 0.5 * P.tol * bn || sweep_iters >= P.sweep_cap;
-                else
-                    stop = rn <= P.tol * bn;
-                if (!rfinite((double)nb) || !(rz > 0.0) || (flags & CS_IF_BREAKDOWN)) {
-                    nb = 0.f;
-                    stop = true;
+                if (!(delta > 0.0) || !rfinite((double)alpha)) {
                     flags |= CS_IF_BREAKDOWN;
+                    phase = PH_RES;
+                    continue;
                 }
-                beta = nb;
-                if (stop || iters >= P.max_iters) phase = PH_RES;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    p[c] = u[c];
+                    sv3[c] = wv[c];
+                }
+                phase = PH_CG;
+                continue;
+            }
+            // PH_CG: the iteration's x and r updates are done; stopping test on ||r||
+            iters += 1;
+            sweep_iters += 1;
+            const double rn = sqrt(rr);
+            bool stop;
+            if (mixed)
+                stop = rn <= P.inner_tol * res0 || rn <= 0.5 * P.tol * bn || sweep_iters >= P.sweep_cap;
+            else
+                stop = rn <= P.tol * bn;
+            float nb, na;
+            double na_d;
+            if (mixed) {
+                const double bd = gnew / gam;
+                na_d = gnew / (dnew - bd * gnew / alpha_d);
+                nb = (float)bd;
+                na = (float)na_d;
+            } else {
+                nb = (float)gnew / (float)gam;
+                na = (float)gnew / ((float)dnew - nb * (float)gnew / alpha);
+                na_d = (double)na;
+            }
+            if (!rfinite((double)nb) || !rfinite((double)na) || !(gnew > 0.0) || !(na > 0.f)) {
+                flags |= CS_IF_BREAKDOWN;
+                stop = true;
+            }
+            gam = gnew;
+            delta = dnew;
+            if (stop || iters >= P.max_iters) {
+                phase = PH_RES;
+                continue;
+            }
+            beta = nb;
+            alpha = na;
+            alpha_d = na_d;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                p[c] = __fmaf_rn(beta, p[c], u[c]);
+                sv3[c] = __fmaf_rn(beta, sv3[c], wv[c]);
             }
         }
-        if (live && trips > P.loop_cap) {
+        if (!ok) {
+            res_abort(cl, S, ncta, err);
+            flags |= CS_IF_BREAKDOWN;
+        }
+        if (live && (!ok || trips > P.loop_cap)) {
 #pragma unroll
             for (int c = 0; c < 3; c++) B.dv64[3 * g + c] += (double)e[c];
         }
-        if (rank == 0 && threadIdx.x == 0) {
+        if (rank == 0 && tid == 0) {
             InstState& I = B.inst[s];
-            I.rz = rz;
+            I.rz = gam;
             I.rr = rr;
-            I.pq = pq;
+            I.pq = delta;
             I.res0 = res0;
             I.resnorm = resnorm;
             I.first_res = first_res;
@@ -370,6 +535,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
             I.flags = flags;
             I.phase = PH_DONE;
         }
-        cl.sync();  // shared data of this sheet no longer read by any CTA
+        if (!ok) break;
     }
+    cl.sync();  // no CTA leaves while another may still address its shared memory
 }
