@@ -19,9 +19,10 @@
 //     partials travel the same way.  A CTA waits only on its own mbarriers.  Sends for step
 //     k+1 depend on every CTA's step-k partial, so one halo buffer and two reduction buffers
 //     suffice (a sender is never two steps ahead of a receiver);
-//   * sums deterministically: butterflies within warps, over warp partials, over CTA
-//     partials (IEEE addition is commutative, so every lane of a butterfly ends with the same
-//     bits), every CTA summing the same partials: all CTAs take identical decisions.
+//   * sums deterministically: a butterfly within each warp (IEEE addition is commutative, so
+//     every lane ends with the same bits), then warp and CTA partials in a fixed order, every
+//     CTA summing the same partials: all CTAs take identical decisions;
+//   * runs the SpMV's local slots while the halo values travel, the halo slots after.
 // Every wait is bounded.  A CTA whose wait runs out raises an abort flag in all CTAs and an
 // error word for the host, and all CTAs leave through the kernel's final cluster barrier (the
 // only one after start-up), so no CTA exits while another may still address its memory.
@@ -38,7 +39,7 @@ namespace cg = cooperative_groups;
 
 namespace {
 
-constexpr uint32_t RES_WAIT_TRIES = 1u << 20;
+constexpr uint32_t RES_WAIT_TRIES = 1u << 24;  // polls of a phase before a CTA gives up (well over 0.1 s)
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -56,15 +57,29 @@ __device__ __forceinline__ void rbar_expect(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-__device__ __forceinline__ bool rbar_try(uint32_t bar, uint32_t parity) {
+// Non-blocking test of a phase (test_wait, not try_wait: try_wait may suspend the thread for
+// a system-defined time).  CLUSTER = false: acquire at CTA scope, enough for data that
+// st.async wrote into this CTA's shared memory with completion on this mbarrier; true:
+// cluster scope, for the residual signal that orders other CTAs' global-memory writes.
+template <bool CLUSTER>
+__device__ __forceinline__ bool rbar_test(uint32_t bar, uint32_t parity) {
     uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
+    if (CLUSTER)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
     return ok != 0;
 }
 
@@ -116,10 +131,11 @@ struct __align__(16) ResShared {
 // Waits for `parity` of `bar` on every thread, at most RES_WAIT_TRIES polls, giving up early
 // once another CTA raised the abort flag.  Returns true on every thread only if the whole
 // CTA saw the phase complete.
+template <bool CLUSTER = false>
 __device__ __forceinline__ bool res_wait(ResShared& S, uint32_t bar, uint32_t parity) {
     bool ok = false;
     for (uint32_t t = 0; t < RES_WAIT_TRIES; t++) {
-        if (rbar_try(bar, parity)) {
+        if (rbar_test<CLUSTER>(bar, parity)) {
             ok = true;
             break;
         }
@@ -137,8 +153,13 @@ __device__ __forceinline__ void res_abort(const cg::cluster_group& cl, ResShared
 }
 
 // Cluster-wide sum of three values (fp32: in float, the plain FP32 solver; else double).
-// Partials travel by st.async into buffer `nred & 1` of every CTA.  Returns false if the
-// wait gave up (the caller aborts).
+// Order: a butterfly within each warp, then the warp partials in warp order, then the CTA
+// partials in rank order.  The last two are serial sums over broadcast shared-memory reads,
+// done redundantly by every thread that needs the result (no shuffles: with ~20 warps per SM
+// the shuffle pipe is the bottleneck of a butterfly).  Every CTA sums the same partials in
+// the same order, so all threads of the cluster return identical sums.  Partials travel by
+// st.async into buffer `nred & 1` of every CTA.  Returns false if the wait gave up (the
+// caller aborts).
 __device__ __forceinline__ bool cluster_sum3(ResShared& S, int rank, int ncta, uint32_t& nred, double (&v)[3], bool fp32) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int b = (int)(nred & 1u);
@@ -149,43 +170,57 @@ __device__ __forceinline__ bool cluster_sum3(ResShared& S, int rank, int ncta, u
         for (int i = 0; i < 3; i++) S.wsum[w][i] = v[i];
     }
     __syncthreads();
-    if (w == 0) {
+    if (w == 0 && lane < ncta) {
         double t[3];
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            const double x = lane < nw ? S.wsum[lane][i] : 0.0;
-            t[i] = fp32 ? (double)rwarp_sum((float)x) : rwarp_sum(x);
+            if (fp32) {
+                float a = 0.f;
+                for (int j = 0; j < nw; j++) a += (float)S.wsum[j][i];
+                t[i] = (double)a;
+            } else {
+                double a = 0.0;
+                for (int j = 0; j < nw; j++) a += S.wsum[j][i];
+                t[i] = a;
+            }
         }
         const uint32_t bar = saddr(&S.bar[1 + b]);
         if (lane == 0) rbar_expect(bar, (uint32_t)ncta * 32u);
-        __syncwarp();
-        if (lane < ncta) {
-            const uint32_t dst = mapa(saddr(&S.red[b][rank][0]), lane);
-            const uint32_t dbar = mapa(bar, lane);
-            st_async_d2(dst, t[0], t[1], dbar);
-            st_async_d2(dst + 16, t[2], 0.0, dbar);
-        }
+        const uint32_t dst = mapa(saddr(&S.red[b][rank][0]), lane);
+        const uint32_t dbar = mapa(bar, lane);
+        st_async_d2(dst, t[0], t[1], dbar);
+        st_async_d2(dst + 16, t[2], 0.0, dbar);
     }
     const bool ok = res_wait(S, saddr(&S.bar[1 + b]), (nred >> 1) & 1u);
     nred++;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        const double x = lane < ncta ? S.red[b][lane][i] : 0.0;
-        v[i] = fp32 ? (double)rwarp_sum((float)x) : rwarp_sum(x);
+        if (fp32) {
+            float a = 0.f;
+            for (int c = 0; c < ncta; c++) a += (float)S.red[b][c][i];
+            v[i] = (double)a;
+        } else {
+            double a = 0.0;
+            for (int c = 0; c < ncta; c++) a += S.red[b][c][i];
+            v[i] = a;
+        }
     }
     return ok;
 }
 
-// w = (row of A) u over a row's block slots, fully unrolled so that every slot's panel and u
-// loads are in flight together.  `cw` holds the slots' indices into this CTA's u array (own
-// rows, then halo copies of other CTAs' rows), two 16-bit indices per word.  `pn` points at
-// the row's first panel, in shared memory or (beyond the shared-memory budget) global memory.
+// w += (row of A) u over the row's block slots whose u entry is local (HALO = false: own
+// rows) or a halo copy (HALO = true), fully unrolled so that every slot's panel and u loads
+// are in flight together.  The local pass runs while the halo values travel.  `cw` holds the
+// slots' indices into this CTA's u array (own rows below `halo0`, then the halo slots), two
+// 16-bit indices per word.  `pn` points at the row's first panel, in shared memory or
+// (beyond the shared-memory budget) in global memory.
+template <bool HALO>
 __device__ __forceinline__ void row_times_u(const float* __restrict__ pn, int width, const uint32_t (&cw)[CS_RES_MAX_WIDTH / 2],
-                                            const float4* su, int lane, float& q0, float& q1, float& q2) {
+                                            const float4* su, int halo0, int lane, float& q0, float& q1, float& q2) {
 #pragma unroll
     for (int k = 0; k < CS_RES_MAX_WIDTH; k++) {
-        if (k < width) {
-            const int idx = (int)((cw[k >> 1] >> ((k & 1) * 16)) & 0xffffu);
+        const int idx = (int)((cw[k >> 1] >> ((k & 1) * 16)) & 0xffffu);
+        if (k < width && (idx >= halo0) == HALO) {
             const float* pk = pn + k * CS_PANEL_FLOATS;
             const float4 a0 = reinterpret_cast<const float4*>(pk)[lane];
             const float4 a1 = reinterpret_cast<const float4*>(pk + 128)[lane];
@@ -334,7 +369,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     asm volatile("fence.acq_rel.cluster;" ::: "memory");
                     for (int c = 0; c < ncta; c++) rbar_arrive_remote(mapa(sbar, c));
                 }
-                ok = res_wait(S, sbar, nres & 1u);
+                ok = res_wait<true>(S, sbar, nres & 1u);
                 nres++;
                 if (!ok) break;
                 double v[3] = {0.0, 0.0, 0.0};
@@ -418,14 +453,19 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                 const int d = (int)((m >> 12) & 0xfu);
                 st_async_f4(mapa(saddr(&su[halo0 + (int)(m >> 16)]), d), su[m & 0xfffu], mapa(hbar, d));
             }
+            wv[0] = wv[1] = wv[2] = 0.f;
+            const float* pn = in_smem ? sm_panels + (size_t)lp * CS_PANEL_FLOATS : B.A + (size_t)gp * CS_PANEL_FLOATS;
+            if (in_smem)
+                row_times_u<false>(sm_panels + (size_t)lp * CS_PANEL_FLOATS, width, cw, su, halo0, lane, wv[0], wv[1], wv[2]);
+            else
+                row_times_u<false>(pn, width, cw, su, halo0, lane, wv[0], wv[1], wv[2]);
             ok = res_wait(S, hbar, nhalo & 1u);
             nhalo++;
             if (!ok) break;
-            wv[0] = wv[1] = wv[2] = 0.f;
             if (in_smem)
-                row_times_u(sm_panels + (size_t)lp * CS_PANEL_FLOATS, width, cw, su, lane, wv[0], wv[1], wv[2]);
+                row_times_u<true>(sm_panels + (size_t)lp * CS_PANEL_FLOATS, width, cw, su, halo0, lane, wv[0], wv[1], wv[2]);
             else
-                row_times_u(B.A + (size_t)gp * CS_PANEL_FLOATS, width, cw, su, lane, wv[0], wv[1], wv[2]);
+                row_times_u<true>(pn, width, cw, su, halo0, lane, wv[0], wv[1], wv[2]);
             double v[3] = {0.0, 0.0, 0.0};
             if (live) {
                 if (mixed) {
