@@ -1,0 +1,166 @@
+"""Accuracy of one implicit step at every benchmark configuration, against an FP64 oracle
+solve of the same assembled FP32 system (the CPU oracle's LL^T in double, or its FP64
+block-Jacobi PCG to 1e-12 where the direct factorisation is too large).
+
+Reported per configuration (printed; written as JSON to $CS_REPORT_DIR/config_errors.json
+when that variable is set):
+  * dv error  = ||dv_gpu - dv_oracle|| / ||dv_oracle||,
+  * x error   = ||x_gpu - x_oracle|| / ||x_oracle - x_0|| after the step (relative to the
+                step's displacement, the part of x the solve determines),
+for the mixed-precision solver at the benchmark's FP64-checked 1e-6 and at 1e-10, and for
+the plain FP32 solver at 1e-6 where the configuration asks for it (config 2).
+
+Bounds asserted: every solve reaches its FP64-checked tolerance (plain FP32 excepted), and
+at 1e-10 the dv error is below 1e-6 (north-star bound for the mixed solver).  At 1e-6 the dv
+error is bounded by the system's conditioning, not by the kernels; it is reported, with a
+loose sanity bound of 1e-2.
+
+Configurations at full size on the GPU; the oracle runs on every sheet of configs 1 and 2,
+on a seeded subset of the sheets of configs 3 and 4 (the batch is too large for a
+single-threaded oracle in a test), and for config 5 (1,002,001 nodes) on the same scene at
+250 x 250 quads, with the full-size step checked through its FP64 residual recomputed on
+the host from the assembled system.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+pytestmark = pytest.mark.gpu
+
+import pyoracle
+from clothsimulator_b200 import native, scenes
+
+REPORT = {}
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64).reshape(-1)
+    b = np.asarray(b, np.float64).reshape(-1)
+    den = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))
+
+
+def oracle_dv(scene, sheet, method=pyoracle.METHOD_LLT64):
+    c = pyoracle.Cloth(sheet, pyoracle.Material(sheet["material"], "float"))
+    c.assemble(scenes.step_params(scene, sheet))
+    if method == pyoracle.METHOD_PCG64:
+        dv, rr = c.solve(method, tol=1e-12, max_iter=200000)
+        assert rr <= 1e-12
+    else:
+        dv, _ = c.solve(method)
+    return dv
+
+
+def gpu_step(ctx, scene, **kw):
+    """One full step from the scene's initial state; returns per-sheet dv, x, and stats."""
+    x0 = np.concatenate([s["x"] for s in scene.sheets])
+    v0 = np.concatenate([s["v"] for s in scene.sheets])
+    ctx.set_state(x0, v0)
+    p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, max_iters=20000, **kw)
+    stats, code = ctx.step(p, allow_unconverged=kw.get("precision") == native.PREC_PLAIN_FP32)
+    dv = ctx.get_dv().reshape(-1, 3)
+    x, _ = ctx.get_state()
+    out, o = [], 0
+    for s in scene.sheets:
+        n = s["x"].shape[0]
+        out.append((dv[o:o + n].reshape(-1), x[o:o + n].reshape(-1)))
+        o += n
+    return out, stats
+
+
+def sheet_errors(scene, sheet, dv_gpu, x_gpu, dv_or):
+    x0 = sheet["x"].astype(np.float64).reshape(-1)
+    v0 = sheet["v"].astype(np.float64).reshape(-1)
+    x_or = x0 + scene.dt * (v0 + dv_or)
+    return rel(dv_gpu, dv_or), rel(x_gpu - x0, x_or - x0)
+
+
+def record(name, key, errs):
+    d = REPORT.setdefault(name, {})
+    dv = [e[0] for e in errs]
+    xx = [e[1] for e in errs]
+    d[key] = {"dv_err_max": max(dv), "dv_err_mean": float(np.mean(dv)), "x_err_max": max(xx), "sheets": len(errs)}
+    print(f"{name} {key}: dv err max {max(dv):.3e} mean {np.mean(dv):.3e}; x err max {max(xx):.3e} ({len(errs)} sheets)")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def write_report():
+    yield
+    out = os.environ.get("CS_REPORT_DIR")
+    if out and REPORT:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, "config_errors.json"), "w") as f:
+            json.dump(REPORT, f, indent=1)
+
+
+def check_subset(name, scene, ctx, subset, tols=(1e-6, 1e-10)):
+    oracle = {k: oracle_dv(scene, scene.sheets[k]) for k in subset}
+    for tol in tols:
+        res, stats = gpu_step(ctx, scene, tol=tol, precision=native.PREC_MIXED)
+        assert stats.converged == len(scene.sheets) and stats.max_rel_residual <= tol
+        errs = [sheet_errors(scene, scene.sheets[k], res[k][0], res[k][1], oracle[k]) for k in subset]
+        record(name, f"mixed_tol{tol:g}", errs)
+        assert max(e[0] for e in errs) < (1e-6 if tol <= 1e-10 else 1e-2)
+
+
+def test_config1_hang32(ctx_factory):
+    scene = scenes.hang(32, seed=0)
+    check_subset("config1_hang32", scene, ctx_factory(scene.sheets), [0])
+
+
+def test_config2_precision_study(ctx_factory):
+    scene = scenes.precision_sheet(256, seed=0)
+    sheet = scene.sheets[0]
+    ctx = ctx_factory(scene.sheets)
+    dv_or = oracle_dv(scene, sheet, pyoracle.METHOD_PCG64)  # FP64 oracle to 1e-12
+    for key, kw in [("plain_fp32_tol1e-06", dict(tol=1e-6, precision=native.PREC_PLAIN_FP32)),
+                    ("mixed_tol1e-06", dict(tol=1e-6, precision=native.PREC_MIXED)),
+                    ("mixed_tol1e-10", dict(tol=1e-10, precision=native.PREC_MIXED))]:
+        res, stats = gpu_step(ctx, scene, **kw)
+        e = sheet_errors(scene, sheet, res[0][0], res[0][1], dv_or)
+        record("config2_precision256", key, [e])
+        REPORT["config2_precision256"][key]["rel_residual"] = stats.max_rel_residual
+        if kw["precision"] == native.PREC_MIXED:
+            assert stats.converged == 1
+        if kw["tol"] <= 1e-10:
+            assert e[0] < 1e-6
+
+
+def test_config3_uneven512(ctx_factory):
+    scene = scenes.uneven_batch(512, seed=0)
+    rng = np.random.default_rng(3)
+    subset = sorted(rng.choice(len(scene.sheets), 12, replace=False).tolist())
+    check_subset("config3_uneven512", scene, ctx_factory(scene.sheets), subset)
+
+
+def test_config4_windy1024(ctx_factory):
+    scene = scenes.windy_batch(1024, 64, seed=1000)
+    rng = np.random.default_rng(4)
+    subset = sorted(rng.choice(len(scene.sheets), 8, replace=False).tolist())
+    check_subset("config4_windy1024x64", scene, ctx_factory(scene.sheets), subset)
+
+
+def test_config5_irregular(ctx_factory):
+    # the same scene at 250 x 250 quads against the FP64 oracle
+    small = scenes.large_irregular(250, seed=0)
+    check_subset("config5_irregular250", small, ctx_factory(small.sheets), [0])
+    # full size: the FP64 residual of the returned dv, recomputed on the host
+    scene = scenes.large_irregular(1000, seed=0)
+    ctx = ctx_factory(scene.sheets)
+    res, stats = gpu_step(ctx, scene, tol=1e-6, precision=native.PREC_MIXED, advance=0)
+    assert stats.converged == 1 and stats.max_rel_residual <= 1e-6
+    ctx.assemble(native.step_params(scene.dt, scene.gravity, scene.handle_stiffness))
+    rp, ci, val, b = ctx.system()
+    n = len(rp) - 1
+    A = sp.bsr_matrix((val.astype(np.float64), ci, rp), shape=(3 * n, 3 * n)).tocsr()
+    r = b.astype(np.float64) - A @ res[0][0].astype(np.float64)
+    host_rel = float(np.linalg.norm(r) / np.linalg.norm(b.astype(np.float64)))
+    REPORT.setdefault("config5_irregular1000", {})["mixed_tol1e-06"] = {
+        "gpu_fp64_rel_residual": stats.max_rel_residual, "host_fp64_rel_residual_of_fp32_dv": host_rel,
+        "iters": stats.max_iters}
+    print(f"config5 full size: GPU FP64 residual {stats.max_rel_residual:.3e}, host residual of the FP32 dv {host_rel:.3e}")
+    # dv is returned rounded to FP32; its residual may exceed the FP64 one by that rounding only
+    assert host_rel < 1e-5
