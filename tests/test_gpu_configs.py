@@ -156,11 +156,15 @@ def test_config5_irregular(ctx_factory):
     rp, ci, val, b = ctx.system()
     n = len(rp) - 1
     A = sp.bsr_matrix((val.astype(np.float64), ci, rp), shape=(3 * n, 3 * n)).tocsr()
-    r = b.astype(np.float64) - A @ res[0][0].astype(np.float64)
-    host_rel = float(np.linalg.norm(r) / np.linalg.norm(b.astype(np.float64)))
+    dv = res[0][0].astype(np.float64)
+    bn = np.linalg.norm(b.astype(np.float64))
+    host_rel = float(np.linalg.norm(b.astype(np.float64) - A @ dv) / bn)
+    # dv is returned rounded to FP32 (relative error <= 2^-24 per entry); that rounding moves
+    # the residual by at most || |A| |dv| || 2^-24 / ||b||
+    rounding = float(np.linalg.norm(abs(A) @ np.abs(dv)) * 2.0 ** -24 / bn)
     REPORT.setdefault("config5_irregular1000", {})["mixed_tol1e-06"] = {
         "gpu_fp64_rel_residual": stats.max_rel_residual, "host_fp64_rel_residual_of_fp32_dv": host_rel,
-        "iters": stats.max_iters}
-    print(f"config5 full size: GPU FP64 residual {stats.max_rel_residual:.3e}, host residual of the FP32 dv {host_rel:.3e}")
-    # dv is returned rounded to FP32; its residual may exceed the FP64 one by that rounding only
-    assert host_rel < 1e-5
+        "fp32_rounding_bound": rounding, "iters": stats.max_iters}
+    print(f"config5 full size: GPU FP64 residual {stats.max_rel_residual:.3e}, host residual of the FP32 dv "
+          f"{host_rel:.3e} (rounding bound {rounding:.3e}), {stats.max_iters} iterations")
+    assert host_rel <= stats.max_rel_residual + rounding
