@@ -39,7 +39,10 @@ namespace cg = cooperative_groups;
 
 namespace {
 
-constexpr uint32_t RES_WAIT_TRIES = 1u << 24;  // polls of a phase before a CTA gives up (well over 0.1 s)
+constexpr uint32_t RES_WAIT_TRIES = 1u << 22;  // polls of a phase before a CTA gives up (about 0.1 s)
+#ifndef RES_POLL_NS
+#define RES_POLL_NS 32
+#endif
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -140,6 +143,8 @@ __device__ __forceinline__ bool res_wait(ResShared& S, uint32_t bar, uint32_t pa
             break;
         }
         if (*(volatile int*)&S.abort_flag) break;
+        // back off: polls share the shared-memory pipe with the remote stores being awaited
+        __nanosleep(RES_POLL_NS);
     }
     return __syncthreads_and(ok ? 1 : 0) != 0;
 }
