@@ -540,6 +540,7 @@ struct cs_ctx {
     MlpDev mlp;
     bool mlpInit = false;
     int mlpGridTile = 0, mlpGridTrain = 0;
+    int mlpGridL1 = 0, mlpGridL23 = 0;  // inference grids: resident CTAs per SM (TMEM: 512 columns per SM)
     long long adamStep = 0;
     float* mlpScratch = nullptr;  // per-epoch loss accumulators, gradient output
     cudaGraphExec_t graphExecLearned = nullptr;
@@ -648,8 +649,8 @@ int launchMlpInference(cs_ctx* c, float* pred) {
     Batch& B = c->B;
     MlpDev& M = c->mlp;
     cs_mlp_features_kernel<<<nblk(B.N, 256), 256, 0, c->stream>>>(B, M, M.feat);
-    cs_mlp_l1_kernel<<<c->mlpGridTile, 128, MLP_SMEM_L1, c->stream>>>(B, M, M.feat, 0, B.N, nullptr);
-    cs_mlp_l23_kernel<<<c->mlpGridTile, 128, MLP_SMEM_L23, c->stream>>>(B, M, 0, B.N, nullptr, nullptr, nullptr, pred);
+    cs_mlp_l1_kernel<<<c->mlpGridL1, 128, MLP_SMEM_L1, c->stream>>>(B, M, M.feat, 0, B.N, nullptr);
+    cs_mlp_l23_kernel<<<c->mlpGridL23, 128, MLP_SMEM_L23, c->stream>>>(B, M, 0, B.N, nullptr, nullptr, nullptr, pred);
     return 3;
 }
 
@@ -1553,6 +1554,10 @@ cs_status cs_mlp_init(cs_ctx* c, int slots, unsigned long long seed) {
     cudaDeviceProp prop;
     CS_CUDA(cudaGetDeviceProperties(&prop, c->device));
     c->mlpGridTile = 2 * prop.multiProcessorCount;
+    // layer 1: 64 TMEM columns per CTA (8 per SM); layers 2-3: 128 columns and 75 KB of shared
+    // memory per CTA (3 per SM)
+    c->mlpGridL1 = 8 * prop.multiProcessorCount;
+    c->mlpGridL23 = 3 * prop.multiProcessorCount;
     c->mlpGridTrain = prop.multiProcessorCount;
     CS_CUDA(cudaFuncSetAttribute(cs_mlp_l1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_SMEM_L1));
     CS_CUDA(cudaFuncSetAttribute(cs_mlp_l23_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_SMEM_L23));

@@ -198,18 +198,30 @@ __global__ void __launch_bounds__(128) cs_mlp_l1_kernel(Batch B, MlpDev M, const
         const bool valid = node < n1;
         float u[32];
         if (valid) {
-            const float* x = fsrc + 16 * (size_t)node;
+            // feature rows are 16 floats = 4 x 16 bytes
+            const float4* x = reinterpret_cast<const float4*>(fsrc + 16 * (size_t)node);
             float acc[16];
 #pragma unroll
-            for (int c = 0; c < 16; c++) {
-                u[c] = (x[c] - sb[64 + c]) / sb[80 + c];
-                acc[c] = 0.f;
+            for (int g = 0; g < 4; g++) {
+                const float4 xv = __ldg(x + g);
+                u[4 * g] = (xv.x - sb[64 + 4 * g]) / sb[80 + 4 * g];
+                u[4 * g + 1] = (xv.y - sb[65 + 4 * g]) / sb[81 + 4 * g];
+                u[4 * g + 2] = (xv.z - sb[66 + 4 * g]) / sb[82 + 4 * g];
+                u[4 * g + 3] = (xv.w - sb[67 + 4 * g]) / sb[83 + 4 * g];
             }
+#pragma unroll
+            for (int c = 0; c < 16; c++) acc[c] = 0.f;
             Nbr nb = neighbours(B, node);
             for (int k = nb.beg; k < nb.end; k++) {
-                const float* xj = fsrc + 16 * (size_t)(B.nbr[k] + nb.off);
+                const float4* xj = reinterpret_cast<const float4*>(fsrc + 16 * (size_t)(B.nbr[k] + nb.off));
 #pragma unroll
-                for (int c = 0; c < 16; c++) acc[c] += xj[c];
+                for (int g = 0; g < 4; g++) {
+                    const float4 xv = __ldg(xj + g);
+                    acc[4 * g] += xv.x;
+                    acc[4 * g + 1] += xv.y;
+                    acc[4 * g + 2] += xv.z;
+                    acc[4 * g + 3] += xv.w;
+                }
             }
             const float inv = nb.end > nb.beg ? 1.0f / (nb.end - nb.beg) : 0.f;
 #pragma unroll
@@ -219,7 +231,12 @@ __global__ void __launch_bounds__(128) cs_mlp_l1_kernel(Batch B, MlpDev M, const
             for (int c = 0; c < 32; c++) u[c] = 0.f;
         }
 #pragma unroll
-        for (int c = 0; c < 32; c++) tc::st_bf16(sA, 128, t, c, u[c]);
+        for (int g = 0; g < 4; g++) {
+            __align__(16) __nv_bfloat16 ub[8];
+#pragma unroll
+            for (int c = 0; c < 8; c++) ub[c] = __float2bfloat16_rn(u[8 * g + c]);
+            *reinterpret_cast<uint4*>(sA + tc::kmajor_offset(128, t, 8 * g)) = *reinterpret_cast<const uint4*>(ub);
+        }
         tc::fence_async_shared();
         sync_tmem();
         if (t == 0) {
@@ -294,7 +311,9 @@ __global__ void __launch_bounds__(128) cs_mlp_l23_kernel(Batch B, MlpDev M, int 
         const bool valid = node < n1;
         // u2 = [h1_i, bf16(mean h1_j)]
         if (valid) {
-            const __nv_bfloat16* hi = M.h1 + 64 * (size_t)node;
+            // rows of h1 are 64 BF16 = 8 x 16 bytes; a K-major tile keeps 8 consecutive k of a
+            // row contiguous, so both the gathers and the tile stores move 16 bytes at a time
+            const uint4* hi = reinterpret_cast<const uint4*>(M.h1 + 64 * (size_t)node);
             Nbr nb = neighbours(B, node);
             const float inv = nb.end > nb.beg ? 1.0f / (nb.end - nb.beg) : 0.f;
 #pragma unroll
@@ -303,18 +322,30 @@ __global__ void __launch_bounds__(128) cs_mlp_l23_kernel(Batch B, MlpDev M, int 
 #pragma unroll
                 for (int c = 0; c < 16; c++) acc[c] = 0.f;
                 for (int k = nb.beg; k < nb.end; k++) {
-                    const __nv_bfloat16* hj = M.h1 + 64 * (size_t)(B.nbr[k] + nb.off) + 16 * q;
+                    const uint4* hj = reinterpret_cast<const uint4*>(M.h1 + 64 * (size_t)(B.nbr[k] + nb.off) + 16 * q);
+                    const uint4 v0 = __ldg(hj), v1 = __ldg(hj + 1);
+                    const __nv_bfloat16* e0 = reinterpret_cast<const __nv_bfloat16*>(&v0);
+                    const __nv_bfloat16* e1 = reinterpret_cast<const __nv_bfloat16*>(&v1);
 #pragma unroll
-                    for (int c = 0; c < 16; c++) acc[c] += __bfloat162float(hj[c]);
+                    for (int c = 0; c < 8; c++) {
+                        acc[c] += __bfloat162float(e0[c]);
+                        acc[8 + c] += __bfloat162float(e1[c]);
+                    }
                 }
+                *reinterpret_cast<uint4*>(sA + tc::kmajor_offset(128, t, 16 * q)) = __ldg(hi + 2 * q);
+                *reinterpret_cast<uint4*>(sA + tc::kmajor_offset(128, t, 16 * q + 8)) = __ldg(hi + 2 * q + 1);
 #pragma unroll
-                for (int c = 0; c < 16; c++) {
-                    *reinterpret_cast<__nv_bfloat16*>(sA + tc::kmajor_offset(128, t, 16 * q + c)) = hi[16 * q + c];
-                    tc::st_bf16(sA, 128, t, 64 + 16 * q + c, acc[c] * inv);
+                for (int hh = 0; hh < 2; hh++) {
+                    __align__(16) __nv_bfloat16 ab[8];
+#pragma unroll
+                    for (int c = 0; c < 8; c++) ab[c] = __float2bfloat16_rn(acc[8 * hh + c] * inv);
+                    *reinterpret_cast<uint4*>(sA + tc::kmajor_offset(128, t, 64 + 16 * q + 8 * hh)) =
+                        *reinterpret_cast<const uint4*>(ab);
                 }
             }
         } else {
-            for (int c = 0; c < 128; c++) tc::st_bf16(sA, 128, t, c, 0.f);
+            const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+            for (int c = 0; c < 128; c += 8) *reinterpret_cast<uint4*>(sA + tc::kmajor_offset(128, t, c)) = zero;
         }
         tc::fence_async_shared();
         sync_tmem();
