@@ -350,7 +350,7 @@ class Context:
         self.check(self.lib.cs_device_pointers(self.h, ctypes.byref(x), ctypes.byref(v), ctypes.byref(dv)))
         return x.value, v.value, dv.value
 
-    KERNELS = ["face", "edge", "gather", "spmv", "vector", "reduce", "spmv_fp64"]
+    KERNELS = ["face", "edge", "gather", "spmv", "vector", "reduce", "spmv_fp64", "resident_solve"]
 
     def profile_kernels(self, params: StepParams, reps: int = 20) -> dict:
         ms = (ctypes.c_float * 8)()

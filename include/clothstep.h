@@ -179,7 +179,9 @@ cs_status cs_device_pointers(cs_ctx* ctx, float** x, float** v, float** dv);
 /* Times each kernel of the step in isolation with CUDA events on the context's stream, `reps`
  * launches each, on the current batch: ms[0] face, [1] edge, [2] gather (assembly),
  * [3] SpMV of a CG iteration, [4] vector update of a CG iteration, [5] per-instance reduction,
- * [6] FP64 residual SpMV.  Overwrites the solver's scratch vectors (not x, v or dv). */
+ * [6] FP64 residual SpMV, [7] one cluster-resident solve of all resident sheets (0 if none;
+ * when every sheet is resident, cs_get_instance_stats then reports that solve).  Overwrites the
+ * solver's scratch vectors and dv64 (not x, v or dv). */
 cs_status cs_profile_kernels(cs_ctx* ctx, const cs_step_params* params, int reps, float* ms);
 /* Cumulative counts since cs_load_batch: [0] steps, [1] solve-loop trips, [2] kernel launches. */
 cs_status cs_get_counters(cs_ctx* ctx, long long* counters);
