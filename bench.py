@@ -68,6 +68,57 @@ def dist_env():
     return rank, world, local
 
 
+class RankGroup:
+    """One process per GPU (torchrun).  Sheets are independent, so ranks exchange no data:
+    the group carries only the barriers around the timed region and the max over ranks of
+    the device times (gloo, host scalars)."""
+
+    def __init__(self, timeout_s: float = 300.0):
+        import datetime
+
+        self.rank, self.world, self.local = dist_env()
+        self.dist = None
+        if self.world > 1:
+            import torch.distributed as dist
+
+            dist.init_process_group("gloo", init_method="env://", timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.dist:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def eval_seed(rank: int) -> int:
+    """Seed of the evaluated workload of a rank."""
+    return 1000 + rank
+
+
+def train_seed(rank: int) -> int:
+    """Seed of a rank's warm-start training trajectories: disjoint from every evaluated seed
+    for up to 32 ranks (7 + 31 r < 1000)."""
+    return 7 + 31 * rank
+
+
+def aggregate_value(nodes_per_rank: int, steps: int, world: int, ms_max: float) -> float:
+    """Whole-job node-steps/s: every rank steps its own batch; time = the slowest rank's."""
+    return nodes_per_rank * steps * world / (ms_max / 1e3)
+
+
 class ClockSampler:
     """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
 
@@ -138,7 +189,7 @@ def scenes_mod():
 
 
 def workload(args, rank):
-    return scenes_mod().windy_batch(args.sheets, args.nq, seed=1000 + rank)
+    return scenes_mod().windy_batch(args.sheets, args.nq, seed=eval_seed(rank))
 
 
 def cpu_baseline(scene, seconds: float, which: str = "ref", threads: int = 1, n_steps: int = 1):
@@ -204,13 +255,11 @@ def run_reference(args):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
 
     from clothsimulator_b200 import native
 
-    rank, world, local = dist_env()
-    if world > 1:
-        dist.init_process_group("gloo", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    group = RankGroup()
+    rank, world, local = group.rank, group.world, group.local
     torch.cuda.set_device(local)
     scene = workload(args, rank)
     ctx = native.Context(local)
@@ -221,16 +270,8 @@ def run_ours(args):
     v0 = np.concatenate([s["v"] for s in scene.sheets])
     stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = group.barrier
+    max_over_ranks = group.max
 
     # Learned warm start: trained on the device on separate seeded trajectories (the
     # evaluated workload's seeds are held out), or loaded from --weights.
@@ -241,7 +282,7 @@ def run_ours(args):
             weights = np.fromfile(args.weights, dtype=np.float32)
             train_info = {"source": args.weights}
         else:
-            tscene = scenes_mod().windy_batch(args.train_sheets, args.nq, seed=7 + 31 * rank)
+            tscene = scenes_mod().windy_batch(args.train_sheets, args.nq, seed=train_seed(rank))
             tctx = native.Context(local)
             tctx.load(tscene.sheets)
             tctx.mlp_init(args.train_steps, 1 + rank)
@@ -300,7 +341,7 @@ def run_ours(args):
         ctx.step(p, allow_unconverged=True)
         it, rr, fl = ctx.instance_stats()
         return {
-            "value": N * args.steps * world / (ms / 1e3),
+            "value": aggregate_value(N, args.steps, world, ms),
             "ms": ms,
             "ms_per_step": ms / args.steps,
             "launches": c1["launches"] - c0["launches"],
@@ -444,8 +485,7 @@ def run_ours(args):
         }
         print(json.dumps(out), flush=True)
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+    group.close()
 
 
 def main():
