@@ -176,16 +176,21 @@ __device__ __forceinline__ bool cluster_sum3(ResShared& S, int rank, int ncta, u
     }
     __syncthreads();
     if (w == 0 && lane < ncta) {
+        // unrolled to the compile-time bound so every load issues before the add chain
         double t[3];
 #pragma unroll
         for (int i = 0; i < 3; i++) {
             if (fp32) {
                 float a = 0.f;
-                for (int j = 0; j < nw; j++) a += (float)S.wsum[j][i];
+#pragma unroll
+                for (int j = 0; j < CS_RES_MAX_WARPS; j++)
+                    if (j < nw) a += (float)S.wsum[j][i];
                 t[i] = (double)a;
             } else {
                 double a = 0.0;
-                for (int j = 0; j < nw; j++) a += S.wsum[j][i];
+#pragma unroll
+                for (int j = 0; j < CS_RES_MAX_WARPS; j++)
+                    if (j < nw) a += S.wsum[j][i];
                 t[i] = a;
             }
         }
@@ -202,11 +207,15 @@ __device__ __forceinline__ bool cluster_sum3(ResShared& S, int rank, int ncta, u
     for (int i = 0; i < 3; i++) {
         if (fp32) {
             float a = 0.f;
-            for (int c = 0; c < ncta; c++) a += (float)S.red[b][c][i];
+#pragma unroll
+            for (int c = 0; c < CS_RES_MAX_CL; c++)
+                if (c < ncta) a += (float)S.red[b][c][i];
             v[i] = (double)a;
         } else {
             double a = 0.0;
-            for (int c = 0; c < ncta; c++) a += S.red[b][c][i];
+#pragma unroll
+            for (int c = 0; c < CS_RES_MAX_CL; c++)
+                if (c < ncta) a += S.red[b][c][i];
             v[i] = a;
         }
     }
