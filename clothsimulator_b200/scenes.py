@@ -215,6 +215,74 @@ def large_irregular(nq: int = 1000, seed: int = 0) -> Scene:
     return Scene(f"irregular{nq}", [s], dt=1.0 / 200, steps=50)
 
 
+def synthetic_proximities(sheet: dict, rng: np.random.Generator, n_vf: int = 6, n_ee: int = 4, n_ext: int = 4,
+                          stiffness: float = 1e4, thickness: float = 5e-3, node_off: int = 0) -> dict:
+    """Seeded proximity records of the kind Cloth::physicsStep receives (Proximity.cu:5-24):
+    vertex-face pairs inside the sheet (weights 1 and minus the barycentric weights of the
+    face point, the face normal), edge-edge pairs (weights 1 - s, s, -(1 - t), -t, the
+    normalised cross product of the edges), and external points (an obstacle-like point
+    near a face: node -1 with its own position, velocity and mass, not free).  Stiffness is
+    `stiffness` times the smaller rest area, as the constructors scale it.  Node ids are
+    offset by `node_off` (for a sheet inside a batch)."""
+    x = sheet["x"].astype(np.float64)
+    v = sheet["v"].astype(np.float64)
+    fx = sheet["fx"]
+    nn = x.shape[0]
+    u = sheet["uv"].astype(np.float64)
+    e1 = u[fx[:, 1]] - u[fx[:, 0]]
+    e2 = u[fx[:, 2]] - u[fx[:, 0]]
+    farea = 0.5 * np.abs(e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0])
+    recs = {k: [] for k in ("nodes", "x", "v", "mass", "free", "normal", "w", "mu", "stiffness")}
+
+    def face_normal(f):
+        a, b_, c = x[fx[f, 0]], x[fx[f, 1]], x[fx[f, 2]]
+        n = np.cross(b_ - a, c - a)
+        return n / np.linalg.norm(n)
+
+    def add(nodes, w, n, mu, k, xe=None, ve=None, me=None, free=0):
+        recs["nodes"].append([(i + node_off) if i >= 0 else -1 for i in nodes])
+        recs["x"].append(xe if xe is not None else np.zeros((4, 3)))
+        recs["v"].append(ve if ve is not None else np.zeros((4, 3)))
+        recs["mass"].append(me if me is not None else np.ones(4))
+        recs["free"].append(free)
+        recs["normal"].append(n)
+        recs["w"].append(w)
+        recs["mu"].append(mu)
+        recs["stiffness"].append(k)
+
+    for _ in range(n_vf):
+        f = int(rng.integers(len(fx)))
+        i = int(rng.integers(nn))
+        while i in fx[f]:
+            i = int(rng.integers(nn))
+        bc = rng.dirichlet(np.ones(3))
+        add([i, *fx[f]], [1.0, -bc[0], -bc[1], -bc[2]], face_normal(f), rng.uniform(0.1, 0.6),
+            stiffness * farea[f] * rng.uniform(0.5, 1.0))
+    for _ in range(n_ee):
+        f0, f1 = rng.choice(len(fx), 2, replace=False)
+        p0, p1 = fx[f0, 0], fx[f0, 1]
+        q0, q1 = fx[f1, 1], fx[f1, 2]
+        if len({p0, p1, q0, q1}) < 4:
+            continue
+        n = np.cross(x[p1] - x[p0], x[q1] - x[q0])
+        n = n / np.linalg.norm(n) if np.linalg.norm(n) > 1e-12 else np.array([0.0, 0.0, 1.0])
+        s_, t_ = rng.uniform(0, 1, 2)
+        add([p0, p1, q0, q1], [1 - s_, s_, -(1 - t_), -t_], n, rng.uniform(0.1, 0.6),
+            stiffness * min(farea[f0], farea[f1]))
+    for _ in range(n_ext):
+        f = int(rng.integers(len(fx)))
+        bc = rng.dirichlet(np.ones(3))
+        n = face_normal(f)
+        pt = bc @ x[fx[f]] + n * rng.uniform(0.0, thickness)
+        xe = np.zeros((4, 3))
+        ve = np.zeros((4, 3))
+        xe[0] = pt
+        ve[0] = rng.normal(0, 0.05, 3)
+        me = np.ones(4)
+        add([-1, *fx[f]], [1.0, -bc[0], -bc[1], -bc[2]], n, rng.uniform(0.1, 0.6), stiffness * farea[f], xe, ve, me)
+    return {k: np.asarray(vv, dtype=np.int32 if k in ("nodes", "free") else np.float64) for k, vv in recs.items()}
+
+
 WORKLOADS = {
     "hang32": lambda seed=0: hang(32, seed),
     "precision256": lambda seed=0: precision_sheet(256, seed),

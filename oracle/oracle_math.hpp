@@ -359,6 +359,69 @@ inline void bendingForce(const Material<T>& mat, const V3<T>& x0, const V3<T>& x
     if (theta_out) *theta_out = angle;
 }
 
+// ---------------------------------------------------------------------------------------
+// Proximity forces (the repulsion and friction terms of Cloth::physicsStep,
+// Cloth.cu:171-192).  A proximity (Proximity.cuh:11-21) couples four nodes through weights
+// w (vertex-face: 1 and minus the barycentric weights; edge-edge: the edge weights), a unit
+// normal n, a friction coefficient mu and a stiffness already scaled by the smaller area
+// (Proximity.cu:7-24).
+
+// impulseForce (PhysicsHelper.cu:398-406): f = 1/2 k/h d^2 N, J = -k/h d N N^T with
+// N = (w_0 n, w_1 n, w_2 n, w_3 n).
+template <class T>
+inline void impulseForce(const T w[4], const V3<T>& n, T stiffness, T d, T thickness, T f[12], T J[144]) {
+    T N[12];
+    for (int i = 0; i < 4; i++)
+        for (int c = 0; c < 3; c++) N[3 * i + c] = w[i] * n[c];
+    const T sf = T(0.5) * stiffness / thickness * (d * d);
+    for (int p = 0; p < 12; p++) f[p] = sf * N[p];
+    const T sj = -stiffness / thickness * d;
+    for (int p = 0; p < 12; p++)
+        for (int q = 0; q < 12; q++) J[12 * p + q] = sj * (N[p] * N[q]);
+}
+
+// frictionForce (PhysicsHelper.cu:408-432): tangential relative velocity vt of the weighted
+// nodes, magnitude f_v = min(mu F / |vt|, 1 / (dt sum_free w_i^2 / m_i)), f = -f_v (w_i vt),
+// J_ij = -f_v w_i w_j (I - n n^T).
+template <class T>
+inline void frictionForce(const T w[4], const V3<T>& n, T mu, T stiffness, T d, T thickness, T dt, const V3<T> vel[4],
+                          const T mass[4], int freeMask, T f[12], T J[144]) {
+    const T F = T(0.5) * stiffness / thickness * (d * d);
+    V3<T> v = v3(T(0), T(0), T(0));
+    T invMass = T(0);
+    for (int i = 0; i < 4; i++) {
+        V3<T> wv = scl(w[i], vel[i]);
+        v = add(v, wv);
+        if (freeMask & (1 << i)) invMass += (w[i] * w[i]) / mass[i];
+    }
+    T Tm[3][3];
+    for (int k = 0; k < 3; k++)
+        for (int h = 0; h < 3; h++) Tm[k][h] = (k == h ? T(1) : T(0)) - n[k] * n[h];
+    V3<T> vt;
+    for (int k = 0; k < 3; k++) {
+        T acc = T(0);
+        for (int h = 0; h < 3; h++) acc += Tm[k][h] * v[h];
+        vt[k] = acc;
+    }
+    const T f_v = mn(mu * F / norm(vt), T(1) / (dt * invMass));
+    for (int i = 0; i < 4; i++)
+        for (int c = 0; c < 3; c++) f[3 * i + c] = -f_v * (w[i] * vt[c]);
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+            const T s = -f_v * w[i] * w[j];
+            for (int k = 0; k < 3; k++)
+                for (int h = 0; h < 3; h++) J[(3 * i + k) * 12 + 3 * j + h] = s * Tm[k][h];
+        }
+}
+
+// Penetration depth below the thickness (Cloth.cu:179-182): d = max(h - sum_i w_i n.x_i, 0).
+template <class T>
+inline T proximityDepth(const T w[4], const V3<T>& n, const V3<T> x[4], T thickness) {
+    T d = -thickness;
+    for (int i = 0; i < 4; i++) d += w[i] * dot(n, x[i]);
+    return mx(-d, T(0));
+}
+
 }  // namespace orc
 
 #endif

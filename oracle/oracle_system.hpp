@@ -97,6 +97,19 @@ struct StepParams {
     double handleStiffness;
 };
 
+// One proximity as Cloth::physicsStep receives it (Proximity.cuh:11-21).  node[i] >= 0: a
+// node of this cloth (its x, v, mass are the cloth's; cloth nodes are free, Mesh.cu:349);
+// node[i] < 0: a point outside the cloth (another cloth's node or an obstacle's) with the
+// given x, v, mass and free flag (bit i of freeMask); its rows and columns are skipped, as
+// Cloth.cu:176-177 marks nodes the mesh does not contain with index -1.
+template <class T>
+struct ProximityRec {
+    int node[4];
+    T x[4][3], v[4][3], mass[4];
+    int freeMask;
+    T n[3], w[4], mu, stiffness;
+};
+
 // Sparse block accumulator with the reference's accumulation order: one float (or
 // double) per scalar entry, updated element by element in mesh order exactly like
 // Eigen's coeffRef(i,j) += v (Cloth.cu:42-76).  The pattern is fixed per mesh.
@@ -125,6 +138,10 @@ struct Cloth {
     std::function<void(Cloth&)> syncHook;
     std::function<void(int, T*, T*)> faceHook;
     std::function<void(int, T*, T*, T*)> edgeHook;
+    // (proximity, depth, thickness, dt, impulse f, J, friction f, J)
+    std::function<void(int, T, T, T, T*, T*, T*, T*)> proxHook;
+    std::vector<ProximityRec<T>> prox;
+    T proxThickness = T(0);
     std::vector<T> x, v, u;           // 3N, 3N, 2U
     std::vector<T> finv, farea, fmass, fn;  // per face: 4, 1, 1, 3 (normal)
     std::vector<T> mass;              // per node
@@ -188,6 +205,11 @@ struct Cloth {
                 edgeNodes(e, ids);
                 link(ids, 4);
             }
+        // proximity pairs enter the pattern as Eigen's coeffRef inserts them
+        for (const ProximityRec<T>& pr : prox)
+            for (int a = 0; a < 4; a++)
+                for (int b = 0; b < 4; b++)
+                    if (pr.node[a] >= 0 && pr.node[b] >= 0) adj[pr.node[a]].push_back(pr.node[b]);
         sys.n = n;
         sys.rowPtr.assign(n + 1, 0);
         sys.col.clear();
@@ -226,6 +248,60 @@ struct Cloth {
         T d0[2] = {u[2 * ev[1]] - u[2 * ev[0]], u[2 * ev[1] + 1] - u[2 * ev[0] + 1]};
         T d1[2] = {u[2 * ev[3]] - u[2 * ev[2]], u[2 * ev[3] + 1] - u[2 * ev[2] + 1]};
         bendingForce<T>(*mat, X(ids[0]), X(ids[1]), X(ids[2]), X(ids[3]), N(f0), N(f1), area, d0, d1, fo, J, theta);
+    }
+
+    // Sets the proximities of the next steps (rebuilds the pattern).
+    void setProximities(const std::vector<ProximityRec<T>>& recs, T thickness) {
+        prox = recs;
+        proxThickness = thickness;
+        buildPattern();
+    }
+
+    // Position, velocity of a proximity's node i (Cloth.cu:174, 180-181).
+    V3<T> proxX(const ProximityRec<T>& pr, int i) const {
+        return pr.node[i] >= 0 ? X(pr.node[i]) : v3(pr.x[i][0], pr.x[i][1], pr.x[i][2]);
+    }
+    V3<T> proxV(const ProximityRec<T>& pr, int i) const {
+        return pr.node[i] >= 0 ? Vel(pr.node[i]) : v3(pr.v[i][0], pr.v[i][1], pr.v[i][2]);
+    }
+
+    // Depth and the impulse and friction forces and Jacobians of proximity p at the current
+    // state (Cloth.cu:179-190).
+    T proximityForces(int p, T dt, T fI[12], T JI[144], T fF[12], T JF[144]) const {
+        const ProximityRec<T>& pr = prox[p];
+        V3<T> xs[4], vs[4];
+        T ms[4];
+        int freeMask = 0;
+        for (int i = 0; i < 4; i++) {
+            xs[i] = proxX(pr, i);
+            vs[i] = proxV(pr, i);
+            ms[i] = pr.node[i] >= 0 ? mass[pr.node[i]] : pr.mass[i];
+            if (pr.node[i] >= 0 || (pr.freeMask & (1 << i))) freeMask |= 1 << i;
+        }
+        const V3<T> n = v3(pr.n[0], pr.n[1], pr.n[2]);
+        const T d = proximityDepth<T>(pr.w, n, xs, proxThickness);
+        if (proxHook) {
+            proxHook(p, d, proxThickness, dt, fI, JI, fF, JF);
+            return d;
+        }
+        impulseForce<T>(pr.w, n, pr.stiffness, d, proxThickness, fI, JI);
+        frictionForce<T>(pr.w, n, pr.mu, pr.stiffness, d, proxThickness, dt, vs, ms, freeMask, fF, JF);
+        return d;
+    }
+
+    // Cloth.cu:42-76 with rows and columns of index -1 skipped.
+    void addElementSkip(const T* B, const T* bb, const int* ids) {
+        for (int i = 0; i < 4; i++) {
+            int xi = ids[i];
+            if (xi < 0) continue;
+            for (int j = 0; j < 4; j++) {
+                if (ids[j] < 0) continue;
+                int blk = sys.find(xi, ids[j]);
+                for (int k = 0; k < 3; k++)
+                    for (int h = 0; h < 3; h++) sys.val[9 * blk + 3 * k + h] += B[(3 * i + k) * 12 + 3 * j + h];
+            }
+            for (int j = 0; j < 3; j++) sys.b[3 * xi + j] += bb[3 * i + j];
+        }
     }
 
     template <int K>
@@ -320,6 +396,23 @@ struct Cloth {
             V3<T> p = v3(handlePos[3 * h], handlePos[3 * h + 1], handlePos[3 * h + 2]);
             V3<T> fh = mul(scl(dt, sub(sub(p, X(i)), scl(dt, Vel(i)))), k);
             for (int j = 0; j < 3; j++) sys.b[3 * i + j] += fh[j];
+        }
+        // addProximityForces (Cloth.cu:171-192): per proximity, the impulse term
+        // (-dt^2 J, dt (f + dt J v)) then the friction term (-dt J, dt f)
+        for (size_t pi = 0; pi < prox.size(); pi++) {
+            const ProximityRec<T>& pr = prox[pi];
+            T fI[12], JI[144], fF[12], JF[144];
+            proximityForces((int)pi, dt, fI, JI, fF, JF);
+            for (int a = 0; a < 4; a++) {
+                V3<T> va = proxV(pr, a);
+                for (int c = 0; c < 3; c++) vel[3 * a + c] = va[c];
+            }
+            elementSystem<4>(dt, fI, JI, vel, B, bb);
+            addElementSkip(B, bb, pr.node);
+            const T sF = -dt;
+            for (int q = 0; q < 144; q++) B[q] = sF * JF[q];
+            for (int q = 0; q < 12; q++) bb[q] = dt * fF[q];
+            addElementSkip(B, bb, pr.node);
         }
     }
 

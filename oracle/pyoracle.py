@@ -86,6 +86,9 @@ class Lib:
         f("cloth_normals", None, [_vp, _dp])
         f("cloth_step", ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _dp])
         f("cloth_factor_nnz", ctypes.c_longlong, [_vp])
+        f("cloth_set_proximities", None, [_vp, ctypes.c_int, _ip, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp,
+                                          ctypes.c_double])
+        f("cloth_proximity_forces", None, [_vp, ctypes.c_double, _dp, _dp, _dp, _dp, _dp])
         f("run_cloths", ctypes.c_double, [ctypes.POINTER(_vp), ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, _ip])
         if which == "oracle":
@@ -263,6 +266,28 @@ class Cloth:
         m = np.zeros(3 * self.nf)
         self.L.cloth_normals(self.h, _ptr(m, _dp))
         return m.reshape(-1, 3)
+
+    def set_proximities(self, prox: dict, thickness: float):
+        """Proximities of the next steps (Cloth::physicsStep's `proximities`): a dict of arrays
+        nodes (n, 4) int (-1: a point outside the cloth), x, v (n, 4, 3) and mass (n, 4) of
+        those points, free (n,) bit mask, normal (n, 3), w (n, 4), mu (n,), stiffness (n,)."""
+        n = len(prox["mu"])
+        self._prox = {k: (_i(v) if k in ("nodes", "free") else _d(v)) for k, v in prox.items()}
+        P = self._prox
+        self.L.cloth_set_proximities(self.h, n, _ptr(P["nodes"], _ip), _ptr(P["x"], _dp), _ptr(P["v"], _dp),
+                                     _ptr(P["mass"], _dp), _ptr(P["free"], _ip), _ptr(P["normal"], _dp),
+                                     _ptr(P["w"], _dp), _ptr(P["mu"], _dp), _ptr(P["stiffness"], _dp), thickness)
+        self.n_prox = n
+
+    def proximity_forces(self, dt: float):
+        """(depth, impulse f, impulse J, friction f, friction J) of every proximity."""
+        n = self.n_prox
+        fI, fF = np.zeros((n, 12)), np.zeros((n, 12))
+        JI, JF = np.zeros((n, 12, 12)), np.zeros((n, 12, 12))
+        d = np.zeros(n)
+        self.L.cloth_proximity_forces(self.h, dt, _ptr(fI, _dp), _ptr(JI, _dp), _ptr(fF, _dp), _ptr(JF, _dp),
+                                      _ptr(d, _dp))
+        return d, fI, JI, fF, JF
 
     def topology_mismatches(self) -> int:
         return self.L.cloth_topology_mismatches(self.h)

@@ -24,6 +24,7 @@
 #include "Material.cuh"
 #include "Node.cuh"
 #include "PhysicsHelper.cuh"
+#include "Proximity.cuh"
 #include "Vertex.cuh"
 
 #include "oracle_system.hpp"
@@ -150,6 +151,7 @@ void* ref_cloth_new(void* mat, int nn, const double* x, const double* v, int nv,
         for (size_t i = 0; i < r.nodes.size(); i++) {
             r.nodes[i].x = Vector3f(cl.x[3 * i], cl.x[3 * i + 1], cl.x[3 * i + 2]);
             r.nodes[i].v = Vector3f(cl.v[3 * i], cl.v[3 * i + 1], cl.v[3 * i + 2]);
+            r.nodes[i].mass = cl.mass[i];
         }
         for (size_t f = 0; f < r.faces.size(); f++) {
             r.faces[f].update();
@@ -174,6 +176,40 @@ void* ref_cloth_new(void* mat, int nn, const double* x, const double* v, int nv,
             for (int q = 0; q < 12; q++) J[12 * p + q] = JJ(p, q);
         }
         if (theta) *theta = self->rc.edges[e].angle();
+    };
+    // The reference's impulseForce and frictionForce (PhysicsHelper.cu:398-432) on a Proximity
+    // whose nodes are this cloth's reference Nodes or, for points outside the cloth, Nodes
+    // built from the given position, velocity, mass and free flag.
+    c->c.proxHook = [self](int p, float d, float thickness, float dt, float* fI, float* JI, float* fF, float* JF) {
+        const orc::ProximityRec<float>& pr = self->c.prox[p];
+        Node ext[4];
+        Proximity prox;
+        for (int i = 0; i < 4; i++) {
+            if (pr.node[i] >= 0) {
+                prox.nodes[i] = &self->rc.nodes[pr.node[i]];
+            } else {
+                ext[i] = Node(Vector3f(pr.x[i][0], pr.x[i][1], pr.x[i][2]), ((pr.freeMask >> i) & 1) != 0);
+                ext[i].v = Vector3f(pr.v[i][0], pr.v[i][1], pr.v[i][2]);
+                ext[i].mass = pr.mass[i];
+                prox.nodes[i] = &ext[i];
+            }
+            prox.w[i] = pr.w[i];
+        }
+        prox.n = Vector3f(pr.n[0], pr.n[1], pr.n[2]);
+        prox.mu = pr.mu;
+        prox.stiffness = pr.stiffness;
+        Vector12f f;
+        Matrix12x12f J;
+        impulseForce(prox, d, thickness, f, J);
+        for (int q = 0; q < 12; q++) {
+            fI[q] = f(q);
+            for (int k = 0; k < 12; k++) JI[12 * q + k] = J(q, k);
+        }
+        frictionForce(prox, d, thickness, dt, f, J);
+        for (int q = 0; q < 12; q++) {
+            fF[q] = f(q);
+            for (int k = 0; k < 12; k++) JF[12 * q + k] = J(q, k);
+        }
     };
     c->c.syncHook(c->c);
     return static_cast<ClothBase*>(c);

@@ -10,6 +10,9 @@ bendingForce and Face code (PhysicsHelper.cu:264-353, Material.cu:3-156, Face.cu
 124-132), the system assembled around them in the reference order (Cloth.cu:42-169) and
 one CPU-path step (FP32 sparse Cholesky).  Materials are seeded synthetic parameter sets
 (anisotropic stretching rows, varied bending samples), not the reference's material files.
+ref_prox9.npz adds seeded proximities: the reference's impulseForce and frictionForce per
+proximity and the step with them (`python tests/golden/make_golden.py ref_prox9` makes only
+that file).
 """
 import os
 import sys
@@ -69,8 +72,47 @@ def make_case(seed, nq, amp):
     )
 
 
+THICKNESS = 5e-3
+
+
+def make_prox_case(seed, nq):
+    """A hanging sheet with seeded proximities (vertex-face, edge-edge, external points): the
+    reference's impulseForce and frictionForce (PhysicsHelper.cu:398-432) per proximity, the
+    system assembled with them in the reference order (Cloth.cu:171-192) and one CPU step."""
+    rng = np.random.default_rng(seed)
+    scene = scenes.hang(nq, seed=seed)
+    s = scene.sheets[0]
+    s["x"] = (s["x"] + rng.normal(0, 0.01, s["x"].shape)).astype(np.float32)
+    s["v"] = rng.normal(0, 0.1, s["v"].shape).astype(np.float32)
+    prox = scenes.synthetic_proximities(s, rng, thickness=THICKNESS)
+    c = pyoracle.Cloth(s, pyoracle.Material(s["material"], which="ref"))
+    c.set_proximities(prox, THICKNESS)
+    params = np.array(scenes.step_params(scene, s))
+    d, fI, JI, fF, JF = c.proximity_forces(scene.dt)
+    rp, ci, val, b = c.assemble(params)
+    dv, _ = c.step(params, pyoracle.METHOD_LLT)
+    x1, v1 = c.state()
+    out = dict(x=s["x"], v=s["v"], uv=s["uv"], fx=s["fx"], fu=s["fu"], handles=s["handles"], params=params,
+               thickness=THICKNESS, depth=d.astype(np.float32), impulse_f=fI.astype(np.float32),
+               impulse_J=JI.astype(np.float32), friction_f=fF.astype(np.float32), friction_J=JF.astype(np.float32),
+               row_ptr=rp, col=ci, val=val.astype(np.float32), b=b.astype(np.float32), dv=dv.astype(np.float32),
+               x1=x1.astype(np.float32), v1=v1.astype(np.float32))
+    out.update({"prox_" + k: v for k, v in prox.items()})
+    out["material_stretching"] = np.array(s["material"]["stretching"])
+    out["material_bending"] = np.array(s["material"]["bending"])
+    out["material_density"] = s["material"]["density"]
+    return out
+
+
 if __name__ == "__main__":
+    only = sys.argv[1:]
     for name, seed, nq, amp in [("ref_sheet6", 11, 6, 0.03), ("ref_sheet9", 12, 9, 0.01)]:
+        if only and name not in only:
+            continue
         case = make_case(seed, nq, amp)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **case)
         print(name, {k: np.asarray(v).shape for k, v in case.items() if np.asarray(v).size > 1})
+    if not only or "ref_prox9" in only:
+        case = make_prox_case(21, 9)
+        np.savez_compressed(os.path.join(HERE, "ref_prox9.npz"), **case)
+        print("ref_prox9", {k: np.asarray(v).shape for k, v in case.items() if np.asarray(v).size > 1})

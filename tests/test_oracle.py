@@ -19,7 +19,63 @@ import scipy.sparse.linalg as spla
 import pyoracle
 from clothsimulator_b200 import scenes
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_sheet*.npz")))
+GOLDEN_PROX = os.path.join(os.path.dirname(__file__), "golden", "ref_prox9.npz")
+
+
+def golden_prox(g):
+    mat = {"density": float(g["material_density"]), "stretching": g["material_stretching"].tolist(),
+           "bending": g["material_bending"].tolist(), "thicken": 1.0, "density_mult": 1.0,
+           "stretching_mult": 1.0, "bending_mult": 1.0}
+    sheet = {k: g[k] for k in ("x", "v", "uv", "fx", "fu", "handles")}
+    sheet["material"] = mat
+    prox = {k[5:]: g[k] for k in g.files if k.startswith("prox_")}
+    return sheet, prox
+
+
+def test_oracle_reproduces_reference_proximity_golden():
+    """Repulsion and friction of seeded proximities (the reference's impulseForce and
+    frictionForce, PhysicsHelper.cu:398-432), the system assembled with them (Cloth.cu:171-192)
+    and one CPU step, bit for bit."""
+    g = np.load(GOLDEN_PROX)
+    sheet, prox = golden_prox(g)
+    c = pyoracle.Cloth(sheet, pyoracle.Material(sheet["material"], "float"))
+    c.set_proximities(prox, float(g["thickness"]))
+    d, fI, JI, fF, JF = c.proximity_forces(float(g["params"][0]))
+    for a, k in [(d, "depth"), (fI, "impulse_f"), (JI, "impulse_J"), (fF, "friction_f"), (JF, "friction_J")]:
+        assert np.array_equal(a.astype(np.float32), g[k]), k
+    rp, ci, val, b = c.assemble(g["params"])
+    assert np.array_equal(rp, g["row_ptr"]) and np.array_equal(ci, g["col"])
+    assert np.array_equal(val.astype(np.float32), g["val"]) and np.array_equal(b.astype(np.float32), g["b"])
+    dv, _ = c.step(g["params"], pyoracle.METHOD_LLT)
+    x1, v1 = c.state()
+    assert np.array_equal(dv.astype(np.float32), g["dv"])
+    assert np.array_equal(x1.astype(np.float32), g["x1"]) and np.array_equal(v1.astype(np.float32), g["v1"])
+
+
+@pytest.mark.ref
+def test_oracle_proximities_match_reference_adapter_live():
+    if not os.path.exists(pyoracle.LIB_REF):
+        pytest.skip("reference adapter not built")
+    for seed in range(3):
+        rng = np.random.default_rng(100 + seed)
+        scene = scenes.uneven_batch(1, seed=seed, nq_range=(6, 12))
+        s = scene.sheets[0]
+        s["x"] = (s["x"] + rng.normal(0, 0.01, s["x"].shape)).astype(np.float32)
+        s["v"] = rng.normal(0, 0.2, s["v"].shape).astype(np.float32)
+        prox = scenes.synthetic_proximities(s, rng, n_vf=8, n_ee=6, n_ext=6)
+        co = pyoracle.Cloth(s, pyoracle.Material(s["material"]))
+        cr = pyoracle.Cloth(s, pyoracle.Material(s["material"], which="ref"))
+        for c in (co, cr):
+            c.set_proximities(prox, 5e-3)
+        for u, w in zip(co.proximity_forces(scene.dt), cr.proximity_forces(scene.dt)):
+            assert np.array_equal(u, w)
+        p = scenes.step_params(scene, s)
+        for u, w in zip(co.assemble(p), cr.assemble(p)):
+            assert np.array_equal(u, w)
+        d1, _ = co.step(p)
+        d2, _ = cr.step(p)
+        assert np.array_equal(d1, d2)
 
 
 def golden_sheet(g):
