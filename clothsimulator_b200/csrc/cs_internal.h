@@ -119,6 +119,26 @@ struct DevParams {
     int solver;            // CS_SOLVER_AUTO_DEV: resident sheets on the cluster kernel; BATCHED: loop only
 };
 
+// One proximity as seen by one sheet it touches (cs_set_proximities): node[i] is a batch
+// node or -1; bit i of `local` marks the nodes of this sheet (their rows and columns get
+// blocks); other points enter through their state only.
+struct ProxInst {
+    int node[4];
+    int local, free_mask, sheet;
+    float thickness;
+    float n[3], w[4], mu, stiffness;
+    float xe[4][3], ve[4][3], me[4];  // points outside the batch (node -1)
+};
+
+// Per-instance record written by cs_prox_kernel: -dt^2 J of the impulse (12x12), -dt J of
+// the friction (12x12), the impulse right-hand side dt (f + dt J v) (12), the friction one dt f.
+#define CS_PROX_REC 312
+// Contribution code: bits 5.. instance, bit 4 friction (1) / impulse (0), bits 2..3 local row
+// corner a, bits 0..1 column corner b.
+__host__ __device__ inline uint32_t cs_pcode(int inst, int friction, int a, int b) {
+    return ((uint32_t)inst << 5) | ((uint32_t)friction << 4) | ((uint32_t)a << 2) | (uint32_t)b;
+}
+
 struct Batch {
     int N = 0, F = 0, E = 0, S = 0;
     int n_slices = 0, n_panels = 0, n_tpanels = 0, n_tables = 0;
@@ -170,6 +190,23 @@ struct Batch {
     uint32_t* rsend = nullptr;   // halo sends: src slot | dst rank << 12 | dst halo index << 16
     int* rhalo = nullptr;        // per topology: CS_RES_MAX_CL + 1 halo slot counts per rank
     int res_halo0 = 0;           // first halo slot of every CTA's p array (= own slots per CTA)
+    // proximities (cs_set_proximities); all lists in the reference's accumulation order
+    int n_pinst = 0, n_pfix = 0, n_pb = 0, n_pdiag = 0, n_px = 0;
+    const ProxInst* pinst = nullptr;
+    float* prec = nullptr;        // CS_PROX_REC per instance
+    int* pfix_slot = nullptr;     // pattern slots that receive blocks: panel * 32 + lane
+    int* pfix_ptr = nullptr;      // their contribution ranges (n_pfix + 1)
+    uint32_t* pfix_code = nullptr;
+    int* pb_row = nullptr;        // rows whose right-hand side receives terms
+    int* pb_ptr = nullptr;
+    uint32_t* pb_code = nullptr;
+    int* pdiag_row = nullptr;     // rows whose diagonal block changed (block-Jacobi inverse redone)
+    int* xptr = nullptr;          // N + 1: blocks outside the pattern, per row (null: none)
+    int* xcol = nullptr;          // their columns (batch nodes)
+    int* xcptr = nullptr;         // their contribution ranges (n_px + 1)
+    uint32_t* xcode = nullptr;
+    float* xval = nullptr;        // 9 per block, summed each step
+    int* sheet_prox = nullptr;    // per sheet: 1 if a proximity touches it (batched loop this step)
 };
 
 #endif

@@ -44,6 +44,12 @@ __global__ void cs_advance_kernel(Batch B);
 __global__ void cs_spmv_plain_kernel(Batch B, const float* x, float* y);
 __global__ void cs_profile_setup_kernel(Batch B, int phase);
 __global__ void cs_resident_pcg_kernel(Batch B);
+__global__ void cs_prox_kernel(Batch B);
+__global__ void cs_prox_fix_kernel(Batch B);
+__global__ void cs_prox_rhs_kernel(Batch B);
+__global__ void cs_prox_diag_kernel(Batch B);
+__global__ void cs_prox_extra_kernel(Batch B);
+__global__ void cs_slice_bnorm_kernel(Batch B);
 
 namespace {
 
@@ -547,8 +553,13 @@ struct cs_ctx {
     cudaGraph_t graphLearned = nullptr;
     // cluster-resident solver launch (resident.cu): CTAs per cluster, threads per CTA,
     // clusters in the persistent grid, dynamic shared memory per CTA
-    int resCL = 0, resThreads = 0, resClusters = 0;
+    int resCL = 0, resThreads = 0, resClusters = 0, resClustersMax = 0;
     size_t resSmem = 0;
+    std::vector<int> rlistAll;  // resident sheets before the proximity filter
+    // proximities (cs_set_proximities): their device lists, and the host copies of the
+    // blocks outside the pattern that cs_get_system merges
+    std::vector<void*> proxAllocs;
+    std::vector<int> hxptr, hxcol;
 };
 
 namespace {
@@ -603,6 +614,11 @@ void freeBatch(cs_ctx* c) {
     c->mlpScratch = nullptr;
     for (void* p : c->allocs) cudaFree(p);
     c->allocs.clear();
+    for (void* p : c->proxAllocs) cudaFree(p);
+    c->proxAllocs.clear();
+    c->hxptr.clear();
+    c->hxcol.clear();
+    c->rlistAll.clear();
     c->B = Batch();
     c->loaded = false;
     c->lastStepValid = false;
@@ -616,6 +632,17 @@ int launchAssembly(cs_ctx* c) {
     if (B.F) cs_face_kernel<<<nblk(B.F, 64), 64, 0, c->stream>>>(B), n++;
     if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B), n++;
     cs_gather_kernel<<<c->gatherGrid, 128, 0, c->stream>>>(B);
+    if (B.n_pinst > 0) {
+        // proximity terms after the handles (Cloth.cu:676-684): records, pattern slots,
+        // right-hand sides, the changed diagonal inverses, ||b|| partials, outside blocks
+        cs_prox_kernel<<<nblk(B.n_pinst, 128), 128, 0, c->stream>>>(B);
+        cs_prox_fix_kernel<<<nblk(B.n_pfix, 128), 128, 0, c->stream>>>(B);
+        cs_prox_rhs_kernel<<<nblk(B.n_pb, 128), 128, 0, c->stream>>>(B);
+        cs_prox_diag_kernel<<<nblk(B.n_pdiag, 128), 128, 0, c->stream>>>(B);
+        cs_slice_bnorm_kernel<<<nblk((long long)B.n_slices * 32, 128), 128, 0, c->stream>>>(B);
+        n += 5;
+        if (B.n_px > 0) cs_prox_extra_kernel<<<nblk(B.n_px, 128), 128, 0, c->stream>>>(B), n++;
+    }
     return n;
 }
 
@@ -1068,7 +1095,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     B.n_resident = (int)hrlist.size();
     B.res_cap = resCap;
     B.res_halo0 = resW * CS_SLICE;
+    c->resClustersMax = c->resClusters;
     c->resClusters = std::min(c->resClusters, B.n_resident);
+    c->rlistAll = hrlist;
     c->sheets = hs;
     c->slices = hslices;
 
@@ -1161,7 +1190,7 @@ cs_status cs_get_sizes(const cs_ctx* c, long long* sizes) {
     sizes[3] = (long long)c->B.n_panels * CS_SLICE;
     sizes[4] = c->B.n_slices;
     sizes[5] = c->B.S;
-    sizes[6] = c->nnzb_pattern;
+    sizes[6] = c->nnzb_pattern + c->B.n_px;
     return CS_OK;
 }
 
@@ -1171,6 +1200,223 @@ cs_status cs_set_state(cs_ctx* c, const float* x, const float* v) {
     size_t n = 3 * (size_t)c->B.N * sizeof(float);
     if (x) CS_CUDA(cudaMemcpyAsync(c->B.x, x, n, cudaMemcpyHostToDevice, c->stream));
     if (v) CS_CUDA(cudaMemcpyAsync(c->B.v, v, n, cudaMemcpyHostToDevice, c->stream));
+    return CS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+void destroyGraphs(cs_ctx* c) {
+    if (c->graphExec) cudaGraphExecDestroy(c->graphExec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    if (c->graphExecLearned) cudaGraphExecDestroy(c->graphExecLearned);
+    if (c->graphLearned) cudaGraphDestroy(c->graphLearned);
+    c->graphExec = nullptr;
+    c->graph = nullptr;
+    c->graphExecLearned = nullptr;
+    c->graphLearned = nullptr;
+}
+
+template <class T>
+cs_status proxUpload(cs_ctx* c, T** p, const std::vector<T>& h) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(h.size(), 1) * sizeof(T));
+    if (e != cudaSuccess) return fail(c, CS_ERR_CUDA, "cudaMalloc(%zu bytes): %s", h.size() * sizeof(T), cudaGetErrorString(e));
+    c->proxAllocs.push_back(q);
+    *p = (T*)q;
+    if (!h.empty()) CS_CUDA(cudaMemcpy(q, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return CS_OK;
+}
+
+void clearProximities(cs_ctx* c) {
+    Batch& B = c->B;
+    for (void* p : c->proxAllocs) cudaFree(p);
+    c->proxAllocs.clear();
+    c->hxptr.clear();
+    c->hxcol.clear();
+    B.n_pinst = B.n_pfix = B.n_pb = B.n_pdiag = B.n_px = 0;
+    B.pinst = nullptr;
+    B.prec = nullptr;
+    B.pfix_slot = B.pfix_ptr = B.pb_row = B.pb_ptr = B.pdiag_row = nullptr;
+    B.pfix_code = B.pb_code = B.xcode = nullptr;
+    B.xptr = B.xcol = B.xcptr = nullptr;
+    B.xval = nullptr;
+    B.sheet_prox = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Per (proximity, sheet it touches) one instance; its 3x3 contributions are listed per target
+// in the order Cloth::addProximityForces accumulates them (Cloth.cu:171-192 through
+// addElement's coeffRef, Cloth.cu:42-76): proximity, impulse before friction, row corner,
+// column corner.  Targets are pattern slots (summed onto the gathered block), right-hand-side
+// rows, and blocks outside the mesh pattern (kept in a row-sorted side list).
+cs_status cs_set_proximities(cs_ctx* c, const cs_proximity_desc* px, int n, float thickness) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    if (n < 0 || (n > 0 && !px)) return fail(c, CS_ERR_INVALID_ARG, "bad proximity list");
+    if (n > 0 && !(std::isfinite(thickness) && thickness > 0.0f))
+        return fail(c, CS_ERR_INVALID_ARG, "repulsion thickness must be positive");
+    Batch& B = c->B;
+    auto finite = [](const float* a, int k) {
+        for (int i = 0; i < k; i++)
+            if (!std::isfinite(a[i])) return false;
+        return true;
+    };
+    for (int p = 0; p < n; p++) {
+        const cs_proximity_desc& d = px[p];
+        for (int i = 0; i < 4; i++) {
+            if (d.nodes[i] < -1 || d.nodes[i] >= B.N)
+                return fail(c, CS_ERR_INVALID_ARG, "proximity %d: node %d out of range", p, d.nodes[i]);
+            if (d.nodes[i] < 0 && !(finite(d.x[i], 3) && finite(d.v[i], 3)))
+                return fail(c, CS_ERR_INVALID_ARG, "proximity %d: non-finite outside point", p);
+            if (d.nodes[i] < 0 && ((d.free_mask >> i) & 1) && !(std::isfinite(d.mass[i]) && d.mass[i] > 0.0f))
+                return fail(c, CS_ERR_INVALID_ARG, "proximity %d: free outside point without a positive mass", p);
+        }
+        if (!finite(d.normal, 3) || !finite(d.w, 4) || !std::isfinite(d.mu) || !std::isfinite(d.stiffness))
+            return fail(c, CS_ERR_INVALID_ARG, "proximity %d: non-finite normal, weights or coefficients", p);
+    }
+    CS_CUDA(cudaSetDevice(c->device));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    destroyGraphs(c);  // the captured launches hold the old lists
+    clearProximities(c);
+
+    const int S = B.S;
+    std::vector<int> offs(S);
+    for (int s = 0; s < S; s++) offs[s] = c->sheets[s].node_off;
+    auto sheetOf = [&](int node) { return (int)(std::upper_bound(offs.begin(), offs.end(), node) - offs.begin()) - 1; };
+    std::vector<ProxInst> inst;
+    std::vector<int> touched(S, 0);
+    for (int p = 0; p < n; p++) {
+        const cs_proximity_desc& d = px[p];
+        int sh[4];
+        for (int i = 0; i < 4; i++) sh[i] = d.nodes[i] >= 0 ? sheetOf(d.nodes[i]) : -1;
+        for (int i = 0; i < 4; i++) {
+            if (sh[i] < 0) continue;
+            bool seen = false;
+            for (int k = 0; k < i; k++) seen |= sh[k] == sh[i];
+            if (seen) continue;
+            ProxInst I{};
+            I.sheet = sh[i];
+            I.local = 0;
+            for (int k = 0; k < 4; k++) {
+                I.node[k] = d.nodes[k];
+                if (sh[k] == sh[i]) I.local |= 1 << k;
+                for (int e = 0; e < 3; e++) {
+                    I.xe[k][e] = d.x[k][e];
+                    I.ve[k][e] = d.v[k][e];
+                }
+                I.me[k] = d.mass[k];
+                I.w[k] = d.w[k];
+            }
+            I.free_mask = d.free_mask;
+            I.thickness = thickness;
+            for (int e = 0; e < 3; e++) I.n[e] = d.normal[e];
+            I.mu = d.mu;
+            I.stiffness = d.stiffness;
+            inst.push_back(I);
+            touched[sh[i]] = 1;
+        }
+    }
+    if ((long long)inst.size() >= (1LL << 26)) return fail(c, CS_ERR_INVALID_ARG, "too many proximities");
+    if (!inst.empty()) {
+        std::map<int, std::vector<uint32_t>> fix, rhs;
+        std::map<std::pair<int, int>, std::vector<uint32_t>> extra;
+        std::map<int, int> diag;
+        for (size_t t = 0; t < inst.size(); t++) {
+            const ProxInst& I = inst[t];
+            const SheetDesc& sd = c->sheets[I.sheet];
+            const Topo& T = *c->sheetTopo[I.sheet];
+            const int panelBase = c->slices[sd.slice_off].panel0 - T.slice_tpanel0[0];
+            auto slotOf = [&](int i, int j) {
+                const int* lo = T.csr_col.data() + T.csr_ptr[i];
+                const int* hi = T.csr_col.data() + T.csr_ptr[i + 1];
+                const int* q = std::lower_bound(lo, hi, j);
+                if (q == hi || *q != j) return -1;
+                const int slot = T.csr_slot[q - T.csr_col.data()];
+                return (panelBase + slot / CS_SLICE) * CS_SLICE + slot % CS_SLICE;
+            };
+            for (int fr = 0; fr < 2; fr++)
+                for (int a = 0; a < 4; a++) {
+                    if (!((I.local >> a) & 1)) continue;
+                    const int row = I.node[a], i = row - sd.node_off;
+                    rhs[row].push_back(cs_pcode((int)t, fr, a, 0));
+                    diag[row] = slotOf(i, i);
+                    if (diag[row] < 0) return fail(c, CS_ERR_STATE, "node %d: no diagonal block in the pattern", row);
+                    for (int b = 0; b < 4; b++) {
+                        if (!((I.local >> b) & 1)) continue;
+                        const int col = I.node[b];
+                        const uint32_t code = cs_pcode((int)t, fr, a, b);
+                        const int slot = slotOf(i, col - sd.node_off);
+                        if (slot >= 0) fix[slot].push_back(code);
+                        else extra[{row, col}].push_back(code);
+                    }
+                }
+        }
+        std::vector<int> fslot, fptr{0}, brow, bptr{0}, drow, xcptr{0};
+        std::vector<uint32_t> fcode, bcode, xcode;
+        for (auto& kv : fix) {
+            fslot.push_back(kv.first);
+            fcode.insert(fcode.end(), kv.second.begin(), kv.second.end());
+            fptr.push_back((int)fcode.size());
+        }
+        for (auto& kv : rhs) {
+            brow.push_back(kv.first);
+            bcode.insert(bcode.end(), kv.second.begin(), kv.second.end());
+            bptr.push_back((int)bcode.size());
+        }
+        for (auto& kv : diag) {
+            drow.push_back(kv.first);
+            drow.push_back(kv.second);
+        }
+        cs_status st;
+#define PUP(field, vec) \
+    if ((st = proxUpload(c, &B.field, vec)) != CS_OK) return st;
+        PUP(pfix_slot, fslot);
+        PUP(pfix_ptr, fptr);
+        PUP(pfix_code, fcode);
+        PUP(pb_row, brow);
+        PUP(pb_ptr, bptr);
+        PUP(pb_code, bcode);
+        PUP(pdiag_row, drow);
+        if (!extra.empty()) {
+            c->hxptr.assign(B.N + 1, 0);
+            for (auto& kv : extra) {
+                c->hxptr[kv.first.first + 1]++;
+                c->hxcol.push_back(kv.first.second);
+                xcode.insert(xcode.end(), kv.second.begin(), kv.second.end());
+                xcptr.push_back((int)xcode.size());
+            }
+            for (int r = 0; r < B.N; r++) c->hxptr[r + 1] += c->hxptr[r];
+            PUP(xptr, c->hxptr);
+            PUP(xcol, c->hxcol);
+            PUP(xcptr, xcptr);
+            PUP(xcode, xcode);
+            PUP(xval, std::vector<float>(9 * extra.size(), 0.0f));
+        }
+        ProxInst* dinst = nullptr;
+        PUP(prec, std::vector<float>(CS_PROX_REC * inst.size(), 0.0f));
+        if ((st = proxUpload(c, &dinst, inst)) != CS_OK) return st;
+        PUP(sheet_prox, touched);
+#undef PUP
+        B.pinst = dinst;
+        B.n_pinst = (int)inst.size();
+        B.n_pfix = (int)fslot.size();
+        B.n_pb = (int)brow.size();
+        B.n_pdiag = (int)diag.size();
+        B.n_px = (int)extra.size();
+    }
+    // sheets with proximities leave the cluster-resident solver (their systems carry blocks
+    // outside the pattern, which only the batched loop's SpMV reads)
+    std::vector<int> rl;
+    for (int s : c->rlistAll)
+        if (!touched[s]) rl.push_back(s);
+    if (!rl.empty()) CS_CUDA(cudaMemcpy(B.rlist, rl.data(), rl.size() * sizeof(int), cudaMemcpyHostToDevice));
+    B.n_resident = (int)rl.size();
+    c->resClusters = std::min(c->resClustersMax, B.n_resident);
     return CS_OK;
 }
 
@@ -1276,7 +1522,8 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
     if (p->use_graph) {
         c->graphSteps++;
         c->graphLaunchesFixed += (c->B.F ? 1 : 0) + (c->B.E ? 1 : 0) + 1 + 3 + (learned ? 3 : 0) +
-                                 (c->resClusters > 0 ? 1 : 0);
+                                 (c->resClusters > 0 ? 1 : 0) +
+                                 (c->B.n_pinst > 0 ? 5 + (c->B.n_px > 0 ? 1 : 0) : 0);
     }
     if (!stats) return CS_OK;
     std::vector<InstState> inst(c->B.S);
@@ -1354,6 +1601,9 @@ cs_status cs_get_system(cs_ctx* c, int32_t* row_ptr, int32_t* col, float* val, f
     std::vector<float> A((size_t)B.n_panels * CS_PANEL_FLOATS);
     CS_CUDA(cudaMemcpy(A.data(), B.A, A.size() * sizeof(float), cudaMemcpyDeviceToHost));
     if (b) CS_CUDA(cudaMemcpy(b, B.b, 3 * (size_t)B.N * sizeof(float), cudaMemcpyDeviceToHost));
+    // proximity blocks outside the pattern, merged into each row in column order
+    std::vector<float> X(9 * (size_t)B.n_px);
+    if (B.n_px > 0) CS_CUDA(cudaMemcpy(X.data(), B.xval, X.size() * sizeof(float), cudaMemcpyDeviceToHost));
     long long pos = 0;
     int rowBase = 0;
     if (row_ptr) row_ptr[0] = 0;
@@ -1362,7 +1612,17 @@ cs_status cs_get_system(cs_ctx* c, int32_t* row_ptr, int32_t* col, float* val, f
         const SheetDesc& sd = c->sheets[s];
         int panelBase = c->slices[sd.slice_off].panel0 - T.slice_tpanel0[0];
         for (int i = 0; i < T.n_nodes; i++) {
+            const int row = rowBase + i;
+            int m = B.n_px > 0 ? c->hxptr[row] : 0;
+            const int mEnd = B.n_px > 0 ? c->hxptr[row + 1] : 0;
+            auto putExtra = [&]() {
+                if (col) col[pos] = c->hxcol[m];
+                if (val) std::copy(X.begin() + 9 * (size_t)m, X.begin() + 9 * (size_t)m + 9, val + 9 * pos);
+                pos++;
+                m++;
+            };
             for (int p = T.csr_ptr[i]; p < T.csr_ptr[i + 1]; p++) {
+                while (m < mEnd && c->hxcol[m] < rowBase + T.csr_col[p]) putExtra();
                 int slot = T.csr_slot[p];
                 int lane = slot % CS_SLICE, panel = panelBase + slot / CS_SLICE;
                 const float* P = A.data() + (size_t)panel * CS_PANEL_FLOATS;
@@ -1375,7 +1635,8 @@ cs_status cs_get_system(cs_ctx* c, int32_t* row_ptr, int32_t* col, float* val, f
                 }
                 pos++;
             }
-            if (row_ptr) row_ptr[rowBase + i + 1] = (int32_t)pos;
+            while (m < mEnd) putExtra();
+            if (row_ptr) row_ptr[row + 1] = (int32_t)pos;
         }
         rowBase += T.n_nodes;
     }

@@ -49,6 +49,47 @@ __device__ __forceinline__ float maxf_(float a, float b) { return a > b ? a : b;
 __device__ __forceinline__ float minf_(float a, float b) { return a < b ? a : b; }
 __device__ __forceinline__ float absf_(float a) { return a < 0.0f ? -a : a; }
 
+// 3x3 block-Jacobi inverse in double (adjugate / determinant), stored in float.
+__device__ __forceinline__ void block_inverse(const float a[9], float* Pi) {
+    const double m00 = a[0], m01 = a[1], m02 = a[2], m10 = a[3], m11 = a[4], m12 = a[5], m20 = a[6], m21 = a[7],
+                 m22 = a[8];
+    const double c00 = m11 * m22 - m12 * m21, c01 = m12 * m20 - m10 * m22, c02 = m10 * m21 - m11 * m20;
+    const double det = m00 * c00 + m01 * c01 + m02 * c02;
+    const double id = det != 0.0 ? 1.0 / det : 0.0;
+    Pi[0] = (float)(c00 * id);
+    Pi[1] = (float)((m02 * m21 - m01 * m22) * id);
+    Pi[2] = (float)((m01 * m12 - m02 * m11) * id);
+    Pi[3] = (float)(c01 * id);
+    Pi[4] = (float)((m00 * m22 - m02 * m20) * id);
+    Pi[5] = (float)((m02 * m10 - m00 * m12) * id);
+    Pi[6] = (float)(c02 * id);
+    Pi[7] = (float)((m01 * m20 - m00 * m21) * id);
+    Pi[8] = (float)((m00 * m11 - m01 * m10) * id);
+}
+
+// A SELL panel slot (panel * 32 + lane) as a row-major 3x3 block.
+__device__ __forceinline__ void load_slot(const float* A, int slot, float a[9]) {
+    const float* pn = A + (size_t)(slot >> 5) * CS_PANEL_FLOATS;
+    const int lane = slot & 31;
+    for (int e = 0; e < 4; e++) a[e] = pn[4 * lane + e];
+    for (int e = 0; e < 4; e++) a[4 + e] = pn[128 + 4 * lane + e];
+    a[8] = pn[256 + lane];
+}
+__device__ __forceinline__ void store_slot(float* A, int slot, const float a[9]) {
+    float* pn = A + (size_t)(slot >> 5) * CS_PANEL_FLOATS;
+    const int lane = slot & 31;
+    for (int e = 0; e < 4; e++) pn[4 * lane + e] = a[e];
+    for (int e = 0; e < 4; e++) pn[128 + 4 * lane + e] = a[4 + e];
+    pn[256 + lane] = a[8];
+}
+
+// The 3x3 block (a, b) of a proximity contribution code (cs_pcode) from its record.
+__device__ __forceinline__ const float* prox_block(const Batch& B, uint32_t code, int& rowstride) {
+    const int inst = (int)(code >> 5), fr = (code >> 4) & 1, a = (code >> 2) & 3, b = code & 3;
+    rowstride = 12;
+    return B.prec + (size_t)inst * CS_PROX_REC + fr * 144 + (3 * a) * 12 + 3 * b;
+}
+
 // Material::stretchingStiffness (Material.cu:91-124): trilinear lookup on the 30^3 table.
 __device__ __forceinline__ float4 stretch_stiffness(const float4* __restrict__ T, float G00, float G01, float G11) {
     const float hi = (float)(CS_TABLE_N - 1) - 1e-6f;
@@ -456,22 +497,7 @@ __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
                 B.b[3 * row + 1] = b1;
                 B.b[3 * row + 2] = b2;
                 bsq = (double)b0 * b0 + (double)b1 * b1 + (double)b2 * b2;
-                // 3x3 block-Jacobi inverse in double, stored in float.
-                const double m00 = a[0], m01 = a[1], m02 = a[2], m10 = a[3], m11 = a[4], m12 = a[5], m20 = a[6],
-                             m21 = a[7], m22 = a[8];
-                const double c00 = m11 * m22 - m12 * m21, c01 = m12 * m20 - m10 * m22, c02 = m10 * m21 - m11 * m20;
-                const double det = m00 * c00 + m01 * c01 + m02 * c02;
-                const double id = det != 0.0 ? 1.0 / det : 0.0;
-                float* Pi = B.Pinv + 9 * (size_t)row;
-                Pi[0] = (float)(c00 * id);
-                Pi[1] = (float)((m02 * m21 - m01 * m22) * id);
-                Pi[2] = (float)((m01 * m12 - m02 * m11) * id);
-                Pi[3] = (float)(c01 * id);
-                Pi[4] = (float)((m00 * m22 - m02 * m20) * id);
-                Pi[5] = (float)((m02 * m10 - m00 * m12) * id);
-                Pi[6] = (float)(c02 * id);
-                Pi[7] = (float)((m01 * m20 - m00 * m21) * id);
-                Pi[8] = (float)((m00 * m11 - m01 * m10) * id);
+                block_inverse(a, B.Pinv + 9 * (size_t)row);
             }
         }
 #pragma unroll
@@ -497,4 +523,173 @@ __global__ void __launch_bounds__(128) cs_expand_kernel(Batch B, float* face_f, 
             for (int q = 0; q < 12; q++) edge_J[144 * (size_t)i + 12 * p + q] = coef * (r[p] * r[q]);
         }
     }
+}
+
+// ---------------------------------------------------------------------------------------
+// Proximity terms (Cloth::addProximityForces, Cloth.cu:171-192), one thread per (proximity,
+// sheet) instance: penetration depth below the thickness, the impulse and friction forces
+// and Jacobians of impulseForce / frictionForce (PhysicsHelper.cu:398-432) in FP32 with the
+// reference's operation order (this file is built without FMA contraction), written as the
+// element blocks -dt^2 J_imp, -dt J_fr and right-hand sides dt (f_imp + dt J_imp v), dt f_fr.
+__global__ void __launch_bounds__(128) cs_prox_kernel(Batch B) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= B.n_pinst) return;
+    const ProxInst& P = B.pinst[t];
+    const float dt = B.params->dt;
+    const float th = P.thickness;
+    f3 xs[4], vs[4];
+    float ms[4];
+    int freeMask = 0;
+    for (int i = 0; i < 4; i++) {
+        const int nd = P.node[i];
+        if (nd >= 0) {
+            xs[i] = ld3(B.x, nd);
+            vs[i] = ld3(B.v, nd);
+            ms[i] = B.mass[nd];
+            freeMask |= 1 << i;  // cloth nodes are free (Mesh.cu:349)
+        } else {
+            xs[i] = mk(P.xe[i][0], P.xe[i][1], P.xe[i][2]);
+            vs[i] = mk(P.ve[i][0], P.ve[i][1], P.ve[i][2]);
+            ms[i] = P.me[i];
+            if ((P.free_mask >> i) & 1) freeMask |= 1 << i;
+        }
+    }
+    const f3 n = mk(P.n[0], P.n[1], P.n[2]);
+    // d = max(h - sum_i w_i n.x_i, 0) (Cloth.cu:179-182)
+    float d = -th;
+    for (int i = 0; i < 4; i++) d += P.w[i] * dot(n, xs[i]);
+    d = maxf_(-d, 0.0f);
+    float* rec = B.prec + (size_t)t * CS_PROX_REC;
+    // impulseForce: f = 1/2 k/h d^2 N, J = -k/h d N N^T
+    float N[12], vel[12];
+    for (int i = 0; i < 4; i++) {
+        N[3 * i] = P.w[i] * n.x;
+        N[3 * i + 1] = P.w[i] * n.y;
+        N[3 * i + 2] = P.w[i] * n.z;
+        vel[3 * i] = vs[i].x;
+        vel[3 * i + 1] = vs[i].y;
+        vel[3 * i + 2] = vs[i].z;
+    }
+    const float sf = 0.5f * P.stiffness / th * (d * d);
+    const float sj = -P.stiffness / th * d;
+    const float s2 = -dt * dt;
+    for (int p = 0; p < 12; p++) {
+        float jv = 0.0f;
+        for (int q = 0; q < 12; q++) {
+            const float J = sj * (N[p] * N[q]);
+            rec[12 * p + q] = s2 * J;
+            jv += (dt * J) * vel[q];
+        }
+        rec[288 + p] = dt * (sf * N[p] + jv);
+    }
+    // frictionForce: F = 1/2 k/h d^2; vt = (I - n n^T) sum_i w_i v_i;
+    // f_v = min(mu F / |vt|, 1 / (dt sum_free w_i^2 / m_i)); f = -f_v (w_i vt);
+    // J_ij = -f_v w_i w_j (I - n n^T)
+    const float F = 0.5f * P.stiffness / th * (d * d);
+    f3 v = mk(0.0f, 0.0f, 0.0f);
+    float invMass = 0.0f;
+    for (int i = 0; i < 4; i++) {
+        v = add(v, scl(P.w[i], vs[i]));
+        if ((freeMask >> i) & 1) invMass += (P.w[i] * P.w[i]) / ms[i];
+    }
+    float T[3][3];
+    const float nn[3] = {n.x, n.y, n.z};
+    for (int k = 0; k < 3; k++)
+        for (int h = 0; h < 3; h++) T[k][h] = (k == h ? 1.0f : 0.0f) - nn[k] * nn[h];
+    const float vv[3] = {v.x, v.y, v.z};
+    float vt[3];
+    for (int k = 0; k < 3; k++) {
+        float acc = 0.0f;
+        for (int h = 0; h < 3; h++) acc += T[k][h] * vv[h];
+        vt[k] = acc;
+    }
+    const float vtn = sqrtf(0.0f + vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
+    const float f_v = minf_(P.mu * F / vtn, 1.0f / (dt * invMass));
+    const float s1 = -dt;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+            const float s = -f_v * P.w[i] * P.w[j];
+            for (int k = 0; k < 3; k++)
+                for (int h = 0; h < 3; h++) rec[144 + (3 * i + k) * 12 + 3 * j + h] = s1 * (s * T[k][h]);
+        }
+    for (int i = 0; i < 4; i++)
+        for (int c = 0; c < 3; c++) rec[300 + 3 * i + c] = dt * (-f_v * (P.w[i] * vt[c]));
+}
+
+// Proximity blocks into the pattern slots they fall on, in order after the gather's sums.
+__global__ void cs_prox_fix_kernel(Batch B) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= B.n_pfix) return;
+    const int slot = B.pfix_slot[m];
+    float a[9];
+    load_slot(B.A, slot, a);
+    for (int c = B.pfix_ptr[m]; c < B.pfix_ptr[m + 1]; c++) {
+        int rs;
+        const float* blk = prox_block(B, B.pfix_code[c], rs);
+        for (int k = 0; k < 3; k++)
+            for (int h = 0; h < 3; h++) a[3 * k + h] += blk[k * rs + h];
+    }
+    store_slot(B.A, slot, a);
+}
+
+// Proximity right-hand sides, in order after the gather's (handles last there).
+__global__ void cs_prox_rhs_kernel(Batch B) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= B.n_pb) return;
+    const int row = B.pb_row[m];
+    float b0 = B.b[3 * row], b1 = B.b[3 * row + 1], b2 = B.b[3 * row + 2];
+    for (int c = B.pb_ptr[m]; c < B.pb_ptr[m + 1]; c++) {
+        const uint32_t code = B.pb_code[c];
+        const int inst = (int)(code >> 5), fr = (code >> 4) & 1, a = (code >> 2) & 3;
+        const float* r = B.prec + (size_t)inst * CS_PROX_REC + (fr ? 300 : 288) + 3 * a;
+        b0 += r[0];
+        b1 += r[1];
+        b2 += r[2];
+    }
+    B.b[3 * row] = b0;
+    B.b[3 * row + 1] = b1;
+    B.b[3 * row + 2] = b2;
+}
+
+// Block-Jacobi inverse of the rows whose diagonal block received proximity terms
+// (pdiag_row: row, diagonal slot pairs).
+__global__ void cs_prox_diag_kernel(Batch B) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= B.n_pdiag) return;
+    const int row = B.pdiag_row[2 * m], slot = B.pdiag_row[2 * m + 1];
+    float a[9];
+    load_slot(B.A, slot, a);
+    block_inverse(a, B.Pinv + 9 * (size_t)row);
+}
+
+// Blocks outside the pattern: sums of their contributions in order.
+__global__ void cs_prox_extra_kernel(Batch B) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= B.n_px) return;
+    float a[9];
+    for (int e = 0; e < 9; e++) a[e] = 0.0f;
+    for (int c = B.xcptr[m]; c < B.xcptr[m + 1]; c++) {
+        int rs;
+        const float* blk = prox_block(B, B.xcode[c], rs);
+        for (int k = 0; k < 3; k++)
+            for (int h = 0; h < 3; h++) a[3 * k + h] += blk[k * rs + h];
+    }
+    for (int e = 0; e < 9; e++) B.xval[9 * (size_t)m + e] = a[e];
+}
+
+// ||b||^2 per slice after the proximity right-hand sides (the gather's partials otherwise).
+__global__ void __launch_bounds__(128) cs_slice_bnorm_kernel(Batch B) {
+    const int slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (slice >= B.n_slices) return;
+    const SliceDesc sd = B.slices[slice];
+    double bsq = 0.0;
+    if (lane < sd.rows) {
+        const int row = sd.row0 + B.rowmap[sd.topo_slice * CS_SLICE + lane];
+        const float b0 = B.b[3 * row], b1 = B.b[3 * row + 1], b2 = B.b[3 * row + 2];
+        bsq = (double)b0 * b0 + (double)b1 * b1 + (double)b2 * b2;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bsq += __shfl_xor_sync(0xffffffffu, bsq, o);
+    if (lane == 0) B.part[2 * slice] = bsq;
 }

@@ -83,6 +83,22 @@ __global__ void __launch_bounds__(128) cs_spmv_kernel(Batch B) {
                 y1 += a0.w * p0 + a1.x * p1 + a1.y * p2;
                 y2 += a1.z * p0 + a1.w * p1 + a8 * p2;
             }
+            if (B.xptr) {
+                // proximity blocks outside the pattern (cs_set_proximities)
+                for (int m = B.xptr[row]; m < B.xptr[row + 1]; m++) {
+                    const int col = B.xcol[m];
+                    const float* a = B.xval + 9 * (size_t)m;
+                    float p0 = z[3 * col], p1 = z[3 * col + 1], p2 = z[3 * col + 2];
+                    if (beta != 0.f) {
+                        p0 = __fmaf_rn(beta, pOld[3 * col], p0);
+                        p1 = __fmaf_rn(beta, pOld[3 * col + 1], p1);
+                        p2 = __fmaf_rn(beta, pOld[3 * col + 2], p2);
+                    }
+                    y0 += a[0] * p0 + a[1] * p1 + a[2] * p2;
+                    y1 += a[3] * p0 + a[4] * p1 + a[5] * p2;
+                    y2 += a[6] * p0 + a[7] * p1 + a[8] * p2;
+                }
+            }
             float p0 = z[3 * row], p1 = z[3 * row + 1], p2 = z[3 * row + 2];
             if (beta != 0.f) {
                 p0 = __fmaf_rn(beta, pOld[3 * row], p0);
@@ -122,6 +138,18 @@ __global__ void __launch_bounds__(128) cs_spmv_kernel(Batch B) {
                 y0 += (double)a0.x * d0 + (double)a0.y * d1 + (double)a0.z * d2;
                 y1 += (double)a0.w * d0 + (double)a1.x * d1 + (double)a1.y * d2;
                 y2 += (double)a1.z * d0 + (double)a1.w * d1 + (double)a8 * d2;
+            }
+            if (B.xptr) {
+                for (int m = B.xptr[row]; m < B.xptr[row + 1]; m++) {
+                    const int col = B.xcol[m];
+                    const float* a = B.xval + 9 * (size_t)m;
+                    const double d0 = B.dv64[3 * col] + (double)B.e[3 * col];
+                    const double d1 = B.dv64[3 * col + 1] + (double)B.e[3 * col + 1];
+                    const double d2 = B.dv64[3 * col + 2] + (double)B.e[3 * col + 2];
+                    y0 += (double)a[0] * d0 + (double)a[1] * d1 + (double)a[2] * d2;
+                    y1 += (double)a[3] * d0 + (double)a[4] * d1 + (double)a[5] * d2;
+                    y2 += (double)a[6] * d0 + (double)a[7] * d1 + (double)a[8] * d2;
+                }
             }
             double r0 = (double)B.b[3 * row] - y0, r1 = (double)B.b[3 * row + 1] - y1, r2 = (double)B.b[3 * row + 2] - y2;
             B.r[3 * row] = (float)r0;
@@ -374,7 +402,7 @@ __global__ void __launch_bounds__(128) cs_solve_setup_kernel(Batch B) {
         I.resnorm = I.first_res = -1.0;
         I.alpha = I.beta = 0.f;
         I.sweep_iters = I.iters = I.sweeps = I.flags = 0;
-        if (sh.resident && B.params->solver == CS_SOLVER_AUTO_DEV)
+        if (sh.resident && B.params->solver == CS_SOLVER_AUTO_DEV && !(B.sheet_prox && B.sheet_prox[s]))
             I.phase = PH_RESIDENT;  // solved by cs_resident_pcg_kernel before the loop runs
         else
             I.phase = B.params->warm ? PH_RES : PH_INIT;
@@ -424,6 +452,16 @@ __global__ void __launch_bounds__(128) cs_spmv_plain_kernel(Batch B, const float
         y0 += a0.x * p0 + a0.y * p1 + a0.z * p2;
         y1 += a0.w * p0 + a1.x * p1 + a1.y * p2;
         y2 += a1.z * p0 + a1.w * p1 + a8 * p2;
+    }
+    if (B.xptr) {
+        for (int m = B.xptr[row]; m < B.xptr[row + 1]; m++) {
+            const int col = B.xcol[m];
+            const float* a = B.xval + 9 * (size_t)m;
+            const float p0 = x[3 * col], p1 = x[3 * col + 1], p2 = x[3 * col + 2];
+            y0 += a[0] * p0 + a[1] * p1 + a[2] * p2;
+            y1 += a[3] * p0 + a[4] * p1 + a[5] * p2;
+            y2 += a[6] * p0 + a[7] * p1 + a[8] * p2;
+        }
     }
     y[3 * row] = y0;
     y[3 * row + 1] = y1;

@@ -37,7 +37,7 @@ EXPORTED = [
     "cs_device_pointers", "cs_profile_kernels", "cs_get_counters", "cs_get_stream",
     "cs_solve_block_csr_noalloc", "cs_tc_gemm_check", "cs_mlp_init", "cs_mlp_record", "cs_mlp_fit_normalization",
     "cs_mlp_train", "cs_mlp_gradient", "cs_mlp_predict", "cs_mlp_get_record", "cs_mlp_get_weights",
-    "cs_mlp_set_weights", "cs_get_solver_info",
+    "cs_mlp_set_weights", "cs_get_solver_info", "cs_set_proximities",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -89,6 +89,32 @@ class StepStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+# cs_proximity_desc, field for field (all 4-byte members: no padding)
+PROXIMITY_DTYPE = np.dtype([
+    ("nodes", "<i4", (4,)), ("x", "<f4", (4, 3)), ("v", "<f4", (4, 3)), ("mass", "<f4", (4,)),
+    ("free_mask", "<i4"), ("normal", "<f4", (3,)), ("w", "<f4", (4,)), ("mu", "<f4"), ("stiffness", "<f4"),
+])
+assert PROXIMITY_DTYPE.itemsize == 168
+
+
+def proximity_records(prox: dict) -> np.ndarray:
+    """cs_proximity_desc array from a dict of arrays: nodes (n, 4) batch node ids or -1, x, v
+    (n, 4, 3) and mass (n, 4) of the points outside the batch, free (n,) bit mask, normal
+    (n, 3), w (n, 4), mu (n,), stiffness (n,)."""
+    n = len(prox["mu"])
+    rec = np.zeros(n, PROXIMITY_DTYPE)
+    rec["nodes"] = np.asarray(prox["nodes"]).reshape(n, 4)
+    rec["x"] = np.asarray(prox["x"]).reshape(n, 4, 3)
+    rec["v"] = np.asarray(prox["v"]).reshape(n, 4, 3)
+    rec["mass"] = np.asarray(prox["mass"]).reshape(n, 4)
+    rec["free_mask"] = np.asarray(prox["free"]).reshape(n)
+    rec["normal"] = np.asarray(prox["normal"]).reshape(n, 3)
+    rec["w"] = np.asarray(prox["w"]).reshape(n, 4)
+    rec["mu"] = np.asarray(prox["mu"]).reshape(n)
+    rec["stiffness"] = np.asarray(prox["stiffness"]).reshape(n)
+    return rec
+
+
 _LIB = None
 
 
@@ -106,6 +132,7 @@ def load_library() -> ctypes.CDLL:
         "cs_load_batch": [vp, ctypes.POINTER(MaterialDesc), ctypes.c_int, ctypes.POINTER(SheetDesc), ctypes.c_int],
         "cs_get_sizes": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "cs_get_solver_info": [vp, ctypes.POINTER(ctypes.c_int)],
+        "cs_set_proximities": [vp, vp, ctypes.c_int, ctypes.c_float],
         "cs_set_state": [vp, _fp, _fp],
         "cs_get_state": [vp, _fp, _fp],
         "cs_set_state_device": [vp, vp, vp],
@@ -270,6 +297,15 @@ class Context:
         self.check(self.lib.cs_get_solver_info(self.h, s))
         keys = ("resident_sheets", "ctas_per_cluster", "threads_per_cta", "clusters", "panels_in_smem", "smem_bytes")
         return dict(zip(keys, [int(v) for v in s]))
+
+    def set_proximities(self, prox: dict | None, thickness: float = 0.0):
+        """Proximities of the following steps (None or an empty dict clears them); see
+        proximity_records for the arrays."""
+        rec = proximity_records(prox) if prox and len(prox["mu"]) else np.zeros(0, PROXIMITY_DTYPE)
+        self._prox = rec  # kept alive for the call only; the library copies it
+        self.check(self.lib.cs_set_proximities(self.h, rec.ctypes.data if len(rec) else None, len(rec),
+                                               float(thickness)))
+        self.sizes = self.get_sizes()
 
     def set_state(self, x=None, v=None):
         xa = _f32(x) if x is not None else None

@@ -122,7 +122,8 @@ cs_status cs_load_batch(cs_ctx* ctx, const cs_material_desc* materials, int n_ma
                         const cs_sheet_desc* sheets, int n_sheets);
 
 /* sizes[0..6] = nodes, faces, interior edges, stored 3x3 blocks (incl. padding), slices,
- * sheets, nonzero blocks of the pattern. */
+ * sheets, nonzero blocks of the system (the mesh pattern's, plus proximity blocks outside
+ * it while proximities are set). */
 cs_status cs_get_sizes(const cs_ctx* ctx, long long* sizes);
 
 /* info[0..5] = sheets solved cluster-resident, CTAs per cluster, threads per CTA, clusters
@@ -132,6 +133,36 @@ cs_status cs_get_solver_info(const cs_ctx* ctx, int* info);
 
 /* Node state of the whole batch, sheets concatenated in load order (3 floats per node). */
 cs_status cs_set_state(cs_ctx* ctx, const float* x, const float* v);
+
+/* One proximity as Cloth::physicsStep receives it (Proximity.cuh:11-21; built by the
+ * collision detection the reference runs before the step, Simulator.cu:300-349): four
+ * points with weights w (vertex-face: 1 and minus the face point's barycentric weights;
+ * edge-edge: 1-s, s, -(1-t), -t), a unit normal, a friction coefficient and a stiffness
+ * already scaled by the smaller area (Proximity.cu:5-24).  nodes[i] is a node of the batch
+ * (its sheet's node_off + local index) or -1 for a point outside the batch (an obstacle's
+ * node), whose position, velocity, mass and free flag (bit i of free_mask) are given here. */
+typedef struct cs_proximity_desc {
+    int nodes[4];
+    float x[4][3];
+    float v[4][3];
+    float mass[4];
+    int free_mask;
+    float normal[3];
+    float w[4];
+    float mu;
+    float stiffness;
+} cs_proximity_desc;
+
+/* Proximities of the following steps (until the next call; n = 0 clears them) and the
+ * repulsion thickness (Magic::repulsionThickness, Magic.cu:9).  Each step then adds the
+ * repulsion and friction terms of Cloth::addProximityForces (Cloth.cu:171-192) to every
+ * sheet that holds one of a proximity's nodes, after the handle terms, in proximity order;
+ * nodes of other sheets enter a sheet's terms through their state at the start of the step
+ * (the reference steps cloths one after another, so a later cloth there sees an earlier
+ * cloth's updated velocities).  Blocks outside the mesh's pattern are kept beside it;
+ * cs_get_system returns them merged.  Sheets with proximities are solved by the batched
+ * loop. */
+cs_status cs_set_proximities(cs_ctx* ctx, const cs_proximity_desc* proximities, int n, float thickness);
 cs_status cs_get_state(cs_ctx* ctx, float* x, float* v);
 /* Same with device pointers (no host copy). */
 cs_status cs_set_state_device(cs_ctx* ctx, const float* x, const float* v);
