@@ -209,4 +209,39 @@ struct Batch {
     int* sheet_prox = nullptr;    // per sheet: 1 if a proximity touches it (batched loop this step)
 };
 
+// Proximity detection (contact.cu, cs_detect_proximities).  Scene-wide ids: nodes and faces as
+// in Batch, edges (every edge, not only interior ones) of all sheets concatenated in sheet order.
+struct ContactRec {
+    int nodes[4];
+    float n[3], w[4], mu, stiffness, depth;
+    int kind;  // 0 node key, 1 edge key, 2 face key
+    int pad[3];
+};
+
+struct Contact {
+    int E = 0;               // edges
+    int n_keys = 0;          // 2 N + 2 E + 2 F
+    int hash_bits = 0;       // grid buckets = 1 << hash_bits
+    float repulsion = 0.f, stiffness = 0.f, friction = 0.f;
+    const int4* face_edges = nullptr;  // 3 edges + collision group per face
+    const int4* edges = nullptr;       // node 0, node 1, face side 0, face side 1
+    const int* nf_ptr = nullptr;       // N + 1
+    const int* nf_code = nullptr;      // face << 2 | corner, faces in index order
+    const float* node_area = nullptr;  // Mesh::updateNodeGeometries (Mesh.cu:190-198)
+    const float* edge_area = nullptr;  // Edge::area (Edge.cu:89-95)
+    float* fn = nullptr;               // face normals (3 per face)
+    float* nn = nullptr;               // node normals (3 per node)
+    float* box = nullptr;              // face bounds: lo xyz, hi xyz
+    unsigned* ext = nullptr;           // [0] largest face extent (float bits), [1] error flags
+    int* head = nullptr;               // grid bucket heads (-1: empty)
+    int* next = nullptr;               // 8 entries per face: next entry in the bucket
+    unsigned long long* keys = nullptr;  // per (node|edge|face, side): distance bits << 32 | other id
+    int* block_count = nullptr;        // compaction: valid keys per block, then exclusive offsets
+    int* total = nullptr;
+    ContactRec* out = nullptr;
+    int out_cap = 0;
+};
+
+#define CS_CONTACT_ITEMS 4096  // keys per compaction block (256 threads x 16)
+
 #endif

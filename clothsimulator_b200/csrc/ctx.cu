@@ -50,6 +50,13 @@ __global__ void cs_prox_rhs_kernel(Batch B);
 __global__ void cs_prox_diag_kernel(Batch B);
 __global__ void cs_prox_extra_kernel(Batch B);
 __global__ void cs_slice_bnorm_kernel(Batch B);
+__global__ void cs_contact_face_kernel(Batch B, Contact C);
+__global__ void cs_contact_node_kernel(Batch B, Contact C);
+__global__ void cs_contact_grid_kernel(Batch B, Contact C, const int* sheet_group);
+__global__ void cs_contact_pair_kernel(Batch B, Contact C, const int* sheet_group);
+__global__ void cs_contact_count_kernel(Contact C);
+__global__ void cs_contact_scan_kernel(Contact C, int nblocks);
+__global__ void cs_contact_write_kernel(Batch B, Contact C);
 
 namespace {
 
@@ -159,6 +166,9 @@ struct Topo {
     long long nnzb = 0;
     // one-ring mesh neighbours (nodes sharing a face edge), sorted, for the learned warm start
     std::vector<int> nbr_ptr, nbr;
+    // every edge (reference order): nodes, adjacent faces per side (-1: none); per face its
+    // edges (v0 v1), (v1 v2), (v2 v0); per node its (face, corner) pairs in face order
+    std::vector<int> e_nodes, e_faces, f_edges, nf_ptr, nf_code;
 };
 
 struct TopoKey {
@@ -239,8 +249,20 @@ std::shared_ptr<Topo> buildTopo(const cs_sheet_desc& s, std::string& err) {
         init(e0, 2, f);
         init(e1, 0, f);
         init(e2, 1, f);
+        t->f_edges.insert(t->f_edges.end(), {e0, e1, e2});
     }
     const int ne = (int)eN.size() / 2;
+    t->e_nodes = eN;
+    t->e_faces = eF;
+    t->nf_ptr.assign(nn + 1, 0);
+    for (int i = 0; i < 3 * nf; i++) t->nf_ptr[t->fx[i] + 1]++;
+    for (int i = 0; i < nn; i++) t->nf_ptr[i + 1] += t->nf_ptr[i];
+    t->nf_code.resize(3 * (size_t)nf);
+    {
+        std::vector<int> fill(t->nf_ptr.begin(), t->nf_ptr.end() - 1);
+        for (int f = 0; f < nf; f++)
+            for (int k = 0; k < 3; k++) t->nf_code[fill[t->fx[3 * f + k]]++] = (f << 2) | k;
+    }
     for (int e = 0; e < ne; e++) {
         if (eF[2 * e] < 0 || eF[2 * e + 1] < 0) continue;
         int n0 = eN[2 * e], n1 = eN[2 * e + 1];
@@ -560,6 +582,12 @@ struct cs_ctx {
     // blocks outside the pattern that cs_get_system merges
     std::vector<void*> proxAllocs;
     std::vector<int> hxptr, hxcol;
+    std::vector<cs_proximity_desc> proxHost;  // the set in force (cs_get_proximities)
+    // proximity detection (contact.cu): static scene data built at the first detection
+    Contact contact;
+    bool contactReady = false;
+    int* sheetGroupDev = nullptr;
+    std::vector<void*> contactAllocs;
 };
 
 namespace {
@@ -618,6 +646,12 @@ void freeBatch(cs_ctx* c) {
     c->proxAllocs.clear();
     c->hxptr.clear();
     c->hxcol.clear();
+    c->proxHost.clear();
+    for (void* p : c->contactAllocs) cudaFree(p);
+    c->contactAllocs.clear();
+    c->contact = Contact();
+    c->contactReady = false;
+    c->sheetGroupDev = nullptr;
     c->rlistAll.clear();
     c->B = Batch();
     c->loaded = false;
@@ -1245,18 +1279,12 @@ void clearProximities(cs_ctx* c) {
     B.sheet_prox = nullptr;
 }
 
-}  // namespace
-
-extern "C" {
-
 // Per (proximity, sheet it touches) one instance; its 3x3 contributions are listed per target
 // in the order Cloth::addProximityForces accumulates them (Cloth.cu:171-192 through
 // addElement's coeffRef, Cloth.cu:42-76): proximity, impulse before friction, row corner,
 // column corner.  Targets are pattern slots (summed onto the gathered block), right-hand-side
 // rows, and blocks outside the mesh pattern (kept in a row-sorted side list).
-cs_status cs_set_proximities(cs_ctx* c, const cs_proximity_desc* px, int n, float thickness) {
-    if (!c) return CS_ERR_INVALID_ARG;
-    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+cs_status setProximities(cs_ctx* c, const cs_proximity_desc* px, int n, float thickness) {
     if (n < 0 || (n > 0 && !px)) return fail(c, CS_ERR_INVALID_ARG, "bad proximity list");
     if (n > 0 && !(std::isfinite(thickness) && thickness > 0.0f))
         return fail(c, CS_ERR_INVALID_ARG, "repulsion thickness must be positive");
@@ -1417,6 +1445,187 @@ cs_status cs_set_proximities(cs_ctx* c, const cs_proximity_desc* px, int n, floa
     if (!rl.empty()) CS_CUDA(cudaMemcpy(B.rlist, rl.data(), rl.size() * sizeof(int), cudaMemcpyHostToDevice));
     B.n_resident = (int)rl.size();
     c->resClusters = std::min(c->resClustersMax, B.n_resident);
+    c->proxHost.assign(px, px + n);
+    return CS_OK;
+}
+
+template <class T>
+cs_status contactAlloc(cs_ctx* c, T** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) return fail(c, CS_ERR_CUDA, "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+    c->contactAllocs.push_back(q);
+    *p = (T*)q;
+    return CS_OK;
+}
+
+// Scene-wide edges, face edges, node-face adjacency and rest areas for detection (once per batch).
+cs_status buildContact(cs_ctx* c) {
+    Batch& B = c->B;
+    Contact& C = c->contact;
+    std::vector<float> farea(B.F);
+    CS_CUDA(cudaMemcpy(farea.data(), B.face_area, B.F * sizeof(float), cudaMemcpyDeviceToHost));
+    std::vector<int4> fedges, edges;
+    std::vector<int> nfptr{0}, nfcode;
+    std::vector<float> narea(B.N, 0.0f), earea;
+    int eoff = 0;
+    for (int s = 0; s < B.S; s++) {
+        const Topo& T = *c->sheetTopo[s];
+        const SheetDesc& sd = c->sheets[s];
+        const int noff = sd.node_off, foff = sd.face_off;
+        for (int f = 0; f < T.n_faces; f++)
+            fedges.push_back(make_int4(eoff + T.f_edges[3 * f], eoff + T.f_edges[3 * f + 1], eoff + T.f_edges[3 * f + 2], s));
+        const int ne = (int)T.e_nodes.size() / 2;
+        for (int e = 0; e < ne; e++) {
+            const int f0 = T.e_faces[2 * e], f1 = T.e_faces[2 * e + 1];
+            edges.push_back(make_int4(noff + T.e_nodes[2 * e], noff + T.e_nodes[2 * e + 1], f0 < 0 ? -1 : foff + f0,
+                                      f1 < 0 ? -1 : foff + f1));
+            // Edge::area (Edge.cu:89-95)
+            float a = 0.0f;
+            if (f0 >= 0) a += farea[foff + f0];
+            if (f1 >= 0) a += farea[foff + f1];
+            earea.push_back(a);
+        }
+        for (int i = 0; i < T.n_nodes; i++) {
+            for (int k = T.nf_ptr[i]; k < T.nf_ptr[i + 1]; k++) nfcode.push_back(T.nf_code[k] + (foff << 2));
+            nfptr.push_back((int)nfcode.size());
+        }
+        // Mesh::updateNodeGeometries (Mesh.cu:190-198): a third of each face's area, faces in order
+        for (int f = 0; f < T.n_faces; f++) {
+            const float a = farea[foff + f] / 3.0f;
+            for (int k = 0; k < 3; k++) narea[noff + T.fx[3 * f + k]] += a;
+        }
+        eoff += ne;
+    }
+    C.E = eoff;
+    C.n_keys = (int)std::min<long long>(2LL * (B.N + (long long)C.E + B.F), INT32_MAX);
+    if (2LL * (B.N + (long long)C.E + B.F) >= INT32_MAX || (long long)B.F * 8 >= INT32_MAX)
+        return fail(c, CS_ERR_INVALID_ARG, "batch too large for proximity detection");
+    int bits = 10;
+    while ((1LL << bits) < 4LL * B.F && bits < 30) bits++;
+    C.hash_bits = bits;
+    cs_status st;
+    int4 *dfe = nullptr, *de = nullptr;
+    int *dnp = nullptr, *dnc = nullptr;
+    float *dna = nullptr, *dea = nullptr;
+#define CUP(ptr, vec)                                                                                    \
+    if ((st = contactAlloc(c, &ptr, vec.size())) != CS_OK) return st;                                    \
+    if (!vec.empty()) CS_CUDA(cudaMemcpy(ptr, vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice));
+    CUP(dfe, fedges);
+    CUP(de, edges);
+    CUP(dnp, nfptr);
+    CUP(dnc, nfcode);
+    CUP(dna, narea);
+    CUP(dea, earea);
+#undef CUP
+    C.face_edges = dfe;
+    C.edges = de;
+    C.nf_ptr = dnp;
+    C.nf_code = dnc;
+    C.node_area = dna;
+    C.edge_area = dea;
+#define CAL(ptr, n) \
+    if ((st = contactAlloc(c, &ptr, (size_t)(n))) != CS_OK) return st;
+    CAL(C.fn, 3LL * B.F);
+    CAL(C.nn, 3LL * B.N);
+    CAL(C.box, 6LL * B.F);
+    CAL(C.ext, 2);
+    CAL(C.head, 1LL << bits);
+    CAL(C.next, 8LL * B.F);
+    CAL(C.keys, (long long)C.n_keys);
+    CAL(C.block_count, (C.n_keys + CS_CONTACT_ITEMS - 1) / CS_CONTACT_ITEMS);
+    CAL(C.total, 1);
+    CAL(c->sheetGroupDev, B.S);
+#undef CAL
+    c->contactReady = true;
+    return CS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cs_status cs_set_proximities(cs_ctx* c, const cs_proximity_desc* px, int n, float thickness) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    return setProximities(c, px, n, thickness);
+}
+
+// Simulator::physicsStep's detection (Simulator.cu:571-586, findProximitiesGpu :300-349) on
+// the batch's current state, then cs_set_proximities with the result.
+cs_status cs_detect_proximities(cs_ctx* c, const cs_detect_params* p, int* count) {
+    if (!c || !p) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    if (!(std::isfinite(p->repulsion_thickness) && p->repulsion_thickness > 0.0f) || !std::isfinite(p->collision_stiffness) ||
+        !std::isfinite(p->friction))
+        return fail(c, CS_ERR_INVALID_ARG, "detection parameters must be finite, the thickness positive");
+    CS_CUDA(cudaSetDevice(c->device));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    cs_status st;
+    if (!c->contactReady && (st = buildContact(c)) != CS_OK) return st;
+    Batch& B = c->B;
+    Contact& C = c->contact;
+    C.repulsion = p->repulsion_thickness;
+    C.stiffness = p->collision_stiffness;
+    C.friction = p->friction;
+    std::vector<int> groups(B.S, 0);
+    if (p->sheet_group) groups.assign(p->sheet_group, p->sheet_group + B.S);
+    CS_CUDA(cudaMemcpyAsync(c->sheetGroupDev, groups.data(), B.S * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CS_CUDA(cudaMemsetAsync(C.ext, 0, 2 * sizeof(unsigned), c->stream));
+    CS_CUDA(cudaMemsetAsync(C.head, 0xFF, (sizeof(int) << C.hash_bits), c->stream));
+    CS_CUDA(cudaMemsetAsync(C.keys, 0xFF, (size_t)C.n_keys * sizeof(unsigned long long), c->stream));
+    const int nblocks = (C.n_keys + CS_CONTACT_ITEMS - 1) / CS_CONTACT_ITEMS;
+    cs_contact_face_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C);
+    cs_contact_node_kernel<<<nblk(B.N, 128), 128, 0, c->stream>>>(B, C);
+    cs_contact_grid_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C, c->sheetGroupDev);
+    cs_contact_pair_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C, c->sheetGroupDev);
+    cs_contact_count_kernel<<<nblocks, 256, 0, c->stream>>>(C);
+    cs_contact_scan_kernel<<<1, 1024, 0, c->stream>>>(C, nblocks);
+    CS_CUDA(cudaGetLastError());
+    unsigned flags[2];
+    int total = 0;
+    CS_CUDA(cudaMemcpyAsync(flags, C.ext, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaMemcpyAsync(&total, C.total, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    if (flags[1] & 1u) return fail(c, CS_ERR_INVALID_ARG, "non-finite node state");
+    if (flags[1]) return fail(c, CS_ERR_STATE, "proximity grid overflow (flags %u)", flags[1]);
+    if (total > C.out_cap) {
+        if (C.out) cudaFree(C.out);
+        C.out = nullptr;
+        C.out_cap = 0;
+        const int cap = std::max(total, 2 * C.out_cap);
+        CS_CUDA(cudaMalloc(&C.out, (size_t)std::max(cap, 1) * sizeof(ContactRec)));
+        C.out_cap = cap;
+    }
+    cs_contact_write_kernel<<<nblocks, 256, 0, c->stream>>>(B, C);
+    CS_CUDA(cudaGetLastError());
+    std::vector<ContactRec> rec(total);
+    if (total > 0)
+        CS_CUDA(cudaMemcpyAsync(rec.data(), C.out, total * sizeof(ContactRec), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    std::vector<cs_proximity_desc> desc(total);
+    for (int i = 0; i < total; i++) {
+        cs_proximity_desc& d = desc[i];
+        std::memset(&d, 0, sizeof(d));
+        for (int k = 0; k < 4; k++) {
+            d.nodes[k] = rec[i].nodes[k];
+            d.w[k] = rec[i].w[k];
+        }
+        for (int k = 0; k < 3; k++) d.normal[k] = rec[i].n[k];
+        d.mu = rec[i].mu;
+        d.stiffness = rec[i].stiffness;
+    }
+    if ((st = setProximities(c, desc.data(), total, p->repulsion_thickness)) != CS_OK) return st;
+    if (count) *count = total;
+    return CS_OK;
+}
+
+cs_status cs_get_proximities(cs_ctx* c, cs_proximity_desc* out, int cap, int* count) {
+    if (!c || (cap > 0 && !out)) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    const int n = (int)c->proxHost.size();
+    for (int i = 0; i < n && i < cap; i++) out[i] = c->proxHost[i];
+    if (count) *count = n;
     return CS_OK;
 }
 

@@ -37,7 +37,8 @@ EXPORTED = [
     "cs_device_pointers", "cs_profile_kernels", "cs_get_counters", "cs_get_stream",
     "cs_solve_block_csr_noalloc", "cs_tc_gemm_check", "cs_mlp_init", "cs_mlp_record", "cs_mlp_fit_normalization",
     "cs_mlp_train", "cs_mlp_gradient", "cs_mlp_predict", "cs_mlp_get_record", "cs_mlp_get_weights",
-    "cs_mlp_set_weights", "cs_get_solver_info", "cs_set_proximities",
+    "cs_mlp_set_weights", "cs_get_solver_info", "cs_set_proximities", "cs_detect_proximities",
+    "cs_get_proximities",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -115,6 +116,13 @@ def proximity_records(prox: dict) -> np.ndarray:
     return rec
 
 
+class DetectParams(ctypes.Structure):
+    _fields_ = [
+        ("repulsion_thickness", ctypes.c_float), ("collision_stiffness", ctypes.c_float),
+        ("friction", ctypes.c_float), ("sheet_group", ctypes.POINTER(ctypes.c_int32)),
+    ]
+
+
 _LIB = None
 
 
@@ -133,6 +141,8 @@ def load_library() -> ctypes.CDLL:
         "cs_get_sizes": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "cs_get_solver_info": [vp, ctypes.POINTER(ctypes.c_int)],
         "cs_set_proximities": [vp, vp, ctypes.c_int, ctypes.c_float],
+        "cs_detect_proximities": [vp, ctypes.POINTER(DetectParams), ctypes.POINTER(ctypes.c_int)],
+        "cs_get_proximities": [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
         "cs_set_state": [vp, _fp, _fp],
         "cs_get_state": [vp, _fp, _fp],
         "cs_set_state_device": [vp, vp, vp],
@@ -306,6 +316,30 @@ class Context:
         self.check(self.lib.cs_set_proximities(self.h, rec.ctypes.data if len(rec) else None, len(rec),
                                                float(thickness)))
         self.sizes = self.get_sizes()
+
+    def detect_proximities(self, repulsion_thickness: float = 1e-3, collision_stiffness: float = 1e9,
+                           friction: float = 0.6, groups=None) -> int:
+        """Detects proximities among the sheets' current states on the device and sets them
+        (cs_detect_proximities); sheets with equal `groups` entries interact (all when None).
+        Returns how many were found."""
+        g = None if groups is None else np.ascontiguousarray(groups, np.int32)
+        p = DetectParams(repulsion_thickness, collision_stiffness, friction,
+                         g.ctypes.data_as(_ip) if g is not None else None)
+        n = ctypes.c_int(0)
+        self.check(self.lib.cs_detect_proximities(self.h, ctypes.byref(p), ctypes.byref(n)))
+        self.sizes = self.get_sizes()
+        return n.value
+
+    def get_proximities(self) -> dict:
+        """The proximities in force, as a dict of arrays (see proximity_records)."""
+        n = ctypes.c_int(0)
+        self.check(self.lib.cs_get_proximities(self.h, None, 0, ctypes.byref(n)))
+        rec = np.zeros(n.value, PROXIMITY_DTYPE)
+        if n.value:
+            self.check(self.lib.cs_get_proximities(self.h, rec.ctypes.data, n.value, ctypes.byref(n)))
+        return {"nodes": rec["nodes"].copy(), "x": rec["x"].copy(), "v": rec["v"].copy(), "mass": rec["mass"].copy(),
+                "free": rec["free_mask"].copy(), "normal": rec["normal"].copy(), "w": rec["w"].copy(),
+                "mu": rec["mu"].copy(), "stiffness": rec["stiffness"].copy()}
 
     def set_state(self, x=None, v=None):
         xa = _f32(x) if x is not None else None

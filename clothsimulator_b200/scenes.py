@@ -283,6 +283,50 @@ def synthetic_proximities(sheet: dict, rng: np.random.Generator, n_vf: int = 6, 
     return {k: np.asarray(vv, dtype=np.int32 if k in ("nodes", "free") else np.float64) for k, vv in recs.items()}
 
 
+def folded_sheet(nq: int = 16, gap: float = 1.5e-3, seed: int = 0) -> Scene:
+    """Self-contact: a 1 m sheet of nq x nq quads (nq even) folded over itself along x = 0.5,
+    the upper half `gap` above the lower one and shifted in-plane by (0.3 h, 0.2 h) so its
+    nodes project inside the lower faces; z noise N(0, 0.1 mm).  Crease nodes stay on the
+    lower layer; the lower edge at x = 0 is pinned.  dt 1/100."""
+    assert nq % 2 == 0
+    rng = np.random.default_rng(seed)
+    s = grid_sheet(nq, rng=rng)
+    h = 1.0 / nq
+    x = s["x"].astype(np.float64)
+    upper = x[:, 0] > 0.5 + 1e-9
+    x[upper, 0] = 1.0 - x[upper, 0] + 0.3 * h
+    x[upper, 1] += 0.2 * h
+    x[upper, 2] = gap
+    x[:, 2] += rng.normal(0.0, 1e-4, size=x.shape[0])
+    s["x"] = x.astype(np.float32)
+    n = nq + 1
+    s["handles"] = (np.arange(n) * n).astype(np.int32)  # column x = 0
+    s["material"] = isotropic_material(50.0, 1e-5)
+    s["wind"] = no_wind()
+    return Scene(f"folded{nq}", [s], dt=1.0 / 100, steps=20, meta={"gap": gap})
+
+
+def stacked_sheets(nq: int = 16, gap: float = 1.5e-3, n_layers: int = 2, seed: int = 0) -> Scene:
+    """Cross-sheet contact: n_layers sheets of nq x nq quads stacked `gap` apart, each layer
+    shifted in-plane by (0.3 h, 0.2 h) from the one below, z noise N(0, 0.1 mm), top edges
+    pinned.  dt 1/100."""
+    rng = np.random.default_rng(seed)
+    sheets = []
+    h = 1.0 / nq
+    for k in range(n_layers):
+        s = grid_sheet(nq, rng=rng)
+        x = s["x"].astype(np.float64)
+        x[:, 0] += 0.3 * h * k
+        x[:, 1] += 0.2 * h * k
+        x[:, 2] = gap * k + rng.normal(0.0, 1e-4, size=x.shape[0])
+        s["x"] = x.astype(np.float32)
+        s["handles"] = top_edge(nq)
+        s["material"] = isotropic_material(50.0, 1e-5)
+        s["wind"] = no_wind()
+        sheets.append(s)
+    return Scene(f"stacked{n_layers}x{nq}", sheets, dt=1.0 / 100, steps=20, meta={"gap": gap})
+
+
 WORKLOADS = {
     "hang32": lambda seed=0: hang(32, seed),
     "precision256": lambda seed=0: precision_sheet(256, seed),

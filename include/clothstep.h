@@ -163,6 +163,28 @@ typedef struct cs_proximity_desc {
  * cs_get_system returns them merged.  Sheets with proximities are solved by the batched
  * loop. */
 cs_status cs_set_proximities(cs_ctx* ctx, const cs_proximity_desc* proximities, int n, float thickness);
+
+/* Proximity detection: what Simulator::physicsStep runs before stepping the cloths
+ * (Simulator.cu:571-586, findProximitiesGpu Simulator.cu:300-349).  Every pair of faces of
+ * sheets in one collision group whose bounds overlap after dilating one of them by
+ * 2 x repulsion_thickness is tested for vertex-face and edge-edge proximity
+ * (Simulator.cu:198-269); per (node | edge | face, side) the nearest candidate is kept
+ * (ties: the lower element index), and those nearer than 2 x repulsion_thickness become
+ * proximities (Proximity.cu:5-21) in the reference's order -- node keys, edge keys, face keys,
+ * by element index and side.  They replace the set in force as cs_set_proximities does, with
+ * repulsion_thickness as its thickness.  Runs on the device; *count receives the number. */
+typedef struct cs_detect_params {
+    float repulsion_thickness; /* Magic::repulsionThickness, default 1e-3 (Magic.cu:8) */
+    float collision_stiffness; /* Magic::collisionStiffness, default 1e9 (Magic.cu:7) */
+    float friction;            /* the scene's "friction", default 0.6 (Simulator.cu:25) */
+    const int* sheet_group;    /* per sheet; sheets with equal groups interact.  NULL: all
+                                  sheets interact, as the cloths of one scene */
+} cs_detect_params;
+cs_status cs_detect_proximities(cs_ctx* ctx, const cs_detect_params* params, int* count);
+
+/* The proximities in force (set or detected): up to cap records; *count receives how many
+ * there are. */
+cs_status cs_get_proximities(cs_ctx* ctx, cs_proximity_desc* out, int cap, int* count);
 cs_status cs_get_state(cs_ctx* ctx, float* x, float* v);
 /* Same with device pointers (no host copy). */
 cs_status cs_set_state_device(cs_ctx* ctx, const float* x, const float* v);

@@ -89,6 +89,9 @@ class Lib:
         f("cloth_set_proximities", None, [_vp, ctypes.c_int, _ip, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp,
                                           ctypes.c_double])
         f("cloth_proximity_forces", None, [_vp, ctypes.c_double, _dp, _dp, _dp, _dp, _dp])
+        f("detect_proximities", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _ip, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_double, ctypes.c_int, _ip, _dp, _dp, _dp,
+                                               _dp, _dp, _ip])
         f("run_cloths", ctypes.c_double, [ctypes.POINTER(_vp), ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, _ip])
         if which == "oracle":
@@ -291,6 +294,29 @@ class Cloth:
 
     def topology_mismatches(self) -> int:
         return self.L.cloth_topology_mismatches(self.h)
+
+
+def detect_proximities(cloths, groups=None, repulsion_thickness: float = 1e-3, collision_stiffness: float = 1e9,
+                       friction: float = 0.6) -> dict:
+    """Proximities among the cloths' current states (Simulator::findProximities): node ids
+    are scene ids, the cloths' nodes concatenated in the given order; cloths with equal
+    groups interact (all of them when groups is None).  Returns a dict of arrays nodes (n, 4),
+    normal (n, 3), w (n, 4), mu, stiffness, depth (n,) and kind (n,: 0 node key, 1 edge key,
+    2 face key), in the reference's output order."""
+    L = cloths[0].L
+    arr = (_vp * len(cloths))(*[c.h for c in cloths])
+    g = _i(np.zeros(len(cloths)) if groups is None else np.asarray(groups))
+    args = (arr, len(cloths), _ptr(g, _ip), repulsion_thickness, collision_stiffness, friction)
+    z_i, z_d = np.zeros(1, np.int32), np.zeros(1)
+    n = L.detect_proximities(*args, 0, _ptr(z_i, _ip), _ptr(z_d, _dp), _ptr(z_d, _dp), _ptr(z_d, _dp),
+                             _ptr(z_d, _dp), _ptr(z_d, _dp), _ptr(z_i, _ip))
+    out = {"nodes": np.zeros((n, 4), np.int32), "normal": np.zeros((n, 3)), "w": np.zeros((n, 4)),
+           "mu": np.zeros(n), "stiffness": np.zeros(n), "depth": np.zeros(n), "kind": np.zeros(n, np.int32)}
+    if n:
+        L.detect_proximities(*args, n, _ptr(out["nodes"], _ip), _ptr(out["normal"], _dp), _ptr(out["w"], _dp),
+                             _ptr(out["mu"], _dp), _ptr(out["stiffness"], _dp), _ptr(out["depth"], _dp),
+                             _ptr(out["kind"], _ip))
+    return out
 
 
 def run_cloths(cloths, params_list, steps: int, method: int = METHOD_LLT, threads: int = 1):

@@ -27,8 +27,15 @@
 #include "Proximity.cuh"
 #include "Vertex.cuh"
 
+#include "oracle_detect.hpp"
 #include "oracle_system.hpp"
 
+namespace {
+struct ClothBase;
+}
+// Installs the reference's own detection predicates (defined below).
+static void orcDetectHooks(orc::Detector& D, const std::vector<ClothBase*>& cloths, const orc::DetectScene& S);
+#define ORC_DETECT_HOOKS 1
 #define ORC_API(name) ref_##name
 #define ORC_NO_DEFAULT_FACTORIES 1
 #include "oracle_capi.inc"
@@ -238,3 +245,86 @@ int ref_cloth_topology_mismatches(void* cb) {
 }
 
 }  // extern "C"
+
+// Proximity detection through the reference's own signedVertexFaceDistance and
+// signedEdgeEdgeDistance (MathHelper.cu:38-69), inEdge (PhysicsHelper.cu:3-18) and Proximity
+// constructors (Proximity.cu:5-21), on each cloth's reference Node, Face and Edge objects
+// (face normals by Face::update, edge areas by Edge::area).  Node normals and areas are the
+// oracle's restatement of Mesh::updateNodeGeometries (Mesh.cu:182-203): Mesh.cu, which holds
+// it, needs the renderer and is not compiled here.
+static void orcDetectHooks(orc::Detector& D, const std::vector<ClothBase*>& cloths, const orc::DetectScene& S) {
+    struct Span {
+        RefClothImpl* c;
+        int n0, f0, e0;
+    };
+    auto spans = std::make_shared<std::vector<Span>>();
+    int n0 = 0, f0 = 0, e0 = 0;
+    for (ClothBase* b : cloths) {
+        auto* c = static_cast<RefClothImpl*>(b);
+        c->c.syncHook(c->c);  // state into the reference objects, Face::update
+        RefCloth& r = c->rc;
+        for (size_t i = 0; i < r.nodes.size(); i++) {
+            r.nodes[i].n = Vector3f(S.nn[3 * (n0 + i)], S.nn[3 * (n0 + i) + 1], S.nn[3 * (n0 + i) + 2]);
+            r.nodes[i].area = S.narea[n0 + i];
+        }
+        spans->push_back({c, n0, f0, e0});
+        n0 += (int)r.nodes.size();
+        f0 += (int)r.faces.size();
+        e0 += (int)r.edges.size();
+    }
+    auto find = [spans](int id, int Span::*off) -> const Span& {
+        size_t k = 0;
+        while (k + 1 < spans->size() && (*spans)[k + 1].*off <= id) k++;
+        return (*spans)[k];
+    };
+    auto node = [find](int id) { const Span& s = find(id, &Span::n0); return &s.c->rc.nodes[id - s.n0]; };
+    auto face = [find](int id) { const Span& s = find(id, &Span::f0); return &s.c->rc.faces[id - s.f0]; };
+    auto edge = [find](int id) { const Span& s = find(id, &Span::e0); return &s.c->rc.edges[id - s.e0]; };
+    auto sceneId = [spans](const Node* p) {
+        for (const Span& s : *spans) {
+            const std::vector<Node>& v = s.c->rc.nodes;
+            if (p >= v.data() && p < v.data() + v.size()) return s.n0 + (int)(p - v.data());
+        }
+        return -1;
+    };
+    auto copyOut = [](const Vector3f& n, const float* w, orc::V3<float>& no, float* wo) {
+        for (int c = 0; c < 3; c++) no[c] = n(c);
+        for (int i = 0; i < 4; i++) wo[i] = w[i];
+    };
+    D.vfHook = [=](int nd, int fc, orc::V3<float>& n, float* w, float& h) {
+        const Face* f = face(fc);
+        Vector3f nn;
+        float ww[4] = {0.f, 0.f, 0.f, 0.f};
+        h = signedVertexFaceDistance(node(nd)->x, f->vertices[0]->node->x, f->vertices[1]->node->x,
+                                     f->vertices[2]->node->x, nn, ww);
+        if (std::isinf(h)) return false;
+        copyOut(nn, ww, n, w);
+        return true;
+    };
+    D.eeHook = [=](int a, int b, orc::V3<float>& n, float* w, float& h) {
+        const Edge* ea = edge(a);
+        const Edge* eb = edge(b);
+        Vector3f nn;
+        float ww[4] = {0.f, 0.f, 0.f, 0.f};
+        h = signedEdgeEdgeDistance(ea->nodes[0]->x, ea->nodes[1]->x, eb->nodes[0]->x, eb->nodes[1]->x, nn, ww);
+        if (std::isinf(h)) return false;
+        copyOut(nn, ww, n, w);
+        return true;
+    };
+    D.inEdgeHook = [=](float w, int a, int b) { return inEdge(w, edge(a), edge(b)); };
+    auto fill = [=](const Proximity& p, orc::DetectedProximity& r) {
+        for (int i = 0; i < 4; i++) {
+            r.nodes[i] = sceneId(p.nodes[i]);
+            r.w[i] = p.w[i];
+        }
+        for (int c = 0; c < 3; c++) r.n[c] = p.n(c);
+        r.mu = p.mu;
+        r.stiffness = p.stiffness;
+    };
+    D.proxVFHook = [=](int nd, int fc, const orc::DetectParams& P, orc::DetectedProximity& r) {
+        fill(Proximity(node(nd), face(fc), P.collisionStiffness, P.clothFriction, 0.3f), r);
+    };
+    D.proxEEHook = [=](int a, int b, const orc::DetectParams& P, orc::DetectedProximity& r) {
+        fill(Proximity(edge(a), edge(b), P.collisionStiffness, P.clothFriction, 0.3f), r);
+    };
+}

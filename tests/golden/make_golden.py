@@ -12,7 +12,10 @@ one CPU-path step (FP32 sparse Cholesky).  Materials are seeded synthetic parame
 (anisotropic stretching rows, varied bending samples), not the reference's material files.
 ref_prox9.npz adds seeded proximities: the reference's impulseForce and frictionForce per
 proximity and the step with them (`python tests/golden/make_golden.py ref_prox9` makes only
-that file).
+that file).  ref_detect.npz holds proximity detection over three cloths (a sheet folded over
+itself, two stacked sheets) through the reference's own signedVertexFaceDistance,
+signedEdgeEdgeDistance, inEdge and Proximity constructors (MathHelper.cu:38-69,
+PhysicsHelper.cu:3-18, Proximity.cu:5-21).
 """
 import os
 import sys
@@ -104,6 +107,27 @@ def make_prox_case(seed, nq):
     return out
 
 
+def make_detect_case(seed):
+    """Proximities among a folded sheet (moved 2 m along x, apart from the others) and two
+    stacked sheets, detected through the reference's predicates (Simulator.cu:198-298)."""
+    folded = scenes.folded_sheet(8, seed=seed).sheets[0]
+    folded["x"] = (folded["x"] + np.array([2.0, 0.0, 0.0], np.float32)).astype(np.float32)
+    cloths = [folded] + scenes.stacked_sheets(8, n_layers=2, seed=seed + 1).sheets
+    refs = [pyoracle.Cloth(c, pyoracle.Material(c["material"], which="ref")) for c in cloths]
+    det = pyoracle.detect_proximities(refs, repulsion_thickness=1e-3)
+    out = {"n_cloths": len(cloths), "repulsion_thickness": 1e-3, "collision_stiffness": 1e9, "friction": 0.6}
+    for i, c in enumerate(cloths):
+        for k in ("x", "v", "uv", "fx", "fu", "handles"):
+            out[f"c{i}_{k}"] = c[k]
+    m = cloths[0]["material"]
+    out["material_stretching"] = np.array(m["stretching"])
+    out["material_bending"] = np.array(m["bending"])
+    out["material_density"] = m["density"]
+    for k, v in det.items():
+        out["det_" + k] = v.astype(np.float32) if v.dtype == np.float64 else v
+    return out
+
+
 if __name__ == "__main__":
     only = sys.argv[1:]
     for name, seed, nq, amp in [("ref_sheet6", 11, 6, 0.03), ("ref_sheet9", 12, 9, 0.01)]:
@@ -116,3 +140,7 @@ if __name__ == "__main__":
         case = make_prox_case(21, 9)
         np.savez_compressed(os.path.join(HERE, "ref_prox9.npz"), **case)
         print("ref_prox9", {k: np.asarray(v).shape for k, v in case.items() if np.asarray(v).size > 1})
+    if not only or "ref_detect" in only:
+        case = make_detect_case(31)
+        np.savez_compressed(os.path.join(HERE, "ref_detect.npz"), **case)
+        print("ref_detect", {k: np.asarray(v).shape for k, v in case.items() if k.startswith("det_")})

@@ -21,6 +21,7 @@ pytestmark = pytest.mark.gpu
 
 import pyoracle
 from clothsimulator_b200 import native, scenes
+from proxutil import offsets, oracle_proximities, touched_sheets
 
 THICKNESS = 5e-3
 
@@ -32,8 +33,6 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))
 
 
-def offsets(scene):
-    return np.cumsum([0] + [s["x"].shape[0] for s in scene.sheets]).astype(int)
 
 
 def face_normal(x, f):
@@ -96,29 +95,8 @@ def oracle_cloths(scene):
     return [pyoracle.Cloth(s, pyoracle.Material(s["material"], "float")) for s in scene.sheets]
 
 
-def oracle_proximities(prox, k, offs, x, v, mass):
-    """The proximities sheet k's cloth receives: its nodes local, every other point -1 with
-    the state it has at the start of the step (a free point, with its lumped mass)."""
-    lo, hi = offs[k], offs[k + 1]
-    sel = [p for p in range(len(prox["mu"])) if np.any((prox["nodes"][p] >= lo) & (prox["nodes"][p] < hi))]
-    out = {key: np.array(val[sel]) for key, val in prox.items()}
-    for r, p in enumerate(sel):
-        for i in range(4):
-            nd = int(prox["nodes"][p, i])
-            if lo <= nd < hi:
-                out["nodes"][r, i] = nd - lo
-            elif nd >= 0:
-                out["nodes"][r, i] = -1
-                out["x"][r, i] = x[nd]
-                out["v"][r, i] = v[nd]
-                out["mass"][r, i] = mass[nd]
-                out["free"][r] |= 1 << i
-    return out
 
 
-def touched_sheets(prox, offs):
-    nodes = prox["nodes"][prox["nodes"] >= 0]
-    return sorted({int(np.searchsorted(offs, nd, side="right") - 1) for nd in nodes})
 
 
 def params_for(scene, **kw):

@@ -21,6 +21,7 @@ from clothsimulator_b200 import scenes
 
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_sheet*.npz")))
 GOLDEN_PROX = os.path.join(os.path.dirname(__file__), "golden", "ref_prox9.npz")
+GOLDEN_DETECT = os.path.join(os.path.dirname(__file__), "golden", "ref_detect.npz")
 
 
 def golden_prox(g):
@@ -217,3 +218,42 @@ def test_topology_counts_for_grid():
         # a grid of nq x nq quads has 3nq^2 + 2nq edges, of which 4nq lie on the boundary
         assert c.L.cloth_num_edges(c.h) == 3 * nq * nq + 2 * nq
         assert c.n_interior == 3 * nq * nq - 2 * nq
+
+
+def test_oracle_reproduces_reference_detection_golden():
+    """Proximity detection over three cloths (a folded sheet, two stacked sheets) as the
+    reference's predicates produced it (signedVertexFaceDistance, signedEdgeEdgeDistance,
+    inEdge, Proximity constructors): the same proximities, in the same order, bit for bit."""
+    g = np.load(GOLDEN_DETECT)
+    mat = {"density": float(g["material_density"]), "stretching": g["material_stretching"].tolist(),
+           "bending": g["material_bending"].tolist(), "thicken": 1.0, "density_mult": 1.0,
+           "stretching_mult": 1.0, "bending_mult": 1.0}
+    cloths = []
+    for i in range(int(g["n_cloths"])):
+        sheet = {k: g[f"c{i}_{k}"] for k in ("x", "v", "uv", "fx", "fu", "handles")}
+        cloths.append(pyoracle.Cloth(sheet, pyoracle.Material(mat, "float")))
+    det = pyoracle.detect_proximities(cloths, repulsion_thickness=float(g["repulsion_thickness"]),
+                                      collision_stiffness=float(g["collision_stiffness"]),
+                                      friction=float(g["friction"]))
+    assert len(det["mu"]) == len(g["det_mu"]) > 0
+    for k, v in det.items():
+        ref = g["det_" + k]
+        assert np.array_equal(v.astype(ref.dtype), ref), k
+
+
+@pytest.mark.ref
+def test_oracle_detection_matches_reference_adapter_live():
+    """The restated detection against the same detection run through the reference's own
+    predicates, on self-contact and cross-cloth contact with collision groups."""
+    if not os.path.exists(pyoracle.LIB_REF):
+        pytest.skip("reference adapter not built")
+    cases = [(scenes.folded_sheet(12, seed=1).sheets, None), (scenes.stacked_sheets(10, n_layers=3, seed=2).sheets, None),
+             (scenes.stacked_sheets(10, n_layers=3, seed=3).sheets, [0, 0, 1])]
+    for sheets, groups in cases:
+        out = []
+        for which in ("oracle", "ref"):
+            cl = [pyoracle.Cloth(s, pyoracle.Material(s["material"], "float", which=which)) for s in sheets]
+            out.append(pyoracle.detect_proximities(cl, groups=groups))
+        assert len(out[0]["mu"]) > 0
+        for k in out[0]:
+            assert np.array_equal(out[0][k], out[1][k]), k
