@@ -359,9 +359,13 @@ __global__ void __launch_bounds__(1024) cs_contact_scan_kernel(Contact C, int nb
 
 namespace {
 // Proximity(node, face) (Proximity.cu:5-12) and Proximity(edge0, edge1) (Proximity.cu:14-21)
-__device__ void make_record(const Batch& B, const Contact& C, long long k, unsigned long long v, ContactRec& r) {
+__device__ void make_record(const Batch& B, const Contact& C, long long k, unsigned long long v, cs_proximity_desc& r) {
     const int other = (int)(unsigned)v;
-    r.depth = __uint_as_float((unsigned)(v >> 32));
+    for (int i = 0; i < 4; i++) {
+        for (int e = 0; e < 3; e++) r.x[i][e] = r.v[i][e] = 0.0f;
+        r.mass[i] = 0.0f;
+    }
+    r.free_mask = 0;  // every node is a batch node
     r.mu = C.friction;  // cloth nodes are free (Mesh.cu:349): the cloth friction
     const long long nodeKeys = 2LL * B.N, edgeKeys = 2LL * C.E;
     v3 n;
@@ -371,7 +375,6 @@ __device__ void make_record(const Batch& B, const Contact& C, long long k, unsig
         const int node = nodeKey ? (int)(k >> 1) : other;
         const int face = nodeKey ? other : (int)((k - nodeKeys - edgeKeys) >> 1);
         const int4 y = B.face_nodes[face];
-        r.kind = nodeKey ? 0 : 2;
         r.nodes[0] = node;
         r.nodes[1] = y.x;
         r.nodes[2] = y.y;
@@ -381,7 +384,6 @@ __device__ void make_record(const Batch& B, const Contact& C, long long k, unsig
     } else {
         const int e0 = (int)((k - nodeKeys) >> 1), e1 = other;
         const int4 a = C.edges[e0], b = C.edges[e1];
-        r.kind = 1;
         r.nodes[0] = a.x;
         r.nodes[1] = a.y;
         r.nodes[2] = b.x;
@@ -390,9 +392,9 @@ __device__ void make_record(const Batch& B, const Contact& C, long long k, unsig
         signed_ee(ldx(B.x, a.x), ldx(B.x, a.y), ldx(B.x, b.x), ldx(B.x, b.y), n, r.w, h);
     }
     if (h < 0.0f) n = neg(n);
-    r.n[0] = n.x;
-    r.n[1] = n.y;
-    r.n[2] = n.z;
+    r.normal[0] = n.x;
+    r.normal[1] = n.y;
+    r.normal[2] = n.z;
 }
 }  // namespace
 
@@ -418,7 +420,7 @@ __global__ void __launch_bounds__(256) cs_contact_write_kernel(Batch B, Contact 
     for (int j = 0; j < 16; j++) {
         if (!admitted(C, base + j, v)) continue;
         if (pos < C.out_cap) {
-            ContactRec r;
+            cs_proximity_desc r;
             make_record(B, C, base + j, v, r);
             C.out[pos] = r;
         }

@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "clothstep.h"
+
 #define CS_SLICE 32
 #define CS_PANEL_FLOATS 288  // 32 lanes x 9 entries
 #define CS_TABLE_N 30
@@ -48,6 +50,8 @@ struct SheetDesc {
     int nbr_ptr_off, nbr_off;   // this sheet's topology in the one-ring neighbour arrays
     int row2slot_off;           // this sheet's topology in the row -> slot map
     int resident;               // 1: solved by the cluster-resident kernel (resident.cu)
+    int csr_ptr_off;            // this sheet's topology in tcsr_ptr (block CSR for slot lookups)
+    int panel_off;              // first value panel: global slot = panel_off * 32 + topology slot
 };
 
 struct SliceDesc {
@@ -133,11 +137,6 @@ struct ProxInst {
 // Per-instance record written by cs_prox_kernel: -dt^2 J of the impulse (12x12), -dt J of
 // the friction (12x12), the impulse right-hand side dt (f + dt J v) (12), the friction one dt f.
 #define CS_PROX_REC 312
-// Contribution code: bits 5.. instance, bit 4 friction (1) / impulse (0), bits 2..3 local row
-// corner a, bits 0..1 column corner b.
-__host__ __device__ inline uint32_t cs_pcode(int inst, int friction, int a, int b) {
-    return ((uint32_t)inst << 5) | ((uint32_t)friction << 4) | ((uint32_t)a << 2) | (uint32_t)b;
-}
 
 struct Batch {
     int N = 0, F = 0, E = 0, S = 0;
@@ -190,34 +189,24 @@ struct Batch {
     uint32_t* rsend = nullptr;   // halo sends: src slot | dst rank << 12 | dst halo index << 16
     int* rhalo = nullptr;        // per topology: CS_RES_MAX_CL + 1 halo slot counts per rank
     int res_halo0 = 0;           // first halo slot of every CTA's p array (= own slots per CTA)
-    // proximities (cs_set_proximities); all lists in the reference's accumulation order
-    int n_pinst = 0, n_pfix = 0, n_pb = 0, n_pdiag = 0, n_px = 0;
+    // per-topology block CSR (local ids, columns ascending) with the SELL slot of each block
+    int* tcsr_ptr = nullptr;
+    int* tcsr_col = nullptr;
+    int* tcsr_slot = nullptr;
+    // proximities (cs_set_proximities, cs_detect_proximities)
+    int n_pinst = 0, n_px = 0;
     const ProxInst* pinst = nullptr;
     float* prec = nullptr;        // CS_PROX_REC per instance
-    int* pfix_slot = nullptr;     // pattern slots that receive blocks: panel * 32 + lane
-    int* pfix_ptr = nullptr;      // their contribution ranges (n_pfix + 1)
-    uint32_t* pfix_code = nullptr;
-    int* pb_row = nullptr;        // rows whose right-hand side receives terms
-    int* pb_ptr = nullptr;
-    uint32_t* pb_code = nullptr;
-    int* pdiag_row = nullptr;     // rows whose diagonal block changed (block-Jacobi inverse redone)
+    const int* prow_ptr = nullptr;   // N + 1: the instances holding each row's node
+    const int* prow_inst = nullptr;  // ascending per row
     int* xptr = nullptr;          // N + 1: blocks outside the pattern, per row (null: none)
-    int* xcol = nullptr;          // their columns (batch nodes)
-    int* xcptr = nullptr;         // their contribution ranges (n_px + 1)
-    uint32_t* xcode = nullptr;
+    int* xcol = nullptr;          // their columns (batch nodes), ascending per row
     float* xval = nullptr;        // 9 per block, summed each step
-    int* sheet_prox = nullptr;    // per sheet: 1 if a proximity touches it (batched loop this step)
+    int* sheet_prox = nullptr;    // per sheet: 1 if a proximity touches it (batched loop)
 };
 
 // Proximity detection (contact.cu, cs_detect_proximities).  Scene-wide ids: nodes and faces as
 // in Batch, edges (every edge, not only interior ones) of all sheets concatenated in sheet order.
-struct ContactRec {
-    int nodes[4];
-    float n[3], w[4], mu, stiffness, depth;
-    int kind;  // 0 node key, 1 edge key, 2 face key
-    int pad[3];
-};
-
 struct Contact {
     int E = 0;               // edges
     int n_keys = 0;          // 2 N + 2 E + 2 F
@@ -238,10 +227,11 @@ struct Contact {
     unsigned long long* keys = nullptr;  // per (node|edge|face, side): distance bits << 32 | other id
     int* block_count = nullptr;        // compaction: valid keys per block, then exclusive offsets
     int* total = nullptr;
-    ContactRec* out = nullptr;
+    cs_proximity_desc* out = nullptr;  // detected proximities
     int out_cap = 0;
 };
 
 #define CS_CONTACT_ITEMS 4096  // keys per compaction block (256 threads x 16)
+#define CS_SCAN_ITEMS 4096     // ints per block of the exclusive scan (1024 threads x 4)
 
 #endif

@@ -45,11 +45,19 @@ __global__ void cs_spmv_plain_kernel(Batch B, const float* x, float* y);
 __global__ void cs_profile_setup_kernel(Batch B, int phase);
 __global__ void cs_resident_pcg_kernel(Batch B);
 __global__ void cs_prox_kernel(Batch B);
-__global__ void cs_prox_fix_kernel(Batch B);
-__global__ void cs_prox_rhs_kernel(Batch B);
-__global__ void cs_prox_diag_kernel(Batch B);
-__global__ void cs_prox_extra_kernel(Batch B);
+__global__ void cs_prox_row_kernel(Batch B);
 __global__ void cs_slice_bnorm_kernel(Batch B);
+__global__ void cs_scan_sums_kernel(const int* data, int n, int* partial);
+__global__ void cs_scan_partials_kernel(int* partial, int nb, int* total);
+__global__ void cs_scan_apply_kernel(int* data, int n, const int* partial);
+__global__ void cs_prox_count_kernel(Batch B, const cs_proximity_desc* d, int n, int* icount);
+__global__ void cs_prox_expand_kernel(Batch B, const cs_proximity_desc* d, int n, const int* ioff, float thickness,
+                                      ProxInst* inst, int* sheet_prox);
+__global__ void cs_prox_rowcount_kernel(const ProxInst* inst, int T, int* rowCount);
+__global__ void cs_prox_rowfill_kernel(const ProxInst* inst, int T, const int* rowPtr, int* rowFill, int* rowInst);
+__global__ void cs_prox_rowsort_kernel(int N, const int* rowPtr, int* rowInst);
+__global__ void cs_prox_outside_kernel(Batch B, const int* rowPtr, const int* rowInst, const ProxInst* inst,
+                                       const int* xptr, int* out);
 __global__ void cs_contact_face_kernel(Batch B, Contact C);
 __global__ void cs_contact_node_kernel(Batch B, Contact C);
 __global__ void cs_contact_grid_kernel(Batch B, Contact C, const int* sheet_group);
@@ -544,6 +552,31 @@ ResidentPlan residentPlan(const Topo& T, int ncta) {
 
 // ---------------------------------------------------------------------------------------
 
+// Device buffers of the proximity terms, grown as needed (applyProximities).
+struct ProxBuffers {
+    cs_proximity_desc* desc = nullptr;  // the proximities in force
+    int* icount = nullptr;              // instances per proximity, then their offsets
+    ProxInst* inst = nullptr;
+    float* rec = nullptr;
+    int* rowPtr = nullptr;              // N + 1
+    int* rowFill = nullptr;             // N + 1
+    int* xptr = nullptr;                // N + 1
+    int* rowInst = nullptr;
+    int* xcol = nullptr;
+    float* xval = nullptr;
+    int* sheetProx = nullptr;
+    int* partial = nullptr;             // scan block sums
+    size_t descCap = 0, icountCap = 0, instCap = 0, recCap = 0, rowCap = 0, rowFillCap = 0, xptrCap = 0,
+           rowInstCap = 0, xcolCap = 0, xvalCap = 0, sheetCap = 0, partialCap = 0;
+    int n = 0;  // proximities in force
+    void release() {
+        void* ps[] = {desc, icount, inst, rec, rowPtr, rowFill, xptr, rowInst, xcol, xval, sheetProx, partial};
+        for (void* q : ps)
+            if (q) cudaFree(q);
+        *this = ProxBuffers();
+    }
+};
+
 struct cs_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -580,9 +613,7 @@ struct cs_ctx {
     std::vector<int> rlistAll;  // resident sheets before the proximity filter
     // proximities (cs_set_proximities): their device lists, and the host copies of the
     // blocks outside the pattern that cs_get_system merges
-    std::vector<void*> proxAllocs;
-    std::vector<int> hxptr, hxcol;
-    std::vector<cs_proximity_desc> proxHost;  // the set in force (cs_get_proximities)
+    ProxBuffers prox;
     // proximity detection (contact.cu): static scene data built at the first detection
     Contact contact;
     bool contactReady = false;
@@ -642,11 +673,7 @@ void freeBatch(cs_ctx* c) {
     c->mlpScratch = nullptr;
     for (void* p : c->allocs) cudaFree(p);
     c->allocs.clear();
-    for (void* p : c->proxAllocs) cudaFree(p);
-    c->proxAllocs.clear();
-    c->hxptr.clear();
-    c->hxcol.clear();
-    c->proxHost.clear();
+    c->prox.release();
     for (void* p : c->contactAllocs) cudaFree(p);
     c->contactAllocs.clear();
     c->contact = Contact();
@@ -667,15 +694,12 @@ int launchAssembly(cs_ctx* c) {
     if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B), n++;
     cs_gather_kernel<<<c->gatherGrid, 128, 0, c->stream>>>(B);
     if (B.n_pinst > 0) {
-        // proximity terms after the handles (Cloth.cu:676-684): records, pattern slots,
-        // right-hand sides, the changed diagonal inverses, ||b|| partials, outside blocks
+        // proximity terms after the handles (Cloth.cu:676-684): records, then per row the
+        // blocks, right-hand side and block-Jacobi inverse, then the ||b|| partials
         cs_prox_kernel<<<nblk(B.n_pinst, 128), 128, 0, c->stream>>>(B);
-        cs_prox_fix_kernel<<<nblk(B.n_pfix, 128), 128, 0, c->stream>>>(B);
-        cs_prox_rhs_kernel<<<nblk(B.n_pb, 128), 128, 0, c->stream>>>(B);
-        cs_prox_diag_kernel<<<nblk(B.n_pdiag, 128), 128, 0, c->stream>>>(B);
+        cs_prox_row_kernel<<<nblk(B.N, 128), 128, 0, c->stream>>>(B);
         cs_slice_bnorm_kernel<<<nblk((long long)B.n_slices * 32, 128), 128, 0, c->stream>>>(B);
-        n += 5;
-        if (B.n_px > 0) cs_prox_extra_kernel<<<nblk(B.n_px, 128), 128, 0, c->stream>>>(B), n++;
+        n += 3;
     }
     return n;
 }
@@ -913,6 +937,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     std::vector<int> topoRow2Slot0(topos.size());
     std::vector<int> topoNbrPtr0(topos.size()), topoNbr0(topos.size());
     std::vector<int> topoPanel0(topos.size()), topoSlice0(topos.size());
+    std::vector<int> htcsr_ptr, htcsr_col, htcsr_slot, topoCsrPtr0(topos.size());
     // Cluster-resident solve plan (resident.cu).  CS_RESIDENT_CL sets the CTAs per cluster
     // (2, 4, 8 or 16; 0 solves every sheet in the batched loop); default 8, the portable size.
     int resCL = 8;
@@ -1004,6 +1029,10 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             hrowmap.insert(hrowmap.end(), T.rowmap.begin(), T.rowmap.end());
             topoRow2Slot0[t] = (int)hrow2slot.size();
             hrow2slot.insert(hrow2slot.end(), T.row2slot.begin(), T.row2slot.end());
+            topoCsrPtr0[t] = (int)htcsr_ptr.size();
+            for (int v : T.csr_ptr) htcsr_ptr.push_back(v + (int)htcsr_col.size());
+            htcsr_col.insert(htcsr_col.end(), T.csr_col.begin(), T.csr_col.end());
+            htcsr_slot.insert(htcsr_slot.end(), T.csr_slot.begin(), T.csr_slot.end());
             topoNbrPtr0[t] = (int)hnbr_ptr.size();
             topoNbr0[t] = (int)hnbr.size();
             hnbr_ptr.insert(hnbr_ptr.end(), T.nbr_ptr.begin(), T.nbr_ptr.end());
@@ -1034,6 +1063,8 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         sd.row2slot_off = topoRow2Slot0[sheetTopoId[s]];
         sd.nbr_off = topoNbr0[sheetTopoId[s]];
         sd.resident = topoResident[sheetTopoId[s]];
+        sd.csr_ptr_off = topoCsrPtr0[sheetTopoId[s]];
+        sd.panel_off = panel_off;
         hnode_sheet.insert(hnode_sheet.end(), d.n_nodes, s);
         float bmult = m.bending_mult * m.thicken;
         for (int i = 0; i < 15; i++) sd.bending[i] = m.bending[i / 5][i % 5] * bmult;
@@ -1160,6 +1191,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     UP(node_sheet, hnode_sheet);
     UP(rowmap, hrowmap);
     UP(row2slot, hrow2slot);
+    UP(tcsr_ptr, htcsr_ptr);
+    UP(tcsr_col, htcsr_col);
+    UP(tcsr_slot, htcsr_slot);
     UP(rlist, hrlist);
     UP(rsplit, hrsplit);
     UP(rcode, hrcode);
@@ -1253,37 +1287,122 @@ void destroyGraphs(cs_ctx* c) {
 }
 
 template <class T>
-cs_status proxUpload(cs_ctx* c, T** p, const std::vector<T>& h) {
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, std::max<size_t>(h.size(), 1) * sizeof(T));
-    if (e != cudaSuccess) return fail(c, CS_ERR_CUDA, "cudaMalloc(%zu bytes): %s", h.size() * sizeof(T), cudaGetErrorString(e));
-    c->proxAllocs.push_back(q);
-    *p = (T*)q;
-    if (!h.empty()) CS_CUDA(cudaMemcpy(q, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+cs_status grow(cs_ctx* c, T*& p, size_t& cap, size_t need) {
+    if (need <= cap && p) return CS_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t n = std::max<size_t>(need + need / 4, 16);
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) return fail(c, CS_ERR_CUDA, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    cap = n;
+    return CS_OK;
+}
+
+// Exclusive scan of n ints on the device, in place; data[n] receives the total (and *total,
+// when given, after a stream synchronisation).
+cs_status scanInts(cs_ctx* c, int* data, int n, int* total) {
+    ProxBuffers& P = c->prox;
+    const int nb = std::max(1, (n + CS_SCAN_ITEMS - 1) / CS_SCAN_ITEMS);
+    cs_status st;
+    if ((st = grow(c, P.partial, P.partialCap, nb)) != CS_OK) return st;
+    cs_scan_sums_kernel<<<nb, 1024, 0, c->stream>>>(data, n, P.partial);
+    cs_scan_partials_kernel<<<1, 1024, 0, c->stream>>>(P.partial, nb, data + n);
+    cs_scan_apply_kernel<<<nb, 1024, 0, c->stream>>>(data, n, P.partial);
+    CS_CUDA(cudaGetLastError());
+    if (total) {
+        CS_CUDA(cudaMemcpyAsync(total, data + n, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CS_CUDA(cudaStreamSynchronize(c->stream));
+    }
     return CS_OK;
 }
 
 void clearProximities(cs_ctx* c) {
     Batch& B = c->B;
-    for (void* p : c->proxAllocs) cudaFree(p);
-    c->proxAllocs.clear();
-    c->hxptr.clear();
-    c->hxcol.clear();
-    B.n_pinst = B.n_pfix = B.n_pb = B.n_pdiag = B.n_px = 0;
+    B.n_pinst = B.n_px = 0;
     B.pinst = nullptr;
     B.prec = nullptr;
-    B.pfix_slot = B.pfix_ptr = B.pb_row = B.pb_ptr = B.pdiag_row = nullptr;
-    B.pfix_code = B.pb_code = B.xcode = nullptr;
-    B.xptr = B.xcol = B.xcptr = nullptr;
+    B.prow_ptr = B.prow_inst = nullptr;
+    B.xptr = B.xcol = nullptr;
     B.xval = nullptr;
     B.sheet_prox = nullptr;
+    c->prox.n = 0;
 }
 
-// Per (proximity, sheet it touches) one instance; its 3x3 contributions are listed per target
-// in the order Cloth::addProximityForces accumulates them (Cloth.cu:171-192 through
-// addElement's coeffRef, Cloth.cu:42-76): proximity, impulse before friction, row corner,
-// column corner.  Targets are pattern slots (summed onto the gathered block), right-hand-side
-// rows, and blocks outside the mesh pattern (kept in a row-sorted side list).
+// The proximities in prox.desc (n on the device) become the terms of the following steps:
+// one instance per (proximity, sheet holding one of its nodes) in proximity order, per-row
+// instance lists and the outside-pattern side list, all built on the device (proxlist.cu);
+// cs_prox_row_kernel then adds the terms in the reference's order (Cloth.cu:171-192).
+cs_status applyProximities(cs_ctx* c, int n, float thickness) {
+    Batch& B = c->B;
+    ProxBuffers& P = c->prox;
+    destroyGraphs(c);  // the captured launches hold the old lists
+    clearProximities(c);
+    std::vector<int> touched(B.S, 0);
+    cs_status st;
+    if (n > 0) {
+        const size_t N1 = (size_t)B.N + 1;
+        if ((st = grow(c, P.icount, P.icountCap, (size_t)n + 1)) != CS_OK) return st;
+        cs_prox_count_kernel<<<nblk(n, 128), 128, 0, c->stream>>>(B, P.desc, n, P.icount);
+        int T = 0;
+        if ((st = scanInts(c, P.icount, n, &T)) != CS_OK) return st;
+        if ((st = grow(c, P.inst, P.instCap, (size_t)T)) != CS_OK) return st;
+        if ((st = grow(c, P.rec, P.recCap, (size_t)T * CS_PROX_REC)) != CS_OK) return st;
+        if ((st = grow(c, P.sheetProx, P.sheetCap, (size_t)B.S)) != CS_OK) return st;
+        CS_CUDA(cudaMemsetAsync(P.sheetProx, 0, B.S * sizeof(int), c->stream));
+        cs_prox_expand_kernel<<<nblk(n, 128), 128, 0, c->stream>>>(B, P.desc, n, P.icount, thickness, P.inst,
+                                                                     P.sheetProx);
+        if ((st = grow(c, P.rowPtr, P.rowCap, N1)) != CS_OK) return st;
+        if ((st = grow(c, P.rowFill, P.rowFillCap, N1)) != CS_OK) return st;
+        if ((st = grow(c, P.xptr, P.xptrCap, N1)) != CS_OK) return st;
+        CS_CUDA(cudaMemsetAsync(P.rowPtr, 0, N1 * sizeof(int), c->stream));
+        CS_CUDA(cudaMemsetAsync(P.rowFill, 0, N1 * sizeof(int), c->stream));
+        cs_prox_rowcount_kernel<<<nblk(T, 128), 128, 0, c->stream>>>(P.inst, T, P.rowPtr);
+        int L = 0;
+        if ((st = scanInts(c, P.rowPtr, B.N, &L)) != CS_OK) return st;
+        if ((st = grow(c, P.rowInst, P.rowInstCap, (size_t)L)) != CS_OK) return st;
+        cs_prox_rowfill_kernel<<<nblk(T, 128), 128, 0, c->stream>>>(P.inst, T, P.rowPtr, P.rowFill, P.rowInst);
+        cs_prox_rowsort_kernel<<<nblk(B.N, 128), 128, 0, c->stream>>>(B.N, P.rowPtr, P.rowInst);
+        // the lists cs_prox_outside_kernel reads through B
+        B.prow_ptr = P.rowPtr;
+        B.prow_inst = P.rowInst;
+        cs_prox_outside_kernel<<<nblk(B.N, 128), 128, 0, c->stream>>>(B, P.rowPtr, P.rowInst, P.inst, nullptr, P.xptr);
+        int X = 0;
+        if ((st = scanInts(c, P.xptr, B.N, &X)) != CS_OK) return st;
+        if (X > 0) {
+            if ((st = grow(c, P.xcol, P.xcolCap, (size_t)X)) != CS_OK) return st;
+            if ((st = grow(c, P.xval, P.xvalCap, 9 * (size_t)X)) != CS_OK) return st;
+            cs_prox_outside_kernel<<<nblk(B.N, 128), 128, 0, c->stream>>>(B, P.rowPtr, P.rowInst, P.inst, P.xptr,
+                                                                           P.xcol);
+            CS_CUDA(cudaMemsetAsync(P.xval, 0, 9 * (size_t)X * sizeof(float), c->stream));
+        }
+        CS_CUDA(cudaGetLastError());
+        CS_CUDA(cudaMemcpyAsync(touched.data(), P.sheetProx, B.S * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CS_CUDA(cudaStreamSynchronize(c->stream));
+        B.n_pinst = T;
+        B.pinst = P.inst;
+        B.prec = P.rec;
+        B.prow_ptr = P.rowPtr;
+        B.prow_inst = P.rowInst;
+        B.n_px = X;
+        B.xptr = X > 0 ? P.xptr : nullptr;
+        B.xcol = X > 0 ? P.xcol : nullptr;
+        B.xval = X > 0 ? P.xval : nullptr;
+        B.sheet_prox = P.sheetProx;
+        P.n = n;
+    }
+    // sheets with proximities leave the cluster-resident kernel's work list for the batched
+    // loop (their systems carry blocks outside the pattern, which only its SpMV reads)
+    std::vector<int> rl;
+    for (int s : c->rlistAll)
+        if (!touched[s]) rl.push_back(s);
+    if (!rl.empty()) CS_CUDA(cudaMemcpy(B.rlist, rl.data(), rl.size() * sizeof(int), cudaMemcpyHostToDevice));
+    B.n_resident = (int)rl.size();
+    c->resClusters = std::min(c->resClustersMax, B.n_resident);
+    return CS_OK;
+}
+
+// Host proximities: validated, copied to the device, applied.
 cs_status setProximities(cs_ctx* c, const cs_proximity_desc* px, int n, float thickness) {
     if (n < 0 || (n > 0 && !px)) return fail(c, CS_ERR_INVALID_ARG, "bad proximity list");
     if (n > 0 && !(std::isfinite(thickness) && thickness > 0.0f))
@@ -1309,144 +1428,12 @@ cs_status setProximities(cs_ctx* c, const cs_proximity_desc* px, int n, float th
     }
     CS_CUDA(cudaSetDevice(c->device));
     CS_CUDA(cudaStreamSynchronize(c->stream));
-    destroyGraphs(c);  // the captured launches hold the old lists
-    clearProximities(c);
-
-    const int S = B.S;
-    std::vector<int> offs(S);
-    for (int s = 0; s < S; s++) offs[s] = c->sheets[s].node_off;
-    auto sheetOf = [&](int node) { return (int)(std::upper_bound(offs.begin(), offs.end(), node) - offs.begin()) - 1; };
-    std::vector<ProxInst> inst;
-    std::vector<int> touched(S, 0);
-    for (int p = 0; p < n; p++) {
-        const cs_proximity_desc& d = px[p];
-        int sh[4];
-        for (int i = 0; i < 4; i++) sh[i] = d.nodes[i] >= 0 ? sheetOf(d.nodes[i]) : -1;
-        for (int i = 0; i < 4; i++) {
-            if (sh[i] < 0) continue;
-            bool seen = false;
-            for (int k = 0; k < i; k++) seen |= sh[k] == sh[i];
-            if (seen) continue;
-            ProxInst I{};
-            I.sheet = sh[i];
-            I.local = 0;
-            for (int k = 0; k < 4; k++) {
-                I.node[k] = d.nodes[k];
-                if (sh[k] == sh[i]) I.local |= 1 << k;
-                for (int e = 0; e < 3; e++) {
-                    I.xe[k][e] = d.x[k][e];
-                    I.ve[k][e] = d.v[k][e];
-                }
-                I.me[k] = d.mass[k];
-                I.w[k] = d.w[k];
-            }
-            I.free_mask = d.free_mask;
-            I.thickness = thickness;
-            for (int e = 0; e < 3; e++) I.n[e] = d.normal[e];
-            I.mu = d.mu;
-            I.stiffness = d.stiffness;
-            inst.push_back(I);
-            touched[sh[i]] = 1;
-        }
+    cs_status st;
+    if (n > 0) {
+        if ((st = grow(c, c->prox.desc, c->prox.descCap, (size_t)n)) != CS_OK) return st;
+        CS_CUDA(cudaMemcpyAsync(c->prox.desc, px, n * sizeof(cs_proximity_desc), cudaMemcpyHostToDevice, c->stream));
     }
-    if ((long long)inst.size() >= (1LL << 26)) return fail(c, CS_ERR_INVALID_ARG, "too many proximities");
-    if (!inst.empty()) {
-        std::map<int, std::vector<uint32_t>> fix, rhs;
-        std::map<std::pair<int, int>, std::vector<uint32_t>> extra;
-        std::map<int, int> diag;
-        for (size_t t = 0; t < inst.size(); t++) {
-            const ProxInst& I = inst[t];
-            const SheetDesc& sd = c->sheets[I.sheet];
-            const Topo& T = *c->sheetTopo[I.sheet];
-            const int panelBase = c->slices[sd.slice_off].panel0 - T.slice_tpanel0[0];
-            auto slotOf = [&](int i, int j) {
-                const int* lo = T.csr_col.data() + T.csr_ptr[i];
-                const int* hi = T.csr_col.data() + T.csr_ptr[i + 1];
-                const int* q = std::lower_bound(lo, hi, j);
-                if (q == hi || *q != j) return -1;
-                const int slot = T.csr_slot[q - T.csr_col.data()];
-                return (panelBase + slot / CS_SLICE) * CS_SLICE + slot % CS_SLICE;
-            };
-            for (int fr = 0; fr < 2; fr++)
-                for (int a = 0; a < 4; a++) {
-                    if (!((I.local >> a) & 1)) continue;
-                    const int row = I.node[a], i = row - sd.node_off;
-                    rhs[row].push_back(cs_pcode((int)t, fr, a, 0));
-                    diag[row] = slotOf(i, i);
-                    if (diag[row] < 0) return fail(c, CS_ERR_STATE, "node %d: no diagonal block in the pattern", row);
-                    for (int b = 0; b < 4; b++) {
-                        if (!((I.local >> b) & 1)) continue;
-                        const int col = I.node[b];
-                        const uint32_t code = cs_pcode((int)t, fr, a, b);
-                        const int slot = slotOf(i, col - sd.node_off);
-                        if (slot >= 0) fix[slot].push_back(code);
-                        else extra[{row, col}].push_back(code);
-                    }
-                }
-        }
-        std::vector<int> fslot, fptr{0}, brow, bptr{0}, drow, xcptr{0};
-        std::vector<uint32_t> fcode, bcode, xcode;
-        for (auto& kv : fix) {
-            fslot.push_back(kv.first);
-            fcode.insert(fcode.end(), kv.second.begin(), kv.second.end());
-            fptr.push_back((int)fcode.size());
-        }
-        for (auto& kv : rhs) {
-            brow.push_back(kv.first);
-            bcode.insert(bcode.end(), kv.second.begin(), kv.second.end());
-            bptr.push_back((int)bcode.size());
-        }
-        for (auto& kv : diag) {
-            drow.push_back(kv.first);
-            drow.push_back(kv.second);
-        }
-        cs_status st;
-#define PUP(field, vec) \
-    if ((st = proxUpload(c, &B.field, vec)) != CS_OK) return st;
-        PUP(pfix_slot, fslot);
-        PUP(pfix_ptr, fptr);
-        PUP(pfix_code, fcode);
-        PUP(pb_row, brow);
-        PUP(pb_ptr, bptr);
-        PUP(pb_code, bcode);
-        PUP(pdiag_row, drow);
-        if (!extra.empty()) {
-            c->hxptr.assign(B.N + 1, 0);
-            for (auto& kv : extra) {
-                c->hxptr[kv.first.first + 1]++;
-                c->hxcol.push_back(kv.first.second);
-                xcode.insert(xcode.end(), kv.second.begin(), kv.second.end());
-                xcptr.push_back((int)xcode.size());
-            }
-            for (int r = 0; r < B.N; r++) c->hxptr[r + 1] += c->hxptr[r];
-            PUP(xptr, c->hxptr);
-            PUP(xcol, c->hxcol);
-            PUP(xcptr, xcptr);
-            PUP(xcode, xcode);
-            PUP(xval, std::vector<float>(9 * extra.size(), 0.0f));
-        }
-        ProxInst* dinst = nullptr;
-        PUP(prec, std::vector<float>(CS_PROX_REC * inst.size(), 0.0f));
-        if ((st = proxUpload(c, &dinst, inst)) != CS_OK) return st;
-        PUP(sheet_prox, touched);
-#undef PUP
-        B.pinst = dinst;
-        B.n_pinst = (int)inst.size();
-        B.n_pfix = (int)fslot.size();
-        B.n_pb = (int)brow.size();
-        B.n_pdiag = (int)diag.size();
-        B.n_px = (int)extra.size();
-    }
-    // sheets with proximities leave the cluster-resident solver (their systems carry blocks
-    // outside the pattern, which only the batched loop's SpMV reads)
-    std::vector<int> rl;
-    for (int s : c->rlistAll)
-        if (!touched[s]) rl.push_back(s);
-    if (!rl.empty()) CS_CUDA(cudaMemcpy(B.rlist, rl.data(), rl.size() * sizeof(int), cudaMemcpyHostToDevice));
-    B.n_resident = (int)rl.size();
-    c->resClusters = std::min(c->resClustersMax, B.n_resident);
-    c->proxHost.assign(px, px + n);
-    return CS_OK;
+    return applyProximities(c, n, thickness);
 }
 
 template <class T>
@@ -1589,33 +1576,12 @@ cs_status cs_detect_proximities(cs_ctx* c, const cs_detect_params* p, int* count
     CS_CUDA(cudaStreamSynchronize(c->stream));
     if (flags[1] & 1u) return fail(c, CS_ERR_INVALID_ARG, "non-finite node state");
     if (flags[1]) return fail(c, CS_ERR_STATE, "proximity grid overflow (flags %u)", flags[1]);
-    if (total > C.out_cap) {
-        if (C.out) cudaFree(C.out);
-        C.out = nullptr;
-        C.out_cap = 0;
-        const int cap = std::max(total, 2 * C.out_cap);
-        CS_CUDA(cudaMalloc(&C.out, (size_t)std::max(cap, 1) * sizeof(ContactRec)));
-        C.out_cap = cap;
-    }
+    if ((st = grow(c, c->prox.desc, c->prox.descCap, (size_t)std::max(total, 1))) != CS_OK) return st;
+    C.out = c->prox.desc;
+    C.out_cap = (int)std::min<size_t>(c->prox.descCap, INT32_MAX);
     cs_contact_write_kernel<<<nblocks, 256, 0, c->stream>>>(B, C);
     CS_CUDA(cudaGetLastError());
-    std::vector<ContactRec> rec(total);
-    if (total > 0)
-        CS_CUDA(cudaMemcpyAsync(rec.data(), C.out, total * sizeof(ContactRec), cudaMemcpyDeviceToHost, c->stream));
-    CS_CUDA(cudaStreamSynchronize(c->stream));
-    std::vector<cs_proximity_desc> desc(total);
-    for (int i = 0; i < total; i++) {
-        cs_proximity_desc& d = desc[i];
-        std::memset(&d, 0, sizeof(d));
-        for (int k = 0; k < 4; k++) {
-            d.nodes[k] = rec[i].nodes[k];
-            d.w[k] = rec[i].w[k];
-        }
-        for (int k = 0; k < 3; k++) d.normal[k] = rec[i].n[k];
-        d.mu = rec[i].mu;
-        d.stiffness = rec[i].stiffness;
-    }
-    if ((st = setProximities(c, desc.data(), total, p->repulsion_thickness)) != CS_OK) return st;
+    if ((st = applyProximities(c, total, p->repulsion_thickness)) != CS_OK) return st;
     if (count) *count = total;
     return CS_OK;
 }
@@ -1623,8 +1589,11 @@ cs_status cs_detect_proximities(cs_ctx* c, const cs_detect_params* p, int* count
 cs_status cs_get_proximities(cs_ctx* c, cs_proximity_desc* out, int cap, int* count) {
     if (!c || (cap > 0 && !out)) return CS_ERR_INVALID_ARG;
     if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
-    const int n = (int)c->proxHost.size();
-    for (int i = 0; i < n && i < cap; i++) out[i] = c->proxHost[i];
+    const int n = c->prox.n;
+    if (n > 0 && cap > 0) {
+        CS_CUDA(cudaStreamSynchronize(c->stream));
+        CS_CUDA(cudaMemcpy(out, c->prox.desc, std::min(n, cap) * sizeof(cs_proximity_desc), cudaMemcpyDeviceToHost));
+    }
     if (count) *count = n;
     return CS_OK;
 }
@@ -1732,7 +1701,7 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
         c->graphSteps++;
         c->graphLaunchesFixed += (c->B.F ? 1 : 0) + (c->B.E ? 1 : 0) + 1 + 3 + (learned ? 3 : 0) +
                                  (c->resClusters > 0 ? 1 : 0) +
-                                 (c->B.n_pinst > 0 ? 5 + (c->B.n_px > 0 ? 1 : 0) : 0);
+                                 (c->B.n_pinst > 0 ? 3 : 0);
     }
     if (!stats) return CS_OK;
     std::vector<InstState> inst(c->B.S);
@@ -1812,7 +1781,13 @@ cs_status cs_get_system(cs_ctx* c, int32_t* row_ptr, int32_t* col, float* val, f
     if (b) CS_CUDA(cudaMemcpy(b, B.b, 3 * (size_t)B.N * sizeof(float), cudaMemcpyDeviceToHost));
     // proximity blocks outside the pattern, merged into each row in column order
     std::vector<float> X(9 * (size_t)B.n_px);
-    if (B.n_px > 0) CS_CUDA(cudaMemcpy(X.data(), B.xval, X.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    std::vector<int> hxptr, hxcol(B.n_px);
+    if (B.n_px > 0) {
+        hxptr.resize((size_t)B.N + 1);
+        CS_CUDA(cudaMemcpy(X.data(), B.xval, X.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        CS_CUDA(cudaMemcpy(hxptr.data(), B.xptr, hxptr.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        CS_CUDA(cudaMemcpy(hxcol.data(), B.xcol, hxcol.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    }
     long long pos = 0;
     int rowBase = 0;
     if (row_ptr) row_ptr[0] = 0;
@@ -1822,16 +1797,16 @@ cs_status cs_get_system(cs_ctx* c, int32_t* row_ptr, int32_t* col, float* val, f
         int panelBase = c->slices[sd.slice_off].panel0 - T.slice_tpanel0[0];
         for (int i = 0; i < T.n_nodes; i++) {
             const int row = rowBase + i;
-            int m = B.n_px > 0 ? c->hxptr[row] : 0;
-            const int mEnd = B.n_px > 0 ? c->hxptr[row + 1] : 0;
+            int m = B.n_px > 0 ? hxptr[row] : 0;
+            const int mEnd = B.n_px > 0 ? hxptr[row + 1] : 0;
             auto putExtra = [&]() {
-                if (col) col[pos] = c->hxcol[m];
+                if (col) col[pos] = hxcol[m];
                 if (val) std::copy(X.begin() + 9 * (size_t)m, X.begin() + 9 * (size_t)m + 9, val + 9 * pos);
                 pos++;
                 m++;
             };
             for (int p = T.csr_ptr[i]; p < T.csr_ptr[i + 1]; p++) {
-                while (m < mEnd && c->hxcol[m] < rowBase + T.csr_col[p]) putExtra();
+                while (m < mEnd && hxcol[m] < rowBase + T.csr_col[p]) putExtra();
                 int slot = T.csr_slot[p];
                 int lane = slot % CS_SLICE, panel = panelBase + slot / CS_SLICE;
                 const float* P = A.data() + (size_t)panel * CS_PANEL_FLOATS;

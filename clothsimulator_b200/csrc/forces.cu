@@ -83,13 +83,6 @@ __device__ __forceinline__ void store_slot(float* A, int slot, const float a[9])
     pn[256 + lane] = a[8];
 }
 
-// The 3x3 block (a, b) of a proximity contribution code (cs_pcode) from its record.
-__device__ __forceinline__ const float* prox_block(const Batch& B, uint32_t code, int& rowstride) {
-    const int inst = (int)(code >> 5), fr = (code >> 4) & 1, a = (code >> 2) & 3, b = code & 3;
-    rowstride = 12;
-    return B.prec + (size_t)inst * CS_PROX_REC + fr * 144 + (3 * a) * 12 + 3 * b;
-}
-
 // Material::stretchingStiffness (Material.cu:91-124): trilinear lookup on the 30^3 table.
 __device__ __forceinline__ float4 stretch_stiffness(const float4* __restrict__ T, float G00, float G01, float G11) {
     const float hi = (float)(CS_TABLE_N - 1) - 1e-6f;
@@ -616,65 +609,79 @@ __global__ void __launch_bounds__(128) cs_prox_kernel(Batch B) {
         for (int c = 0; c < 3; c++) rec[300 + 3 * i + c] = dt * (-f_v * (P.w[i] * vt[c]));
 }
 
-// Proximity blocks into the pattern slots they fall on, in order after the gather's sums.
-__global__ void cs_prox_fix_kernel(Batch B) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= B.n_pfix) return;
-    const int slot = B.pfix_slot[m];
-    float a[9];
-    load_slot(B.A, slot, a);
-    for (int c = B.pfix_ptr[m]; c < B.pfix_ptr[m + 1]; c++) {
-        int rs;
-        const float* blk = prox_block(B, B.pfix_code[c], rs);
-        for (int k = 0; k < 3; k++)
-            for (int h = 0; h < 3; h++) a[3 * k + h] += blk[k * rs + h];
-    }
-    store_slot(B.A, slot, a);
-}
-
-// Proximity right-hand sides, in order after the gather's (handles last there).
-__global__ void cs_prox_rhs_kernel(Batch B) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= B.n_pb) return;
-    const int row = B.pb_row[m];
+// Proximity terms onto the system, one thread per row holding a proximity node, in the order
+// Cloth::addProximityForces accumulates them (Cloth.cu:171-192 through addElement's coeffRef,
+// Cloth.cu:42-76): instances ascending, impulse before friction, row corner, column corner;
+// after the gather's handle terms.  Blocks on the mesh pattern are summed onto their slot,
+// others onto the row's side list (zeroed first); the row's block-Jacobi inverse is redone.
+__global__ void __launch_bounds__(128) cs_prox_row_kernel(Batch B) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= B.N) return;
+    const int q0 = B.prow_ptr[row], q1 = B.prow_ptr[row + 1];
+    if (q0 == q1) return;
+    const SheetDesc& sd = B.sheets[B.node_sheet[row]];
+    const int* cp = B.tcsr_ptr + sd.csr_ptr_off;
+    const int li = row - sd.node_off;
+    const int c0 = cp[li], c1 = cp[li + 1];
+    // SELL slot of block (row, col) on the mesh pattern, or -1
+    auto slot_of = [&](int col) {
+        const int lj = col - sd.node_off;
+        int lo = c0, hi = c1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (B.tcsr_col[mid] < lj) lo = mid + 1;
+            else hi = mid;
+        }
+        return (lo < c1 && B.tcsr_col[lo] == lj) ? sd.panel_off * CS_SLICE + B.tcsr_slot[lo] : -1;
+    };
+    const int x0 = B.xptr ? B.xptr[row] : 0, x1 = B.xptr ? B.xptr[row + 1] : 0;
+    for (int m = x0; m < x1; m++)
+        for (int e = 0; e < 9; e++) B.xval[9 * (size_t)m + e] = 0.0f;
     float b0 = B.b[3 * row], b1 = B.b[3 * row + 1], b2 = B.b[3 * row + 2];
-    for (int c = B.pb_ptr[m]; c < B.pb_ptr[m + 1]; c++) {
-        const uint32_t code = B.pb_code[c];
-        const int inst = (int)(code >> 5), fr = (code >> 4) & 1, a = (code >> 2) & 3;
-        const float* r = B.prec + (size_t)inst * CS_PROX_REC + (fr ? 300 : 288) + 3 * a;
-        b0 += r[0];
-        b1 += r[1];
-        b2 += r[2];
+    for (int q = q0; q < q1; q++) {
+        const int inst = B.prow_inst[q];
+        const ProxInst& P = B.pinst[inst];
+        const float* rec = B.prec + (size_t)inst * CS_PROX_REC;
+        for (int fr = 0; fr < 2; fr++)
+            for (int a = 0; a < 4; a++) {
+                if (!((P.local >> a) & 1) || P.node[a] != row) continue;
+                const float* r = rec + (fr ? 300 : 288) + 3 * a;
+                b0 += r[0];
+                b1 += r[1];
+                b2 += r[2];
+                for (int bb = 0; bb < 4; bb++) {
+                    if (!((P.local >> bb) & 1)) continue;
+                    const int col = P.node[bb];
+                    const float* blk = rec + fr * 144 + (3 * a) * 12 + 3 * bb;
+                    const int slot = slot_of(col);
+                    float acc[9];
+                    float* dst = nullptr;
+                    if (slot >= 0) {
+                        load_slot(B.A, slot, acc);
+                    } else {
+                        int m = x0;
+                        while (m < x1 && B.xcol[m] != col) m++;
+                        if (m == x1) continue;  // not listed: cannot happen for a consistent list
+                        dst = B.xval + 9 * (size_t)m;
+                        for (int e = 0; e < 9; e++) acc[e] = dst[e];
+                    }
+                    for (int k = 0; k < 3; k++)
+                        for (int h = 0; h < 3; h++) acc[3 * k + h] += blk[k * 12 + h];
+                    if (slot >= 0) store_slot(B.A, slot, acc);
+                    else
+                        for (int e = 0; e < 9; e++) dst[e] = acc[e];
+                }
+            }
     }
     B.b[3 * row] = b0;
     B.b[3 * row + 1] = b1;
     B.b[3 * row + 2] = b2;
-}
-
-// Block-Jacobi inverse of the rows whose diagonal block received proximity terms
-// (pdiag_row: row, diagonal slot pairs).
-__global__ void cs_prox_diag_kernel(Batch B) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= B.n_pdiag) return;
-    const int row = B.pdiag_row[2 * m], slot = B.pdiag_row[2 * m + 1];
-    float a[9];
-    load_slot(B.A, slot, a);
-    block_inverse(a, B.Pinv + 9 * (size_t)row);
-}
-
-// Blocks outside the pattern: sums of their contributions in order.
-__global__ void cs_prox_extra_kernel(Batch B) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= B.n_px) return;
-    float a[9];
-    for (int e = 0; e < 9; e++) a[e] = 0.0f;
-    for (int c = B.xcptr[m]; c < B.xcptr[m + 1]; c++) {
-        int rs;
-        const float* blk = prox_block(B, B.xcode[c], rs);
-        for (int k = 0; k < 3; k++)
-            for (int h = 0; h < 3; h++) a[3 * k + h] += blk[k * rs + h];
+    const int ds = slot_of(row);
+    if (ds >= 0) {
+        float a[9];
+        load_slot(B.A, ds, a);
+        block_inverse(a, B.Pinv + 9 * (size_t)row);
     }
-    for (int e = 0; e < 9; e++) B.xval[9 * (size_t)m + e] = a[e];
 }
 
 // ||b||^2 per slice after the proximity right-hand sides (the gather's partials otherwise).
