@@ -17,8 +17,10 @@
 //                            its bounds touch (lock-free singly linked lists; buckets by the
 //                            spatial hash of Teschner et al. 2003 with a final bit mix)
 //   cs_contact_pair_kernel   thread per face f: walks the cells of its dilated bounds and
-//                            tests each face g > f of its collision group whose bounds
+//                            appends each face g > f of its collision group whose bounds
 //                            overlap, once per pair (in the lowest cell the two share)
+//   cs_contact_vf/ee_kernel  thread per (pair, vertex-face test) and per (pair, edge-edge
+//                            test): every lane of a warp runs the same test
 //   cs_contact_count/scan/write_kernel: ordered compaction of the admitted keys (distance
 //                            below 2 x repulsionThickness) into proximity records, in the
 //                            reference's output order: node keys, edge keys, face keys
@@ -239,62 +241,97 @@ __global__ void __launch_bounds__(128) cs_contact_grid_kernel(Batch B, Contact C
             }
 }
 
+// Candidate face pairs: thread per face f, walking the cells of its dilated bounds; each pair
+// (f, g > f) of one collision group whose bounds overlap is appended once (in the lowest cell
+// the two share).  Pairs are staged per thread and appended with one atomic per warp.
 __global__ void __launch_bounds__(128) cs_contact_pair_kernel(Batch B, Contact C, const int* sheet_group) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= B.F || C.ext[1]) return;
-    const float c = cell_size(C);
-    const float t = 2.0f * C.repulsion;  // Simulator.cu:274: traverse with 2 x repulsionThickness
-    const int group = sheet_group[B.face_nodes[f].w];
-    float dlo[3], dhi[3];
-    int qlo[3], qhi[3];
-    for (int k = 0; k < 3; k++) {
-        dlo[k] = C.box[6 * (size_t)f + k] - t;  // Bounds::dilate (Bounds.cu:60-68)
-        dhi[k] = C.box[6 * (size_t)f + 3 + k] + t;
-        qlo[k] = cell_of(dlo[k], c);
-        qhi[k] = cell_of(dhi[k], c);
-        if (qhi[k] - qlo[k] > 2) {
-            atomicOr(&C.ext[1], 4u);
-            return;
+    int2 buf[CS_PAIR_STAGE];
+    int nb = 0;
+    if (f < B.F && !C.ext[1]) {
+        const float c = cell_size(C);
+        const float t = 2.0f * C.repulsion;  // Simulator.cu:274: traverse with 2 x repulsionThickness
+        const int group = sheet_group[B.face_nodes[f].w];
+        float dlo[3], dhi[3];
+        int qlo[3], qhi[3];
+        bool ok = true;
+        for (int k = 0; k < 3; k++) {
+            dlo[k] = C.box[6 * (size_t)f + k] - t;  // Bounds::dilate (Bounds.cu:60-68)
+            dhi[k] = C.box[6 * (size_t)f + 3 + k] + t;
+            qlo[k] = cell_of(dlo[k], c);
+            qhi[k] = cell_of(dhi[k], c);
+            ok &= qhi[k] - qlo[k] <= 2;
         }
-    }
-    const int4 fe = C.face_edges[f];
-    const int4 fy = B.face_nodes[f];
-    const long long walk_cap = 8LL * B.F + 8;
-    for (int ix = qlo[0]; ix <= qhi[0]; ix++)
-        for (int iy = qlo[1]; iy <= qhi[1]; iy++)
-            for (int iz = qlo[2]; iz <= qhi[2]; iz++) {
-                long long walked = 0;
-                for (int e = C.head[bucket(C, group, ix, iy, iz)]; e >= 0; e = C.next[e]) {
-                    if (++walked > walk_cap) {
-                        atomicOr(&C.ext[1], 8u);
-                        return;
+        if (!ok) atomicOr(&C.ext[1], 4u);
+        const long long walk_cap = 8LL * B.F + 8;
+        for (int ix = qlo[0]; ok && ix <= qhi[0]; ix++)
+            for (int iy = qlo[1]; ok && iy <= qhi[1]; iy++)
+                for (int iz = qlo[2]; ok && iz <= qhi[2]; iz++) {
+                    long long walked = 0;
+                    for (int e = C.head[bucket(C, group, ix, iy, iz)]; e >= 0; e = C.next[e]) {
+                        if (++walked > walk_cap) {
+                            atomicOr(&C.ext[1], 8u);
+                            ok = false;
+                            break;
+                        }
+                        const int g = e >> 3;
+                        if (g <= f) continue;
+                        if (sheet_group[B.face_nodes[g].w] != group) continue;
+                        const float* gb = C.box + 6 * (size_t)g;
+                        // Bounds::overlap(b, thickness) (Bounds.cu:85-101): g against f dilated
+                        if (gb[0] > dhi[0] || gb[3] < dlo[0] || gb[1] > dhi[1] || gb[4] < dlo[1] || gb[2] > dhi[2] ||
+                            gb[5] < dlo[2])
+                            continue;
+                        // one test per pair: in the lowest cell both cover
+                        if (max(qlo[0], cell_of(gb[0], c)) != ix || max(qlo[1], cell_of(gb[1], c)) != iy ||
+                            max(qlo[2], cell_of(gb[2], c)) != iz)
+                            continue;
+                        if (nb == CS_PAIR_STAGE) {
+                            const int base = atomicAdd(C.pair_count, nb);
+                            for (int k = 0; k < nb; k++)
+                                if (base + k < C.pair_cap) C.pairs[base + k] = buf[k];
+                            nb = 0;
+                        }
+                        buf[nb++] = make_int2(f, g);
                     }
-                    const int g = e >> 3;
-                    if (g <= f) continue;
-                    const int4 gy = B.face_nodes[g];
-                    if (sheet_group[gy.w] != group) continue;
-                    const float* gb = C.box + 6 * (size_t)g;
-                    // Bounds::overlap(b, thickness) (Bounds.cu:85-101): g against f dilated
-                    if (gb[0] > dhi[0] || gb[3] < dlo[0] || gb[1] > dhi[1] || gb[4] < dlo[1] || gb[2] > dhi[2] ||
-                        gb[5] < dlo[2])
-                        continue;
-                    // one test per pair: in the lowest cell both cover
-                    if (max(qlo[0], cell_of(gb[0], c)) != ix || max(qlo[1], cell_of(gb[1], c)) != iy ||
-                        max(qlo[2], cell_of(gb[2], c)) != iz)
-                        continue;
-                    // checkProximities (Simulator.cu:263-269)
-                    check_vf(B, C, fy.x, g);
-                    check_vf(B, C, fy.y, g);
-                    check_vf(B, C, fy.z, g);
-                    check_vf(B, C, gy.x, f);
-                    check_vf(B, C, gy.y, f);
-                    check_vf(B, C, gy.z, f);
-                    const int4 ge = C.face_edges[g];
-                    const int fa[3] = {fe.x, fe.y, fe.z}, ga[3] = {ge.x, ge.y, ge.z};
-                    for (int i = 0; i < 3; i++)
-                        for (int j = 0; j < 3; j++) check_ee(B, C, fa[i], ga[j]);
                 }
-            }
+    }
+    // warp-aggregated append of the staged pairs
+    const int lane = threadIdx.x & 31;
+    int incl = nb;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    int base = 0;
+    if (lane == 31 && incl > 0) base = atomicAdd(C.pair_count, incl);
+    base = __shfl_sync(0xffffffffu, base, 31) + incl - nb;
+    for (int k = 0; k < nb; k++)
+        if (base + k < C.pair_cap) C.pairs[base + k] = buf[k];
+}
+
+// checkProximities (Simulator.cu:263-269), vertex-face part: thread per (pair, corner): the
+// three corners of the first face against the second, then the reverse.
+__global__ void __launch_bounds__(256) cs_contact_vf_kernel(Batch B, Contact C, int npairs) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6LL * npairs) return;
+    const int p = (int)(t / 6), k = (int)(t % 6);
+    const int2 pr = C.pairs[p];
+    const int f = k < 3 ? pr.x : pr.y, g = k < 3 ? pr.y : pr.x;
+    const int4 y = B.face_nodes[f];
+    const int i = k % 3;
+    check_vf(B, C, i == 0 ? y.x : i == 1 ? y.y : y.z, g);
+}
+
+// checkProximities, edge-edge part: thread per (pair, edge of the first face, edge of the second).
+__global__ void __launch_bounds__(256) cs_contact_ee_kernel(Batch B, Contact C, int npairs) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 9LL * npairs) return;
+    const int p = (int)(t / 9), k = (int)(t % 9);
+    const int2 pr = C.pairs[p];
+    const int4 fe = C.face_edges[pr.x], ge = C.face_edges[pr.y];
+    const int i = k / 3, j = k % 3;
+    check_ee(B, C, i == 0 ? fe.x : i == 1 ? fe.y : fe.z, j == 0 ? ge.x : j == 1 ? ge.y : ge.z);
 }
 
 namespace {

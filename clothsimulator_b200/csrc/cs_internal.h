@@ -225,6 +225,9 @@ struct Contact {
     int* head = nullptr;               // grid bucket heads (-1: empty)
     int* next = nullptr;               // 8 entries per face: next entry in the bucket
     unsigned long long* keys = nullptr;  // per (node|edge|face, side): distance bits << 32 | other id
+    int2* pairs = nullptr;             // candidate face pairs (f, g > f)
+    int pair_cap = 0;
+    int* pair_count = nullptr;
     int* block_count = nullptr;        // compaction: valid keys per block, then exclusive offsets
     int* total = nullptr;
     cs_proximity_desc* out = nullptr;  // detected proximities
@@ -232,6 +235,7 @@ struct Contact {
 };
 
 #define CS_CONTACT_ITEMS 4096  // keys per compaction block (256 threads x 16)
+#define CS_PAIR_STAGE 16       // candidate pairs staged per thread before appending
 #define CS_SCAN_ITEMS 4096     // ints per block of the exclusive scan (1024 threads x 4)
 
 #endif

@@ -62,6 +62,8 @@ __global__ void cs_contact_face_kernel(Batch B, Contact C);
 __global__ void cs_contact_node_kernel(Batch B, Contact C);
 __global__ void cs_contact_grid_kernel(Batch B, Contact C, const int* sheet_group);
 __global__ void cs_contact_pair_kernel(Batch B, Contact C, const int* sheet_group);
+__global__ void cs_contact_vf_kernel(Batch B, Contact C, int npairs);
+__global__ void cs_contact_ee_kernel(Batch B, Contact C, int npairs);
 __global__ void cs_contact_count_kernel(Contact C);
 __global__ void cs_contact_scan_kernel(Contact C, int nblocks);
 __global__ void cs_contact_write_kernel(Batch B, Contact C);
@@ -676,6 +678,7 @@ void freeBatch(cs_ctx* c) {
     c->prox.release();
     for (void* p : c->contactAllocs) cudaFree(p);
     c->contactAllocs.clear();
+    if (c->contact.pairs) cudaFree(c->contact.pairs);
     c->contact = Contact();
     c->contactReady = false;
     c->sheetGroupDev = nullptr;
@@ -1522,6 +1525,7 @@ cs_status buildContact(cs_ctx* c) {
     CAL(C.keys, (long long)C.n_keys);
     CAL(C.block_count, (C.n_keys + CS_CONTACT_ITEMS - 1) / CS_CONTACT_ITEMS);
     CAL(C.total, 1);
+    CAL(C.pair_count, 1);
     CAL(c->sheetGroupDev, B.S);
 #undef CAL
     c->contactReady = true;
@@ -1565,7 +1569,25 @@ cs_status cs_detect_proximities(cs_ctx* c, const cs_detect_params* p, int* count
     cs_contact_face_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C);
     cs_contact_node_kernel<<<nblk(B.N, 128), 128, 0, c->stream>>>(B, C);
     cs_contact_grid_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C, c->sheetGroupDev);
-    cs_contact_pair_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C, c->sheetGroupDev);
+    // candidate pairs (regrown and repeated when the buffer was too small)
+    int npairs = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        if (C.pair_cap == 0 || npairs > C.pair_cap) {
+            size_t cap = (size_t)C.pair_cap;
+            if ((st = grow(c, C.pairs, cap, std::max<size_t>((size_t)npairs, 8 * (size_t)B.F))) != CS_OK) return st;
+            C.pair_cap = (int)std::min<size_t>(cap, INT32_MAX);
+        }
+        CS_CUDA(cudaMemsetAsync(C.pair_count, 0, sizeof(int), c->stream));
+        cs_contact_pair_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C, c->sheetGroupDev);
+        CS_CUDA(cudaMemcpyAsync(&npairs, C.pair_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CS_CUDA(cudaStreamSynchronize(c->stream));
+        if (npairs <= C.pair_cap) break;
+    }
+    if (npairs > C.pair_cap) return fail(c, CS_ERR_STATE, "candidate pair buffer overflow");
+    if (npairs > 0) {
+        cs_contact_vf_kernel<<<nblk(6LL * npairs, 256), 256, 0, c->stream>>>(B, C, npairs);
+        cs_contact_ee_kernel<<<nblk(9LL * npairs, 256), 256, 0, c->stream>>>(B, C, npairs);
+    }
     cs_contact_count_kernel<<<nblocks, 256, 0, c->stream>>>(C);
     cs_contact_scan_kernel<<<1, 1024, 0, c->stream>>>(C, nblocks);
     CS_CUDA(cudaGetLastError());
