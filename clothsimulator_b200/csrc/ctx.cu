@@ -1339,6 +1339,7 @@ void clearProximities(cs_ctx* c) {
 cs_status applyProximities(cs_ctx* c, int n, float thickness) {
     Batch& B = c->B;
     ProxBuffers& P = c->prox;
+    if (n == 0 && P.n == 0 && B.n_pinst == 0) return CS_OK;  // none before, none now: nothing changes
     destroyGraphs(c);  // the captured launches hold the old lists
     clearProximities(c);
     std::vector<int> touched(B.S, 0);

@@ -329,6 +329,7 @@ Simulator::Simulator(SimulationMode mode, const std::string& path, const std::st
     gravity_ = parseVec3(json_["gravity"]);
     wind_ = Wind(json_["wind"]);
     magic_ = Magic(json_["magic"]);
+    clothFriction_ = parseFloat(json_["friction"], 0.6f);  // Simulator.cu:25
     solver_ = parseSolver(json_["solver"]);
     for (const Json& c : json_["cloths"].items()) cloths_.emplace_back(c, wind_);
     if (cloths_.empty()) throw std::runtime_error("scene has no cloths");
@@ -393,7 +394,16 @@ void Simulator::loadBatch(int device) {
     }
 }
 
+// Simulator.cu:571-600: proximities among the cloths' current states (findProximitiesGpu), then
+// every cloth's implicit step with them, then the position update (inside cs_step).
 void Simulator::physicsStep() {
+    cs_detect_params dp{};
+    dp.repulsion_thickness = magic_.repulsionThickness;
+    dp.collision_stiffness = magic_.collisionStiffness;
+    dp.friction = clothFriction_;
+    dp.sheet_group = nullptr;  // the cloths of one scene interact
+    if (cs_detect_proximities(ctx_, &dp, &proximities_) != CS_OK)
+        throw std::runtime_error(std::string("cs_detect_proximities: ") + cs_last_error(ctx_));
     cs_step_params p{};
     p.dt = dt_;
     p.gravity[0] = gravity_.x;
@@ -418,8 +428,8 @@ void Simulator::simulateStep() {
     if ((++nSteps_) % frameSteps_ == 0) nFrames_++;
     std::cout << "Frame [" << nFrames_ << "], Step [" << nSteps_ << "]:" << std::endl;
     physicsStep();
-    std::cout << "Physics Step: " << stats_.ms / 1000.0 << "s (" << stats_.max_iters << " CG iterations, relative residual "
-              << stats_.max_rel_residual << ")" << std::endl;
+    std::cout << "Physics Step: " << stats_.ms / 1000.0 << "s (" << proximities_ << " proximities, " << stats_.max_iters
+              << " CG iterations, relative residual " << stats_.max_rel_residual << ")" << std::endl;
     if (nSteps_ % frameSteps_ == 0) save();
 }
 

@@ -124,6 +124,7 @@ public:
     int frames() const { return nFrames_; }
     std::vector<Cloth>& cloths() { return cloths_; }
     cs_step_stats lastStats() const { return stats_; }
+    int lastProximities() const { return proximities_; }
 
 private:
     SimulationMode mode_;
@@ -134,6 +135,8 @@ private:
     Vec3 gravity_;
     Wind wind_;
     Magic magic_;
+    float clothFriction_ = 0.6f;  // Simulator.cu:25
+    int proximities_ = 0;
     SolverOptions solver_;
     std::vector<Cloth> cloths_;
     cs_ctx* ctx_ = nullptr;

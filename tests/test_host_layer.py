@@ -96,6 +96,7 @@ def test_simulate_offline_matches_c_abi(tmp_path):
     p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=1e-8, max_iters=8000)
     for k in range(8):
         p.warm_start = native.WARM_ZERO if k == 0 else native.WARM_PREVIOUS
+        ctx.detect_proximities(1e-3)  # the host layer detects before every step, as Simulator.cu:571-586
         ctx.step(p)
     x, _ = ctx.get_state()
     assert np.array_equal(np.array(xs, np.float32), x)
@@ -106,4 +107,41 @@ def test_simulate_offline_matches_c_abi(tmp_path):
     st = lib.cs_sim_run(b"resume_offline", b"", out.encode(), 0, ctypes.byref(steps))
     assert st == 0, lib.cs_sim_last_error()
     assert os.path.exists(os.path.join(out, "frame3_cloth0.obj"))
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_contact_scene_through_host_layer_matches_c_abi(tmp_path):
+    """Two sheets stacked 1.5 mm apart: the host layer detects proximities before every step
+    (Simulator::physicsStep, Simulator.cu:571-586) and steps with them; the same sequence through
+    the C ABI gives the same frames bit for bit."""
+    scene = scenes.stacked_sheets(10, n_layers=2, seed=4)
+    path = scenes.write_scene(scene, str(tmp_path / "scene"), frames=1,
+                              solver={"tol": 1e-8, "max_iters": 8000, "warm_start": "previous"})
+    out = str(tmp_path / "out")
+    lib = host()
+    steps = ctypes.c_int(0)
+    st = lib.cs_sim_run(b"simulate_offline", path.encode(), out.encode(), 0, ctypes.byref(steps))
+    assert st == 0, lib.cs_sim_last_error()
+    cfg = json.loads(open(path).read().split("\n", 1)[1])  # after the generator's comment line
+    n_steps = int(cfg["frame_steps"])
+    assert steps.value == n_steps
+    ctx = native.Context(0)
+    ctx.load(scene.sheets)
+    p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=1e-8, max_iters=8000)
+    found = []
+    for k in range(n_steps):
+        p.warm_start = native.WARM_ZERO if k == 0 else native.WARM_PREVIOUS
+        found.append(ctx.detect_proximities(1e-3, 1e9, 0.6))
+        ctx.step(p)
+    assert min(found) > 0
+    x, _ = ctx.get_state()
+    x = x.reshape(-1, 3)
+    o = 0
+    for i, s in enumerate(scene.sheets):
+        n = s["x"].shape[0]
+        xs = [list(map(float, l.split()[1:])) for l in open(os.path.join(out, f"frame1_cloth{i}.obj"))
+              if l.startswith("v ")]
+        assert np.array_equal(np.array(xs, np.float32), x[o:o + n])
+        o += n
     ctx.close()
