@@ -1,0 +1,462 @@
+// The collision step on the device (cs_collision_step): Simulator::collisionStep as the
+// reference's GPU path runs it after the implicit step (Simulator.cu:602-684).
+//
+// Each round: candidate face pairs from the contact grid over the start-of-step and current
+// positions (contact.cu with ccd bounds, dilated by the collision thickness), then
+//   cs_impact_vf/ee_kernel   thread per (pair, test): the bounds check and continuous
+//                            impact test of checkVertexFaceImpact / checkEdgeEdgeImpact
+//                            (CollisionHelper.cu:61-136: the cubic for coplanarity along the
+//                            linear trajectories, solveCubic / solveQuadratic /
+//                            newtonsMethod :3-59, the distance and side at the root);
+//   cs_impact_sort_kernel    rank sort by impact time (ties by node ids);
+//   cs_impact_select_kernel  the independent impacts, earliest first, one per node
+//                            (Simulator.cu:394-420; one thread, sequential by definition);
+//   cs_opt_*_kernel          the impact zone's nodes (ascending), each impact's node slots,
+//                            each node's constraint list in constraint order;
+//   cs_opt_kernel            one CTA: CollisionOptimization (CollisionOptimization.cu) solved
+//                            by Optimization::solve's augmented Lagrangian gradient descent
+//                            (Optimization.cu:94-137).  Element terms are computed in
+//                            parallel; every sum runs in the CPU loop's order on one thread,
+//                            so the iterates are the FP32 CPU path's bit for bit.
+// After the rounds, cs_collide_velocity_kernel sets v = (x - x0) / dt (Mesh.cu:238-247).
+// Built without FMA contraction.
+#include "cs_internal.h"
+
+namespace {
+
+struct f3 {
+    float x, y, z;
+};
+__device__ __forceinline__ f3 mk(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ f3 ld(const float* p, int i) { return mk(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+__device__ __forceinline__ void st(float* p, int i, f3 a) {
+    p[3 * i] = a.x;
+    p[3 * i + 1] = a.y;
+    p[3 * i + 2] = a.z;
+}
+__device__ __forceinline__ f3 sub(f3 a, f3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ f3 add(f3 a, f3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ f3 scl(float s, f3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+// Vector.cuh:126-176 (dot and norm2 from zero, division by the reciprocal)
+__device__ __forceinline__ float dot0(f3 a, f3 b) {
+    float s = 0.0f;
+    s += a.x * b.x;
+    s += a.y * b.y;
+    s += a.z * b.z;
+    return s;
+}
+__device__ __forceinline__ f3 dvd(f3 a, float s) {
+    const float inv = 1.0f / s;
+    return mk(a.x * inv, a.y * inv, a.z * inv);
+}
+__device__ __forceinline__ f3 normalized(f3 a) { return dvd(a, sqrtf(dot0(a, a))); }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float mixed(f3 a, f3 b, f3 c) { return dot0(a, cross(b, c)); }  // MathHelper.cuh:43-45
+__device__ __forceinline__ float mn(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float mx(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float ab(float x) { return x < 0.0f ? -x : x; }
+
+// signedVertexFaceDistance / signedEdgeEdgeDistance (MathHelper.cu:38-69); false for INFINITY
+__device__ bool signed_vf(f3 x, f3 y0, f3 y1, f3 y2, f3& n, float w[4], float& h) {
+    n = cross(normalized(sub(y1, y0)), normalized(sub(y2, y0)));
+    if (dot0(n, n) < 1e-6f) return false;
+    n = normalized(n);
+    h = dot0(sub(x, y0), n);
+    const float b0 = mixed(sub(y1, x), sub(y2, x), n);
+    const float b1 = mixed(sub(y2, x), sub(y0, x), n);
+    const float b2 = mixed(sub(y0, x), sub(y1, x), n);
+    w[0] = 1.0f;
+    w[1] = -b0 / (b0 + b1 + b2);
+    w[2] = -b1 / (b0 + b1 + b2);
+    w[3] = -b2 / (b0 + b1 + b2);
+    return true;
+}
+__device__ bool signed_ee(f3 x0, f3 x1, f3 y0, f3 y1, f3& n, float w[4], float& h) {
+    n = cross(normalized(sub(x1, x0)), normalized(sub(y1, y0)));
+    if (dot0(n, n) < 1e-6f) return false;
+    n = normalized(n);
+    h = dot0(sub(x0, y0), n);
+    const float a0 = mixed(sub(y1, x1), sub(y0, x1), n);
+    const float a1 = mixed(sub(y0, x0), sub(y1, x0), n);
+    const float b0 = mixed(sub(x0, y1), sub(x1, y1), n);
+    const float b1 = mixed(sub(x1, y0), sub(x0, y0), n);
+    w[0] = a0 / (a0 + a1);
+    w[1] = a1 / (a0 + a1);
+    w[2] = -b0 / (b0 + b1);
+    w[3] = -b1 / (b0 + b1);
+    return true;
+}
+
+// CollisionHelper.cu:3-20
+__device__ float newtons_method(float a, float b, float c, float d, float x0, int dir) {
+    if (dir != 0) {
+        const float y0 = d + x0 * (c + x0 * (b + x0 * a));
+        const float ddy0 = 2.0f * b + x0 * (6.0f * a);
+        x0 += (float)dir * sqrtf(ab(2.0f * y0 / ddy0));
+    }
+    for (int iter = 0; iter < 100; iter++) {
+        const float y = d + x0 * (c + x0 * (b + x0 * a));
+        const float dy = c + x0 * (2.0f * b + 3.0f * x0 * a);
+        if (dy == 0) return x0;
+        const float x1 = x0 - y / dy;
+        if (ab(x0 - x1) < 1e-6f) return x0;
+        x0 = x1;
+    }
+    return x0;
+}
+
+// CollisionHelper.cu:22-37
+__device__ int solve_quadratic(float a, float b, float c, float x[2]) {
+    const float d = b * b - 4.0f * a * c;
+    if (d < 0.0f) {
+        x[0] = -b / (2.0f * a);
+        return 0;
+    }
+    const float q = -(b + (float)(b < 0.0f ? -1 : 1) * sqrtf(d)) * 0.5f;
+    int i = 0;
+    if (ab(a) > 1e-12f * ab(q)) x[i++] = q / a;
+    if (ab(q) > 1e-12f * ab(c)) x[i++] = c / q;
+    if (i == 2 && x[0] > x[1]) {
+        const float t = x[0];
+        x[0] = x[1];
+        x[1] = t;
+    }
+    return i;
+}
+
+// CollisionHelper.cu:39-59.  Where solve_quadratic finds no root without writing one (both of
+// its guards fail: a degenerate derivative), Newton's method starts from 0, as the oracle does
+// (the reference reads an uninitialised value there).
+__device__ int solve_cubic(float a, float b, float c, float d, float x[3]) {
+    float xc[2] = {0.0f, 0.0f};
+    const int n = solve_quadratic(3.0f * a, 2.0f * b, c, xc);
+    if (n == 0) {
+        x[0] = newtons_method(a, b, c, d, xc[0], 0);
+        return 1;
+    }
+    if (n == 1) return solve_quadratic(b, c, d, x);
+    const float yc[2] = {d + xc[0] * (c + xc[0] * (b + xc[0] * a)), d + xc[1] * (c + xc[1] * (b + xc[1] * a))};
+    int i = 0;
+    if (yc[0] * a >= 0.0f) x[i++] = newtons_method(a, b, c, d, xc[0], -1);
+    if (yc[0] * yc[1] <= 0.0f) {
+        const int closer = ab(yc[0]) < ab(yc[1]) ? 0 : 1;
+        x[i++] = newtons_method(a, b, c, d, xc[closer], closer == 0 ? 1 : -1);
+    }
+    if (yc[1] * a <= 0.0f) x[i++] = newtons_method(a, b, c, d, xc[1], 1);
+    return i;
+}
+
+// checkImpact (CollisionHelper.cu:61-110)
+__device__ bool check_impact(int type, const f3 p[4], const f3 q[4], ImpactRec& r) {
+    const f3 x0 = p[0];
+    const f3 v0 = sub(q[0], x0);
+    const f3 x1 = sub(p[1], x0), x2 = sub(p[2], x0), x3 = sub(p[3], x0);
+    const f3 v1 = sub(sub(q[1], p[1]), v0), v2 = sub(sub(q[2], p[2]), v0), v3 = sub(sub(q[3], p[3]), v0);
+    const float a0 = mixed(x1, x2, x3);
+    const float a1 = mixed(v1, x2, x3) + mixed(x1, v2, x3) + mixed(x1, x2, v3);
+    const float a2 = mixed(x1, v2, v3) + mixed(v1, x2, v3) + mixed(v1, v2, x3);
+    const float a3 = mixed(v1, v2, v3);
+    float t[3] = {0.0f, 0.0f, 0.0f};
+    const int ns = solve_cubic(a3, a2, a1, a0, t);
+    for (int i = 0; i < ns; i++) {
+        if (t[i] < 0.0f || t[i] > 1.0f) continue;
+        f3 y[4];
+        for (int k = 0; k < 4; k++) y[k] = add(p[k], scl(t[i], sub(q[k], p[k])));  // Node::position
+        f3 n;
+        float w[4], h;
+        bool inside;
+        if (type == 0) {
+            if (!signed_vf(y[0], y[1], y[2], y[3], n, w, h)) continue;
+            inside = mn(-w[1], mn(-w[2], -w[3])) >= -1e-6f;
+        } else {
+            if (!signed_ee(y[0], y[1], y[2], y[3], n, w, h)) continue;
+            inside = mn(mn(w[0], w[1]), mn(-w[2], -w[3])) >= -1e-6f;
+        }
+        if (dot0(n, add(add(scl(w[1], v1), scl(w[2], v2)), scl(w[3], v3))) > 0.0f) n = mk(-n.x, -n.y, -n.z);
+        if (ab(h) < 1e-6f && inside) {
+            r.type = type;
+            r.t = t[i];
+            for (int k = 0; k < 4; k++) r.w[k] = w[k];
+            r.n[0] = n.x;
+            r.n[1] = n.y;
+            r.n[2] = n.z;
+            return true;
+        }
+    }
+    return false;
+}
+
+// Bounds of a node set over its start and current positions (Node/Face/Edge::bounds(ccd)).
+__device__ void ccd_box(const Batch& B, const int* nodes, int k, float lo[3], float hi[3]) {
+    for (int c = 0; c < 3; c++) {
+        lo[c] = 3.0e38f;
+        hi[c] = -3.0e38f;
+    }
+    for (int i = 0; i < k; i++) {
+        const float* a = B.x + 3 * (size_t)nodes[i];
+        const float* b = B.x0 + 3 * (size_t)nodes[i];
+        for (int c = 0; c < 3; c++) {
+            lo[c] = mn(mn(lo[c], a[c]), b[c]);
+            hi[c] = mx(mx(hi[c], a[c]), b[c]);
+        }
+    }
+}
+// Bounds::overlap(b, thickness) (Bounds.cu:85-101): a against b dilated
+__device__ bool overlap(const float alo[3], const float ahi[3], const float blo[3], const float bhi[3], float t) {
+    for (int c = 0; c < 3; c++) {
+        if (alo[c] > bhi[c] + t) return false;
+        if (ahi[c] < blo[c] - t) return false;
+    }
+    return true;
+}
+
+__device__ void impact_test(const Batch& B, const Collide& K, int type, const int nodes[4]) {
+    float alo[3], ahi[3], blo[3], bhi[3];
+    if (type == 0) {
+        ccd_box(B, nodes, 1, alo, ahi);
+        ccd_box(B, nodes + 1, 3, blo, bhi);
+    } else {
+        ccd_box(B, nodes, 2, alo, ahi);
+        ccd_box(B, nodes + 2, 2, blo, bhi);
+    }
+    if (!overlap(alo, ahi, blo, bhi, K.thickness)) return;
+    f3 p[4], q[4];
+    for (int k = 0; k < 4; k++) {
+        p[k] = ld(B.x0, nodes[k]);
+        q[k] = ld(B.x, nodes[k]);
+    }
+    ImpactRec r;
+    if (!check_impact(type, p, q, r)) return;
+    for (int k = 0; k < 4; k++) r.nodes[k] = nodes[k];
+    const int slot = atomicAdd(&K.counters[0], 1);
+    if (slot < K.found_cap) K.found[slot] = r;
+}
+
+__device__ __forceinline__ bool before(const ImpactRec& a, const ImpactRec& b) {
+    if (a.t != b.t) return a.t < b.t;
+    for (int i = 0; i < 4; i++)
+        if (a.nodes[i] != b.nodes[i]) return a.nodes[i] < b.nodes[i];
+    return a.type < b.type;
+}
+
+}  // namespace
+
+// checkImpacts (Simulator.cu:369-381), vertex-face part: (pair, corner) per thread.
+__global__ void __launch_bounds__(256) cs_impact_vf_kernel(Batch B, Contact C, Collide K, int npairs) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6LL * npairs) return;
+    const int p = (int)(t / 6), k = (int)(t % 6);
+    const int2 pr = C.pairs[p];
+    const int f = k < 3 ? pr.x : pr.y, g = k < 3 ? pr.y : pr.x;
+    const int4 y = B.face_nodes[f], z = B.face_nodes[g];
+    const int i = k % 3;
+    const int node = i == 0 ? y.x : i == 1 ? y.y : y.z;
+    if (node == z.x || node == z.y || node == z.z) return;
+    const int nodes[4] = {node, z.x, z.y, z.z};
+    impact_test(B, K, 0, nodes);
+}
+
+// edge-edge part: (pair, edge of the first face, edge of the second) per thread.
+__global__ void __launch_bounds__(256) cs_impact_ee_kernel(Batch B, Contact C, Collide K, int npairs) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 9LL * npairs) return;
+    const int p = (int)(t / 9), k = (int)(t % 9);
+    const int2 pr = C.pairs[p];
+    const int4 fe = C.face_edges[pr.x], ge = C.face_edges[pr.y];
+    const int i = k / 3, j = k % 3;
+    const int4 a = C.edges[i == 0 ? fe.x : i == 1 ? fe.y : fe.z], b = C.edges[j == 0 ? ge.x : j == 1 ? ge.y : ge.z];
+    if (a.x == b.x || a.x == b.y || a.y == b.x || a.y == b.y) return;
+    const int nodes[4] = {a.x, a.y, b.x, b.y};
+    impact_test(B, K, 1, nodes);
+}
+
+// Rank sort of the round's impacts (their number is small).
+__global__ void __launch_bounds__(256) cs_impact_sort_kernel(Collide K, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const ImpactRec a = K.found[i];
+    int rank = 0;
+    for (int j = 0; j < n; j++) {
+        const ImpactRec& b = K.found[j];
+        rank += (before(b, a) || (j < i && !before(a, b))) ? 1 : 0;
+    }
+    K.sorted[rank] = a;
+}
+
+// independentImpacts (Simulator.cu:394-420): earliest first, each node in one impact.
+__global__ void cs_impact_select_kernel(Collide K, int n, int base, int cap) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int m = 0;
+    for (int i = 0; i < n; i++) {
+        const ImpactRec& r = K.sorted[i];
+        bool ok = true;
+        for (int k = 0; k < 4; k++) ok &= K.used[r.nodes[k]] == 0;
+        if (!ok) continue;
+        if (base + m < cap) K.all[base + m] = r;
+        m++;
+        for (int k = 0; k < 4; k++) K.used[r.nodes[k]] = 1;
+    }
+    for (int i = 0; i < m && base + i < cap; i++)
+        for (int k = 0; k < 4; k++) K.used[K.all[base + i].nodes[k]] = 0;
+    K.counters[1] = m;
+}
+
+// The projection's nodes: marked, then (after an exclusive scan of mark) listed ascending.
+__global__ void cs_opt_mark_kernel(Collide K, int nc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * nc) return;
+    K.mark[K.all[t >> 2].nodes[t & 3]] = 1;
+}
+__global__ void cs_opt_nodes_kernel(Collide K, int N) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    if (K.mark[i + 1] > K.mark[i]) K.nodes[K.mark[i]] = i;
+}
+__global__ void cs_opt_idx_kernel(Collide K, int nc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * nc) return;
+    const int slot = K.mark[K.all[t >> 2].nodes[t & 3]];
+    K.idx[t] = slot;
+    atomicAdd(&K.nptr[slot], 1);
+}
+__global__ void cs_opt_fill_kernel(Collide K, int nc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * nc) return;
+    const int slot = K.idx[t];
+    K.nlist[K.nptr[slot] + atomicAdd(&K.nfill[slot], 1)] = t;
+}
+__global__ void cs_opt_sort_kernel(Collide K, int nn) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nn) return;
+    const int q0 = K.nptr[s], q1 = K.nptr[s + 1];
+    for (int q = q0 + 1; q < q1; q++) {
+        const int v = K.nlist[q];
+        int r = q - 1;
+        while (r >= q0 && K.nlist[r] > v) {
+            K.nlist[r + 1] = K.nlist[r];
+            r--;
+        }
+        K.nlist[r + 1] = v;
+    }
+}
+
+namespace {
+constexpr float kMu = 1e3f;          // Optimization::solve (Optimization.cu:96)
+constexpr float kEpsS = 1e-12f;      // Optimization.cuh:16
+constexpr float kEpsF = 1e-10f;      // Optimization.cuh:17
+constexpr int kMaxOptIterations = 100;
+
+// CollisionOptimization::constraint (CollisionOptimization.cu:91-103)
+__device__ float constraint(const Collide& K, const float* x, int c) {
+    const ImpactRec& r = K.all[c];
+    const f3 n = mk(r.n[0], r.n[1], r.n[2]);
+    float a = -K.thickness;
+    for (int k = 0; k < 4; k++) a += r.w[k] * dot0(n, ld(x, K.idx[4 * c + k]));
+    return a;
+}
+
+// Optimization::value's terms at x: per node mass |x - x1|^2, per constraint its clamped
+// violation (coef) and 0.5 mu coef^2.
+__device__ void value_terms(const Batch& B, const Collide& K, const float* x, int nn, int nc) {
+    for (int i = threadIdx.x; i < nn; i += blockDim.x) {
+        const int node = K.nodes[i];
+        const f3 d = sub(ld(x, i), ld(K.x1, node));
+        K.nterm[i] = B.mass[node] * dot0(d, d);
+    }
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+        const float co = mn(constraint(K, x, c) + K.lambda[c] / kMu, 0.0f);  // clampViolation(x, +1)
+        K.coef[c] = co;
+        K.cterm[c] = 0.5f * kMu * (co * co);
+    }
+}
+
+// The sum of those terms in the CPU loop's order (thread 0).
+__device__ float value_sum(const Collide& K, int nn, int nc, float invMass) {
+    float a = 0.0f;
+    for (int i = 0; i < nn; i++) a += K.nterm[i];
+    a = 0.5f * a * invMass;
+    for (int c = 0; c < nc; c++)
+        if (K.coef[c] != 0.0f) a += K.cterm[c];
+    return a;
+}
+}  // namespace
+
+// One CTA: Optimization::solve (Optimization.cu:94-137) of CollisionOptimization over the
+// accumulated impacts; the result is written back into B.x.
+__global__ void __launch_bounds__(1024) cs_opt_kernel(Batch B, Collide K, int nn, int nc) {
+    __shared__ float sf, sft, ss, sg2, sInv;
+    __shared__ int sgo;
+    const int tid = threadIdx.x, T = blockDim.x;
+    for (int i = tid; i < nn; i += T) st(K.cur, i, ld(B.x, K.nodes[i]));
+    for (int c = tid; c < nc; c += T) K.lambda[c] = 0.0f;
+    if (tid == 0) {
+        // CollisionOptimization.cu:22-35: the mean inverse mass
+        float inv = 0.0f;
+        for (int i = 0; i < nn; i++) inv += 1.0f / B.mass[K.nodes[i]];
+        sInv = inv / (float)nn;
+        ss = 1e-3f * (float)nn;
+    }
+    __syncthreads();
+    const float invMass = sInv;
+    for (int iter = 0; iter < kMaxOptIterations; iter++) {
+        // valueAndGradient (Optimization.cu:51-63) at cur
+        value_terms(B, K, K.cur, nn, nc);
+        __syncthreads();
+        for (int i = tid; i < nn; i += T) {
+            const int node = K.nodes[i];
+            f3 g = scl(invMass * B.mass[node], sub(ld(K.cur, i), ld(K.x1, node)));
+            for (int q = K.nptr[i]; q < K.nptr[i + 1]; q++) {
+                const int c = K.nlist[q] >> 2, k = K.nlist[q] & 3;
+                const float co = K.coef[c];
+                if (co == 0.0f) continue;
+                const ImpactRec& r = K.all[c];
+                g = add(g, scl((kMu * co) * r.w[k], mk(r.n[0], r.n[1], r.n[2])));
+            }
+            st(K.grad, i, g);
+            K.gterm[i] = dot0(g, g);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            sf = value_sum(K, nn, nc, invMass);
+            float g2 = 0.0f;
+            for (int i = 0; i < nn; i++) g2 += K.gterm[i];
+            sg2 = g2;
+            ss /= 0.7f;
+        }
+        __syncthreads();
+        // backtracking line search
+        for (;;) {
+            if (tid == 0) ss *= 0.7f;
+            __syncthreads();
+            const float s = ss;
+            for (int i = tid; i < nn; i += T) st(K.next, i, sub(ld(K.cur, i), scl(s, ld(K.grad, i))));
+            __syncthreads();
+            value_terms(B, K, K.next, nn, nc);
+            __syncthreads();
+            if (tid == 0) {
+                const float ft = value_sum(K, nn, nc, invMass);
+                sft = ft;
+                sgo = (ft >= sf - 0.5f * s * sg2 && s >= kEpsS && ab(sf - ft) >= kEpsF) ? 1 : 0;
+            }
+            __syncthreads();
+            if (!sgo) break;
+        }
+        if (ss < kEpsS || ab(sf - sft) < kEpsF) break;
+        for (int i = tid; i < nn; i += T) st(K.cur, i, ld(K.next, i));
+        __syncthreads();
+        // updateMultiplier (Optimization.cu:85-92)
+        for (int c = tid; c < nc; c += T) K.lambda[c] = mn(K.lambda[c] + kMu * constraint(K, K.cur, c), 0.0f);
+        __syncthreads();
+    }
+    __syncthreads();
+    for (int i = tid; i < nn; i += T) st(B.x, K.nodes[i], ld(K.cur, i));
+}
+
+// Mesh::updateVelocities (Mesh.cu:238-247): v = (x - x0) * (1 / dt)
+__global__ void cs_collide_velocity_kernel(Batch B, float invDt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * B.N) return;
+    B.v[i] = (B.x[i] - B.x0[i]) * invDt;
+}

@@ -152,8 +152,7 @@ __device__ void check_ee(const Batch& B, const Contact& C, int e0, int e1) {
 }
 
 __device__ __forceinline__ float cell_size(const Contact& C) {
-    const float t = 2.0f * C.repulsion;
-    return (__uint_as_float(C.ext[0]) + 2.0f * t) * 1.0001f + 1e-30f;
+    return (__uint_as_float(C.ext[0]) + 2.0f * C.dilate) * 1.0001f + 1e-30f;
 }
 __device__ __forceinline__ int cell_of(float v, float c) {
     return (int)fminf(fmaxf(floorf(v / c), -1073741824.0f), 1073741824.0f);
@@ -180,8 +179,17 @@ __global__ void __launch_bounds__(128) cs_contact_face_kernel(Batch B, Contact C
     C.fn[3 * (size_t)f] = n.x;
     C.fn[3 * (size_t)f + 1] = n.y;
     C.fn[3 * (size_t)f + 2] = n.z;
-    const float lo[3] = {mn(mn(a.x, b.x), c.x), mn(mn(a.y, b.y), c.y), mn(mn(a.z, b.z), c.z)};
-    const float hi[3] = {mx(mx(a.x, b.x), c.x), mx(mx(a.y, b.y), c.y), mx(mx(a.z, b.z), c.z)};
+    float lo[3] = {mn(mn(a.x, b.x), c.x), mn(mn(a.y, b.y), c.y), mn(mn(a.z, b.z), c.z)};
+    float hi[3] = {mx(mx(a.x, b.x), c.x), mx(mx(a.y, b.y), c.y), mx(mx(a.z, b.z), c.z)};
+    if (C.ccd) {  // Face::bounds(ccd) (Face.cu:94-103): the start-of-step positions too
+        const v3 a0 = ldx(B.x0, y.x), b0 = ldx(B.x0, y.y), c0 = ldx(B.x0, y.z);
+        const float l0[3] = {mn(mn(a0.x, b0.x), c0.x), mn(mn(a0.y, b0.y), c0.y), mn(mn(a0.z, b0.z), c0.z)};
+        const float h0[3] = {mx(mx(a0.x, b0.x), c0.x), mx(mx(a0.y, b0.y), c0.y), mx(mx(a0.z, b0.z), c0.z)};
+        for (int k = 0; k < 3; k++) {
+            lo[k] = mn(lo[k], l0[k]);
+            hi[k] = mx(hi[k], h0[k]);
+        }
+    }
     float ext = 0.0f;
     bool finite = true;
     for (int k = 0; k < 3; k++) {
@@ -250,7 +258,7 @@ __global__ void __launch_bounds__(128) cs_contact_pair_kernel(Batch B, Contact C
     int nb = 0;
     if (f < B.F && !C.ext[1]) {
         const float c = cell_size(C);
-        const float t = 2.0f * C.repulsion;  // Simulator.cu:274: traverse with 2 x repulsionThickness
+        const float t = C.dilate;  // 2 x repulsionThickness (Simulator.cu:274) or the collision thickness
         const int group = sheet_group[B.face_nodes[f].w];
         float dlo[3], dhi[3];
         int qlo[3], qhi[3];

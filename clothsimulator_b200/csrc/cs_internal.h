@@ -143,6 +143,7 @@ struct Batch {
     int n_slices = 0, n_panels = 0, n_tpanels = 0, n_tables = 0;
     // nodes
     float *x = nullptr, *v = nullptr, *dv = nullptr, *mass = nullptr;
+    float* x0 = nullptr;     // positions at the start of the last step (Node::x0, Mesh.cu:226-231)
     float4* handle = nullptr;
     double* dv64 = nullptr;
     float* warm = nullptr;   // warm-start vector (previous dv or learned prediction)
@@ -212,6 +213,8 @@ struct Contact {
     int n_keys = 0;          // 2 N + 2 E + 2 F
     int hash_bits = 0;       // grid buckets = 1 << hash_bits
     float repulsion = 0.f, stiffness = 0.f, friction = 0.f;
+    float dilate = 0.f;      // bounds dilation of the candidate pairs (2 x repulsion; collision thickness)
+    int ccd = 0;             // 1: face bounds over x0 and x (continuous impacts)
     const int4* face_edges = nullptr;  // 3 edges + collision group per face
     const int4* edges = nullptr;       // node 0, node 1, face side 0, face side 1
     const int* nf_ptr = nullptr;       // N + 1
@@ -232,6 +235,35 @@ struct Contact {
     int* total = nullptr;
     cs_proximity_desc* out = nullptr;  // detected proximities
     int out_cap = 0;
+};
+
+// Collision step (collide.cu, cs_collision_step): continuous impacts and their projection.
+struct ImpactRec {
+    int nodes[4];
+    float t, w[4], n[3];
+    int type;  // 0 vertex-face, 1 edge-edge
+    int pad[3];
+};
+
+struct Collide {
+    float thickness = 0.f;
+    ImpactRec* found = nullptr;   // impacts of this round
+    int found_cap = 0;
+    int* counters = nullptr;      // [0] impacts found, [1] impacts selected
+    ImpactRec* sorted = nullptr;  // by time (then node ids)
+    ImpactRec* all = nullptr;     // independent impacts accumulated this deformation level
+    int* used = nullptr;          // per node: taken by a selected impact of this round
+    // the projection's nodes and constraints
+    int* mark = nullptr;          // N + 1: node in an impact, then its slot (exclusive scan)
+    int* nodes = nullptr;         // slot -> node, ascending
+    int* idx = nullptr;           // 4 per impact: slots of its nodes
+    int* nptr = nullptr;          // slots + 1: each slot's constraint corners
+    int* nfill = nullptr;
+    int* nlist = nullptr;         // 4 impact + corner, ascending per slot
+    float* x1 = nullptr;          // 3N: positions when the collision step began
+    float *cur = nullptr, *next = nullptr, *grad = nullptr;  // 3 per slot
+    float *lambda = nullptr, *coef = nullptr, *cterm = nullptr;  // per constraint
+    float *nterm = nullptr, *gterm = nullptr;                  // per slot
 };
 
 #define CS_CONTACT_ITEMS 4096  // keys per compaction block (256 threads x 16)

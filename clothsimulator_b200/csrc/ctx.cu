@@ -63,6 +63,17 @@ __global__ void cs_contact_node_kernel(Batch B, Contact C);
 __global__ void cs_contact_grid_kernel(Batch B, Contact C, const int* sheet_group);
 __global__ void cs_contact_pair_kernel(Batch B, Contact C, const int* sheet_group);
 __global__ void cs_contact_vf_kernel(Batch B, Contact C, int npairs);
+__global__ void cs_impact_vf_kernel(Batch B, Contact C, Collide K, int npairs);
+__global__ void cs_impact_ee_kernel(Batch B, Contact C, Collide K, int npairs);
+__global__ void cs_impact_sort_kernel(Collide K, int n);
+__global__ void cs_impact_select_kernel(Collide K, int n, int base, int cap);
+__global__ void cs_opt_mark_kernel(Collide K, int nc);
+__global__ void cs_opt_nodes_kernel(Collide K, int N);
+__global__ void cs_opt_idx_kernel(Collide K, int nc);
+__global__ void cs_opt_fill_kernel(Collide K, int nc);
+__global__ void cs_opt_sort_kernel(Collide K, int nn);
+__global__ void cs_opt_kernel(Batch B, Collide K, int nn, int nc);
+__global__ void cs_collide_velocity_kernel(Batch B, float invDt);
 __global__ void cs_contact_ee_kernel(Batch B, Contact C, int npairs);
 __global__ void cs_contact_count_kernel(Contact C);
 __global__ void cs_contact_scan_kernel(Contact C, int nblocks);
@@ -579,6 +590,10 @@ struct ProxBuffers {
     }
 };
 
+struct CollideCaps {
+    size_t found = 0, all = 0;
+};
+
 struct cs_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -621,6 +636,9 @@ struct cs_ctx {
     bool contactReady = false;
     int* sheetGroupDev = nullptr;
     std::vector<void*> contactAllocs;
+    // collision step (collide.cu)
+    Collide coll;
+    CollideCaps collCaps;
 };
 
 namespace {
@@ -679,6 +697,15 @@ void freeBatch(cs_ctx* c) {
     for (void* p : c->contactAllocs) cudaFree(p);
     c->contactAllocs.clear();
     if (c->contact.pairs) cudaFree(c->contact.pairs);
+    {
+        Collide& K = c->coll;
+        void* ps[] = {K.found, K.counters, K.sorted, K.all, K.used, K.mark, K.nodes, K.idx, K.nptr, K.nfill,
+                      K.nlist, K.x1, K.cur, K.next, K.grad, K.lambda, K.coef, K.cterm, K.nterm, K.gterm};
+        for (void* q : ps)
+            if (q) cudaFree(q);
+        c->coll = Collide();
+        c->collCaps = CollideCaps();
+    }
     c->contact = Contact();
     c->contactReady = false;
     c->sheetGroupDev = nullptr;
@@ -1207,6 +1234,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
 #define AL(field, n) \
     if ((st = dalloc(c, &B.field, (size_t)(n))) != CS_OK) return st;
     AL(dv, 3LL * B.N);
+    AL(x0, 3LL * B.N);
     AL(dv64, 3LL * B.N);
     AL(warm, 3LL * B.N);
     AL(face_rec, (long long)B.F * CS_FACE_REC);
@@ -1226,6 +1254,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     AL(loop, 8);
 #undef AL
     CS_CUDA(cudaMemset(B.dv, 0, 3LL * B.N * sizeof(float)));
+    CS_CUDA(cudaMemcpy(B.x0, B.x, 3LL * B.N * sizeof(float), cudaMemcpyDeviceToDevice));  // Node::Node
     CS_CUDA(cudaMemset(B.warm, 0, 3LL * B.N * sizeof(float)));
     CS_CUDA(cudaMemset(B.A, 0, (size_t)B.n_panels * CS_PANEL_FLOATS * sizeof(float)));
     CS_CUDA(cudaMemset(B.inst, 0, B.S * sizeof(InstState)));
@@ -1533,6 +1562,101 @@ cs_status buildContact(cs_ctx* c) {
     return CS_OK;
 }
 
+// Candidate face pairs of the contact grid (contact.cu) with the dilation and bounds mode set
+// in c->contact: face bounds (and, for proximities, node normals), the grid, the pairs
+// (buffer regrown and the pass repeated when it was too small).
+cs_status candidatePairs(cs_ctx* c, const int* sheetGroup, int& npairs) {
+    Batch& B = c->B;
+    Contact& C = c->contact;
+    cs_status st;
+    std::vector<int> groups(B.S, 0);
+    if (sheetGroup) groups.assign(sheetGroup, sheetGroup + B.S);
+    CS_CUDA(cudaMemcpyAsync(c->sheetGroupDev, groups.data(), B.S * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CS_CUDA(cudaMemsetAsync(C.ext, 0, 2 * sizeof(unsigned), c->stream));
+    CS_CUDA(cudaMemsetAsync(C.head, 0xFF, (sizeof(int) << C.hash_bits), c->stream));
+    cs_contact_face_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C);
+    if (!C.ccd) cs_contact_node_kernel<<<nblk(B.N, 128), 128, 0, c->stream>>>(B, C);
+    cs_contact_grid_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C, c->sheetGroupDev);
+    npairs = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        if (C.pair_cap == 0 || npairs > C.pair_cap) {
+            size_t cap = (size_t)C.pair_cap;
+            if ((st = grow(c, C.pairs, cap, std::max<size_t>((size_t)npairs, 8 * (size_t)B.F))) != CS_OK) return st;
+            C.pair_cap = (int)std::min<size_t>(cap, INT32_MAX);
+        }
+        CS_CUDA(cudaMemsetAsync(C.pair_count, 0, sizeof(int), c->stream));
+        cs_contact_pair_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C, c->sheetGroupDev);
+        CS_CUDA(cudaMemcpyAsync(&npairs, C.pair_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CS_CUDA(cudaStreamSynchronize(c->stream));
+        if (npairs <= C.pair_cap) break;
+    }
+    CS_CUDA(cudaGetLastError());
+    unsigned flags[2];
+    CS_CUDA(cudaMemcpy(flags, C.ext, sizeof(flags), cudaMemcpyDeviceToHost));
+    if (flags[1] & 1u) return fail(c, CS_ERR_INVALID_ARG, "non-finite node state");
+    if (flags[1]) return fail(c, CS_ERR_STATE, "contact grid overflow (flags %u)", flags[1]);
+    if (npairs > C.pair_cap) return fail(c, CS_ERR_STATE, "candidate pair buffer overflow");
+    return CS_OK;
+}
+
+// Scratch of the collision step: node-sized arrays once per batch, impact-sized ones grown.
+cs_status collideScratch(cs_ctx* c, int nFound, int nAll) {
+    Batch& B = c->B;
+    Collide& K = c->coll;
+    CollideCaps& P = c->collCaps;
+    cs_status st;
+    if (!K.mark) {
+        size_t cap = 0;
+        const size_t N = (size_t)B.N;
+        if ((st = grow(c, K.mark, cap = 0, N + 1)) != CS_OK) return st;
+        if ((st = grow(c, K.used, cap = 0, N)) != CS_OK) return st;
+        if ((st = grow(c, K.nodes, cap = 0, N)) != CS_OK) return st;
+        if ((st = grow(c, K.nptr, cap = 0, N + 1)) != CS_OK) return st;
+        if ((st = grow(c, K.nfill, cap = 0, N + 1)) != CS_OK) return st;
+        if ((st = grow(c, K.x1, cap = 0, 3 * N)) != CS_OK) return st;
+        if ((st = grow(c, K.cur, cap = 0, 3 * N)) != CS_OK) return st;
+        if ((st = grow(c, K.next, cap = 0, 3 * N)) != CS_OK) return st;
+        if ((st = grow(c, K.grad, cap = 0, 3 * N)) != CS_OK) return st;
+        if ((st = grow(c, K.nterm, cap = 0, N)) != CS_OK) return st;
+        if ((st = grow(c, K.gterm, cap = 0, N)) != CS_OK) return st;
+        if ((st = grow(c, K.counters, cap = 0, 2)) != CS_OK) return st;
+        CS_CUDA(cudaMemset(K.used, 0, N * sizeof(int)));
+    }
+    if ((size_t)nFound > P.found) {
+        if ((st = grow(c, K.found, P.found, (size_t)nFound)) != CS_OK) return st;
+        size_t cap = 0;
+        if (K.sorted) cudaFree(K.sorted);
+        K.sorted = nullptr;
+        if ((st = grow(c, K.sorted, cap, P.found)) != CS_OK) return st;
+        K.found_cap = (int)std::min<size_t>(P.found, INT32_MAX);
+    }
+    if ((size_t)nAll > P.all) {
+        // the accumulated impacts survive a regrow
+        ImpactRec* old = K.all;
+        const size_t oldCap = P.all;
+        K.all = nullptr;
+        P.all = 0;
+        if ((st = grow(c, K.all, P.all, (size_t)nAll)) != CS_OK) return st;
+        if (old) {
+            CS_CUDA(cudaMemcpyAsync(K.all, old, oldCap * sizeof(ImpactRec), cudaMemcpyDeviceToDevice, c->stream));
+            CS_CUDA(cudaStreamSynchronize(c->stream));
+            cudaFree(old);
+        }
+        size_t cap;
+        for (int** q : {&K.idx, &K.nlist}) {
+            if (*q) cudaFree(*q);
+            *q = nullptr;
+            if ((st = grow(c, *q, cap = 0, 4 * P.all)) != CS_OK) return st;
+        }
+        for (float** q : {&K.lambda, &K.coef, &K.cterm}) {
+            if (*q) cudaFree(*q);
+            *q = nullptr;
+            if ((st = grow(c, *q, cap = 0, P.all)) != CS_OK) return st;
+        }
+    }
+    return CS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1560,31 +1684,12 @@ cs_status cs_detect_proximities(cs_ctx* c, const cs_detect_params* p, int* count
     C.repulsion = p->repulsion_thickness;
     C.stiffness = p->collision_stiffness;
     C.friction = p->friction;
-    std::vector<int> groups(B.S, 0);
-    if (p->sheet_group) groups.assign(p->sheet_group, p->sheet_group + B.S);
-    CS_CUDA(cudaMemcpyAsync(c->sheetGroupDev, groups.data(), B.S * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    CS_CUDA(cudaMemsetAsync(C.ext, 0, 2 * sizeof(unsigned), c->stream));
-    CS_CUDA(cudaMemsetAsync(C.head, 0xFF, (sizeof(int) << C.hash_bits), c->stream));
+    C.dilate = 2.0f * p->repulsion_thickness;  // Simulator.cu:274
+    C.ccd = 0;
+    int npairs = 0;
+    if ((st = candidatePairs(c, p->sheet_group, npairs)) != CS_OK) return st;
     CS_CUDA(cudaMemsetAsync(C.keys, 0xFF, (size_t)C.n_keys * sizeof(unsigned long long), c->stream));
     const int nblocks = (C.n_keys + CS_CONTACT_ITEMS - 1) / CS_CONTACT_ITEMS;
-    cs_contact_face_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C);
-    cs_contact_node_kernel<<<nblk(B.N, 128), 128, 0, c->stream>>>(B, C);
-    cs_contact_grid_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C, c->sheetGroupDev);
-    // candidate pairs (regrown and repeated when the buffer was too small)
-    int npairs = 0;
-    for (int attempt = 0; attempt < 2; attempt++) {
-        if (C.pair_cap == 0 || npairs > C.pair_cap) {
-            size_t cap = (size_t)C.pair_cap;
-            if ((st = grow(c, C.pairs, cap, std::max<size_t>((size_t)npairs, 8 * (size_t)B.F))) != CS_OK) return st;
-            C.pair_cap = (int)std::min<size_t>(cap, INT32_MAX);
-        }
-        CS_CUDA(cudaMemsetAsync(C.pair_count, 0, sizeof(int), c->stream));
-        cs_contact_pair_kernel<<<nblk(B.F, 128), 128, 0, c->stream>>>(B, C, c->sheetGroupDev);
-        CS_CUDA(cudaMemcpyAsync(&npairs, C.pair_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        CS_CUDA(cudaStreamSynchronize(c->stream));
-        if (npairs <= C.pair_cap) break;
-    }
-    if (npairs > C.pair_cap) return fail(c, CS_ERR_STATE, "candidate pair buffer overflow");
     if (npairs > 0) {
         cs_contact_vf_kernel<<<nblk(6LL * npairs, 256), 256, 0, c->stream>>>(B, C, npairs);
         cs_contact_ee_kernel<<<nblk(9LL * npairs, 256), 256, 0, c->stream>>>(B, C, npairs);
@@ -1592,13 +1697,9 @@ cs_status cs_detect_proximities(cs_ctx* c, const cs_detect_params* p, int* count
     cs_contact_count_kernel<<<nblocks, 256, 0, c->stream>>>(C);
     cs_contact_scan_kernel<<<1, 1024, 0, c->stream>>>(C, nblocks);
     CS_CUDA(cudaGetLastError());
-    unsigned flags[2];
     int total = 0;
-    CS_CUDA(cudaMemcpyAsync(flags, C.ext, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
     CS_CUDA(cudaMemcpyAsync(&total, C.total, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CS_CUDA(cudaStreamSynchronize(c->stream));
-    if (flags[1] & 1u) return fail(c, CS_ERR_INVALID_ARG, "non-finite node state");
-    if (flags[1]) return fail(c, CS_ERR_STATE, "proximity grid overflow (flags %u)", flags[1]);
     if ((st = grow(c, c->prox.desc, c->prox.descCap, (size_t)std::max(total, 1))) != CS_OK) return st;
     C.out = c->prox.desc;
     C.out_cap = (int)std::min<size_t>(c->prox.descCap, INT32_MAX);
@@ -1606,6 +1707,92 @@ cs_status cs_detect_proximities(cs_ctx* c, const cs_detect_params* p, int* count
     CS_CUDA(cudaGetLastError());
     if ((st = applyProximities(c, total, p->repulsion_thickness)) != CS_OK) return st;
     if (count) *count = total;
+    return CS_OK;
+}
+
+// Simulator::collisionStep (Simulator.cu:602-684, its GPU branch) after cs_step: rounds of
+// continuous impact detection between x0 and x, selection of independent impacts and
+// projection of all impacts found so far (collide.cu), up to 100 rounds on each of the two
+// deformation levels; then v = (x - x0) / dt for every node.
+cs_status cs_collision_step(cs_ctx* c, const cs_collision_params* p, cs_collision_stats* out) {
+    if (!c || !p) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    if (!(std::isfinite(p->thickness) && p->thickness > 0.0f) || !(std::isfinite(p->dt) && p->dt > 0.0f))
+        return fail(c, CS_ERR_INVALID_ARG, "collision thickness and time step must be positive");
+    CS_CUDA(cudaSetDevice(c->device));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    cs_status st;
+    if (!c->contactReady && (st = buildContact(c)) != CS_OK) return st;
+    Batch& B = c->B;
+    Contact& C = c->contact;
+    Collide& K = c->coll;
+    if ((st = collideScratch(c, 1, 1)) != CS_OK) return st;
+    K.thickness = p->thickness;
+    C.dilate = p->thickness;  // traverse with the collision thickness (Simulator.cu:385)
+    C.ccd = 1;
+    CS_CUDA(cudaMemcpyAsync(K.x1, B.x, 3 * (size_t)B.N * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+    int rounds = 0, total = 0;
+    bool success = false;
+    for (int deform = 0; deform < 2 && !success; deform++) {
+        int nAll = 0;
+        for (int round = 0; round < 100; round++) {
+            rounds++;
+            int npairs = 0;
+            st = candidatePairs(c, p->sheet_group, npairs);
+            if (st != CS_OK) {
+                C.ccd = 0;
+                return st;
+            }
+            int nFound = 0;
+            for (int attempt = 0; attempt < 2; attempt++) {
+                if ((st = collideScratch(c, std::max(nFound, 1024), nAll + 1)) != CS_OK) return st;
+                CS_CUDA(cudaMemsetAsync(K.counters, 0, 2 * sizeof(int), c->stream));
+                if (npairs > 0) {
+                    cs_impact_vf_kernel<<<nblk(6LL * npairs, 256), 256, 0, c->stream>>>(B, C, K, npairs);
+                    cs_impact_ee_kernel<<<nblk(9LL * npairs, 256), 256, 0, c->stream>>>(B, C, K, npairs);
+                }
+                CS_CUDA(cudaMemcpyAsync(&nFound, K.counters, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+                CS_CUDA(cudaStreamSynchronize(c->stream));
+                if (nFound <= K.found_cap) break;
+            }
+            if (nFound == 0) {
+                success = true;
+                break;
+            }
+            if (nFound > K.found_cap) return fail(c, CS_ERR_STATE, "impact buffer overflow");
+            if ((st = collideScratch(c, nFound, nAll + nFound)) != CS_OK) return st;
+            cs_impact_sort_kernel<<<nblk(nFound, 256), 256, 0, c->stream>>>(K, nFound);
+            cs_impact_select_kernel<<<1, 1, 0, c->stream>>>(K, nFound, nAll, (int)c->collCaps.all);
+            int sel[2];
+            CS_CUDA(cudaMemcpyAsync(sel, K.counters, sizeof(sel), cudaMemcpyDeviceToHost, c->stream));
+            CS_CUDA(cudaStreamSynchronize(c->stream));
+            nAll += sel[1];
+            total += sel[1];
+            // the projection's nodes and constraints
+            CS_CUDA(cudaMemsetAsync(K.mark, 0, ((size_t)B.N + 1) * sizeof(int), c->stream));
+            cs_opt_mark_kernel<<<nblk(4LL * nAll, 256), 256, 0, c->stream>>>(K, nAll);
+            int nn = 0;
+            if ((st = scanInts(c, K.mark, B.N, &nn)) != CS_OK) return st;
+            cs_opt_nodes_kernel<<<nblk(B.N, 256), 256, 0, c->stream>>>(K, B.N);
+            CS_CUDA(cudaMemsetAsync(K.nptr, 0, ((size_t)nn + 1) * sizeof(int), c->stream));
+            CS_CUDA(cudaMemsetAsync(K.nfill, 0, ((size_t)nn + 1) * sizeof(int), c->stream));
+            cs_opt_idx_kernel<<<nblk(4LL * nAll, 256), 256, 0, c->stream>>>(K, nAll);
+            if ((st = scanInts(c, K.nptr, nn, nullptr)) != CS_OK) return st;
+            cs_opt_fill_kernel<<<nblk(4LL * nAll, 256), 256, 0, c->stream>>>(K, nAll);
+            cs_opt_sort_kernel<<<nblk(nn, 256), 256, 0, c->stream>>>(K, nn);
+            cs_opt_kernel<<<1, 1024, 0, c->stream>>>(B, K, nn, nAll);
+            CS_CUDA(cudaGetLastError());
+        }
+    }
+    C.ccd = 0;
+    cs_collide_velocity_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B, 1.0f / p->dt);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    if (out) {
+        out->rounds = rounds;
+        out->impacts = total;
+    }
+    if (!success) return fail(c, CS_ERR_NOT_CONVERGED, "collision step failed: impacts remain after %d rounds", rounds);
     return CS_OK;
 }
 

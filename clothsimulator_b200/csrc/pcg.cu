@@ -428,7 +428,9 @@ __global__ void cs_advance_kernel(Batch B) {
     if (B.params->advance) {
         float v = __fadd_rn(B.v[i], d);
         B.v[i] = v;
-        B.x[i] = __fadd_rn(B.x[i], __fmul_rn(B.params->dt, v));
+        const float x = B.x[i];
+        B.x0[i] = x;  // Mesh::updatePositions (Mesh.cu:226-231)
+        B.x[i] = __fadd_rn(x, __fmul_rn(B.params->dt, v));
     }
 }
 

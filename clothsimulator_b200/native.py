@@ -38,7 +38,7 @@ EXPORTED = [
     "cs_solve_block_csr_noalloc", "cs_tc_gemm_check", "cs_mlp_init", "cs_mlp_record", "cs_mlp_fit_normalization",
     "cs_mlp_train", "cs_mlp_gradient", "cs_mlp_predict", "cs_mlp_get_record", "cs_mlp_get_weights",
     "cs_mlp_set_weights", "cs_get_solver_info", "cs_set_proximities", "cs_detect_proximities",
-    "cs_get_proximities",
+    "cs_get_proximities", "cs_collision_step",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -123,6 +123,14 @@ class DetectParams(ctypes.Structure):
     ]
 
 
+class CollisionParams(ctypes.Structure):
+    _fields_ = [("thickness", ctypes.c_float), ("dt", ctypes.c_float), ("sheet_group", ctypes.POINTER(ctypes.c_int32))]
+
+
+class CollisionStats(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_int), ("impacts", ctypes.c_int)]
+
+
 _LIB = None
 
 
@@ -143,6 +151,7 @@ def load_library() -> ctypes.CDLL:
         "cs_set_proximities": [vp, vp, ctypes.c_int, ctypes.c_float],
         "cs_detect_proximities": [vp, ctypes.POINTER(DetectParams), ctypes.POINTER(ctypes.c_int)],
         "cs_get_proximities": [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
+        "cs_collision_step": [vp, ctypes.POINTER(CollisionParams), ctypes.POINTER(CollisionStats)],
         "cs_set_state": [vp, _fp, _fp],
         "cs_get_state": [vp, _fp, _fp],
         "cs_set_state_device": [vp, vp, vp],
@@ -329,6 +338,17 @@ class Context:
         self.check(self.lib.cs_detect_proximities(self.h, ctypes.byref(p), ctypes.byref(n)))
         self.sizes = self.get_sizes()
         return n.value
+
+    def collision_step(self, dt: float, thickness: float = 1e-4, groups=None, allow_unresolved: bool = False):
+        """The collision step after cs_step (cs_collision_step): impacts between the positions at
+        the start of the last step and the current ones are resolved, then v = (x - x0) / dt.
+        Returns (rounds, impacts, status)."""
+        g = None if groups is None else np.ascontiguousarray(groups, np.int32)
+        p = CollisionParams(thickness, dt, g.ctypes.data_as(_ip) if g is not None else None)
+        s = CollisionStats()
+        allow = (CS_OK, CS_ERR_NOT_CONVERGED) if allow_unresolved else (CS_OK,)
+        st = self.check(self.lib.cs_collision_step(self.h, ctypes.byref(p), ctypes.byref(s)), allow)
+        return s.rounds, s.impacts, st
 
     def get_proximities(self) -> dict:
         """The proximities in force, as a dict of arrays (see proximity_records)."""

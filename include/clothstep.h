@@ -185,6 +185,25 @@ cs_status cs_detect_proximities(cs_ctx* ctx, const cs_detect_params* params, int
 /* The proximities in force (set or detected): up to cap records; *count receives how many
  * there are. */
 cs_status cs_get_proximities(cs_ctx* ctx, cs_proximity_desc* out, int cap, int* count);
+
+/* The collision step Simulator::simulateStep runs after every physics step
+ * (Simulator::collisionStep, Simulator.cu:602-684): rounds of continuous impact detection
+ * between each node's position at the start of the last cs_step (x0) and its current one
+ * (CollisionHelper.cu:3-136), selection of independent impacts by impact time
+ * (Simulator.cu:394-420), and projection of the positions onto the impacts' constraints
+ * (optimization/CollisionOptimization.cu, Optimization.cu); then v = (x - x0) / dt for
+ * every node (Mesh.cu:238-247).  On the device.  CS_ERR_NOT_CONVERGED when impacts remain
+ * after 2 x 100 rounds (the reference exits). */
+typedef struct cs_collision_params {
+    float thickness;         /* Magic::collisionThickness, default 1e-4 (Magic.cu:9-16) */
+    float dt;                /* the step's time step */
+    const int* sheet_group;  /* as in cs_detect_params */
+} cs_collision_params;
+typedef struct cs_collision_stats {
+    int rounds;   /* detection rounds run */
+    int impacts;  /* independent impacts projected */
+} cs_collision_stats;
+cs_status cs_collision_step(cs_ctx* ctx, const cs_collision_params* params, cs_collision_stats* stats);
 cs_status cs_get_state(cs_ctx* ctx, float* x, float* v);
 /* Same with device pointers (no host copy). */
 cs_status cs_set_state_device(cs_ctx* ctx, const float* x, const float* v);

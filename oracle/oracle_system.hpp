@@ -143,6 +143,7 @@ struct Cloth {
     std::vector<ProximityRec<T>> prox;
     T proxThickness = T(0);
     std::vector<T> x, v, u;           // 3N, 3N, 2U
+    std::vector<T> x0;                // positions at the start of the last step (Node::x0)
     std::vector<T> finv, farea, fmass, fn;  // per face: 4, 1, 1, 3 (normal)
     std::vector<T> mass;              // per node
     std::vector<int> handleNode;
@@ -156,6 +157,7 @@ struct Cloth {
         topo.build(nn, nv, nf, fxIn, fuIn);
         vnode = vertexNodes(topo);
         x.assign(xIn, xIn + 3 * nn);
+        x0 = x;  // Node::Node (Node.cu:5-11)
         v.assign(vIn, vIn + 3 * nn);
         u.assign(uIn, uIn + 2 * nv);
         finv.resize(4 * nf); farea.resize(nf); fmass.resize(nf); fn.resize(3 * nf);
@@ -421,6 +423,7 @@ struct Cloth {
     void advance(const T* dv, T dt) {
         int n = topo.nNodes;
         for (int i = 0; i < 3 * n; i++) v[i] += dv[i];
+        x0 = x;
         for (int i = 0; i < 3 * n; i++) x[i] += dt * v[i];
         updateGeometry();
     }

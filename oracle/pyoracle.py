@@ -92,6 +92,8 @@ class Lib:
         f("detect_proximities", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _ip, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_double, ctypes.c_int, _ip, _dp, _dp, _dp,
                                                _dp, _dp, _ip])
+        f("collision_step", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _ip, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_int, _ip])
         f("run_cloths", ctypes.c_double, [ctypes.POINTER(_vp), ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, _ip])
         if which == "oracle":
@@ -317,6 +319,17 @@ def detect_proximities(cloths, groups=None, repulsion_thickness: float = 1e-3, c
                              _ptr(out["mu"], _dp), _ptr(out["stiffness"], _dp), _ptr(out["depth"], _dp),
                              _ptr(out["kind"], _ip))
     return out
+
+
+def collision_step(cloths, dt: float, thickness: float = 1e-4, groups=None, max_rounds: int = 0):
+    """Simulator::collisionStep over the cloths after their step (positions x0 -> x): resolves
+    the impacts, then v = (x - x0) / dt.  Returns (rounds, impacts); rounds -1: unresolved."""
+    L = cloths[0].L
+    arr = (_vp * len(cloths))(*[c.h for c in cloths])
+    g = _i(np.zeros(len(cloths)) if groups is None else np.asarray(groups))
+    imp = np.zeros(1, np.int32)
+    rounds = L.collision_step(arr, len(cloths), _ptr(g, _ip), thickness, dt, max_rounds, _ptr(imp, _ip))
+    return int(rounds), int(imp[0])
 
 
 def run_cloths(cloths, params_list, steps: int, method: int = METHOD_LLT, threads: int = 1):

@@ -19,6 +19,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include "CollisionHelper.cuh"
+#include "CollisionOptimization.cuh"
 #include "Edge.cuh"
 #include "Face.cuh"
 #include "Material.cuh"
@@ -27,15 +29,21 @@
 #include "Proximity.cuh"
 #include "Vertex.cuh"
 
+#include "oracle_collide.hpp"
 #include "oracle_detect.hpp"
 #include "oracle_system.hpp"
+
+// The reference's global CPU/GPU switch (main.cu:7): the CPU branches of the optimization run.
+bool gpu = false;
 
 namespace {
 struct ClothBase;
 }
-// Installs the reference's own detection predicates (defined below).
+// Install the reference's own detection predicates and collision step parts (defined below).
 static void orcDetectHooks(orc::Detector& D, const std::vector<ClothBase*>& cloths, const orc::DetectScene& S);
+static void orcCollideHooks(orc::Collider& K, const std::vector<ClothBase*>& cloths, orc::CollideScene& S);
 #define ORC_DETECT_HOOKS 1
+#define ORC_COLLIDE_HOOKS 1
 #define ORC_API(name) ref_##name
 #define ORC_NO_DEFAULT_FACTORIES 1
 #include "oracle_capi.inc"
@@ -326,5 +334,102 @@ static void orcDetectHooks(orc::Detector& D, const std::vector<ClothBase*>& clot
     };
     D.proxEEHook = [=](int a, int b, const orc::DetectParams& P, orc::DetectedProximity& r) {
         fill(Proximity(edge(a), edge(b), P.collisionStiffness, P.clothFriction, 0.3f), r);
+    };
+}
+
+// Collision step parts through the reference's own code: checkVertexFaceImpact and
+// checkEdgeEdgeImpact (CollisionHelper.cu:112-136, with checkImpact and its cubic solver) on
+// the cloths' reference Node/Face/Edge objects, and CollisionOptimization (CPU branch of
+// Optimization::solve, Optimization.cu:94-137) over reference Impacts.  The reference orders
+// the optimization's nodes by address (the memory pool's allocation order, cloth by cloth),
+// so the optimization runs on copies of the scene's nodes laid out in scene order.
+static void orcCollideHooks(orc::Collider& K, const std::vector<ClothBase*>& cloths, orc::CollideScene& S) {
+    struct Span {
+        RefClothImpl* c;
+        int n0, f0, e0;
+        std::vector<int> nodeVert;  // a uv vertex of each node
+    };
+    auto spans = std::make_shared<std::vector<Span>>();
+    int n0 = 0, f0 = 0, e0 = 0;
+    for (ClothBase* b : cloths) {
+        auto* c = static_cast<RefClothImpl*>(b);
+        RefCloth& r = c->rc;
+        Span sp{c, n0, f0, e0, std::vector<int>(r.nodes.size(), -1)};
+        for (size_t i = 0; i < r.nodes.size(); i++) {
+            Node& nd = r.nodes[i];
+            nd.x = Vector3f(S.S.x[3 * (n0 + i)], S.S.x[3 * (n0 + i) + 1], S.S.x[3 * (n0 + i) + 2]);
+            nd.x0 = Vector3f(S.x0[3 * (n0 + i)], S.x0[3 * (n0 + i) + 1], S.x0[3 * (n0 + i) + 2]);
+            nd.x1 = nd.x;  // Mesh::updateNodeGeometries after the physics step (Mesh.cu:185)
+            nd.mass = S.mass[n0 + i];
+            nd.isFree = true;
+        }
+        for (size_t f = 0; f < r.faces.size(); f++)
+            for (int k = 0; k < 3; k++) {
+                const Vertex* v = r.faces[f].vertices[k];
+                sp.nodeVert[v->node - r.nodes.data()] = (int)(v - r.verts.data());
+            }
+        spans->push_back(std::move(sp));
+        n0 += (int)r.nodes.size();
+        f0 += (int)r.faces.size();
+        e0 += (int)r.edges.size();
+    }
+    auto find = [spans](int id, int Span::*off) -> const Span& {
+        size_t k = 0;
+        while (k + 1 < spans->size() && (*spans)[k + 1].*off <= id) k++;
+        return (*spans)[k];
+    };
+    auto sceneId = [spans](const Node* p) {
+        for (const Span& s : *spans) {
+            const std::vector<Node>& v = s.c->rc.nodes;
+            if (p >= v.data() && p < v.data() + v.size()) return s.n0 + (int)(p - v.data());
+        }
+        return -1;
+    };
+    auto nodePtr = [find](int id) {
+        const Span& s = find(id, &Span::n0);
+        return &s.c->rc.nodes[id - s.n0];
+    };
+    K.impactHook = [=](int type, int a, int b, float thickness, orc::Impact& imp) {
+        ::Impact r;
+        bool hit;
+        if (type == 0) {
+            const Span& sn = find(a, &Span::n0);
+            const Span& sf = find(b, &Span::f0);
+            const Vertex* v = &sn.c->rc.verts[sn.nodeVert[a - sn.n0]];
+            hit = checkVertexFaceImpact(v, &sf.c->rc.faces[b - sf.f0], thickness, r);
+        } else {
+            const Span& s0 = find(a, &Span::e0);
+            const Span& s1 = find(b, &Span::e0);
+            hit = checkEdgeEdgeImpact(&s0.c->rc.edges[a - s0.e0], &s1.c->rc.edges[b - s1.e0], thickness, r);
+        }
+        if (!hit) return false;
+        imp.type = type;
+        imp.t = r.t;
+        for (int k = 0; k < 4; k++) {
+            imp.nodes[k] = sceneId(r.nodes[k]);
+            imp.w[k] = r.w[k];
+        }
+        for (int k = 0; k < 3; k++) imp.n[k] = r.n(k);
+        return true;
+    };
+    const int nTotal = n0;
+    K.optimizeHook = [=](const std::vector<orc::Impact>& imps, float thickness, std::vector<float>& x) {
+        std::vector<Node> scene(nTotal);  // node copies in scene order
+        for (int id = 0; id < nTotal; id++) scene[id] = *nodePtr(id);
+        std::vector<::Impact> ref(imps.size());
+        for (size_t i = 0; i < imps.size(); i++) {
+            for (int k = 0; k < 4; k++) {
+                ref[i].nodes[k] = &scene[imps[i].nodes[k]];
+                ref[i].w[k] = imps[i].w[k];
+            }
+            ref[i].t = imps[i].t;
+            ref[i].n = Vector3f(imps[i].n[0], imps[i].n[1], imps[i].n[2]);
+        }
+        CollisionOptimization opt(ref, thickness, 0, 1e3f);
+        opt.solve();
+        for (int id = 0; id < nTotal; id++) {
+            nodePtr(id)->x = scene[id].x;
+            for (int c = 0; c < 3; c++) x[3 * id + c] = scene[id].x(c);
+        }
     };
 }

@@ -15,7 +15,10 @@ proximity and the step with them (`python tests/golden/make_golden.py ref_prox9`
 that file).  ref_detect.npz holds proximity detection over three cloths (a sheet folded over
 itself, two stacked sheets) through the reference's own signedVertexFaceDistance,
 signedEdgeEdgeDistance, inEdge and Proximity constructors (MathHelper.cu:38-69,
-PhysicsHelper.cu:3-18, Proximity.cu:5-21).
+PhysicsHelper.cu:3-18, Proximity.cu:5-21).  ref_collide.npz holds collision steps
+(Simulator::collisionStep) through the reference's own checkVertexFaceImpact,
+checkEdgeEdgeImpact and CollisionOptimization: two stacked sheets and a folded sheet whose upper
+layers were driven through the lower ones during the step.
 """
 import os
 import sys
@@ -128,6 +131,43 @@ def make_detect_case(seed):
     return out
 
 
+def collide_cases(seed):
+    """(name, scene, end positions per cloth): layers driven through each other in a step."""
+    stacked = scenes.stacked_sheets(8, n_layers=2, seed=seed)
+    xs = [s["x"].astype(np.float32).copy() for s in stacked.sheets]
+    xs[1][:, 2] -= np.float32(3e-3)
+    folded = scenes.folded_sheet(10, seed=seed + 1)
+    xf = folded.sheets[0]["x"].astype(np.float32).copy()
+    up = xf[:, 2] > 0.75e-3
+    xf[up, 2] -= np.float32(3.75e-3)
+    return [("stacked", stacked, xs), ("folded", folded, [xf])]
+
+
+def make_collide_case(seed):
+    out = {"dt": 0.01, "thickness": 1e-4}
+    m = None
+    for name, scene, xs in collide_cases(seed):
+        cl = [pyoracle.Cloth(s, pyoracle.Material(s["material"], which="ref")) for s in scene.sheets]
+        for c, xe in zip(cl, xs):
+            c.set_state(xe.astype(np.float64), np.zeros(xe.shape))
+        rounds, impacts = pyoracle.collision_step(cl, 0.01, 1e-4)
+        out[f"{name}_n_cloths"] = len(scene.sheets)
+        for i, (s, xe, c) in enumerate(zip(scene.sheets, xs, cl)):
+            for k in ("x", "uv", "fx", "fu", "handles"):
+                out[f"{name}_c{i}_{k}"] = s[k]
+            out[f"{name}_c{i}_xend"] = xe
+            x, v = c.state()
+            out[f"{name}_c{i}_xout"] = x.astype(np.float32)
+            out[f"{name}_c{i}_vout"] = v.astype(np.float32)
+        out[f"{name}_rounds"] = rounds
+        out[f"{name}_impacts"] = impacts
+        m = scene.sheets[0]["material"]
+    out["material_stretching"] = np.array(m["stretching"])
+    out["material_bending"] = np.array(m["bending"])
+    out["material_density"] = m["density"]
+    return out
+
+
 if __name__ == "__main__":
     only = sys.argv[1:]
     for name, seed, nq, amp in [("ref_sheet6", 11, 6, 0.03), ("ref_sheet9", 12, 9, 0.01)]:
@@ -140,6 +180,10 @@ if __name__ == "__main__":
         case = make_prox_case(21, 9)
         np.savez_compressed(os.path.join(HERE, "ref_prox9.npz"), **case)
         print("ref_prox9", {k: np.asarray(v).shape for k, v in case.items() if np.asarray(v).size > 1})
+    if not only or "ref_collide" in only:
+        case = make_collide_case(41)
+        np.savez_compressed(os.path.join(HERE, "ref_collide.npz"), **case)
+        print("ref_collide", {k: int(v) for k, v in case.items() if k.endswith(("rounds", "impacts"))})
     if not only or "ref_detect" in only:
         case = make_detect_case(31)
         np.savez_compressed(os.path.join(HERE, "ref_detect.npz"), **case)
