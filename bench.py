@@ -55,10 +55,11 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--detect", default="", choices=["", "windy", "stacked", "folded"],
-                    help="time proximity detection (and detection + step) on a contact workload instead: "
-                         "windy = the 1,024-sheet batch, a group per sheet; stacked = two 256x256 sheets "
-                         "1.5 mm apart; folded = one 256x256 sheet folded onto itself")
+    ap.add_argument("--detect", default="", choices=["", "windy", "stacked", "folded", "crossing"],
+                    help="time proximity detection, the step and the collision step on a contact workload "
+                         "instead: windy = the 1,024-sheet batch, a group per sheet; stacked = two 256x256 "
+                         "sheets 1.5 mm apart; folded = one 256x256 sheet folded onto itself; crossing = "
+                         "stacked with the upper sheet moving down at 0.5 m/s")
     ap.add_argument("--host-loop", action="store_true",
                     help="launch the solve loop from the host instead of the CUDA graph (profilers cannot "
                          "see kernels inside a graph with conditional nodes)")
@@ -493,35 +494,48 @@ def run_ours(args):
 
 
 def run_detect(args):
-    """Simulator::physicsStep's detection (Simulator.cu:571-586) on the device, timed per call
-    (the call synchronises), and detection followed by one implicit step with the detected
-    proximities (mixed precision, previous-step warm start).  One JSON line."""
+    """Simulator::simulateStep's physics and collision parts on the device: proximity detection
+    (Simulator.cu:571-586), the implicit step with the detected proximities (mixed precision,
+    previous-step warm start) and the collision step (Simulator.cu:602-684), each call timed
+    (detection and the collision step synchronise).  One JSON line."""
     import numpy as np
     sc = scenes_mod()
     from clothsimulator_b200 import native
     if args.detect == "windy":
         scene, groups = sc.windy_batch(args.sheets, args.nq, seed=eval_seed(0)), np.arange(args.sheets)
-    elif args.detect == "stacked":
+    elif args.detect in ("stacked", "crossing"):
         scene, groups = sc.stacked_sheets(256, n_layers=2, seed=1), None
+        if args.detect == "crossing":
+            scene.sheets[1]["v"] = scene.sheets[1]["v"].copy()
+            scene.sheets[1]["v"][:, 2] = -0.5
     else:
         scene, groups = sc.folded_sheet(256, seed=1), None
     ctx = native.Context(0).load(scene.sheets)
     p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol, max_iters=20000,
                            precision=native.PREC_MIXED, warm_start=native.WARM_PREVIOUS)
-    det, both, counts = [], [], []
+    det, both, col, full, counts, impacts = [], [], [], [], [], []
+    thickness = float(np.float32(0.1) * np.float32(1e-3))  # Magic::collisionThickness default
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         counts.append(ctx.detect_proximities(1e-3, groups=groups))
         t1 = time.perf_counter()
         stats, _ = ctx.step(p, allow_unconverged=True)
+        ctx.sync()
         t2 = time.perf_counter()
+        rounds, imp, _ = ctx.collision_step(scene.dt, thickness, groups=groups, allow_unresolved=True)
+        t3 = time.perf_counter()
+        impacts.append(imp)
         if i >= args.warmup:
             det.append(1e3 * (t1 - t0))
             both.append(1e3 * (t2 - t0))
+            col.append(1e3 * (t3 - t2))
+            full.append(1e3 * (t3 - t0))
     out = {"mode": "detect", "workload": scene.name, "faces": scene.n_faces, "nodes": scene.n_nodes,
            "proximities": counts[-1], "steps": args.steps, "warmup": args.warmup,
            "detect_ms_median": float(np.median(det)), "detect_and_step_ms_median": float(np.median(both)),
-           "node_steps_per_s_with_detection": scene.n_nodes / (1e-3 * float(np.median(both))),
+           "collision_step_ms_median": float(np.median(col)), "impacts_last": impacts[-1],
+           "detect_step_collide_ms_median": float(np.median(full)),
+           "node_steps_per_s_with_contact": scene.n_nodes / (1e-3 * float(np.median(full))),
            "last_step_converged": int(stats.converged), "last_step_iters": int(stats.max_iters)}
     print(json.dumps(out), flush=True)
     ctx.close()

@@ -287,7 +287,7 @@ static void checkSupported(const Json& json) {
     if (!json["motions"].isNull() && json["motions"].size() > 0)
         throw std::runtime_error("\"motions\" are not provided: this implementation covers the implicit cloth step only");
     if (!json["obstacles"].isNull() && (json["obstacles"].size() > 0 || json["obstacles"].type() == Json::String))
-        throw std::runtime_error("\"obstacles\" are not provided: collision handling is outside the implicit step");
+        throw std::runtime_error("\"obstacles\" are not provided: collisions are handled among cloths only");
     bool remeshingOff = false;
     for (const Json& d : json["disable"].items())
         if (d.type() == Json::String && d.asString() == "remeshing") remeshingOff = true;
@@ -424,12 +424,26 @@ void Simulator::physicsStep() {
         throw std::runtime_error(std::string("cs_step: ") + cs_last_error(ctx_));
 }
 
+// Simulator.cu:571-684: the positions cs_step produced are resolved against the impacts
+// between the start and the end of the step, then v = (x - x0) / dt.
+void Simulator::collisionStep() {
+    cs_collision_params cp{};
+    cp.thickness = magic_.collisionThickness;
+    cp.dt = dt_;
+    cp.sheet_group = nullptr;
+    cs_status st = cs_collision_step(ctx_, &cp, &collision_);
+    if (st == CS_ERR_NOT_CONVERGED) throw std::runtime_error("Collision step failed!");  // Simulator.cu:668-671
+    if (st != CS_OK) throw std::runtime_error(std::string("cs_collision_step: ") + cs_last_error(ctx_));
+}
+
 void Simulator::simulateStep() {
     if ((++nSteps_) % frameSteps_ == 0) nFrames_++;
     std::cout << "Frame [" << nFrames_ << "], Step [" << nSteps_ << "]:" << std::endl;
     physicsStep();
     std::cout << "Physics Step: " << stats_.ms / 1000.0 << "s (" << proximities_ << " proximities, " << stats_.max_iters
-              << " CG iterations, relative residual " << stats_.max_rel_residual << ")" << std::endl;
+              << " CG iterations, relative residual " << stats_.max_rel_residual << ")";
+    collisionStep();
+    std::cout << ", Collision Step: " << collision_.rounds << " rounds, " << collision_.impacts << " impacts" << std::endl;
     if (nSteps_ % frameSteps_ == 0) save();
 }
 

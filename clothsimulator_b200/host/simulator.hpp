@@ -108,7 +108,7 @@ struct SolverOptions {
 
 enum SimulationMode { SimulateOffline, ResumeOffline };
 
-// Simulator.cu:3-116 (constructor), 571-600 (physicsStep), 838-897 (simulateStep),
+// Simulator.cu:3-116 (constructor), 571-600 (physicsStep), 602-684 (collisionStep), 838-897 (simulateStep),
 // 950-977 (save, lastFrame, finished), 1015-1043 / 1070-1083 (offline modes).
 class Simulator {
 public:
@@ -116,6 +116,7 @@ public:
     ~Simulator();
     void start();
     void physicsStep();
+    void collisionStep();
     void simulateStep();
     bool finished() const;
     void save();
@@ -137,6 +138,7 @@ private:
     Magic magic_;
     float clothFriction_ = 0.6f;  // Simulator.cu:25
     int proximities_ = 0;
+    cs_collision_stats collision_{};
     SolverOptions solver_;
     std::vector<Cloth> cloths_;
     cs_ctx* ctx_ = nullptr;

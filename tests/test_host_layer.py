@@ -78,6 +78,11 @@ def test_interactive_modes_report_unavailable():
         assert b"unavailable" in lib.cs_sim_last_error()
 
 
+# Magic::collisionThickness default, computed as the host layer does: 0.1f x repulsionThickness
+# (Magic.cu:9-16) in FP32
+COLLISION_THICKNESS = float(np.float32(0.1) * np.float32(1e-3))
+
+
 @pytest.mark.gpu
 def test_simulate_offline_matches_c_abi(tmp_path):
     scene = scenes.hang(12, seed=2)
@@ -98,6 +103,7 @@ def test_simulate_offline_matches_c_abi(tmp_path):
         p.warm_start = native.WARM_ZERO if k == 0 else native.WARM_PREVIOUS
         ctx.detect_proximities(1e-3)  # the host layer detects before every step, as Simulator.cu:571-586
         ctx.step(p)
+        ctx.collision_step(scene.dt, COLLISION_THICKNESS)  # and the collision step after it (Simulator.cu:602-684)
     x, _ = ctx.get_state()
     assert np.array_equal(np.array(xs, np.float32), x)
     # resume continues from the last frame
@@ -134,6 +140,7 @@ def test_contact_scene_through_host_layer_matches_c_abi(tmp_path):
         p.warm_start = native.WARM_ZERO if k == 0 else native.WARM_PREVIOUS
         found.append(ctx.detect_proximities(1e-3, 1e9, 0.6))
         ctx.step(p)
+        ctx.collision_step(scene.dt, COLLISION_THICKNESS)
     assert min(found) > 0
     x, _ = ctx.get_state()
     x = x.reshape(-1, 3)
