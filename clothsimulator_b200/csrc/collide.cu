@@ -9,8 +9,8 @@
 //                            linear trajectories, solveCubic / solveQuadratic /
 //                            newtonsMethod :3-59, the distance and side at the root);
 //   cs_impact_sort_kernel    rank sort by impact time (ties by node ids);
-//   cs_impact_select_kernel  the independent impacts, earliest first, one per node
-//                            (Simulator.cu:394-420; one thread, sequential by definition);
+//   cs_select_*_kernel       the independent impacts, earliest first, one per node
+//                            (Simulator.cu:394-420), by rounds of per-node minima;
 //   cs_opt_*_kernel          the impact zone's nodes (ascending), each impact's node slots,
 //                            each node's constraint list in constraint order;
 //   cs_opt_kernel            one CTA: CollisionOptimization (CollisionOptimization.cu) solved
@@ -234,13 +234,6 @@ __device__ void impact_test(const Batch& B, const Collide& K, int type, const in
     if (slot < K.found_cap) K.found[slot] = r;
 }
 
-__device__ __forceinline__ bool before(const ImpactRec& a, const ImpactRec& b) {
-    if (a.t != b.t) return a.t < b.t;
-    for (int i = 0; i < 4; i++)
-        if (a.nodes[i] != b.nodes[i]) return a.nodes[i] < b.nodes[i];
-    return a.type < b.type;
-}
-
 }  // namespace
 
 // checkImpacts (Simulator.cu:369-381), vertex-face part: (pair, corner) per thread.
@@ -272,35 +265,92 @@ __global__ void __launch_bounds__(256) cs_impact_ee_kernel(Batch B, Contact C, C
     impact_test(B, K, 1, nodes);
 }
 
-// Rank sort of the round's impacts (their number is small).
+// Rank sort of the round's impacts by (time, node ids, type): each thread ranks one impact
+// against all others, the keys staged through shared memory in tiles.
 __global__ void __launch_bounds__(256) cs_impact_sort_kernel(Collide K, int n) {
+    struct Key {
+        float t;
+        int n0, n1, n2, n3, type;
+    };
+    __shared__ Key tile[256];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const ImpactRec a = K.found[i];
+    ImpactRec a;
+    if (i < n) a = K.found[i];
     int rank = 0;
-    for (int j = 0; j < n; j++) {
-        const ImpactRec& b = K.found[j];
-        rank += (before(b, a) || (j < i && !before(a, b))) ? 1 : 0;
+    for (int j0 = 0; j0 < n; j0 += 256) {
+        const int j = j0 + threadIdx.x;
+        if (j < n) {
+            const ImpactRec& r = K.found[j];
+            tile[threadIdx.x] = Key{r.t, r.nodes[0], r.nodes[1], r.nodes[2], r.nodes[3], r.type};
+        }
+        __syncthreads();
+        if (i < n) {
+            const int m = min(256, n - j0);
+            for (int k = 0; k < m; k++) {
+                const Key& q = tile[k];
+                bool lt;  // q before a
+                if (q.t != a.t) lt = q.t < a.t;
+                else if (q.n0 != a.nodes[0]) lt = q.n0 < a.nodes[0];
+                else if (q.n1 != a.nodes[1]) lt = q.n1 < a.nodes[1];
+                else if (q.n2 != a.nodes[2]) lt = q.n2 < a.nodes[2];
+                else if (q.n3 != a.nodes[3]) lt = q.n3 < a.nodes[3];
+                else if (q.type != a.type) lt = q.type < a.type;
+                else lt = j0 + k < i;  // equal keys: by index
+                rank += lt ? 1 : 0;
+            }
+        }
+        __syncthreads();
     }
-    K.sorted[rank] = a;
+    if (i < n) K.sorted[rank] = a;
 }
 
-// independentImpacts (Simulator.cu:394-420): earliest first, each node in one impact.
-__global__ void cs_impact_select_kernel(Collide K, int n, int base, int cap) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    int m = 0;
-    for (int i = 0; i < n; i++) {
-        const ImpactRec& r = K.sorted[i];
-        bool ok = true;
-        for (int k = 0; k < 4; k++) ok &= K.used[r.nodes[k]] == 0;
-        if (!ok) continue;
-        if (base + m < cap) K.all[base + m] = r;
-        m++;
-        for (int k = 0; k < 4; k++) K.used[r.nodes[k]] = 1;
-    }
-    for (int i = 0; i < m && base + i < cap; i++)
-        for (int k = 0; k < 4; k++) K.used[K.all[base + i].nodes[k]] = 0;
-    K.counters[1] = m;
+// independentImpacts (Simulator.cu:394-420) in parallel: the earliest-first greedy choice of
+// impacts with disjoint nodes equals, round by round, the impacts that are the earliest live
+// impact at each of their nodes; those are chosen, and the live impacts sharing a node with
+// them drop out (the reference's GPU branch uses the same scheme, Simulator.cu:422-468).
+__global__ void cs_select_init_kernel(Collide K, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    if (i < n) K.alive[i] = 1;
+    K.chosen[i] = 0;
+}
+__global__ void cs_select_reset_kernel(Collide K, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !K.alive[i]) return;
+    for (int k = 0; k < 4; k++) K.nodemin[K.sorted[i].nodes[k]] = 0x7fffffff;
+}
+__global__ void cs_select_min_kernel(Collide K, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !K.alive[i]) return;
+    for (int k = 0; k < 4; k++) atomicMin(&K.nodemin[K.sorted[i].nodes[k]], i);
+}
+__global__ void cs_select_choose_kernel(Collide K, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !K.alive[i]) return;
+    const ImpactRec& r = K.sorted[i];
+    bool first = true;
+    for (int k = 0; k < 4; k++) first &= K.nodemin[r.nodes[k]] == i;
+    if (!first) return;
+    K.chosen[i] = 1;
+    K.alive[i] = 0;
+    for (int k = 0; k < 4; k++) K.used[r.nodes[k]] = 1;
+}
+__global__ void cs_select_drop_kernel(Collide K, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !K.alive[i]) return;
+    const ImpactRec& r = K.sorted[i];
+    bool hit = false;
+    for (int k = 0; k < 4; k++) hit |= K.used[r.nodes[k]] != 0;
+    if (hit) K.alive[i] = 0;
+    else atomicAdd(&K.counters[1], 1);  // still live: another round
+}
+// The chosen impacts (exclusive offsets in chosen) appended in order; the node flags cleared.
+__global__ void cs_select_write_kernel(Collide K, int n, int base, int cap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const ImpactRec& r = K.sorted[i];
+    if (K.chosen[i + 1] > K.chosen[i] && base + K.chosen[i] < cap) K.all[base + K.chosen[i]] = r;
+    for (int k = 0; k < 4; k++) K.used[r.nodes[k]] = 0;
 }
 
 // The projection's nodes: marked, then (after an exclusive scan of mark) listed ascending.
@@ -368,18 +418,44 @@ __device__ void value_terms(const Batch& B, const Collide& K, const float* x, in
     for (int c = threadIdx.x; c < nc; c += blockDim.x) {
         const float co = mn(constraint(K, x, c) + K.lambda[c] / kMu, 0.0f);  // clampViolation(x, +1)
         K.coef[c] = co;
-        K.cterm[c] = 0.5f * kMu * (co * co);
+        // skipped terms (coefficient 0) enter as +0: the running sum is >= +0, so adding +0
+        // leaves it unchanged, bit for bit
+        K.cterm[c] = co != 0.0f ? 0.5f * kMu * (co * co) : 0.0f;
     }
 }
 
-// The sum of those terms in the CPU loop's order (thread 0).
-__device__ float value_sum(const Collide& K, int nn, int nc, float invMass) {
-    float a = 0.0f;
-    for (int i = 0; i < nn; i++) a += K.nterm[i];
-    a = 0.5f * a * invMass;
-    for (int c = 0; c < nc; c++)
-        if (K.coef[c] != 0.0f) a += K.cterm[c];
-    return a;
+constexpr int kStage = 8192;  // floats staged in shared memory per chunk of a sequential sum
+
+// acc + src[0] + src[1] + ... in that order (the CPU loop's), by thread 0, with the terms
+// staged through shared memory by the whole block; every thread calls it; the result is
+// thread 0's.
+__device__ float ordered_sum(const float* src, int n, float acc, float* stage) {
+    for (int base = 0; base < n; base += kStage) {
+        const int m = min(kStage, n - base);
+        for (int i = threadIdx.x; i < m; i += blockDim.x) stage[i] = src[base + i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int i = 0;
+            for (; i + 8 <= m; i += 8) {
+                float v[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) v[k] = stage[i + k];
+#pragma unroll
+                for (int k = 0; k < 8; k++) acc += v[k];
+            }
+            for (; i < m; i++) acc += stage[i];
+        }
+        __syncthreads();
+    }
+    return acc;
+}
+
+// Optimization::value (Optimization.cu:24-35) from those terms: the objective's sum, scaled,
+// then the constraints' terms, in the CPU loop's order (thread 0's result).
+__device__ float value_sum(const Collide& K, int nn, int nc, float invMass, float* stage) {
+    float a = ordered_sum(K.nterm, nn, 0.0f, stage);
+    a = 0.5f * a * invMass;  // meaningful in thread 0
+    return ordered_sum(K.cterm, nc, a, stage);
 }
 }  // namespace
 
@@ -388,6 +464,7 @@ __device__ float value_sum(const Collide& K, int nn, int nc, float invMass) {
 __global__ void __launch_bounds__(1024) cs_opt_kernel(Batch B, Collide K, int nn, int nc) {
     __shared__ float sf, sft, ss, sg2, sInv;
     __shared__ int sgo;
+    __shared__ float stage[kStage];
     const int tid = threadIdx.x, T = blockDim.x;
     for (int i = tid; i < nn; i += T) st(K.cur, i, ld(B.x, K.nodes[i]));
     for (int c = tid; c < nc; c += T) K.lambda[c] = 0.0f;
@@ -418,12 +495,14 @@ __global__ void __launch_bounds__(1024) cs_opt_kernel(Batch B, Collide K, int nn
             K.gterm[i] = dot0(g, g);
         }
         __syncthreads();
-        if (tid == 0) {
-            sf = value_sum(K, nn, nc, invMass);
-            float g2 = 0.0f;
-            for (int i = 0; i < nn; i++) g2 += K.gterm[i];
-            sg2 = g2;
-            ss /= 0.7f;
+        {
+            const float f = value_sum(K, nn, nc, invMass, stage);
+            const float g2 = ordered_sum(K.gterm, nn, 0.0f, stage);
+            if (tid == 0) {
+                sf = f;
+                sg2 = g2;
+                ss /= 0.7f;
+            }
         }
         __syncthreads();
         // backtracking line search
@@ -435,8 +514,8 @@ __global__ void __launch_bounds__(1024) cs_opt_kernel(Batch B, Collide K, int nn
             __syncthreads();
             value_terms(B, K, K.next, nn, nc);
             __syncthreads();
+            const float ft = value_sum(K, nn, nc, invMass, stage);
             if (tid == 0) {
-                const float ft = value_sum(K, nn, nc, invMass);
                 sft = ft;
                 sgo = (ft >= sf - 0.5f * s * sg2 && s >= kEpsS && ab(sf - ft) >= kEpsF) ? 1 : 0;
             }

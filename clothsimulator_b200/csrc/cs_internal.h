@@ -253,6 +253,9 @@ struct Collide {
     ImpactRec* sorted = nullptr;  // by time (then node ids)
     ImpactRec* all = nullptr;     // independent impacts accumulated this deformation level
     int* used = nullptr;          // per node: taken by a selected impact of this round
+    int* nodemin = nullptr;       // per node: lowest live impact index touching it (selection)
+    int* alive = nullptr;         // per found impact: still a candidate of the selection
+    int* chosen = nullptr;        // per found impact (+1): selected, then its output offset
     // the projection's nodes and constraints
     int* mark = nullptr;          // N + 1: node in an impact, then its slot (exclusive scan)
     int* nodes = nullptr;         // slot -> node, ascending

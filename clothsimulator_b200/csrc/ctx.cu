@@ -66,7 +66,12 @@ __global__ void cs_contact_vf_kernel(Batch B, Contact C, int npairs);
 __global__ void cs_impact_vf_kernel(Batch B, Contact C, Collide K, int npairs);
 __global__ void cs_impact_ee_kernel(Batch B, Contact C, Collide K, int npairs);
 __global__ void cs_impact_sort_kernel(Collide K, int n);
-__global__ void cs_impact_select_kernel(Collide K, int n, int base, int cap);
+__global__ void cs_select_init_kernel(Collide K, int n);
+__global__ void cs_select_reset_kernel(Collide K, int n);
+__global__ void cs_select_min_kernel(Collide K, int n);
+__global__ void cs_select_choose_kernel(Collide K, int n);
+__global__ void cs_select_drop_kernel(Collide K, int n);
+__global__ void cs_select_write_kernel(Collide K, int n, int base, int cap);
 __global__ void cs_opt_mark_kernel(Collide K, int nc);
 __global__ void cs_opt_nodes_kernel(Collide K, int N);
 __global__ void cs_opt_idx_kernel(Collide K, int nc);
@@ -699,8 +704,9 @@ void freeBatch(cs_ctx* c) {
     if (c->contact.pairs) cudaFree(c->contact.pairs);
     {
         Collide& K = c->coll;
-        void* ps[] = {K.found, K.counters, K.sorted, K.all, K.used, K.mark, K.nodes, K.idx, K.nptr, K.nfill,
-                      K.nlist, K.x1, K.cur, K.next, K.grad, K.lambda, K.coef, K.cterm, K.nterm, K.gterm};
+        void* ps[] = {K.found, K.counters, K.sorted, K.all, K.used, K.nodemin, K.alive, K.chosen, K.mark, K.nodes,
+                      K.idx, K.nptr, K.nfill, K.nlist, K.x1, K.cur, K.next, K.grad, K.lambda, K.coef,
+                      K.cterm, K.nterm, K.gterm};
         for (void* q : ps)
             if (q) cudaFree(q);
         c->coll = Collide();
@@ -1606,20 +1612,21 @@ cs_status collideScratch(cs_ctx* c, int nFound, int nAll) {
     CollideCaps& P = c->collCaps;
     cs_status st;
     if (!K.mark) {
-        size_t cap = 0;
+        // per node (the projection's nodes are a subset of the batch's)
         const size_t N = (size_t)B.N;
-        if ((st = grow(c, K.mark, cap = 0, N + 1)) != CS_OK) return st;
-        if ((st = grow(c, K.used, cap = 0, N)) != CS_OK) return st;
-        if ((st = grow(c, K.nodes, cap = 0, N)) != CS_OK) return st;
-        if ((st = grow(c, K.nptr, cap = 0, N + 1)) != CS_OK) return st;
-        if ((st = grow(c, K.nfill, cap = 0, N + 1)) != CS_OK) return st;
-        if ((st = grow(c, K.x1, cap = 0, 3 * N)) != CS_OK) return st;
-        if ((st = grow(c, K.cur, cap = 0, 3 * N)) != CS_OK) return st;
-        if ((st = grow(c, K.next, cap = 0, 3 * N)) != CS_OK) return st;
-        if ((st = grow(c, K.grad, cap = 0, 3 * N)) != CS_OK) return st;
-        if ((st = grow(c, K.nterm, cap = 0, N)) != CS_OK) return st;
-        if ((st = grow(c, K.gterm, cap = 0, N)) != CS_OK) return st;
-        if ((st = grow(c, K.counters, cap = 0, 2)) != CS_OK) return st;
+        size_t cap = 0;
+        auto once = [&](auto*& q, size_t n) {
+            cap = 0;
+            return grow(c, q, cap, n);
+        };
+        if ((st = once(K.mark, N + 1)) != CS_OK || (st = once(K.used, N)) != CS_OK ||
+            (st = once(K.nodes, N)) != CS_OK || (st = once(K.nptr, N + 1)) != CS_OK ||
+            (st = once(K.nfill, N + 1)) != CS_OK || (st = once(K.x1, 3 * N)) != CS_OK ||
+            (st = once(K.cur, 3 * N)) != CS_OK || (st = once(K.next, 3 * N)) != CS_OK ||
+            (st = once(K.grad, 3 * N)) != CS_OK || (st = once(K.nterm, N)) != CS_OK ||
+            (st = once(K.gterm, N)) != CS_OK || (st = once(K.counters, 2)) != CS_OK ||
+            (st = once(K.nodemin, N)) != CS_OK)
+            return st;
         CS_CUDA(cudaMemset(K.used, 0, N * sizeof(int)));
     }
     if ((size_t)nFound > P.found) {
@@ -1628,6 +1635,12 @@ cs_status collideScratch(cs_ctx* c, int nFound, int nAll) {
         if (K.sorted) cudaFree(K.sorted);
         K.sorted = nullptr;
         if ((st = grow(c, K.sorted, cap, P.found)) != CS_OK) return st;
+        for (int** q : {&K.alive, &K.chosen}) {
+            if (*q) cudaFree(*q);
+            *q = nullptr;
+            cap = 0;
+            if ((st = grow(c, *q, cap, P.found + 1)) != CS_OK) return st;
+        }
         K.found_cap = (int)std::min<size_t>(P.found, INT32_MAX);
     }
     if ((size_t)nAll > P.all) {
@@ -1642,17 +1655,17 @@ cs_status collideScratch(cs_ctx* c, int nFound, int nAll) {
             CS_CUDA(cudaStreamSynchronize(c->stream));
             cudaFree(old);
         }
-        size_t cap;
-        for (int** q : {&K.idx, &K.nlist}) {
-            if (*q) cudaFree(*q);
-            *q = nullptr;
-            if ((st = grow(c, *q, cap = 0, 4 * P.all)) != CS_OK) return st;
-        }
-        for (float** q : {&K.lambda, &K.coef, &K.cterm}) {
-            if (*q) cudaFree(*q);
-            *q = nullptr;
-            if ((st = grow(c, *q, cap = 0, P.all)) != CS_OK) return st;
-        }
+        // per constraint (reallocated: their contents are rebuilt each round)
+        auto fresh = [&](auto*& q, size_t n) {
+            if (q) cudaFree(q);
+            q = nullptr;
+            size_t cap = 0;
+            return grow(c, q, cap, n);
+        };
+        if ((st = fresh(K.idx, 4 * P.all)) != CS_OK || (st = fresh(K.nlist, 4 * P.all)) != CS_OK ||
+            (st = fresh(K.lambda, P.all)) != CS_OK || (st = fresh(K.coef, P.all)) != CS_OK ||
+            (st = fresh(K.cterm, P.all)) != CS_OK)
+            return st;
     }
     return CS_OK;
 }
@@ -1762,12 +1775,25 @@ cs_status cs_collision_step(cs_ctx* c, const cs_collision_params* p, cs_collisio
             if (nFound > K.found_cap) return fail(c, CS_ERR_STATE, "impact buffer overflow");
             if ((st = collideScratch(c, nFound, nAll + nFound)) != CS_OK) return st;
             cs_impact_sort_kernel<<<nblk(nFound, 256), 256, 0, c->stream>>>(K, nFound);
-            cs_impact_select_kernel<<<1, 1, 0, c->stream>>>(K, nFound, nAll, (int)c->collCaps.all);
-            int sel[2];
-            CS_CUDA(cudaMemcpyAsync(sel, K.counters, sizeof(sel), cudaMemcpyDeviceToHost, c->stream));
-            CS_CUDA(cudaStreamSynchronize(c->stream));
-            nAll += sel[1];
-            total += sel[1];
+            // independent impacts: rounds of per-node minima until no impact is live
+            const int g = nblk(nFound, 256);
+            cs_select_init_kernel<<<nblk(nFound + 1, 256), 256, 0, c->stream>>>(K, nFound);
+            for (int pass = 0; pass < nFound; pass++) {
+                int live = 0;
+                cs_select_reset_kernel<<<g, 256, 0, c->stream>>>(K, nFound);
+                cs_select_min_kernel<<<g, 256, 0, c->stream>>>(K, nFound);
+                cs_select_choose_kernel<<<g, 256, 0, c->stream>>>(K, nFound);
+                CS_CUDA(cudaMemsetAsync(K.counters + 1, 0, sizeof(int), c->stream));
+                cs_select_drop_kernel<<<g, 256, 0, c->stream>>>(K, nFound);
+                CS_CUDA(cudaMemcpyAsync(&live, K.counters + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+                CS_CUDA(cudaStreamSynchronize(c->stream));
+                if (live == 0) break;
+            }
+            int sel = 0;
+            if ((st = scanInts(c, K.chosen, nFound, &sel)) != CS_OK) return st;
+            cs_select_write_kernel<<<g, 256, 0, c->stream>>>(K, nFound, nAll, (int)c->collCaps.all);
+            nAll += sel;
+            total += sel;
             // the projection's nodes and constraints
             CS_CUDA(cudaMemsetAsync(K.mark, 0, ((size_t)B.N + 1) * sizeof(int), c->stream));
             cs_opt_mark_kernel<<<nblk(4LL * nAll, 256), 256, 0, c->stream>>>(K, nAll);
