@@ -102,8 +102,31 @@ class RankGroup:
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
+    def sum_host(self, a):
+        """Sum of a float64 numpy array over the ranks (gloo)."""
+        if not self.dist:
+            return a
+        import torch
+
+        t = torch.from_numpy(np.array(a, np.float64))
+        self.dist.all_reduce(t)
+        return t.numpy()
+
+    def device_allreduce(self):
+        """An in-place sum of CUDA tensors over the ranks: NCCL over NVLink (a group of its own
+        beside the gloo group of the host scalars)."""
+        if not self.dist:
+            return None
+        if getattr(self, "_nccl", None) is None:
+            self._nccl = self.dist.new_group(backend="nccl")
+        grp = self._nccl
+        return lambda t: self.dist.all_reduce(t, group=grp)
+
     def close(self):
         if self.dist:
+            if getattr(self, "_nccl", None) is not None:
+                self.dist.destroy_process_group(self._nccl)
+                self._nccl = None
             self.dist.destroy_process_group()
             self.dist = None
 
@@ -290,7 +313,7 @@ def run_ours(args):
             tscene = scenes_mod().windy_batch(args.train_sheets, args.nq, seed=train_seed(rank))
             tctx = native.Context(local)
             tctx.load(tscene.sheets)
-            tctx.mlp_init(args.train_steps, 1 + rank)
+            tctx.mlp_init(args.train_steps, 1)  # the same initial weights on every rank
             tp = native.step_params(tscene.dt, tscene.gravity, tscene.handle_stiffness, tol=1e-7, max_iters=8000)
             for _ in range(2):
                 tctx.step(tp, allow_unconverged=True)
@@ -300,13 +323,27 @@ def run_ours(args):
                 tctx.mlp_record(t, 0)
                 tctx.step(tp, allow_unconverged=True)
                 tctx.mlp_record(t, 1)
-            tctx.mlp_fit_normalization(args.train_steps)
-            losses = tctx.mlp_train(args.train_steps, args.epochs, lr=1e-3, sheets_per_batch=32, seed=3)
+            if world == 1:
+                tctx.mlp_fit_normalization(args.train_steps)
+                losses = tctx.mlp_train(args.train_steps, args.epochs, lr=1e-3, sheets_per_batch=32, seed=3)
+            else:
+                # data parallel: every rank trains on its own trajectories, gradients summed over
+                # NCCL and averaged, normalisation from the moments summed over the ranks
+                from clothsimulator_b200 import training
+
+                losses = training.train_data_parallel(tctx, args.train_steps, args.train_sheets, args.epochs, 1e-3,
+                                                      32, 3, allreduce_sum=group.device_allreduce(), world=world,
+                                                      sum_host=group.sum_host)
             weights = tctx.mlp_get_weights()
             tctx.close()
             train_info = {"sheets": args.train_sheets, "steps": args.train_steps, "epochs": args.epochs,
                           "seeds": "disjoint from the evaluated workload",
                           "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
+            if world > 1:
+                digest = float(np.float64(weights).sum())
+                train_info["data_parallel"] = {
+                    "ranks": world, "gradients": "NCCL all-reduce, averaged",
+                    "weights_identical": group.max(digest) == -group.max(-digest)}
         train_info["seconds"] = time.perf_counter() - t0
         ctx.mlp_init(0, 0)
         ctx.mlp_set_weights(weights)

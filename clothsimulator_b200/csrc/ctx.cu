@@ -2321,10 +2321,13 @@ cs_status cs_mlp_record(cs_ctx* c, int slot, int what) {
     return CS_OK;
 }
 
-cs_status cs_mlp_fit_normalization(cs_ctx* c, int n_slots) {
-    if (!c) return CS_ERR_INVALID_ARG;
+// Sums of the 16 features, the 3 targets and their squares over the recorded slots
+// (38 doubles: 16 + 3 sums, then 16 + 3 sums of squares) and the node count.
+cs_status cs_mlp_moments(cs_ctx* c, int n_slots, double* sums, long long* count) {
+    if (!c || !sums) return CS_ERR_INVALID_ARG;
     if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
     if (n_slots <= 0 || n_slots > c->mlp.slots) return fail(c, CS_ERR_INVALID_ARG, "bad slot count");
+    CS_CUDA(cudaSetDevice(c->device));
     const int blocks = 296;
     double* part = nullptr;
     CS_CUDA(cudaMalloc(&part, (size_t)blocks * 38 * sizeof(double)));
@@ -2335,9 +2338,17 @@ cs_status cs_mlp_fit_normalization(cs_ctx* c, int n_slots) {
     if (e == cudaSuccess) e = cudaMemcpy(h.data(), part, h.size() * sizeof(double), cudaMemcpyDeviceToHost);
     cudaFree(part);
     if (e != cudaSuccess) return fail(c, CS_ERR_CUDA, "moments: %s", cudaGetErrorString(e));
-    double sum[38] = {0};
+    for (int k = 0; k < 38; k++) sums[k] = 0.0;
     for (int b = 0; b < blocks; b++)
-        for (int k = 0; k < 38; k++) sum[k] += h[38 * b + k];
+        for (int k = 0; k < 38; k++) sums[k] += h[38 * b + k];
+    if (count) *count = n;
+    return CS_OK;
+}
+
+// The input and output normalisation from moment sums (one rank's, or summed over ranks).
+cs_status cs_mlp_set_moments(cs_ctx* c, const double* sum, long long n) {
+    if (!c || !sum || n <= 0) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
     std::vector<float> stats(MLP_NSTAT);
     for (int k = 0; k < 16; k++) {
         double mu = sum[k] / n, var = sum[19 + k] / n - mu * mu;
@@ -2351,6 +2362,45 @@ cs_status cs_mlp_fit_normalization(cs_ctx* c, int n_slots) {
     }
     CS_CUDA(cudaMemcpy(c->mlp.stats, stats.data(), MLP_NSTAT * sizeof(float), cudaMemcpyHostToDevice));
     return CS_OK;
+}
+
+cs_status cs_mlp_fit_normalization(cs_ctx* c, int n_slots) {
+    double sums[38];
+    long long n = 0;
+    cs_status st = cs_mlp_moments(c, n_slots, sums, &n);
+    if (st != CS_OK) return st;
+    return cs_mlp_set_moments(c, sums, n);
+}
+
+// One minibatch's gradient into a device buffer (for an all-reduce across ranks).
+cs_status cs_mlp_gradient_device(cs_ctx* c, int slot, int s0, int s1, float* grad, float* loss) {
+    if (!c || !grad) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    if (slot < 0 || slot >= c->mlp.slots || s0 < 0 || s1 <= s0 || s1 > c->B.S)
+        return fail(c, CS_ERR_INVALID_ARG, "bad slot or sheet range");
+    CS_CUDA(cudaSetDevice(c->device));
+    float* acc = c->mlpScratch;
+    CS_CUDA(cudaMemsetAsync(acc, 0, sizeof(float), c->stream));
+    mlpForwardBackward(c, slot, s0, s1);
+    cs_mlp_adam_kernel<<<nblk(MLP_P, 256), 256, 0, c->stream>>>(c->mlp, c->mlpGridTrain, 0.f, 0.f, 0.f, 0.f, 1, grad);
+    cs_mlp_loss_acc_kernel<<<1, 32, 0, c->stream>>>(c->mlp, c->mlpGridTrain, acc);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    if (loss) CS_CUDA(cudaMemcpy(loss, acc, sizeof(float), cudaMemcpyDeviceToHost));
+    return mlpCheckErr(c);
+}
+
+// The Adam step cs_mlp_train takes after each minibatch, with a given (device) gradient.
+cs_status cs_mlp_apply_gradient(cs_ctx* c, const float* grad, float lr) {
+    if (!c || !grad || !(lr > 0)) return CS_ERR_INVALID_ARG;
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    CS_CUDA(cudaSetDevice(c->device));
+    c->adamStep++;
+    cs_mlp_adam_ext_kernel<<<nblk(MLP_P, 256), 256, 0, c->stream>>>(c->mlp, grad, lr, 0.9f, 0.999f, 1e-8f,
+                                                                     (int)c->adamStep);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    return mlpCheckErr(c);
 }
 
 cs_status cs_mlp_gradient(cs_ctx* c, int slot, int s0, int s1, float* grad, float* loss) {

@@ -695,6 +695,24 @@ __global__ void cs_mlp_adam_kernel(MlpDev M, int ncta, float lr, float b1, float
     M.wb[p] = __float2bfloat16_rn(w);
 }
 
+// The same Adam update from a gradient held in a device buffer (summed or averaged over
+// ranks by the caller).
+__global__ void cs_mlp_adam_ext_kernel(MlpDev M, const float* __restrict__ grad, float lr, float b1, float b2,
+                                       float eps, int step) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= MLP_P) return;
+    const float g = grad[p];
+    const float m = b1 * M.m[p] + (1.f - b1) * g;
+    const float v = b2 * M.v[p] + (1.f - b2) * g * g;
+    M.m[p] = m;
+    M.v[p] = v;
+    const float mh = m / (1.f - powf(b1, (float)step));
+    const float vh = v / (1.f - powf(b2, (float)step));
+    const float w = M.w[p] - lr * mh / (sqrtf(vh) + eps);
+    M.w[p] = w;
+    M.wb[p] = __float2bfloat16_rn(w);
+}
+
 // Training pair bookkeeping: the dataset slot receives the raw features of the current
 // assembled system (with the previous dv held in B.warm) and, after the solve, the target
 // dv - previous dv.

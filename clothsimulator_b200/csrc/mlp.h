@@ -42,6 +42,7 @@ __global__ void cs_mlp_bwd23_kernel(Batch B, MlpDev M, int n0, int n1, const flo
 __global__ void cs_mlp_bwd1_kernel(Batch B, MlpDev M, const float* fsrc, int n0, int n1);
 __global__ void cs_mlp_adam_kernel(MlpDev M, int ncta, float lr, float b1, float b2, float eps, int step,
                                    float* grad_out);
+__global__ void cs_mlp_adam_ext_kernel(MlpDev M, const float* grad, float lr, float b1, float b2, float eps, int step);
 __global__ void cs_mlp_target_kernel(Batch B, const float* feat, float* target);
 __global__ void cs_mlp_moments_kernel(const float* feat, const float* target, long long n, double* out);
 __global__ void cs_mlp_loss_acc_kernel(MlpDev M, int ncta, float* acc);

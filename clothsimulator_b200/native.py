@@ -38,7 +38,8 @@ EXPORTED = [
     "cs_solve_block_csr_noalloc", "cs_tc_gemm_check", "cs_mlp_init", "cs_mlp_record", "cs_mlp_fit_normalization",
     "cs_mlp_train", "cs_mlp_gradient", "cs_mlp_predict", "cs_mlp_get_record", "cs_mlp_get_weights",
     "cs_mlp_set_weights", "cs_get_solver_info", "cs_set_proximities", "cs_detect_proximities",
-    "cs_get_proximities", "cs_collision_step",
+    "cs_get_proximities", "cs_collision_step", "cs_mlp_moments", "cs_mlp_set_moments", "cs_mlp_gradient_device",
+    "cs_mlp_apply_gradient",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -177,6 +178,10 @@ def load_library() -> ctypes.CDLL:
         "cs_mlp_fit_normalization": [vp, ctypes.c_int],
         "cs_mlp_train": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_ulonglong, _fp],
         "cs_mlp_gradient": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _fp, _fp],
+        "cs_mlp_moments": [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_longlong)],
+        "cs_mlp_set_moments": [vp, _dp, ctypes.c_longlong],
+        "cs_mlp_gradient_device": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, _fp],
+        "cs_mlp_apply_gradient": [vp, vp, ctypes.c_float],
         "cs_mlp_predict": [vp, _fp],
         "cs_mlp_get_record": [vp, ctypes.c_int, _fp, _fp],
         "cs_mlp_get_weights": [vp, _fp, ctypes.c_int],
@@ -252,6 +257,7 @@ class Context:
         if st != CS_OK:
             raise ClothStepError(st, "cs_create failed (no usable sm_100 CUDA device)")
         self.h = h
+        self.device = device
         self._keep = []
         self.n = 0
 
@@ -478,6 +484,35 @@ class Context:
         loss = ctypes.c_float(0)
         self.check(self.lib.cs_mlp_gradient(self.h, slot, s0, s1, g.ctypes.data_as(_fp), ctypes.byref(loss)))
         return g, loss.value
+
+    @property
+    def torch_device(self):
+        import torch
+
+        return torch.device("cuda", self.device)
+
+    def mlp_moments(self, n_slots: int):
+        """Normalisation moment sums (38) and node count of the recorded slots."""
+        sums = np.zeros(38, np.float64)
+        n = ctypes.c_longlong(0)
+        self.check(self.lib.cs_mlp_moments(self.h, n_slots, sums.ctypes.data_as(_dp), ctypes.byref(n)))
+        return sums, n.value
+
+    def mlp_set_moments(self, sums, count: int):
+        a = np.ascontiguousarray(sums, np.float64)
+        self.check(self.lib.cs_mlp_set_moments(self.h, a.ctypes.data_as(_dp), int(count)))
+
+    def mlp_gradient_device(self, slot: int, s0: int, s1: int, grad) -> float:
+        """One minibatch's gradient into `grad`, a CUDA tensor of MLP_TRAINED floats on this
+        context's device; returns the minibatch loss."""
+        loss = ctypes.c_float(0.0)
+        self.check(self.lib.cs_mlp_gradient_device(self.h, slot, s0, s1, ctypes.c_void_p(grad.data_ptr()),
+                                                   ctypes.byref(loss)))
+        return loss.value
+
+    def mlp_apply_gradient(self, grad, lr: float):
+        """The Adam step of cs_mlp_train with the gradient in `grad` (CUDA tensor)."""
+        self.check(self.lib.cs_mlp_apply_gradient(self.h, ctypes.c_void_p(grad.data_ptr()), lr))
 
     def mlp_predict(self):
         p = np.zeros((self.n, 3), np.float32)

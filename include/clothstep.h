@@ -284,6 +284,17 @@ cs_status cs_mlp_train(cs_ctx* ctx, int n_slots, int epochs, float lr, int sheet
                        unsigned long long seed, float* epoch_loss);
 /* Gradient (CS_MLP_PARAMS - 38 floats) and loss of one minibatch, without updating. */
 cs_status cs_mlp_gradient(cs_ctx* ctx, int slot, int sheet_begin, int sheet_end, float* grad, float* loss);
+/* Data-parallel training across ranks (one context per GPU, each on its own trajectories):
+ * cs_mlp_moments gives the normalisation's sums (38 doubles: 16 feature and 3 target sums, then
+ * their 19 sums of squares) and node count for an all-reduce, cs_mlp_set_moments sets the
+ * normalisation from the summed moments (cs_mlp_fit_normalization = the two on one rank);
+ * cs_mlp_gradient_device writes one minibatch's gradient into a DEVICE buffer of
+ * CS_MLP_PARAMS - 38 floats (to all-reduce in place, e.g. with NCCL) and cs_mlp_apply_gradient
+ * takes the Adam step cs_mlp_train takes after each minibatch, with that buffer's gradient. */
+cs_status cs_mlp_moments(cs_ctx* ctx, int n_slots, double* sums, long long* count);
+cs_status cs_mlp_set_moments(cs_ctx* ctx, const double* sums, long long count);
+cs_status cs_mlp_gradient_device(cs_ctx* ctx, int slot, int sheet_begin, int sheet_end, float* grad, float* loss);
+cs_status cs_mlp_apply_gradient(cs_ctx* ctx, const float* grad, float lr);
 /* The prediction for the system assembled by the last cs_assemble (3 floats per node). */
 cs_status cs_mlp_predict(cs_ctx* ctx, float* pred);
 /* A recorded training pair: 16 raw features and 3 target values per node (host arrays). */

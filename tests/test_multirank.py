@@ -98,3 +98,92 @@ def test_single_rank_group_is_local():
         for k, v in saved.items():
             if v is not None:
                 os.environ[k] = v
+
+
+class FakeTrainingContext:
+    """Stands in for native.Context in train_data_parallel on CPU: parameters w, gradient of
+    0.5 |w - target|^2 with a target per (rank, slot, minibatch), plain descent as the step."""
+
+    def __init__(self, rank, n):
+        import torch
+
+        self.rank, self.w = rank, np.zeros(n, np.float32)
+        self.torch_device = torch.device("cpu")
+        self.moments = None
+
+    def target(self, rank, slot, s0):
+        return np.full(self.w.shape, 0.1 * (1 + rank) + 0.01 * slot + 0.001 * s0, np.float32)
+
+    def mlp_moments(self, n_slots):
+        return np.arange(38, dtype=np.float64) * (1 + self.rank), 10 * (1 + self.rank)
+
+    def mlp_set_moments(self, sums, count):
+        self.moments = (np.array(sums), count)
+
+    def mlp_gradient_device(self, slot, s0, s1, grad):
+        g = self.w - self.target(self.rank, slot, s0)
+        grad.numpy()[:] = g
+        return float(0.5 * (g * g).sum())
+
+    def mlp_apply_gradient(self, grad, lr):
+        self.w = (self.w - np.float32(lr) * grad.numpy()).astype(np.float32)
+
+
+def _dp_rank(rank, world, port, out):
+    os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from clothsimulator_b200 import native, training
+
+    dist.init_process_group("gloo", init_method="env://", timeout=datetime.timedelta(seconds=60))
+    ctx = FakeTrainingContext(rank, native.MLP_TRAINED)
+
+    def sum_host(a):
+        t = torch.from_numpy(np.array(a, np.float64))
+        dist.all_reduce(t)
+        return t.numpy()
+
+    training.train_data_parallel(ctx, 2, 5, 2, 0.5, 2, 9, allreduce_sum=dist.all_reduce, world=world,
+                                 sum_host=sum_host)
+    out[rank] = {"w": ctx.w.copy(), "moments": ctx.moments}
+    dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+def test_data_parallel_training_two_gloo_ranks():
+    """train_data_parallel over two gloo ranks: identical parameters on both, equal to serial
+    descent on the averaged gradients, and the normalisation from the summed moments."""
+    sys.path.insert(0, ROOT)
+    from clothsimulator_b200 import native, training
+
+    world = 2
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        ctx = mp.get_context("spawn")
+        procs = [ctx.Process(target=_dp_rank, args=(r, world, port, out)) for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(150)
+        codes = [p.exitcode for p in procs]
+        for p in procs:
+            if p.is_alive():
+                p.kill()
+        assert codes == [0, 0], codes
+        res = dict(out)
+    assert np.array_equal(res[0]["w"], res[1]["w"])
+    ref = [FakeTrainingContext(r, native.MLP_TRAINED) for r in range(world)]
+    w = np.zeros(native.MLP_TRAINED, np.float32)
+    for batches in training.minibatch_schedule(2, 5, 2, 2, 9):
+        for slot, s0, s1 in batches:
+            g = sum((w - c.target(c.rank, slot, s0)) for c in ref) * np.float32(1.0 / world)
+            w = (w - np.float32(0.5) * g.astype(np.float32)).astype(np.float32)
+    assert np.allclose(res[0]["w"], w, rtol=1e-6, atol=1e-7)
+    sums, count = res[0]["moments"]
+    assert count == 30 and np.allclose(sums, np.arange(38) * 3)
