@@ -974,73 +974,103 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     std::vector<int> topoNbrPtr0(topos.size()), topoNbr0(topos.size());
     std::vector<int> topoPanel0(topos.size()), topoSlice0(topos.size());
     std::vector<int> htcsr_ptr, htcsr_col, htcsr_slot, topoCsrPtr0(topos.size());
-    // Cluster-resident solve plan (resident.cu).  CS_RESIDENT_CL sets the CTAs per cluster
-    // (2, 4, 8 or 16; 0 solves every sheet in the batched loop); default 8, the portable size.
-    int resCL = 8;
-    if (const char* ev = std::getenv("CS_RESIDENT_CL")) resCL = std::atoi(ev);
-    if (resCL != 0 && resCL != 2 && resCL != 4 && resCL != 8 && resCL != 16)
-        return fail(c, CS_ERR_INVALID_ARG, "CS_RESIDENT_CL must be 0, 2, 4, 8 or 16");
+    // Cluster-resident solve plan (resident.cu).  Clusters must fit a GPC, so the number of
+    // SMs a cluster size keeps busy varies: 8- and 9-CTA clusters are planned and the one that
+    // makes the most sheets resident, then keeps the most SMs busy, is taken (on the B200, 15
+    // clusters of 8 occupy 120 SMs, 15 clusters of 9 occupy 135).  CS_RESIDENT_CL (2..16)
+    // forces a size; 0 solves every sheet in the batched loop.
+    std::vector<int> candidates = {8, 9};
+    if (const char* ev = std::getenv("CS_RESIDENT_CL")) {
+        const int v = std::atoi(ev);
+        if (v != 0 && (v < 2 || v > CS_RES_MAX_CL))
+            return fail(c, CS_ERR_INVALID_ARG, "CS_RESIDENT_CL must be 0 or 2..16");
+        candidates = {v};
+    }
+    struct ResChoice {
+        int cl = 0, w = 0, panels = 0, halo = 0, cap = 0, clusters = 0;
+        long long sheets = 0;
+        size_t smem = 0;
+        std::vector<ResidentPlan> plans;
+        std::vector<char> resident;
+    };
+    cudaDeviceProp devProp;
+    CS_CUDA(cudaGetDeviceProperties(&devProp, c->device));
+    cudaFuncAttributes resAttr;
+    CS_CUDA(cudaFuncGetAttributes(&resAttr, cs_resident_pcg_kernel));
+    auto planFor = [&](int cl) {
+        ResChoice R;
+        R.cl = cl;
+        R.plans.resize(topos.size());
+        R.resident.assign(topos.size(), 0);
+        for (size_t t = 0; t < topos.size() && cl > 0; t++) {
+            R.plans[t] = residentPlan(*topos[t], cl);
+            const ResidentPlan& P = R.plans[t];
+            // p indices (own slots + halo) are 12-bit in the kernel's packed column codes
+            if (P.w > CS_RES_MAX_WARPS || P.max_width > CS_RES_MAX_WIDTH || P.max_halo + CS_RES_MAX_WARPS * CS_SLICE >= 4096)
+                continue;
+            R.resident[t] = 1;
+            R.w = std::max(R.w, P.w);
+            R.panels = std::max(R.panels, P.max_panels);
+            R.halo = std::max(R.halo, P.max_halo);
+        }
+        if (R.w == 0) return R;
+        const size_t pbytes = ((size_t)R.w * CS_SLICE + R.halo) * sizeof(float4);
+        const size_t budget = devProp.sharedMemPerBlockOptin > resAttr.sharedSizeBytes + pbytes
+                                  ? devProp.sharedMemPerBlockOptin - resAttr.sharedSizeBytes - pbytes : 0;
+        R.cap = (int)std::min<size_t>((size_t)R.panels, budget / (CS_PANEL_FLOATS * sizeof(float)));
+        R.smem = (size_t)R.cap * CS_PANEL_FLOATS * sizeof(float) + pbytes;
+        if (budget > 0) {
+            cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R.smem);
+            if (cl > 8) cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = cl;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(cl);
+            cfg.blockDim = dim3(R.w * CS_SLICE);
+            cfg.dynamicSmemBytes = R.smem;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            if (cudaOccupancyMaxActiveClusters(&R.clusters, cs_resident_pcg_kernel, &cfg) != cudaSuccess) R.clusters = 0;
+            cudaGetLastError();
+        }
+        if (R.clusters <= 0) {
+            R.clusters = 0;
+            std::fill(R.resident.begin(), R.resident.end(), 0);
+        }
+        for (int sh = 0; sh < n_sheets; sh++) R.sheets += R.resident[sheetTopoId[sh]];
+        return R;
+    };
+    ResChoice res;
+    for (int cl : candidates) {
+        ResChoice R = planFor(cl);
+        const bool better = res.cl == 0 || R.sheets > res.sheets ||
+                            (R.sheets == res.sheets && (long long)R.clusters * R.cl > (long long)res.clusters * res.cl);
+        if (better) res = std::move(R);
+    }
     std::vector<int> hrsplit(topos.size() * (CS_RES_MAX_CL + 1), 0), hrcode;
     std::vector<int> hrsendptr(topos.size() * (CS_RES_MAX_CL + 1), 0);
     std::vector<int> hrhalo(topos.size() * (CS_RES_MAX_CL + 1), 0);
     std::vector<uint32_t> hrsend;
-    std::vector<char> topoResident(topos.size(), 0);
-    std::vector<ResidentPlan> plans(topos.size());
-    int resW = 0, resPanels = 0, resHalo = 0;
-    for (size_t t = 0; t < topos.size() && resCL > 0; t++) {
-        plans[t] = residentPlan(*topos[t], resCL);
-        const ResidentPlan& P = plans[t];
-        // p indices (own slots + halo) are 12-bit in the kernel's packed column codes
-        if (P.w > CS_RES_MAX_WARPS || P.max_width > CS_RES_MAX_WIDTH || P.max_halo + CS_RES_MAX_WARPS * CS_SLICE >= 4096)
-            continue;
-        topoResident[t] = 1;
-        resW = std::max(resW, P.w);
-        resPanels = std::max(resPanels, P.max_panels);
-        resHalo = std::max(resHalo, P.max_halo);
-        std::copy(P.split.begin(), P.split.end(), hrsplit.begin() + t * (CS_RES_MAX_CL + 1));
-        std::copy(P.halo_count.begin(), P.halo_count.end(), hrhalo.begin() + t * (CS_RES_MAX_CL + 1));
-    }
+    std::vector<char>& topoResident = res.resident;
+    std::vector<ResidentPlan>& plans = res.plans;
+    const int resW = res.w, resCap = res.cap;
+    for (size_t t = 0; t < topos.size(); t++)
+        if (topoResident[t]) {
+            std::copy(plans[t].split.begin(), plans[t].split.end(), hrsplit.begin() + t * (CS_RES_MAX_CL + 1));
+            std::copy(plans[t].halo_count.begin(), plans[t].halo_count.end(), hrhalo.begin() + t * (CS_RES_MAX_CL + 1));
+        }
     c->resCL = c->resThreads = c->resClusters = 0;
     c->resSmem = 0;
-    int resCap = 0;
-    if (resW > 0) {
-        cudaDeviceProp prop;
-        CS_CUDA(cudaGetDeviceProperties(&prop, c->device));
-        cudaFuncAttributes fa;
-        CS_CUDA(cudaFuncGetAttributes(&fa, cs_resident_pcg_kernel));
-        const size_t pbytes = ((size_t)resW * CS_SLICE + resHalo) * sizeof(float4);
-        const size_t budget = prop.sharedMemPerBlockOptin > fa.sharedSizeBytes + pbytes
-                                  ? prop.sharedMemPerBlockOptin - fa.sharedSizeBytes - pbytes : 0;
-        resCap = (int)std::min<size_t>((size_t)resPanels, budget / (CS_PANEL_FLOATS * sizeof(float)));
-        const size_t smem = (size_t)resCap * CS_PANEL_FLOATS * sizeof(float) + pbytes;
-        int nclusters = 0;
-        if (budget > 0) {
-            CS_CUDA(cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            if (resCL > 8) CS_CUDA(cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-            cudaLaunchConfig_t cfg = {};
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeClusterDimension;
-            at[0].val.clusterDim.x = resCL;
-            at[0].val.clusterDim.y = 1;
-            at[0].val.clusterDim.z = 1;
-            cfg.gridDim = dim3(resCL);
-            cfg.blockDim = dim3(resW * CS_SLICE);
-            cfg.dynamicSmemBytes = smem;
-            cfg.attrs = at;
-            cfg.numAttrs = 1;
-            if (cudaOccupancyMaxActiveClusters(&nclusters, cs_resident_pcg_kernel, &cfg) != cudaSuccess) {
-                cudaGetLastError();
-                nclusters = 0;
-            }
-        }
-        if (nclusters > 0) {
-            c->resCL = resCL;
-            c->resThreads = resW * CS_SLICE;
-            c->resClusters = nclusters;
-            c->resSmem = smem;
-        } else {
-            std::fill(topoResident.begin(), topoResident.end(), 0);
-        }
+    if (res.clusters > 0) {
+        // the launch attributes of the chosen plan (the evaluation set others)
+        CS_CUDA(cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)res.smem));
+        c->resCL = res.cl;
+        c->resThreads = resW * CS_SLICE;
+        c->resClusters = res.clusters;
+        c->resSmem = res.smem;
     }
     {
         int tp = 0, ts = 0;

@@ -58,7 +58,8 @@ def test_plan_covers_sheets_that_fit(ctx_factory):
     ctx = ctx_factory(scene.sheets)
     info = ctx.solver_info()
     assert info["resident_sheets"] == 6
-    assert info["ctas_per_cluster"] == 8 and info["clusters"] >= 1
+    # 8 or 9 CTAs per cluster: whichever keeps more SMs busy for this plan
+    assert info["ctas_per_cluster"] in (8, 9) and info["clusters"] >= 1
     assert info["threads_per_cta"] % 32 == 0 and info["threads_per_cta"] <= 768
     # a 128x128 sheet needs more than 24 slices per CTA: it stays in the batched loop
     big = scenes.windy_batch(1, 128, seed=12).sheets + scenes.windy_batch(2, 32, seed=13).sheets
