@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--warm", default="learned", choices=["previous", "zero", "learned"])
     ap.add_argument("--solver", default="auto", choices=["auto", "batched"],
                     help="auto: sheets that fit a cluster's shared memory are solved cluster-resident")
+    ap.add_argument("--precond-degree", type=int, default=3,
+                    help="cluster-resident solver's preconditioner: 1 block-Jacobi, odd 3..15 a strip-local "
+                         "Chebyshev polynomial of that degree (the batched loop always uses block-Jacobi)")
     ap.add_argument("--train-sheets", type=int, default=256, help="sheets of the training trajectories")
     ap.add_argument("--train-steps", type=int, default=24, help="recorded steps per training trajectory")
     ap.add_argument("--epochs", type=int, default=16)
@@ -350,11 +353,11 @@ def run_ours(args):
 
     solver_code = {"auto": native.SOLVER_AUTO, "batched": native.SOLVER_BATCHED}
 
-    def timed_arm(precision, warm, solver, clocks=None):
+    def timed_arm(precision, warm, solver, clocks=None, degree=args.precond_degree):
         ctx.set_state(x0, v0)
         p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol, max_iters=4000,
                                precision=precision, warm_start=native.WARM_ZERO, use_graph=0 if args.host_loop else 1,
-                               solver=solver_code[solver])
+                               solver=solver_code[solver], precond_degree=degree)
         for i in range(args.warmup):
             ctx.step(p, allow_unconverged=True)
             p.warm_start = warm
@@ -401,17 +404,23 @@ def run_ours(args):
     node_steps = N * args.steps * world
     value = best["value"]
     head = f"mixed_{args.warm}_{args.solver}"
-    arms = {head: {k: best[k] for k in keys}}
+    arms = {head: dict({k: best[k] for k in keys}, precond_degree=args.precond_degree if args.solver == "auto" else 1)}
     if not args.no_plain:
-        for name, prec, warm, solver in [("mixed_zero_auto", native.PREC_MIXED, native.WARM_ZERO, "auto"),
-                                         ("mixed_previous_auto", native.PREC_MIXED, native.WARM_PREVIOUS, "auto"),
-                                         ("plain_fp32_zero_auto", native.PREC_PLAIN_FP32, native.WARM_ZERO, "auto"),
-                                         ("mixed_previous_batched", native.PREC_MIXED, native.WARM_PREVIOUS, "batched"),
-                                         ("plain_fp32_zero_batched", native.PREC_PLAIN_FP32, native.WARM_ZERO, "batched")]:
-            if name in arms:
+        # the plain FP32 arms keep block-Jacobi (the reference's solver structure); the mixed arms
+        # use --precond-degree, with block-Jacobi beside them
+        deg = args.precond_degree
+        for name, prec, warm, solver, d in [
+                ("mixed_zero_auto", native.PREC_MIXED, native.WARM_ZERO, "auto", deg),
+                ("mixed_previous_auto", native.PREC_MIXED, native.WARM_PREVIOUS, "auto", deg),
+                ("mixed_learned_auto_block_jacobi", native.PREC_MIXED, native.WARM_LEARNED, "auto", 1),
+                ("mixed_zero_auto_block_jacobi", native.PREC_MIXED, native.WARM_ZERO, "auto", 1),
+                ("plain_fp32_zero_auto", native.PREC_PLAIN_FP32, native.WARM_ZERO, "auto", 1),
+                ("mixed_previous_batched", native.PREC_MIXED, native.WARM_PREVIOUS, "batched", 1),
+                ("plain_fp32_zero_batched", native.PREC_PLAIN_FP32, native.WARM_ZERO, "batched", 1)]:
+            if name in arms or (warm == native.WARM_LEARNED and args.warm != "learned") or (d == deg and name.endswith("block_jacobi")):
                 continue
-            r = timed_arm(prec, warm, solver)
-            arms[name] = {k: r[k] for k in keys}
+            r = timed_arm(prec, warm, solver, degree=d)
+            arms[name] = dict({k: r[k] for k in keys}, precond_degree=d if solver == "auto" else 1)
     plain = arms.get("plain_fp32_zero_batched")
 
     # Rooflines, timed live on the context's stream (cs_profile_kernels).  The dominant kernel
@@ -420,7 +429,7 @@ def run_ours(args):
     # blocks x 40 B + nodes x 48 B), the same per-iteration figure as the batched SpMV's; the
     # resident kernel serves them from shared memory, so its DRAM traffic is far below them.
     prof = ctx.profile_kernels(native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol,
-                                                  max_iters=4000), reps=5)
+                                                  max_iters=4000, precond_degree=args.precond_degree), reps=5)
     it_res, _, _ = ctx.instance_stats()
     nnzb = sizes[6]
     peaks = measured_peaks()
@@ -443,13 +452,20 @@ def run_ours(args):
     if prof["resident_solve"] > 0:
         per_sheet = np.array([(s_["fx"].shape[0], s_["x"].shape[0]) for s_ in scene.sheets], np.float64)
         nnzb_sheet = nnzb / len(scene.sheets)  # identical topologies in this workload
-        res_bytes = float(np.sum(it_res * (nnzb_sheet * 40 + per_sheet[:, 1] * 48)))
+        # a CG iteration is one full SpMV plus, with the strip-local Chebyshev preconditioner,
+        # (degree - 1) SpMVs over the strip-local blocks; each solve adds the power iterations
+        rb = ctx.resident_blocks()
+        local_frac = rb["local_blocks"] / max(rb["blocks"], 1)
+        local_spmvs = it_res * (args.precond_degree - 1) + rb["power_iters"] if args.precond_degree >= 3 else 0 * it_res
+        res_bytes = float(np.sum(it_res * (nnzb_sheet * 40 + per_sheet[:, 1] * 48)
+                                 + local_spmvs * (local_frac * nnzb_sheet * 40 + per_sheet[:, 1] * 48)))
         res_achieved = res_bytes / (prof["resident_solve"] * 1e-3) / 1e9
         roof_res = {"bound": "hbm", "achieved": res_achieved, "peak": peak, "unit": "GB/s",
                     "frac": res_achieved / peak,
                     "traffic": traffic_per_launch("cs_resident_pcg_kernel_windy32x64_traffic.json", len(scene.sheets)),
                     "kernel": "cs_resident_pcg_kernel", "bytes_per_launch": res_bytes,
                     "ms_per_launch": prof["resident_solve"], "cg_iterations_per_launch": int(it_res.sum()),
+                    "local_spmvs_per_launch": int(np.sum(local_spmvs)), "local_block_frac": local_frac,
                     "note": "per-iteration operands served from shared memory: achieved is the rate at which the "
                             "solve consumes SpMV bytes, against the HBM roofline of the streaming formulation"}
     roofline = roof_res if (roof_res and args.solver == "auto") else roof_spmv
@@ -466,7 +482,7 @@ def run_ours(args):
     pv = C.cast(hv.data_ptr(), fp)
     p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol, max_iters=4000,
                            precision=native.PREC_MIXED, warm_start=native.WARM_ZERO, use_graph=0 if args.host_loop else 1,
-                           solver=solver_code[args.solver])
+                           solver=solver_code[args.solver], precond_degree=args.precond_degree)
     ctx.set_state(x0, v0)
     for i in range(args.warmup):
         ctx.check(ctx.lib.cs_set_state(ctx.h, px, pv))
@@ -504,6 +520,8 @@ def run_ours(args):
                 "nnzb_per_gpu": nnzb, "tol": args.tol, "solver": "mixed FP32 PCG + FP64 refinement",
                 "warm_start": args.warm,
                 "solver": args.solver,
+                "precond": ("strip-local Chebyshev degree %d over block-Jacobi" % args.precond_degree
+                            if args.precond_degree >= 3 and args.solver == "auto" else "block-Jacobi"),
                 "l2": "inputs larger than L2 (system matrix %.2f GB per GPU)" % (sizes[3] * 36 / 1e9),
                 "parallelism": f"sheets x{world} (no collective on the data path)",
                 "launch": "host loop" if args.host_loop else "CUDA graph with a device-driven while loop",

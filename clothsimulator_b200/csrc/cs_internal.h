@@ -78,8 +78,9 @@ enum InstPhase : int {
 // Cluster-resident solver limits: CTAs per cluster, warps (slices) per CTA, block slots per
 // row (the SpMV over a row is fully unrolled to this width; column codes live in registers).
 #define CS_RES_MAX_CL 16
-#define CS_RES_MAX_WARPS 18
+#define CS_RES_MAX_WARPS 16
 #define CS_RES_MAX_WIDTH 16
+#define CS_CHEB_POWER_ITERS 10  // power iterations per sheet solve for the strip-local Chebyshev bound
 #define CS_SOLVER_AUTO_DEV 0
 #define CS_SOLVER_BATCHED_DEV 1
 
@@ -121,6 +122,7 @@ struct DevParams {
     int loop_cap;          // hard bound on loop trips per step
     int advance;           // 1: v += dv, x += dt v at the end of the step
     int solver;            // CS_SOLVER_AUTO_DEV: resident sheets on the cluster kernel; BATCHED: loop only
+    int cheb_degree;       // resident solver: 1 block-Jacobi; odd >= 3 strip-local Chebyshev of that degree
 };
 
 // One proximity as seen by one sheet it touches (cs_set_proximities): node[i] is a batch
@@ -190,6 +192,7 @@ struct Batch {
     uint32_t* rsend = nullptr;   // halo sends: src slot | dst rank << 12 | dst halo index << 16
     int* rhalo = nullptr;        // per topology: CS_RES_MAX_CL + 1 halo slot counts per rank
     int res_halo0 = 0;           // first halo slot of every CTA's p array (= own slots per CTA)
+    int res_alt = 0;             // first slot of the second own-row buffer (strip-local Chebyshev)
     // per-topology block CSR (local ids, columns ascending) with the SELL slot of each block
     int* tcsr_ptr = nullptr;
     int* tcsr_col = nullptr;

@@ -505,6 +505,7 @@ struct ResidentPlan {
     std::vector<int> split, code, sendptr, halo_count;
     std::vector<uint32_t> send;
     int w = 0, max_halo = 0, max_panels = 0, max_width = 0;
+    long long blocks = 0, local_blocks = 0;  // pattern blocks; those with row and column on one CTA
 };
 
 #define CS_RES_HALO_BIT 0x40000000
@@ -554,6 +555,11 @@ ResidentPlan residentPlan(const Topo& T, int ncta) {
                     }
                 }
     }
+    for (int i = 0; i < nn; i++)
+        for (int q = T.csr_ptr[i]; q < T.csr_ptr[i + 1]; q++) {
+            P.blocks++;
+            P.local_blocks += owner[T.csr_col[q]] == owner[i];
+        }
     P.sendptr.assign(CS_RES_MAX_CL + 1, 0);
     for (int c = 0; c < ncta; c++) {
         P.sendptr[c] = (int)P.send.size();
@@ -633,6 +639,8 @@ struct cs_ctx {
     int resCL = 0, resThreads = 0, resClusters = 0, resClustersMax = 0;
     size_t resSmem = 0;
     std::vector<int> rlistAll;  // resident sheets before the proximity filter
+    std::vector<int> rlistCur;  // resident sheets now
+    std::vector<long long> sheetBlocks, sheetLocalBlocks;  // per sheet: pattern blocks, strip-local ones
     // proximities (cs_set_proximities): their device lists, and the host copies of the
     // blocks outside the pattern that cs_get_system merges
     ProxBuffers prox;
@@ -716,6 +724,7 @@ void freeBatch(cs_ctx* c) {
     c->contactReady = false;
     c->sheetGroupDev = nullptr;
     c->rlistAll.clear();
+    c->rlistCur.clear();
     c->B = Batch();
     c->loaded = false;
     c->lastStepValid = false;
@@ -838,6 +847,7 @@ DevParams toDev(const cs_step_params* p) {
     d.loop_cap = 2 * d.max_iters + 256;
     d.advance = p->advance;
     d.solver = p->solver == CS_SOLVER_BATCHED ? CS_SOLVER_BATCHED_DEV : CS_SOLVER_AUTO_DEV;
+    d.cheb_degree = p->precond_degree >= 3 ? p->precond_degree : 1;
     return d;
 }
 
@@ -977,9 +987,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     // Cluster-resident solve plan (resident.cu).  Clusters must fit a GPC, so the number of
     // SMs a cluster size keeps busy varies: 8- and 9-CTA clusters are planned and the one that
     // makes the most sheets resident, then keeps the most SMs busy, is taken (on the B200, 15
-    // clusters of 8 occupy 120 SMs, 15 clusters of 9 occupy 135).  CS_RESIDENT_CL (2..16)
-    // forces a size; 0 solves every sheet in the batched loop.
-    std::vector<int> candidates = {8, 9};
+    // clusters of 8 occupy 120 SMs, 15 clusters of 9 occupy 135, 11 of 10 occupy 110).
+    // CS_RESIDENT_CL (2..16) forces a size; 0 solves every sheet in the batched loop.
+    std::vector<int> candidates = {8, 9, 10};
     if (const char* ev = std::getenv("CS_RESIDENT_CL")) {
         const int v = std::atoi(ev);
         if (v != 0 && (v < 2 || v > CS_RES_MAX_CL))
@@ -1014,7 +1024,8 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             R.halo = std::max(R.halo, P.max_halo);
         }
         if (R.w == 0) return R;
-        const size_t pbytes = ((size_t)R.w * CS_SLICE + R.halo) * sizeof(float4);
+        // p array: own slots, halo slots, then a second own-slot buffer (strip-local Chebyshev)
+        const size_t pbytes = ((size_t)2 * R.w * CS_SLICE + R.halo) * sizeof(float4);
         const size_t budget = devProp.sharedMemPerBlockOptin > resAttr.sharedSizeBytes + pbytes
                                   ? devProp.sharedMemPerBlockOptin - resAttr.sharedSizeBytes - pbytes : 0;
         R.cap = (int)std::min<size_t>((size_t)R.panels, budget / (CS_PANEL_FLOATS * sizeof(float)));
@@ -1226,9 +1237,17 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     B.n_resident = (int)hrlist.size();
     B.res_cap = resCap;
     B.res_halo0 = resW * CS_SLICE;
+    B.res_alt = resW * CS_SLICE + res.halo;
     c->resClustersMax = c->resClusters;
     c->resClusters = std::min(c->resClusters, B.n_resident);
     c->rlistAll = hrlist;
+    c->rlistCur = hrlist;
+    c->sheetBlocks.assign(n_sheets, 0);
+    c->sheetLocalBlocks.assign(n_sheets, 0);
+    for (int s : hrlist) {
+        c->sheetBlocks[s] = plans[sheetTopoId[s]].blocks;
+        c->sheetLocalBlocks[s] = plans[sheetTopoId[s]].local_blocks;
+    }
     c->sheets = hs;
     c->slices = hslices;
 
@@ -1314,6 +1333,18 @@ cs_status cs_get_solver_info(const cs_ctx* c, int* info) {
     info[3] = c->resClusters;
     info[4] = c->B.res_cap;
     info[5] = (int)c->resSmem;
+    return CS_OK;
+}
+
+cs_status cs_get_resident_blocks(const cs_ctx* c, long long* out) {
+    if (!c || !out) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return CS_ERR_STATE;
+    out[0] = out[1] = 0;
+    for (int s : c->rlistCur) {
+        out[0] += c->sheetBlocks[s];
+        out[1] += c->sheetLocalBlocks[s];
+    }
+    out[2] = CS_CHEB_POWER_ITERS;
     return CS_OK;
 }
 
@@ -1467,6 +1498,7 @@ cs_status applyProximities(cs_ctx* c, int n, float thickness) {
         if (!touched[s]) rl.push_back(s);
     if (!rl.empty()) CS_CUDA(cudaMemcpy(B.rlist, rl.data(), rl.size() * sizeof(int), cudaMemcpyHostToDevice));
     B.n_resident = (int)rl.size();
+    c->rlistCur = rl;
     c->resClusters = std::min(c->resClustersMax, B.n_resident);
     return CS_OK;
 }
@@ -1910,6 +1942,8 @@ static cs_status validateParams(cs_ctx* c, const cs_step_params* p) {
     if (p->precision != CS_PREC_PLAIN_FP32 && p->precision != CS_PREC_MIXED) return fail(c, CS_ERR_INVALID_ARG, "bad precision");
     if (p->warm_start < CS_WARM_ZERO || p->warm_start > CS_WARM_GIVEN) return fail(c, CS_ERR_INVALID_ARG, "bad warm start");
     if (p->solver != CS_SOLVER_AUTO && p->solver != CS_SOLVER_BATCHED) return fail(c, CS_ERR_INVALID_ARG, "bad solver");
+    if (p->precond_degree < 0 || p->precond_degree > CS_PRECOND_MAX_DEGREE || (p->precond_degree > 1 && p->precond_degree % 2 == 0))
+        return fail(c, CS_ERR_INVALID_ARG, "precond_degree must be 0, 1 or odd up to CS_PRECOND_MAX_DEGREE");
     if (p->warm_start == CS_WARM_LEARNED && !c->mlpInit)
         return fail(c, CS_ERR_NOT_TRAINED, "learned warm start: no network (cs_mlp_init / cs_mlp_set_weights)");
     return CS_OK;

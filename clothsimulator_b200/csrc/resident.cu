@@ -129,7 +129,15 @@ struct __align__(16) ResShared {
     uint64_t bar[5];                   // 0 halo, 1-2 reduction buffers, 3 residual signal, 4 work item
     int next;                          // work item sent by rank 0
     int abort_flag;                    // raised by any CTA whose wait ran out
+    // strip-local Chebyshev preconditioner of the current sheet: degree (1: block-Jacobi),
+    // 1/theta, and per step k the coefficients of d_k = a_k d_{k-1} + b_k P^-1 (r - A_loc x)
+    int cheb_deg;
+    float cheb_inv_th;
+    float cheb_a[CS_PRECOND_MAX_DEGREE], cheb_b[CS_PRECOND_MAX_DEGREE];
 };
+
+constexpr float CHEB_LMAX_MARGIN = 1.1f; // the estimate approaches lambda_max from below
+constexpr float CHEB_LMIN_RATIO = 1.0f / 30.0f;
 
 // Waits for `parity` of `bar` on every thread, at most RES_WAIT_TRIES polls, giving up early
 // once another CTA raised the abort flag.  Returns true on every thread only if the whole
@@ -220,6 +228,33 @@ __device__ __forceinline__ bool cluster_sum3(ResShared& S, int rank, int ncta, u
         }
     }
     return ok;
+}
+
+// CTA-wide sums of two values in FP64, in a fixed order (warp butterfly, then warp partials in
+// warp order); every thread returns the same sums.  Ends with a barrier, so S.wsum is free again.
+__device__ __forceinline__ void cta_sum2(ResShared& S, double& a, double& b) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    a = rwarp_sum(a);
+    b = rwarp_sum(b);
+    if (lane == 0) {
+        S.wsum[w][0] = a;
+        S.wsum[w][1] = b;
+    }
+    __syncthreads();
+    double sa = 0.0, sb = 0.0;
+    for (int j = 0; j < nw; j++) {
+        sa += S.wsum[j][0];
+        sb += S.wsum[j][1];
+    }
+    a = sa;
+    b = sb;
+    __syncthreads();
+}
+
+__device__ __forceinline__ void mat3_vec(const float (&M)[9], const float (&x)[3], float (&y)[3]) {
+    y[0] = M[0] * x[0] + M[1] * x[1] + M[2] * x[2];
+    y[1] = M[3] * x[0] + M[4] * x[1] + M[5] * x[2];
+    y[2] = M[6] * x[0] + M[7] * x[1] + M[8] * x[2];
 }
 
 // w += (row of A) u over the row's block slots whose u entry is local (HALO = false: own
@@ -363,6 +398,63 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
         int phase = P.warm ? PH_RES : PH_INIT;
         bool ok = true;
 
+        // q = A_loc x over this CTA's own rows (the strip's diagonal block of A), x in `buf`
+        float4* const su_alt = su + B.res_alt;
+        auto local_spmv = [&](const float4* buf, float (&q)[3]) {
+            q[0] = q[1] = q[2] = 0.f;
+            if (in_smem)
+                row_times_u<false>(sm_panels + (size_t)lp * CS_PANEL_FLOATS, width, cw, buf, halo0, lane, q[0], q[1], q[2]);
+            else
+                row_times_u<false>(B.A + (size_t)gp * CS_PANEL_FLOATS, width, cw, buf, halo0, lane, q[0], q[1], q[2]);
+        };
+        // Strip-local Chebyshev preconditioner: the largest eigenvalue of P^-1 A_loc by power
+        // iteration from a hashed +-1 vector (the first barrier also covers the panel copy),
+        // then the coefficients of the Chebyshev iteration on [lmax / 30, lmax].  An odd
+        // degree keeps the polynomial positive on all of (0, inf), so the preconditioner is
+        // SPD whatever the estimate.
+        if (P.cheb_degree >= 3) {
+            float v[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const uint32_t h = (uint32_t)(3 * row + c) * 0x9E3779B1u;
+                v[c] = live ? (((h >> 16) & 1u) ? 1.f : -1.f) : 0.f;
+            }
+            double lam = 0.0;
+            for (int it = 0; it < CS_CHEB_POWER_ITERS; it++) {
+                if (live) su_alt[myslot] = make_float4(v[0], v[1], v[2], 0.f);
+                __syncthreads();
+                float q[3], z[3];
+                local_spmv(su_alt, q);
+                mat3_vec(Pi, q, z);
+                double zz = (double)z[0] * z[0] + (double)z[1] * z[1] + (double)z[2] * z[2];
+                double vv = (double)v[0] * v[0] + (double)v[1] * v[1] + (double)v[2] * v[2];
+                cta_sum2(S, zz, vv);
+                lam = vv > 0.0 ? sqrt(zz / vv) : 0.0;
+                const float sc = zz > 0.0 ? (float)(1.0 / sqrt(zz)) : 0.f;
+#pragma unroll
+                for (int c = 0; c < 3; c++) v[c] = z[c] * sc;
+            }
+            if (tid == 0) {
+                int deg = P.cheb_degree;
+                if (!(lam > 0.0) || !rfinite(lam)) deg = 1;
+                const float lmax = CHEB_LMAX_MARGIN * (float)lam, lmin = lmax * CHEB_LMIN_RATIO;
+                const float th = 0.5f * (lmax + lmin), de = 0.5f * (lmax - lmin), sig = th / de;
+                float rho = 1.f / sig;
+                S.cheb_inv_th = 1.f / th;
+                for (int k = 1; k < deg; k++) {
+                    const float rn = 1.f / (2.f * sig - rho);
+                    S.cheb_a[k] = rn * rho;
+                    S.cheb_b[k] = 2.f * rn / de;
+                    rho = rn;
+                }
+                S.cheb_deg = deg;
+            }
+        } else if (tid == 0) {
+            S.cheb_deg = 1;
+        }
+        __syncthreads();
+        const int cdeg = S.cheb_deg;
+
         while (phase != PH_FINISH) {
             if (++trips > P.loop_cap) {
                 flags |= CS_IF_CAPPED;
@@ -456,9 +548,36 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     r[c] = __fmaf_rn(-alpha, sv3[c], r[c]);
                 }
             }
-            u[0] = Pi[0] * r[0] + Pi[1] * r[1] + Pi[2] * r[2];
-            u[1] = Pi[3] * r[0] + Pi[4] * r[1] + Pi[5] * r[2];
-            u[2] = Pi[6] * r[0] + Pi[7] * r[1] + Pi[8] * r[2];
+            mat3_vec(Pi, r, u);
+            if (cdeg >= 3) {
+                // u = x after cdeg steps of the Chebyshev iteration for A_loc x = r from x = 0.
+                // Steps alternate between the two own-row buffers, ending on su_alt (cdeg - 1
+                // is even), so one barrier per step orders every write after the reads of the
+                // buffer's previous contents, the final su write included.
+                float d[3];
+                const float ith = S.cheb_inv_th;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    d[c] = u[c] * ith;
+                    u[c] = d[c];
+                }
+                for (int k = 1; k < cdeg; k++) {
+                    float4* const buf = (k & 1) ? su : su_alt;
+                    if (live) buf[myslot] = make_float4(u[0], u[1], u[2], 0.f);
+                    __syncthreads();
+                    float q[3], t[3];
+                    local_spmv(buf, q);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) q[c] = r[c] - q[c];
+                    mat3_vec(Pi, q, t);
+                    const float ca = S.cheb_a[k], cb = S.cheb_b[k];
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        d[c] = ca * d[c] + cb * t[c];
+                        u[c] += d[c];
+                    }
+                }
+            }
             if (live) su[myslot] = make_float4(u[0], u[1], u[2], 0.f);
             __syncthreads();
             if (tid == 0) rbar_expect(hbar, halo_bytes);

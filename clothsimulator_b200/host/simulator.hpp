@@ -103,6 +103,7 @@ struct SolverOptions {
     int maxIters = 2000;
     int precision = CS_PREC_MIXED;
     int warmStart = CS_WARM_PREVIOUS;
+    int precondDegree = 3;  // strip-local Chebyshev of the cluster-resident solver (1: block-Jacobi)
     std::string network;  // weights for the learned warm start (CS_MLP_PARAMS floats, binary)
 };
 

@@ -39,7 +39,7 @@ EXPORTED = [
     "cs_mlp_train", "cs_mlp_gradient", "cs_mlp_predict", "cs_mlp_get_record", "cs_mlp_get_weights",
     "cs_mlp_set_weights", "cs_get_solver_info", "cs_set_proximities", "cs_detect_proximities",
     "cs_get_proximities", "cs_collision_step", "cs_mlp_moments", "cs_mlp_set_moments", "cs_mlp_gradient_device",
-    "cs_mlp_apply_gradient",
+    "cs_mlp_apply_gradient", "cs_get_resident_blocks",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -77,6 +77,7 @@ class StepParams(ctypes.Structure):
         ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double), ("max_iters", ctypes.c_int),
         ("sweep_cap", ctypes.c_int), ("precision", ctypes.c_int), ("warm_start", ctypes.c_int),
         ("advance", ctypes.c_int), ("use_graph", ctypes.c_int), ("solver", ctypes.c_int),
+        ("precond_degree", ctypes.c_int),
     ]
 
 
@@ -149,6 +150,7 @@ def load_library() -> ctypes.CDLL:
         "cs_load_batch": [vp, ctypes.POINTER(MaterialDesc), ctypes.c_int, ctypes.POINTER(SheetDesc), ctypes.c_int],
         "cs_get_sizes": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "cs_get_solver_info": [vp, ctypes.POINTER(ctypes.c_int)],
+        "cs_get_resident_blocks": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "cs_set_proximities": [vp, vp, ctypes.c_int, ctypes.c_float],
         "cs_detect_proximities": [vp, ctypes.POINTER(DetectParams), ctypes.POINTER(ctypes.c_int)],
         "cs_get_proximities": [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
@@ -229,7 +231,7 @@ def material_desc(spec: dict) -> MaterialDesc:
 
 def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, inner_tol=1e-4, max_iters=2000,
                 sweep_cap=0, precision=PREC_MIXED, warm_start=WARM_ZERO, advance=1, use_graph=1,
-                solver=0) -> StepParams:
+                solver=0, precond_degree=1) -> StepParams:
     p = StepParams()
     p.dt = dt
     for i in range(3):
@@ -244,6 +246,7 @@ def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, in
     p.advance = advance
     p.use_graph = use_graph
     p.solver = solver
+    p.precond_degree = precond_degree
     return p
 
 
@@ -322,6 +325,13 @@ class Context:
         self.check(self.lib.cs_get_solver_info(self.h, s))
         keys = ("resident_sheets", "ctas_per_cluster", "threads_per_cta", "clusters", "panels_in_smem", "smem_bytes")
         return dict(zip(keys, [int(v) for v in s]))
+
+    def resident_blocks(self) -> dict:
+        """Blocks of the resident sheets' systems, the strip-local ones (read by each local SpMV
+        of the Chebyshev preconditioner), and the power iterations per resident solve."""
+        s = (ctypes.c_longlong * 3)()
+        self.check(self.lib.cs_get_resident_blocks(self.h, s))
+        return {"blocks": int(s[0]), "local_blocks": int(s[1]), "power_iters": int(s[2])}
 
     def set_proximities(self, prox: dict | None, thickness: float = 0.0):
         """Proximities of the following steps (None or an empty dict clears them); see

@@ -88,7 +88,14 @@ typedef struct cs_step_params {
     int advance;              /* 1: v += dv and x += dt v (a full step); 0: solve only */
     int use_graph;            /* 1: run the captured CUDA graph; 0: host-driven launches */
     int solver;               /* CS_SOLVER_*: which PCG kernels solve the sheets */
+    int precond_degree;       /* cluster-resident solver's preconditioner: 0 or 1 the 3x3
+                                 block-Jacobi inverse; an odd degree 3..CS_PRECOND_MAX_DEGREE a
+                                 Chebyshev polynomial of that degree in the block-Jacobi-scaled
+                                 matrix of each CTA's strip of rows (no exchange between CTAs).
+                                 The batched loop always uses block-Jacobi. */
 } cs_step_params;
+
+#define CS_PRECOND_MAX_DEGREE 15
 
 /* CS_SOLVER_AUTO: sheets whose system fits one thread-block cluster's shared memory are
  * solved by a cluster each, the system resident on chip for the whole solve; the others by
@@ -130,6 +137,13 @@ cs_status cs_get_sizes(const cs_ctx* ctx, long long* sizes);
  * in the persistent grid, SELL panels per CTA in shared memory, dynamic shared memory bytes
  * per CTA.  No counterpart in the reference (its solver has no such plan). */
 cs_status cs_get_solver_info(const cs_ctx* ctx, int* info);
+
+/* out[0..2] = 3x3 blocks of the systems of the sheets now solved cluster-resident (the mesh
+ * pattern's), those among them whose row and column belong to the same CTA's strip of rows
+ * (what one strip-local SpMV of the Chebyshev preconditioner reads), and the power iterations
+ * each resident solve runs for that preconditioner's eigenvalue bound.  For work accounting
+ * (rooflines); no counterpart in the reference. */
+cs_status cs_get_resident_blocks(const cs_ctx* ctx, long long* out);
 
 /* Node state of the whole batch, sheets concatenated in load order (3 floats per node). */
 cs_status cs_set_state(cs_ctx* ctx, const float* x, const float* v);

@@ -58,8 +58,8 @@ def test_plan_covers_sheets_that_fit(ctx_factory):
     ctx = ctx_factory(scene.sheets)
     info = ctx.solver_info()
     assert info["resident_sheets"] == 6
-    # 8 or 9 CTAs per cluster: whichever keeps more SMs busy for this plan
-    assert info["ctas_per_cluster"] in (8, 9) and info["clusters"] >= 1
+    # 8, 9 or 10 CTAs per cluster: whichever keeps more SMs busy for this plan
+    assert info["ctas_per_cluster"] in (8, 9, 10) and info["clusters"] >= 1
     assert info["threads_per_cta"] % 32 == 0 and info["threads_per_cta"] <= 768
     # a 128x128 sheet needs more than 24 slices per CTA: it stays in the batched loop
     big = scenes.windy_batch(1, 128, seed=12).sheets + scenes.windy_batch(2, 32, seed=13).sheets
@@ -160,3 +160,65 @@ def test_mixed_resident_and_batched_batch(ctx_factory):
     assert stats.converged == 3
     for s, dv in zip(scene.sheets, split_dv(ctx, scene)):
         assert rel(dv, oracle_dv(scene, s)) < 1e-6
+
+
+# Strip-local Chebyshev preconditioner (precond_degree 3..15, odd): a different but fixed SPD
+# preconditioner, so the solution must still meet the FP64-checked tolerance and match the
+# direct solve; the iteration counts must fall well below block-Jacobi's.
+
+@pytest.mark.parametrize("degree", [3, 5, 7])
+def test_chebyshev_resident_matches_oracle(ctx_factory, degree):
+    scene = scenes.windy_batch(3, 32, seed=21)
+    scene.sheets += scenes.windy_batch(1, 64, seed=22).sheets
+    ctx = ctx_factory(scene.sheets)
+    assert ctx.solver_info()["resident_sheets"] == 4
+    x0, v0 = initial_state(scene)
+    it = {}
+    for deg in (1, degree):
+        ctx.set_state(x0, v0)
+        stats, _ = ctx.step(params_for(scene, precond_degree=deg))
+        assert stats.converged == 4
+        it[deg], rr, fl = ctx.instance_stats()
+        assert np.all(rr <= 1e-10)
+        for s, dv in zip(scene.sheets, split_dv(ctx, scene)):
+            assert rel(dv, oracle_dv(scene, s)) < 1e-6
+    # degree 3 needs about half of block-Jacobi's iterations, 5 and 7 about a third
+    bound = 0.7 if degree == 3 else 0.55
+    assert it[degree].sum() <= bound * it[1].sum(), (it[degree], it[1])
+
+
+def test_chebyshev_plain_fp32_and_determinism(ctx_factory):
+    scene = scenes.windy_batch(3, 32, seed=71)
+    ctx = ctx_factory(scene.sheets)
+    x0, v0 = initial_state(scene)
+    out = []
+    for _ in range(2):
+        ctx.set_state(x0, v0)
+        ctx.step(params_for(scene, tol=1e-6, precond_degree=5))
+        out.append(ctx.get_dv().copy())
+    assert np.array_equal(out[0], out[1])
+    ctx.set_state(x0, v0)
+    ctx.step(params_for(scene, tol=1e-6, precision=native.PREC_PLAIN_FP32, precond_degree=5), allow_unconverged=True)
+    it, rr, fl = ctx.instance_stats()
+    assert np.all(it > 0) and np.all(rr < 1e-3)
+    assert np.array_equal((fl & 1) > 0, rr <= 1e-6)
+
+
+def test_chebyshev_degree_is_ignored_by_batched_loop(ctx_factory):
+    scene = scenes.windy_batch(2, 32, seed=91)
+    ctx = ctx_factory(scene.sheets)
+    x0, v0 = initial_state(scene)
+    res = []
+    for deg in (1, 5):
+        ctx.set_state(x0, v0)
+        ctx.step(params_for(scene, solver=native.SOLVER_BATCHED, precond_degree=deg))
+        res.append((ctx.get_dv().copy(), ctx.instance_stats()[0].copy()))
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+def test_chebyshev_degree_validation(ctx_factory):
+    scene = scenes.windy_batch(1, 16, seed=92)
+    ctx = ctx_factory(scene.sheets)
+    for bad in (-1, 2, 4, 17):
+        st = ctx.lib.cs_step(ctx.h, native.ctypes.byref(params_for(scene, precond_degree=bad)), None)
+        assert st == native.CS_ERR_INVALID_ARG, bad
