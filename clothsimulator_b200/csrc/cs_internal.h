@@ -69,7 +69,8 @@ struct SliceDesc {
 enum InstPhase : int {
     PH_CG = 0,        // one preconditioned CG iteration on the FP32 correction system
     PH_RES = 1,       // FP64 residual b - A (dv64 + e) and its norm
-    PH_INIT = 2,      // start a CG sweep: dv64 += e, e = 0, z = P r, p = z
+    PH_INIT = 2,      // start a CG sweep: dv64 += e, e = 0, z = P r, p = z (or, continuing after a
+                      // reliable update, p = z + beta p with the FP64 residual in r)
     PH_FINISH = 3,    // dv64 += e, then done
     PH_DONE = 4,
     PH_RESIDENT = 5,  // owned by the cluster-resident kernel this step (skipped by the loop)
@@ -80,6 +81,9 @@ enum InstPhase : int {
 #define CS_RES_MAX_CL 16
 #define CS_RES_MAX_WARPS 16
 #define CS_RES_MAX_WIDTH 16
+// Reliable updates keep the search direction only while the recursive residual has drifted
+// from the FP64 one by at most this fraction of the latter (larger drift: restart).
+#define CS_RELIABLE_DRIFT 0.1
 #define CS_CHEB_POWER_ITERS 10  // power iterations per sheet solve for the strip-local Chebyshev bound
 #define CS_SOLVER_AUTO_DEV 0
 #define CS_SOLVER_BATCHED_DEV 1
@@ -93,7 +97,7 @@ enum InstPhase : int {
 struct InstState {
     double bnorm2;      // ||b||^2 (FP64)
     double rz;          // r.z of the current iteration
-    double rz_new;
+    double rz_prev;     // r.z of the iteration before (a reliable update's beta)
     double pq;
     double rr;          // ||r||^2 of the recursive residual
     double res0;        // FP64 true residual norm at the start of the current sweep
@@ -105,7 +109,7 @@ struct InstState {
     int iters;          // total CG iterations this step
     int sweeps;         // FP64 residual evaluations this step
     int flags;
-    int pad;
+    int cont;           // the next PH_INIT keeps the search direction (reliable update)
 };
 
 // Step parameters in device memory (read by every kernel of the captured step graph).
@@ -114,7 +118,7 @@ struct DevParams {
     float gravity[3];
     float handle_stiffness;
     double tol;            // FP64-checked relative residual target
-    double inner_tol;      // relative reduction per CG sweep (mixed precision)
+    double inner_tol;      // mixed precision: residual reduction between FP64 residual replacements
     int max_iters;         // CG iterations per instance per step
     int sweep_cap;         // CG iterations per sweep
     int mixed;             // 1: FP32 CG + FP64 refinement; 0: plain FP32 CG (FP32 dots)

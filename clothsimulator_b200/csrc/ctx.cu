@@ -839,7 +839,7 @@ DevParams toDev(const cs_step_params* p) {
     for (int i = 0; i < 3; i++) d.gravity[i] = p->gravity[i];
     d.handle_stiffness = p->handle_stiffness;
     d.tol = p->tol > 0 ? p->tol : 1e-6;
-    d.inner_tol = p->inner_tol > 0 ? p->inner_tol : 1e-4;
+    d.inner_tol = p->inner_tol > 0 ? p->inner_tol : 1e-2;
     d.max_iters = p->max_iters > 0 ? p->max_iters : 2000;
     d.sweep_cap = p->sweep_cap > 0 ? p->sweep_cap : 1000000;
     d.mixed = p->precision == CS_PREC_MIXED;

@@ -9,11 +9,18 @@
 //   cs_spmv_kernel    PH_CG : p_new = z + beta p_old (fused), q = A p_new, partial p.q
 //                     PH_RES: r = b - A (dv64 + e) in FP64, partial ||r||^2
 //   cs_reduce1_kernel PH_CG : alpha = rz / pq
-//                     PH_RES: accept (PH_FINISH) or restart a sweep (PH_INIT)
+//                     PH_RES: accept (PH_FINISH) or go on with a new sweep (PH_INIT)
 //   cs_vector_kernel  PH_CG : e += alpha p, r -= alpha q, z = P^-1 r, partials r.z, r.r
 //                     PH_INIT / PH_FINISH: dv64 += e, e = 0 (and z, r.z for a new sweep)
 //   cs_reduce2_kernel PH_CG : beta, inner stopping test; the last block counts unfinished
 //                     instances and sets the CUDA-graph while-loop condition.
+//
+// Mixed precision uses reliable updates (Sleijpen and van der Vorst, 1996): a sweep ends when
+// the recursive residual fell by inner_tol, the FP64 residual b - A dv64 replaces r, and CG
+// goes on with the same search direction (beta = r.z / the previous iteration's r.z) instead
+// of restarting from p = z, which would discard the Krylov space built so far.  It restarts
+// when the replaced residual had drifted from the FP64 one by more than CS_RELIABLE_DRIFT of
+// its norm: the kept direction would then no longer be conjugate to the new residual's.
 //
 // Reductions are deterministic: per-slice partials (one warp per slice), then one block per
 // instance summing its slices in a fixed order.  p is double-buffered by loop-trip parity.
@@ -124,7 +131,7 @@ __global__ void __launch_bounds__(128) cs_spmv_kernel(Batch B) {
             if (lane == 0) B.part[2 * slice] = (double)df;
         }
     } else {
-        double y0 = 0.0, y1 = 0.0, y2 = 0.0, sq = 0.0;
+        double y0 = 0.0, y1 = 0.0, y2 = 0.0, sq = 0.0, dq = 0.0;
         if (live) {
             for (int k = 0; k < sd.width; k++) {
                 const int col = __ldg(&B.tcol[(sd.tpanel0 + k) * CS_SLICE + lane]) + node_off;
@@ -152,13 +159,21 @@ __global__ void __launch_bounds__(128) cs_spmv_kernel(Batch B) {
                 }
             }
             double r0 = (double)B.b[3 * row] - y0, r1 = (double)B.b[3 * row + 1] - y1, r2 = (double)B.b[3 * row + 2] - y2;
+            // drift of the recursive residual it replaces
+            const double q0 = r0 - (double)B.r[3 * row], q1 = r1 - (double)B.r[3 * row + 1],
+                         q2 = r2 - (double)B.r[3 * row + 2];
+            dq = q0 * q0 + q1 * q1 + q2 * q2;
             B.r[3 * row] = (float)r0;
             B.r[3 * row + 1] = (float)r1;
             B.r[3 * row + 2] = (float)r2;
             sq = r0 * r0 + r1 * r1 + r2 * r2;
         }
         sq = warp_sum(sq);
-        if (lane == 0) B.part[2 * slice] = sq;
+        dq = warp_sum(dq);
+        if (lane == 0) {
+            B.part[2 * slice] = sq;
+            B.part[2 * slice + 1] = dq;
+        }
     }
 }
 
@@ -191,6 +206,7 @@ __global__ void __launch_bounds__(128) cs_reduce1_kernel(Batch B) {
     const bool mixed = P.mixed != 0;
     const SheetDesc& sh = B.sheets[s];
     double sum = inst_sum(B, sh, 0, mixed, shd, shf);
+    const double drift2 = (ph == PH_RES && mixed) ? inst_sum(B, sh, 1, true, shd, shf) : 0.0;
     if (threadIdx.x != 0) return;
     if (ph == PH_CG) {
         float alpha;
@@ -228,8 +244,10 @@ __global__ void __launch_bounds__(128) cs_reduce1_kernel(Batch B) {
         I.flags |= CS_IF_CAPPED;
         I.phase = PH_FINISH;
     } else if (mixed || I.rz == 0.0) {
-        // mixed: a new CG sweep on the FP64 residual; plain: the first sweep after a warm start
+        // mixed: a new CG sweep on the FP64 residual, continuing the search direction of the
+        // last one if it ran; plain: the first sweep after a warm start
         I.res0 = res;
+        I.cont = mixed && I.sweep_iters > 0 && !(I.flags & CS_IF_BREAKDOWN) && sqrt(drift2) <= CS_RELIABLE_DRIFT * res;
         I.phase = PH_INIT;
     } else {
         // Plain FP32 PCG stopped on its own recursive residual; the FP64 check above measured
@@ -267,6 +285,15 @@ __global__ void __launch_bounds__(128) cs_vector_kernel(Batch B) {
             }
         } else {
             const bool reset = (ph == PH_INIT) && (I.flags & CS_IF_WARM_REJECTED) && I.sweeps == 1;
+            if (ph == PH_INIT && I.cont) {
+                // the last direction is in this trip's old buffer (written two trips ago, the
+                // FP64 residual trip between); the next trip reads its old p from the other one
+                const int par = B.loop[0] & 1;
+                const float* __restrict__ pLast = par ? B.pB : B.pA;
+                float* __restrict__ pKeep = par ? B.pA : B.pB;
+#pragma unroll
+                for (int c = 0; c < 3; c++) pKeep[3 * row + c] = pLast[3 * row + c];
+            }
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 int i = 3 * row + c;
@@ -328,13 +355,21 @@ __global__ void __launch_bounds__(128) cs_reduce2_kernel(Batch B, cudaGraphCondi
         if (threadIdx.x == 0) {
             const double bn = sqrt(I.bnorm2);
             if (ph == PH_INIT) {
+                float beta = 0.f;
+                if (I.cont) {
+                    // reliable update: r.z of the FP64 residual over the last iteration's r.z
+                    const double bd = rz / I.rz_prev;
+                    if (rz > 0.0 && finite_d(bd)) beta = (float)bd;
+                    I.cont = 0;
+                }
                 I.rz = rz;
                 I.rr = rr;
-                I.beta = 0.f;
+                I.beta = beta;
                 I.sweep_iters = 0;
                 I.phase = (rz > 0.0 && finite_d(rz)) ? PH_CG : PH_RES;
             } else {
                 float beta = mixed ? (float)(rz / I.rz) : (float)rz / (float)I.rz;
+                I.rz_prev = I.rz;
                 I.rz = rz;
                 I.rr = rr;
                 I.iters += 1;
@@ -397,7 +432,8 @@ __global__ void __launch_bounds__(128) cs_solve_setup_kernel(Batch B) {
     if (threadIdx.x == 0) {
         InstState& I = B.inst[s];
         I.bnorm2 = acc;
-        I.rz = I.rz_new = I.pq = I.rr = 0.0;
+        I.rz = I.rz_prev = I.pq = I.rr = 0.0;
+        I.cont = 0;
         I.res0 = sqrt(acc);
         I.resnorm = I.first_res = -1.0;
         I.alpha = I.beta = 0.f;

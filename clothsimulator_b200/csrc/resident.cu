@@ -392,7 +392,9 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
             for (int k = 0; k < 9; k++) Pi[k] = 0.f;
         }
         const double bn = sqrt(B.inst[s].bnorm2);
-        double gam = 0.0, rr = 0.0, delta = 0.0, alpha_d = 0.0, res0 = bn, resnorm = -1.0, first_res = -1.0;
+        double gam = 0.0, gam_prev = 0.0, rr = 0.0, delta = 0.0, alpha_d = 0.0, res0 = bn, resnorm = -1.0,
+               first_res = -1.0;
+        bool cont = false;  // the next PH_INIT keeps the search direction (reliable update)
         float alpha = 0.f, beta = 0.f;
         int iters = 0, sweeps = 0, sweep_iters = 0, flags = 0, trips = 0;
         int phase = P.warm ? PH_RES : PH_INIT;
@@ -496,10 +498,13 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     }
                     const double r0 = (double)B.b[3 * g] - y0, r1 = (double)B.b[3 * g + 1] - y1,
                                  r2 = (double)B.b[3 * g + 2] - y2;
+                    // drift of the recursive residual it replaces
+                    const double q0 = r0 - (double)r[0], q1 = r1 - (double)r[1], q2 = r2 - (double)r[2];
                     r[0] = (float)r0;
                     r[1] = (float)r1;
                     r[2] = (float)r2;
                     v[0] = r0 * r0 + r1 * r1 + r2 * r2;
+                    v[1] = q0 * q0 + q1 * q1 + q2 * q2;
                 }
                 ok = cluster_sum3(S, rank, ncta, nred, v, false);
                 if (!ok) break;
@@ -523,7 +528,11 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     flags |= CS_IF_CAPPED;
                     phase = PH_FINISH;
                 } else if (mixed || gam == 0.0) {
+                    // mixed: a reliable update (the FP64 residual replaced r; the direction
+                    // of the last sweep is kept if it ran and r had drifted little); plain:
+                    // the first sweep after a warm start
                     res0 = res;
+                    cont = mixed && sweep_iters > 0 && !(flags & CS_IF_BREAKDOWN) && sqrt(v[1]) <= CS_RELIABLE_DRIFT * res;
                     phase = PH_INIT;
                 } else {
                     // plain FP32 CG stopped on its recursive residual and the FP64 check failed
@@ -615,6 +624,36 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
             if (!ok) break;
             const double gnew = v[0], dnew = v[1];
             rr = v[2];
+            if (phase == PH_INIT && cont) {
+                // p = u + beta p and s = w + beta s with beta = (r.u) / (the last iteration's
+                // r.u); r no longer follows the recursion that the Chronopoulos-Gear step
+                // length assumes, so alpha = r.u / p.s is computed with one more reduction
+                cont = false;
+                const double bd = gnew / gam_prev;
+                if (gnew > 0.0 && rfinite(gnew) && rfinite(bd)) {
+                    const float bc = (float)bd;
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        p[c] = __fmaf_rn(bc, p[c], u[c]);
+                        sv3[c] = __fmaf_rn(bc, sv3[c], wv[c]);
+                    }
+                    double v2[3] = {0.0, 0.0, 0.0};
+                    if (live) v2[0] = (double)p[0] * sv3[0] + (double)p[1] * sv3[1] + (double)p[2] * sv3[2];
+                    ok = cluster_sum3(S, rank, ncta, nred, v2, false);
+                    if (!ok) break;
+                    if (v2[0] > 0.0 && rfinite(v2[0]) && rfinite(gnew / v2[0])) {
+                        gam = gnew;
+                        delta = dnew;
+                        sweep_iters = 0;
+                        beta = bc;
+                        alpha_d = gnew / v2[0];
+                        alpha = (float)alpha_d;
+                        phase = PH_CG;
+                        continue;
+                    }
+                }
+                // otherwise: restart from p = u below
+            }
             if (phase == PH_INIT) {
                 gam = gnew;
                 delta = dnew;
@@ -669,6 +708,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                 flags |= CS_IF_BREAKDOWN;
                 stop = true;
             }
+            gam_prev = gam;
             gam = gnew;
             delta = dnew;
             if (stop || iters >= P.max_iters) {

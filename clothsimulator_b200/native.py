@@ -229,7 +229,7 @@ def material_desc(spec: dict) -> MaterialDesc:
     return m
 
 
-def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, inner_tol=1e-4, max_iters=2000,
+def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, inner_tol=1e-2, max_iters=2000,
                 sweep_cap=0, precision=PREC_MIXED, warm_start=WARM_ZERO, advance=1, use_graph=1,
                 solver=0, precond_degree=1) -> StepParams:
     p = StepParams()

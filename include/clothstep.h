@@ -67,8 +67,10 @@ typedef struct cs_sheet_desc {
 /* CS_PREC_PLAIN_FP32: FP32 PCG with FP32 dot products from the guess, stopping when its own
  * recursive residual meets tol (as the reference's solve does, Cloth.cu:784-788); its true
  * residual is then checked in FP64 and reported, and the sheet counts as converged only if that
- * meets tol.  CS_PREC_MIXED: FP32 PCG sweeps with FP64 dot products inside FP64 iterative
- * refinement (outer residual b - A dv in FP64) until the FP64 residual meets tol. */
+ * meets tol.  CS_PREC_MIXED: FP32 PCG with FP64 dot products inside FP64 iterative
+ * refinement until the FP64 residual b - A dv meets tol: whenever the recursive residual fell
+ * by inner_tol, the FP64 residual replaces it and CG goes on with the same search direction
+ * (reliable updates). */
 enum { CS_PREC_PLAIN_FP32 = 0, CS_PREC_MIXED = 1 };
 enum { CS_WARM_ZERO = 0, CS_WARM_PREVIOUS = 1, CS_WARM_LEARNED = 2, CS_WARM_GIVEN = 3 };
 
@@ -80,7 +82,8 @@ typedef struct cs_step_params {
     float gravity[3];
     float handle_stiffness;   /* Magic::handleStiffness, default 1e3 (Magic.cu:6) */
     double tol;               /* relative residual ||b - A dv|| / ||b||, checked in FP64 */
-    double inner_tol;         /* mixed precision: residual reduction per CG sweep */
+    double inner_tol;         /* mixed precision: residual reduction between FP64 residual
+                                 replacements (reliable updates; 0: 1e-2) */
     int max_iters;            /* CG iterations per sheet per step */
     int sweep_cap;            /* mixed precision: CG iterations per sweep (0: no cap) */
     int precision;            /* CS_PREC_* */

@@ -81,6 +81,8 @@ def test_interactive_modes_report_unavailable():
 # Magic::collisionThickness default, computed as the host layer does: 0.1f x repulsionThickness
 # (Magic.cu:9-16) in FP32
 COLLISION_THICKNESS = float(np.float32(0.1) * np.float32(1e-3))
+# the host layer's default solver.precond_degree (SolverOptions::precondDegree)
+HOST_PRECOND_DEGREE = 3
 
 
 @pytest.mark.gpu
@@ -98,7 +100,8 @@ def test_simulate_offline_matches_c_abi(tmp_path):
     # the same scene through the C ABI directly (OBJ text has 20 significant digits: exact floats)
     ctx = native.Context(0)
     ctx.load(scene.sheets)
-    p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=1e-8, max_iters=8000)
+    p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=1e-8, max_iters=8000,
+                           precond_degree=HOST_PRECOND_DEGREE)
     for k in range(8):
         p.warm_start = native.WARM_ZERO if k == 0 else native.WARM_PREVIOUS
         ctx.detect_proximities(1e-3)  # the host layer detects before every step, as Simulator.cu:571-586
@@ -134,7 +137,8 @@ def test_contact_scene_through_host_layer_matches_c_abi(tmp_path):
     assert steps.value == n_steps
     ctx = native.Context(0)
     ctx.load(scene.sheets)
-    p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=1e-8, max_iters=8000)
+    p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=1e-8, max_iters=8000,
+                           precond_degree=HOST_PRECOND_DEGREE)
     found = []
     for k in range(n_steps):
         p.warm_start = native.WARM_ZERO if k == 0 else native.WARM_PREVIOUS
