@@ -1,14 +1,16 @@
 """Benchmark of the implicit cloth step on B200.
 
-Workload (default): 1,024 sheets of 64x64 quads (4,325,376 nodes), top edge pinned, per-sheet
+Workload (default): 1,024 sheets of 64x64 quads (4,326,400 nodes), top edge pinned, per-sheet
 horizontal wind, stretching log-U[10, 500] N/m and bending log-U[1e-6, 1e-3] N m through the
 material multipliers, dt = 1/100 s: the learned-warm-start configuration, which fits one GPU.
 One step = assembly + batched PCG to an FP64-checked relative residual of 1e-6 for every sheet
 + v += dv, x += dt v, with the state resident in HBM.
 
 Metric: node-steps/s (sum over sheets of nodes x steps / device time).  The line reports the
-mixed-precision solver with its warm start (`value`) and the plain FP32 PCG from a zero guess
-on the same GPU (`plain_fp32`).  `--impl reference` times the reference's CPU path for this
+mixed-precision solver with its warm start (`value`: cluster-resident solve, strip-local
+Chebyshev preconditioner of degree `--precond-degree`, reliable updates) and, in `arms`, the
+same solver from other starts and with block-Jacobi, and plain FP32 PCG from a zero guess on
+the same GPU.  `--impl reference` times the reference's CPU path for this
 workload (the reference's own force code compiled from its sources + FP32 sparse Cholesky).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -426,8 +428,10 @@ def run_ours(args):
     # Rooflines, timed live on the context's stream (cs_profile_kernels).  The dominant kernel
     # of the default (resident) solver is cs_resident_pcg_kernel: its algorithmic bytes per
     # launch are the CG iterations it ran times the bytes one SpMV iteration moves (stored
-    # blocks x 40 B + nodes x 48 B), the same per-iteration figure as the batched SpMV's; the
-    # resident kernel serves them from shared memory, so its DRAM traffic is far below them.
+    # blocks x 40 B + nodes x 48 B, the same per-iteration figure as the batched SpMV's), plus
+    # the Chebyshev preconditioner's strip-local SpMVs at the same rate over the strip-local
+    # blocks; the resident kernel serves them from shared memory, so its DRAM traffic is far
+    # below them.
     prof = ctx.profile_kernels(native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol,
                                                   max_iters=4000, precond_degree=args.precond_degree), reps=5)
     it_res, _, _ = ctx.instance_stats()
@@ -467,7 +471,9 @@ def run_ours(args):
                     "ms_per_launch": prof["resident_solve"], "cg_iterations_per_launch": int(it_res.sum()),
                     "local_spmvs_per_launch": int(np.sum(local_spmvs)), "local_block_frac": local_frac,
                     "note": "per-iteration operands served from shared memory: achieved is the rate at which the "
-                            "solve consumes SpMV bytes, against the HBM roofline of the streaming formulation"}
+                            "solve consumes SpMV bytes (the CG SpMVs and the Chebyshev preconditioner's strip-local "
+                            "SpMVs), against the HBM roofline of the streaming formulation; above 1 means faster than "
+                            "any solve that streams the system from HBM could run"}
     roofline = roof_res if (roof_res and args.solver == "auto") else roof_spmv
 
     # end to end through the C ABI with pinned host buffers: H2D of x, v, step, D2H of x, v
@@ -517,7 +523,8 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {
                 "workload": scene.name, "sheets": len(scene.sheets), "nq": args.nq, "nodes_per_gpu": N,
-                "nnzb_per_gpu": nnzb, "tol": args.tol, "solver": "mixed FP32 PCG + FP64 refinement",
+                "nnzb_per_gpu": nnzb, "tol": args.tol,
+                "scheme": "mixed FP32 PCG, FP64 dot products, FP64 residual replacements (reliable updates)",
                 "warm_start": args.warm,
                 "solver": args.solver,
                 "precond": ("strip-local Chebyshev degree %d over block-Jacobi" % args.precond_degree
