@@ -28,7 +28,12 @@
 #define CS_PANEL_FLOATS 288  // 32 lanes x 9 entries
 #define CS_TABLE_N 30
 #define CS_TABLE_ENTRIES (CS_TABLE_N * CS_TABLE_N * CS_TABLE_N)
-#define CS_FACE_REC 96
+// Element records, laid out for 16-byte loads in the gather.  Face (120 floats): block
+// (a, b) of -dt^2 J at [12 (3a + b) + 3 kp + kq] (three float4, the last three floats zero);
+// dt (f + dt J v) of node a at [108 + 4a + kp]; wind force at [111], [115], [119].  Edge (32
+// floats): node i's (dtheta_i, coefficient) at [4i .. 4i + 3]; dt (f + dt J v) of node i at
+// [16 + 4i + c]; theta at [19].
+#define CS_FACE_REC 120
 #define CS_EDGE_REC 32
 
 // Contributor code: bit 31 = edge (1) / face (0); bits 4..30 = sheet-local element id;

@@ -1318,7 +1318,11 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     {
         cudaDeviceProp prop;
         CS_CUDA(cudaGetDeviceProperties(&prop, c->device));
-        c->gatherGrid = std::max(1, std::min(nblk((long long)B.n_slices * 32, 128), 2 * prop.multiProcessorCount));
+        // persistent gather: CTAs per SM (CS_GATHER_CTAS_PER_SM, 1..16) bound the slices in
+        // flight, so the element records they read stay in L2
+        int perSM = 4;
+        if (const char* ev = std::getenv("CS_GATHER_CTAS_PER_SM")) perSM = std::min(16, std::max(1, std::atoi(ev)));
+        c->gatherGrid = std::max(1, std::min(nblk((long long)B.n_slices * 32, 128), perSM * prop.multiProcessorCount));
     }
     c->loaded = true;
     return CS_OK;

@@ -167,9 +167,11 @@ __device__ __forceinline__ float stretch_h(float fu_p, float fv_p, float fu_q, f
 
 }  // namespace
 
-// Face record (CS_FACE_REC = 96 floats): [0..80] the face's 9x9 contribution to A,
-// -dt*dt*J, as nine contiguous row-major 3x3 blocks (block (a, b) at 9 (3a + b)), [81..89]
-// dt*(f + dt*J*v) of the stretching term, [90..92] dt * wind force added to each node.
+// Face record (CS_FACE_REC = 120 floats, 16-byte aligned pieces for the gather's vector
+// loads): the face's 9x9 contribution to A, -dt*dt*J, as nine row-major 3x3 blocks (block
+// (a, b) at 12 (3a + b), three zero floats after each), dt*(f + dt*J*v) of the stretching
+// term for node a at 108 + 4a .. 108 + 4a + 2, and dt * wind force added to each node at
+// 111, 115, 119.
 //
 // face_eval evaluates one face exactly as Face::update (normal), the wind loop of
 // Cloth::addExternalForces and stretchingForce (PhysicsHelper.cu:264-291) do.  With
@@ -247,20 +249,22 @@ __device__ __forceinline__ void face_eval(const Batch& B, int f, float* __restri
                                       gu, gv, kp == kq);
             const float J = -area * h;
             jv += (dt * J) * vel[q];
-            if (rec) rec[9 * (3 * a + b) + 3 * kp + kq] = s * J;  // block (a, b) contiguous
+            if (rec) rec[12 * (3 * a + b) + 3 * kp + kq] = s * J;  // block (a, b): three float4
             if (Jo) Jo[9 * p + q] = J;
         }
-        if (rec) rec[81 + p] = dt * (fp + jv);
+        if (rec) rec[108 + 4 * a + kp] = dt * (fp + jv);
         if (fo) fo[p] = fp;
     }
     if (rec) {
-        rec[90] = fw.x;
-        rec[91] = fw.y;
-        rec[92] = fw.z;
+#pragma unroll
+        for (int blk = 0; blk < 9; blk++) rec[12 * blk + 9] = rec[12 * blk + 10] = rec[12 * blk + 11] = 0.0f;
+        rec[111] = fw.x;
+        rec[115] = fw.y;
+        rec[119] = fw.z;
     }
 }
 
-// One thread per face; the block's records are staged in shared memory (row stride 97 floats,
+// One thread per face; the block's records are staged in shared memory (row stride 121 floats,
 // conflict-free) and written out as one contiguous, coalesced range.
 __global__ void __launch_bounds__(64) cs_face_kernel(Batch B) {
     constexpr int kStride = CS_FACE_REC + 1;
@@ -275,8 +279,8 @@ __global__ void __launch_bounds__(64) cs_face_kernel(Batch B) {
         out[e] = stage[(e / CS_FACE_REC) * kStride + e % CS_FACE_REC];
 }
 
-// Edge record (32 floats): [0..11] dtheta, [12] coefficient, [13] theta, [16..27]
-// dt*(f + dt*J*v) of the bending term.
+// Edge record (32 floats): node i's (dtheta_i, coefficient) at [4i .. 4i + 3], dt*(f + dt*J*v)
+// of the bending term for node i at [16 + 4i .. 16 + 4i + 2], theta at [19].
 __global__ void __launch_bounds__(128) cs_edge_kernel(Batch B) {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= B.E) return;
@@ -354,13 +358,11 @@ __global__ void __launch_bounds__(128) cs_edge_kernel(Batch B) {
         bb[p] = dt * (ca * dth[p] + jv);
     }
     float4* out = reinterpret_cast<float4*>(B.edge_rec + (size_t)e * CS_EDGE_REC);
-    out[0] = make_float4(dth[0], dth[1], dth[2], dth[3]);
-    out[1] = make_float4(dth[4], dth[5], dth[6], dth[7]);
-    out[2] = make_float4(dth[8], dth[9], dth[10], dth[11]);
-    out[3] = make_float4(coef, angle, 0.0f, 0.0f);
-    out[4] = make_float4(bb[0], bb[1], bb[2], bb[3]);
-    out[5] = make_float4(bb[4], bb[5], bb[6], bb[7]);
-    out[6] = make_float4(bb[8], bb[9], bb[10], bb[11]);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        out[i] = make_float4(dth[3 * i], dth[3 * i + 1], dth[3 * i + 2], coef);
+        out[4 + i] = make_float4(bb[3 * i], bb[3 * i + 1], bb[3 * i + 2], i == 0 ? angle : 0.0f);
+    }
 }
 
 // Assembly gather.  Warps walk the slices grid-stride (a persistent launch of a few warps per
@@ -407,15 +409,17 @@ __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
                         const int elem = (int)((code[j] >> 4) & 0x7FFFFFFu);
                         const int ca = (code[j] >> 2) & 3, cb = code[j] & 3;
                         if (!(code[j] & CS_CODE_EDGE)) {
-                            const float* r = frec + (size_t)elem * CS_FACE_REC + 9 * (3 * ca + cb);
-#pragma unroll
-                            for (int e = 0; e < 9; e++) v[j][e] = __ldg(r + e);
+                            const float4* r = reinterpret_cast<const float4*>(frec + (size_t)elem * CS_FACE_REC +
+                                                                              12 * (3 * ca + cb));
+                            const float4 q0 = __ldg(r), q1 = __ldg(r + 1), q2 = __ldg(r + 2);
+                            v[j][0] = q0.x; v[j][1] = q0.y; v[j][2] = q0.z; v[j][3] = q0.w;
+                            v[j][4] = q1.x; v[j][5] = q1.y; v[j][6] = q1.z; v[j][7] = q1.w;
+                            v[j][8] = q2.x;
                         } else {
-                            const float* r = erec + (size_t)elem * CS_EDGE_REC;
-                            const float coef = __ldg(r + 12);
-                            const float d0 = __ldg(r + 3 * ca), d1 = __ldg(r + 3 * ca + 1), d2 = __ldg(r + 3 * ca + 2);
-                            const float e0 = __ldg(r + 3 * cb), e1 = __ldg(r + 3 * cb + 1), e2 = __ldg(r + 3 * cb + 2);
-                            const float da[3] = {d0, d1, d2}, db[3] = {e0, e1, e2};
+                            const float4* r = reinterpret_cast<const float4*>(erec + (size_t)elem * CS_EDGE_REC);
+                            const float4 qa = __ldg(r + ca), qb = __ldg(r + cb);
+                            const float coef = qa.w;
+                            const float da[3] = {qa.x, qa.y, qa.z}, db[3] = {qb.x, qb.y, qb.z};
 #pragma unroll
                             for (int kk = 0; kk < 3; kk++)
 #pragma unroll
@@ -460,12 +464,19 @@ __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
                             if (edge != (pass == 2)) continue;
                             const int elem = (int)((code >> 4) & 0x7FFFFFFu);
                             const int ca = (code >> 2) & 3;
-                            const float* r = pass == 0 ? frec + (size_t)elem * CS_FACE_REC + 90
-                                           : pass == 1 ? frec + (size_t)elem * CS_FACE_REC + 81 + 3 * ca
-                                                       : erec + (size_t)elem * CS_EDGE_REC + 16 + 3 * ca;
-                            w[j][0] = __ldg(r);
-                            w[j][1] = __ldg(r + 1);
-                            w[j][2] = __ldg(r + 2);
+                            if (pass == 0) {
+                                const float* r = frec + (size_t)elem * CS_FACE_REC;
+                                w[j][0] = __ldg(r + 111);
+                                w[j][1] = __ldg(r + 115);
+                                w[j][2] = __ldg(r + 119);
+                            } else {
+                                const float4 q = __ldg(reinterpret_cast<const float4*>(
+                                    pass == 1 ? frec + (size_t)elem * CS_FACE_REC + 108 + 4 * ca
+                                              : erec + (size_t)elem * CS_EDGE_REC + 16 + 4 * ca));
+                                w[j][0] = q.x;
+                                w[j][1] = q.y;
+                                w[j][2] = q.z;
+                            }
                             use[j] = true;
                         }
 #pragma unroll
@@ -509,11 +520,13 @@ __global__ void __launch_bounds__(128) cs_expand_kernel(Batch B, float* face_f, 
     if (i < B.F) face_eval(B, i, nullptr, face_f + 9 * (size_t)i, face_J + 81 * (size_t)i);
     if (i < B.E) {
         const float* r = B.edge_rec + (size_t)i * CS_EDGE_REC;
-        const float coef = r[12], angle = r[13];
+        const float coef = r[3], angle = r[19];
         const float ca = coef * angle;
+        float d[12];
+        for (int p = 0; p < 12; p++) d[p] = r[4 * (p / 3) + p % 3];
         for (int p = 0; p < 12; p++) {
-            edge_f[12 * (size_t)i + p] = ca * r[p];
-            for (int q = 0; q < 12; q++) edge_J[144 * (size_t)i + 12 * p + q] = coef * (r[p] * r[q]);
+            edge_f[12 * (size_t)i + p] = ca * d[p];
+            for (int q = 0; q < 12; q++) edge_J[144 * (size_t)i + 12 * p + q] = coef * (d[p] * d[q]);
         }
     }
 }
