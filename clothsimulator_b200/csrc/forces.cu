@@ -440,10 +440,12 @@ __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
                     }
                 }
             }
+            // streaming stores: A is read back from DRAM by the solvers, while the element
+            // records this kernel re-reads should keep their place in L2
             float* panel = B.A + (size_t)(sd.panel0 + k) * CS_PANEL_FLOATS;
-            reinterpret_cast<float4*>(panel)[lane] = make_float4(a[0], a[1], a[2], a[3]);
-            reinterpret_cast<float4*>(panel + 128)[lane] = make_float4(a[4], a[5], a[6], a[7]);
-            panel[256 + lane] = a[8];
+            __stcs(reinterpret_cast<float4*>(panel) + lane, make_float4(a[0], a[1], a[2], a[3]));
+            __stcs(reinterpret_cast<float4*>(panel + 128) + lane, make_float4(a[4], a[5], a[6], a[7]));
+            __stcs(panel + 256 + lane, a[8]);
 
             if (k == 0 && live) {
                 // Right-hand side in the reference's order: gravity, wind (faces), stretching
