@@ -395,6 +395,9 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
         double gam = 0.0, gam_prev = 0.0, rr = 0.0, delta = 0.0, alpha_d = 0.0, res0 = bn, resnorm = -1.0,
                first_res = -1.0;
         bool cont = false;  // the next PH_INIT keeps the search direction (reliable update)
+        // 1 / gam and 1 / (gam alpha), computed when gam and alpha are set, so that the next
+        // iteration's step length costs one division after the reduction instead of three
+        double inv_gam = 0.0, inv_ga = 0.0;
         float alpha = 0.f, beta = 0.f;
         int iters = 0, sweeps = 0, sweep_iters = 0, flags = 0, trips = 0;
         int phase = P.warm ? PH_RES : PH_INIT;
@@ -648,6 +651,8 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                         beta = bc;
                         alpha_d = gnew / v2[0];
                         alpha = (float)alpha_d;
+                        inv_gam = 1.0 / gam;
+                        inv_ga = 1.0 / (gam * alpha_d);
                         phase = PH_CG;
                         continue;
                     }
@@ -666,6 +671,8 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                 if (mixed) {
                     alpha_d = gam / delta;
                     alpha = (float)alpha_d;
+                    inv_gam = 1.0 / gam;
+                    inv_ga = 1.0 / (gam * alpha_d);
                 } else {
                     alpha = (float)gam / (float)delta;
                     alpha_d = (double)alpha;
@@ -686,17 +693,21 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
             // PH_CG: the iteration's x and r updates are done; stopping test on ||r||
             iters += 1;
             sweep_iters += 1;
-            const double rn = sqrt(rr);
+            // ||r|| against the thresholds, squared (no square root on the critical path)
             bool stop;
-            if (mixed)
-                stop = rn <= P.inner_tol * res0 || rn <= 0.5 * P.tol * bn || sweep_iters >= P.sweep_cap;
-            else
-                stop = rn <= P.tol * bn;
+            if (mixed) {
+                const double ti = P.inner_tol * res0, tt = 0.5 * P.tol * bn;
+                stop = rr <= ti * ti || rr <= tt * tt || sweep_iters >= P.sweep_cap;
+            } else {
+                const double tt = P.tol * bn;
+                stop = rr <= tt * tt;
+            }
             float nb, na;
             double na_d;
             if (mixed) {
-                const double bd = gnew / gam;
-                na_d = gnew / (dnew - bd * gnew / alpha_d);
+                // beta = gnew / gam; alpha = gnew / (dnew - beta gnew / alpha_prev)
+                const double bd = gnew * inv_gam;
+                na_d = gnew / (dnew - gnew * gnew * inv_ga);
                 nb = (float)bd;
                 na = (float)na_d;
             } else {
@@ -722,6 +733,10 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
             for (int c = 0; c < 3; c++) {
                 p[c] = __fmaf_rn(beta, p[c], u[c]);
                 sv3[c] = __fmaf_rn(beta, sv3[c], wv[c]);
+            }
+            if (mixed) {
+                inv_gam = 1.0 / gam;
+                inv_ga = 1.0 / (gam * alpha_d);
             }
         }
         if (!ok) {
