@@ -89,7 +89,13 @@ enum InstPhase : int {
 // Reliable updates keep the search direction only while the recursive residual has drifted
 // from the FP64 one by at most this fraction of the latter (larger drift: restart).
 #define CS_RELIABLE_DRIFT 0.1
-#define CS_CHEB_POWER_ITERS 10  // power iterations per sheet solve for the strip-local Chebyshev bound
+#define CS_CHEB_POWER_ITERS 10
+// A sheet uses the strip-local Chebyshev preconditioner only if at least this share of its
+// blocks couple rows of one strip.  Small sheets split into thin strips do better with
+// block-Jacobi; measured on the B200 (hanging and windy sheets, tol 1e-6): 24x24 (0.54 of the
+// blocks strip-local) and 28x28 (0.59) need fewer or as many iterations with block-Jacobi, 32x32
+// (0.71), 40x40 (0.65), 48x48 (0.84) and 64x64 (0.89) fewer with the Chebyshev polynomial.
+#define CS_CHEB_MIN_LOCAL 0.62  // power iterations per sheet solve for the strip-local Chebyshev bound
 #define CS_SOLVER_AUTO_DEV 0
 #define CS_SOLVER_BATCHED_DEV 1
 
@@ -200,6 +206,7 @@ struct Batch {
     int* rsendptr = nullptr;     // per topology: CS_RES_MAX_CL + 1 offsets into rsend per owner rank
     uint32_t* rsend = nullptr;   // halo sends: src slot | dst rank << 12 | dst halo index << 16
     int* rhalo = nullptr;        // per topology: CS_RES_MAX_CL + 1 halo slot counts per rank
+    int* rcheb = nullptr;        // per topology and rank: 1 if the strip uses the Chebyshev preconditioner when asked
     int res_halo0 = 0;           // first halo slot of every CTA's p array (= own slots per CTA)
     int res_alt = 0;             // first slot of the second own-row buffer (strip-local Chebyshev)
     // per-topology block CSR (local ids, columns ascending) with the SELL slot of each block

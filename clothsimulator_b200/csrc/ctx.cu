@@ -1064,6 +1064,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     std::vector<int> hrsplit(topos.size() * (CS_RES_MAX_CL + 1), 0), hrcode;
     std::vector<int> hrsendptr(topos.size() * (CS_RES_MAX_CL + 1), 0);
     std::vector<int> hrhalo(topos.size() * (CS_RES_MAX_CL + 1), 0);
+    // sheets whose strips keep enough of the couplings use the strip-local Chebyshev
+    // preconditioner (when asked for); the others stay with block-Jacobi
+    std::vector<int> hrcheb(topos.size() * (CS_RES_MAX_CL + 1), 0);
     std::vector<uint32_t> hrsend;
     std::vector<char>& topoResident = res.resident;
     std::vector<ResidentPlan>& plans = res.plans;
@@ -1072,6 +1075,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         if (topoResident[t]) {
             std::copy(plans[t].split.begin(), plans[t].split.end(), hrsplit.begin() + t * (CS_RES_MAX_CL + 1));
             std::copy(plans[t].halo_count.begin(), plans[t].halo_count.end(), hrhalo.begin() + t * (CS_RES_MAX_CL + 1));
+            const bool cheb = plans[t].blocks > 0 &&
+                              (double)plans[t].local_blocks >= CS_CHEB_MIN_LOCAL * (double)plans[t].blocks;
+            for (int r = 0; r <= CS_RES_MAX_CL; r++) hrcheb[t * (CS_RES_MAX_CL + 1) + r] = cheb;
         }
     c->resCL = c->resThreads = c->resClusters = 0;
     c->resSmem = 0;
@@ -1285,6 +1291,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     UP(rsendptr, hrsendptr);
     UP(rsend, hrsend);
     UP(rhalo, hrhalo);
+    UP(rcheb, hrcheb);
 #undef UP
 #define AL(field, n) \
     if ((st = dalloc(c, &B.field, (size_t)(n))) != CS_OK) return st;

@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
         // then the coefficients of the Chebyshev iteration on [lmax / 30, lmax].  An odd
         // degree keeps the polynomial positive on all of (0, inf), so the preconditioner is
         // SPD whatever the estimate.
-        if (P.cheb_degree >= 3) {
+        if (P.cheb_degree >= 3 && B.rcheb[tb + rank]) {
             float v[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {

@@ -222,3 +222,35 @@ def test_chebyshev_degree_validation(ctx_factory):
     for bad in (-1, 2, 4, 17):
         st = ctx.lib.cs_step(ctx.h, native.ctypes.byref(params_for(scene, precond_degree=bad)), None)
         assert st == native.CS_ERR_INVALID_ARG, bad
+
+
+def test_resident_blocks_accounting(ctx_factory):
+    """cs_get_resident_blocks: the resident sheets' pattern blocks (the system's, with no
+    proximities), the strip-local ones among them, and the power iterations per solve."""
+    scene = scenes.windy_batch(3, 32, seed=93)
+    scene.sheets += scenes.windy_batch(1, 64, seed=94).sheets
+    ctx = ctx_factory(scene.sheets)
+    rb = ctx.resident_blocks()
+    assert ctx.solver_info()["resident_sheets"] == 4
+    assert rb["blocks"] == ctx.sizes[6]
+    # most blocks couple rows of the same strip; the strips' borders couple the rest
+    assert 0.5 * rb["blocks"] < rb["local_blocks"] < rb["blocks"]
+    assert rb["power_iters"] == 10
+
+
+def test_chebyshev_falls_back_on_thin_strips(ctx_factory):
+    """Sheets split into strips that keep less than 0.62 of their blocks (16x16 sheets over a
+    cluster) solve with block-Jacobi even when the Chebyshev preconditioner is asked for: the
+    same iterations and the same dv bits as precond_degree 1."""
+    scene = scenes.windy_batch(3, 16, seed=95)
+    ctx = ctx_factory(scene.sheets)
+    rb = ctx.resident_blocks()
+    assert rb["local_blocks"] < 0.62 * rb["blocks"]
+    x0, v0 = initial_state(scene)
+    res = []
+    for deg in (1, 3):
+        ctx.set_state(x0, v0)
+        stats, _ = ctx.step(params_for(scene, precond_degree=deg))
+        assert stats.converged == 3
+        res.append((ctx.get_dv().copy(), ctx.instance_stats()[0].copy()))
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
