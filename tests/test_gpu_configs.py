@@ -96,14 +96,17 @@ def write_report():
             json.dump(REPORT, f, indent=1)
 
 
-def check_subset(name, scene, ctx, subset, tols=(1e-6, 1e-10)):
+def check_subset(name, scene, ctx, subset, tols=(1e-6, 1e-10), degrees=(1,)):
+    """degrees: the cluster-resident solver's preconditioner (1 block-Jacobi, 3 the strip-local
+    Chebyshev polynomial the bench uses); the bounds are the same for each."""
     oracle = {k: oracle_dv(scene, scene.sheets[k]) for k in subset}
-    for tol in tols:
-        res, stats = gpu_step(ctx, scene, tol=tol, precision=native.PREC_MIXED)
-        assert stats.converged == len(scene.sheets) and stats.max_rel_residual <= tol
-        errs = [sheet_errors(scene, scene.sheets[k], res[k][0], res[k][1], oracle[k]) for k in subset]
-        record(name, f"mixed_tol{tol:g}", errs)
-        assert max(e[0] for e in errs) < (1e-6 if tol <= 1e-10 else 1e-2)
+    for deg in degrees:
+        for tol in tols:
+            res, stats = gpu_step(ctx, scene, tol=tol, precision=native.PREC_MIXED, precond_degree=deg)
+            assert stats.converged == len(scene.sheets) and stats.max_rel_residual <= tol
+            errs = [sheet_errors(scene, scene.sheets[k], res[k][0], res[k][1], oracle[k]) for k in subset]
+            record(name, f"mixed_tol{tol:g}" + ("" if deg == 1 else f"_chebyshev{deg}"), errs)
+            assert max(e[0] for e in errs) < (1e-6 if tol <= 1e-10 else 1e-2)
 
 
 def test_config1_hang32(ctx_factory):
@@ -133,14 +136,14 @@ def test_config3_uneven512(ctx_factory):
     scene = scenes.uneven_batch(512, seed=0)
     rng = np.random.default_rng(3)
     subset = sorted(rng.choice(len(scene.sheets), 12, replace=False).tolist())
-    check_subset("config3_uneven512", scene, ctx_factory(scene.sheets), subset)
+    check_subset("config3_uneven512", scene, ctx_factory(scene.sheets), subset, degrees=(1, 3))
 
 
 def test_config4_windy1024(ctx_factory):
     scene = scenes.windy_batch(1024, 64, seed=1000)
     rng = np.random.default_rng(4)
     subset = sorted(rng.choice(len(scene.sheets), 8, replace=False).tolist())
-    check_subset("config4_windy1024x64", scene, ctx_factory(scene.sheets), subset)
+    check_subset("config4_windy1024x64", scene, ctx_factory(scene.sheets), subset, degrees=(1, 3))
 
 
 def test_config5_irregular(ctx_factory):
