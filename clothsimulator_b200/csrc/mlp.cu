@@ -316,14 +316,20 @@ __global__ void __launch_bounds__(128) cs_mlp_l23_kernel(Batch B, MlpDev M, int 
             const uint4* hi = reinterpret_cast<const uint4*>(M.h1 + 64 * (size_t)node);
             Nbr nb = neighbours(B, node);
             const float inv = nb.end > nb.beg ? 1.0f / (nb.end - nb.beg) : 0.f;
+            // the first kNbr neighbours' rows, looked up once for the four quarters of the row;
+            // their loads are issued kBatch at a time before the (ordered) additions
+            constexpr int kNbr = 8, kBatch = 4;
+            const int cnt = nb.end - nb.beg;
+            const uint4* nrow[kNbr];
+#pragma unroll
+            for (int j = 0; j < kNbr; j++)
+                nrow[j] = reinterpret_cast<const uint4*>(M.h1 + 64 * (size_t)(j < cnt ? B.nbr[nb.beg + j] + nb.off : node));
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 float acc[16];
 #pragma unroll
                 for (int c = 0; c < 16; c++) acc[c] = 0.f;
-                for (int k = nb.beg; k < nb.end; k++) {
-                    const uint4* hj = reinterpret_cast<const uint4*>(M.h1 + 64 * (size_t)(B.nbr[k] + nb.off) + 16 * q);
-                    const uint4 v0 = __ldg(hj), v1 = __ldg(hj + 1);
+                auto add_row = [&](const uint4& v0, const uint4& v1) {
                     const __nv_bfloat16* e0 = reinterpret_cast<const __nv_bfloat16*>(&v0);
                     const __nv_bfloat16* e1 = reinterpret_cast<const __nv_bfloat16*>(&v1);
 #pragma unroll
@@ -331,6 +337,23 @@ __global__ void __launch_bounds__(128) cs_mlp_l23_kernel(Batch B, MlpDev M, int 
                         acc[c] += __bfloat162float(e0[c]);
                         acc[8 + c] += __bfloat162float(e1[c]);
                     }
+                };
+#pragma unroll
+                for (int j0 = 0; j0 < kNbr; j0 += kBatch) {
+                    uint4 v0[kBatch], v1[kBatch];
+#pragma unroll
+                    for (int j = 0; j < kBatch; j++)
+                        if (j0 + j < cnt) {
+                            v0[j] = __ldg(nrow[j0 + j] + 2 * q);
+                            v1[j] = __ldg(nrow[j0 + j] + 2 * q + 1);
+                        }
+#pragma unroll
+                    for (int j = 0; j < kBatch; j++)
+                        if (j0 + j < cnt) add_row(v0[j], v1[j]);
+                }
+                for (int k = nb.beg + kNbr; k < nb.end; k++) {
+                    const uint4* hj = reinterpret_cast<const uint4*>(M.h1 + 64 * (size_t)(B.nbr[k] + nb.off) + 16 * q);
+                    add_row(__ldg(hj), __ldg(hj + 1));
                 }
                 *reinterpret_cast<uint4*>(sA + tc::kmajor_offset(128, t, 16 * q)) = __ldg(hi + 2 * q);
                 *reinterpret_cast<uint4*>(sA + tc::kmajor_offset(128, t, 16 * q + 8)) = __ldg(hi + 2 * q + 1);
