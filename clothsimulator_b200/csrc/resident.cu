@@ -2,17 +2,21 @@
 // held in the cluster's distributed shared memory for the whole solve.
 //
 // The batched loop of pcg.cu streams every sheet's matrix from HBM once per CG iteration
-// (about 1.7 MB per 64x64 sheet, ~330 iterations per step).  A sheet of that size fits in
-// the shared memory of an 8-CTA cluster (8 x 227 KB), so here each cluster
+// (about 1.7 MB per 64x64 sheet, ~300 iterations per step).  A sheet of that size fits in
+// the shared memory of a cluster of 8 to 10 CTAs (227 KB each), so here each cluster
 //   * takes the next sheet from a device work counter (persistent clusters; a sheet that
 //     converges early frees its cluster at once, there is no batch-wide tail),
 //   * copies its share of the sheet's SELL-32 panels (a contiguous strip of slices) into
 //     shared memory once per solve,
 //   * runs the per-instance state machine of the batched loop (FP32 CG on the correction
-//     system, FP64 dot products and norms, FP64 outer residual b - A dv64, warm-start
-//     guard, inner and outer stopping tests) with the FP32 vectors in registers, one thread
-//     per row.  The CG recurrence is the Chronopoulos-Gear form: per iteration one SpMV
-//     w = A u and ONE fused reduction of (r.u, w.u, r.r), instead of two reductions;
+//     system, FP64 dot products and norms, FP64 residual replacements with the search
+//     direction kept (reliable updates), warm-start guard, inner and outer stopping tests)
+//     with the FP32 vectors in registers, one thread per row.  The CG recurrence is the
+//     Chronopoulos-Gear form: per iteration one SpMV w = A u and ONE fused reduction of
+//     (r.u, w.u, r.r), instead of two reductions;
+//   * preconditions with the 3x3 block-Jacobi inverse or, when asked and the sheet's strips
+//     keep enough of its couplings, with a Chebyshev polynomial in the block-Jacobi-scaled
+//     strip of rows each CTA holds (its SpMVs read only the CTA's own shared memory);
 //   * exchanges data without cluster barriers: after u = P^-1 r each CTA pushes the values
 //     of its strip's boundary rows into the halo slots of the CTAs that read them with
 //     st.async remote stores, which complete bytes on the receiver's mbarrier; reduction
@@ -29,8 +33,8 @@
 // Rows of a slice beyond the shared-memory panel budget are read from global memory.
 //
 // Replaces the reference's per-cloth GPU solve (Cloth.cu:766-809) like pcg.cu does; the
-// preconditioner is the 3x3 block inverse from the gather kernel (the reference builds the
-// scalar Jacobi one, PhysicsHelper.cu:479-485).
+// block-Jacobi preconditioner is the 3x3 block inverse from the gather kernel (the reference
+// builds the scalar Jacobi one, PhysicsHelper.cu:479-485).
 #include <cooperative_groups.h>
 
 #include "cs_internal.h"
