@@ -8,7 +8,8 @@
 //                            (CollisionHelper.cu:61-136: the cubic for coplanarity along the
 //                            linear trajectories, solveCubic / solveQuadratic /
 //                            newtonsMethod :3-59, the distance and side at the root);
-//   cs_impact_sort_kernel    rank sort by impact time (ties by node ids);
+//   cs_impact_keys/gather_kernel  keys of the stable radix sorts by impact time (ties by node
+//                            ids, type, index; the sorts are CUB's, in ctx.cu), then the gather;
 //   cs_select_*_kernel       the independent impacts, earliest first, one per node
 //                            (Simulator.cu:394-420), by rounds of per-node minima;
 //   cs_opt_*_kernel          the impact zone's nodes (ascending), each impact's node slots,
@@ -267,41 +268,29 @@ __global__ void __launch_bounds__(256) cs_impact_ee_kernel(Batch B, Contact C, C
 
 // Rank sort of the round's impacts by (time, node ids, type): each thread ranks one impact
 // against all others, the keys staged through shared memory in tiles.
-__global__ void __launch_bounds__(256) cs_impact_sort_kernel(Collide K, int n) {
-    struct Key {
-        float t;
-        int n0, n1, n2, n3, type;
-    };
-    __shared__ Key tile[256];
+// Order of the found impacts: by time, then node ids, then type, then index (std::sort in
+// Simulator::independentImpacts orders by time; the rest makes the order total).  A least-
+// significant-first sequence of stable radix sorts (CUB, in ctx.cu) over the key parts: type,
+// (n2, n3), n1, (t, n0).  t >= 0, so its IEEE bits order like its values; node ids are >= 0.
+// pass 0 also starts the permutation at the identity.
+__global__ void cs_impact_keys_kernel(Collide K, int n, int pass, const int* __restrict__ perm,
+                                      unsigned long long* __restrict__ key, int* __restrict__ perm_out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    ImpactRec a;
-    if (i < n) a = K.found[i];
-    int rank = 0;
-    for (int j0 = 0; j0 < n; j0 += 256) {
-        const int j = j0 + threadIdx.x;
-        if (j < n) {
-            const ImpactRec& r = K.found[j];
-            tile[threadIdx.x] = Key{r.t, r.nodes[0], r.nodes[1], r.nodes[2], r.nodes[3], r.type};
-        }
-        __syncthreads();
-        if (i < n) {
-            const int m = min(256, n - j0);
-            for (int k = 0; k < m; k++) {
-                const Key& q = tile[k];
-                bool lt;  // q before a
-                if (q.t != a.t) lt = q.t < a.t;
-                else if (q.n0 != a.nodes[0]) lt = q.n0 < a.nodes[0];
-                else if (q.n1 != a.nodes[1]) lt = q.n1 < a.nodes[1];
-                else if (q.n2 != a.nodes[2]) lt = q.n2 < a.nodes[2];
-                else if (q.n3 != a.nodes[3]) lt = q.n3 < a.nodes[3];
-                else if (q.type != a.type) lt = q.type < a.type;
-                else lt = j0 + k < i;  // equal keys: by index
-                rank += lt ? 1 : 0;
-            }
-        }
-        __syncthreads();
-    }
-    if (i < n) K.sorted[rank] = a;
+    if (i >= n) return;
+    const int src = pass == 0 ? i : perm[i];
+    if (pass == 0) perm_out[i] = i;
+    const ImpactRec& r = K.found[src];
+    unsigned long long k;
+    if (pass == 0) k = (unsigned long long)(unsigned)r.type;
+    else if (pass == 1) k = ((unsigned long long)(unsigned)r.nodes[2] << 32) | (unsigned)r.nodes[3];
+    else if (pass == 2) k = (unsigned long long)(unsigned)r.nodes[1];
+    else k = ((unsigned long long)__float_as_uint(r.t) << 32) | (unsigned)r.nodes[0];
+    key[i] = k;
+}
+
+__global__ void cs_impact_gather_kernel(Collide K, int n, const int* __restrict__ perm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) K.sorted[i] = K.found[perm[i]];
 }
 
 // independentImpacts (Simulator.cu:394-420) in parallel: the earliest-first greedy choice of

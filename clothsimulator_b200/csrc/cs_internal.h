@@ -270,6 +270,11 @@ struct Collide {
     int found_cap = 0;
     int* counters = nullptr;      // [0] impacts found, [1] impacts selected
     ImpactRec* sorted = nullptr;  // by time (then node ids)
+    // radix sort of the found impacts: key and permutation double buffers, CUB temp storage
+    unsigned long long *skey[2] = {nullptr, nullptr};
+    int* sperm[2] = {nullptr, nullptr};
+    void* stmp = nullptr;
+    size_t stmp_bytes = 0;
     ImpactRec* all = nullptr;     // independent impacts accumulated this deformation level
     int* used = nullptr;          // per node: taken by a selected impact of this round
     int* nodemin = nullptr;       // per node: lowest live impact index touching it (selection)

@@ -25,6 +25,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "../../include/clothstep.h"
 #include "cs_internal.h"
 #include "mlp.h"
@@ -65,7 +67,9 @@ __global__ void cs_contact_pair_kernel(Batch B, Contact C, const int* sheet_grou
 __global__ void cs_contact_vf_kernel(Batch B, Contact C, int npairs);
 __global__ void cs_impact_vf_kernel(Batch B, Contact C, Collide K, int npairs);
 __global__ void cs_impact_ee_kernel(Batch B, Contact C, Collide K, int npairs);
-__global__ void cs_impact_sort_kernel(Collide K, int n);
+__global__ void cs_impact_keys_kernel(Collide K, int n, int pass, const int* perm, unsigned long long* key,
+                                      int* perm_out);
+__global__ void cs_impact_gather_kernel(Collide K, int n, const int* perm);
 __global__ void cs_select_init_kernel(Collide K, int n);
 __global__ void cs_select_reset_kernel(Collide K, int n);
 __global__ void cs_select_min_kernel(Collide K, int n);
@@ -714,7 +718,7 @@ void freeBatch(cs_ctx* c) {
         Collide& K = c->coll;
         void* ps[] = {K.found, K.counters, K.sorted, K.all, K.used, K.nodemin, K.alive, K.chosen, K.mark, K.nodes,
                       K.idx, K.nptr, K.nfill, K.nlist, K.x1, K.cur, K.next, K.grad, K.lambda, K.coef,
-                      K.cterm, K.nterm, K.gterm};
+                      K.cterm, K.nterm, K.gterm, K.skey[0], K.skey[1], K.sperm[0], K.sperm[1], K.stmp};
         for (void* q : ps)
             if (q) cudaFree(q);
         c->coll = Collide();
@@ -1708,12 +1712,31 @@ cs_status collideScratch(cs_ctx* c, int nFound, int nAll) {
         if (K.sorted) cudaFree(K.sorted);
         K.sorted = nullptr;
         if ((st = grow(c, K.sorted, cap, P.found)) != CS_OK) return st;
-        for (int** q : {&K.alive, &K.chosen}) {
+        for (int** q : {&K.alive, &K.chosen, &K.sperm[0], &K.sperm[1]}) {
             if (*q) cudaFree(*q);
             *q = nullptr;
             cap = 0;
             if ((st = grow(c, *q, cap, P.found + 1)) != CS_OK) return st;
         }
+        for (unsigned long long** q : {&K.skey[0], &K.skey[1]}) {
+            if (*q) cudaFree(*q);
+            *q = nullptr;
+            cap = 0;
+            if ((st = grow(c, *q, cap, P.found)) != CS_OK) return st;
+        }
+        // temp storage of the radix sorts (impactSort), for the largest key width
+        size_t bytes = 0;
+        for (int bits : {1, 32, 64}) {
+            size_t b = 0;
+            CS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, K.skey[0], K.skey[1], K.sperm[0], K.sperm[1],
+                                                    (int)std::min<size_t>(P.found, INT32_MAX), 0, bits, c->stream));
+            bytes = std::max(bytes, b);
+        }
+        if (K.stmp) cudaFree(K.stmp);
+        K.stmp = nullptr;
+        K.stmp_bytes = 0;
+        CS_CUDA(cudaMalloc(&K.stmp, std::max<size_t>(bytes, 16)));
+        K.stmp_bytes = std::max<size_t>(bytes, 16);
         K.found_cap = (int)std::min<size_t>(P.found, INT32_MAX);
     }
     if ((size_t)nAll > P.all) {
@@ -1847,7 +1870,18 @@ cs_status cs_collision_step(cs_ctx* c, const cs_collision_params* p, cs_collisio
             }
             if (nFound > K.found_cap) return fail(c, CS_ERR_STATE, "impact buffer overflow");
             if ((st = collideScratch(c, nFound, nAll + nFound)) != CS_OK) return st;
-            cs_impact_sort_kernel<<<nblk(nFound, 256), 256, 0, c->stream>>>(K, nFound);
+            // the round's impacts in order (time, node ids, type, index): four stable radix
+            // sorts over the key parts, least significant first, then one gather
+            int pin = 0;
+            for (int pass = 0; pass < 4; pass++) {
+                cs_impact_keys_kernel<<<nblk(nFound, 256), 256, 0, c->stream>>>(K, nFound, pass, K.sperm[pin], K.skey[0],
+                                                                               K.sperm[pin]);
+                size_t bytes = K.stmp_bytes;
+                CS_CUDA(cub::DeviceRadixSort::SortPairs(K.stmp, bytes, K.skey[0], K.skey[1], K.sperm[pin], K.sperm[pin ^ 1],
+                                                        nFound, 0, pass == 0 ? 1 : pass == 2 ? 32 : 64, c->stream));
+                pin ^= 1;
+            }
+            cs_impact_gather_kernel<<<nblk(nFound, 256), 256, 0, c->stream>>>(K, nFound, K.sperm[pin]);
             // independent impacts: rounds of per-node minima until no impact is live
             const int g = nblk(nFound, 256);
             cs_select_init_kernel<<<nblk(nFound + 1, 256), 256, 0, c->stream>>>(K, nFound);
