@@ -574,7 +574,8 @@ def run_detect(args):
         scene, groups = sc.folded_sheet(256, seed=1), None
     ctx = native.Context(0).load(scene.sheets)
     p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol, max_iters=20000,
-                           precision=native.PREC_MIXED, warm_start=native.WARM_PREVIOUS)
+                           precision=native.PREC_MIXED, warm_start=native.WARM_PREVIOUS,
+                           precond_degree=args.precond_degree)
     det, both, col, full, counts, impacts = [], [], [], [], [], []
     thickness = float(np.float32(0.1) * np.float32(1e-3))  # Magic::collisionThickness default
     for i in range(args.warmup + args.steps):

@@ -3,8 +3,9 @@
 //
 // Each round: candidate face pairs from the contact grid over the start-of-step and current
 // positions (contact.cu with ccd bounds, dilated by the collision thickness), then
-//   cs_impact_vf/ee_kernel   thread per (pair, test): the bounds check and continuous
-//                            impact test of checkVertexFaceImpact / checkEdgeEdgeImpact
+//   cs_impact_kernel         per (pair, test) the shared-node and swept-box filters, the
+//                            survivors compacted per block, then the continuous impact test
+//                            of checkVertexFaceImpact / checkEdgeEdgeImpact
 //                            (CollisionHelper.cu:61-136: the cubic for coplanarity along the
 //                            linear trajectories, solveCubic / solveQuadratic /
 //                            newtonsMethod :3-59, the distance and side at the root);
@@ -213,7 +214,9 @@ __device__ bool overlap(const float alo[3], const float ahi[3], const float blo[
     return true;
 }
 
-__device__ void impact_test(const Batch& B, const Collide& K, int type, const int nodes[4]) {
+// The swept-box filter of checkVertexFaceImpact / checkEdgeEdgeImpact (type 0: vertex-face,
+// 1: edge-edge): false where the bounds of the two elements over the step stay apart.
+__device__ bool impact_boxes_meet(const Batch& B, const Collide& K, int type, const int nodes[4]) {
     float alo[3], ahi[3], blo[3], bhi[3];
     if (type == 0) {
         ccd_box(B, nodes, 1, alo, ahi);
@@ -222,7 +225,11 @@ __device__ void impact_test(const Batch& B, const Collide& K, int type, const in
         ccd_box(B, nodes, 2, alo, ahi);
         ccd_box(B, nodes + 2, 2, blo, bhi);
     }
-    if (!overlap(alo, ahi, blo, bhi, K.thickness)) return;
+    return overlap(alo, ahi, blo, bhi, K.thickness);
+}
+
+// The continuous test of one element pair that passed the filters; an impact is appended.
+__device__ void impact_test(const Batch& B, const Collide& K, int type, const int nodes[4]) {
     f3 p[4], q[4];
     for (int k = 0; k < 4; k++) {
         p[k] = ld(B.x0, nodes[k]);
@@ -235,39 +242,72 @@ __device__ void impact_test(const Batch& B, const Collide& K, int type, const in
     if (slot < K.found_cap) K.found[slot] = r;
 }
 
+// The nodes of test k (0-5 vertex-face, 6-14 edge-edge) of candidate pair pr, or false where
+// the two elements share a node (checkImpacts skips those, Simulator.cu:369-381).
+__device__ bool impact_nodes(const Batch& B, const Contact& C, int2 pr, int k, int& type, int nodes[4]) {
+    if (k < 6) {
+        // vertex-face: corner k % 3 of one face against the other face
+        const int f = k < 3 ? pr.x : pr.y, g = k < 3 ? pr.y : pr.x;
+        const int4 y = B.face_nodes[f], z = B.face_nodes[g];
+        const int i = k % 3;
+        const int node = i == 0 ? y.x : i == 1 ? y.y : y.z;
+        if (node == z.x || node == z.y || node == z.z) return false;
+        type = 0;
+        nodes[0] = node;
+        nodes[1] = z.x;
+        nodes[2] = z.y;
+        nodes[3] = z.z;
+        return true;
+    }
+    // edge-edge: edge i of the first face against edge j of the second
+    const int4 fe = C.face_edges[pr.x], ge = C.face_edges[pr.y];
+    const int i = (k - 6) / 3, j = (k - 6) % 3;
+    const int4 a = C.edges[i == 0 ? fe.x : i == 1 ? fe.y : fe.z], b = C.edges[j == 0 ? ge.x : j == 1 ? ge.y : ge.z];
+    if (a.x == b.x || a.x == b.y || a.y == b.x || a.y == b.y) return false;
+    type = 1;
+    nodes[0] = a.x;
+    nodes[1] = a.y;
+    nodes[2] = b.x;
+    nodes[3] = b.y;
+    return true;
+}
+
 }  // namespace
 
-// checkImpacts (Simulator.cu:369-381), vertex-face part: (pair, corner) per thread.
-__global__ void __launch_bounds__(256) cs_impact_vf_kernel(Batch B, Contact C, Collide K, int npairs) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 6LL * npairs) return;
-    const int p = (int)(t / 6), k = (int)(t % 6);
-    const int2 pr = C.pairs[p];
-    const int f = k < 3 ? pr.x : pr.y, g = k < 3 ? pr.y : pr.x;
-    const int4 y = B.face_nodes[f], z = B.face_nodes[g];
-    const int i = k % 3;
-    const int node = i == 0 ? y.x : i == 1 ? y.y : y.z;
-    if (node == z.x || node == z.y || node == z.z) return;
-    const int nodes[4] = {node, z.x, z.y, z.z};
-    impact_test(B, K, 0, nodes);
+// checkImpacts (Simulator.cu:369-381): per candidate pair its 6 vertex-face and 9 edge-edge
+// tests.  Each block takes kImpactItems consecutive (pair, test) items: first every thread
+// applies the cheap filters (shared nodes, swept boxes) to its items and queues the survivors
+// in shared memory, then the block's threads share out the queued continuous tests, so the
+// cubic solves run with full warps instead of beside threads that have nothing to do.  The
+// impacts' order in `found` does not matter: the round sorts them by a total order.
+constexpr int kImpactThreads = 256, kImpactPerThread = 8, kImpactItems = kImpactThreads * kImpactPerThread;
+__global__ void __launch_bounds__(kImpactThreads) cs_impact_kernel(Batch B, Contact C, Collide K, int npairs) {
+    __shared__ int4 qnodes[kImpactItems];
+    __shared__ unsigned char qtype[kImpactItems];
+    __shared__ int qcount;
+    if (threadIdx.x == 0) qcount = 0;
+    __syncthreads();
+    const long long total = 15LL * npairs, base = (long long)blockIdx.x * kImpactItems;
+    for (int j = 0; j < kImpactPerThread; j++) {
+        const long long item = base + j * kImpactThreads + threadIdx.x;
+        if (item >= total) break;
+        const int2 pr = C.pairs[(int)(item / 15)];
+        int type, nodes[4];
+        if (!impact_nodes(B, C, pr, (int)(item % 15), type, nodes)) continue;
+        if (!impact_boxes_meet(B, K, type, nodes)) continue;
+        const int slot = atomicAdd(&qcount, 1);
+        qnodes[slot] = make_int4(nodes[0], nodes[1], nodes[2], nodes[3]);
+        qtype[slot] = (unsigned char)type;
+    }
+    __syncthreads();
+    const int n = qcount;
+    for (int q = threadIdx.x; q < n; q += kImpactThreads) {
+        const int4 v = qnodes[q];
+        const int nodes[4] = {v.x, v.y, v.z, v.w};
+        impact_test(B, K, qtype[q], nodes);
+    }
 }
 
-// edge-edge part: (pair, edge of the first face, edge of the second) per thread.
-__global__ void __launch_bounds__(256) cs_impact_ee_kernel(Batch B, Contact C, Collide K, int npairs) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 9LL * npairs) return;
-    const int p = (int)(t / 9), k = (int)(t % 9);
-    const int2 pr = C.pairs[p];
-    const int4 fe = C.face_edges[pr.x], ge = C.face_edges[pr.y];
-    const int i = k / 3, j = k % 3;
-    const int4 a = C.edges[i == 0 ? fe.x : i == 1 ? fe.y : fe.z], b = C.edges[j == 0 ? ge.x : j == 1 ? ge.y : ge.z];
-    if (a.x == b.x || a.x == b.y || a.y == b.x || a.y == b.y) return;
-    const int nodes[4] = {a.x, a.y, b.x, b.y};
-    impact_test(B, K, 1, nodes);
-}
-
-// Rank sort of the round's impacts by (time, node ids, type): each thread ranks one impact
-// against all others, the keys staged through shared memory in tiles.
 // Order of the found impacts: by time, then node ids, then type, then index (std::sort in
 // Simulator::independentImpacts orders by time; the rest makes the order total).  A least-
 // significant-first sequence of stable radix sorts (CUB, in ctx.cu) over the key parts: type,

@@ -65,8 +65,7 @@ __global__ void cs_contact_node_kernel(Batch B, Contact C);
 __global__ void cs_contact_grid_kernel(Batch B, Contact C, const int* sheet_group);
 __global__ void cs_contact_pair_kernel(Batch B, Contact C, const int* sheet_group);
 __global__ void cs_contact_vf_kernel(Batch B, Contact C, int npairs);
-__global__ void cs_impact_vf_kernel(Batch B, Contact C, Collide K, int npairs);
-__global__ void cs_impact_ee_kernel(Batch B, Contact C, Collide K, int npairs);
+__global__ void cs_impact_kernel(Batch B, Contact C, Collide K, int npairs);
 __global__ void cs_impact_keys_kernel(Collide K, int n, int pass, const int* perm, unsigned long long* key,
                                       int* perm_out);
 __global__ void cs_impact_gather_kernel(Collide K, int n, const int* perm);
@@ -1857,8 +1856,8 @@ cs_status cs_collision_step(cs_ctx* c, const cs_collision_params* p, cs_collisio
                 if ((st = collideScratch(c, std::max(nFound, 1024), nAll + 1)) != CS_OK) return st;
                 CS_CUDA(cudaMemsetAsync(K.counters, 0, 2 * sizeof(int), c->stream));
                 if (npairs > 0) {
-                    cs_impact_vf_kernel<<<nblk(6LL * npairs, 256), 256, 0, c->stream>>>(B, C, K, npairs);
-                    cs_impact_ee_kernel<<<nblk(9LL * npairs, 256), 256, 0, c->stream>>>(B, C, K, npairs);
+                    // 256 threads, 2,048 (pair, test) items per block (collide.cu)
+                    cs_impact_kernel<<<nblk(15LL * npairs, 2048), 256, 0, c->stream>>>(B, C, K, npairs);
                 }
                 CS_CUDA(cudaMemcpyAsync(&nFound, K.counters, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
                 CS_CUDA(cudaStreamSynchronize(c->stream));
