@@ -311,8 +311,10 @@ __global__ void __launch_bounds__(kImpactThreads) cs_impact_kernel(Batch B, Cont
 // Order of the found impacts: by time, then node ids, then type, then index (std::sort in
 // Simulator::independentImpacts orders by time; the rest makes the order total).  A least-
 // significant-first sequence of stable radix sorts (CUB, in ctx.cu) over the key parts: type,
-// (n2, n3), n1, (t, n0).  t >= 0, so its IEEE bits order like its values; node ids are >= 0.
-// pass 0 also starts the permutation at the identity.
+// (n2, n3), n1, (t, n0).  t >= 0, so its IEEE bits order like its values once -0.0 (which the
+// impact tests accept: it is not below 0, and the quadratic's c / q yields it for a start that
+// is exactly coplanar) is taken as +0.0, as the oracle's comparison of times does; node ids
+// are >= 0.  pass 0 also starts the permutation at the identity.
 __global__ void cs_impact_keys_kernel(Collide K, int n, int pass, const int* __restrict__ perm,
                                       unsigned long long* __restrict__ key, int* __restrict__ perm_out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -324,7 +326,7 @@ __global__ void cs_impact_keys_kernel(Collide K, int n, int pass, const int* __r
     if (pass == 0) k = (unsigned long long)(unsigned)r.type;
     else if (pass == 1) k = ((unsigned long long)(unsigned)r.nodes[2] << 32) | (unsigned)r.nodes[3];
     else if (pass == 2) k = (unsigned long long)(unsigned)r.nodes[1];
-    else k = ((unsigned long long)__float_as_uint(r.t) << 32) | (unsigned)r.nodes[0];
+    else k = ((unsigned long long)(r.t == 0.0f ? 0u : __float_as_uint(r.t)) << 32) | (unsigned)r.nodes[0];
     key[i] = k;
 }
 

@@ -106,6 +106,9 @@ __global__ void __launch_bounds__(kThreads) noalloc_pcg_kernel(int n, int nnzb, 
     }
     __syncthreads();
     if (bad) {
+        // x becomes NaN, so that a caller of the asynchronous form (which gets no status from
+        // the device) cannot take stale contents of x for a solution
+        for (int i = t; i < 3 * n; i += kThreads) x[i] = __int_as_float(0x7fc00000);
         if (t == 0) {
             S.stats[0] = 0;
             S.stats[1] = -1.0;

@@ -331,8 +331,15 @@ cs_status cs_mlp_set_weights(cs_ctx* ctx, const float* in, int n);
  * row pointers or columns.  Every call on a device shares the one scratch array: calls that
  * overlap on the GPU race and must be serialised.  The first call on each device looks up the
  * array's address (cudaGetSymbolAddress) with that device current; make it before any stream
- * capture.  If iters or rel_residual (host pointers) are given, the call waits for the stream
- * and returns CS_OK or CS_ERR_NOT_CONVERGED; otherwise it returns after the launch. */
+ * capture.  Two forms:
+ *   - synchronous (iters or rel_residual, host pointers, given): the call waits for the stream
+ *     and returns CS_OK, CS_ERR_NOT_CONVERGED (the iteration cap was reached; x holds the last
+ *     iterate) or CS_ERR_INVALID_ARG (the device found a row pointer or column out of range;
+ *     x is then NaN);
+ *   - asynchronous (both NULL): the call returns after the launch, with CS_OK or an error of
+ *     the arguments or of the launch only.  The device's own checks and the convergence are
+ *     not reported to this form: a rejected system leaves NaN in x, and a caller that needs
+ *     the status uses the synchronous form. */
 #define CS_NOALLOC_MAX_ROWS 16384
 cs_status cs_solve_block_csr_noalloc(int n_rows, int nnzb, const int32_t* row_ptr, const int32_t* col,
                                      const float* val, const float* b, float* x, double tol, int max_iters,

@@ -23,7 +23,22 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_ORACLE = os.path.join(HERE, "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libclothref.so")
-REFERENCE_SRC = "/root/reference/src"
+# The reference checkout's src/ directory, from which the adapter library is compiled: given by
+# the CLOTHSIM_REFERENCE_SRC environment variable (the build entry point sets it where the
+# checkout exists).  Only needed to build _ref/libclothref.so or to make the golden fixtures.
+REFERENCE_ENV = "CLOTHSIM_REFERENCE_SRC"
+
+
+def reference_src(required: bool = True) -> str | None:
+    """The reference's src/ directory named by CLOTHSIM_REFERENCE_SRC.  Raises a clear error
+    when it is required and unset or missing; returns None otherwise."""
+    p = os.environ.get(REFERENCE_ENV, "")
+    if p and os.path.isdir(p):
+        return p
+    if required:
+        raise RuntimeError(f"{REFERENCE_ENV} must name the reference checkout's src/ directory "
+                           f"(got {p!r})")
+    return None
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -37,8 +52,9 @@ METHOD_PCG64 = 2    # FP64 block-Jacobi PCG to a relative residual
 def build(ref: bool = True) -> None:
     """Builds liboracle.so and, when the reference checkout is present, _ref/libclothref.so."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if ref and os.path.isdir(REFERENCE_SRC):
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REFSRC={REFERENCE_SRC}"], check=True)
+    src = reference_src(required=False) if ref else None
+    if src:
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REFSRC={src}"], check=True)
 
 
 def _d(a) -> np.ndarray:
@@ -136,10 +152,13 @@ class Material:
                                          spec.get("stretching_mult", 1.0), spec.get("bending_mult", 1.0))
         else:
             import json
-            wd = workdir or tempfile.mkdtemp(prefix="clothref_")
-            path = os.path.join(wd, "material_%d.json" % id(self))
-            with open(path, "w") as fh:
-                json.dump({k: spec[k] for k in ("density", "stretching", "bending")}, fh)
+            path = spec.get("data_file")
+            if not path:
+                # no data file of the reference's own: write the parameters as one
+                wd = workdir or tempfile.mkdtemp(prefix="clothref_")
+                path = os.path.join(wd, "material_%d.json" % id(self))
+                with open(path, "w") as fh:
+                    json.dump({k: spec[k] for k in ("density", "stretching", "bending")}, fh)
             text = json.dumps({"data": path, "thicken": spec.get("thicken", 1.0),
                                "density_mult": spec.get("density_mult", 1.0),
                                "stretching_mult": spec.get("stretching_mult", 1.0),

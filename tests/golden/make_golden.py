@@ -78,6 +78,61 @@ def make_case(seed, nq, amp):
     )
 
 
+REFERENCE_MATERIALS = ("gray-interlock", "11oz-black-denim", "paper")
+
+
+def read_material_file(path):
+    """Density, stretching rows and bending samples of a material data file in the reference's
+    format (materials/*.json; `//` comment lines allowed, as the reference's reader takes them)."""
+    import json
+
+    text = "\n".join(line for line in open(path).read().splitlines() if not line.lstrip().startswith("//"))
+    d = json.loads(text)
+    return {"density": float(d["density"]), "stretching": [[float(v) for v in r] for r in d["stretching"]],
+            "bending": [[float(v) for v in r] for r in d["bending"]]}
+
+
+def make_materials_case(materials_dir, nq=32, seed=51):
+    """A 32x32 sheet, top edge pinned, per-material wind, perturbed state, run through each of
+    three of the reference's own material files (Material.cu:3-41 reads the file itself here):
+    the reference's stretching lookups at seeded strains, and per material the right-hand side
+    b of the system assembled in the reference order (Cloth.cu:78-169, wind included), the
+    CPU-path step's dv (FP32 sparse LL^T) and the state after it."""
+    rng = np.random.default_rng(seed)
+    base = scenes.grid_sheet(nq, rng=rng, z_noise=1e-3)
+    out = {"names": np.array(REFERENCE_MATERIALS), "uv": base["uv"], "fx": base["fx"], "fu": base["fu"],
+           "handles": scenes.top_edge(nq)}
+    G = np.column_stack([rng.uniform(-0.3, 1.0, 400), rng.uniform(-0.6, 0.6, 400), rng.uniform(-0.3, 1.0, 400)])
+    out["G"] = G
+    for i, name in enumerate(REFERENCE_MATERIALS):
+        path = os.path.join(materials_dir, name + ".json")
+        mat = read_material_file(path)
+        mat.update({"thicken": 1.0, "density_mult": 1.0, "stretching_mult": 1.0, "bending_mult": 1.0})
+        s = {k: base[k] for k in ("uv", "fx", "fu")}
+        s["handles"] = out["handles"]
+        s["x"] = (base["x"] + rng.normal(0, 4e-3, base["x"].shape)).astype(np.float32)
+        s["v"] = rng.normal(0, 0.05, base["x"].shape).astype(np.float32)
+        phi = rng.uniform(0.0, 2.0 * np.pi)
+        speed = rng.uniform(2.0, 8.0)
+        s["wind"] = {"density": 1.0, "drag": 1.0, "velocity": [speed * np.cos(phi), 0.0, speed * np.sin(phi)]}
+        s["material"] = mat
+        scene = scenes.Scene("materials", [s], dt=1.0 / 100, steps=1)
+        m = pyoracle.Material(dict(mat, data_file=path), which="ref")
+        c = pyoracle.Cloth(s, m)
+        assert c.topology_mismatches() == 0
+        params = np.array(scenes.step_params(scene, s))
+        _, _, _, b = c.assemble(params)
+        dv, _ = c.step(params, pyoracle.METHOD_LLT)
+        x1, v1 = c.state()
+        p = f"m{i}_"
+        out.update({p + "density": mat["density"], p + "stretching": np.array(mat["stretching"]),
+                    p + "bending": np.array(mat["bending"]), p + "ref_density": m.density,
+                    p + "k": m.stretching(G), p + "x": s["x"], p + "v": s["v"], p + "params": params,
+                    p + "b": b.astype(np.float32), p + "dv": dv.astype(np.float32), p + "x1": x1.astype(np.float32),
+                    p + "v1": v1.astype(np.float32)})
+    return out
+
+
 THICKNESS = 5e-3
 
 
@@ -184,6 +239,14 @@ if __name__ == "__main__":
         case = make_collide_case(41)
         np.savez_compressed(os.path.join(HERE, "ref_collide.npz"), **case)
         print("ref_collide", {k: int(v) for k, v in case.items() if k.endswith(("rounds", "impacts"))})
+    if not only or "ref_materials32" in only:
+        # the reference checkout's materials directory: REFERENCE_MATERIALS_DIR, else next to
+        # the sources the oracle's adapter was built from
+        mdir = os.environ.get("REFERENCE_MATERIALS_DIR") or os.path.join(
+            os.path.dirname(pyoracle.reference_src()), "materials")
+        case = make_materials_case(mdir)
+        np.savez_compressed(os.path.join(HERE, "ref_materials32.npz"), **case)
+        print("ref_materials32", [str(n) for n in case["names"]])
     if not only or "ref_detect" in only:
         case = make_detect_case(31)
         np.savez_compressed(os.path.join(HERE, "ref_detect.npz"), **case)

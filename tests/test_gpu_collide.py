@@ -105,3 +105,32 @@ def test_reference_loop_leaves_no_impacts(ctx_factory):
         again = ctx.collision_step(scene.dt)
         assert again[:2] == (1, 0), f"step {k}: impacts left after the collision step"
     assert seen >= 0
+
+
+def test_coplanar_start_matches_oracle(ctx_factory):
+    """Impacts at t = 0 exactly: one row of the upper layer starts in the plane of the lower
+    layer (both at z = 0), the rest 1.5 mm above, and the layer moves up 1 mm.  The quadratic's
+    c / q gives some of those times as -0.0, which the order of impacts (time, then node ids,
+    type, index) must take as equal to +0.0, as the oracle's comparison does.  A start that is
+    coplanar stays coplanar in every round (x0 does not move), so both sides give up after
+    2 x 100 rounds, with the same impacts chosen and projected in each round."""
+    scene = scenes.stacked_sheets(6, n_layers=2, seed=7)
+    n = 7
+    for k, s in enumerate(scene.sheets):
+        s["x"] = s["x"].copy()
+        s["x"][:, 2] = 0.0 if k == 0 else 1.5e-3
+        if k == 1:
+            s["x"][2 * n:3 * n, 2] = 0.0
+    xs = dropped(scene, lambda k, x: np.full(len(x), k == 1), -1e-3)
+    ctx = ctx_factory(scene.sheets)
+    ctx.set_state(np.concatenate(xs), np.zeros((sum(len(x) for x in xs), 3), np.float32))
+    rounds, impacts, st = ctx.collision_step(DT, allow_unresolved=True)
+    x, _ = ctx.get_state()
+    cl = oracle_cloths(scene)
+    for c, xe in zip(cl, xs):
+        c.set_state(xe.astype(np.float64), np.zeros(xe.shape))
+    orounds, oimpacts = pyoracle.collision_step(cl, DT)
+    ox = np.concatenate([c.state()[0] for c in cl])
+    assert orounds == -1 and st == native.CS_ERR_NOT_CONVERGED
+    assert oimpacts > 0 and impacts == oimpacts
+    assert np.array_equal(x.reshape(-1, 3), ox.astype(np.float32))

@@ -10,19 +10,22 @@ when that variable is set):
 for the mixed-precision solver at the benchmark's FP64-checked 1e-6 and at 1e-10, and for
 the plain FP32 solver at 1e-6 where the configuration asks for it (config 2).
 
-Bounds asserted: every solve reaches its FP64-checked tolerance (plain FP32 excepted), and
-at 1e-10 the dv error is below 1e-6 (north-star bound for the mixed solver).  At 1e-6 the dv
-error is bounded by the system's conditioning, not by the kernels; it is reported, with a
-loose sanity bound of 1e-2.
+Bounds asserted: every solve reaches its FP64-checked tolerance (plain FP32 excepted); at
+1e-10 the dv error is below 1e-6; at the benchmark's 1e-6, where the
+error is set by the system's conditioning (an FP64-checked residual of 1e-6 allows up to
+cond(A) x 1e-6), the bound is about three times the error measured on the B200 (DV_BOUND_1E6),
+so that a regression of the kernels shows.  Config 4 also runs a sweep of tolerances and
+asserts the dv bound of 1e-6 at DV_TOL_1E6, the largest tolerance found to meet it on every
+checked sheet.
 
 Configurations at full size on the GPU; the oracle runs on every sheet of configs 1 and 2,
-on a seeded subset of the sheets of configs 3 and 4 (the batch is too large for a
-single-threaded oracle in a test), and for config 5 (1,002,001 nodes) on the same scene at
-250 x 250 quads, with the full-size step checked through its FP64 residual recomputed on
-the host from the assembled system.
+on 64 seeded sheets of configs 3 and 4 (solved on a pool of host threads), and for config 5
+(1,002,001 nodes) on the same scene at 250 x 250 quads, with the full-size step checked
+through its FP64 residual recomputed on the host from the assembled system.
 """
 import json
 import os
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import pytest
@@ -34,6 +37,15 @@ import pyoracle
 from clothsimulator_b200 import native, scenes
 
 REPORT = {}
+
+# dv error bound at the FP64-checked relative residual 1e-6, per configuration: about three
+# times the largest error measured on the B200 over the checked sheets
+DV_BOUND_1E6 = {"config1_hang32": 2e-6, "config2_precision256": 5e-4, "config3_uneven512": 1e-4,
+                "config4_windy1024x64": 1e-4, "config5_irregular250": 1e-6}
+# the largest tolerance at which config 4's dv is within 1e-6 of the FP64 oracle on every
+# checked sheet (the sweep below reports the errors at each tolerance)
+DV_TOL_1E6 = 1e-8
+N_CHECKED = 64
 
 
 def rel(a, b):
@@ -96,17 +108,38 @@ def write_report():
             json.dump(REPORT, f, indent=1)
 
 
-def check_subset(name, scene, ctx, subset, tols=(1e-6, 1e-10), degrees=(1,)):
+def oracle_dvs(scene, subset):
+    """FP64 oracle solves of the given sheets on a pool of host threads (the oracle's C calls
+    release the interpreter lock)."""
+    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+        return dict(zip(subset, ex.map(lambda k: oracle_dv(scene, scene.sheets[k]), subset)))
+
+
+def dv_bound(name, tol):
+    if tol <= 1e-10:
+        return 1e-6
+    if tol >= 1e-6:
+        return DV_BOUND_1E6[name]
+    return None
+
+
+def check_subset(name, scene, ctx, subset, tols=(1e-6, 1e-10), degrees=(1,), oracle=None):
     """degrees: the cluster-resident solver's preconditioner (1 block-Jacobi, 3 the strip-local
     Chebyshev polynomial the bench uses); the bounds are the same for each."""
-    oracle = {k: oracle_dv(scene, scene.sheets[k]) for k in subset}
+    oracle = oracle if oracle is not None else oracle_dvs(scene, subset)
+    worst = {}
     for deg in degrees:
         for tol in tols:
             res, stats = gpu_step(ctx, scene, tol=tol, precision=native.PREC_MIXED, precond_degree=deg)
             assert stats.converged == len(scene.sheets) and stats.max_rel_residual <= tol
             errs = [sheet_errors(scene, scene.sheets[k], res[k][0], res[k][1], oracle[k]) for k in subset]
             record(name, f"mixed_tol{tol:g}" + ("" if deg == 1 else f"_chebyshev{deg}"), errs)
-            assert max(e[0] for e in errs) < (1e-6 if tol <= 1e-10 else 1e-2)
+            err = max(e[0] for e in errs)
+            worst[(deg, tol)] = err
+            bound = dv_bound(name, tol)
+            if bound is not None:
+                assert err < bound, f"{name} tol {tol:g} degree {deg}: dv error {err:.3e} >= {bound:.1e}"
+    return worst
 
 
 def test_config1_hang32(ctx_factory):
@@ -128,22 +161,28 @@ def test_config2_precision_study(ctx_factory):
         REPORT["config2_precision256"][key]["rel_residual"] = stats.max_rel_residual
         if kw["precision"] == native.PREC_MIXED:
             assert stats.converged == 1
-        if kw["tol"] <= 1e-10:
-            assert e[0] < 1e-6
+        if kw["precision"] == native.PREC_MIXED:
+            assert e[0] < dv_bound("config2_precision256", kw["tol"])
 
 
 def test_config3_uneven512(ctx_factory):
     scene = scenes.uneven_batch(512, seed=0)
     rng = np.random.default_rng(3)
-    subset = sorted(rng.choice(len(scene.sheets), 12, replace=False).tolist())
+    subset = sorted(rng.choice(len(scene.sheets), N_CHECKED, replace=False).tolist())
     check_subset("config3_uneven512", scene, ctx_factory(scene.sheets), subset, degrees=(1, 3))
 
 
 def test_config4_windy1024(ctx_factory):
     scene = scenes.windy_batch(1024, 64, seed=1000)
     rng = np.random.default_rng(4)
-    subset = sorted(rng.choice(len(scene.sheets), 8, replace=False).tolist())
-    check_subset("config4_windy1024x64", scene, ctx_factory(scene.sheets), subset, degrees=(1, 3))
+    subset = sorted(rng.choice(len(scene.sheets), N_CHECKED, replace=False).tolist())
+    ctx = ctx_factory(scene.sheets)
+    oracle = oracle_dvs(scene, subset)
+    check_subset("config4_windy1024x64", scene, ctx, subset, degrees=(1, 3), oracle=oracle)
+    # tolerance sweep with the bench's preconditioner: the dv error against the FP64 oracle
+    worst = check_subset("config4_windy1024x64", scene, ctx, subset, tols=(1e-7, 1e-8, 1e-9), degrees=(3,),
+                         oracle=oracle)
+    assert worst[(3, DV_TOL_1E6)] < 1e-6, f"dv error {worst[(3, DV_TOL_1E6)]:.3e} at tol {DV_TOL_1E6:g}"
 
 
 def test_config5_irregular(ctx_factory):

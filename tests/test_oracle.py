@@ -319,3 +319,42 @@ def test_oracle_collision_matches_reference_adapter_live():
             for (xa, va), (xb, vb) in zip(res[0][1], res[1][1]):
                 assert_collided(xa, xb, (seed, name))
                 assert_collided(va, vb, (seed, name), tol=1e-4)
+
+
+GOLDEN_MATERIALS = os.path.join(os.path.dirname(__file__), "golden", "ref_materials32.npz")
+
+
+def golden_material_sheets(g):
+    """(scene, sheets) of ref_materials32.npz: one 32x32 sheet per reference material file."""
+    sheets = []
+    for i in range(len(g["names"])):
+        p = f"m{i}_"
+        par = g[p + "params"]
+        mat = {"density": float(g[p + "density"]), "stretching": g[p + "stretching"].tolist(),
+               "bending": g[p + "bending"].tolist(), "thicken": 1.0, "density_mult": 1.0, "stretching_mult": 1.0,
+               "bending_mult": 1.0}
+        s = {"x": g[p + "x"], "v": g[p + "v"], "uv": g["uv"], "fx": g["fx"], "fu": g["fu"], "handles": g["handles"],
+             "material": mat, "wind": {"density": float(par[4]), "drag": float(par[5]), "velocity": list(map(float, par[6:9]))}}
+        sheets.append(s)
+    scene = scenes.Scene("materials", sheets, dt=float(g["m0_params"][0]), steps=1,
+                         handle_stiffness=float(g["m0_params"][9]))
+    return scene, sheets
+
+
+def test_oracle_reproduces_reference_material_files():
+    """Three of the reference's own material files (gray-interlock, 11oz-black-denim, paper),
+    read by the reference's Material: stretching lookups, the windy system's b, the CPU step."""
+    g = np.load(GOLDEN_MATERIALS)
+    scene, sheets = golden_material_sheets(g)
+    for i, s in enumerate(sheets):
+        p = f"m{i}_"
+        m = pyoracle.Material(s["material"], "float")
+        assert m.density == float(g[p + "ref_density"])
+        assert np.array_equal(m.stretching(g["G"]), g[p + "k"]), g["names"][i]
+        c = pyoracle.Cloth(s, m)
+        _, _, _, b = c.assemble(g[p + "params"])
+        assert np.array_equal(b.astype(np.float32), g[p + "b"]), g["names"][i]
+        dv, _ = c.step(g[p + "params"], pyoracle.METHOD_LLT)
+        x1, v1 = c.state()
+        assert np.array_equal(dv.astype(np.float32), g[p + "dv"]), g["names"][i]
+        assert np.array_equal(x1.astype(np.float32), g[p + "x1"]) and np.array_equal(v1.astype(np.float32), g[p + "v1"])

@@ -88,3 +88,70 @@ def test_noalloc_rejects_oversized_and_malformed_input():
     xx = torch.zeros(3, dtype=torch.float32, device=dev)
     st, _, _ = _call(lib, 1, 1, rp.data_ptr(), ci.data_ptr(), val.data_ptr(), bb.data_ptr(), xx.data_ptr())
     assert st == native.CS_ERR_INVALID_ARG
+
+
+def test_noalloc_matches_fp64_oracle_and_reports_its_cap():
+    """Against the FP64 direct solve of the same system (the CPU oracle), and with a cap of one
+    iteration: CS_ERR_NOT_CONVERGED with one iteration reported."""
+    import torch
+    import pyoracle
+
+    scene = scenes.hang(24, seed=5)
+    s = scene.sheets[0]
+    rng = np.random.default_rng(5)
+    s["x"] = (s["x"] + rng.normal(0, 0.01, s["x"].shape)).astype(np.float32)
+    s["v"] = rng.normal(0, 0.1, s["v"].shape).astype(np.float32)
+    oc = pyoracle.Cloth(s, pyoracle.Material(s["material"], "float"))
+    rp, ci, val, b = oc.assemble(scenes.step_params(scene, s))
+    exact, _ = oc.solve(pyoracle.METHOD_LLT64)
+    lib = native.load_library()
+    dev = torch.device("cuda", 0)
+    d_rp = torch.from_numpy(rp.astype(np.int32)).to(dev)
+    d_ci = torch.from_numpy(ci.astype(np.int32)).to(dev)
+    d_val = torch.from_numpy(val.astype(np.float32).reshape(-1)).to(dev)
+    d_b = torch.from_numpy(b.astype(np.float32)).to(dev)
+    n = len(rp) - 1
+    d_x = torch.zeros(3 * n, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    st, it, rr = _call(lib, n, len(ci), d_rp.data_ptr(), d_ci.data_ptr(), d_val.data_ptr(), d_b.data_ptr(),
+                       d_x.data_ptr())
+    assert st == native.CS_OK and rr <= 1e-10
+    assert rel(d_x.cpu().numpy(), exact) < TOL
+    st, it, rr = _call(lib, n, len(ci), d_rp.data_ptr(), d_ci.data_ptr(), d_val.data_ptr(), d_b.data_ptr(),
+                       d_x.data_ptr(), max_iters=1)
+    assert st == native.CS_ERR_NOT_CONVERGED and it == 1 and rr > 1e-10
+
+
+def test_noalloc_asynchronous_form_on_a_stream():
+    """The asynchronous form (no statistics pointers) on a non-default stream: it returns after
+    the launch; after the stream is synchronised x holds the solution.  A system the device
+    rejects leaves NaN in x."""
+    import torch
+
+    ctx, dv_ref, rp, ci, val, b = _system(nq=20, seed=9)
+    lib = native.load_library()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(stream):
+        d_rp = torch.from_numpy(rp).to(dev)
+        d_ci = torch.from_numpy(ci).to(dev)
+        d_val = torch.from_numpy(val.reshape(-1)).to(dev)
+        d_b = torch.from_numpy(b).to(dev)
+        d_x = torch.zeros(3 * ctx.n, dtype=torch.float32, device=dev)
+    st = lib.cs_solve_block_csr_noalloc(ctx.n, len(ci), d_rp.data_ptr(), d_ci.data_ptr(), d_val.data_ptr(),
+                                        d_b.data_ptr(), d_x.data_ptr(), 1e-10, 20000,
+                                        ctypes.c_void_p(stream.cuda_stream), None, None)
+    assert st == native.CS_OK
+    stream.synchronize()
+    assert rel(d_x.cpu().numpy(), dv_ref) < TOL
+    # out-of-range column: the asynchronous form cannot report it, x becomes NaN
+    with torch.cuda.stream(stream):
+        bad_ci = d_ci.clone()
+        bad_ci[0] = 10 * ctx.n
+    st = lib.cs_solve_block_csr_noalloc(ctx.n, len(ci), d_rp.data_ptr(), bad_ci.data_ptr(), d_val.data_ptr(),
+                                        d_b.data_ptr(), d_x.data_ptr(), 1e-10, 20000,
+                                        ctypes.c_void_p(stream.cuda_stream), None, None)
+    assert st == native.CS_OK
+    stream.synchronize()
+    assert np.all(np.isnan(d_x.cpu().numpy()))
+    ctx.close()
