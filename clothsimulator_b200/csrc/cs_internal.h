@@ -96,6 +96,14 @@ enum InstPhase : int {
 // blocks strip-local) and 28x28 (0.59) need fewer or as many iterations with block-Jacobi, 32x32
 // (0.71), 40x40 (0.65), 48x48 (0.84) and 64x64 (0.89) fewer with the Chebyshev polynomial.
 #define CS_CHEB_MIN_LOCAL 0.62  // power iterations per sheet solve for the strip-local Chebyshev bound
+// Coarse-space correction of the cluster-resident solver (with the strip-local Chebyshev
+// preconditioner): each CTA's strip of rows is cut into K segments along the principal axis of
+// its nodes' rest (uv) coordinates, K = min(CS_COARSE_MAX_K, CS_COARSE_AGGS / CTAs per cluster);
+// the coarse space holds one constant per (segment, component).
+#define CS_COARSE_MAX_K 8
+#define CS_COARSE_AGGS 54
+// Threads of the per-sheet set-up kernel that forms and inverts the coarse matrix.
+#define CS_COARSE_THREADS 512
 #define CS_SOLVER_AUTO_DEV 0
 #define CS_SOLVER_BATCHED_DEV 1
 
@@ -138,6 +146,7 @@ struct DevParams {
     int advance;           // 1: v += dv, x += dt v at the end of the step
     int solver;            // CS_SOLVER_AUTO_DEV: resident sheets on the cluster kernel; BATCHED: loop only
     int cheb_degree;       // resident solver: 1 block-Jacobi; odd >= 3 strip-local Chebyshev of that degree
+    int coarse;            // resident solver with the Chebyshev preconditioner: 1 adds the coarse-space correction
 };
 
 // One proximity as seen by one sheet it touches (cs_set_proximities): node[i] is a batch
@@ -209,6 +218,23 @@ struct Batch {
     int* rcheb = nullptr;        // per topology and rank: 1 if the strip uses the Chebyshev preconditioner when asked
     int res_halo0 = 0;           // first halo slot of every CTA's p array (= own slots per CTA)
     int res_alt = 0;             // first slot of the second own-row buffer (strip-local Chebyshev)
+    // coarse-space correction (resident.cu): per topology {coarse unknowns nc (0: none), segments
+    // per strip K, first and last entry of the coarse pattern in cpair}; per topology row its
+    // sheet-local aggregate (rank * K + segment; at row2slot offsets); per topology, rank and
+    // warp the segments among the warp's rows (bit k: segment k); the coarse pattern's block
+    // pairs {aggregate a, aggregate b, first, last contributor in ccontrib} with their stored
+    // blocks as topology slots; per resident work item the inverse coarse matrix (nc x nc) and
+    // whether it was formed.
+    int4* rcoarse = nullptr;
+    int* ragg = nullptr;
+    int* rwmask = nullptr;       // per topology: CS_RES_MAX_CL x CS_RES_MAX_WARPS
+    int4* cpair = nullptr;
+    int* ccontrib = nullptr;
+    float* cinv = nullptr;
+    int* cvalid = nullptr;
+    int res_cnc = 0;             // largest nc over the resident topologies (0: no coarse correction)
+    int res_ck = 0;              // largest K
+    int res_coff = 0;            // byte offset of the coarse region in the resident kernel's shared memory
     // per-topology block CSR (local ids, columns ascending) with the SELL slot of each block
     int* tcsr_ptr = nullptr;
     int* tcsr_col = nullptr;

@@ -22,6 +22,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -46,6 +47,7 @@ __global__ void cs_advance_kernel(Batch B);
 __global__ void cs_spmv_plain_kernel(Batch B, const float* x, float* y);
 __global__ void cs_profile_setup_kernel(Batch B, int phase);
 __global__ void cs_resident_pcg_kernel(Batch B);
+__global__ void cs_coarse_setup_kernel(Batch B);
 __global__ void cs_prox_kernel(Batch B);
 __global__ void cs_prox_row_kernel(Batch B);
 __global__ void cs_slice_bnorm_kernel(Batch B);
@@ -198,6 +200,9 @@ struct Topo {
     // every edge (reference order): nodes, adjacent faces per side (-1: none); per face its
     // edges (v0 v1), (v1 v2), (v2 v0); per node its (face, corner) pairs in face order
     std::vector<int> e_nodes, e_faces, f_edges, nf_ptr, nf_code;
+    // rest (uv) coordinates of every node, from the first sheet of this connectivity: the
+    // geometry the coarse-space segments of the cluster-resident solver are cut along
+    std::vector<float> node_uv;
 };
 
 struct TopoKey {
@@ -231,6 +236,16 @@ std::shared_ptr<Topo> buildTopo(const cs_sheet_desc& s, std::string& err) {
             err = "face index out of range";
             return nullptr;
         }
+    }
+    t->node_uv.assign(2 * (size_t)nn, 0.0f);
+    {
+        std::vector<char> seen(nn, 0);
+        for (int i = 0; i < 3 * nf; i++)
+            if (!seen[t->fx[i]]) {
+                seen[t->fx[i]] = 1;
+                t->node_uv[2 * t->fx[i]] = s.uv[2 * t->fu[i]];
+                t->node_uv[2 * t->fx[i] + 1] = s.uv[2 * t->fu[i] + 1];
+            }
     }
     // Edges: first appearance order, nodes[0] < nodes[1]; sides per Edge::initialize.
     std::unordered_map<uint64_t, int> map;
@@ -504,12 +519,162 @@ int residentSplit(const Topo& T, int ncta, std::vector<int>& split) {
 // (owner rank, owner slot).  code: per panel slot, the local p index of its column (own slot,
 // or CS_RES_HALO_BIT | halo index, rebased once the batch's own-slot count is known).  send:
 // per owner CTA (sendptr), the entries src slot | dst rank << 12 | dst halo index << 16.
+struct CoarsePlan {
+    int K = 0, nc = 0;             // segments per strip, coarse unknowns (3 per aggregate)
+    std::vector<int> agg;          // per local row: rank * K + segment
+    std::vector<int> wmask;        // CS_RES_MAX_CL x CS_RES_MAX_WARPS: segments among each warp's rows (bits)
+    std::vector<int4> pairs;       // coarse block pairs {a, b, first, last contributor}
+    std::vector<int> contrib;      // topology slots of the stored blocks, per pair ascending
+};
+
 struct ResidentPlan {
     std::vector<int> split, code, sendptr, halo_count;
     std::vector<uint32_t> send;
     int w = 0, max_halo = 0, max_panels = 0, max_width = 0;
     long long blocks = 0, local_blocks = 0;  // pattern blocks; those with row and column on one CTA
+    CoarsePlan coarse;
 };
+
+// Segments per strip of the coarse-space correction on a cluster of `ncta` CTAs; CS_COARSE_SEGMENTS
+// (0..CS_COARSE_MAX_K, at most CS_COARSE_AGGS / ncta) sets it, 0 turns the correction off.
+int coarseSegments(int ncta) {
+    const int cap = CS_COARSE_AGGS / std::max(ncta, 1);
+    if (const char* ev = std::getenv("CS_COARSE_SEGMENTS")) return std::max(0, std::min({std::atoi(ev), CS_COARSE_MAX_K, cap}));
+    return std::min(CS_COARSE_MAX_K, cap);
+}
+
+// Shared memory of the coarse region of the resident kernel (resident.cu lays it out the same
+// way, each part rounded up to 4 floats): the CTA's rows of the inverse coarse matrix (3K x nc
+// floats), the coarse residual in FP32 (nc), the
+// correction of the CTA's aggregates and its partial sums (CP = 3K rounded up to 4, each), the
+// partials of every CTA in two buffers (2 x ncta x CP), then the coarse residual and search
+// direction in FP64 (nc each).
+size_t coarseSmemBytes(int ncta, int K) {
+    if (K <= 0) return 0;
+    auto r4 = [](size_t n) { return (n + 3) / 4 * 4; };  // every part starts on 16 bytes
+    const size_t nc = 3 * (size_t)ncta * K, cp = r4(3 * (size_t)K);
+    const size_t f = r4(3 * (size_t)K * nc) + r4(nc) + 2 * cp + 2 * (size_t)ncta * cp;
+    return f * sizeof(float) + 2 * nc * sizeof(double);
+}
+
+// Reorders the lanes of every SELL slice of a topology so that rows of one coarse aggregate sit
+// in consecutive lanes (stable within an aggregate).  A slice keeps its rows and width; only
+// which lane holds which row changes, with every slot-indexed array (columns, contributor
+// lists, the block-CSR view's slots) moved along.  Per warp, the resident solver then sums a
+// vector over each aggregate with one segmented scan.
+void permuteLanesByAggregate(Topo& T, const std::vector<int>& agg) {
+    const size_t nslot = (size_t)T.n_tpanels * CS_SLICE;
+    std::vector<int> newOf(nslot), rowmap = T.rowmap;
+    for (int s = 0; s < T.n_slices; s++) {
+        const int rows = T.slice_rows[s];
+        std::vector<int> perm(rows), lnew(CS_SLICE);
+        for (int l = 0; l < rows; l++) perm[l] = l;
+        std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+            return agg[T.rowmap[s * CS_SLICE + a]] < agg[T.rowmap[s * CS_SLICE + b]];
+        });
+        for (int l = 0; l < CS_SLICE; l++) lnew[l] = l;
+        for (int pos = 0; pos < rows; pos++) {
+            lnew[perm[pos]] = pos;
+            rowmap[s * CS_SLICE + pos] = T.rowmap[s * CS_SLICE + perm[pos]];
+        }
+        for (int k = 0; k < T.slice_width[s]; k++)
+            for (int l = 0; l < CS_SLICE; l++)
+                newOf[(size_t)(T.slice_tpanel0[s] + k) * CS_SLICE + l] = (T.slice_tpanel0[s] + k) * CS_SLICE + lnew[l];
+    }
+    std::vector<int> oldOf(nslot), tcol(nslot), tcptr(nslot + 1);
+    for (size_t o = 0; o < nslot; o++) oldOf[newOf[o]] = (int)o;
+    std::vector<uint32_t> tcontrib;
+    tcontrib.reserve(T.tcontrib.size());
+    for (size_t q = 0; q < nslot; q++) {
+        const int o = oldOf[q];
+        tcol[q] = T.tcol[o];
+        tcptr[q] = (int)tcontrib.size();
+        tcontrib.insert(tcontrib.end(), T.tcontrib.begin() + T.tcptr[o], T.tcontrib.begin() + T.tcptr[o + 1]);
+    }
+    tcptr[nslot] = (int)tcontrib.size();
+    for (int& q : T.csr_slot) q = newOf[q];
+    T.rowmap = rowmap;
+    for (int s = 0; s < T.n_slices; s++)
+        for (int l = 0; l < T.slice_rows[s]; l++) T.row2slot[rowmap[s * CS_SLICE + l]] = s * CS_SLICE + l;
+    T.tcol.swap(tcol);
+    T.tcptr.swap(tcptr);
+    T.tcontrib.swap(tcontrib);
+}
+
+// Coarse-space plan of one topology on a cluster of `ncta` CTAs: each CTA's strip of rows is cut
+// into K segments of equal row count along the principal axis of the rows' rest coordinates (a
+// strip of a grid sheet is a band of grid rows; its segments are blocks side by side), and the
+// coarse pattern lists, per pair of aggregates, the stored blocks coupling them in slot order.
+void coarsePlan(const Topo& T, ResidentPlan& P, int ncta, int K) {
+    CoarsePlan& C = P.coarse;
+    C = CoarsePlan();
+    C.K = K;
+    C.nc = 3 * ncta * K;
+    C.agg.assign(T.n_nodes, -1);
+    C.wmask.assign(CS_RES_MAX_CL * CS_RES_MAX_WARPS, 0);
+    for (int c = 0; c < ncta; c++) {
+        std::vector<std::pair<int, int>> rows;  // (local row, own slot)
+        for (int sl = P.split[c]; sl < P.split[c + 1]; sl++)
+            for (int l = 0; l < T.slice_rows[sl]; l++)
+                rows.push_back({T.rowmap[sl * CS_SLICE + l], (sl - P.split[c]) * CS_SLICE + l});
+        const int n = (int)rows.size();
+        double mx = 0.0, my = 0.0;
+        for (auto& r : rows) {
+            mx += T.node_uv[2 * r.first];
+            my += T.node_uv[2 * r.first + 1];
+        }
+        mx /= std::max(n, 1);
+        my /= std::max(n, 1);
+        double sxx = 0.0, sxy = 0.0, syy = 0.0;
+        for (auto& r : rows) {
+            const double dx = T.node_uv[2 * r.first] - mx, dy = T.node_uv[2 * r.first + 1] - my;
+            sxx += dx * dx;
+            sxy += dx * dy;
+            syy += dy * dy;
+        }
+        // principal axis: eigenvector of the larger eigenvalue of the 2x2 scatter matrix
+        const double tr = sxx + syy, det = sxx * syy - sxy * sxy;
+        const double l1 = 0.5 * tr + std::sqrt(std::max(0.0, 0.25 * tr * tr - det));
+        double ax = 1.0, ay = 0.0;
+        if (std::fabs(sxy) > 0.0) {
+            ax = l1 - syy;
+            ay = sxy;
+        } else if (syy > sxx) {
+            ax = 0.0;
+            ay = 1.0;
+        }
+        std::vector<std::pair<double, int>> key(n);
+        for (int i = 0; i < n; i++) {
+            const int r = rows[i].first;
+            key[i] = {(T.node_uv[2 * r] - mx) * ax + (T.node_uv[2 * r + 1] - my) * ay, i};
+        }
+        std::sort(key.begin(), key.end());
+        for (int k = 0; k < K; k++)
+            for (int i = (int)((long long)k * n / K); i < (int)((long long)(k + 1) * n / K); i++) {
+                const auto& r = rows[key[i].second];
+                C.agg[r.first] = c * K + k;
+                C.wmask[c * CS_RES_MAX_WARPS + r.second / CS_SLICE] |= 1 << k;  // own slot / 32 = warp
+            }
+    }
+    // coarse pattern: every stored block (slots with contributors; padding has none)
+    std::vector<std::tuple<int, int, int>> blk;  // (a, b, slot)
+    for (int sl = 0; sl < T.n_slices; sl++)
+        for (int k = 0; k < T.slice_width[sl]; k++)
+            for (int l = 0; l < T.slice_rows[sl]; l++) {
+                const int slot = (T.slice_tpanel0[sl] + k) * CS_SLICE + l;
+                if (T.tcptr[slot + 1] == T.tcptr[slot]) continue;
+                blk.emplace_back(C.agg[T.rowmap[sl * CS_SLICE + l]], C.agg[T.tcol[slot]], slot);
+            }
+    std::sort(blk.begin(), blk.end());
+    for (size_t i = 0; i < blk.size();) {
+        size_t j = i;
+        while (j < blk.size() && std::get<0>(blk[j]) == std::get<0>(blk[i]) && std::get<1>(blk[j]) == std::get<1>(blk[i])) j++;
+        C.pairs.push_back(make_int4(std::get<0>(blk[i]), std::get<1>(blk[i]), (int)C.contrib.size(),
+                                    (int)(C.contrib.size() + (j - i))));
+        for (size_t q = i; q < j; q++) C.contrib.push_back(std::get<2>(blk[q]));
+        i = j;
+    }
+}
 
 #define CS_RES_HALO_BIT 0x40000000
 
@@ -761,6 +926,10 @@ void launchSolvePrologue(cs_ctx* c) {
 // Sheets that fit a cluster's shared memory: one persistent cluster per sheet at a time.
 void launchResident(cs_ctx* c) {
     if (c->resClusters <= 0) return;
+    // the coarse matrices of the resident sheets, formed and inverted for this step's systems
+    if (c->B.res_cnc > 0 && c->B.n_resident > 0)
+        cs_coarse_setup_kernel<<<c->B.n_resident, CS_COARSE_THREADS,
+                                 (size_t)(c->B.res_cnc + 4) * c->B.res_cnc * sizeof(float), c->stream>>>(c->B);
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -851,6 +1020,7 @@ DevParams toDev(const cs_step_params* p) {
     d.advance = p->advance;
     d.solver = p->solver == CS_SOLVER_BATCHED ? CS_SOLVER_BATCHED_DEV : CS_SOLVER_AUTO_DEV;
     d.cheb_degree = p->precond_degree >= 3 ? p->precond_degree : 1;
+    d.coarse = p->coarse != 0;
     return d;
 }
 
@@ -1000,7 +1170,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         candidates = {v};
     }
     struct ResChoice {
-        int cl = 0, w = 0, panels = 0, halo = 0, cap = 0, clusters = 0;
+        int cl = 0, w = 0, panels = 0, halo = 0, cap = 0, clusters = 0, ck = 0;
         long long sheets = 0;
         size_t smem = 0;
         std::vector<ResidentPlan> plans;
@@ -1027,8 +1197,18 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             R.halo = std::max(R.halo, P.max_halo);
         }
         if (R.w == 0) return R;
-        // p array: own slots, halo slots, then a second own-slot buffer (strip-local Chebyshev)
-        const size_t pbytes = ((size_t)2 * R.w * CS_SLICE + R.halo) * sizeof(float4);
+        // coarse-space correction for the topologies with the strip-local Chebyshev
+        // preconditioner (it needs a second warp for the segment sums)
+        R.ck = coarseSegments(cl);
+        bool anyCoarse = false;
+        for (size_t t = 0; t < topos.size(); t++)
+            anyCoarse |= R.resident[t] && R.plans[t].blocks > 0 &&
+                         (double)R.plans[t].local_blocks >= CS_CHEB_MIN_LOCAL * (double)R.plans[t].blocks;
+        if (!anyCoarse || R.ck < 2 || R.w < 2) R.ck = 0;
+        // p array: own slots, halo slots, then a second own-slot buffer (strip-local Chebyshev),
+        // then the coarse region
+        const size_t ubytes = ((size_t)2 * R.w * CS_SLICE + R.halo) * sizeof(float4);
+        const size_t pbytes = ubytes + coarseSmemBytes(cl, R.ck);
         const size_t budget = devProp.sharedMemPerBlockOptin > resAttr.sharedSizeBytes + pbytes
                                   ? devProp.sharedMemPerBlockOptin - resAttr.sharedSizeBytes - pbytes : 0;
         R.cap = (int)std::min<size_t>((size_t)R.panels, budget / (CS_PANEL_FLOATS * sizeof(float)));
@@ -1081,9 +1261,42 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             const bool cheb = plans[t].blocks > 0 &&
                               (double)plans[t].local_blocks >= CS_CHEB_MIN_LOCAL * (double)plans[t].blocks;
             for (int r = 0; r <= CS_RES_MAX_CL; r++) hrcheb[t * (CS_RES_MAX_CL + 1) + r] = cheb;
+            if (cheb && res.ck > 0) {
+                // segments, then the lanes of each slice grouped by segment, then the plans
+                // again over the moved slots (the slices and their rows stay)
+                coarsePlan(*topos[t], plans[t], res.cl, res.ck);
+                permuteLanesByAggregate(*topos[t], plans[t].coarse.agg);
+                plans[t] = residentPlan(*topos[t], res.cl);
+                coarsePlan(*topos[t], plans[t], res.cl, res.ck);
+            }
         }
+    // coarse-space arrays, per topology concatenated
+    std::vector<int4> hrcoarse(topos.size(), make_int4(0, 0, 0, 0)), hcpair;
+    std::vector<int> hragg, hrwmask(topos.size() * CS_RES_MAX_CL * CS_RES_MAX_WARPS, 0), hccontrib;
+    for (size_t t = 0; t < topos.size(); t++) {
+        static const CoarsePlan none;
+        const CoarsePlan& C = t < plans.size() ? plans[t].coarse : none;
+        if (topoResident[t] && C.nc > 0) {
+            const int p0 = (int)hcpair.size(), c0 = (int)hccontrib.size();
+            for (const int4& q : C.pairs) hcpair.push_back(make_int4(q.x, q.y, q.z + c0, q.w + c0));
+            hccontrib.insert(hccontrib.end(), C.contrib.begin(), C.contrib.end());
+            std::copy(C.wmask.begin(), C.wmask.end(), hrwmask.begin() + t * CS_RES_MAX_CL * CS_RES_MAX_WARPS);
+            hrcoarse[t] = make_int4(C.nc, C.K, p0, (int)hcpair.size());
+            hragg.insert(hragg.end(), C.agg.begin(), C.agg.end());
+        } else {
+            hragg.insert(hragg.end(), topos[t]->n_nodes, -1);
+        }
+    }
     c->resCL = c->resThreads = c->resClusters = 0;
     c->resSmem = 0;
+    B.res_cnc = B.res_ck = B.res_coff = 0;
+    if (res.clusters > 0 && res.ck > 0) {
+        B.res_ck = res.ck;
+        B.res_cnc = 3 * res.cl * res.ck;
+        B.res_coff = (int)(res.smem - coarseSmemBytes(res.cl, res.ck));
+        CS_CUDA(cudaFuncSetAttribute(cs_coarse_setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (B.res_cnc + 4) * B.res_cnc * (int)sizeof(float)));
+    }
     if (res.clusters > 0) {
         // the launch attributes of the chosen plan (the evaluation set others)
         CS_CUDA(cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)res.smem));
@@ -1295,6 +1508,11 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     UP(rsend, hrsend);
     UP(rhalo, hrhalo);
     UP(rcheb, hrcheb);
+    UP(rcoarse, hrcoarse);
+    UP(ragg, hragg);
+    UP(rwmask, hrwmask);
+    UP(cpair, hcpair);
+    UP(ccontrib, hccontrib);
 #undef UP
 #define AL(field, n) \
     if ((st = dalloc(c, &B.field, (size_t)(n))) != CS_OK) return st;
@@ -1317,6 +1535,8 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     AL(inst, B.S);
     AL(params, 1);
     AL(loop, 8);
+    AL(cinv, B.res_cnc > 0 ? (long long)hrlist.size() * B.res_cnc * B.res_cnc : 1);
+    AL(cvalid, std::max<size_t>(hrlist.size(), 1));
 #undef AL
     CS_CUDA(cudaMemset(B.dv, 0, 3LL * B.N * sizeof(float)));
     CS_CUDA(cudaMemcpy(B.x0, B.x, 3LL * B.N * sizeof(float), cudaMemcpyDeviceToDevice));  // Node::Node

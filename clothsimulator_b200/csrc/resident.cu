@@ -234,6 +234,134 @@ __device__ __forceinline__ bool cluster_sum3(ResShared& S, int rank, int ncta, u
     return ok;
 }
 
+// The coarse-space correction's state in one CTA's shared memory: the coarse region the loader
+// sizes with coarseSmemBytes, each part rounded up to 4 floats.  Offsets come from the kernel
+// parameters (res_cnc = nc, res_ck = K), so they hold no registers.
+//   ai   this CTA's rows of the inverse coarse matrix, 3K x nc
+//   r32  the coarse residual R r in FP32 (the matrix-vector product's input), nc
+//   ce   the correction of this CTA's aggregates, 3K (CP = 3K rounded up to 4)
+//   part this CTA's segment sums before they are sent, CP
+//   red  every CTA's segment sums: [buffer][rank][CP]
+//   r64, s64  the coarse residual R r and search direction R s in FP64, nc each
+struct CoarseSm {
+    unsigned char* base;
+    int nc, k3, cp;
+    __device__ __forceinline__ CoarseSm(unsigned char* b, int nc_, int k) : base(b), nc(nc_), k3(3 * k), cp((3 * k + 3) / 4 * 4) {}
+    __device__ __forceinline__ static int r4(int n) { return (n + 3) / 4 * 4; }
+    __device__ __forceinline__ float* ai() const { return reinterpret_cast<float*>(base); }
+    __device__ __forceinline__ float* r32() const { return ai() + r4(k3 * nc); }
+    __device__ __forceinline__ float* ce() const { return r32() + r4(nc); }
+    __device__ __forceinline__ float* part() const { return ce() + cp; }
+    __device__ __forceinline__ float* red() const { return part() + cp; }
+    __device__ __forceinline__ double* r64(int ncta) const { return reinterpret_cast<double*>(red() + 2 * ncta * cp); }
+    __device__ __forceinline__ double* s64(int ncta) const { return r64(ncta) + nc; }
+    // entry q of the coarse vector in one buffer of `red` (rank q / 3K, segment and component
+    // q % 3K)
+    __device__ __forceinline__ int off(int q) const { return (q / k3) * cp + q % k3; }
+};
+
+// cluster_sum3 that also carries the coarse vector R y of a per-row vector y.  The lanes of a
+// slice hold the rows of one segment consecutively (the loader orders them so); `cseg` packs this
+// lane's run: the run's first lane (bits 0-4), whether this lane ends it (bit 5), the segment + 1
+// (bits 8-15; 0 for a lane without a row) and, for the gathering lanes of warp 1, the warps
+// holding the lane's segment (bits 16-31); bit 6 is the caller's.  A segmented inclusive scan (5 shuffle steps per
+// component) leaves each run's sum in its last lane, which stages it in `wp` (warp-major, CP
+// floats per warp); after the first barrier lane 3k + c of warp 1 adds component c of segment
+// k over the warps holding it (bits 16-31 of its cseg), in warp order, and those sums travel
+// with the three values to every CTA.  On return buffer (nred - 1) & 1 of C.red holds R y, entry
+// q at C.off(q) (q = 3 (rank K + k) + c); it may be overwritten by the reduction after next.
+// Deterministic like cluster_sum3.
+__device__ __forceinline__ bool cluster_sum3c(ResShared& S, int rank, int ncta, uint32_t& nred, double (&v)[3], bool fp32,
+                                              const float (&y)[3], bool live, int cseg, float* wp, const CoarseSm& C) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int b = (int)(nred & 1u);
+    {
+        const int rs = cseg & 31, sg = ((cseg >> 8) & 0xff) - 1;
+        float a0 = live ? y[0] : 0.f, a1 = live ? y[1] : 0.f, a2 = live ? y[2] : 0.f;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const float t0 = __shfl_up_sync(0xffffffffu, a0, d), t1 = __shfl_up_sync(0xffffffffu, a1, d),
+                        t2 = __shfl_up_sync(0xffffffffu, a2, d);
+            if (lane - d >= rs) {
+                a0 += t0;
+                a1 += t1;
+                a2 += t2;
+            }
+        }
+        if (((cseg >> 5) & 1) && sg >= 0 && 3 * sg < C.k3) {
+            wp[w * C.cp + 3 * sg] = a0;
+            wp[w * C.cp + 3 * sg + 1] = a1;
+            wp[w * C.cp + 3 * sg + 2] = a2;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) v[i] = fp32 ? (double)rwarp_sum((float)v[i]) : rwarp_sum(v[i]);
+    if (lane == 0) {
+#pragma unroll
+        for (int i = 0; i < 3; i++) S.wsum[w][i] = v[i];
+    }
+    __syncthreads();
+    double t[3] = {0.0, 0.0, 0.0};
+    if (w == 0 && lane < ncta) {
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            if (fp32) {
+                float a = 0.f;
+#pragma unroll
+                for (int j = 0; j < CS_RES_MAX_WARPS; j++)
+                    if (j < nw) a += (float)S.wsum[j][i];
+                t[i] = (double)a;
+            } else {
+                double a = 0.0;
+#pragma unroll
+                for (int j = 0; j < CS_RES_MAX_WARPS; j++)
+                    if (j < nw) a += S.wsum[j][i];
+                t[i] = a;
+            }
+        }
+    }
+    if (w == 1 && lane < C.cp) {
+        float a = 0.f;
+        const unsigned wk = (unsigned)cseg >> 16;  // the warps holding this lane's segment
+#pragma unroll
+        for (int j = 0; j < CS_RES_MAX_WARPS; j++)
+            if ((wk >> j) & 1u) a += wp[j * C.cp + lane];
+        C.part()[lane] = a;
+    }
+    // warps 0 and 1 only (named barrier 1 of 64 threads): the segment sums are in place before
+    // warp 0 sends them; the other warps go straight to the wait
+    if (w < 2) asm volatile("bar.sync 1, 64;" ::: "memory");
+    if (w == 0 && lane < ncta) {
+        const uint32_t bar = saddr(&S.bar[1 + b]);
+        if (lane == 0) rbar_expect(bar, (uint32_t)ncta * (32u + 4u * (uint32_t)C.cp));
+        const uint32_t dst = mapa(saddr(&S.red[b][rank][0]), lane);
+        const uint32_t dbar = mapa(bar, lane);
+        st_async_d2(dst, t[0], t[1], dbar);
+        st_async_d2(dst + 16, t[2], 0.0, dbar);
+        const uint32_t cdst = mapa(saddr(C.red() + ((size_t)b * ncta + rank) * C.cp), lane);
+        for (int q = 0; q < C.cp / 4; q++) st_async_f4(cdst + 16u * q, reinterpret_cast<const float4*>(C.part())[q], dbar);
+    }
+    const bool ok = res_wait(S, saddr(&S.bar[1 + b]), (nred >> 1) & 1u);
+    nred++;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        if (fp32) {
+            float a = 0.f;
+#pragma unroll
+            for (int c = 0; c < CS_RES_MAX_CL; c++)
+                if (c < ncta) a += (float)S.red[b][c][i];
+            v[i] = (double)a;
+        } else {
+            double a = 0.0;
+#pragma unroll
+            for (int c = 0; c < CS_RES_MAX_CL; c++)
+                if (c < ncta) a += S.red[b][c][i];
+            v[i] = a;
+        }
+    }
+    return ok;
+}
+
 // CTA-wide sums of two values in FP64, in a fixed order (warp butterfly, then warp partials in
 // warp order); every thread returns the same sums.  Ends with a barrier, so S.wsum is free again.
 __device__ __forceinline__ void cta_sum2(ResShared& S, double& a, double& b) {
@@ -301,7 +429,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
     const int ncta = (int)cl.num_blocks();
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
     const int cap = B.res_cap, halo0 = B.res_halo0;
     const float* sm_panels = reinterpret_cast<const float*>(cs_res_smem);
     float4* su = reinterpret_cast<float4*>(cs_res_smem + (size_t)cap * CS_PANEL_FLOATS * sizeof(float));
@@ -383,6 +511,36 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
         const uint32_t my_send = snd0 + tid < snd1 ? __ldg(&B.rsend[snd0 + tid]) : 0u;
         const uint32_t halo_bytes = (uint32_t)B.rhalo[tb + rank] * 16u;
 
+        // coarse-space correction (uniform over the cluster): its shared-memory region, this
+        // CTA's rows of the inverse coarse matrix, this thread's segment and, for the lanes of
+        // warp 1 that sum segments, their slot ranges
+        const int4 cinfo = B.rcoarse[sh.topo];
+        const bool coarse = P.coarse && P.cheb_degree >= 3 && B.rcheb[tb + rank] && cinfo.x == B.res_cnc &&
+                            cinfo.x > 0 && B.cvalid[idx] && nw >= 2;
+#define C CoarseSm(cs_res_smem + B.res_coff, B.res_cnc, B.res_ck)
+        // the segment masks of this CTA's warps (tb = topology x (CS_RES_MAX_CL + 1))
+#define WMASKS (B.rwmask + (tb / (CS_RES_MAX_CL + 1)) * CS_RES_MAX_CL * CS_RES_MAX_WARPS + rank * CS_RES_MAX_WARPS)
+        int cseg = 0;  // this lane's segment run, the warps holding its segment (cluster_sum3c)
+        // this thread's entry of the coarse vectors in a buffer of C.red (q = tid, the common case)
+        const int coff = coarse && tid < C.nc ? C.off(tid) : 0;
+        if (coarse) {
+            const float* src = B.cinv + (size_t)idx * B.res_cnc * B.res_cnc + (size_t)rank * C.k3 * C.nc;
+            for (int i = tid; i < C.k3 * C.nc; i += blockDim.x) C.ai()[i] = __ldcg(src + i);
+            for (int i = tid; i < C.nc; i += blockDim.x) C.s64(ncta)[i] = 0.0;
+            const int myseg = live ? B.ragg[sh.row2slot_off + row] - rank * B.res_ck : -1;
+            // this lane's run of equal segments (consecutive lanes; -1: no row)
+            const unsigned same = __match_any_sync(0xffffffffu, myseg);
+            cseg = (__ffs(same) - 1) | ((lane == 31 || !((same >> (lane + 1)) & 1u)) ? 32 : 0) |
+                   ((live ? myseg + 1 : 0) << 8);
+            if (w == 1 && lane < C.k3) {
+                // the warps whose rows include this lane's segment (the gather of cluster_sum3c)
+                int wk = 0;
+                for (int j = 0; j < nw; j++) wk |= ((__ldg(&WMASKS[j]) >> (lane / 3)) & 1) << j;
+                cseg |= wk << 16;
+            }
+        }
+        // bit 6 of cseg: the buffer of C.red holding the last coarse vector received
+
         float Pi[9];
         float e[3] = {0.f, 0.f, 0.f}, r[3] = {0.f, 0.f, 0.f}, u[3], wv[3], p[3] = {0.f, 0.f, 0.f},
               sv3[3] = {0.f, 0.f, 0.f};
@@ -404,7 +562,9 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
         double inv_gam = 0.0, inv_ga = 0.0;
         float alpha = 0.f, beta = 0.f;
         int iters = 0, sweeps = 0, sweep_iters = 0, flags = 0, trips = 0;
-        int phase = P.warm ? PH_RES : PH_INIT;
+        // with the coarse correction every solve starts with an FP64 residual: its reduction
+        // carries the coarse residual R r that the first preconditioner application needs
+        int phase = (P.warm || coarse) ? PH_RES : PH_INIT;
         bool ok = true;
 
         // q = A_loc x over this CTA's own rows (the strip's diagonal block of A), x in `buf`
@@ -415,6 +575,48 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                 row_times_u<false>(sm_panels + (size_t)lp * CS_PANEL_FLOATS, width, cw, buf, halo0, lane, q[0], q[1], q[2]);
             else
                 row_times_u<false>(B.A + (size_t)gp * CS_PANEL_FLOATS, width, cw, buf, halo0, lane, q[0], q[1], q[2]);
+        };
+        // ce = this CTA's rows of A_c^-1 times the coarse residual (a warp per row, lanes over
+        // the columns, butterfly sum: a fixed order)
+        auto coarse_matvec = [&]() {
+            const float* ai = C.ai();
+            const float* r32 = C.r32();
+            // rows j and j + nw together (their loads in flight at once), columns fully unrolled
+            for (int j = w; j < C.k3; j += 2 * nw) {
+                const int j1 = j + nw;
+                float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+                for (int n = 0; n < 6; n++) {
+                    const int t = lane + 32 * n;
+                    if (t < C.nc) {
+                        const float rt = r32[t];
+                        a0 = fmaf(ai[j * C.nc + t], rt, a0);
+                        if (j1 < C.k3) a1 = fmaf(ai[j1 * C.nc + t], rt, a1);
+                    }
+                }
+                a0 = rwarp_sum(a0);
+                if (lane == 0) C.ce()[j] = a0;
+                if (j1 < C.k3) {
+                    a1 = rwarp_sum(a1);
+                    if (lane == 0) C.ce()[j1] = a1;
+                }
+            }
+        };
+        // The coarse images of the CG recurrences, replicated in every CTA: with s = w + beta s
+        // and the next iteration's r -= alpha s, R s = R w + beta R s and R r -= alpha R s
+        // (R w from the reduction just done); R r is what the next preconditioner application
+        // reads.  An FP64 residual replaces R r exactly (PH_RES).
+        auto coarse_step = [&](double beta_c, double alpha_c) {
+            double* s64 = C.s64(ncta);
+            double* r64 = C.r64(ncta);
+            const float* red = C.red() + (size_t)((cseg >> 6) & 1) * ncta * C.cp;  // R w of the last CG reduction
+            for (int q = tid; q < C.nc; q += blockDim.x) {
+                const double sq = (double)red[q == tid ? coff : C.off(q)] + beta_c * s64[q];
+                s64[q] = sq;
+                const double rq = r64[q] - alpha_c * sq;
+                r64[q] = rq;
+                C.r32()[q] = (float)rq;
+            }
         };
         // Strip-local Chebyshev preconditioner: the largest eigenvalue of P^-1 A_loc by power
         // iteration from a hashed +-1 vector (the first barrier also covers the panel copy),
@@ -513,7 +715,18 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     v[0] = r0 * r0 + r1 * r1 + r2 * r2;
                     v[1] = q0 * q0 + q1 * q1 + q2 * q2;
                 }
-                ok = cluster_sum3(S, rank, ncta, nred, v, false);
+                if (coarse) {
+                    // the coarse residual R r of the replaced r travels with the norms
+                    ok = cluster_sum3c(S, rank, ncta, nred, v, false, r, live, cseg, reinterpret_cast<float*>(su_alt), C);
+                    const float* red = C.red() + (size_t)((nred - 1) & 1u) * ncta * C.cp;
+                    for (int q = tid; q < C.nc; q += blockDim.x) {
+                        const float rq = red[q == tid ? coff : C.off(q)];
+                        C.r64(ncta)[q] = (double)rq;
+                        C.r32()[q] = rq;
+                    }
+                } else {
+                    ok = cluster_sum3(S, rank, ncta, nred, v, false);
+                }
                 if (!ok) break;
                 const double res = sqrt(v[0]);
                 resnorm = res;
@@ -525,6 +738,14 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                         flags |= CS_IF_WARM_REJECTED;
                         res0 = bn;
                         phase = PH_INIT;
+                        if (coarse) {
+                            // r = b and its coarse residual come from one more residual of dv = 0
+                            if (live) {
+#pragma unroll
+                                for (int c = 0; c < 3; c++) B.dv64[3 * g + c] = 0.0;
+                            }
+                            phase = PH_RES;
+                        }
                         continue;
                     }
                 }
@@ -581,6 +802,8 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     float4* const buf = (k & 1) ? su : su_alt;
                     if (live) buf[myslot] = make_float4(u[0], u[1], u[2], 0.f);
                     __syncthreads();
+                    // the coarse correction of this CTA's aggregates, read after the next barrier
+                    if (coarse && k == 1) coarse_matvec();
                     float q[3], t[3];
                     local_spmv(buf, q);
 #pragma unroll
@@ -592,6 +815,19 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                         d[c] = ca * d[c] + cb * t[c];
                         u[c] += d[c];
                     }
+                }
+            }
+            if (coarse) {
+                if (cdeg < 3) {
+                    // this CTA's spectrum bound failed (block-Jacobi): barriers of its own
+                    __syncthreads();
+                    coarse_matvec();
+                    __syncthreads();
+                }
+                // u = C r + R^T A_c^-1 R r: the additive coarse-space correction
+                if (live) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) u[c] += C.ce()[3 * (((cseg >> 8) & 0xff) - 1) + c];
                 }
             }
             if (live) su[myslot] = make_float4(u[0], u[1], u[2], 0.f);
@@ -627,7 +863,13 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     v[2] = (double)(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
                 }
             }
-            ok = cluster_sum3(S, rank, ncta, nred, v, fp32);
+            if (coarse) {
+                // R w travels with the dot products (the coarse recurrences below)
+                ok = cluster_sum3c(S, rank, ncta, nred, v, fp32, wv, live, cseg, reinterpret_cast<float*>(su_alt), C);
+                cseg = (cseg & ~64) | (int)(((nred - 1) & 1u) << 6);
+            } else {
+                ok = cluster_sum3(S, rank, ncta, nred, v, fp32);
+            }
             if (!ok) break;
             const double gnew = v[0], dnew = v[1];
             rr = v[2];
@@ -657,6 +899,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                         alpha = (float)alpha_d;
                         inv_gam = 1.0 / gam;
                         inv_ga = 1.0 / (gam * alpha_d);
+                        if (coarse) coarse_step((double)bc, alpha_d);
                         phase = PH_CG;
                         continue;
                     }
@@ -691,6 +934,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     p[c] = u[c];
                     sv3[c] = wv[c];
                 }
+                if (coarse) coarse_step(0.0, alpha_d);
                 phase = PH_CG;
                 continue;
             }
@@ -738,6 +982,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                 p[c] = __fmaf_rn(beta, p[c], u[c]);
                 sv3[c] = __fmaf_rn(beta, sv3[c], wv[c]);
             }
+            if (coarse) coarse_step((double)beta, alpha_d);
             if (mixed) {
                 inv_gam = 1.0 / gam;
                 inv_ga = 1.0 / (gam * alpha_d);
@@ -769,5 +1014,114 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
         }
         if (!ok) break;
     }
+#undef C
+#undef WMASKS
     cl.sync();  // no CTA leaves while another may still address its shared memory
+}
+
+// Coarse matrix of each resident sheet for the coarse-space correction of the solve above:
+// A_c = R A R^T, where R sums the rows of each aggregate (a segment of a CTA's strip) per
+// component, so block (a, b) of A_c is the sum of the stored blocks A_ij with row i in
+// aggregate a and column j in aggregate b.  The loader lists those blocks per pair (a, b) in
+// slot order; a warp sums a pair, lane l taking the blocks l, l + 32, ... in order, and a
+// butterfly combines the lanes (a fixed order: deterministic, no atomics).  A_c is SPD (A is,
+// and R has full row rank), so Gauss-Jordan elimination inverts it in place in shared memory
+// without pivoting, in FP32: per pivot one FMA sweep over every entry with the pivot row and
+// column read from copies (two buffers), then the pivot row and column themselves.  The inverse, symmetrised,
+// is stored per work item for the resident kernel, which applies its CTA's rows each CG
+// iteration.  A non-positive or non-finite pivot marks the work item's coarse matrix invalid
+// and the solve runs without the correction.  One CTA per resident work item; dynamic shared
+// memory (nc + 4) x nc floats.
+static_assert(3 * CS_COARSE_AGGS <= 6 * 32, "the elimination's column loop covers at most 192 columns");
+
+__global__ void __launch_bounds__(CS_COARSE_THREADS) cs_coarse_setup_kernel(Batch B) {
+    const DevParams P = *B.params;
+    if (P.solver != CS_SOLVER_AUTO_DEV || P.cheb_degree < 3 || !P.coarse) return;  // uniform
+    const int idx = blockIdx.x;
+    if (idx >= B.n_resident) return;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+    const SheetDesc sh = B.sheets[B.rlist[idx]];
+    const int4 ci = B.rcoarse[sh.topo];
+    const int nc = ci.x;
+    if (nc == 0 || nc > B.res_cnc) {
+        if (tid == 0) B.cvalid[idx] = 0;
+        return;
+    }
+    float* M = reinterpret_cast<float*>(cs_res_smem);
+    float* colb = M + nc * nc;   // [2][nc] pivot columns
+    float* rowb = colb + 2 * nc;  // [2][nc] pivot rows
+    for (int i = tid; i < nc * nc; i += blockDim.x) M[i] = 0.f;
+    __syncthreads();
+    for (int q = ci.z + w; q < ci.w; q += nw) {
+        const int4 pr = B.cpair[q];
+        float acc[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int k = pr.z + lane; k < pr.w; k += 32) {
+            const int slot = __ldg(&B.ccontrib[k]);
+            const float* pk = B.A + (size_t)(sh.panel_off + slot / CS_SLICE) * CS_PANEL_FLOATS;
+            const int l = slot % CS_SLICE;
+            const float4 a0 = __ldg(reinterpret_cast<const float4*>(pk) + l);
+            const float4 a1 = __ldg(reinterpret_cast<const float4*>(pk + 128) + l);
+            const float a8 = __ldg(pk + 256 + l);
+            acc[0] += a0.x; acc[1] += a0.y; acc[2] += a0.z;
+            acc[3] += a0.w; acc[4] += a1.x; acc[5] += a1.y;
+            acc[6] += a1.z; acc[7] += a1.w; acc[8] += a8;
+        }
+#pragma unroll
+        for (int i = 0; i < 9; i++) acc[i] = rwarp_sum(acc[i]);
+        if (lane == 0) {
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) M[(3 * pr.x + i) * nc + 3 * pr.y + j] = acc[3 * i + j];
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < nc; i += blockDim.x) {
+        colb[i] = M[i * nc];
+        rowb[i] = M[i];
+    }
+    __syncthreads();
+    bool ok = true;
+    for (int k = 0; k < nc; k++) {
+        const float* cb = colb + (k & 1) * nc;
+        const float* rb = rowb + (k & 1) * nc;
+        float* cn = colb + ((k + 1) & 1) * nc;
+        float* rn = rowb + ((k + 1) & 1) * nc;
+        const float piv = rb[k];  // every thread reads the same value: a uniform decision
+        if (!(piv > 0.f) || !(piv < 3.0e38f)) {
+            ok = false;
+            break;
+        }
+        const float ip = 1.f / piv;
+        // a_ij <- a_ij - a_ik a_kj / p everywhere (one FMA per entry, no branches); then the
+        // pivot column (a_ik <- -a_ik / p) and row (a_kj <- a_kj / p, a_kk <- 1/p)
+        for (int i = w; i < nc; i += nw) {
+            const float c = cb[i];
+            float* Mi = M + i * nc;
+#pragma unroll
+            for (int n = 0; n < 6; n++) {
+                const int j = lane + 32 * n;
+                if (j < nc) Mi[j] = fmaf(-c, rb[j] * ip, Mi[j]);
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < nc; i += blockDim.x) {
+            M[i * nc + k] = i == k ? ip : -cb[i] * ip;
+            if (i != k) M[k * nc + i] = rb[i] * ip;
+        }
+        __syncthreads();
+        // the next step's pivot row and column
+        if (k + 1 < nc)
+            for (int i = tid; i < nc; i += blockDim.x) {
+                cn[i] = M[i * nc + k + 1];
+                rn[i] = M[(k + 1) * nc + i];
+            }
+        __syncthreads();
+    }
+    // written out symmetrised
+    float* out = B.cinv + (size_t)idx * B.res_cnc * B.res_cnc;
+    if (ok)
+        for (int i = w; i < nc; i += nw)
+            for (int j = lane; j < nc; j += 32) out[i * nc + j] = 0.5f * (M[i * nc + j] + M[j * nc + i]);
+    if (tid == 0) B.cvalid[idx] = ok ? 1 : 0;
 }

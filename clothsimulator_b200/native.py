@@ -77,7 +77,7 @@ class StepParams(ctypes.Structure):
         ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double), ("max_iters", ctypes.c_int),
         ("sweep_cap", ctypes.c_int), ("precision", ctypes.c_int), ("warm_start", ctypes.c_int),
         ("advance", ctypes.c_int), ("use_graph", ctypes.c_int), ("solver", ctypes.c_int),
-        ("precond_degree", ctypes.c_int),
+        ("precond_degree", ctypes.c_int), ("coarse", ctypes.c_int),
     ]
 
 
@@ -231,7 +231,7 @@ def material_desc(spec: dict) -> MaterialDesc:
 
 def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, inner_tol=1e-2, max_iters=2000,
                 sweep_cap=0, precision=PREC_MIXED, warm_start=WARM_ZERO, advance=1, use_graph=1,
-                solver=0, precond_degree=1) -> StepParams:
+                solver=0, precond_degree=1, coarse=1) -> StepParams:
     p = StepParams()
     p.dt = dt
     for i in range(3):
@@ -247,6 +247,7 @@ def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, in
     p.use_graph = use_graph
     p.solver = solver
     p.precond_degree = precond_degree
+    p.coarse = coarse
     return p
 
 

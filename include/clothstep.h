@@ -96,6 +96,10 @@ typedef struct cs_step_params {
                                  Chebyshev polynomial of that degree in the block-Jacobi-scaled
                                  matrix of each CTA's strip of rows (no exchange between CTAs).
                                  The batched loop always uses block-Jacobi. */
+    int coarse;               /* cluster-resident solver with the Chebyshev preconditioner: 1 adds
+                                 a coarse-space correction (one constant per component on each of
+                                 a few geometric segments of every CTA's strip, the coarse matrix
+                                 inverted per sheet and step), 0 leaves it out */
 } cs_step_params;
 
 #define CS_PRECOND_MAX_DEGREE 15

@@ -121,7 +121,9 @@ def test_reference_material_files_batch(ctx_factory):
 
 def test_reference_material_files_step_positions(ctx_factory):
     """A full step (v += dv, x += dt v) of the three material sheets against the reference CPU
-    path's state after its step: x within 1e-5 of the step's displacement, v within the dv bar."""
+    path's state after its step: v - v0 within the dv bar; x differs from the reference's by no
+    more than dt times the difference of the velocities plus one FP32 rounding of x (the
+    reference's FP32 LL^T carries its own error into both, largest for the stiff paper)."""
     g = np.load(GOLDEN_MATERIALS)
     scene, sheets = golden_material_sheets(g)
     ctx = ctx_factory(sheets)
@@ -132,8 +134,9 @@ def test_reference_material_files_step_positions(ctx_factory):
     for i, s in enumerate(sheets):
         name = str(g["names"][i])
         xi, vi = x[i * n:(i + 1) * n], v[i * n:(i + 1) * n]
-        disp = g[f"m{i}_x1"].astype(np.float64) - s["x"]
-        assert np.linalg.norm(xi - g[f"m{i}_x1"]) <= 1e-4 * np.linalg.norm(disp) + 1e-7 * np.sqrt(xi.size), name
+        dt = float(g[f"m{i}_params"][0])
+        dvel = np.linalg.norm(vi.astype(np.float64) - g[f"m{i}_v1"])
+        assert np.linalg.norm(xi.astype(np.float64) - g[f"m{i}_x1"]) <= 1.01 * dt * dvel + 1.2e-7 * np.sqrt(xi.size), name
         exact = fp64_solve(s, g[f"m{i}_params"])
         ref_err = rel(g[f"m{i}_dv"], exact)
         assert rel(vi - s["v"], g[f"m{i}_v1"] - s["v"]) < max(1e-5, 1.5 * ref_err) + 1e-6, name

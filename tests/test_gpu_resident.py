@@ -254,3 +254,75 @@ def test_chebyshev_falls_back_on_thin_strips(ctx_factory):
         assert stats.converged == 3
         res.append((ctx.get_dv().copy(), ctx.instance_stats()[0].copy()))
     assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+# Coarse-space correction (coarse=1 with the Chebyshev preconditioner): each CTA's strip cut
+# into geometric segments, one coarse unknown per (segment, component), the coarse matrix
+# R A R^T inverted per sheet and step; an additive SPD term, so the solve must still meet the
+# FP64-checked tolerance and match the direct solve, in fewer iterations.
+
+def test_coarse_correction_matches_oracle_and_cuts_iterations(ctx_factory):
+    scene = scenes.windy_batch(5, 64, seed=301)
+    scene.sheets += scenes.windy_batch(2, 48, seed=302).sheets
+    ctx = ctx_factory(scene.sheets)
+    assert ctx.solver_info()["resident_sheets"] == len(scene.sheets)
+    x0, v0 = initial_state(scene)
+    it = {}
+    for coarse in (0, 1):
+        ctx.set_state(x0, v0)
+        stats, _ = ctx.step(params_for(scene, precond_degree=3, coarse=coarse))
+        assert stats.converged == len(scene.sheets)
+        it[coarse], rr, fl = ctx.instance_stats()
+        assert np.all(rr <= 1e-10)
+        for s, dv in zip(scene.sheets, split_dv(ctx, scene)):
+            assert rel(dv, oracle_dv(scene, s)) < 1e-6
+    print("CG iterations without / with the coarse correction:", it[0].tolist(), it[1].tolist())
+    assert it[1].sum() <= 0.8 * it[0].sum(), (it[1], it[0])
+
+
+def test_coarse_correction_deterministic_and_guarded(ctx_factory):
+    scene = scenes.windy_batch(4, 64, seed=311)
+    ctx = ctx_factory(scene.sheets)
+    x0, v0 = initial_state(scene)
+    out = []
+    for _ in range(2):
+        ctx.set_state(x0, v0)
+        ctx.step(params_for(scene, tol=1e-6, precond_degree=3, coarse=1))
+        out.append((ctx.get_dv().copy(), ctx.instance_stats()[0].copy()))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    # a warm start worse than the zero guess is discarded: the solve restarts from dv = 0
+    ctx.set_state(x0, v0)
+    ctx.set_warm_start(np.full((ctx.n, 3), 1e3, np.float32))
+    stats, _ = ctx.step(params_for(scene, precond_degree=3, coarse=1, warm_start=native.WARM_GIVEN))
+    it, rr, fl = ctx.instance_stats()
+    assert stats.converged == 4 and stats.warm_rejected == 4 and np.all(fl & 2) and np.all(rr <= 1e-10)
+    for s, dv in zip(scene.sheets, split_dv(ctx, scene)):
+        assert rel(dv, oracle_dv(scene, s)) < 1e-6
+    # the exact solution as the warm start needs no iteration
+    ctx.set_warm_start(ctx.get_dv())
+    ctx.set_state(x0, v0)
+    stats, _ = ctx.step(params_for(scene, tol=1e-6, precond_degree=3, coarse=1, warm_start=native.WARM_GIVEN))
+    assert stats.converged == 4 and stats.max_iters == 0 and stats.warm_rejected == 0
+
+
+def test_coarse_correction_plain_fp32(ctx_factory):
+    scene = scenes.windy_batch(3, 64, seed=321)
+    ctx = ctx_factory(scene.sheets)
+    stats, _ = ctx.step(params_for(scene, tol=1e-6, precision=native.PREC_PLAIN_FP32, precond_degree=3, coarse=1),
+                        allow_unconverged=True)
+    it, rr, fl = ctx.instance_stats()
+    assert np.all(it > 0) and np.all(rr < 1e-3)
+    assert np.array_equal((fl & 1) > 0, rr <= 1e-6)
+
+
+def test_coarse_flag_inert_without_chebyshev(ctx_factory):
+    """With block-Jacobi (degree 1) the coarse flag changes nothing, bit for bit."""
+    scene = scenes.windy_batch(2, 64, seed=331)
+    ctx = ctx_factory(scene.sheets)
+    x0, v0 = initial_state(scene)
+    res = []
+    for coarse in (0, 1):
+        ctx.set_state(x0, v0)
+        ctx.step(params_for(scene, precond_degree=1, coarse=coarse))
+        res.append((ctx.get_dv().copy(), ctx.instance_stats()[0].copy()))
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
