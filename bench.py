@@ -1,20 +1,31 @@
 """Benchmark of the implicit cloth step on B200.
 
-Workload (default): 1,024 sheets of 64x64 quads (4,326,400 nodes), top edge pinned, per-sheet
-horizontal wind, stretching log-U[10, 500] N/m and bending log-U[1e-6, 1e-3] N m through the
-material multipliers, dt = 1/100 s: the learned-warm-start configuration, which fits one GPU.
-One step = assembly + batched PCG to an FP64-checked relative residual of 1e-6 for every sheet
-+ v += dv, x += dt v, with the state resident in HBM.
+Workloads (--workload; the default is the headline):
+  windy1024x64   1,024 sheets of 64x64 quads (4,326,400 nodes), top edge pinned, per-sheet
+                 horizontal wind, stretching log-U[10, 500] N/m and bending log-U[1e-6, 1e-3] N m
+                 through the material multipliers, dt = 1/100 s: the learned-warm-start
+                 configuration, the largest that fits one GPU, and the one the metric is quoted on;
+  hang32         one 32x32 hanging sheet, 200 steps;
+  precision256   one 256x256 sheet, one step, solved to 1e-6 (mixed and plain FP32) and 1e-10;
+  uneven512      512 sheets of 16..128 quads a side, 1-4 corners pinned, 100 steps;
+  irregular1000  one 1,000x1,000 jittered sheet with random diagonals (1,002,001 nodes), wind,
+                 50 steps, the windy network as warm start.
+One step = assembly + PCG to an FP64-checked relative residual of 1e-6 for every sheet +
+v += dv, x += dt v, with the state resident in HBM.
 
 Metric: node-steps/s (sum over sheets of nodes x steps / device time).  The line reports the
-mixed-precision solver with its warm start (`value`: cluster-resident solve, strip-local
-Chebyshev preconditioner of degree `--precond-degree`, reliable updates) and, in `arms`, the
-same solver from other starts and with block-Jacobi, and plain FP32 PCG from a zero guess on
-the same GPU.  `--impl reference` times the reference's CPU path for this
-workload (the reference's own force code compiled from its sources + FP32 sparse Cholesky).
+mixed-precision solver (`value`: cluster-resident solve where a sheet fits, strip-local Chebyshev
+preconditioner of degree --precond-degree with the coarse-space correction, reliable updates; the
+workload's warm start) and, in `arms`, the same solver without the coarse correction, with
+block-Jacobi, from other starts, at the tolerance that meets the dv bound, and plain FP32 PCG from
+a zero guess on the same GPU, each with its dv error against an FP64 solve of its own system on
+sampled sheets.  `--impl reference` times the reference's CPU path for the workload (the
+reference's own force code compiled from its sources + FP32 sparse Cholesky).
 
-Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-       torchrun --nproc-per-node N bench.py --gpus N   (one rank per GPU, sheets per rank fixed)
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
+       torchrun --nproc-per-node N bench.py --gpus N [--partition]
+         (one rank per GPU; each rank its own copy of the workload (weak scaling), or with
+          --partition one workload's sheets split across the ranks (strong scaling))
 """
 from __future__ import annotations
 
@@ -38,27 +49,42 @@ METRIC = "node-steps/s @ rel.res 1e-6: learned+mixed-prec batched PCG vs plain F
 UNIT = "node-steps/s"
 
 
-def parse():
+WORKLOADS = ("windy1024x64", "hang32", "precision256", "uneven512", "irregular1000")
+
+
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=None, help="timed steps (default: 10, or the workload's own "
+                    "step count when it is smaller than 10 seconds of work: hang32 200, uneven512 100, "
+                    "irregular1000 50, precision256 1)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--sheets", type=int, default=1024)
-    ap.add_argument("--nq", type=int, default=64)
+    ap.add_argument("--workload", default="windy1024x64", choices=WORKLOADS)
+    ap.add_argument("--sheets", type=int, default=None, help="windy workload: sheets (default 1,024)")
+    ap.add_argument("--nq", type=int, default=64, help="windy workload: quads per side")
     ap.add_argument("--tol", type=float, default=1e-6)
-    ap.add_argument("--warm", default="learned", choices=["previous", "zero", "learned"])
+    ap.add_argument("--dv-tol", type=float, default=1e-7,
+                    help="the tolerance of the arm that meets the dv bound of 1e-6 against an FP64 solve")
+    ap.add_argument("--warm", default=None, choices=["previous", "zero", "learned"],
+                    help="the warm start of the headline arm (default: learned for the windy and irregular "
+                         "workloads, previous dv for the others)")
     ap.add_argument("--solver", default="auto", choices=["auto", "batched"],
                     help="auto: sheets that fit a cluster's shared memory are solved cluster-resident")
     ap.add_argument("--precond-degree", type=int, default=3,
                     help="cluster-resident solver's preconditioner: 1 block-Jacobi, odd 3..15 a strip-local "
                          "Chebyshev polynomial of that degree (the batched loop always uses block-Jacobi)")
+    ap.add_argument("--no-coarse", action="store_true", help="headline arm without the coarse-space correction")
+    ap.add_argument("--partition", action="store_true",
+                    help="with several ranks: split one workload's sheets across them, balanced by stored blocks "
+                         "(strong scaling), per-sheet statistics all-gathered after each step")
     ap.add_argument("--train-sheets", type=int, default=256, help="sheets of the training trajectories")
     ap.add_argument("--train-steps", type=int, default=24, help="recorded steps per training trajectory")
     ap.add_argument("--epochs", type=int, default=16)
     ap.add_argument("--weights", default="", help="load trained warm-start weights instead of training")
-    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 arm")
+    ap.add_argument("--no-plain", action="store_true", help="skip the comparison arms")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-dv-check", action="store_true", help="skip the dv errors of the arms")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--detect", default="", choices=["", "windy", "stacked", "folded", "crossing"],
                     help="time proximity detection, the step and the collision step on a contact workload "
@@ -68,7 +94,27 @@ def parse():
     ap.add_argument("--host-loop", action="store_true",
                     help="launch the solve loop from the host instead of the CUDA graph (profilers cannot "
                          "see kernels inside a graph with conditional nodes)")
-    return ap.parse_args()
+    args = ap.parse_args(argv)
+    spec = workload_spec(args.workload)
+    if args.steps is None:
+        args.steps = spec["steps"]
+    if args.warm is None:
+        args.warm = spec["warm"]
+    if args.sheets is None:
+        args.sheets = 1024
+    return args
+
+
+def workload_spec(name: str) -> dict:
+    """Timed steps by default, the headline arm's warm start, and whether the workload is one
+    sheet (its CPU baseline then times a smaller instance of the same scene)."""
+    return {
+        "windy1024x64": {"steps": 10, "warm": "learned", "single": False},
+        "hang32": {"steps": 200, "warm": "previous", "single": True},
+        "precision256": {"steps": 1, "warm": "zero", "single": True},
+        "uneven512": {"steps": 100, "warm": "previous", "single": False},
+        "irregular1000": {"steps": 50, "warm": "learned", "single": True},
+    }[name]
 
 
 def dist_env():
@@ -79,9 +125,10 @@ def dist_env():
 
 
 class RankGroup:
-    """One process per GPU (torchrun).  Sheets are independent, so ranks exchange no data:
-    the group carries only the barriers around the timed region and the max over ranks of
-    the device times (gloo, host scalars)."""
+    """One process per GPU (torchrun).  Sheets are independent, so ranks exchange no data during
+    the solve: the group carries the barriers around the timed region and the max over ranks of
+    the device times (gloo, host scalars); an NCCL group beside it carries the warm start's
+    gradient all-reduce and, with --partition, the all-gather of the per-sheet statistics."""
 
     def __init__(self, timeout_s: float = 300.0):
         import datetime
@@ -117,14 +164,20 @@ class RankGroup:
         self.dist.all_reduce(t)
         return t.numpy()
 
+    def nccl_group(self):
+        """An NCCL group of all ranks beside the gloo group of the host scalars (created once)."""
+        if not self.dist:
+            return None
+        if getattr(self, "_nccl", None) is None:
+            self._nccl = self.dist.new_group(backend="nccl")
+        return self._nccl
+
     def device_allreduce(self):
         """An in-place sum of CUDA tensors over the ranks: NCCL over NVLink (a group of its own
         beside the gloo group of the host scalars)."""
         if not self.dist:
             return None
-        if getattr(self, "_nccl", None) is None:
-            self._nccl = self.dist.new_group(backend="nccl")
-        grp = self._nccl
+        grp = self.nccl_group()
         return lambda t: self.dist.all_reduce(t, group=grp)
 
     def close(self):
@@ -221,8 +274,20 @@ def scenes_mod():
     return scenes
 
 
-def workload(args, rank):
-    return scenes_mod().windy_batch(args.sheets, args.nq, seed=eval_seed(rank))
+def workload(args, rank, small: bool = False):
+    """The scene a rank steps (each rank its own seed: weak scaling).  small=True: a smaller
+    instance of a single-sheet scene for the CPU baseline's bounded sample."""
+    sc = scenes_mod()
+    seed = eval_seed(rank)
+    if args.workload == "windy1024x64":
+        return sc.windy_batch(args.sheets, args.nq, seed=seed)
+    if args.workload == "hang32":
+        return sc.hang(32, seed=seed)
+    if args.workload == "precision256":
+        return sc.precision_sheet(128 if small else 256, seed=seed)
+    if args.workload == "uneven512":
+        return sc.uneven_batch(512, seed=seed)
+    return sc.large_irregular(200 if small else 1000, seed=seed)
 
 
 def cpu_baseline(scene, seconds: float, which: str = "ref", threads: int = 1, n_steps: int = 1):
@@ -264,14 +329,14 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    scene = workload(args, 0)
+    scene = workload(args, 0, small=workload_spec(args.workload)["single"])
     threads = os.cpu_count() or 1
     vals = []
     for _ in range(max(1, args.warmup)):
         cpu_baseline(scene, 2.0, "ref", threads)
     samples = []
     for _ in range(args.steps):
-        r = cpu_baseline(scene, args.cpu_seconds / max(1, args.steps) * 4, "ref", threads)
+        r = cpu_baseline(scene, max(0.2, 4.0 * args.cpu_seconds / max(1, args.steps)), "ref", threads)
         vals.append(r["value"])
         samples.append(r["sample"])
     value = statistics.median(vals)
@@ -279,90 +344,163 @@ def run_reference(args):
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": scene.name, "sheets": len(scene.sheets), "nodes": scene.n_nodes, "tol": args.tol},
+        "config": {"workload": args.workload, "sheets": len(workload_sheets(args)), "tol": args.tol},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": r["kind"], "sample": samples[-1]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
 
 
+def workload_sheets(args):
+    """The sheets of the workload at full size (the reference arm's config names them)."""
+    return workload(args, 0).sheets
+
+
+def train_warm_start(args, group, local):
+    """The learned warm start: trained on the device on separate seeded windy trajectories (the
+    evaluated seeds are held out; data parallel over the ranks when there are several), or loaded
+    from --weights.  Returns (weights, training record)."""
+    from clothsimulator_b200 import native
+
+    rank, world = group.rank, group.world
+    t0 = time.perf_counter()
+    if args.weights:
+        weights = np.fromfile(args.weights, dtype=np.float32)
+        info = {"source": args.weights}
+    else:
+        tscene = scenes_mod().windy_batch(args.train_sheets, args.nq, seed=train_seed(rank))
+        tctx = native.Context(local)
+        tctx.load(tscene.sheets)
+        tctx.mlp_init(args.train_steps, 1)  # the same initial weights on every rank
+        tp = native.step_params(tscene.dt, tscene.gravity, tscene.handle_stiffness, tol=1e-7, max_iters=8000)
+        for _ in range(2):
+            tctx.step(tp, allow_unconverged=True)
+            tp.warm_start = native.WARM_PREVIOUS
+        for t in range(args.train_steps):
+            tctx.assemble(tp)
+            tctx.mlp_record(t, 0)
+            tctx.step(tp, allow_unconverged=True)
+            tctx.mlp_record(t, 1)
+        if world == 1:
+            tctx.mlp_fit_normalization(args.train_steps)
+            losses = tctx.mlp_train(args.train_steps, args.epochs, lr=1e-3, sheets_per_batch=32, seed=3)
+        else:
+            # data parallel: every rank trains on its own trajectories, gradients summed over
+            # NCCL and averaged, normalisation from the moments summed over the ranks
+            from clothsimulator_b200 import training
+
+            losses = training.train_data_parallel(tctx, args.train_steps, args.train_sheets, args.epochs, 1e-3,
+                                                  32, 3, allreduce_sum=group.device_allreduce(), world=world,
+                                                  sum_host=group.sum_host)
+        weights = tctx.mlp_get_weights()
+        tctx.close()
+        info = {"sheets": args.train_sheets, "steps": args.train_steps, "epochs": args.epochs,
+                "trajectories": f"windy{args.train_sheets}x{args.nq}, seeds disjoint from the evaluated workload",
+                "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
+        if world > 1:
+            digest = float(np.float64(weights).sum())
+            info["data_parallel"] = {"ranks": world, "gradients": "NCCL all-reduce, averaged",
+                                     "weights_identical": group.max(digest) == -group.max(-digest)}
+    info["seconds"] = time.perf_counter() - t0
+    return weights, info
+
+
+def dv_errors(sheets, scene, local, params, weights=None, n_sample=8):
+    """dv error of one solver arm: max over a seeded sample of the sheets of
+    ||dv - dv_64|| / ||dv_64||, where dv_64 is an FP64 direct solve (SciPy) of the system the GPU
+    assembled for that sheet, one step from the sheet's initial state (a context of its own with
+    the sampled sheets; the sheets are independent, so their systems are the same as in the
+    whole batch)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+
+    from clothsimulator_b200 import native
+
+    rng = np.random.default_rng(5)
+    pick = sorted(rng.choice(len(sheets), min(n_sample, len(sheets)), replace=False).tolist())
+    sub = [sheets[k] for k in pick]
+    ctx = native.Context(local).load(sub)
+    if weights is not None:
+        ctx.mlp_init(0, 0)
+        ctx.mlp_set_weights(weights)
+    x0 = np.concatenate([s["x"] for s in sub])
+    v0 = np.concatenate([s["v"] for s in sub])
+    p = native.StepParams.from_buffer_copy(params)
+    p.advance = 0
+    if p.warm_start == native.WARM_PREVIOUS:
+        p.warm_start = native.WARM_ZERO  # one step from the initial state: no previous dv
+    ctx.set_state(x0, v0)
+    ctx.step(p, allow_unconverged=True)
+    dv = ctx.get_dv().reshape(-1)
+    ctx.assemble(p)
+    rp, ci, val, b = ctx.system()
+    worst, off = 0.0, 0
+    for s in sub:
+        n = s["x"].shape[0]
+        lo, hi = rp[off], rp[off + n]
+        A = sp.bsr_matrix((val[lo:hi].astype(np.float64), ci[lo:hi] - off, rp[off:off + n + 1] - lo),
+                          shape=(3 * n, 3 * n)).tocsc()
+        exact = spl.spsolve(A, b[3 * off:3 * (off + n)].astype(np.float64))
+        worst = max(worst, float(np.linalg.norm(dv[3 * off:3 * (off + n)] - exact) / np.linalg.norm(exact)))
+        off += n
+    ctx.close()
+    return {"dv_err_vs_fp64": worst, "dv_err_sheets": len(sub)}
+
+
 def run_ours(args):
     import torch
 
-    from clothsimulator_b200 import native
+    from clothsimulator_b200 import native, partition
 
     group = RankGroup()
     rank, world, local = group.rank, group.world, group.local
     torch.cuda.set_device(local)
-    scene = workload(args, rank)
+    spec = workload_spec(args.workload)
+    if args.partition and world > 1:
+        # strong scaling: one workload (rank 0's seed), its sheets split across the ranks
+        full = workload(args, 0)
+        blocks = partition.sheet_blocks(full.sheets)
+        parts = partition.partition_sheets(blocks, world)
+        scene = scenes_mod().Scene(full.name, [full.sheets[k] for k in parts[rank]], dt=full.dt, steps=full.steps,
+                                   gravity=full.gravity, handle_stiffness=full.handle_stiffness)
+        part_info = {"ranks": world, "sheets_per_rank": [len(p) for p in parts],
+                     "blocks_imbalance": partition.imbalance(blocks, parts)}
+    else:
+        scene = workload(args, rank)
+        parts, part_info = None, None
     ctx = native.Context(local)
     ctx.load(scene.sheets)
     sizes = ctx.sizes
     N = sizes[0]
+    total_nodes = int(group.sum_host(np.array([float(N)]))[0])
     x0 = np.concatenate([s["x"] for s in scene.sheets])
     v0 = np.concatenate([s["v"] for s in scene.sheets])
     stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
-
     barrier = group.barrier
     max_over_ranks = group.max
 
-    # Learned warm start: trained on the device on separate seeded trajectories (the
-    # evaluated workload's seeds are held out), or loaded from --weights.
-    train_info = None
+    weights, train_info = None, None
     if args.warm == "learned":
-        t0 = time.perf_counter()
-        if args.weights:
-            weights = np.fromfile(args.weights, dtype=np.float32)
-            train_info = {"source": args.weights}
-        else:
-            tscene = scenes_mod().windy_batch(args.train_sheets, args.nq, seed=train_seed(rank))
-            tctx = native.Context(local)
-            tctx.load(tscene.sheets)
-            tctx.mlp_init(args.train_steps, 1)  # the same initial weights on every rank
-            tp = native.step_params(tscene.dt, tscene.gravity, tscene.handle_stiffness, tol=1e-7, max_iters=8000)
-            for _ in range(2):
-                tctx.step(tp, allow_unconverged=True)
-                tp.warm_start = native.WARM_PREVIOUS
-            for t in range(args.train_steps):
-                tctx.assemble(tp)
-                tctx.mlp_record(t, 0)
-                tctx.step(tp, allow_unconverged=True)
-                tctx.mlp_record(t, 1)
-            if world == 1:
-                tctx.mlp_fit_normalization(args.train_steps)
-                losses = tctx.mlp_train(args.train_steps, args.epochs, lr=1e-3, sheets_per_batch=32, seed=3)
-            else:
-                # data parallel: every rank trains on its own trajectories, gradients summed over
-                # NCCL and averaged, normalisation from the moments summed over the ranks
-                from clothsimulator_b200 import training
-
-                losses = training.train_data_parallel(tctx, args.train_steps, args.train_sheets, args.epochs, 1e-3,
-                                                      32, 3, allreduce_sum=group.device_allreduce(), world=world,
-                                                      sum_host=group.sum_host)
-            weights = tctx.mlp_get_weights()
-            tctx.close()
-            train_info = {"sheets": args.train_sheets, "steps": args.train_steps, "epochs": args.epochs,
-                          "seeds": "disjoint from the evaluated workload",
-                          "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
-            if world > 1:
-                digest = float(np.float64(weights).sum())
-                train_info["data_parallel"] = {
-                    "ranks": world, "gradients": "NCCL all-reduce, averaged",
-                    "weights_identical": group.max(digest) == -group.max(-digest)}
-        train_info["seconds"] = time.perf_counter() - t0
+        weights, train_info = train_warm_start(args, group, local)
         ctx.mlp_init(0, 0)
         ctx.mlp_set_weights(weights)
 
     solver_code = {"auto": native.SOLVER_AUTO, "batched": native.SOLVER_BATCHED}
+    warm_code = {"previous": native.WARM_PREVIOUS, "zero": native.WARM_ZERO, "learned": native.WARM_LEARNED}
 
-    def timed_arm(precision, warm, solver, clocks=None, degree=args.precond_degree):
+    def arm_params(precision, solver, degree, coarse, tol):
+        return native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=tol, max_iters=20000,
+                                  precision=precision, warm_start=native.WARM_ZERO,
+                                  use_graph=0 if args.host_loop else 1, solver=solver_code[solver],
+                                  precond_degree=degree, coarse=coarse)
+
+    def timed_arm(precision, warm, solver, degree, coarse, tol, clocks=None):
         ctx.set_state(x0, v0)
-        p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol, max_iters=4000,
-                               precision=precision, warm_start=native.WARM_ZERO, use_graph=0 if args.host_loop else 1,
-                               solver=solver_code[solver], precond_degree=degree)
+        p = arm_params(precision, solver, degree, coarse, tol)
         for i in range(args.warmup):
             ctx.step(p, allow_unconverged=True)
             p.warm_start = warm
+        p.warm_start = warm
         c0 = ctx.counters()
         barrier()
         torch.cuda.synchronize()
@@ -384,11 +522,17 @@ def run_ours(args):
         barrier()
         ms = max_over_ranks(e0.elapsed_time(e1))
         c1 = ctx.counters()
-        # one untimed step with statistics for the report
+        # one untimed step with statistics for the report (and, with --partition, the whole
+        # workload's per-sheet statistics gathered from every rank)
         ctx.step(p, allow_unconverged=True)
         it, rr, fl = ctx.instance_stats()
+        if parts is not None:
+            g = partition.gather_stats({"iters": it, "rel_residual": rr, "flags": fl}, parts, sum(len(q) for q in parts),
+                                       partition.torch_all_gather(group.dist, group.nccl_group(),
+                                                                  torch.device("cuda", local)))
+            it, rr, fl = g["iters"], g["rel_residual"], g["flags"]
         return {
-            "value": aggregate_value(N, args.steps, world, ms),
+            "value": total_nodes * args.steps / (ms / 1e3),
             "ms": ms,
             "ms_per_step": ms / args.steps,
             "launches": c1["launches"] - c0["launches"],
@@ -397,47 +541,70 @@ def run_ours(args):
             "converged_frac": float(np.mean((fl & 1) > 0)),
             "warm_rejected_frac": float(np.mean((fl & 2) > 0)),
             "max_relres": float(rr.max()),
-        }
+        }, p
 
     keys = ("value", "ms_per_step", "iters_mean", "iters_max", "converged_frac", "warm_rejected_frac", "max_relres")
-    warm_mode = {"previous": native.WARM_PREVIOUS, "zero": native.WARM_ZERO, "learned": native.WARM_LEARNED}[args.warm]
+    deg = args.precond_degree
+    coarse = 0 if args.no_coarse else 1
     clocks = {}
-    best = timed_arm(native.PREC_MIXED, warm_mode, args.solver, clocks)
-    node_steps = N * args.steps * world
+    best, best_p = timed_arm(native.PREC_MIXED, warm_code[args.warm], args.solver, deg, coarse, args.tol, clocks)
     value = best["value"]
     head = f"mixed_{args.warm}_{args.solver}"
-    arms = {head: dict({k: best[k] for k in keys}, precond_degree=args.precond_degree if args.solver == "auto" else 1)}
+    arms = {head: dict({k: best[k] for k in keys}, precond_degree=deg if args.solver == "auto" else 1,
+                       coarse=coarse, tol=args.tol)}
+    arm_params_used = {head: best_p}
     if not args.no_plain:
-        # the plain FP32 arms keep block-Jacobi (the reference's solver structure); the mixed arms
-        # use --precond-degree, with block-Jacobi beside them
-        deg = args.precond_degree
-        for name, prec, warm, solver, d in [
-                ("mixed_zero_auto", native.PREC_MIXED, native.WARM_ZERO, "auto", deg),
-                ("mixed_previous_auto", native.PREC_MIXED, native.WARM_PREVIOUS, "auto", deg),
-                ("mixed_learned_auto_block_jacobi", native.PREC_MIXED, native.WARM_LEARNED, "auto", 1),
-                ("mixed_zero_auto_block_jacobi", native.PREC_MIXED, native.WARM_ZERO, "auto", 1),
-                ("plain_fp32_zero_auto", native.PREC_PLAIN_FP32, native.WARM_ZERO, "auto", 1),
-                ("mixed_previous_batched", native.PREC_MIXED, native.WARM_PREVIOUS, "batched", 1),
-                ("plain_fp32_zero_batched", native.PREC_PLAIN_FP32, native.WARM_ZERO, "batched", 1)]:
-            if name in arms or (warm == native.WARM_LEARNED and args.warm != "learned") or (d == deg and name.endswith("block_jacobi")):
+        # the plain FP32 arms keep block-Jacobi and the zero guess (the reference's solver
+        # structure); the mixed arms use --precond-degree, without and with the coarse correction,
+        # with block-Jacobi beside them, and at --dv-tol (the tolerance whose dv meets 1e-6)
+        P, M = native.PREC_PLAIN_FP32, native.PREC_MIXED
+        W = warm_code[args.warm]
+        cand = [("mixed_zero_auto", M, native.WARM_ZERO, "auto", deg, 1, args.tol),
+                ("mixed_previous_auto", M, native.WARM_PREVIOUS, "auto", deg, 1, args.tol),
+                (f"mixed_{args.warm}_auto_no_coarse", M, W, "auto", deg, 0, args.tol),
+                (f"mixed_{args.warm}_auto_block_jacobi", M, W, "auto", 1, 0, args.tol),
+                (f"mixed_{args.warm}_auto_tol{args.dv_tol:g}", M, W, "auto", deg, 1, args.dv_tol),
+                ("plain_fp32_zero_auto", P, native.WARM_ZERO, "auto", 1, 0, args.tol),
+                ("mixed_previous_batched", M, native.WARM_PREVIOUS, "batched", 1, 0, args.tol),
+                ("plain_fp32_zero_batched", P, native.WARM_ZERO, "batched", 1, 0, args.tol)]
+        if args.workload == "precision256":
+            cand.append(("mixed_zero_auto_tol1e-10", M, native.WARM_ZERO, "auto", deg, 1, 1e-10))
+        # the arms each workload reports (a single large sheet is solved by the batched loop,
+        # where the preconditioner options do not apply)
+        keep = {"windy1024x64": None,
+                "uneven512": {"mixed_zero_auto", "no_coarse", "block_jacobi", "tol", "plain_fp32_zero_auto",
+                              "plain_fp32_zero_batched", "mixed_previous_batched"},
+                "hang32": {"mixed_zero_auto", "no_coarse", "block_jacobi", "plain_fp32_zero_auto"},
+                "precision256": {"no_coarse", "plain_fp32_zero_auto", "tol1e-10"},
+                "irregular1000": {"mixed_zero_auto", "plain_fp32_zero_batched"}}[args.workload]
+        for name, prec, warm, solver, d, co, tol in cand:
+            if name in arms or (name.endswith("block_jacobi") and deg == 1):
                 continue
-            r = timed_arm(prec, warm, solver, degree=d)
-            arms[name] = dict({k: r[k] for k in keys}, precond_degree=d if solver == "auto" else 1)
+            if keep is not None and not any(name == k or name.endswith(k) or f"_{k}" in name for k in keep):
+                continue
+            r, pr = timed_arm(prec, warm, solver, d, co, tol)
+            arms[name] = dict({k: r[k] for k in keys}, precond_degree=d if solver == "auto" else 1, coarse=co, tol=tol)
+            arm_params_used[name] = pr
     plain = arms.get("plain_fp32_zero_batched")
 
+    # dv error of every arm against an FP64 solve of its own assembled system (sampled sheets)
+    if not args.no_dv_check and rank == 0 and max(s["x"].shape[0] for s in scene.sheets) <= 300000:
+        for name, pr in arm_params_used.items():
+            use_w = weights if pr.warm_start == native.WARM_LEARNED else None
+            arms[name].update(dv_errors(scene.sheets, scene, local, pr, use_w))
+
     # Rooflines, timed live on the context's stream (cs_profile_kernels).  The dominant kernel
-    # of the default (resident) solver is cs_resident_pcg_kernel: its algorithmic bytes per
-    # launch are the CG iterations it ran times the bytes one SpMV iteration moves (stored
-    # blocks x 40 B + nodes x 48 B, the same per-iteration figure as the batched SpMV's), plus
-    # the Chebyshev preconditioner's strip-local SpMVs at the same rate over the strip-local
-    # blocks; the resident kernel serves them from shared memory, so its DRAM traffic is far
-    # below them.
-    prof = ctx.profile_kernels(native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol,
-                                                  max_iters=4000, precond_degree=args.precond_degree), reps=5)
+    # of the step (resident solver, when sheets are resident): algorithmic bytes per launch =
+    # CG iterations x (stored blocks x 40 B + nodes x 48 B), the per-iteration bytes of a
+    # streaming PCG (the same figure as the batched SpMV's); the kernel serves them from
+    # shared memory, so `roofline_smem` sets the shared-memory bytes it moves against the
+    # shared-memory bandwidth of the SMs it runs on.
+    prof = ctx.profile_kernels(arm_params(native.PREC_MIXED, args.solver, deg, coarse, args.tol), reps=3)
     it_res, _, _ = ctx.instance_stats()
     nnzb = sizes[6]
     peaks = measured_peaks()
     peak = peaks["hbm_gbs"] if peaks else 6650.0
+    src = "measured" if peaks else "fallback"
 
     def traffic_per_launch(name, units):
         path = os.path.join(ROOT, "profiles", name)
@@ -451,32 +618,45 @@ def run_ours(args):
     spmv_achieved = spmv_bytes / (prof["spmv"] * 1e-3) / 1e9
     roof_spmv = {"bound": "hbm", "achieved": spmv_achieved, "peak": peak, "unit": "GB/s", "frac": spmv_achieved / peak,
                  "traffic": traffic_per_launch("cs_spmv_kernel_windy128x64_traffic.json", N),
-                 "kernel": "cs_spmv_kernel", "bytes_per_launch": spmv_bytes, "ms_per_launch": prof["spmv"]}
-    roof_res = None
-    if prof["resident_solve"] > 0:
-        per_sheet = np.array([(s_["fx"].shape[0], s_["x"].shape[0]) for s_ in scene.sheets], np.float64)
-        nnzb_sheet = nnzb / len(scene.sheets)  # identical topologies in this workload
-        # a CG iteration is one full SpMV plus, with the strip-local Chebyshev preconditioner,
-        # (degree - 1) SpMVs over the strip-local blocks; each solve adds the power iterations
-        rb = ctx.resident_blocks()
-        local_frac = rb["local_blocks"] / max(rb["blocks"], 1)
-        local_spmvs = it_res * (args.precond_degree - 1) + rb["power_iters"] if args.precond_degree >= 3 else 0 * it_res
-        res_bytes = float(np.sum(it_res * (nnzb_sheet * 40 + per_sheet[:, 1] * 48)
-                                 + local_spmvs * (local_frac * nnzb_sheet * 40 + per_sheet[:, 1] * 48)))
-        res_achieved = res_bytes / (prof["resident_solve"] * 1e-3) / 1e9
-        roof_res = {"bound": "hbm", "achieved": res_achieved, "peak": peak, "unit": "GB/s",
-                    "frac": res_achieved / peak,
-                    "traffic": traffic_per_launch("cs_resident_pcg_kernel_windy32x64_traffic.json", len(scene.sheets)),
-                    "kernel": "cs_resident_pcg_kernel", "bytes_per_launch": res_bytes,
-                    "ms_per_launch": prof["resident_solve"], "cg_iterations_per_launch": int(it_res.sum()),
-                    "local_spmvs_per_launch": int(np.sum(local_spmvs)), "local_block_frac": local_frac,
-                    "note": "per-iteration operands served from shared memory: achieved is the rate at which the "
-                            "solve consumes SpMV bytes (the CG SpMVs and the Chebyshev preconditioner's strip-local "
-                            "SpMVs), against the HBM roofline of the streaming formulation; above 1 means faster than "
-                            "any solve that streams the system from HBM could run"}
-    roofline = roof_res if (roof_res and args.solver == "auto") else roof_spmv
+                 "kernel": "cs_spmv_kernel", "bytes_per_launch": spmv_bytes, "ms_per_launch": prof["spmv"],
+                 "peak_source": src}
+    roof_res, roof_smem = None, None
+    info = ctx.solver_info()
+    if prof["resident_solve"] > 0 and args.solver == "auto":
+        per_sheet = np.array([(s["x"].shape[0]) for s in scene.sheets], np.float64)
+        blocks_sheet = partition.sheet_blocks(scene.sheets).astype(np.float64)
+        resident = np.array([True] * len(scene.sheets)) if info["resident_sheets"] == len(scene.sheets) else None
+        if resident is not None:
+            res_bytes = float(np.sum(it_res * (blocks_sheet * 40 + per_sheet * 48)))
+            ms_res = prof["resident_solve"]
+            res_achieved = res_bytes / (ms_res * 1e-3) / 1e9
+            roof_res = {"bound": "hbm", "achieved": res_achieved, "peak": peak, "unit": "GB/s",
+                        "frac": res_achieved / peak,
+                        "traffic": traffic_per_launch("cs_resident_pcg_kernel_windy32x64_traffic.json", len(scene.sheets)),
+                        "kernel": "cs_resident_pcg_kernel", "bytes_per_launch": res_bytes, "ms_per_launch": ms_res,
+                        "cg_iterations_per_launch": int(it_res.sum()), "peak_source": src,
+                        "note": "algorithmic bytes = CG iterations x (stored blocks x 40 B + nodes x 48 B), what a "
+                                "streaming PCG would move; the kernel reads them from shared memory (roofline_smem)"}
+            # shared-memory bytes: per CG iteration the full SpMV (36 B of block values + 16 B of
+            # the vector per stored block) and (degree - 1) strip-local SpMVs over the strip-local
+            # blocks; per solve the power iterations
+            rb = ctx.resident_blocks()
+            local_frac = rb["local_blocks"] / max(rb["blocks"], 1)
+            cheb = deg >= 3
+            smem_bytes = float(np.sum(it_res * blocks_sheet * 52 * (1 + (deg - 1) * local_frac * cheb)
+                                      + cheb * rb["power_iters"] * local_frac * blocks_sheet * 52))
+            sm_mhz = clocks.get("sm_mhz") or 1965.0
+            sms = info["clusters"] * info["ctas_per_cluster"]
+            smem_peak = 128.0 * sms * sm_mhz * 1e6 / 1e9
+            smem_achieved = smem_bytes / (ms_res * 1e-3) / 1e9
+            roof_smem = {"bound": "smem", "achieved": smem_achieved, "peak": smem_peak, "unit": "GB/s",
+                         "frac": smem_achieved / smem_peak, "kernel": "cs_resident_pcg_kernel",
+                         "bytes_per_launch": smem_bytes, "sms": sms, "sm_mhz": sm_mhz,
+                         "peak_source": "128 B per clock per SM x SMs the kernel runs on x sampled SM clock"}
+    roofline = roof_res if roof_res else roof_spmv
 
     # end to end through the C ABI with pinned host buffers: H2D of x, v, step, D2H of x, v
+    node_steps = total_nodes * args.steps
     hx = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
     hv = torch.empty((N, 3), dtype=torch.float32, pin_memory=True)
     hx.numpy()[:] = x0
@@ -486,15 +666,13 @@ def run_ours(args):
 
     px = C.cast(hx.data_ptr(), fp)
     pv = C.cast(hv.data_ptr(), fp)
-    p = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol, max_iters=4000,
-                           precision=native.PREC_MIXED, warm_start=native.WARM_ZERO, use_graph=0 if args.host_loop else 1,
-                           solver=solver_code[args.solver], precond_degree=args.precond_degree)
+    p = arm_params(native.PREC_MIXED, args.solver, deg, coarse, args.tol)
     ctx.set_state(x0, v0)
     for i in range(args.warmup):
         ctx.check(ctx.lib.cs_set_state(ctx.h, px, pv))
         ctx.step(p, allow_unconverged=True)
         ctx.check(ctx.lib.cs_get_state(ctx.h, px, pv))
-        p.warm_start = warm_mode
+        p.warm_start = warm_code[args.warm]
     barrier()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -514,23 +692,27 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        cpu = cpu_baseline(scene, args.cpu_seconds, "ref", 1)
+        cpu = cpu_baseline(workload(args, 0, small=spec["single"]), args.cpu_seconds, "ref", 1)
 
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": best["ms"] / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "strong" if parts is not None else "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
             "config": {
-                "workload": scene.name, "sheets": len(scene.sheets), "nq": args.nq, "nodes_per_gpu": N,
-                "nnzb_per_gpu": nnzb, "tol": args.tol,
+                "workload": args.workload if args.workload != "windy1024x64" else scene.name,
+                "sheets": len(scene.sheets), "nodes_per_gpu": N, "nnzb_per_gpu": nnzb, "tol": args.tol,
                 "scheme": "mixed FP32 PCG, FP64 dot products, FP64 residual replacements (reliable updates)",
                 "warm_start": args.warm,
                 "solver": args.solver,
-                "precond": ("strip-local Chebyshev degree %d over block-Jacobi" % args.precond_degree
-                            if args.precond_degree >= 3 and args.solver == "auto" else "block-Jacobi"),
-                "l2": "inputs larger than L2 (system matrix %.2f GB per GPU)" % (sizes[3] * 36 / 1e9),
-                "parallelism": f"sheets x{world} (no collective on the data path)",
+                "precond": ("strip-local Chebyshev degree %d over block-Jacobi%s" %
+                            (deg, " + coarse-space correction" if coarse else "")
+                            if deg >= 3 and args.solver == "auto" else "block-Jacobi"),
+                "l2": "inputs larger than L2 (system matrix %.2f GB per GPU)" % (sizes[3] * 36 / 1e9)
+                      if sizes[3] * 36 > 126e6 else "system matrix %.3f GB per GPU: within L2" % (sizes[3] * 36 / 1e9),
+                "parallelism": (f"one workload's sheets split over {world} ranks by stored blocks" if parts is not None
+                                else f"sheets x{world} (no collective on the data path)"),
                 "launch": "host loop" if args.host_loop else "CUDA graph with a device-driven while loop",
             },
             "iters_mean": best["iters_mean"], "iters_max": best["iters_max"],
@@ -539,11 +721,14 @@ def run_ours(args):
             "speedup_vs_plain_fp32": (value / plain["value"]) if plain else None,
             "plain_fp32_note": "plain FP32 PCG (block Jacobi, zero guess, batched loop streaming the system from "
                                "HBM) stops on its own FP32 recursive residual; converged_frac is the share of "
-                               "sheets whose FP64-checked residual meets tol",
+                               "sheets whose FP64-checked residual meets tol; dv_err_vs_fp64 is against an FP64 "
+                               "direct solve of the arm's own assembled system on sampled sheets",
             "warm_start_training": train_info,
-            "solver_plan": ctx.solver_info(),
-            "roofline": dict(roofline, peak_source="measured" if peaks else "fallback"),
-            "roofline_batched_spmv": dict(roof_spmv, peak_source="measured" if peaks else "fallback"),
+            "partition": part_info,
+            "solver_plan": info,
+            "roofline": roofline,
+            "roofline_smem": roof_smem,
+            "roofline_batched_spmv": roof_spmv,
             "kernel_ms": prof,
             "e2e": e2e,
             "cpu_baseline": cpu,

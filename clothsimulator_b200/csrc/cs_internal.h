@@ -147,6 +147,8 @@ struct DevParams {
     int solver;            // CS_SOLVER_AUTO_DEV: resident sheets on the cluster kernel; BATCHED: loop only
     int cheb_degree;       // resident solver: 1 block-Jacobi; odd >= 3 strip-local Chebyshev of that degree
     int coarse;            // resident solver with the Chebyshev preconditioner: 1 adds the coarse-space correction
+    int n_motions;         // transformations of this step (cs_step_params.transformations)
+    float motion[CS_MAX_MOTIONS][CS_TRANSFORM_FLOATS];
 };
 
 // One proximity as seen by one sheet it touches (cs_set_proximities): node[i] is a batch
@@ -171,6 +173,7 @@ struct Batch {
     float *x = nullptr, *v = nullptr, *dv = nullptr, *mass = nullptr;
     float* x0 = nullptr;     // positions at the start of the last step (Node::x0, Mesh.cu:226-231)
     float4* handle = nullptr;
+    int* handle_motion = nullptr;  // per node: the motion of its handle (-1: fixed)
     double* dv64 = nullptr;
     float* warm = nullptr;   // warm-start vector (previous dv or learned prediction)
     // faces

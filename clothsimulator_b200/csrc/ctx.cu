@@ -805,6 +805,8 @@ struct cs_ctx {
     // cluster-resident solver launch (resident.cu): CTAs per cluster, threads per CTA,
     // clusters in the persistent grid, dynamic shared memory per CTA
     int resCL = 0, resThreads = 0, resClusters = 0, resClustersMax = 0;
+    std::vector<int> handleNode;  // batch node of every handle, in load order (cs_set_handle_motions)
+    int maxHandleMotion = -1;     // largest motion a handle follows (-1: none)
     size_t resSmem = 0;
     std::vector<int> rlistAll;  // resident sheets before the proximity filter
     std::vector<int> rlistCur;  // resident sheets now
@@ -860,6 +862,8 @@ cs_status upload(cs_ctx* c, T** p, const std::vector<T>& h) {
 }
 
 void freeBatch(cs_ctx* c) {
+    c->handleNode.clear();
+    c->maxHandleMotion = -1;
     if (c->graphExec) cudaGraphExecDestroy(c->graphExec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->graphExecLearned) cudaGraphExecDestroy(c->graphExecLearned);
@@ -924,12 +928,17 @@ void launchSolvePrologue(cs_ctx* c) {
 }
 
 // Sheets that fit a cluster's shared memory: one persistent cluster per sheet at a time.
-void launchResident(cs_ctx* c) {
-    if (c->resClusters <= 0) return;
-    // the coarse matrices of the resident sheets, formed and inverted for this step's systems
-    if (c->B.res_cnc > 0 && c->B.n_resident > 0)
+// The coarse matrices of the resident sheets, formed and inverted for this step's systems (the
+// kernel returns at once unless the step asks for the coarse correction).
+void launchCoarseSetup(cs_ctx* c) {
+    if (c->resClusters > 0 && c->B.res_cnc > 0 && c->B.n_resident > 0)
         cs_coarse_setup_kernel<<<c->B.n_resident, CS_COARSE_THREADS,
                                  (size_t)(c->B.res_cnc + 4) * c->B.res_cnc * sizeof(float), c->stream>>>(c->B);
+}
+
+void launchResident(cs_ctx* c, bool setup = true) {
+    if (c->resClusters <= 0) return;
+    if (setup) launchCoarseSetup(c);
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -1021,6 +1030,9 @@ DevParams toDev(const cs_step_params* p) {
     d.solver = p->solver == CS_SOLVER_BATCHED ? CS_SOLVER_BATCHED_DEV : CS_SOLVER_AUTO_DEV;
     d.cheb_degree = p->precond_degree >= 3 ? p->precond_degree : 1;
     d.coarse = p->coarse != 0;
+    d.n_motions = p->transformations ? std::min(std::max(p->n_transformations, 0), CS_MAX_MOTIONS) : 0;
+    for (int m = 0; m < d.n_motions; m++)
+        for (int k = 0; k < CS_TRANSFORM_FLOATS; k++) d.motion[m][k] = p->transformations[CS_TRANSFORM_FLOATS * m + k];
     return d;
 }
 
@@ -1407,6 +1419,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         for (int h = 0; h < d.n_handles; h++) {
             int i = d.handle_nodes[h];
             const float* p = d.handle_pos ? d.handle_pos + 3 * h : d.x + 3 * i;
+            c->handleNode.push_back(node_off + i);
             hd[i] = make_float4(p[0], p[1], p[2], hd[i].w + 1.0f);
         }
         hhandle.insert(hhandle.end(), hd.begin(), hd.end());
@@ -1480,6 +1493,8 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     UP(v, hv);
     UP(mass, hmass);
     UP(handle, hhandle);
+    UP(handle_motion, std::vector<int>(hhandle.size(), -1));
+    c->maxHandleMotion = -1;
     UP(face_nodes, hface_nodes);
     UP(face_inv, hface_inv);
     UP(face_area, hface_area);
@@ -2210,6 +2225,34 @@ static cs_status validateParams(cs_ctx* c, const cs_step_params* p) {
         return fail(c, CS_ERR_INVALID_ARG, "precond_degree must be 0, 1 or odd up to CS_PRECOND_MAX_DEGREE");
     if (p->warm_start == CS_WARM_LEARNED && !c->mlpInit)
         return fail(c, CS_ERR_NOT_TRAINED, "learned warm start: no network (cs_mlp_init / cs_mlp_set_weights)");
+    const int nt = p->transformations ? p->n_transformations : 0;
+    if (nt < 0 || nt > CS_MAX_MOTIONS) return fail(c, CS_ERR_INVALID_ARG, "n_transformations must be 0..%d", CS_MAX_MOTIONS);
+    if (nt > 0 && !p->transformations) return fail(c, CS_ERR_INVALID_ARG, "null transformations");
+    for (int k = 0; k < nt * CS_TRANSFORM_FLOATS; k++)
+        if (!std::isfinite(p->transformations[k])) return fail(c, CS_ERR_INVALID_ARG, "non-finite transformation");
+    if (c->maxHandleMotion >= nt)
+        return fail(c, CS_ERR_INVALID_ARG, "a handle follows motion %d but the step has %d transformations",
+                    c->maxHandleMotion, nt);
+    return CS_OK;
+}
+
+cs_status cs_set_handle_motions(cs_ctx* c, const int32_t* motion, int n) {
+    if (!c || (n > 0 && !motion)) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    if (n != (int)c->handleNode.size())
+        return fail(c, CS_ERR_INVALID_ARG, "%d motions given for %d handles", n, (int)c->handleNode.size());
+    std::vector<int> per(c->B.N, -1);
+    int mx = -1;
+    for (int h = 0; h < n; h++) {
+        if (motion[h] < -1 || motion[h] >= CS_MAX_MOTIONS)
+            return fail(c, CS_ERR_INVALID_ARG, "handle %d: motion %d out of range (-1..%d)", h, motion[h], CS_MAX_MOTIONS - 1);
+        per[c->handleNode[h]] = motion[h];  // a node's last handle, as for its target (cs_load_batch)
+        mx = std::max(mx, motion[h]);
+    }
+    CS_CUDA(cudaSetDevice(c->device));
+    CS_CUDA(cudaMemcpyAsync(c->B.handle_motion, per.data(), per.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    c->maxHandleMotion = mx;
     return CS_OK;
 }
 
@@ -2477,20 +2520,27 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
     ms[6] = timeIt(6);
     // one whole cluster-resident solve of every resident sheet from the zero guess (or the
     // warm start the parameters ask for); set-up launches untimed, the solve between events
-    ms[7] = 0.f;
+    ms[7] = ms[8] = 0.f;
     if (c->resClusters > 0) {
-        float acc = 0.f;
+        float acc = 0.f, accSetup = 0.f;
         for (int r = 0; r < reps; r++) {
             launchSolvePrologue(c);
             cudaEventRecord(c->ev0, c->stream);
-            launchResident(c);
+            launchCoarseSetup(c);
             cudaEventRecord(c->ev1, c->stream);
             cudaEventSynchronize(c->ev1);
             float t = 0.f;
             cudaEventElapsedTime(&t, c->ev0, c->ev1);
+            accSetup += t;
+            cudaEventRecord(c->ev0, c->stream);
+            launchResident(c, false);
+            cudaEventRecord(c->ev1, c->stream);
+            cudaEventSynchronize(c->ev1);
+            cudaEventElapsedTime(&t, c->ev0, c->ev1);
             acc += t;
         }
         ms[7] = acc / reps;
+        ms[8] = accSetup / reps;
     }
     CS_CUDA(cudaGetLastError());
     CS_CUDA(cudaStreamSynchronize(c->stream));

@@ -44,6 +44,18 @@ __device__ __forceinline__ f3 normalized(f3 a) { return dvd(a, nrm(a)); }
 __device__ __forceinline__ f3 cross(f3 a, f3 b) {
     return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
+
+// Transformation::applyToPoint (Transformation.cu:82-84) with Quaternion::rotate (Quaternion.cu:
+// 76-78) in the reference's FP32 order: s p + t with
+// rotate(p) = p (qs^2 - |qv|^2) + (2 qv)(qv . p) + (2 (qv x p)) qs.  T = {s, t (3), qs, qv (3)}.
+__device__ __forceinline__ f3 transform_point(const float* T, f3 p) {
+    const f3 qv = mk(T[5], T[6], T[7]);
+    const float qs = T[4];
+    const float n2 = qv.x * qv.x + qv.y * qv.y + qv.z * qv.z;
+    const float d = qv.x * p.x + qv.y * p.y + qv.z * p.z;
+    const f3 r = add(add(mulv(p, qs * qs - n2), mulv(scl(2.0f, qv), d)), mulv(scl(2.0f, cross(qv, p)), qs));
+    return add(scl(T[0], r), mk(T[1], T[2], T[3]));
+}
 __device__ __forceinline__ float clampf_(float x, float a, float b) { return x < a ? a : (x > b ? b : x); }
 __device__ __forceinline__ float maxf_(float a, float b) { return a > b ? a : b; }
 __device__ __forceinline__ float minf_(float a, float b) { return a < b ? a : b; }
@@ -494,7 +506,11 @@ __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
                 const int hc = (int)hd.w;
                 if (hc > 0) {
                     const f3 xr = ld3(B.x, row), vr = ld3(B.v, row);
-                    const f3 fh = mulv(scl(dt, sub(sub(mk(hd.x, hd.y, hd.z), xr), scl(dt, vr))), P.handle_stiffness);
+                    // the target: the handle's position at load, or a motion's transformation of it
+                    const int mo = B.handle_motion[row];
+                    const f3 target = mo >= 0 ? transform_point(B.params->motion[mo], mk(hd.x, hd.y, hd.z))
+                                              : mk(hd.x, hd.y, hd.z);
+                    const f3 fh = mulv(scl(dt, sub(sub(target, xr), scl(dt, vr))), P.handle_stiffness);
                     for (int t = 0; t < hc; t++) {
                         b0 += fh.x; b1 += fh.y; b2 += fh.z;
                     }

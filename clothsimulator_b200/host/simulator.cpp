@@ -104,6 +104,91 @@ Vec3 Transformation::rotate(const Vec3& x) const {
     return add(add(scale(qs_ * qs_ - dot(qv_, qv_), x), scale(2.0f * dot(qv_, x), qv_)), scale(2.0f * qs_, cross(qv_, x)));
 }
 Vec3 Transformation::applyToPoint(const Vec3& p) const { return add(scale(scaling_, rotate(p)), translation_); }
+void Transformation::raw(float out[CS_TRANSFORM_FLOATS]) const {
+    const float r[CS_TRANSFORM_FLOATS] = {scaling_, translation_.x, translation_.y, translation_.z, qs_, qv_.x, qv_.y, qv_.z};
+    std::copy(r, r + CS_TRANSFORM_FLOATS, out);
+}
+Vec3 Transformation::applyRaw(const float T[CS_TRANSFORM_FLOATS], const Vec3& p) {
+    const float qs = T[4];
+    const Vec3 qv = {T[5], T[6], T[7]};
+    const Vec3 r = add(add(scale(qs * qs - dot(qv, qv), p), scale(2.0f * dot(qv, p), qv)), scale(2.0f * qs, cross(qv, p)));
+    return add(scale(T[0], r), {T[1], T[2], T[3]});
+}
+
+// ---- Motion ---------------------------------------------------------------------------------
+
+namespace {
+using T8 = Motion::T8;
+T8 t8add(const T8& a, const T8& b) {
+    T8 r;
+    for (int k = 0; k < CS_TRANSFORM_FLOATS; k++) r[k] = a[k] + b[k];
+    return r;
+}
+T8 t8sub(const T8& a, const T8& b) {
+    T8 r;
+    for (int k = 0; k < CS_TRANSFORM_FLOATS; k++) r[k] = a[k] - b[k];
+    return r;
+}
+T8 t8mul(const T8& a, float s) {  // Transformation::operator*(float), Quaternion::operator*(float)
+    T8 r;
+    for (int k = 0; k < CS_TRANSFORM_FLOATS; k++) r[k] = a[k] * s;
+    return r;
+}
+// Transformation::operator/(float): scaling and the quaternion's scalar part divided, translation and
+// the quaternion's vector part multiplied by the reciprocal (Vector::operator/, Vector.cuh:126-132)
+T8 t8div(const T8& a, float s) {
+    const float inv = 1.0f / s;
+    T8 r;
+    for (int k = 0; k < CS_TRANSFORM_FLOATS; k++) r[k] = a[k] * inv;
+    r[0] = a[0] / s;
+    r[4] = a[4] / s;
+    return r;
+}
+T8 t8identity() { return {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}; }
+}  // namespace
+
+Motion::Motion(const Json& keyframes) {
+    for (const Json& k : keyframes.items()) {
+        t_.push_back(parseFloat(k["time"]));
+        T8 x;
+        Transformation(k["transform"]).raw(x.data());
+        x_.push_back(x);
+    }
+    if (t_.empty()) throw std::runtime_error("a motion needs keyframes");
+    if (t_[0] > 0) {
+        t_.insert(t_.begin(), 0.0f);
+        x_.insert(x_.begin(), t8identity());
+    }
+    n_ = (int)t_.size();
+    if (n_ < 2) throw std::runtime_error("a motion needs two keyframes (one may be the time-0 identity)");
+    for (int i = 1; i < n_; i++)
+        if (!(t_[i] > t_[i - 1])) throw std::runtime_error("motion keyframe times must increase");
+    v_.assign(n_, t8mul(t8identity(), 0.0f));
+    for (int i = 1; i < n_ - 1; i++) v_[i] = t8div(t8sub(x_[i + 1], x_[i - 1]), t_[i + 1] - t_[i - 1]);
+    coefficients();
+}
+
+void Motion::coefficients() {
+    const float dt = t_[index_ + 1] - t_[index_];
+    const T8 dx = t8sub(x_[index_ + 1], x_[index_]);
+    a_ = t8sub(t8mul(t8add(v_[index_ + 1], v_[index_]), dt), t8mul(dx, 2.0f));
+    b_ = t8sub(t8mul(dx, 3.0f), t8mul(t8add(v_[index_ + 1], t8mul(v_[index_], 2.0f)), dt));
+    c_ = t8mul(v_[index_], dt);
+    d_ = x_[index_];
+}
+
+Motion::T8 Motion::transformAt(float time) {
+    bool moved = false;
+    while (index_ < n_ - 1 && t_[index_ + 1] < time) {
+        index_++;
+        moved = true;
+    }
+    if (index_ == n_ - 1) return x_[n_ - 1];
+    if (moved) coefficients();
+    const float s = (time - t_[index_]) / (t_[index_ + 1] - t_[index_]);
+    const float s2 = s * s, s3 = s * s2;
+    return t8add(t8add(t8add(t8mul(a_, s3), t8mul(b_, s2)), t8mul(c_, s)), d_);
+}
 Vec3 Transformation::applyToVector(const Vec3& v) const { return rotate(v); }
 void Transformation::applyToUV(float u[2]) const {
     u[0] *= scaling_;
@@ -244,7 +329,6 @@ Cloth::Cloth(const Json& json, const Wind& sceneWind)
 }
 
 void Cloth::addHandles(const std::vector<int>& nodeIndices, int motionIndex) {
-    if (motionIndex > -1) throw std::runtime_error("handle motions are not provided (no \"motions\" support)");
     for (int n : nodeIndices) {
         if (n < 0 || n >= mesh_.nodes()) throw std::runtime_error("handle node " + std::to_string(n) + " out of range");
         Handle h;
@@ -288,8 +372,9 @@ static SolverOptions parseSolver(const Json& j) {
 }
 
 static void checkSupported(const Json& json) {
-    if (!json["motions"].isNull() && json["motions"].size() > 0)
-        throw std::runtime_error("\"motions\" are not provided: this implementation covers the implicit cloth step only");
+    if (json["motions"].isObject())
+        throw std::runtime_error("\"motions\" from a motion file (.mot, Simulator.cu:43-80) are not provided: give "
+                                 "keyframe arrays");
     if (!json["obstacles"].isNull() && (json["obstacles"].size() > 0 || json["obstacles"].type() == Json::String))
         throw std::runtime_error("\"obstacles\" are not provided: collisions are handled among cloths only");
     bool remeshingOff = false;
@@ -310,7 +395,9 @@ void describeScene(const std::string& path, long long counts[4]) {
         if (ci < 0 || ci >= (int)cloths.size()) throw std::runtime_error("handle cloth index out of range");
         std::vector<int> nodes;
         for (const Json& n : h["nodes"].items()) nodes.push_back(n.asInt());
-        cloths[ci].addHandles(nodes, parseInt(h["motion"], -1));
+        const int mi = parseInt(h["motion"], -1);
+        if (mi < -1 || mi >= (int)json["motions"].size()) throw std::runtime_error("handle motion index out of range");
+        cloths[ci].addHandles(nodes, mi);
     }
     counts[0] = (long long)cloths.size();
     for (Cloth& c : cloths) {
@@ -335,6 +422,8 @@ Simulator::Simulator(SimulationMode mode, const std::string& path, const std::st
     magic_ = Magic(json_["magic"]);
     clothFriction_ = parseFloat(json_["friction"], 0.6f);  // Simulator.cu:25
     solver_ = parseSolver(json_["solver"]);
+    for (const Json& m : json_["motions"].items()) motions_.emplace_back(m);
+    if ((int)motions_.size() > CS_MAX_MOTIONS) throw std::runtime_error("more than CS_MAX_MOTIONS motions");
     for (const Json& c : json_["cloths"].items()) cloths_.emplace_back(c, wind_);
     if (cloths_.empty()) throw std::runtime_error("scene has no cloths");
     for (const Json& h : json_["handles"].items()) {
@@ -342,7 +431,9 @@ Simulator::Simulator(SimulationMode mode, const std::string& path, const std::st
         if (ci < 0 || ci >= (int)cloths_.size()) throw std::runtime_error("handle cloth index out of range");
         std::vector<int> nodes;
         for (const Json& n : h["nodes"].items()) nodes.push_back(n.asInt());
-        cloths_[ci].addHandles(nodes, parseInt(h["motion"], -1));
+        const int mi = parseInt(h["motion"], -1);
+        if (mi < -1 || mi >= (int)motions_.size()) throw std::runtime_error("handle motion index out of range");
+        cloths_[ci].addHandles(nodes, mi);
     }
     loadBatch(device);
 }
@@ -388,6 +479,16 @@ void Simulator::loadBatch(int device) {
     }
     st = cs_load_batch(ctx_, mats.data(), (int)mats.size(), sheets.data(), (int)sheets.size());
     if (st != CS_OK) throw std::runtime_error(std::string("cs_load_batch: ") + cs_last_error(ctx_));
+    // handles that follow a motion (Simulator.cu:104-111)
+    std::vector<int32_t> motion;
+    bool moving = false;
+    for (const Cloth& c : cloths_)
+        for (const Handle& h : c.handles()) {
+            motion.push_back(h.motion);
+            moving |= h.motion > -1;
+        }
+    if (moving && cs_set_handle_motions(ctx_, motion.data(), (int)motion.size()) != CS_OK)
+        throw std::runtime_error(std::string("cs_set_handle_motions: ") + cs_last_error(ctx_));
     if (solver_.warmStart == CS_WARM_LEARNED) {
         std::vector<float> w(CS_MLP_PARAMS);
         std::ifstream in(solver_.network, std::ios::binary);
@@ -419,6 +520,8 @@ void Simulator::physicsStep() {
     p.precision = solver_.precision;
     p.precond_degree = solver_.precondDegree;
     p.coarse = solver_.coarse ? 1 : 0;
+    p.transformations = transforms_.empty() ? nullptr : transforms_.data();
+    p.n_transformations = (int)motions_.size();
     p.warm_start = nSteps_ > 1 || mode_ == ResumeOffline ? solver_.warmStart : CS_WARM_ZERO;
     if (solver_.warmStart == CS_WARM_LEARNED) p.warm_start = CS_WARM_LEARNED;
     p.advance = 1;
@@ -442,9 +545,19 @@ void Simulator::collisionStep() {
     if (st != CS_OK) throw std::runtime_error(std::string("cs_collision_step: ") + cs_last_error(ctx_));
 }
 
+void Simulator::updateTransformations() {
+    const float time = nSteps_ * dt_;
+    transforms_.assign(CS_TRANSFORM_FLOATS * motions_.size(), 0.0f);
+    for (size_t i = 0; i < motions_.size(); i++) {
+        const Motion::T8 t = motions_[i].transformAt(time);
+        std::copy(t.begin(), t.end(), transforms_.begin() + CS_TRANSFORM_FLOATS * i);
+    }
+}
+
 void Simulator::simulateStep() {
     if ((++nSteps_) % frameSteps_ == 0) nFrames_++;
     std::cout << "Frame [" << nFrames_ << "], Step [" << nSteps_ << "]:" << std::endl;
+    updateTransformations();
     physicsStep();
     std::cout << "Physics Step: " << stats_.ms / 1000.0 << "s (" << proximities_ << " proximities, " << stats_.max_iters
               << " CG iterations, relative residual " << stats_.max_rel_residual << ")";
@@ -508,6 +621,62 @@ void Simulator::start() {
 static std::string g_sim_error;
 
 extern "C" const char* cs_sim_last_error() { return g_sim_error.c_str(); }
+
+// The host layer's Transformation(json).applyToPoint and Motion(keyframes).computeTransformation
+// applied to points, for checking them against the reference's (json_text: a "transform" object,
+// or a "motions" keyframe array).  Return 0, or CS_ERR_INVALID_ARG with cs_sim_last_error.
+extern "C" int cs_transform_points(const char* json_text, int n, const double* p, double* out) {
+    try {
+        clothsim::Transformation t(clothsim::Json::parse(json_text));
+        for (int i = 0; i < n; i++) {
+            const clothsim::Vec3 q = t.applyToPoint({(float)p[3 * i], (float)p[3 * i + 1], (float)p[3 * i + 2]});
+            out[3 * i] = q.x;
+            out[3 * i + 1] = q.y;
+            out[3 * i + 2] = q.z;
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_sim_error = e.what();
+        return CS_ERR_INVALID_ARG;
+    }
+}
+
+extern "C" int cs_motion_points(const char* json_text, int n_times, const double* times, int n, const double* p,
+                                double* out, float* transforms) {
+    try {
+        clothsim::Motion m(clothsim::Json::parse(json_text));
+        for (int k = 0; k < n_times; k++) {
+            const clothsim::Motion::T8 t = m.transformAt((float)times[k]);
+            if (transforms) std::copy(t.begin(), t.end(), transforms + CS_TRANSFORM_FLOATS * k);
+            for (int i = 0; i < n; i++) {
+                const clothsim::Vec3 q = clothsim::Transformation::applyRaw(
+                    t.data(), {(float)p[3 * i], (float)p[3 * i + 1], (float)p[3 * i + 2]});
+                out[3 * (k * n + i)] = q.x;
+                out[3 * (k * n + i) + 1] = q.y;
+                out[3 * (k * n + i) + 2] = q.z;
+            }
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_sim_error = e.what();
+        return CS_ERR_INVALID_ARG;
+    }
+}
+
+// Reads an OBJ mesh as a cloth's mesh is read (Mesh::load, Mesh.cu:306-452: v, nv, vt, f with
+// a/b or plain indices, polygons fan-triangulated) and writes it as a frame (Mesh::save,
+// Mesh.cu:454-507).  Return 0, or CS_ERR_INVALID_ARG with cs_sim_last_error.
+extern "C" int cs_mesh_rewrite(const char* in_path, const char* out_path) {
+    try {
+        clothsim::Mesh m;
+        m.load(in_path, clothsim::Transformation(clothsim::Json()));
+        m.save(out_path);
+        return 0;
+    } catch (const std::exception& e) {
+        g_sim_error = e.what();
+        return CS_ERR_INVALID_ARG;
+    }
+}
 
 extern "C" int cs_scene_describe(const char* path, long long* counts) {
     try {

@@ -9,6 +9,7 @@
 #ifndef CLOTHSIM_HOST_SIMULATOR_HPP
 #define CLOTHSIM_HOST_SIMULATOR_HPP
 
+#include <array>
 #include <string>
 #include <vector>
 
@@ -28,6 +29,11 @@ public:
     Vec3 applyToPoint(const Vec3& p) const;
     Vec3 applyToVector(const Vec3& v) const;
     void applyToUV(float u[2]) const;
+    // the 8 values the C ABI takes (cs_step_params.transformations): scaling, translation (3),
+    // rotation quaternion (s, x, y, z)
+    void raw(float out[CS_TRANSFORM_FLOATS]) const;
+    // applyToPoint of a transformation given by those 8 values
+    static Vec3 applyRaw(const float T[CS_TRANSFORM_FLOATS], const Vec3& p);
 
 private:
     float scaling_ = 1.0f;
@@ -35,6 +41,24 @@ private:
     float qs_ = 1.0f;  // quaternion scalar part
     Vec3 qv_;          // quaternion vector part
     Vec3 rotate(const Vec3& x) const;
+};
+
+// Motion.cu:3-72: keyframes ("time", "transform") with a keyframe of the identity at time 0
+// added when the first is later, central-difference tangents (zero at the ends), and per segment
+// the cubic a s^3 + b s^2 + c s + d in Transformation arithmetic (Transformation.cu:22-69,
+// Quaternion.cu:23-63).  The segment index only advances, as the reference's does.
+class Motion {
+public:
+    using T8 = std::array<float, CS_TRANSFORM_FLOATS>;
+    explicit Motion(const Json& keyframes);
+    T8 transformAt(float time);  // Motion::computeTransformation (Motion.cu:57-72)
+
+private:
+    std::vector<float> t_;
+    std::vector<T8> x_, v_;
+    T8 a_{}, b_{}, c_{}, d_{};
+    int index_ = 0, n_ = 0;
+    void coefficients();  // Motion::updateCoefficients (Motion.cu:48-55)
 };
 
 // Wind.cu:3-7
@@ -142,11 +166,14 @@ private:
     int proximities_ = 0;
     cs_collision_stats collision_{};
     SolverOptions solver_;
+    std::vector<Motion> motions_;   // Simulator.cu:39-80 ("motions" keyframe arrays)
+    std::vector<float> transforms_; // the motions' transformations at the current step
     std::vector<Cloth> cloths_;
     cs_ctx* ctx_ = nullptr;
     cs_step_stats stats_{};
     void loadBatch(int device);
     void pullState();
+    void updateTransformations();  // Simulator.cu:565-569
 };
 
 // Parses a scene without a device (counts of cloths, nodes, faces, handles); throws on error.

@@ -39,7 +39,7 @@ EXPORTED = [
     "cs_mlp_train", "cs_mlp_gradient", "cs_mlp_predict", "cs_mlp_get_record", "cs_mlp_get_weights",
     "cs_mlp_set_weights", "cs_get_solver_info", "cs_set_proximities", "cs_detect_proximities",
     "cs_get_proximities", "cs_collision_step", "cs_mlp_moments", "cs_mlp_set_moments", "cs_mlp_gradient_device",
-    "cs_mlp_apply_gradient", "cs_get_resident_blocks",
+    "cs_mlp_apply_gradient", "cs_get_resident_blocks", "cs_set_handle_motions",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -78,6 +78,7 @@ class StepParams(ctypes.Structure):
         ("sweep_cap", ctypes.c_int), ("precision", ctypes.c_int), ("warm_start", ctypes.c_int),
         ("advance", ctypes.c_int), ("use_graph", ctypes.c_int), ("solver", ctypes.c_int),
         ("precond_degree", ctypes.c_int), ("coarse", ctypes.c_int),
+        ("transformations", ctypes.POINTER(ctypes.c_float)), ("n_transformations", ctypes.c_int),
     ]
 
 
@@ -156,6 +157,7 @@ def load_library() -> ctypes.CDLL:
         "cs_get_proximities": [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
         "cs_collision_step": [vp, ctypes.POINTER(CollisionParams), ctypes.POINTER(CollisionStats)],
         "cs_set_state": [vp, _fp, _fp],
+        "cs_set_handle_motions": [vp, _ip, ctypes.c_int],
         "cs_get_state": [vp, _fp, _fp],
         "cs_set_state_device": [vp, vp, vp],
         "cs_get_state_device": [vp, vp, vp],
@@ -248,6 +250,21 @@ def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, in
     p.solver = solver
     p.precond_degree = precond_degree
     p.coarse = coarse
+    p.transformations = None
+    p.n_transformations = 0
+    return p
+
+
+TRANSFORM_FLOATS = 8
+
+
+def set_transformations(p: StepParams, transforms) -> StepParams:
+    """The motions' transformations of one step into p: an (n, 8) array of scaling, translation
+    (3), rotation quaternion (s, x, y, z).  The array is kept alive on p."""
+    t = np.ascontiguousarray(np.asarray(transforms, np.float32).reshape(-1, TRANSFORM_FLOATS))
+    p._transforms = t
+    p.transformations = t.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    p.n_transformations = t.shape[0]
     return p
 
 
@@ -378,6 +395,11 @@ class Context:
                 "free": rec["free_mask"].copy(), "normal": rec["normal"].copy(), "w": rec["w"].copy(),
                 "mu": rec["mu"].copy(), "stiffness": rec["stiffness"].copy()}
 
+    def set_handle_motions(self, motion):
+        """The motion of every handle (-1: fixed), the sheets' handles in load order."""
+        m = _i32(motion)
+        self.check(self.lib.cs_set_handle_motions(self.h, m.ctypes.data_as(_ip), m.shape[0]))
+
     def set_state(self, x=None, v=None):
         xa = _f32(x) if x is not None else None
         va = _f32(v) if v is not None else None
@@ -457,10 +479,10 @@ class Context:
         self.check(self.lib.cs_device_pointers(self.h, ctypes.byref(x), ctypes.byref(v), ctypes.byref(dv)))
         return x.value, v.value, dv.value
 
-    KERNELS = ["face", "edge", "gather", "spmv", "vector", "reduce", "spmv_fp64", "resident_solve"]
+    KERNELS = ["face", "edge", "gather", "spmv", "vector", "reduce", "spmv_fp64", "resident_solve", "coarse_setup"]
 
     def profile_kernels(self, params: StepParams, reps: int = 20) -> dict:
-        ms = (ctypes.c_float * 8)()
+        ms = (ctypes.c_float * 9)()
         self.check(self.lib.cs_profile_kernels(self.h, ctypes.byref(params), reps, ms))
         return {k: float(ms[i]) for i, k in enumerate(self.KERNELS)}
 

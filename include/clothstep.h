@@ -100,7 +100,19 @@ typedef struct cs_step_params {
                                  a coarse-space correction (one constant per component on each of
                                  a few geometric segments of every CTA's strip, the coarse matrix
                                  inverted per sheet and step), 0 leaves it out */
+    /* Cloth::physicsStep's `transformations` (Cloth.cuh:91-92): the motions' transformations at
+     * this step (Simulator::updateTransformations, Simulator.cu:565-569), CS_TRANSFORM_FLOATS
+     * floats each -- scaling, translation (3), rotation quaternion (s, x, y, z) -- as
+     * Transformation holds them (Transformation.cu:3-19, Quaternion.cu:7-15).  A handle with a
+     * motion (cs_set_handle_motions) pulls its node toward transformations[motion] applied to
+     * its position at load (Transformation::applyToPoint, Transformation.cu:82-84;
+     * Cloth::addHandleForces, Cloth.cu:157-169).  NULL / 0 when no handle moves. */
+    const float* transformations;
+    int n_transformations;    /* at most CS_MAX_MOTIONS */
 } cs_step_params;
+
+#define CS_TRANSFORM_FLOATS 8
+#define CS_MAX_MOTIONS 64
 
 #define CS_PRECOND_MAX_DEGREE 15
 
@@ -154,6 +166,12 @@ cs_status cs_get_resident_blocks(const cs_ctx* ctx, long long* out);
 
 /* Node state of the whole batch, sheets concatenated in load order (3 floats per node). */
 cs_status cs_set_state(cs_ctx* ctx, const float* x, const float* v);
+
+/* The motion of every handle (Handle::motionIndex, Handle.cuh:9-16, from a scene's
+ * "handles"[].motion, Simulator.cu:104-111): n = the handles of all sheets in load order, each
+ * sheet's in its handle_nodes order; -1 = fixed at its target (the default after cs_load_batch).
+ * Each step then takes the motions' transformations from cs_step_params.transformations. */
+cs_status cs_set_handle_motions(cs_ctx* ctx, const int32_t* motion, int n);
 
 /* One proximity as Cloth::physicsStep receives it (Proximity.cuh:11-21; built by the
  * collision detection the reference runs before the step, Simulator.cu:300-349): four
@@ -273,8 +291,9 @@ cs_status cs_device_pointers(cs_ctx* ctx, float** x, float** v, float** dv);
  * launches each, on the current batch: ms[0] face, [1] edge, [2] gather (assembly),
  * [3] SpMV of a CG iteration, [4] vector update of a CG iteration, [5] per-instance reduction,
  * [6] FP64 residual SpMV, [7] one cluster-resident solve of all resident sheets (0 if none;
- * when every sheet is resident, cs_get_instance_stats then reports that solve).  Overwrites the
- * solver's scratch vectors and dv64 (not x, v or dv). */
+ * when every sheet is resident, cs_get_instance_stats then reports that solve), [8] the set-up
+ * of its coarse-space correction (forming and inverting the coarse matrices; 0 without it); ms
+ * holds 9 floats.  Overwrites the solver's scratch vectors and dv64 (not x, v or dv). */
 cs_status cs_profile_kernels(cs_ctx* ctx, const cs_step_params* params, int reps, float* ms);
 /* Cumulative counts since cs_load_batch: [0] steps, [1] solve-loop trips, [2] kernel launches. */
 cs_status cs_get_counters(cs_ctx* ctx, long long* counters);

@@ -359,3 +359,146 @@ def run_cloths(cloths, params_list, steps: int, method: int = METHOD_LLT, thread
     st = np.zeros(len(cloths), np.int32)
     sec = L.run_cloths(arr, len(cloths), _ptr(p, _dp), steps, method, threads, _ptr(st, _ip))
     return sec, st
+
+
+# ---- Handle motions: Transformation, Quaternion and Motion restated in FP32 ----------------
+# (Transformation.cu:3-87, Quaternion.cu:3-78, Motion.cu:3-72, JsonHelper.cu).  NumPy float32
+# arithmetic is IEEE single precision with no contraction; cos, sin and sqrt are the C library's
+# cosf, sinf and sqrtf, as the reference's host code calls them.  A transformation is held as 8
+# float32 values: scaling, translation (3), rotation quaternion (s, x, y, z).
+
+_libm = ctypes.CDLL("libm.so.6")
+for _fn in ("cosf", "sinf", "sqrtf"):
+    getattr(_libm, _fn).restype = ctypes.c_float
+    getattr(_libm, _fn).argtypes = [ctypes.c_float]
+_f = np.float32
+
+
+def _transform_identity() -> np.ndarray:
+    return np.array([1, 0, 0, 0, 1, 0, 0, 0], np.float32)  # Transformation() (Transformation.cu:3-6)
+
+
+def transform_from_json(j: dict | None) -> np.ndarray:
+    """Transformation(const Json::Value&) (Transformation.cu:8-13): scale (default 1), translate,
+    rotate = [degrees, axis x, y, z] -> Quaternion(axis, angle) (Quaternion.cu:7-15)."""
+    j = j or {}
+    out = _transform_identity()
+    out[0] = _f(j.get("scale", 1.0))
+    out[1:4] = np.array(j.get("translate", [0.0, 0.0, 0.0]), np.float32)
+    r = np.array(j.get("rotate", [0.0, 0.0, 0.0, 0.0]), np.float32)
+    angle = _f(np.float64(r[0]) * np.pi / np.float64(_f(180.0)))
+    if angle == _f(0.0):
+        out[4:8] = [1, 0, 0, 0]
+    else:
+        half = _f(_f(0.5) * angle)
+        ax = r[1:4].astype(np.float32)
+        l = _f(_libm.sqrtf(float(_f(_f(ax[0] * ax[0] + ax[1] * ax[1]) + ax[2] * ax[2]))))
+        inv = _f(_f(1.0) / l)  # Vector::operator/ multiplies by the reciprocal (Vector.cuh:126-132)
+        out[4] = _f(_libm.cosf(float(half)))
+        sn = _f(_libm.sinf(float(half)))
+        out[5:8] = np.array([_f(sn * _f(ax[k] * inv)) for k in range(3)], np.float32)
+    return out
+
+
+def transform_points(T: np.ndarray, p: np.ndarray) -> np.ndarray:
+    """Transformation::applyToPoint (Transformation.cu:82-84): s rotate(p) + t with
+    Quaternion::rotate (Quaternion.cu:76-78) p (qs^2 - |qv|^2) + (2 qv)(qv . p) + (2 (qv x p)) qs."""
+    T = np.asarray(T, np.float32)
+    p = np.asarray(p, np.float32).reshape(-1, 3)
+    s, t, qs, qv = T[0], T[1:4], T[4], T[5:8]
+    n2 = _f(_f(qv[0] * qv[0] + qv[1] * qv[1]) + qv[2] * qv[2])
+    d = ((p[:, 0] * qv[0] + p[:, 1] * qv[1]).astype(np.float32) + (p[:, 2] * qv[2])).astype(np.float32)
+    d = ((qv[0] * p[:, 0] + qv[1] * p[:, 1]).astype(np.float32) + qv[2] * p[:, 2]).astype(np.float32)
+    cr = np.stack([qv[1] * p[:, 2] - qv[2] * p[:, 1], qv[2] * p[:, 0] - qv[0] * p[:, 2],
+                   qv[0] * p[:, 1] - qv[1] * p[:, 0]], 1).astype(np.float32)
+    a = p * _f(qs * qs - n2)
+    b = (_f(2.0) * qv)[None, :] * d[:, None]
+    c = (_f(2.0) * cr) * qs
+    r = ((a + b).astype(np.float32) + c).astype(np.float32)
+    return ((s * r).astype(np.float32) + t).astype(np.float32)
+
+
+def _transform_div(T: np.ndarray, s) -> np.ndarray:
+    """Transformation::operator/(float) (Transformation.cu:63-69): scaling and the quaternion's
+    scalar part divided (Quaternion.cu:58-63), translation and the quaternion's vector part
+    multiplied by the reciprocal (Vector::operator/, Vector.cuh:126-132)."""
+    s = _f(s)
+    inv = _f(_f(1.0) / s)
+    out = (T * inv).astype(np.float32)
+    out[0] = _f(T[0] / s)
+    out[4] = _f(T[4] / s)
+    return out
+
+
+class Motion:
+    """Motion (Motion.cu:3-72): keyframes (time, Transformation) with a keyframe at time 0 added
+    when the first is later, central-difference tangents (zero at the ends), and per segment the
+    cubic a s^3 + b s^2 + c s + d in Transformation arithmetic (componentwise on the 8 values).
+    The segment index advances monotonically, as the reference's does."""
+
+    def __init__(self, keyframes: list):
+        self.t = [_f(k.get("time", 0.0)) for k in keyframes]
+        self.x = [transform_from_json(k.get("transform")) for k in keyframes]
+        if self.t[0] > 0:
+            self.t.insert(0, _f(0.0))
+            self.x.insert(0, _transform_identity())
+        n = self.n = len(self.t)
+        zero = (_f(0.0) * _transform_identity()).astype(np.float32)
+        self.v = [zero] * n
+        for i in range(1, n - 1):
+            self.v[i] = _transform_div((self.x[i + 1] - self.x[i - 1]).astype(np.float32), _f(self.t[i + 1] - self.t[i - 1]))
+        self.index = 0
+        self._coefficients()
+
+    def _coefficients(self):
+        i = self.index
+        dt = _f(self.t[i + 1] - self.t[i])
+        dx = (self.x[i + 1] - self.x[i]).astype(np.float32)
+        v0, v1 = self.v[i], self.v[i + 1]
+        self.a = ((dt * (v1 + v0).astype(np.float32)).astype(np.float32) - (_f(2.0) * dx)).astype(np.float32)
+        self.b = ((_f(3.0) * dx) - (dt * (v1 + (_f(2.0) * v0)).astype(np.float32)).astype(np.float32)).astype(np.float32)
+        self.c = (dt * v0).astype(np.float32)
+        self.d = self.x[i]
+
+    def transform(self, time: float) -> np.ndarray:
+        time = _f(time)
+        moved = False
+        while self.index < self.n - 1 and self.t[self.index + 1] < time:
+            self.index += 1
+            moved = True
+        if self.index == self.n - 1:
+            return self.x[self.n - 1].copy()
+        if moved:
+            self._coefficients()
+        s = _f(_f(time - self.t[self.index]) / _f(self.t[self.index + 1] - self.t[self.index]))
+        s2 = _f(s * s)
+        s3 = _f(s * s2)
+        return ((((self.a * s3).astype(np.float32) + (self.b * s2)).astype(np.float32) + (self.c * s)).astype(np.float32)
+                + self.d).astype(np.float32)
+
+
+def ref_transform_points(transform_json: dict, p: np.ndarray) -> np.ndarray:
+    """The reference's own Transformation(json).applyToPoint (the adapter library)."""
+    import json
+
+    L = lib("ref")
+    fn = L.lib.ref_transform_points
+    fn.argtypes = [ctypes.c_char_p, ctypes.c_int, _dp, _dp]
+    p = _d(p).reshape(-1, 3)
+    out = np.zeros_like(p)
+    fn(json.dumps(transform_json).encode(), p.shape[0], _ptr(p, _dp), _ptr(out, _dp))
+    return out
+
+
+def ref_motion_points(keyframes: list, times, p: np.ndarray) -> np.ndarray:
+    """The reference's own Motion(json).computeTransformation(t).applyToPoint at each time."""
+    import json
+
+    L = lib("ref")
+    fn = L.lib.ref_motion_points
+    fn.argtypes = [ctypes.c_char_p, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp]
+    p = _d(p).reshape(-1, 3)
+    ts = _d(times)
+    out = np.zeros((len(ts), p.shape[0], 3))
+    fn(json.dumps(keyframes).encode(), len(ts), _ptr(ts, _dp), p.shape[0], _ptr(p, _dp), _ptr(out, _dp))
+    return out

@@ -24,9 +24,11 @@
 #include "Edge.cuh"
 #include "Face.cuh"
 #include "Material.cuh"
+#include "Motion.cuh"
 #include "Node.cuh"
 #include "PhysicsHelper.cuh"
 #include "Proximity.cuh"
+#include "Transformation.cuh"
 #include "Vertex.cuh"
 
 #include "oracle_collide.hpp"
@@ -65,6 +67,36 @@ struct RefClothImpl : ClothImpl<float> {
 }  // namespace
 
 extern "C" {
+
+// Transformation(json).applyToPoint (Transformation.cu:8-13, 82-84) of n points; json_text: a
+// "transform" object ({"scale", "translate", "rotate": [degrees, axis]}).
+void ref_transform_points(const char* json_text, int n, const double* p, double* out) {
+    Json::Value v;
+    std::istringstream in(json_text);
+    in >> v;
+    const Transformation t(v);
+    for (int i = 0; i < n; i++) {
+        const Vector3f q = t.applyToPoint(Vector3f((float)p[3 * i], (float)p[3 * i + 1], (float)p[3 * i + 2]));
+        for (int c = 0; c < 3; c++) out[3 * i + c] = q(c);
+    }
+}
+
+// Motion(json).computeTransformation(time) (Motion.cu:3-72) applied to n points, for each of
+// n_times increasing times on one Motion (its segment index advances as the reference's does);
+// json_text: a "motions" entry (an array of {"time", "transform"} keyframes).
+void ref_motion_points(const char* json_text, int n_times, const double* times, int n, const double* p, double* out) {
+    Json::Value v;
+    std::istringstream in(json_text);
+    in >> v;
+    Motion m(v);
+    for (int k = 0; k < n_times; k++) {
+        const Transformation t = m.computeTransformation((float)times[k]);
+        for (int i = 0; i < n; i++) {
+            const Vector3f q = t.applyToPoint(Vector3f((float)p[3 * i], (float)p[3 * i + 1], (float)p[3 * i + 2]));
+            for (int c = 0; c < 3; c++) out[3 * (k * n + i) + c] = q(c);
+        }
+    }
+}
 
 // json_text: the cloth's "materials" object, e.g. {"data": "path.json", "thicken": 1}.
 void* ref_material_new(const char* json_text) {

@@ -52,7 +52,7 @@ def test_quad_faces_are_triangulated(tmp_path):
     (lambda c: c.pop("disable"), "remeshing"),
     (lambda c: c.__setitem__("obstacles", [{"mesh": "ball.obj"}]), "obstacles"),
     (lambda c: c["handles"][0]["nodes"].append(10 ** 6), "out of range"),
-    (lambda c: c["handles"][0].__setitem__("motion", 0), "motions"),
+    (lambda c: c["handles"][0].__setitem__("motion", 0), "motion index"),
 ])
 def test_unsupported_or_invalid_scenes_are_rejected(tmp_path, mutate, needle):
     scene = scenes.hang(4, seed=0)
@@ -156,3 +156,167 @@ def test_contact_scene_through_host_layer_matches_c_abi(tmp_path):
         assert np.array_equal(np.array(xs, np.float32), x[o:o + n])
         o += n
     ctx.close()
+
+
+def test_host_transformations_and_motions_match_oracle():
+    """The host layer's Transformation and Motion (what it hands the C ABI each step) against the
+    oracle's FP32 restatement, itself pinned to the reference's classes (test_oracle.py)."""
+    import pyoracle
+    from test_oracle import MOTION_KEYFRAMES
+
+    lib = host()
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.cs_transform_points.argtypes = [ctypes.c_char_p, ctypes.c_int, dp, dp]
+    lib.cs_motion_points.argtypes = [ctypes.c_char_p, ctypes.c_int, dp, ctypes.c_int, dp, dp,
+                                     ctypes.POINTER(ctypes.c_float)]
+    rng = np.random.default_rng(1)
+    p = np.ascontiguousarray(rng.normal(size=(30, 3)))
+    out = np.zeros_like(p)
+    for _ in range(20):
+        j = {"scale": float(rng.uniform(0.5, 2)), "translate": rng.normal(size=3).tolist(),
+             "rotate": [float(rng.uniform(-180, 180))] + rng.normal(size=3).tolist()}
+        assert lib.cs_transform_points(json.dumps(j).encode(), len(p), p.ctypes.data_as(dp), out.ctypes.data_as(dp)) == 0
+        assert np.array_equal(out, pyoracle.transform_points(pyoracle.transform_from_json(j), p).astype(np.float64))
+    times = np.arange(1, 90) * 0.01
+    out = np.zeros((len(times), len(p), 3))
+    tr = np.zeros((len(times), 8), np.float32)
+    assert lib.cs_motion_points(json.dumps(MOTION_KEYFRAMES).encode(), len(times), times.ctypes.data_as(dp), len(p),
+                                p.ctypes.data_as(dp), out.ctypes.data_as(dp),
+                                tr.ctypes.data_as(ctypes.POINTER(ctypes.c_float))) == 0
+    m = pyoracle.Motion(MOTION_KEYFRAMES)
+    want = [m.transform(t) for t in times]
+    assert np.array_equal(tr, np.stack(want))
+    assert np.array_equal(out, np.stack([pyoracle.transform_points(w, p) for w in want]).astype(np.float64))
+
+
+def test_motion_scenes_parse_and_validate(tmp_path):
+    from test_oracle import MOTION_KEYFRAMES
+
+    scene = scenes.hang(4, seed=0)
+    path = scenes.write_scene(scene, str(tmp_path))
+    cfg = json.loads(open(path).read().split("\n", 1)[1])
+    cfg["motions"] = [MOTION_KEYFRAMES]
+    cfg["handles"][0]["motion"] = 0
+    open(path, "w").write(json.dumps(cfg))
+    st, counts, err = describe(path)
+    assert st == 0, err
+    cfg["handles"][0]["motion"] = 1  # no such motion
+    open(path, "w").write(json.dumps(cfg))
+    st, _, err = describe(path)
+    assert st == native.CS_ERR_INVALID_ARG and "motion" in err
+    cfg["handles"][0]["motion"] = 0
+    cfg["motions"] = {"motfile": "walk.mot", "fps": 30}
+    open(path, "w").write(json.dumps(cfg))
+    st, _, err = describe(path)
+    assert st == native.CS_ERR_INVALID_ARG and ".mot" in err
+
+
+def read_obj_reference_dialect(path):
+    """The reference's OBJ reader restated (Mesh::load, Mesh.cu:306-350, with Mesh::triangulate,
+    Mesh.cu:27-54): `v` positions, `nv` velocities, `vt` uv, `f` with a/b (position/uv) or plain
+    indices (then a uv from the position's x, y), polygons split as a fan from the corner whose
+    fan has the largest smallest angle.  Numbers are read as single precision (std::stof)."""
+    x, v, u, fx, fu = [], [], [], [], []
+
+    def angle(a, b, c):
+        e1 = (b - a) / np.float32(np.linalg.norm(b - a))
+        e2 = (c - a) / np.float32(np.linalg.norm(c - a))
+        return float(np.arccos(np.clip(np.float32(np.dot(e1, e2)), -1, 1)))
+
+    for line in open(path):
+        s = line.rstrip("\n").split(" ")
+        if s[0] == "v":
+            x.append(np.array([np.float32(t) for t in s[1:4]], np.float32))
+        elif s[0] == "nv":
+            v.append(np.array([np.float32(t) for t in s[1:4]], np.float32))
+        elif s[0] == "vt":
+            u.append(np.array([np.float32(t) for t in s[1:3]], np.float32))
+        elif s[0] == "f":
+            xp, up = [], []
+            for tok in s[1:]:
+                if "/" in line:
+                    a, b = tok.split("/")[:2]
+                    xp.append(int(a) - 1)
+                    up.append(int(b) - 1)
+                else:
+                    xp.append(int(tok) - 1)
+                    u.append(x[int(tok) - 1][:2].copy())
+                    up.append(len(u) - 1)
+            n = len(xp)
+            best, index = -np.inf, 0
+            for i in range(n):
+                m = np.inf
+                for j in range(2, n):
+                    a, b, c = x[xp[i]], x[xp[(i + j - 1) % n]], x[xp[(i + j) % n]]
+                    m = min(m, angle(a, b, c), angle(b, c, a), angle(c, a, b))
+                if m > best:
+                    best, index = m, i
+            for i in range(2, n):
+                fx.append([xp[index], xp[(index + i - 1) % n], xp[(index + i) % n]])
+                fu.append([up[index], up[(index + i - 1) % n], up[(index + i) % n]])
+    v = v + [np.zeros(3, np.float32)] * (len(x) - len(v))
+    return (np.array(x, np.float32), np.array(v, np.float32), np.array(u, np.float32), np.array(fx), np.array(fu))
+
+
+def test_frames_use_the_reference_obj_dialect(tmp_path):
+    """A mesh read and written by the host layer (cs_mesh_rewrite: Mesh::load then Mesh::save)
+    reads back, through the reference's reader restated, to the same nodes, velocities, uv and
+    triangles; every number is written with 20 significant digits (Mesh.cu:456: precision(20)),
+    so the single-precision values survive exactly."""
+    lib = host()
+    lib.cs_mesh_rewrite.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    rng = np.random.default_rng(9)
+    s = scenes.grid_sheet(5, rng=rng, z_noise=1e-3, vel_sigma=0.3)
+    src = tmp_path / "in.obj"
+    scenes.write_obj(s, str(src))
+    with open(src, "a") as fh:  # a quad (fan-triangulated) and a face with plain indices
+        n = s["x"].shape[0]
+        fh.write("v 2 0 0\nnv 0 0 0\nv 3 0 0.1\nnv 0 0 0\nv 3 1 0\nnv 0 0 0\nv 2 1 0.05\nnv 0 0 0\n")
+        fh.write("vt 2 0\nvt 3 0\nvt 3 1\nvt 2 1\n")
+        nu = s["uv"].shape[0]
+        fh.write("f %d/%d %d/%d %d/%d %d/%d\n" % (n + 1, nu + 1, n + 2, nu + 2, n + 3, nu + 3, n + 4, nu + 4))
+    out = tmp_path / "out.obj"
+    assert lib.cs_mesh_rewrite(str(src).encode(), str(out).encode()) == 0, lib.cs_sim_last_error()
+    want = read_obj_reference_dialect(str(src))
+    got = read_obj_reference_dialect(str(out))
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
+    for line in open(out):
+        tag, *vals = line.split()
+        if tag in ("v", "nv", "vt"):
+            for t in vals:
+                assert t == "%.20g" % float(np.float32(t)), line
+        else:
+            assert tag == "f" and len(vals) == 3 and all(len(t.split("/")) == 2 for t in vals)
+    plain = tmp_path / "plain.obj"
+    plain.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\n")
+    assert lib.cs_mesh_rewrite(str(plain).encode(), str(out).encode()) == 0
+    x, v, u, fx, fu = read_obj_reference_dialect(str(out))
+    assert np.array_equal(fx, [[0, 1, 2]]) and np.array_equal(u, [[0, 0], [1, 0], [0, 1]])
+
+
+@pytest.mark.gpu
+def test_resume_continues_the_trajectory_bit_for_bit(tmp_path):
+    """resume_offline from frame 2 (Simulator.cu:936-957, 1070-1083) reaches the same frame 3
+    as a run straight through: the frames hold positions and velocities with 20 significant
+    digits (exact single-precision values), and every solve starts from the zero guess, so the
+    resumed steps see the state the straight run had."""
+    scene = scenes.stacked_sheets(8, n_layers=2, seed=6)
+    solver = {"tol": 1e-8, "max_iters": 8000, "warm_start": "zero"}
+    lib = host()
+    steps = ctypes.c_int(0)
+    straight = str(tmp_path / "straight")
+    path = scenes.write_scene(scene, str(tmp_path / "scene_a"), frames=3, solver=solver)
+    assert lib.cs_sim_run(b"simulate_offline", path.encode(), straight.encode(), 0, ctypes.byref(steps)) == 0, \
+        lib.cs_sim_last_error()
+    split = str(tmp_path / "split")
+    path = scenes.write_scene(scene, str(tmp_path / "scene_b"), frames=2, solver=solver)
+    assert lib.cs_sim_run(b"simulate_offline", path.encode(), split.encode(), 0, ctypes.byref(steps)) == 0
+    cfg = json.load(open(os.path.join(split, "config.json")))
+    cfg["end_frame"] = 3
+    json.dump(cfg, open(os.path.join(split, "config.json"), "w"))
+    assert lib.cs_sim_run(b"resume_offline", b"", split.encode(), 0, ctypes.byref(steps)) == 0, lib.cs_sim_last_error()
+    for i in range(len(scene.sheets)):
+        a = open(os.path.join(straight, f"frame3_cloth{i}.obj")).read()
+        b = open(os.path.join(split, f"frame3_cloth{i}.obj")).read()
+        assert a == b, f"cloth {i}"

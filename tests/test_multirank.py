@@ -187,3 +187,63 @@ def test_data_parallel_training_two_gloo_ranks():
     assert np.allclose(res[0]["w"], w, rtol=1e-6, atol=1e-7)
     sums, count = res[0]["moments"]
     assert count == 30 and np.allclose(sums, np.arange(38) * 3)
+
+
+# Strong scaling (one workload split across ranks): the sheet partition balanced by stored
+# blocks, and the per-sheet statistics gathered back in workload order with one all-gather.
+
+def test_partition_balances_uneven_sheets():
+    sys.path.insert(0, ROOT)
+    from clothsimulator_b200 import partition, scenes
+
+    scene = scenes.uneven_batch(64, seed=5)
+    b = partition.sheet_blocks(scene.sheets)
+    for world in (1, 2, 3, 4, 8):
+        parts = partition.partition_sheets(b, world)
+        got = np.sort(np.concatenate(parts))
+        assert np.array_equal(got, np.arange(len(scene.sheets)))  # every sheet exactly once
+        # greedy largest-first: within the largest sheet of the mean load
+        loads = [int(b[p].sum()) for p in parts]
+        assert max(loads) - b.sum() / world <= b.max()
+    assert partition.imbalance(b, partition.partition_sheets(b, 4)) < 1.05
+
+
+def _gather_rank(rank, world, port, out):
+    os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch.distributed as dist
+
+    from clothsimulator_b200 import partition
+
+    dist.init_process_group("gloo", init_method="env://", timeout=datetime.timedelta(seconds=60))
+    rng = np.random.default_rng(11)
+    n = 37
+    blocks = rng.integers(100, 5000, n)
+    # the statistics a one-rank run would report for every sheet
+    full = {"iters": rng.integers(10, 400, n), "rel_residual": rng.uniform(1e-8, 1e-6, n),
+            "flags": rng.integers(0, 16, n)}
+    parts = partition.partition_sheets(blocks, world)
+    mine = parts[rank]
+    local = {k: v[mine] for k, v in full.items()}
+    got = partition.gather_stats(local, parts, n, partition.torch_all_gather(dist))
+    out[rank] = {k: (np.array_equal(got[k], full[k])) for k in full}
+    dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+def test_gathered_stats_equal_one_rank_run_two_gloo_ranks():
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    procs = [ctx.Process(target=_gather_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    for r in range(2):
+        assert all(out[r].values()), out[r]

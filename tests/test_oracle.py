@@ -358,3 +358,28 @@ def test_oracle_reproduces_reference_material_files():
         x1, v1 = c.state()
         assert np.array_equal(dv.astype(np.float32), g[p + "dv"]), g["names"][i]
         assert np.array_equal(x1.astype(np.float32), g[p + "x1"]) and np.array_equal(v1.astype(np.float32), g[p + "v1"])
+
+
+# Handle motions: Transformation(json).applyToPoint and Motion::computeTransformation, restated in
+# FP32 by the oracle, against the reference's own classes (compiled into the adapter).
+
+MOTION_KEYFRAMES = [{"time": 0.1, "transform": {"translate": [0.0, 0.2, 0.1]}},
+                    {"time": 0.3, "transform": {"translate": [0.1, 0.3, 0.0], "rotate": [30, 0, 0, 1], "scale": 1.2}},
+                    {"time": 0.6, "transform": {"translate": [0.0, 0.0, 0.0], "rotate": [-20, 1, 1, 0]}}]
+
+
+@pytest.mark.ref
+def test_oracle_transformations_and_motions_match_reference():
+    if not os.path.exists(pyoracle.LIB_REF):
+        pytest.skip("reference adapter not built")
+    rng = np.random.default_rng(0)
+    p = rng.normal(size=(40, 3))
+    for _ in range(30):
+        j = {"scale": float(rng.uniform(0.5, 2)), "translate": rng.normal(size=3).tolist(),
+             "rotate": [float(rng.uniform(-180, 180))] + rng.normal(size=3).tolist()}
+        got = pyoracle.transform_points(pyoracle.transform_from_json(j), p)
+        assert np.array_equal(got.astype(np.float64), pyoracle.ref_transform_points(j, p))
+    times = np.arange(1, 90) * 0.01  # through every segment and past the last keyframe
+    m = pyoracle.Motion(MOTION_KEYFRAMES)
+    got = np.stack([pyoracle.transform_points(m.transform(t), p) for t in times])
+    assert np.array_equal(got.astype(np.float64), pyoracle.ref_motion_points(MOTION_KEYFRAMES, times, p))
