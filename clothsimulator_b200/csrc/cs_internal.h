@@ -104,6 +104,16 @@ enum InstPhase : int {
 #define CS_COARSE_AGGS 54
 // Threads of the per-sheet set-up kernel that forms and inverts the coarse matrix.
 #define CS_COARSE_THREADS 512
+// Launch shapes of the batched SpMV that cs_tune times (pcg.cu, kSpmvShapes): threads per block,
+// slices per warp, block slots whose loads are issued together.
+struct SpmvShape {
+    int threads, spw, unroll;
+};
+#define CS_SPMV_CANDIDATES 24
+#define CS_SPMV_DEFAULT 1  // 128 threads, one slice per warp, no unrolling
+struct Batch;
+extern const SpmvShape kSpmvShapes[CS_SPMV_CANDIDATES];
+void launchSpmvShape(const Batch& B, int shape, cudaStream_t st);
 #define CS_SOLVER_AUTO_DEV 0
 #define CS_SOLVER_BATCHED_DEV 1
 

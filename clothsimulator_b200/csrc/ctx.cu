@@ -37,7 +37,6 @@ __global__ void cs_face_kernel(Batch B);
 __global__ void cs_edge_kernel(Batch B);
 __global__ void cs_gather_kernel(Batch B);
 __global__ void cs_expand_kernel(Batch B, float* face_f, float* face_J, float* edge_f, float* edge_J);
-__global__ void cs_spmv_kernel(Batch B);
 __global__ void cs_reduce1_kernel(Batch B);
 __global__ void cs_vector_kernel(Batch B);
 __global__ void cs_reduce2_kernel(Batch B, cudaGraphConditionalHandle handle);
@@ -48,6 +47,7 @@ __global__ void cs_spmv_plain_kernel(Batch B, const float* x, float* y);
 __global__ void cs_profile_setup_kernel(Batch B, int phase);
 __global__ void cs_resident_pcg_kernel(Batch B);
 __global__ void cs_coarse_setup_kernel(Batch B);
+static_assert(CS_SPMV_CANDIDATES == CS_TUNE_SPMV_SHAPES, "the tuner's result holds every SpMV shape");
 __global__ void cs_prox_kernel(Batch B);
 __global__ void cs_prox_row_kernel(Batch B);
 __global__ void cs_slice_bnorm_kernel(Batch B);
@@ -805,6 +805,8 @@ struct cs_ctx {
     // cluster-resident solver launch (resident.cu): CTAs per cluster, threads per CTA,
     // clusters in the persistent grid, dynamic shared memory per CTA
     int resCL = 0, resThreads = 0, resClusters = 0, resClustersMax = 0;
+    int spmvShape = CS_SPMV_DEFAULT;    // launch shape of the batched SpMV (cs_tune)
+    int tunedDegree = 0, tunedCoarse = 0;  // fastest resident preconditioner found by cs_tune (0: not tuned)
     std::vector<int> handleNode;  // batch node of every handle, in load order (cs_set_handle_motions)
     int maxHandleMotion = -1;     // largest motion a handle follows (-1: none)
     size_t resSmem = 0;
@@ -862,6 +864,8 @@ cs_status upload(cs_ctx* c, T** p, const std::vector<T>& h) {
 }
 
 void freeBatch(cs_ctx* c) {
+    c->spmvShape = CS_SPMV_DEFAULT;
+    c->tunedDegree = c->tunedCoarse = 0;
     c->handleNode.clear();
     c->maxHandleMotion = -1;
     if (c->graphExec) cudaGraphExecDestroy(c->graphExec);
@@ -968,7 +972,7 @@ int launchMlpInference(cs_ctx* c, float* pred) {
 void launchTrip(cs_ctx* c, cudaGraphConditionalHandle h) {
     Batch& B = c->B;
     int g = nblk((long long)B.n_slices * 32, 128);
-    cs_spmv_kernel<<<g, 128, 0, c->stream>>>(B);
+    launchSpmvShape(B, c->spmvShape, c->stream);
     cs_reduce1_kernel<<<B.S, 128, 0, c->stream>>>(B);
     cs_vector_kernel<<<g, 128, 0, c->stream>>>(B);
     cs_reduce2_kernel<<<B.S, 128, 0, c->stream>>>(B, h);
@@ -1582,6 +1586,11 @@ cs_status cs_get_solver_info(const cs_ctx* c, int* info) {
     info[3] = c->resClusters;
     info[4] = c->B.res_cap;
     info[5] = (int)c->resSmem;
+    info[6] = kSpmvShapes[c->spmvShape].threads;
+    info[7] = kSpmvShapes[c->spmvShape].spw;
+    info[8] = kSpmvShapes[c->spmvShape].unroll;
+    info[9] = c->tunedDegree;
+    info[10] = c->tunedCoarse;
     return CS_OK;
 }
 
@@ -2496,10 +2505,10 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
                 case 0: if (B.F) cs_face_kernel<<<nblk(B.F, 64), 64, 0, c->stream>>>(B); break;
                 case 1: if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B); break;
                 case 2: cs_gather_kernel<<<c->gatherGrid, 128, 0, c->stream>>>(B); break;
-                case 3: cs_spmv_kernel<<<g, 128, 0, c->stream>>>(B); break;
+                case 3: launchSpmvShape(B, c->spmvShape, c->stream); break;
                 case 4: cs_vector_kernel<<<g, 128, 0, c->stream>>>(B); break;
                 case 5: cs_reduce1_kernel<<<B.S, 128, 0, c->stream>>>(B); break;
-                case 6: cs_spmv_kernel<<<g, 128, 0, c->stream>>>(B); break;
+                case 6: launchSpmvShape(B, c->spmvShape, c->stream); break;
             }
         }
         cudaEventRecord(c->ev1, c->stream);
@@ -2547,6 +2556,113 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
     // the per-sheet statistics of the last timed resident solve stay readable when it solved
     // every sheet of the batch
     c->lastStepValid = c->resClusters > 0 && c->B.n_resident == c->B.S;
+    return CS_OK;
+}
+
+namespace {
+// Order-independent checksum of 32-bit words (XOR of each word mixed with its index).
+__global__ void cs_checksum_kernel(const uint32_t* __restrict__ w, long long n, unsigned salt, unsigned* out) {
+    unsigned acc = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        unsigned h = w[i] ^ (unsigned)(i * 0x9E3779B1ull) ^ salt;
+        h ^= h >> 16;
+        h *= 0x85EBCA6Bu;
+        h ^= h >> 13;
+        acc ^= h;
+    }
+    atomicXor(out, acc);
+}
+}  // namespace
+
+cs_status cs_tune(cs_ctx* c, const cs_step_params* p, int reps, cs_tune_result* out) {
+    if (!c || reps <= 0) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    cs_status st = validateParams(c, p);
+    if (st != CS_OK) return st;
+    CS_CUDA(cudaSetDevice(c->device));
+    Batch& B = c->B;
+    DevParams d = toDev(p);
+    CS_CUDA(cudaMemcpyAsync(B.params, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
+    launchAssembly(c);
+    // the SpMV's shapes on one fixed CG product (every instance in PH_CG, as cs_profile_kernels sets it)
+    cs_solve_setup_kernel<<<B.S, 128, 0, c->stream>>>(B);
+    cs_solve_prologue_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B);
+    cs_profile_setup_kernel<<<nblk(B.S, 128), 128, 0, c->stream>>>(B, PH_CG);
+    unsigned* sum = reinterpret_cast<unsigned*>(B.loop + 7);
+    float bestMs = 1e30f;
+    int best = c->spmvShape;
+    for (int k = 0; k < CS_SPMV_CANDIDATES; k++) {
+        CS_CUDA(cudaMemsetAsync(B.q, 0, 3LL * B.N * sizeof(float), c->stream));
+        launchSpmvShape(B, k, c->stream);
+        CS_CUDA(cudaMemsetAsync(sum, 0, sizeof(unsigned), c->stream));
+        cs_checksum_kernel<<<256, 256, 0, c->stream>>>(reinterpret_cast<const uint32_t*>(B.q), 3LL * B.N, 1u, sum);
+        cs_checksum_kernel<<<64, 256, 0, c->stream>>>(reinterpret_cast<const uint32_t*>(B.part), 4LL * B.n_slices, 2u, sum);
+        unsigned h = 0;
+        CS_CUDA(cudaMemcpyAsync(&h, sum, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        CS_CUDA(cudaEventRecord(c->ev0, c->stream));
+        for (int r = 0; r < reps; r++) launchSpmvShape(B, k, c->stream);
+        CS_CUDA(cudaEventRecord(c->ev1, c->stream));
+        CS_CUDA(cudaEventSynchronize(c->ev1));
+        float ms = 0.f;
+        CS_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        ms /= reps;
+        if (out) {
+            out->spmv_ms[k] = ms;
+            out->spmv_checksum[k] = h;
+            out->spmv_threads[k] = kSpmvShapes[k].threads;
+            out->spmv_spw[k] = kSpmvShapes[k].spw;
+            out->spmv_unroll[k] = kSpmvShapes[k].unroll;
+        }
+        if (ms < bestMs) {
+            bestMs = ms;
+            best = k;
+        }
+    }
+    c->spmvShape = best;
+    if (out) out->best_spmv = best;
+    // the resident solver's preconditioners: one whole solve of the resident sheets each
+    static const int degs[CS_TUNE_PRECONDS] = {1, 3, 3, 5, 5, 7}, coarse[CS_TUNE_PRECONDS] = {0, 0, 1, 0, 1, 1};
+    int bestP = -1;
+    float bestPm = 1e30f;
+    for (int k = 0; k < CS_TUNE_PRECONDS; k++) {
+        float ms = 0.f;
+        if (c->resClusters > 0) {
+            cs_step_params q = *p;
+            q.precond_degree = degs[k];
+            q.coarse = coarse[k];
+            q.solver = CS_SOLVER_AUTO;
+            DevParams dq = toDev(&q);
+            CS_CUDA(cudaMemcpyAsync(B.params, &dq, sizeof(dq), cudaMemcpyHostToDevice, c->stream));
+            // one untimed solve, then the mean of up to three timed ones
+            const int nrep = reps < 3 ? reps : 3;
+            for (int r = 0; r <= nrep; r++) {
+                launchSolvePrologue(c);
+                CS_CUDA(cudaEventRecord(c->ev0, c->stream));
+                launchResident(c);
+                CS_CUDA(cudaEventRecord(c->ev1, c->stream));
+                CS_CUDA(cudaEventSynchronize(c->ev1));
+                float t = 0.f;
+                CS_CUDA(cudaEventElapsedTime(&t, c->ev0, c->ev1));
+                if (r > 0) ms += t / nrep;
+            }
+            if (ms < bestPm) {
+                bestPm = ms;
+                bestP = k;
+            }
+        }
+        if (out) {
+            out->precond_ms[k] = ms;
+            out->precond_degree[k] = degs[k];
+            out->precond_coarse[k] = coarse[k];
+        }
+    }
+    c->tunedDegree = bestP >= 0 ? degs[bestP] : 0;
+    c->tunedCoarse = bestP >= 0 ? coarse[bestP] : 0;
+    if (out) out->best_precond = bestP;
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    destroyGraphs(c);  // the captured steps launch the old SpMV shape
+    c->lastStepValid = false;
     return CS_OK;
 }
 

@@ -52,10 +52,11 @@ __device__ __forceinline__ bool finite_d(double x) { return x == x && x < 1e300 
 
 }  // namespace
 
-__global__ void __launch_bounds__(128) cs_spmv_kernel(Batch B) {
-    int slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    if (slice >= B.n_slices) return;
+// One slice of the batched SpMV (PH_CG: the CG product with the fused direction update; PH_RES:
+// the FP64 residual).  UNROLL: slots whose loads are issued together; the sums still run in slot
+// order, so every launch shape gives the same bits.
+template <int UNROLL>
+__device__ __forceinline__ void spmv_slice(const Batch& B, int slice, int lane) {
     const SliceDesc sd = B.slices[slice];
     const InstState& I = B.inst[sd.sheet];
     const int ph = I.phase;
@@ -74,6 +75,7 @@ __global__ void __launch_bounds__(128) cs_spmv_kernel(Batch B) {
         double dd = 0.0;
         float df = 0.f;
         if (live) {
+#pragma unroll UNROLL
             for (int k = 0; k < sd.width; k++) {
                 const int col = __ldg(&B.tcol[(sd.tpanel0 + k) * CS_SLICE + lane]) + node_off;
                 const float* panel = B.A + (size_t)(sd.panel0 + k) * CS_PANEL_FLOATS;
@@ -133,6 +135,7 @@ __global__ void __launch_bounds__(128) cs_spmv_kernel(Batch B) {
     } else {
         double y0 = 0.0, y1 = 0.0, y2 = 0.0, sq = 0.0, dq = 0.0;
         if (live) {
+#pragma unroll UNROLL
             for (int k = 0; k < sd.width; k++) {
                 const int col = __ldg(&B.tcol[(sd.tpanel0 + k) * CS_SLICE + lane]) + node_off;
                 const float* panel = B.A + (size_t)(sd.panel0 + k) * CS_PANEL_FLOATS;
@@ -175,6 +178,38 @@ __global__ void __launch_bounds__(128) cs_spmv_kernel(Batch B) {
             B.part[2 * slice + 1] = dq;
         }
     }
+}
+
+// The batched SpMV kernel: each warp takes SPW consecutive slices.  Launch shapes (threads per
+// block, SPW, UNROLL) are chosen per batch by cs_tune (ctx.cu); all give bitwise-identical output.
+template <int SPW, int UNROLL>
+__global__ void __launch_bounds__(512) cs_spmv_kernel_t(Batch B) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+#pragma unroll 1
+    for (int i = 0; i < SPW; i++) {
+        const int slice = warp * SPW + i;
+        if (slice >= B.n_slices) return;
+        spmv_slice<UNROLL>(B, slice, lane);
+    }
+}
+
+// the candidates cs_tune times, in the order of CS_SPMV_CANDIDATES (cs_internal.h)
+const SpmvShape kSpmvShapes[CS_SPMV_CANDIDATES] = {
+    {64, 1, 1}, {128, 1, 1}, {256, 1, 1}, {512, 1, 1}, {64, 2, 1}, {128, 2, 1}, {256, 2, 1}, {512, 2, 1},
+    {64, 4, 1}, {128, 4, 1}, {256, 4, 1}, {512, 4, 1}, {64, 1, 4}, {128, 1, 4}, {256, 1, 4}, {512, 1, 4},
+    {64, 2, 4}, {128, 2, 4}, {256, 2, 4}, {512, 2, 4}, {64, 4, 4}, {128, 4, 4}, {256, 4, 4}, {512, 4, 4}};
+
+void launchSpmvShape(const Batch& B, int shape, cudaStream_t st) {
+    const SpmvShape& sh = kSpmvShapes[shape];
+    const long long warps = (B.n_slices + sh.spw - 1) / sh.spw;
+    const int grid = (int)((warps * 32 + sh.threads - 1) / sh.threads);
+    if (grid <= 0) return;
+#define CS_SPMV_LAUNCH(S, U) \
+    if (sh.spw == S && sh.unroll == U) cs_spmv_kernel_t<S, U><<<grid, sh.threads, 0, st>>>(B);
+    CS_SPMV_LAUNCH(1, 1) CS_SPMV_LAUNCH(2, 1) CS_SPMV_LAUNCH(4, 1) CS_SPMV_LAUNCH(1, 4) CS_SPMV_LAUNCH(2, 4)
+    CS_SPMV_LAUNCH(4, 4)
+#undef CS_SPMV_LAUNCH
 }
 
 // Sum of part[2*s + c] over an instance's slices: double for the mixed solver, float for the

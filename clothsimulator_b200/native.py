@@ -39,7 +39,7 @@ EXPORTED = [
     "cs_mlp_train", "cs_mlp_gradient", "cs_mlp_predict", "cs_mlp_get_record", "cs_mlp_get_weights",
     "cs_mlp_set_weights", "cs_get_solver_info", "cs_set_proximities", "cs_detect_proximities",
     "cs_get_proximities", "cs_collision_step", "cs_mlp_moments", "cs_mlp_set_moments", "cs_mlp_gradient_device",
-    "cs_mlp_apply_gradient", "cs_get_resident_blocks", "cs_set_handle_motions",
+    "cs_mlp_apply_gradient", "cs_get_resident_blocks", "cs_set_handle_motions", "cs_tune",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -79,6 +79,15 @@ class StepParams(ctypes.Structure):
         ("advance", ctypes.c_int), ("use_graph", ctypes.c_int), ("solver", ctypes.c_int),
         ("precond_degree", ctypes.c_int), ("coarse", ctypes.c_int),
         ("transformations", ctypes.POINTER(ctypes.c_float)), ("n_transformations", ctypes.c_int),
+    ]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [
+        ("spmv_ms", ctypes.c_float * 24), ("spmv_checksum", ctypes.c_uint32 * 24),
+        ("spmv_threads", ctypes.c_int * 24), ("spmv_spw", ctypes.c_int * 24), ("spmv_unroll", ctypes.c_int * 24),
+        ("precond_ms", ctypes.c_float * 6), ("precond_degree", ctypes.c_int * 6), ("precond_coarse", ctypes.c_int * 6),
+        ("best_spmv", ctypes.c_int), ("best_precond", ctypes.c_int),
     ]
 
 
@@ -158,6 +167,7 @@ def load_library() -> ctypes.CDLL:
         "cs_collision_step": [vp, ctypes.POINTER(CollisionParams), ctypes.POINTER(CollisionStats)],
         "cs_set_state": [vp, _fp, _fp],
         "cs_set_handle_motions": [vp, _ip, ctypes.c_int],
+        "cs_tune": [vp, ctypes.POINTER(StepParams), ctypes.c_int, vp],
         "cs_get_state": [vp, _fp, _fp],
         "cs_set_state_device": [vp, vp, vp],
         "cs_get_state_device": [vp, vp, vp],
@@ -339,10 +349,23 @@ class Context:
 
     def solver_info(self) -> dict:
         """Cluster-resident solve plan of the loaded batch."""
-        s = (ctypes.c_int * 6)()
+        s = (ctypes.c_int * 11)()
         self.check(self.lib.cs_get_solver_info(self.h, s))
-        keys = ("resident_sheets", "ctas_per_cluster", "threads_per_cta", "clusters", "panels_in_smem", "smem_bytes")
+        keys = ("resident_sheets", "ctas_per_cluster", "threads_per_cta", "clusters", "panels_in_smem", "smem_bytes",
+                "spmv_threads_per_block", "spmv_slices_per_warp", "spmv_slots_loaded_together",
+                "tuned_precond_degree", "tuned_coarse")
         return dict(zip(keys, [int(v) for v in s]))
+
+    def tune(self, params: StepParams, reps: int = 10) -> dict:
+        """cs_tune: times the batched SpMV's launch shapes and the resident preconditioners on the
+        loaded batch; the fastest SpMV shape is used from then on."""
+        r = TuneResult()
+        self.check(self.lib.cs_tune(self.h, ctypes.byref(params), reps, ctypes.byref(r)))
+        shapes = [{"threads": r.spmv_threads[k], "slices_per_warp": r.spmv_spw[k], "unroll": r.spmv_unroll[k],
+                   "ms": float(r.spmv_ms[k]), "checksum": int(r.spmv_checksum[k])} for k in range(24)]
+        pre = [{"degree": r.precond_degree[k], "coarse": r.precond_coarse[k], "ms": float(r.precond_ms[k])}
+               for k in range(6)]
+        return {"spmv": shapes, "best_spmv": r.best_spmv, "precond": pre, "best_precond": r.best_precond}
 
     def resident_blocks(self) -> dict:
         """Blocks of the resident sheets' systems, the strip-local ones (read by each local SpMV

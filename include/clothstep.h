@@ -152,10 +152,36 @@ cs_status cs_load_batch(cs_ctx* ctx, const cs_material_desc* materials, int n_ma
  * it while proximities are set). */
 cs_status cs_get_sizes(const cs_ctx* ctx, long long* sizes);
 
-/* info[0..5] = sheets solved cluster-resident, CTAs per cluster, threads per CTA, clusters
+/* info[0..10] = sheets solved cluster-resident, CTAs per cluster, threads per CTA, clusters
  * in the persistent grid, SELL panels per CTA in shared memory, dynamic shared memory bytes
- * per CTA.  No counterpart in the reference (its solver has no such plan). */
+ * per CTA; the batched SpMV's launch shape (threads per block, slices per warp, slots loaded
+ * together; cs_tune); the fastest resident preconditioner cs_tune found (degree, coarse
+ * correction; 0, 0 before tuning).  No counterpart in the reference (its solver has no plan). */
 cs_status cs_get_solver_info(const cs_ctx* ctx, int* info);
+
+/* --- Autotuner ------------------------------------------------------------------------------
+ * No counterpart in the reference, whose GPU solve calls cuSPARSE's COO SpMV with its default
+ * algorithm (Cloth.cu:767-778, 790).  cs_tune times, with CUDA events on the context's stream and
+ * on the loaded batch's system for the current state (params as for cs_step): every launch shape
+ * of the batched SpMV -- threads per block, SELL slices per warp, block slots whose loads are
+ * issued together -- reps launches each, and whole cluster-resident solves with each
+ * preconditioner (block-Jacobi; strip-local Chebyshev of degree 3, 5 and 7 without and with the
+ * coarse-space correction; one untimed, then the mean of min(reps, 3)).  Every SpMV shape computes the same bits (out->spmv_checksum holds a
+ * checksum of each shape's output); the fastest is used by the following steps.  The fastest
+ * preconditioner is reported (cs_get_solver_info info[9], info[10]) for the caller's
+ * cs_step_params.precond_degree / coarse.  Overwrites the solver's scratch vectors (not x, v, dv);
+ * out may be NULL. */
+#define CS_TUNE_SPMV_SHAPES 24
+#define CS_TUNE_PRECONDS 6
+typedef struct cs_tune_result {
+    float spmv_ms[CS_TUNE_SPMV_SHAPES];
+    uint32_t spmv_checksum[CS_TUNE_SPMV_SHAPES];
+    int spmv_threads[CS_TUNE_SPMV_SHAPES], spmv_spw[CS_TUNE_SPMV_SHAPES], spmv_unroll[CS_TUNE_SPMV_SHAPES];
+    float precond_ms[CS_TUNE_PRECONDS];  /* 0 when no sheet is solved cluster-resident */
+    int precond_degree[CS_TUNE_PRECONDS], precond_coarse[CS_TUNE_PRECONDS];
+    int best_spmv, best_precond;         /* indices; best_precond -1 without resident sheets */
+} cs_tune_result;
+cs_status cs_tune(cs_ctx* ctx, const cs_step_params* params, int reps, cs_tune_result* out);
 
 /* out[0..2] = 3x3 blocks of the systems of the sheets now solved cluster-resident (the mesh
  * pattern's), those among them whose row and column belong to the same CTA's strip of rows

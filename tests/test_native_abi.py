@@ -49,7 +49,7 @@ def test_struct_layouts_match_header(tmp_path):
         "cs_material_desc": native.MaterialDesc, "cs_sheet_desc": native.SheetDesc,
         "cs_step_params": native.StepParams, "cs_step_stats": native.StepStats,
         "cs_detect_params": native.DetectParams, "cs_collision_params": native.CollisionParams,
-        "cs_collision_stats": native.CollisionStats,
+        "cs_collision_stats": native.CollisionStats, "cs_tune_result": native.TuneResult,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "clothstep.h"', "int main(void) {"]
     for cname, ct in structs.items():
