@@ -295,28 +295,63 @@ def test_frames_use_the_reference_obj_dialect(tmp_path):
     assert np.array_equal(fx, [[0, 1, 2]]) and np.array_equal(u, [[0, 0], [1, 0], [0, 1]])
 
 
+def _run(lib, mode, config, directory):
+    steps = ctypes.c_int(0)
+    rc = lib.cs_sim_run(mode, config.encode() if config else b"", directory.encode(), 0, ctypes.byref(steps))
+    assert rc == 0, lib.cs_sim_last_error()
+
+
+def _frame(directory, frame, cloth):
+    return open(os.path.join(directory, f"frame{frame}_cloth{cloth}.obj")).read()
+
+
 @pytest.mark.gpu
 def test_resume_continues_the_trajectory_bit_for_bit(tmp_path):
-    """resume_offline from frame 2 (Simulator.cu:936-957, 1070-1083) reaches the same frame 3
-    as a run straight through: the frames hold positions and velocities with 20 significant
-    digits (exact single-precision values), and every solve starts from the zero guess, so the
-    resumed steps see the state the straight run had."""
+    """resume_offline from frame 2 (Simulator.cu:936-957, 1070-1083) of two stacked sheets in
+    contact falling freely reaches the same frame 3 as a run straight through: the frames hold
+    positions and velocities with 20 significant digits (exact single-precision values), and
+    every solve starts from the zero guess, so the resumed steps see the state the straight run
+    had."""
     scene = scenes.stacked_sheets(8, n_layers=2, seed=6)
+    for s in scene.sheets:
+        s["handles"] = np.zeros(0, np.int32)
     solver = {"tol": 1e-8, "max_iters": 8000, "warm_start": "zero"}
     lib = host()
-    steps = ctypes.c_int(0)
-    straight = str(tmp_path / "straight")
-    path = scenes.write_scene(scene, str(tmp_path / "scene_a"), frames=3, solver=solver)
-    assert lib.cs_sim_run(b"simulate_offline", path.encode(), straight.encode(), 0, ctypes.byref(steps)) == 0, \
-        lib.cs_sim_last_error()
-    split = str(tmp_path / "split")
-    path = scenes.write_scene(scene, str(tmp_path / "scene_b"), frames=2, solver=solver)
-    assert lib.cs_sim_run(b"simulate_offline", path.encode(), split.encode(), 0, ctypes.byref(steps)) == 0
+    straight, split = str(tmp_path / "straight"), str(tmp_path / "split")
+    _run(lib, b"simulate_offline", scenes.write_scene(scene, str(tmp_path / "scene_a"), frames=3, solver=solver), straight)
+    _run(lib, b"simulate_offline", scenes.write_scene(scene, str(tmp_path / "scene_b"), frames=2, solver=solver), split)
+    assert _frame(straight, 2, 0) == _frame(split, 2, 0)
     cfg = json.load(open(os.path.join(split, "config.json")))
     cfg["end_frame"] = 3
     json.dump(cfg, open(os.path.join(split, "config.json"), "w"))
-    assert lib.cs_sim_run(b"resume_offline", b"", split.encode(), 0, ctypes.byref(steps)) == 0, lib.cs_sim_last_error()
+    _run(lib, b"resume_offline", None, split)
     for i in range(len(scene.sheets)):
-        a = open(os.path.join(straight, f"frame3_cloth{i}.obj")).read()
-        b = open(os.path.join(split, f"frame3_cloth{i}.obj")).read()
-        assert a == b, f"cloth {i}"
+        assert _frame(straight, 3, i) == _frame(split, 3, i), f"cloth {i}"
+
+
+@pytest.mark.gpu
+def test_resume_takes_handle_targets_from_the_saved_frame(tmp_path):
+    """A resumed simulation is built from the saved config, whose meshes are the last frame's
+    OBJ files (Cloth::save, Cloth.cu:865-887), so a fixed handle's target is its node's position
+    in that frame (Cloth::addHandles, Cloth.cu:653-664), not the first frame's: resuming from
+    frame 2 gives bit for bit the frame a fresh simulate_offline of that saved config reaches
+    after one frame, and differs from the straight run's frame 3 (penalty handles sit a little
+    off their targets)."""
+    scene = scenes.stacked_sheets(8, n_layers=2, seed=6)
+    solver = {"tol": 1e-8, "max_iters": 8000, "warm_start": "zero"}
+    lib = host()
+    straight, split, fresh = str(tmp_path / "straight"), str(tmp_path / "split"), str(tmp_path / "fresh")
+    _run(lib, b"simulate_offline", scenes.write_scene(scene, str(tmp_path / "scene_a"), frames=3, solver=solver), straight)
+    _run(lib, b"simulate_offline", scenes.write_scene(scene, str(tmp_path / "scene_b"), frames=2, solver=solver), split)
+    cfg = json.load(open(os.path.join(split, "config.json")))
+    cfg["end_frame"] = 1
+    os.makedirs(str(tmp_path / "scene_c"))
+    saved = str(tmp_path / "scene_c" / "config.json")
+    json.dump(cfg, open(saved, "w"))
+    _run(lib, b"simulate_offline", saved, fresh)
+    cfg["end_frame"] = 3
+    json.dump(cfg, open(os.path.join(split, "config.json"), "w"))
+    _run(lib, b"resume_offline", None, split)
+    for i in range(len(scene.sheets)):
+        assert _frame(split, 3, i) == _frame(fresh, 1, i), f"cloth {i}"
+    assert any(_frame(split, 3, i) != _frame(straight, 3, i) for i in range(len(scene.sheets)))
