@@ -502,9 +502,13 @@ def run_ours(args):
                   "spmv_default_ms": default["ms"], "spmv_shapes_identical_bits": len({x["checksum"] for x in t["spmv"]}) == 1,
                   "precond": t["precond"][t["best_precond"]] if t["best_precond"] >= 0 else None,
                   "precond_candidates": t["precond"]}
+        tuning["solver_ms"] = t["solver_ms"]
+        tuning["solver"] = t["best_solver"]
         if t["best_precond"] >= 0 and not args.fixed_precond:
             args.precond_degree = t["precond"][t["best_precond"]]["degree"]
             args.no_coarse = not t["precond"][t["best_precond"]]["coarse"]
+        if args.solver == "auto" and t["best_solver"] == "batched" and not args.fixed_precond:
+            args.solver = "batched"
 
     weights, train_info = None, None
     if args.warm == "learned":

@@ -100,6 +100,8 @@ enum InstPhase : int {
 // preconditioner): each CTA's strip of rows is cut into K segments along the principal axis of
 // its nodes' rest (uv) coordinates, K = min(CS_COARSE_MAX_K, CS_COARSE_AGGS / CTAs per cluster);
 // the coarse space holds one constant per (segment, component).
+// threads of the per-instance reduction kernels of the batched loop
+#define CS_REDUCE_THREADS 256
 #define CS_COARSE_MAX_K 8
 #define CS_COARSE_AGGS 54
 // Threads of the per-sheet set-up kernel that forms and inverts the coarse matrix.

@@ -807,6 +807,7 @@ struct cs_ctx {
     int resCL = 0, resThreads = 0, resClusters = 0, resClustersMax = 0;
     int spmvShape = CS_SPMV_DEFAULT;    // launch shape of the batched SpMV (cs_tune)
     int tunedDegree = 0, tunedCoarse = 0;  // fastest resident preconditioner found by cs_tune (0: not tuned)
+    int tunedSolver = -1;                  // faster solve route found by cs_tune (-1: not tuned)
     std::vector<int> handleNode;  // batch node of every handle, in load order (cs_set_handle_motions)
     int maxHandleMotion = -1;     // largest motion a handle follows (-1: none)
     size_t resSmem = 0;
@@ -931,6 +932,14 @@ void launchSolvePrologue(cs_ctx* c) {
     cs_solve_prologue_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B);
 }
 
+// A solve set-up for measurements that re-run the solve on an assembled system after other
+// kernels have reused the slice partials: the ||b||^2 partials first, as the assembly leaves them.
+void launchSolvePrologueAgain(cs_ctx* c) {
+    Batch& B = c->B;
+    cs_slice_bnorm_kernel<<<nblk((long long)B.n_slices * 32, 128), 128, 0, c->stream>>>(B);
+    launchSolvePrologue(c);
+}
+
 // Sheets that fit a cluster's shared memory: one persistent cluster per sheet at a time.
 // The coarse matrices of the resident sheets, formed and inverted for this step's systems (the
 // kernel returns at once unless the step asks for the coarse correction).
@@ -973,9 +982,9 @@ void launchTrip(cs_ctx* c, cudaGraphConditionalHandle h) {
     Batch& B = c->B;
     int g = nblk((long long)B.n_slices * 32, 128);
     launchSpmvShape(B, c->spmvShape, c->stream);
-    cs_reduce1_kernel<<<B.S, 128, 0, c->stream>>>(B);
+    cs_reduce1_kernel<<<B.S, CS_REDUCE_THREADS, 0, c->stream>>>(B);
     cs_vector_kernel<<<g, 128, 0, c->stream>>>(B);
-    cs_reduce2_kernel<<<B.S, 128, 0, c->stream>>>(B, h);
+    cs_reduce2_kernel<<<B.S, CS_REDUCE_THREADS, 0, c->stream>>>(B, h);
 }
 
 cs_status buildGraph(cs_ctx* c, bool learned) {
@@ -2507,7 +2516,7 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
                 case 2: cs_gather_kernel<<<c->gatherGrid, 128, 0, c->stream>>>(B); break;
                 case 3: launchSpmvShape(B, c->spmvShape, c->stream); break;
                 case 4: cs_vector_kernel<<<g, 128, 0, c->stream>>>(B); break;
-                case 5: cs_reduce1_kernel<<<B.S, 128, 0, c->stream>>>(B); break;
+                case 5: cs_reduce1_kernel<<<B.S, CS_REDUCE_THREADS, 0, c->stream>>>(B); break;
                 case 6: launchSpmvShape(B, c->spmvShape, c->stream); break;
             }
         }
@@ -2533,7 +2542,7 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
     if (c->resClusters > 0) {
         float acc = 0.f, accSetup = 0.f;
         for (int r = 0; r < reps; r++) {
-            launchSolvePrologue(c);
+            launchSolvePrologueAgain(c);
             cudaEventRecord(c->ev0, c->stream);
             launchCoarseSetup(c);
             cudaEventRecord(c->ev1, c->stream);
@@ -2573,6 +2582,32 @@ __global__ void cs_checksum_kernel(const uint32_t* __restrict__ w, long long n, 
     atomicXor(out, acc);
 }
 }  // namespace
+
+// One whole solve of the loaded system (already assembled) with parameters q, launched from
+// the host (cluster-resident kernel, then the batched loop polled every 8 trips), timed with
+// CUDA events on the context's stream; -1 if a launch failed.
+static float timeWholeSolve(cs_ctx* c, const cs_step_params& q) {
+    Batch& B = c->B;
+    DevParams d = toDev(&q);
+    if (cudaMemcpyAsync(B.params, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream) != cudaSuccess) return -1.f;
+    launchSolvePrologueAgain(c);
+    cudaEventRecord(c->ev0, c->stream);
+    launchResident(c);
+    int go = 1, trips = 0;
+    while (go) {
+        for (int t = 0; t < 8; t++) launchTrip(c, 0);
+        trips += 8;
+        if (cudaMemcpyAsync(&go, B.loop + 3, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+            cudaStreamSynchronize(c->stream) != cudaSuccess)
+            return -1.f;
+        if (trips > d.loop_cap + 16) break;
+    }
+    cudaEventRecord(c->ev1, c->stream);
+    if (cudaEventSynchronize(c->ev1) != cudaSuccess) return -1.f;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    return ms;
+}
 
 cs_status cs_tune(cs_ctx* c, const cs_step_params* p, int reps, cs_tune_result* out) {
     if (!c || reps <= 0) return CS_ERR_INVALID_ARG;
@@ -2636,7 +2671,7 @@ cs_status cs_tune(cs_ctx* c, const cs_step_params* p, int reps, cs_tune_result* 
             // one untimed solve, then the mean of up to three timed ones
             const int nrep = reps < 3 ? reps : 3;
             for (int r = 0; r <= nrep; r++) {
-                launchSolvePrologue(c);
+                launchSolvePrologueAgain(c);
                 CS_CUDA(cudaEventRecord(c->ev0, c->stream));
                 launchResident(c);
                 CS_CUDA(cudaEventRecord(c->ev1, c->stream));
@@ -2659,6 +2694,34 @@ cs_status cs_tune(cs_ctx* c, const cs_step_params* p, int reps, cs_tune_result* 
     c->tunedDegree = bestP >= 0 ? degs[bestP] : 0;
     c->tunedCoarse = bestP >= 0 ? coarse[bestP] : 0;
     if (out) out->best_precond = bestP;
+    // the whole solve by each route: resident sheets on the cluster kernel (with the fastest
+    // preconditioner) and the rest in the batched loop, or every sheet in the batched loop
+    // (which wins when sheets too large for a cluster set the loop's trip count anyway)
+    {
+        cs_step_params q = *p;
+        if (bestP >= 0) {
+            q.precond_degree = degs[bestP];
+            q.coarse = coarse[bestP];
+        }
+        float ms[2] = {0.f, 0.f};
+        for (int k = 0; k < 2; k++) {
+            q.solver = k == 0 ? CS_SOLVER_AUTO : CS_SOLVER_BATCHED;
+            if (k == 0 && c->resClusters <= 0) continue;
+            const int nrep = reps < 2 ? reps : 2;
+            for (int r = 0; r <= nrep; r++) {
+                const float t = timeWholeSolve(c, q);
+                if (t < 0.f) return fail(c, CS_ERR_CUDA, "cs_tune: solve timing failed");
+                if (r > 0) ms[k] += t / nrep;
+            }
+        }
+        const int bestS = (c->resClusters > 0 && ms[0] <= ms[1]) ? CS_SOLVER_AUTO : CS_SOLVER_BATCHED;
+        c->tunedSolver = bestS;
+        if (out) {
+            out->solver_ms[0] = ms[0];
+            out->solver_ms[1] = ms[1];
+            out->best_solver = bestS;
+        }
+    }
     CS_CUDA(cudaGetLastError());
     CS_CUDA(cudaStreamSynchronize(c->stream));
     destroyGraphs(c);  // the captured steps launch the old SpMV shape

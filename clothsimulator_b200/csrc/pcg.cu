@@ -48,6 +48,28 @@ __device__ __forceinline__ T block_sum(T v, T* sh) {
     return t;
 }
 
+// Deterministic block sums of two values (blockDim.x == CS_REDUCE_THREADS): warp butterflies,
+// then the warps' partials in warp order.
+template <class T>
+__device__ __forceinline__ void block_sum2(T& a, T& b, T* sh) {
+    a = warp_sum(a);
+    b = warp_sum(b);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        sh[2 * w] = a;
+        sh[2 * w + 1] = b;
+    }
+    __syncthreads();
+    a = sh[0];
+    b = sh[1];
+#pragma unroll
+    for (int k = 1; k < CS_REDUCE_THREADS / 32; k++) {
+        a += sh[2 * k];
+        b += sh[2 * k + 1];
+    }
+    __syncthreads();
+}
+
 __device__ __forceinline__ bool finite_d(double x) { return x == x && x < 1e300 && x > -1e300; }
 
 }  // namespace
@@ -212,23 +234,85 @@ void launchSpmvShape(const Batch& B, int shape, cudaStream_t st) {
 #undef CS_SPMV_LAUNCH
 }
 
-// Sum of part[2*s + c] over an instance's slices: double for the mixed solver, float for the
-// plain FP32 solver.
-__device__ __forceinline__ double inst_sum(const Batch& B, const SheetDesc& sh, int c, bool mixed, double* shd,
-                                           float* shf) {
+// Sums of the two partials part[2 s], part[2 s + 1] over an instance's slices: double for the
+// mixed solver, float for the plain FP32 solver.  Each thread takes every CS_REDUCE_THREADS-th
+// slice, CS_REDUCE_UNROLL of them loaded together (16-byte loads of both partials) into as
+// many running sums, added in a fixed order: the same bits on every run, and a sheet of
+// 30,000 slices is summed in a few microseconds instead of one dependent load per slice.
+#define CS_REDUCE_UNROLL 8
+__device__ __forceinline__ void inst_sum2(const Batch& B, const SheetDesc& sh, bool mixed, double& s0, double& s1,
+                                          double* shd, float* shf) {
+    const double2* part = reinterpret_cast<const double2*>(B.part) + sh.slice_off;
+    const int n = sh.n_slices, t = threadIdx.x;
+    constexpr int T = CS_REDUCE_THREADS, U = CS_REDUCE_UNROLL;
     if (mixed) {
-        double acc = 0.0;
-        for (int i = threadIdx.x; i < sh.n_slices; i += blockDim.x) acc += B.part[2 * (sh.slice_off + i) + c];
-        return block_sum(acc, shd);
+        double a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) a[u] = b[u] = 0.0;
+        int i = t;
+        for (; i + (U - 1) * T < n; i += U * T) {
+            double2 v[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) v[u] = part[i + u * T];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                a[u] += v[u].x;
+                b[u] += v[u].y;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (i + u * T < n) {
+                const double2 v = part[i + u * T];
+                a[u] += v.x;
+                b[u] += v.y;
+            }
+        double x = a[0], y = b[0];
+#pragma unroll
+        for (int u = 1; u < U; u++) {
+            x += a[u];
+            y += b[u];
+        }
+        block_sum2(x, y, shd);
+        s0 = x;
+        s1 = y;
+        return;
     }
-    float acc = 0.f;
-    for (int i = threadIdx.x; i < sh.n_slices; i += blockDim.x) acc += (float)B.part[2 * (sh.slice_off + i) + c];
-    return (double)block_sum(acc, shf);
+    float a[U], b[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) a[u] = b[u] = 0.f;
+    int i = t;
+    for (; i + (U - 1) * T < n; i += U * T) {
+        double2 v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) v[u] = part[i + u * T];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            a[u] += (float)v[u].x;
+            b[u] += (float)v[u].y;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+        if (i + u * T < n) {
+            const double2 v = part[i + u * T];
+            a[u] += (float)v.x;
+            b[u] += (float)v.y;
+        }
+    float x = a[0], y = b[0];
+#pragma unroll
+    for (int u = 1; u < U; u++) {
+        x += a[u];
+        y += b[u];
+    }
+    block_sum2(x, y, shf);
+    s0 = (double)x;
+    s1 = (double)y;
 }
 
-__global__ void __launch_bounds__(128) cs_reduce1_kernel(Batch B) {
-    __shared__ double shd[4];
-    __shared__ float shf[4];
+__global__ void __launch_bounds__(CS_REDUCE_THREADS) cs_reduce1_kernel(Batch B) {
+    __shared__ double shd[2 * CS_REDUCE_THREADS / 32];
+    __shared__ float shf[2 * CS_REDUCE_THREADS / 32];
     const int s = blockIdx.x;
     if (s == 0 && threadIdx.x == 0) {
         B.loop[1] = 0;
@@ -240,8 +324,9 @@ __global__ void __launch_bounds__(128) cs_reduce1_kernel(Batch B) {
     const DevParams& P = *B.params;
     const bool mixed = P.mixed != 0;
     const SheetDesc& sh = B.sheets[s];
-    double sum = inst_sum(B, sh, 0, mixed, shd, shf);
-    const double drift2 = (ph == PH_RES && mixed) ? inst_sum(B, sh, 1, true, shd, shf) : 0.0;
+    double sum, drift2;
+    inst_sum2(B, sh, mixed || ph == PH_RES, sum, drift2, shd, shf);
+    if (!(ph == PH_RES && mixed)) drift2 = 0.0;
     if (threadIdx.x != 0) return;
     if (ph == PH_CG) {
         float alpha;
@@ -292,6 +377,10 @@ __global__ void __launch_bounds__(128) cs_reduce1_kernel(Batch B) {
     }
 }
 
+// Warp w takes the rows of slice w's position in natural order: rows 32 k .. 32 k + 31 of the
+// sheet for its k-th slice (a sheet has ceil(rows / 32) slices, the k-th holding as many rows
+// as that range), so every vector access is contiguous; the partials per slice index sum to
+// the same instance totals.
 __global__ void __launch_bounds__(128) cs_vector_kernel(Batch B) {
     int slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
@@ -302,7 +391,7 @@ __global__ void __launch_bounds__(128) cs_vector_kernel(Batch B) {
     if (ph != PH_CG && ph != PH_INIT && ph != PH_FINISH) return;
     const bool mixed = B.params->mixed != 0;
     const bool live = lane < sd.rows;
-    const int row = sd.row0 + (live ? B.rowmap[sd.topo_slice * CS_SLICE + lane] : 0);
+    const int row = sd.row0 + CS_SLICE * (slice - B.sheets[sd.sheet].slice_off) + (live ? lane : 0);
     double rz = 0.0, rr = 0.0;
     float rzf = 0.f, rrf = 0.f;
     if (live) {
@@ -375,9 +464,9 @@ __global__ void __launch_bounds__(128) cs_vector_kernel(Batch B) {
     }
 }
 
-__global__ void __launch_bounds__(128) cs_reduce2_kernel(Batch B, cudaGraphConditionalHandle handle) {
-    __shared__ double shd[4];
-    __shared__ float shf[4];
+__global__ void __launch_bounds__(CS_REDUCE_THREADS) cs_reduce2_kernel(Batch B, cudaGraphConditionalHandle handle) {
+    __shared__ double shd[2 * CS_REDUCE_THREADS / 32];
+    __shared__ float shf[2 * CS_REDUCE_THREADS / 32];
     const int s = blockIdx.x;
     InstState& I = B.inst[s];
     const int ph = I.phase;
@@ -385,8 +474,8 @@ __global__ void __launch_bounds__(128) cs_reduce2_kernel(Batch B, cudaGraphCondi
     const bool mixed = P.mixed != 0;
     const SheetDesc& sh = B.sheets[s];
     if (ph == PH_CG || ph == PH_INIT) {
-        double rz = inst_sum(B, sh, 0, mixed, shd, shf);
-        double rr = inst_sum(B, sh, 1, mixed, shd, shf);
+        double rz, rr;
+        inst_sum2(B, sh, mixed, rz, rr, shd, shf);
         if (threadIdx.x == 0) {
             const double bn = sqrt(I.bnorm2);
             if (ph == PH_INIT) {

@@ -88,6 +88,7 @@ class TuneResult(ctypes.Structure):
         ("spmv_threads", ctypes.c_int * 24), ("spmv_spw", ctypes.c_int * 24), ("spmv_unroll", ctypes.c_int * 24),
         ("precond_ms", ctypes.c_float * 6), ("precond_degree", ctypes.c_int * 6), ("precond_coarse", ctypes.c_int * 6),
         ("best_spmv", ctypes.c_int), ("best_precond", ctypes.c_int),
+        ("solver_ms", ctypes.c_float * 2), ("best_solver", ctypes.c_int),
     ]
 
 
@@ -365,7 +366,9 @@ class Context:
                    "ms": float(r.spmv_ms[k]), "checksum": int(r.spmv_checksum[k])} for k in range(24)]
         pre = [{"degree": r.precond_degree[k], "coarse": r.precond_coarse[k], "ms": float(r.precond_ms[k])}
                for k in range(6)]
-        return {"spmv": shapes, "best_spmv": r.best_spmv, "precond": pre, "best_precond": r.best_precond}
+        return {"spmv": shapes, "best_spmv": r.best_spmv, "precond": pre, "best_precond": r.best_precond,
+                "solver_ms": {"auto": float(r.solver_ms[0]), "batched": float(r.solver_ms[1])},
+                "best_solver": "auto" if r.best_solver == SOLVER_AUTO else "batched"}
 
     def resident_blocks(self) -> dict:
         """Blocks of the resident sheets' systems, the strip-local ones (read by each local SpMV

@@ -166,10 +166,13 @@ cs_status cs_get_solver_info(const cs_ctx* ctx, int* info);
  * of the batched SpMV -- threads per block, SELL slices per warp, block slots whose loads are
  * issued together -- reps launches each, and whole cluster-resident solves with each
  * preconditioner (block-Jacobi; strip-local Chebyshev of degree 3, 5 and 7 without and with the
- * coarse-space correction; one untimed, then the mean of min(reps, 3)).  Every SpMV shape computes the same bits (out->spmv_checksum holds a
+ * coarse-space correction; one untimed, then the mean of min(reps, 3)), then whole solves by
+ * either route (resident sheets on the cluster kernel and the rest in the batched loop, or all
+ * in the batched loop; one untimed, then the mean of min(reps, 2)).  Every SpMV shape computes the same bits (out->spmv_checksum holds a
  * checksum of each shape's output); the fastest is used by the following steps.  The fastest
  * preconditioner is reported (cs_get_solver_info info[9], info[10]) for the caller's
- * cs_step_params.precond_degree / coarse.  Overwrites the solver's scratch vectors (not x, v, dv);
+ * cs_step_params.precond_degree / coarse, and the faster route (out->best_solver) for its
+ * cs_step_params.solver.  Overwrites the solver's scratch vectors (not x, v, dv);
  * out may be NULL. */
 #define CS_TUNE_SPMV_SHAPES 24
 #define CS_TUNE_PRECONDS 6
@@ -180,6 +183,10 @@ typedef struct cs_tune_result {
     float precond_ms[CS_TUNE_PRECONDS];  /* 0 when no sheet is solved cluster-resident */
     int precond_degree[CS_TUNE_PRECONDS], precond_coarse[CS_TUNE_PRECONDS];
     int best_spmv, best_precond;         /* indices; best_precond -1 without resident sheets */
+    /* one whole solve of the system, with the fastest preconditioner: [0] CS_SOLVER_AUTO (0
+     * without resident sheets), [1] CS_SOLVER_BATCHED; best_solver = the faster one's code */
+    float solver_ms[2];
+    int best_solver;
 } cs_tune_result;
 cs_status cs_tune(cs_ctx* ctx, const cs_step_params* params, int reps, cs_tune_result* out);
 

@@ -32,6 +32,10 @@ def test_tuner_shapes_agree_and_the_choice_is_applied(ctx_factory):
     bp = res["precond"][res["best_precond"]]
     assert bp["ms"] == min(q["ms"] for q in res["precond"]) > 0
     assert (info["tuned_precond_degree"], info["tuned_coarse"]) == (bp["degree"], bp["coarse"])
+    # both solve routes timed, the faster reported
+    ms = res["solver_ms"]
+    assert ms["auto"] > 0 and ms["batched"] > 0
+    assert res["best_solver"] == ("auto" if ms["auto"] <= ms["batched"] else "batched")
     # the same step with the tuned shape: the same dv bits (graph rebuilt after tuning)
     ctx.set_state(x0, v0)
     ctx.step(p)
