@@ -81,9 +81,17 @@ def parse(argv=None):
     ap.add_argument("--partition", action="store_true",
                     help="with several ranks: split one workload's sheets across them, balanced by stored blocks "
                          "(strong scaling), per-sheet statistics all-gathered after each step")
-    ap.add_argument("--train-sheets", type=int, default=256, help="sheets of the training trajectories")
-    ap.add_argument("--train-steps", type=int, default=24, help="recorded steps per training trajectory")
-    ap.add_argument("--epochs", type=int, default=16)
+    ap.add_argument("--train-loss", default="energy", choices=["energy", "mse"],
+                    help="energy: online training on the trajectories' own systems, loss = relative error of the "
+                         "prediction in the energy norm (cs_mlp_train_step); mse: recorded (state, dv) pairs, "
+                         "squared error of dv (cs_mlp_train)")
+    ap.add_argument("--train-sheets", type=int, default=None,
+                    help="sheets (trajectories) of the training set (default: energy 1,024, mse 256)")
+    ap.add_argument("--train-steps", type=int, default=None,
+                    help="steps per training trajectory (default: energy 200, mse 24)")
+    ap.add_argument("--epochs", type=int, default=None, help="passes over the trajectories (default: energy 1, mse 16)")
+    ap.add_argument("--train-lr", type=float, default=1e-3)
+    ap.add_argument("--train-batch", type=int, default=16, help="sheets per minibatch (energy training)")
     ap.add_argument("--weights", default="", help="load trained warm-start weights instead of training")
     ap.add_argument("--no-plain", action="store_true", help="skip the comparison arms")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -165,6 +173,16 @@ class RankGroup:
 
         t = torch.from_numpy(np.array(a, np.float64))
         self.dist.all_reduce(t)
+        return t.numpy()
+
+    def bcast_host(self, a):
+        """Rank 0's float32 numpy array on every rank (gloo broadcast)."""
+        if not self.dist:
+            return a
+        import torch
+
+        t = torch.from_numpy(np.array(a, np.float32))
+        self.dist.broadcast(t, src=0)
         return t.numpy()
 
     def nccl_group(self):
@@ -361,44 +379,119 @@ def workload_sheets(args):
 
 def train_warm_start(args, group, local):
     """The learned warm start: trained on the device on separate seeded windy trajectories (the
-    evaluated seeds are held out; data parallel over the ranks when there are several), or loaded
-    from --weights.  Returns (weights, training record)."""
+    evaluated seeds are held out), or loaded from --weights.  Returns (weights, training record).
+
+    energy (default): the network is trained online along 1,024 trajectories of 200 steps (the
+    specified training set), each step solved by the solver without the learned start; between
+    a step's solve and its state update, one Adam step per minibatch of sheets on the relative
+    error of the prediction in the energy norm of that step's system (cs_mlp_train_step), the
+    normalisation fitted first on a few recorded steps.  With several ranks, rank 0 trains and
+    broadcasts the weights.  mse: recorded (state, dv) pairs, squared error (cs_mlp_train), data
+    parallel over the ranks."""
     from clothsimulator_b200 import native
 
     rank, world = group.rank, group.world
     t0 = time.perf_counter()
+    energy = args.train_loss == "energy"
+    sheets = args.train_sheets or (1024 if energy else 256)
+    steps = args.train_steps or (200 if energy else 24)
+    epochs = args.epochs or (1 if energy else 16)
     if args.weights:
         weights = np.fromfile(args.weights, dtype=np.float32)
         info = {"source": args.weights}
+    elif energy:
+        weights = np.zeros(native.MLP_PARAMS, np.float32)
+        info = {}
+        if rank == 0:
+            tscene = scenes_mod().windy_batch(sheets, args.nq, seed=train_seed(0))
+            tctx = native.Context(local)
+            tctx.load(tscene.sheets)
+            n_norm = 6
+            tctx.mlp_init(n_norm, 1)
+            tp = native.step_params(tscene.dt, tscene.gravity, tscene.handle_stiffness, tol=args.tol, max_iters=20000,
+                                    precond_degree=3, coarse=1)
+            # normalisation from the features and targets of steps 10-15 (past the start from
+            # rest); the output is not shifted (mean 0, scale the targets' RMS), so that the
+            # untrained network predicts about the previous dv
+            n_skip = 10
+            for t in range(n_skip + n_norm):
+                if t >= n_skip:
+                    tctx.assemble(tp)
+                    tctx.mlp_record(t - n_skip, 0)
+                tctx.step(tp, allow_unconverged=True)
+                if t >= n_skip:
+                    tctx.mlp_record(t - n_skip, 1)
+                tp.warm_start = native.WARM_PREVIOUS
+            sums, count = tctx.mlp_moments(n_norm)
+            sums[16:19] = 0.0
+            tctx.mlp_set_moments(sums, count)
+            xs = np.concatenate([s["x"] for s in tscene.sheets])
+            vs = np.concatenate([s["v"] for s in tscene.sheets])
+            curve = []
+            for ep in range(epochs):
+                tctx.set_state(xs, vs)
+                tp.warm_start = native.WARM_ZERO
+                ep_loss = []
+                for t in range(steps):
+                    if t < 2:
+                        # the first steps from rest (no previous dv yet) are not trained on
+                        tctx.step(tp, allow_unconverged=True)
+                    else:
+                        _, loss = tctx.mlp_train_step(tp, lr=args.train_lr, sheets_per_batch=args.train_batch,
+                                                      seed=1 + ep * steps + t, allow_unconverged=True)
+                        ep_loss.append(loss)
+                    tp.warm_start = native.WARM_PREVIOUS
+                curve.append(ep_loss)
+            weights = tctx.mlp_get_weights()
+            tctx.close()
+            first, last = curve[0], curve[-1]
+            k = max(1, steps // 10)
+            info = {"loss": "sin^2 of the angle between prediction and solution in the energy inner product of the "
+                            "step's system (the Galerkin-scaled start's squared energy error relative to the zero "
+                            "guess's), mean over sheets",
+                    "sheets": sheets, "steps": steps, "epochs": epochs, "lr": args.train_lr,
+                    "sheets_per_minibatch": args.train_batch,
+                    "adam_steps": epochs * steps * ((sheets + args.train_batch - 1) // args.train_batch),
+                    "trajectories": f"windy{sheets}x{args.nq}, seeds disjoint from the evaluated workload, solved "
+                                    "without the learned start (mixed PCG, Chebyshev-3 + coarse correction)",
+                    "loss_first_epoch_first_steps": float(np.mean(first[:k])),
+                    "loss_first_epoch_last_steps": float(np.mean(first[-k:])),
+                    "loss_last_epoch_first_steps": float(np.mean(last[:k])),
+                    "loss_last_epoch_last_steps": float(np.mean(last[-k:])),
+                    "loss_epoch_means": [float(np.mean(c)) for c in curve]}
+        if world > 1:
+            weights = group.bcast_host(weights)
+            info["ranks"] = world
+            info["trained_on"] = "rank 0, weights broadcast"
     else:
-        tscene = scenes_mod().windy_batch(args.train_sheets, args.nq, seed=train_seed(rank))
+        tscene = scenes_mod().windy_batch(sheets, args.nq, seed=train_seed(rank))
         tctx = native.Context(local)
         tctx.load(tscene.sheets)
-        tctx.mlp_init(args.train_steps, 1)  # the same initial weights on every rank
+        tctx.mlp_init(steps, 1)  # the same initial weights on every rank
         tp = native.step_params(tscene.dt, tscene.gravity, tscene.handle_stiffness, tol=1e-7, max_iters=8000)
         for _ in range(2):
             tctx.step(tp, allow_unconverged=True)
             tp.warm_start = native.WARM_PREVIOUS
-        for t in range(args.train_steps):
+        for t in range(steps):
             tctx.assemble(tp)
             tctx.mlp_record(t, 0)
             tctx.step(tp, allow_unconverged=True)
             tctx.mlp_record(t, 1)
         if world == 1:
-            tctx.mlp_fit_normalization(args.train_steps)
-            losses = tctx.mlp_train(args.train_steps, args.epochs, lr=1e-3, sheets_per_batch=32, seed=3)
+            tctx.mlp_fit_normalization(steps)
+            losses = tctx.mlp_train(steps, epochs, lr=args.train_lr, sheets_per_batch=32, seed=3)
         else:
             # data parallel: every rank trains on its own trajectories, gradients summed over
             # NCCL and averaged, normalisation from the moments summed over the ranks
             from clothsimulator_b200 import training
 
-            losses = training.train_data_parallel(tctx, args.train_steps, args.train_sheets, args.epochs, 1e-3,
+            losses = training.train_data_parallel(tctx, steps, sheets, epochs, args.train_lr,
                                                   32, 3, allreduce_sum=group.device_allreduce(), world=world,
                                                   sum_host=group.sum_host)
         weights = tctx.mlp_get_weights()
         tctx.close()
-        info = {"sheets": args.train_sheets, "steps": args.train_steps, "epochs": args.epochs,
-                "trajectories": f"windy{args.train_sheets}x{args.nq}, seeds disjoint from the evaluated workload",
+        info = {"loss": "squared error of dv", "sheets": sheets, "steps": steps, "epochs": epochs,
+                "trajectories": f"windy{sheets}x{args.nq}, seeds disjoint from the evaluated workload",
                 "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
         if world > 1:
             digest = float(np.float64(weights).sum())
@@ -515,6 +608,21 @@ def run_ours(args):
         weights, train_info = train_warm_start(args, group, local)
         ctx.mlp_init(0, 0)
         ctx.mlp_set_weights(weights)
+        if all(s["x"].shape[0] <= 300000 for s in scene.sheets) and not any(len(s.get("prox", [])) for s in scene.sheets):
+            # the energy-norm loss (sin^2 of the A-angle to the solution; the Galerkin-scaled
+            # start's squared energy error relative to the zero guess's) on this workload at the
+            # state the timed steps start from, for the trained network and for the previous dv
+            # alone (the network with its output layer zeroed)
+            ep = native.step_params(scene.dt, scene.gravity, scene.handle_stiffness, tol=args.tol, max_iters=20000,
+                                    precond_degree=3, coarse=1, warm_start=native.WARM_PREVIOUS, advance=0)
+            _, l_net = ctx.mlp_energy_gradient(ep, 0, ctx.n_sheets)
+            w0 = np.array(weights, np.float32)
+            w0[14528:native.MLP_TRAINED] = 0.0  # output layer W4, b4
+            ctx.mlp_set_weights(w0)
+            _, l_prev = ctx.mlp_energy_gradient(ep, 0, ctx.n_sheets)
+            ctx.mlp_set_weights(weights)
+            train_info["evaluated_sin2"] = {"network": l_net, "previous_dv": l_prev,
+                                            "state": "the evaluated workload after the warm-up steps"}
 
     solver_code = {"auto": native.SOLVER_AUTO, "batched": native.SOLVER_BATCHED}
     warm_code = {"previous": native.WARM_PREVIOUS, "zero": native.WARM_ZERO, "learned": native.WARM_LEARNED}
@@ -528,6 +636,8 @@ def run_ours(args):
     def timed_arm(precision, warm, solver, degree, coarse, tol, clocks=None):
         ctx.set_state(x0, v0)
         p = arm_params(precision, solver, degree, coarse, tol)
+        # the learned start is replaced by its Galerkin multiple before the guard (warm_scale)
+        p.warm_scale = 1 if warm == native.WARM_LEARNED else 0
         for i in range(args.warmup):
             ctx.step(p, allow_unconverged=True)
             p.warm_start = warm

@@ -79,6 +79,7 @@ enum InstPhase : int {
     PH_FINISH = 3,    // dv64 += e, then done
     PH_DONE = 4,
     PH_RESIDENT = 5,  // owned by the cluster-resident kernel this step (skipped by the loop)
+    PH_SCALE = 6,     // dv64 *= wscale (the warm start's Galerkin multiple), then PH_RES
 };
 
 // Cluster-resident solver limits: CTAs per cluster, warps (slices) per CTA, block slots per
@@ -141,6 +142,9 @@ struct InstState {
     int sweeps;         // FP64 residual evaluations this step
     int flags;
     int cont;           // the next PH_INIT keeps the search direction (reliable update)
+    double wscale;      // Galerkin multiple of the warm start (warm_scale)
+    int scaled;         // the warm start's scaling pass is done
+    int pad;
 };
 
 // Step parameters in device memory (read by every kernel of the captured step graph).
@@ -156,6 +160,7 @@ struct DevParams {
     int warm;              // 0 zero guess, 1 warm start from dv64 as preloaded
     int loop_cap;          // hard bound on loop trips per step
     int advance;           // 1: v += dv, x += dt v at the end of the step
+    int warm_scale;        // 1: the warm start replaced by its Galerkin multiple before the guard
     int solver;            // CS_SOLVER_AUTO_DEV: resident sheets on the cluster kernel; BATCHED: loop only
     int cheb_degree;       // resident solver: 1 block-Jacobi; odd >= 3 strip-local Chebyshev of that degree
     int coarse;            // resident solver with the Chebyshev preconditioner: 1 adds the coarse-space correction

@@ -1041,6 +1041,7 @@ DevParams toDev(const cs_step_params* p) {
     d.loop_cap = 2 * d.max_iters + 256;
     d.advance = p->advance;
     d.solver = p->solver == CS_SOLVER_BATCHED ? CS_SOLVER_BATCHED_DEV : CS_SOLVER_AUTO_DEV;
+    d.warm_scale = p->warm_scale != 0;
     d.cheb_degree = p->precond_degree >= 3 ? p->precond_degree : 1;
     d.coarse = p->coarse != 0;
     d.n_motions = p->transformations ? std::min(std::max(p->n_transformations, 0), CS_MAX_MOTIONS) : 0;
@@ -2288,6 +2289,41 @@ cs_status cs_assemble(cs_ctx* c, const cs_step_params* p) {
     return CS_OK;
 }
 
+// The step statistics of the last solve (per-sheet states, trip count), and the status it
+// implies; `timed`: the step's duration between the context's events.
+static cs_status fillStepStats(cs_ctx* c, cs_step_stats* stats, int loop_cap, bool timed) {
+    std::vector<InstState> inst(c->B.S);
+    int loopv[8];
+    CS_CUDA(cudaMemcpyAsync(inst.data(), c->B.inst, c->B.S * sizeof(InstState), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaMemcpyAsync(loopv, c->B.loop, sizeof(loopv), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    memset(stats, 0, sizeof(*stats));
+    stats->n_instances = c->B.S;
+    stats->loop_trips = loopv[0];
+    bool capped = false, breakdown = false;
+    for (int s = 0; s < c->B.S; s++) {
+        const InstState& I = inst[s];
+        stats->converged += (I.flags & CS_IF_CONVERGED) ? 1 : 0;
+        stats->max_iters = std::max(stats->max_iters, I.iters);
+        stats->total_iters += I.iters;
+        stats->max_sweeps = std::max(stats->max_sweeps, I.sweeps);
+        stats->warm_rejected += (I.flags & CS_IF_WARM_REJECTED) ? 1 : 0;
+        double bn = std::sqrt(I.bnorm2);
+        double rel = bn > 0 ? I.resnorm / bn : 0.0;
+        stats->max_rel_residual = std::max(stats->max_rel_residual, rel);
+        if (!(I.flags & CS_IF_CONVERGED)) capped = true;
+        if (I.flags & CS_IF_BREAKDOWN) breakdown = true;
+    }
+    float ms = 0.f;
+    if (timed) CS_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    stats->ms = ms;
+    if (loopv[0] >= loop_cap) return fail(c, CS_ERR_TIMEOUT, "solve loop hit its trip bound (%d)", loop_cap);
+    if (loopv[6]) return fail(c, CS_ERR_TIMEOUT, "cluster-resident solve: a wait on another CTA ran out");
+    if (capped) return fail(c, breakdown ? CS_ERR_NON_SPD : CS_ERR_NOT_CONVERGED, "%d of %d sheets did not converge",
+                            c->B.S - stats->converged, c->B.S);
+    return CS_OK;
+}
+
 cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
     if (!c) return CS_ERR_INVALID_ARG;
     if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
@@ -2329,36 +2365,7 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
                                  (c->B.n_pinst > 0 ? 3 : 0);
     }
     if (!stats) return CS_OK;
-    std::vector<InstState> inst(c->B.S);
-    int loopv[8];
-    CS_CUDA(cudaMemcpyAsync(inst.data(), c->B.inst, c->B.S * sizeof(InstState), cudaMemcpyDeviceToHost, c->stream));
-    CS_CUDA(cudaMemcpyAsync(loopv, c->B.loop, sizeof(loopv), cudaMemcpyDeviceToHost, c->stream));
-    CS_CUDA(cudaStreamSynchronize(c->stream));
-    memset(stats, 0, sizeof(*stats));
-    stats->n_instances = c->B.S;
-    stats->loop_trips = loopv[0];
-    bool capped = false, breakdown = false;
-    for (int s = 0; s < c->B.S; s++) {
-        const InstState& I = inst[s];
-        stats->converged += (I.flags & CS_IF_CONVERGED) ? 1 : 0;
-        stats->max_iters = std::max(stats->max_iters, I.iters);
-        stats->total_iters += I.iters;
-        stats->max_sweeps = std::max(stats->max_sweeps, I.sweeps);
-        stats->warm_rejected += (I.flags & CS_IF_WARM_REJECTED) ? 1 : 0;
-        double bn = std::sqrt(I.bnorm2);
-        double rel = bn > 0 ? I.resnorm / bn : 0.0;
-        stats->max_rel_residual = std::max(stats->max_rel_residual, rel);
-        if (!(I.flags & CS_IF_CONVERGED)) capped = true;
-        if (I.flags & CS_IF_BREAKDOWN) breakdown = true;
-    }
-    float ms = 0.f;
-    CS_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-    stats->ms = ms;
-    if (loopv[0] >= d.loop_cap) return fail(c, CS_ERR_TIMEOUT, "solve loop hit its trip bound (%d)", d.loop_cap);
-    if (loopv[6]) return fail(c, CS_ERR_TIMEOUT, "cluster-resident solve: a wait on another CTA ran out");
-    if (capped) return fail(c, breakdown ? CS_ERR_NON_SPD : CS_ERR_NOT_CONVERGED, "%d of %d sheets did not converge",
-                            c->B.S - stats->converged, c->B.S);
-    return CS_OK;
+    return fillStepStats(c, stats, d.loop_cap, true);
 }
 
 cs_status cs_sync(cs_ctx* c) {
@@ -2788,6 +2795,56 @@ cs_status mlpCheckErr(cs_ctx* c) {
 
 // One forward + backward pass over sheets [s0, s1) of dataset slot `slot`; leaves the
 // per-CTA gradient partials and loss partials in place.
+// Energy-norm forward and backward over sheets [s0, s1): features in M.feat, the system
+// assembled, M.sheet_c holding each sheet's dv*^T b; the prediction goes to M.pred, its
+// gradient partials to M.gpart and the sheets' losses to M.sheet_loss.
+void mlpEnergyForwardBackward(cs_ctx* c, int s0, int s1) {
+    Batch& B = c->B;
+    MlpDev& M = c->mlp;
+    const SheetDesc &a = c->sheets[s0], &z = c->sheets[s1 - 1];
+    const int n0 = a.node_off, n1 = z.node_off + z.n_nodes;
+    const int sl0 = a.slice_off, sl1 = z.slice_off + z.n_slices;
+    cs_mlp_l1_kernel<<<c->mlpGridTile, 128, MLP_SMEM_L1, c->stream>>>(B, M, M.feat, n0, n1, M.z1);
+    cs_mlp_l23_kernel<<<c->mlpGridTile, 128, MLP_SMEM_L23, c->stream>>>(B, M, n0, n1, M.z2, M.z3, M.y, M.pred);
+    cs_mlp_energy_kernel<<<nblk((long long)(sl1 - sl0) * 32, 128), 128, 0, c->stream>>>(B, M, sl0, sl1);
+    cs_mlp_energy_sheet_kernel<<<s1 - s0, 128, 0, c->stream>>>(B, M, s0, s1, 1);
+    cs_mlp_bwd23_kernel<<<c->mlpGridTrain, 128, MLP_SMEM_BWD23, c->stream>>>(B, M, n0, n1, nullptr);
+    cs_mlp_bwd1_kernel<<<c->mlpGridTrain, 128, MLP_SMEM_BWD1, c->stream>>>(B, M, M.feat, n0, n1);
+}
+
+// The first half of a training step: assembly for the current state, the features of that
+// system (with the previous dv in B.warm), the solve (host-driven launches), and every sheet's
+// solution energy dv*^T b.
+cs_status mlpEnergyPrepare(cs_ctx* c, const cs_step_params* p) {
+    if (!c->mlpInit) return fail(c, CS_ERR_STATE, "cs_mlp_init first");
+    if (p->warm_start == CS_WARM_LEARNED)
+        return fail(c, CS_ERR_INVALID_ARG, "training steps solve without the learned warm start");
+    if (c->B.n_pinst > 0) return fail(c, CS_ERR_STATE, "training steps take batches without proximities");
+    cs_status st = validateParams(c, p);
+    if (st != CS_OK) return st;
+    CS_CUDA(cudaSetDevice(c->device));
+    Batch& B = c->B;
+    MlpDev& M = c->mlp;
+    DevParams d = toDev(p);
+    CS_CUDA(cudaMemcpyAsync(B.params, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
+    launchAssembly(c);
+    cs_mlp_features_kernel<<<nblk(B.N, 256), 256, 0, c->stream>>>(B, M, M.feat);
+    launchSolvePrologue(c);
+    launchResident(c);
+    int go = 1, trips = 0;
+    while (go) {
+        for (int t = 0; t < 8; t++) launchTrip(c, 0);
+        trips += 8;
+        CS_CUDA(cudaMemcpyAsync(&go, B.loop + 3, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CS_CUDA(cudaStreamSynchronize(c->stream));
+        if (trips > d.loop_cap + 16) break;
+    }
+    cs_mlp_energy_norm_kernel<<<nblk((long long)B.n_slices * 32, 128), 128, 0, c->stream>>>(B, M, 0, B.n_slices);
+    cs_mlp_energy_sheet_kernel<<<B.S, 128, 0, c->stream>>>(B, M, 0, B.S, 0);
+    CS_CUDA(cudaGetLastError());
+    return CS_OK;
+}
+
 void mlpForwardBackward(cs_ctx* c, int slot, int s0, int s1) {
     Batch& B = c->B;
     MlpDev& M = c->mlp;
@@ -2841,6 +2898,12 @@ cs_status cs_mlp_init(cs_ctx* c, int slots, unsigned long long seed) {
     MA(du2, N * 128);
     MA(dfeat, std::max(1LL, (long long)slots * N * 16));
     MA(dtarget, std::max(1LL, (long long)slots * N * 3));
+    MA(pred, N * 3);
+    MA(dy, N * 3);
+    MA(epart, 2LL * c->B.n_slices);
+    MA(sheet_c, c->B.S);
+    MA(sheet_scale, 2LL * c->B.S);
+    MA(sheet_loss, c->B.S);
     MA(err, 1);
 #undef MA
     if ((st = dalloc(c, &c->mlpScratch, 4096 + MLP_P)) != CS_OK) return st;
@@ -3011,6 +3074,64 @@ cs_status cs_mlp_train(cs_ctx* c, int n_slots, int epochs, float lr, int sheets_
         CS_CUDA(cudaMemcpy(h.data(), acc, epochs * sizeof(float), cudaMemcpyDeviceToHost));
         for (int ep = 0; ep < epochs; ep++) epoch_loss[ep] = h[ep] / (float)order.size();
     }
+    return mlpCheckErr(c);
+}
+
+cs_status cs_mlp_train_step(cs_ctx* c, const cs_step_params* p, float lr, int sheets_per_batch,
+                            unsigned long long seed, cs_step_stats* stats, float* loss) {
+    if (!c || !p || !(lr > 0) || sheets_per_batch <= 0) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    cs_status st = mlpEnergyPrepare(c, p);
+    if (st != CS_OK) return st;
+    const int S = c->B.S;
+    const int groups = (S + sheets_per_batch - 1) / sheets_per_batch;
+    std::vector<int> order(groups);
+    for (int g = 0; g < groups; g++) order[g] = g;
+    uint64_t rs = seed;
+    for (int i = groups; i > 1; i--) std::swap(order[i - 1], order[splitmix(rs) % i]);
+    float* acc = c->mlpScratch;
+    CS_CUDA(cudaMemsetAsync(acc, 0, sizeof(float), c->stream));
+    for (int g : order) {
+        const int s0 = g * sheets_per_batch, s1 = std::min(S, s0 + sheets_per_batch);
+        mlpEnergyForwardBackward(c, s0, s1);
+        cs_mlp_energy_loss_kernel<<<1, 32, 0, c->stream>>>(c->mlp, s0, s1, acc);
+        c->adamStep++;
+        cs_mlp_adam_kernel<<<nblk(MLP_P, 256), 256, 0, c->stream>>>(c->mlp, c->mlpGridTrain, lr, 0.9f, 0.999f, 1e-8f,
+                                                                   (int)c->adamStep, nullptr);
+    }
+    // the end of the step: dv = the solution, v and x updated when asked (cs_advance_kernel)
+    cs_advance_kernel<<<nblk(3LL * c->B.N, 256), 256, 0, c->stream>>>(c->B);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    c->lastStepValid = true;
+    c->steps++;
+    if ((st = mlpCheckErr(c)) != CS_OK) return st;
+    if (loss) {
+        float h = 0.f;
+        CS_CUDA(cudaMemcpy(&h, acc, sizeof(float), cudaMemcpyDeviceToHost));
+        *loss = h / (float)groups;
+    }
+    if (stats) return fillStepStats(c, stats, toDev(p).loop_cap, false);
+    return CS_OK;
+}
+
+cs_status cs_mlp_energy_gradient(cs_ctx* c, const cs_step_params* p, int s0, int s1, float* grad, float* loss) {
+    if (!c || !p || !grad) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    if (s0 < 0 || s1 <= s0 || s1 > c->B.S) return fail(c, CS_ERR_INVALID_ARG, "bad sheet range");
+    cs_status st = mlpEnergyPrepare(c, p);
+    if (st != CS_OK) return st;
+    float* acc = c->mlpScratch;
+    float* gout = c->mlpScratch + 4096;
+    CS_CUDA(cudaMemsetAsync(acc, 0, sizeof(float), c->stream));
+    mlpEnergyForwardBackward(c, s0, s1);
+    cs_mlp_energy_loss_kernel<<<1, 32, 0, c->stream>>>(c->mlp, s0, s1, acc);
+    cs_mlp_adam_kernel<<<nblk(MLP_P, 256), 256, 0, c->stream>>>(c->mlp, c->mlpGridTrain, 0.f, 0.f, 0.f, 0.f, 1, gout);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    c->lastStepValid = false;
+    CS_CUDA(cudaMemcpy(grad, gout, MLP_P * sizeof(float), cudaMemcpyDeviceToHost));
+    if (loss) CS_CUDA(cudaMemcpy(loss, acc, sizeof(float), cudaMemcpyDeviceToHost));
     return mlpCheckErr(c);
 }
 

@@ -440,9 +440,12 @@ __global__ void __launch_bounds__(128) cs_mlp_l23_kernel(Batch B, MlpDev M, int 
 }
 
 // Backward through the output layer, layer 3 and layer 2 over nodes [n0, n1) (one training
-// minibatch of whole sheets, ntot nodes).  Loss = sum_i ||y_i - t_i||^2 / ntot with
-// t_i = (target_i - mu_y) / sigma_y.  Writes du2 (N x 128) for layer 1's backward and this
-// CTA's gradient partials of W2, b2, W3, b3, W4, b4 and of the loss.
+// minibatch of whole sheets, ntot nodes).  With a target: loss = sum_i ||y_i - t_i||^2 / ntot
+// with t_i = (target_i - mu_y) / sigma_y.  Without (target == nullptr): the energy-norm loss,
+// whose gradient with respect to the prediction, ga A p - gb b, the energy kernels left (A p in
+// M.dy, ga and gb per sheet in M.sheet_scale; dL/dy = sigma_y dL/dp); its value comes from those
+// kernels.  Writes du2 (N x 128) for
+// layer 1's backward and this CTA's gradient partials of W2, b2, W3, b3, W4, b4 and of the loss.
 __global__ void __launch_bounds__(128) cs_mlp_bwd23_kernel(Batch B, MlpDev M, int n0, int n1,
                                                          const float* __restrict__ target) {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -486,13 +489,18 @@ __global__ void __launch_bounds__(128) cs_mlp_bwd23_kernel(Batch B, MlpDev M, in
         const bool valid = node < n1;
         // 1. dy, h3, dz3
         float dy[3] = {0.f, 0.f, 0.f};
-        if (valid) {
+        if (valid && target) {
             for (int i = 0; i < 3; i++) {
                 const float tt = (target[3 * (size_t)node + i] - sf[192 + i]) / sf[195 + i];
                 const float d = M.y[3 * (size_t)node + i] - tt;
                 loss += d * d;
                 dy[i] = scale * d;
             }
+        } else if (valid) {
+            const int sh = B.node_sheet[node];
+            const float ga = M.sheet_scale[2 * sh], gb = M.sheet_scale[2 * sh + 1];
+            for (int i = 0; i < 3; i++)
+                dy[i] = (ga * M.dy[3 * (size_t)node + i] - gb * B.b[3 * (size_t)node + i]) * sf[195 + i];
         }
         for (int i = 0; i < 3; i++) sDY[4 * t + i] = dy[i];
         for (int j = 0; j < 64; j++) {
@@ -779,4 +787,140 @@ __global__ void cs_mlp_loss_acc_kernel(MlpDev M, int ncta, float* acc) {
     float s = 0.f;
     for (int c = 0; c < ncta; c++) s += M.loss_part[c];
     *acc += s;
+}
+
+// ---------------------------------------------------------------------------------------
+// Energy-norm training.  For a sheet with system A dv = b and solution dv*, the warm start the
+// solver takes from a prediction p is its Galerkin multiple alpha p, alpha = p^T b / p^T A p
+// (warm_scale), whose error in the energy norm is that of the zero guess times sin(theta),
+// theta the angle between p and dv* in the A inner product.  The loss is therefore
+//     L = sin^2(theta) = 1 - (p^T b)^2 / ((p^T A p)(dv*^T b))      (A dv* = b, in [0, 1]),
+// scale-free and bounded; with u = p^T b, w = p^T A p, c = dv*^T b:
+//     dL/dp = (2 u / (w c)) (alpha A p - b): one SpMV of the prediction.
+// A minibatch's loss is the mean over its sheets.
+
+namespace {
+__device__ __forceinline__ double rwsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+}  // namespace
+
+// Per row q = A p into M.dy over slices [sl0, sl1) (a warp per slice, its rows as the SELL
+// panels hold them), and per slice the FP64 partials of p.b and p.A p.
+__global__ void __launch_bounds__(128) cs_mlp_energy_kernel(Batch B, MlpDev M, int sl0, int sl1) {
+    const int slice = sl0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (slice >= sl1) return;
+    const SliceDesc sd = B.slices[slice];
+    const int node_off = B.sheets[sd.sheet].node_off;
+    const float* __restrict__ x = M.pred;
+    double pb = 0.0, pq = 0.0;
+    if (lane < sd.rows) {
+        const int row = sd.row0 + B.rowmap[sd.topo_slice * CS_SLICE + lane];
+        float y0 = 0.f, y1 = 0.f, y2 = 0.f;
+        for (int k = 0; k < sd.width; k++) {
+            const int col = B.tcol[(sd.tpanel0 + k) * CS_SLICE + lane] + node_off;
+            const float* panel = B.A + (size_t)(sd.panel0 + k) * CS_PANEL_FLOATS;
+            const float4 a0 = reinterpret_cast<const float4*>(panel)[lane];
+            const float4 a1 = reinterpret_cast<const float4*>(panel + 128)[lane];
+            const float a8 = panel[256 + lane];
+            const float p0 = x[3 * col], p1 = x[3 * col + 1], p2 = x[3 * col + 2];
+            y0 += a0.x * p0 + a0.y * p1 + a0.z * p2;
+            y1 += a0.w * p0 + a1.x * p1 + a1.y * p2;
+            y2 += a1.z * p0 + a1.w * p1 + a8 * p2;
+        }
+        if (B.xptr) {
+            for (int m = B.xptr[row]; m < B.xptr[row + 1]; m++) {
+                const int col = B.xcol[m];
+                const float* a = B.xval + 9 * (size_t)m;
+                const float p0 = x[3 * col], p1 = x[3 * col + 1], p2 = x[3 * col + 2];
+                y0 += a[0] * p0 + a[1] * p1 + a[2] * p2;
+                y1 += a[3] * p0 + a[4] * p1 + a[5] * p2;
+                y2 += a[6] * p0 + a[7] * p1 + a[8] * p2;
+            }
+        }
+        const float y[3] = {y0, y1, y2};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            M.dy[3 * row + c] = y[c];
+            pb += (double)x[3 * row + c] * (double)B.b[3 * row + c];
+            pq += (double)x[3 * row + c] * (double)y[c];
+        }
+    }
+    pb = rwsum(pb);
+    pq = rwsum(pq);
+    if (lane == 0) {
+        M.epart[2 * slice] = pb;
+        M.epart[2 * slice + 1] = pq;
+    }
+}
+
+// Per slice the FP64 partial of dv64 . b (the solution's energy dv*^T A dv* = dv*^T b).
+__global__ void __launch_bounds__(128) cs_mlp_energy_norm_kernel(Batch B, MlpDev M, int sl0, int sl1) {
+    const int slice = sl0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (slice >= sl1) return;
+    const SliceDesc sd = B.slices[slice];
+    double e = 0.0;
+    if (lane < sd.rows) {
+        const int row = sd.row0 + B.rowmap[sd.topo_slice * CS_SLICE + lane];
+#pragma unroll
+        for (int c = 0; c < 3; c++) e += B.dv64[3 * row + c] * (double)B.b[3 * row + c];
+    }
+    e = rwsum(e);
+    if (lane == 0) {
+        M.epart[2 * slice] = e;
+        M.epart[2 * slice + 1] = 0.0;
+    }
+}
+
+// A block per sheet of [s0, s1) sums its slices' partials in a fixed order.  mode 0: the
+// solution's energy c into M.sheet_c; mode 1: with u = p.b, w = p.A p, the sheet's loss
+// 1 - u^2 / (w c) and the two coefficients of its gradient dL/dp = ga A p - gb b,
+// gb = 2 u / (w c (s1 - s0)), ga = gb u / w (a sheet with w <= 0 or c <= 0: loss 1, no gradient).
+__global__ void __launch_bounds__(128) cs_mlp_energy_sheet_kernel(Batch B, MlpDev M, int s0, int s1, int mode) {
+    __shared__ double sh[8];
+    const int s = s0 + blockIdx.x;
+    if (s >= s1) return;
+    const SheetDesc& d = B.sheets[s];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < d.n_slices; i += blockDim.x) {
+        a += M.epart[2 * (d.slice_off + i)];
+        b += M.epart[2 * (d.slice_off + i) + 1];
+    }
+    a = rwsum(a);
+    b = rwsum(b);
+    if ((threadIdx.x & 31) == 0) {
+        sh[2 * (threadIdx.x >> 5)] = a;
+        sh[2 * (threadIdx.x >> 5) + 1] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const double u = (sh[0] + sh[2]) + (sh[4] + sh[6]);
+    const double w = (sh[1] + sh[3]) + (sh[5] + sh[7]);
+    if (mode == 0) {
+        M.sheet_c[s] = u;
+        return;
+    }
+    const double c = M.sheet_c[s];
+    if (w > 0.0 && c > 0.0) {
+        const double gb = 2.0 * u / (w * c * (double)(s1 - s0));
+        M.sheet_loss[s] = (float)(1.0 - u * u / (w * c));
+        M.sheet_scale[2 * s] = (float)(gb * u / w);
+        M.sheet_scale[2 * s + 1] = (float)gb;
+    } else {
+        M.sheet_loss[s] = 1.f;
+        M.sheet_scale[2 * s] = 0.f;
+        M.sheet_scale[2 * s + 1] = 0.f;
+    }
+}
+
+// *acc += the mean of the sheets' losses over [s0, s1), summed in sheet order.
+__global__ void cs_mlp_energy_loss_kernel(MlpDev M, int s0, int s1, float* acc) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    float t = 0.f;
+    for (int s = s0; s < s1; s++) t += M.sheet_loss[s];
+    *acc += t / (float)max(s1 - s0, 1);
 }

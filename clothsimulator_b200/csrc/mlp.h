@@ -30,6 +30,13 @@ struct MlpDev {
     float* du2 = nullptr;         // N x 128 gradient w.r.t. u2
     float* dfeat = nullptr;       // dataset: slots x N x 16
     float* dtarget = nullptr;     // dataset: slots x N x 3 (dv - previous dv)
+    // energy-norm training (cs_mlp_train_step / cs_mlp_energy_gradient)
+    float* pred = nullptr;        // N x 3 predictions of the current minibatch
+    float* dy = nullptr;          // N x 3 A pred
+    double* epart = nullptr;      // per slice two FP64 partials
+    double* sheet_c = nullptr;    // per sheet dv*^T b (the solution's energy)
+    float* sheet_scale = nullptr; // per sheet the gradient's coefficients of A pred and of b
+    float* sheet_loss = nullptr;  // per sheet sin^2 of the A-angle between pred and dv*
     int slots = 0, grid = 0;
     int* err = nullptr;           // set if a tensor-core wait gave up
 };
@@ -46,6 +53,10 @@ __global__ void cs_mlp_adam_ext_kernel(MlpDev M, const float* grad, float lr, fl
 __global__ void cs_mlp_target_kernel(Batch B, const float* feat, float* target);
 __global__ void cs_mlp_moments_kernel(const float* feat, const float* target, long long n, double* out);
 __global__ void cs_mlp_loss_acc_kernel(MlpDev M, int ncta, float* acc);
+__global__ void cs_mlp_energy_kernel(Batch B, MlpDev M, int sl0, int sl1);
+__global__ void cs_mlp_energy_norm_kernel(Batch B, MlpDev M, int sl0, int sl1);
+__global__ void cs_mlp_energy_sheet_kernel(Batch B, MlpDev M, int s0, int s1, int mode);
+__global__ void cs_mlp_energy_loss_kernel(MlpDev M, int s0, int s1, float* acc);
 
 // dynamic shared memory of the tile kernels (bytes)
 #define MLP_SMEM_L1 12816

@@ -184,14 +184,24 @@ __device__ __forceinline__ void spmv_slice(const Batch& B, int slice, int lane) 
                 }
             }
             double r0 = (double)B.b[3 * row] - y0, r1 = (double)B.b[3 * row + 1] - y1, r2 = (double)B.b[3 * row + 2] - y2;
-            // drift of the recursive residual it replaces
-            const double q0 = r0 - (double)B.r[3 * row], q1 = r1 - (double)B.r[3 * row + 1],
-                         q2 = r2 - (double)B.r[3 * row + 2];
-            dq = q0 * q0 + q1 * q1 + q2 * q2;
-            B.r[3 * row] = (float)r0;
-            B.r[3 * row + 1] = (float)r1;
-            B.r[3 * row + 2] = (float)r2;
-            sq = r0 * r0 + r1 * r1 + r2 * r2;
+            if (B.params->warm_scale && B.params->warm && !I.scaled) {
+                // the warm start's scaling pass: d.b and d.r (d.A d = d.b - d.r) for its
+                // Galerkin multiple
+                const double d0 = B.dv64[3 * row] + (double)B.e[3 * row];
+                const double d1 = B.dv64[3 * row + 1] + (double)B.e[3 * row + 1];
+                const double d2 = B.dv64[3 * row + 2] + (double)B.e[3 * row + 2];
+                sq = d0 * (double)B.b[3 * row] + d1 * (double)B.b[3 * row + 1] + d2 * (double)B.b[3 * row + 2];
+                dq = d0 * r0 + d1 * r1 + d2 * r2;
+            } else {
+                // drift of the recursive residual it replaces
+                const double q0 = r0 - (double)B.r[3 * row], q1 = r1 - (double)B.r[3 * row + 1],
+                             q2 = r2 - (double)B.r[3 * row + 2];
+                dq = q0 * q0 + q1 * q1 + q2 * q2;
+                B.r[3 * row] = (float)r0;
+                B.r[3 * row + 1] = (float)r1;
+                B.r[3 * row + 2] = (float)r2;
+                sq = r0 * r0 + r1 * r1 + r2 * r2;
+            }
         }
         sq = warp_sum(sq);
         dq = warp_sum(dq);
@@ -326,8 +336,24 @@ __global__ void __launch_bounds__(CS_REDUCE_THREADS) cs_reduce1_kernel(Batch B) 
     const SheetDesc& sh = B.sheets[s];
     double sum, drift2;
     inst_sum2(B, sh, mixed || ph == PH_RES, sum, drift2, shd, shf);
-    if (!(ph == PH_RES && mixed)) drift2 = 0.0;
     if (threadIdx.x != 0) return;
+    if (ph == PH_RES && P.warm_scale && P.warm && !I.scaled) {
+        // the warm start d becomes alpha d, alpha = d.b / d.A d (d.A d = d.b - d.r): the
+        // multiple of d nearest to the solution in the energy norm; the guard then judges it
+        const double db = sum, dad = sum - drift2, a = db / dad;
+        I.scaled = 1;
+        if (dad > 0.0 && finite_d(a)) {
+            I.wscale = a;
+            I.phase = PH_SCALE;
+        } else {
+            I.flags |= CS_IF_WARM_REJECTED;
+            I.sweeps = 1;
+            I.res0 = sqrt(I.bnorm2);
+            I.phase = PH_INIT;
+        }
+        return;
+    }
+    if (!(ph == PH_RES && mixed)) drift2 = 0.0;
     if (ph == PH_CG) {
         float alpha;
         if (mixed)
@@ -388,10 +414,18 @@ __global__ void __launch_bounds__(128) cs_vector_kernel(Batch B) {
     const SliceDesc sd = B.slices[slice];
     const InstState& I = B.inst[sd.sheet];
     const int ph = I.phase;
-    if (ph != PH_CG && ph != PH_INIT && ph != PH_FINISH) return;
+    if (ph != PH_CG && ph != PH_INIT && ph != PH_FINISH && ph != PH_SCALE) return;
     const bool mixed = B.params->mixed != 0;
     const bool live = lane < sd.rows;
     const int row = sd.row0 + CS_SLICE * (slice - B.sheets[sd.sheet].slice_off) + (live ? lane : 0);
+    if (ph == PH_SCALE) {
+        if (live) {
+            const double a = I.wscale;
+#pragma unroll
+            for (int c = 0; c < 3; c++) B.dv64[3 * row + c] *= a;
+        }
+        return;
+    }
     double rz = 0.0, rr = 0.0;
     float rzf = 0.f, rrf = 0.f;
     if (live) {
@@ -515,6 +549,7 @@ __global__ void __launch_bounds__(CS_REDUCE_THREADS) cs_reduce2_kernel(Batch B, 
         }
     } else if (threadIdx.x == 0) {
         if (ph == PH_FINISH) I.phase = PH_DONE;
+        else if (ph == PH_SCALE) I.phase = PH_RES;  // the residual of the scaled warm start
     }
     if (threadIdx.x == 0) {
         if (I.phase != PH_DONE && I.phase != PH_RESIDENT) atomicAdd(&B.loop[1], 1);
@@ -562,6 +597,8 @@ __global__ void __launch_bounds__(128) cs_solve_setup_kernel(Batch B) {
         I.resnorm = I.first_res = -1.0;
         I.alpha = I.beta = 0.f;
         I.sweep_iters = I.iters = I.sweeps = I.flags = 0;
+        I.scaled = 0;
+        I.wscale = 1.0;
         if (sh.resident && B.params->solver == CS_SOLVER_AUTO_DEV && !(B.sheet_prox && B.sheet_prox[s]))
             I.phase = PH_RESIDENT;  // solved by cs_resident_pcg_kernel before the loop runs
         else

@@ -557,6 +557,8 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
         double gam = 0.0, gam_prev = 0.0, rr = 0.0, delta = 0.0, alpha_d = 0.0, res0 = bn, resnorm = -1.0,
                first_res = -1.0;
         bool cont = false;  // the next PH_INIT keeps the search direction (reliable update)
+        // the warm start's scaling pass (warm_scale): its first residual gives d.b and d.r
+        bool scale_pass = P.warm && P.warm_scale;
         // 1 / gam and 1 / (gam alpha), computed when gam and alpha are set, so that the next
         // iteration's step length costs one division after the reduction instead of three
         double inv_gam = 0.0, inv_ga = 0.0;
@@ -712,8 +714,14 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     r[0] = (float)r0;
                     r[1] = (float)r1;
                     r[2] = (float)r2;
-                    v[0] = r0 * r0 + r1 * r1 + r2 * r2;
-                    v[1] = q0 * q0 + q1 * q1 + q2 * q2;
+                    if (scale_pass) {
+                        const double d0 = B.dv64[3 * g], d1 = B.dv64[3 * g + 1], d2 = B.dv64[3 * g + 2];
+                        v[0] = d0 * (double)B.b[3 * g] + d1 * (double)B.b[3 * g + 1] + d2 * (double)B.b[3 * g + 2];
+                        v[1] = d0 * r0 + d1 * r1 + d2 * r2;
+                    } else {
+                        v[0] = r0 * r0 + r1 * r1 + r2 * r2;
+                        v[1] = q0 * q0 + q1 * q1 + q2 * q2;
+                    }
                 }
                 if (coarse) {
                     // the coarse residual R r of the replaced r travels with the norms
@@ -728,6 +736,33 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                     ok = cluster_sum3(S, rank, ncta, nred, v, false);
                 }
                 if (!ok) break;
+                if (scale_pass) {
+                    // d becomes alpha d, alpha = d.b / d.A d (d.A d = d.b - d.r): the multiple of d
+                    // nearest to the solution in the energy norm; the next residual is its guard's.
+                    // Every CTA holds the same sums, so all take the same branch; each scales its
+                    // own rows once every CTA's reads of them are done (they precede the sums).
+                    scale_pass = false;
+                    const double dad = v[0] - v[1], a = v[0] / dad;
+                    if (dad > 0.0 && rfinite(a)) {
+                        if (live) {
+#pragma unroll
+                            for (int c = 0; c < 3; c++) B.dv64[3 * g + c] *= a;
+                        }
+                        continue;  // phase stays PH_RES
+                    }
+                    flags |= CS_IF_WARM_REJECTED;
+                    sweeps = 1;
+                    res0 = bn;
+                    phase = PH_INIT;
+                    if (coarse) {
+                        if (live) {
+#pragma unroll
+                            for (int c = 0; c < 3; c++) B.dv64[3 * g + c] = 0.0;
+                        }
+                        phase = PH_RES;
+                    }
+                    continue;
+                }
                 const double res = sqrt(v[0]);
                 resnorm = res;
                 sweeps += 1;

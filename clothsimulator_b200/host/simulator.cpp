@@ -365,6 +365,7 @@ static SolverOptions parseSolver(const Json& j) {
     if (o.precondDegree < 0 || o.precondDegree > CS_PRECOND_MAX_DEGREE || (o.precondDegree > 1 && o.precondDegree % 2 == 0))
         throw std::runtime_error("solver.precond_degree must be 0, 1 or an odd degree up to 15");
     if (!j["coarse"].isNull()) o.coarse = j["coarse"].asDouble() != 0.0;
+    if (!j["warm_scale"].isNull()) o.warmScale = j["warm_scale"].asDouble() != 0.0;
     o.network = parseString(j["network"]);
     if (o.warmStart == CS_WARM_LEARNED && o.network.empty())
         throw std::runtime_error("solver.warm_start \"learned\" needs solver.network (a weights file)");
@@ -520,6 +521,7 @@ void Simulator::physicsStep() {
     p.precision = solver_.precision;
     p.precond_degree = solver_.precondDegree;
     p.coarse = solver_.coarse ? 1 : 0;
+    p.warm_scale = solver_.warmScale ? 1 : 0;
     p.transformations = transforms_.empty() ? nullptr : transforms_.data();
     p.n_transformations = (int)motions_.size();
     p.warm_start = nSteps_ > 1 || mode_ == ResumeOffline ? solver_.warmStart : CS_WARM_ZERO;

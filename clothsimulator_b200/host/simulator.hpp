@@ -129,6 +129,7 @@ struct SolverOptions {
     int warmStart = CS_WARM_PREVIOUS;
     int precondDegree = 3;  // strip-local Chebyshev of the cluster-resident solver (1: block-Jacobi)
     bool coarse = true;     // with it, the coarse-space correction of the cluster-resident solver
+    bool warmScale = false; // the warm start replaced by its Galerkin multiple before the guard
     std::string network;  // weights for the learned warm start (CS_MLP_PARAMS floats, binary)
 };
 

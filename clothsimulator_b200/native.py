@@ -40,6 +40,7 @@ EXPORTED = [
     "cs_mlp_set_weights", "cs_get_solver_info", "cs_set_proximities", "cs_detect_proximities",
     "cs_get_proximities", "cs_collision_step", "cs_mlp_moments", "cs_mlp_set_moments", "cs_mlp_gradient_device",
     "cs_mlp_apply_gradient", "cs_get_resident_blocks", "cs_set_handle_motions", "cs_tune",
+    "cs_mlp_train_step", "cs_mlp_energy_gradient",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -79,6 +80,7 @@ class StepParams(ctypes.Structure):
         ("advance", ctypes.c_int), ("use_graph", ctypes.c_int), ("solver", ctypes.c_int),
         ("precond_degree", ctypes.c_int), ("coarse", ctypes.c_int),
         ("transformations", ctypes.POINTER(ctypes.c_float)), ("n_transformations", ctypes.c_int),
+        ("warm_scale", ctypes.c_int),
     ]
 
 
@@ -193,6 +195,9 @@ def load_library() -> ctypes.CDLL:
         "cs_mlp_fit_normalization": [vp, ctypes.c_int],
         "cs_mlp_train": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_ulonglong, _fp],
         "cs_mlp_gradient": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _fp, _fp],
+        "cs_mlp_train_step": [vp, ctypes.POINTER(StepParams), ctypes.c_float, ctypes.c_int, ctypes.c_ulonglong,
+                              ctypes.POINTER(StepStats), _fp],
+        "cs_mlp_energy_gradient": [vp, ctypes.POINTER(StepParams), ctypes.c_int, ctypes.c_int, _fp, _fp],
         "cs_mlp_moments": [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_longlong)],
         "cs_mlp_set_moments": [vp, _dp, ctypes.c_longlong],
         "cs_mlp_gradient_device": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, _fp],
@@ -244,7 +249,7 @@ def material_desc(spec: dict) -> MaterialDesc:
 
 def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, inner_tol=1e-2, max_iters=2000,
                 sweep_cap=0, precision=PREC_MIXED, warm_start=WARM_ZERO, advance=1, use_graph=1,
-                solver=0, precond_degree=1, coarse=1) -> StepParams:
+                solver=0, precond_degree=1, coarse=1, warm_scale=0) -> StepParams:
     p = StepParams()
     p.dt = dt
     for i in range(3):
@@ -263,6 +268,7 @@ def step_params(dt, gravity=(0.0, -9.8, 0.0), handle_stiffness=1e3, tol=1e-6, in
     p.coarse = coarse
     p.transformations = None
     p.n_transformations = 0
+    p.warm_scale = warm_scale
     return p
 
 
@@ -560,6 +566,25 @@ class Context:
     def mlp_set_moments(self, sums, count: int):
         a = np.ascontiguousarray(sums, np.float64)
         self.check(self.lib.cs_mlp_set_moments(self.h, a.ctypes.data_as(_dp), int(count)))
+
+    def mlp_train_step(self, params: StepParams, lr: float = 1e-3, sheets_per_batch: int = 64, seed: int = 0,
+                       allow_unconverged: bool = False):
+        """cs_mlp_train_step: one step of the batch with energy-norm Adam updates between the
+        solve and the state update.  Returns (stats, mean minibatch loss)."""
+        stats = StepStats()
+        loss = ctypes.c_float(0.0)
+        st = self.lib.cs_mlp_train_step(self.h, ctypes.byref(params), lr, sheets_per_batch, seed, ctypes.byref(stats),
+                                        ctypes.byref(loss))
+        self.check(st, (CS_OK, CS_ERR_NOT_CONVERGED, CS_ERR_NON_SPD) if allow_unconverged else (CS_OK,))
+        return stats, loss.value
+
+    def mlp_energy_gradient(self, params: StepParams, s0: int, s1: int):
+        """cs_mlp_energy_gradient: the energy-norm loss's gradient and value for sheets [s0, s1)."""
+        g = np.zeros(MLP_TRAINED, np.float32)
+        loss = ctypes.c_float(0)
+        self.check(self.lib.cs_mlp_energy_gradient(self.h, ctypes.byref(params), s0, s1, g.ctypes.data_as(_fp),
+                                                   ctypes.byref(loss)))
+        return g, loss.value
 
     def mlp_gradient_device(self, slot: int, s0: int, s1: int, grad) -> float:
         """One minibatch's gradient into `grad`, a CUDA tensor of MLP_TRAINED floats on this

@@ -109,6 +109,12 @@ typedef struct cs_step_params {
      * Cloth::addHandleForces, Cloth.cu:157-169).  NULL / 0 when no handle moves. */
     const float* transformations;
     int n_transformations;    /* at most CS_MAX_MOTIONS */
+    int warm_scale;           /* 1: a warm start d is first replaced, per sheet, by its Galerkin
+                                 multiple (d^T b / d^T A d) d -- the multiple of d nearest to
+                                 the solution in the energy norm, never farther than the zero
+                                 guess -- before the guard compares its FP64 residual with the
+                                 zero guess's (a sheet with d^T A d <= 0 discards it); 0: the
+                                 warm start as given.  No counterpart in the reference. */
 } cs_step_params;
 
 #define CS_TRANSFORM_FLOATS 8
@@ -357,6 +363,26 @@ cs_status cs_mlp_train(cs_ctx* ctx, int n_slots, int epochs, float lr, int sheet
                        unsigned long long seed, float* epoch_loss);
 /* Gradient (CS_MLP_PARAMS - 38 floats) and loss of one minibatch, without updating. */
 cs_status cs_mlp_gradient(cs_ctx* ctx, int slot, int sheet_begin, int sheet_end, float* grad, float* loss);
+/* Energy-norm training on the solver's own trajectory, one step at a time (the normalisation
+ * set first, e.g. by cs_mlp_fit_normalization on a few recorded steps).  cs_mlp_train_step is
+ * one implicit step of the batch as cs_step takes it with `params` (assembly, the solve from
+ * its zero or previous-dv start -- not the learned one -- then v and x updated when
+ * params->advance), and between the solve and the update, for every minibatch of
+ * sheets_per_batch whole sheets (in an order shuffled by seed), one Adam step on the loss
+ *     L = mean over the minibatch's sheets of 1 - (p^T b)^2 / ((p^T A p)(dv*^T b))
+ * of the network's prediction p for this step's system, dv* the step's solution (A dv* = b to
+ * the solve's tolerance): sin^2 of the angle between p and dv* in the energy inner product,
+ * i.e. the squared energy-norm error of p's Galerkin multiple (the start warm_scale makes of p)
+ * relative to the zero guess's; in [0, 1], and its gradient needs one SpMV of the prediction.
+ * *loss (optional) receives the mean of the minibatches' losses before their updates; stats as
+ * cs_step's.
+ * Batches with proximities are refused.  cs_mlp_energy_gradient: the same loss's gradient
+ * (CS_MLP_PARAMS - 38 floats) and value for sheets [sheet_begin, sheet_end) of the current
+ * state, without updating the weights or the state. */
+cs_status cs_mlp_train_step(cs_ctx* ctx, const cs_step_params* params, float lr, int sheets_per_batch,
+                            unsigned long long seed, cs_step_stats* stats, float* loss);
+cs_status cs_mlp_energy_gradient(cs_ctx* ctx, const cs_step_params* params, int sheet_begin, int sheet_end,
+                                 float* grad, float* loss);
 /* Data-parallel training across ranks (one context per GPU, each on its own trajectories):
  * cs_mlp_moments gives the normalisation's sums (38 doubles: 16 feature and 3 target sums, then
  * their 19 sums of squares) and node count for an all-reduce, cs_mlp_set_moments sets the

@@ -79,7 +79,36 @@ def loss_and_grad(w, feat, target, nb):
     t = (target - p["mu_y"]) / p["sigma_y"]
     d = f["y"] - t
     loss = float((d * d).sum() / n)
-    dy = 2.0 * d / n
+    return loss, backward(f, 2.0 * d / n, nb), f
+
+
+def energy_loss_and_grad(w, feat, A, b, dv_star, node_ranges, nb):
+    """Energy-norm loss of the prediction p = previous dv + sigma_y y + mu_y (the previous dv is
+    features 12-14): the mean over sheets of sin^2 of the angle between p and dv* in the A inner
+    product, 1 - u^2 / (w c) with u = p^T b, w = p^T A p, c = dv*^T b (A dv* = b), and its
+    gradient through dL/dp = (2 u / (w c S)) (u / w A p - b).  A: the batch's 3N x 3N matrix
+    (SciPy), b and dv* 3N vectors, node_ranges the sheets' (first node, end) pairs."""
+    p = unpack(w)
+    f = forward(w, feat, nb)
+    pred = feat[:, 12:15] + p["sigma_y"] * f["y"] + p["mu_y"]
+    pv = pred.reshape(-1)
+    Ap = A @ pv
+    S = len(node_ranges)
+    dp = np.zeros_like(pv)
+    loss = 0.0
+    for n0, n1 in node_ranges:
+        sl = slice(3 * n0, 3 * n1)
+        c = float(dv_star[sl] @ b[sl])
+        u = float(pv[sl] @ b[sl])
+        ww = float(pv[sl] @ Ap[sl])
+        loss += (1.0 - u * u / (ww * c)) / S
+        dp[sl] = 2.0 * u / (ww * c * S) * (u / ww * Ap[sl] - b[sl])
+    dy = dp.reshape(-1, 3) * p["sigma_y"]
+    return loss, backward(f, dy, nb), pred
+
+
+def backward(f, dy, nb):
+    """Gradient of the weights (flat, P floats) from dL/dy, with the GPU path's rounding points."""
     g = {}
     g["W4"] = dy.T @ f["h3"]
     g["b4"] = dy.sum(0)
@@ -102,7 +131,7 @@ def loss_and_grad(w, feat, target, nb):
     flat = np.zeros(P)
     for k, (o, s) in OFF.items():
         flat[o:o + int(np.prod(s))] = g[k].reshape(-1)
-    return loss, flat, f
+    return flat
 
 
 def predict(w, feat, nb):

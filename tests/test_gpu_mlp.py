@@ -85,6 +85,77 @@ def test_mlp_gradient_and_prediction_match_fp64_oracle():
     ctx.close()
 
 
+def test_energy_gradient_matches_fp64_oracle():
+    """The energy-norm loss (sin^2 of the A-angle between prediction and solution) and its
+    gradient (cs_mlp_energy_gradient) against the FP64 restatement on the batch's system at the
+    current state: loss within 1e-4, gradient within 2e-3, over the whole batch and over one
+    sheet of it."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+
+    scene = scenes.windy_batch(3, 8, seed=5)
+    ctx, p = recorded_ctx(scene, 2)
+    p.tol = 1e-11
+    w = ctx.mlp_get_weights()
+    nb = batch_neighbours(scene)
+    ranges, off = [], 0
+    for s in scene.sheets:
+        ranges.append((off, off + s["x"].shape[0]))
+        off += s["x"].shape[0]
+    for s0, s1 in ((0, 3), (1, 2)):
+        g, loss = ctx.mlp_energy_gradient(p, s0, s1)
+        # the same state's features and system (the call changed neither the state nor B.warm)
+        ctx.assemble(p)
+        ctx.mlp_record(0, 0)
+        feat, _ = ctx.mlp_get_record(0)
+        rp, ci, val, b = ctx.system()
+        n = rp.shape[0] - 1
+        A = sp.bsr_matrix((val.astype(np.float64), ci, rp), shape=(3 * n, 3 * n)).tocsr()
+        b64 = b.astype(np.float64)
+        dvs = spl.spsolve(A.tocsc(), b64)
+        n0, n1 = ranges[s0][0], ranges[s1 - 1][1]
+        Asub = A[3 * n0:3 * n1, 3 * n0:3 * n1]
+        sub_ranges = [(a - n0, z - n0) for a, z in ranges[s0:s1]]
+        sub_nb = [j - n0 for j in nb[n0:n1]]
+        loss_ref, g_ref, _ = mlp_oracle.energy_loss_and_grad(w, feat[n0:n1].astype(np.float64), Asub,
+                                                             b64[3 * n0:3 * n1], dvs[3 * n0:3 * n1], sub_ranges, sub_nb)
+        assert abs(loss - loss_ref) / abs(loss_ref) < 1e-4, (s0, s1, loss, loss_ref)
+        assert rel(g, g_ref) < 2e-3, (s0, s1)
+    ctx.close()
+
+
+def test_energy_training_step_lowers_the_energy_loss():
+    """cs_mlp_train_step along a trajectory lowers the energy-norm loss (in [0, 1]) at the
+    trajectory's first state, and the step it takes equals cs_step's (same solve, same update:
+    x, v bit for bit)."""
+    scene = scenes.windy_batch(8, 12, seed=6)
+    ctx, p = recorded_ctx(scene, 4)
+    x, v = ctx.get_state()
+    prev = ctx.get_dv()
+    _, before = ctx.mlp_energy_gradient(p, 0, 8)
+    twin = native.Context(0)
+    twin.load(scene.sheets)
+    twin.set_state(x, v)
+    twin.set_warm_start(prev)
+    q = native.StepParams.from_buffer_copy(p)
+    q.use_graph = 0
+    for t in range(24):
+        st, loss = ctx.mlp_train_step(p, lr=2e-3, sheets_per_batch=2, seed=t)
+        twin.step(q)
+        assert st.converged == 8 and 0.0 <= loss <= 1.0
+    xa, va = ctx.get_state()
+    xb, vb = twin.get_state()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+    # the loss at the trajectory's first state, before and after the training
+    ctx.set_state(x, v)
+    ctx.set_warm_start(prev)
+    _, after = ctx.mlp_energy_gradient(p, 0, 8)
+    print(f"energy loss at the first state: {before:.4f} -> {after:.4f}")
+    assert after < 0.8 * before
+    twin.close()
+    ctx.close()
+
+
 def test_mlp_training_reduces_loss():
     scene = scenes.windy_batch(8, 12, seed=6)
     ctx, _ = recorded_ctx(scene, 4)

@@ -326,3 +326,36 @@ def test_coarse_flag_inert_without_chebyshev(ctx_factory):
         ctx.step(params_for(scene, precond_degree=1, coarse=coarse))
         res.append((ctx.get_dv().copy(), ctx.instance_stats()[0].copy()))
     assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+@pytest.mark.parametrize("route", ["resident_coarse", "resident_jacobi", "batched"])
+def test_galerkin_scaled_warm_start(ctx_factory, route):
+    """warm_scale: warm starts of 4 and -2 times the solution (exact in FP32) have residuals of
+    3 ||b||, which the guard discards; their Galerkin multiples (d.b / d.A d = 1/4, -1/2) are the
+    solution, which the guard keeps, and the solve then needs far fewer iterations than from
+    zero."""
+    scene = scenes.windy_batch(4, 24, seed=71)
+    ctx = ctx_factory(scene.sheets)
+    x0 = np.concatenate([s["x"] for s in scene.sheets])
+    v0 = np.concatenate([s["v"] for s in scene.sheets])
+    kw = {"resident_coarse": dict(precond_degree=3, coarse=1), "resident_jacobi": dict(precond_degree=1, coarse=0),
+          "batched": dict(solver=native.SOLVER_BATCHED)}[route]
+    ctx.set_state(x0, v0)
+    ctx.step(params_for(scene, tol=1e-11, **kw))
+    exact = ctx.get_dv().copy()
+    ctx.set_state(x0, v0)
+    ctx.step(params_for(scene, tol=1e-7, **kw))
+    it_zero, _, _ = ctx.instance_stats()
+    for scale in (0, 1):
+        for mult in (4.0, -2.0):
+            ctx.set_state(x0, v0)
+            ctx.set_warm_start(mult * exact)
+            st, _ = ctx.step(params_for(scene, tol=1e-7, warm_start=native.WARM_PREVIOUS, warm_scale=scale, **kw))
+            it, rr, fl = ctx.instance_stats()
+            assert st.converged == 4 and np.all(rr <= 1e-7)
+            assert rel(ctx.get_dv(), exact) < 1e-5
+            if scale == 0:
+                assert np.all(fl & 2), "a start of 4x or -2x the solution is worse than zero"
+            else:
+                assert not np.any(fl & 2)
+                assert np.all(it <= 0.5 * it_zero), (it, it_zero)
