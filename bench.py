@@ -175,16 +175,6 @@ class RankGroup:
         self.dist.all_reduce(t)
         return t.numpy()
 
-    def bcast_host(self, a):
-        """Rank 0's float32 numpy array on every rank (gloo broadcast)."""
-        if not self.dist:
-            return a
-        import torch
-
-        t = torch.from_numpy(np.array(a, np.float32))
-        self.dist.broadcast(t, src=0)
-        return t.numpy()
-
     def nccl_group(self):
         """An NCCL group of all ranks beside the gloo group of the host scalars (created once)."""
         if not self.dist:
@@ -383,11 +373,11 @@ def train_warm_start(args, group, local):
 
     energy (default): the network is trained online along 1,024 trajectories of 200 steps (the
     specified training set), each step solved by the solver without the learned start; between
-    a step's solve and its state update, one Adam step per minibatch of sheets on the relative
-    error of the prediction in the energy norm of that step's system (cs_mlp_train_step), the
-    normalisation fitted first on a few recorded steps.  With several ranks, rank 0 trains and
-    broadcasts the weights.  mse: recorded (state, dv) pairs, squared error (cs_mlp_train), data
-    parallel over the ranks."""
+    a step's solve and its state update, one Adam step per minibatch of sheets on the energy-norm
+    loss of the prediction for that step's system (cs_mlp_train_step), the normalisation fitted
+    first on a few recorded steps.  mse: recorded (state, dv) pairs, squared error
+    (cs_mlp_train).  With several ranks both train data parallel: each rank on its own
+    trajectories, gradients averaged over NCCL."""
     from clothsimulator_b200 import native
 
     rank, world = group.rank, group.world
@@ -400,69 +390,80 @@ def train_warm_start(args, group, local):
         weights = np.fromfile(args.weights, dtype=np.float32)
         info = {"source": args.weights}
     elif energy:
-        weights = np.zeros(native.MLP_PARAMS, np.float32)
-        info = {}
-        if rank == 0:
-            tscene = scenes_mod().windy_batch(sheets, args.nq, seed=train_seed(0))
-            tctx = native.Context(local)
-            tctx.load(tscene.sheets)
-            n_norm = 6
-            tctx.mlp_init(n_norm, 1)
-            tp = native.step_params(tscene.dt, tscene.gravity, tscene.handle_stiffness, tol=args.tol, max_iters=20000,
-                                    precond_degree=3, coarse=1)
-            # normalisation from the features and targets of steps 10-15 (past the start from
-            # rest); the output is not shifted (mean 0, scale the targets' RMS), so that the
-            # untrained network predicts about the previous dv
-            n_skip = 10
-            for t in range(n_skip + n_norm):
-                if t >= n_skip:
-                    tctx.assemble(tp)
-                    tctx.mlp_record(t - n_skip, 0)
-                tctx.step(tp, allow_unconverged=True)
-                if t >= n_skip:
-                    tctx.mlp_record(t - n_skip, 1)
-                tp.warm_start = native.WARM_PREVIOUS
-            sums, count = tctx.mlp_moments(n_norm)
-            sums[16:19] = 0.0
-            tctx.mlp_set_moments(sums, count)
-            xs = np.concatenate([s["x"] for s in tscene.sheets])
-            vs = np.concatenate([s["v"] for s in tscene.sheets])
-            curve = []
-            for ep in range(epochs):
-                tctx.set_state(xs, vs)
-                tp.warm_start = native.WARM_ZERO
-                ep_loss = []
-                for t in range(steps):
-                    if t < 2:
-                        # the first steps from rest (no previous dv yet) are not trained on
-                        tctx.step(tp, allow_unconverged=True)
-                    else:
-                        _, loss = tctx.mlp_train_step(tp, lr=args.train_lr, sheets_per_batch=args.train_batch,
-                                                      seed=1 + ep * steps + t, allow_unconverged=True)
-                        ep_loss.append(loss)
-                    tp.warm_start = native.WARM_PREVIOUS
-                curve.append(ep_loss)
-            weights = tctx.mlp_get_weights()
-            tctx.close()
-            first, last = curve[0], curve[-1]
-            k = max(1, steps // 10)
-            info = {"loss": "sin^2 of the angle between prediction and solution in the energy inner product of the "
-                            "step's system (the Galerkin-scaled start's squared energy error relative to the zero "
-                            "guess's), mean over sheets",
-                    "sheets": sheets, "steps": steps, "epochs": epochs, "lr": args.train_lr,
-                    "sheets_per_minibatch": args.train_batch,
-                    "adam_steps": epochs * steps * ((sheets + args.train_batch - 1) // args.train_batch),
-                    "trajectories": f"windy{sheets}x{args.nq}, seeds disjoint from the evaluated workload, solved "
-                                    "without the learned start (mixed PCG, Chebyshev-3 + coarse correction)",
-                    "loss_first_epoch_first_steps": float(np.mean(first[:k])),
-                    "loss_first_epoch_last_steps": float(np.mean(first[-k:])),
-                    "loss_last_epoch_first_steps": float(np.mean(last[:k])),
-                    "loss_last_epoch_last_steps": float(np.mean(last[-k:])),
-                    "loss_epoch_means": [float(np.mean(c)) for c in curve]}
+        tscene = scenes_mod().windy_batch(sheets, args.nq, seed=train_seed(rank))
+        tctx = native.Context(local)
+        tctx.load(tscene.sheets)
+        n_norm = 6
+        tctx.mlp_init(n_norm, 1)  # the same initial weights on every rank
+        tp = native.step_params(tscene.dt, tscene.gravity, tscene.handle_stiffness, tol=args.tol, max_iters=20000,
+                                precond_degree=3, coarse=1)
+        # normalisation from the features and targets of steps 10-15 (past the start from rest;
+        # moments summed over the ranks); the output is not shifted (mean 0, scale the targets'
+        # RMS), so that the untrained network predicts about the previous dv
+        n_skip = 10
+        for t in range(n_skip + n_norm):
+            if t >= n_skip:
+                tctx.assemble(tp)
+                tctx.mlp_record(t - n_skip, 0)
+            tctx.step(tp, allow_unconverged=True)
+            if t >= n_skip:
+                tctx.mlp_record(t - n_skip, 1)
+            tp.warm_start = native.WARM_PREVIOUS
+        sums, count = tctx.mlp_moments(n_norm)
         if world > 1:
-            weights = group.bcast_host(weights)
-            info["ranks"] = world
-            info["trained_on"] = "rank 0, weights broadcast"
+            both = group.sum_host(np.concatenate([sums, [float(count)]]))
+            sums, count = both[:38], int(round(both[38]))
+        sums[16:19] = 0.0
+        tctx.mlp_set_moments(sums, count)
+        xs = np.concatenate([s["x"] for s in tscene.sheets])
+        vs = np.concatenate([s["v"] for s in tscene.sheets])
+        curve = []
+        if world > 1:
+            # data parallel: every rank steps its own trajectories, each minibatch's gradient
+            # summed over NCCL and averaged before the common Adam step
+            import torch
+
+            from clothsimulator_b200 import training
+
+            grad = torch.empty(native.MLP_TRAINED, dtype=torch.float32, device=torch.device("cuda", local))
+            allreduce = group.device_allreduce()
+        for ep in range(epochs):
+            tctx.set_state(xs, vs)
+            tp.warm_start = native.WARM_ZERO
+            ep_loss = []
+            for t in range(steps):
+                seed = 1 + ep * steps + t
+                if t < 2:
+                    # the first steps from rest (no previous dv yet) are not trained on
+                    tctx.step(tp, allow_unconverged=True)
+                elif world > 1:
+                    _, loss = training.energy_step_data_parallel(tctx, tp, sheets, args.train_lr, args.train_batch, seed,
+                                                                 allreduce, world, grad=grad)
+                    ep_loss.append(loss)
+                else:
+                    _, loss = tctx.mlp_train_step(tp, lr=args.train_lr, sheets_per_batch=args.train_batch, seed=seed,
+                                                  allow_unconverged=True)
+                    ep_loss.append(loss)
+                tp.warm_start = native.WARM_PREVIOUS
+            curve.append(ep_loss)
+        weights = tctx.mlp_get_weights()
+        tctx.close()
+        first, last = curve[0], curve[-1]
+        k = max(1, len(first) // 10)
+        info = {"loss": "sin^2 of the angle between prediction and solution in the energy inner product of the "
+                        "step's system (the Galerkin-scaled start's squared energy error relative to the zero "
+                        "guess's), mean over sheets",
+                "sheets": sheets, "steps": steps, "epochs": epochs, "lr": args.train_lr,
+                "sheets_per_minibatch": args.train_batch,
+                "adam_steps": epochs * (steps - 2) * ((sheets + args.train_batch - 1) // args.train_batch),
+                "trajectories": f"windy{sheets}x{args.nq} per rank, seeds disjoint from the evaluated workload, "
+                                "solved without the learned start (mixed PCG, Chebyshev-3 + coarse correction)",
+                "loss_first_steps": float(np.mean(first[:k])), "loss_last_steps": float(np.mean(last[-k:])),
+                "loss_epoch_means": [float(np.mean(c)) for c in curve]}
+        if world > 1:
+            digest = float(np.float64(weights).sum())
+            info["data_parallel"] = {"ranks": world, "gradients": "NCCL all-reduce, averaged",
+                                     "weights_identical": group.max(digest) == -group.max(-digest)}
     else:
         tscene = scenes_mod().windy_batch(sheets, args.nq, seed=train_seed(rank))
         tctx = native.Context(local)

@@ -808,6 +808,8 @@ struct cs_ctx {
     int spmvShape = CS_SPMV_DEFAULT;    // launch shape of the batched SpMV (cs_tune)
     int tunedDegree = 0, tunedCoarse = 0;  // fastest resident preconditioner found by cs_tune (0: not tuned)
     int tunedSolver = -1;                  // faster solve route found by cs_tune (-1: not tuned)
+    bool energyBegun = false;              // cs_mlp_energy_begin ran; cs_mlp_energy_end not yet
+    int energyLoopCap = 0;                 // the begun step's trip bound (its statistics)
     std::vector<int> handleNode;  // batch node of every handle, in load order (cs_set_handle_motions)
     int maxHandleMotion = -1;     // largest motion a handle follows (-1: none)
     size_t resSmem = 0;
@@ -3077,11 +3079,50 @@ cs_status cs_mlp_train(cs_ctx* c, int n_slots, int epochs, float lr, int sheets_
     return mlpCheckErr(c);
 }
 
+cs_status cs_mlp_energy_begin(cs_ctx* c, const cs_step_params* p) {
+    if (!c || !p) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    c->energyBegun = false;
+    cs_status st = mlpEnergyPrepare(c, p);
+    if (st != CS_OK) return st;
+    c->energyBegun = true;
+    c->energyLoopCap = toDev(p).loop_cap;
+    return CS_OK;
+}
+
+cs_status cs_mlp_energy_gradient_device(cs_ctx* c, int s0, int s1, float* grad, float* loss) {
+    if (!c || !grad) return CS_ERR_INVALID_ARG;
+    if (!c->energyBegun) return fail(c, CS_ERR_STATE, "cs_mlp_energy_begin first");
+    if (s0 < 0 || s1 <= s0 || s1 > c->B.S) return fail(c, CS_ERR_INVALID_ARG, "bad sheet range");
+    float* acc = c->mlpScratch;
+    CS_CUDA(cudaMemsetAsync(acc, 0, sizeof(float), c->stream));
+    mlpEnergyForwardBackward(c, s0, s1);
+    cs_mlp_energy_loss_kernel<<<1, 32, 0, c->stream>>>(c->mlp, s0, s1, acc);
+    cs_mlp_adam_kernel<<<nblk(MLP_P, 256), 256, 0, c->stream>>>(c->mlp, c->mlpGridTrain, 0.f, 0.f, 0.f, 0.f, 1, grad);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    if (loss) CS_CUDA(cudaMemcpy(loss, acc, sizeof(float), cudaMemcpyDeviceToHost));
+    return mlpCheckErr(c);
+}
+
+cs_status cs_mlp_energy_end(cs_ctx* c, cs_step_stats* stats) {
+    if (!c) return CS_ERR_INVALID_ARG;
+    if (!c->energyBegun) return fail(c, CS_ERR_STATE, "cs_mlp_energy_begin first");
+    c->energyBegun = false;
+    // the end of the step: dv = the solution, v and x updated when asked (cs_advance_kernel)
+    cs_advance_kernel<<<nblk(3LL * c->B.N, 256), 256, 0, c->stream>>>(c->B);
+    CS_CUDA(cudaGetLastError());
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    c->lastStepValid = true;
+    c->steps++;
+    if (stats) return fillStepStats(c, stats, c->energyLoopCap, false);
+    return CS_OK;
+}
+
 cs_status cs_mlp_train_step(cs_ctx* c, const cs_step_params* p, float lr, int sheets_per_batch,
                             unsigned long long seed, cs_step_stats* stats, float* loss) {
     if (!c || !p || !(lr > 0) || sheets_per_batch <= 0) return CS_ERR_INVALID_ARG;
-    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
-    cs_status st = mlpEnergyPrepare(c, p);
+    cs_status st = cs_mlp_energy_begin(c, p);
     if (st != CS_OK) return st;
     const int S = c->B.S;
     const int groups = (S + sheets_per_batch - 1) / sheets_per_batch;
@@ -3099,20 +3140,18 @@ cs_status cs_mlp_train_step(cs_ctx* c, const cs_step_params* p, float lr, int sh
         cs_mlp_adam_kernel<<<nblk(MLP_P, 256), 256, 0, c->stream>>>(c->mlp, c->mlpGridTrain, lr, 0.9f, 0.999f, 1e-8f,
                                                                    (int)c->adamStep, nullptr);
     }
-    // the end of the step: dv = the solution, v and x updated when asked (cs_advance_kernel)
-    cs_advance_kernel<<<nblk(3LL * c->B.N, 256), 256, 0, c->stream>>>(c->B);
     CS_CUDA(cudaGetLastError());
     CS_CUDA(cudaStreamSynchronize(c->stream));
-    c->lastStepValid = true;
-    c->steps++;
-    if ((st = mlpCheckErr(c)) != CS_OK) return st;
+    if ((st = mlpCheckErr(c)) != CS_OK) {
+        c->energyBegun = false;
+        return st;
+    }
     if (loss) {
         float h = 0.f;
         CS_CUDA(cudaMemcpy(&h, acc, sizeof(float), cudaMemcpyDeviceToHost));
         *loss = h / (float)groups;
     }
-    if (stats) return fillStepStats(c, stats, toDev(p).loop_cap, false);
-    return CS_OK;
+    return cs_mlp_energy_end(c, stats);
 }
 
 cs_status cs_mlp_energy_gradient(cs_ctx* c, const cs_step_params* p, int s0, int s1, float* grad, float* loss) {
@@ -3130,6 +3169,7 @@ cs_status cs_mlp_energy_gradient(cs_ctx* c, const cs_step_params* p, int s0, int
     CS_CUDA(cudaGetLastError());
     CS_CUDA(cudaStreamSynchronize(c->stream));
     c->lastStepValid = false;
+    c->energyBegun = false;
     CS_CUDA(cudaMemcpy(grad, gout, MLP_P * sizeof(float), cudaMemcpyDeviceToHost));
     if (loss) CS_CUDA(cudaMemcpy(loss, acc, sizeof(float), cudaMemcpyDeviceToHost));
     return mlpCheckErr(c);

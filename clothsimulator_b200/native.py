@@ -40,7 +40,8 @@ EXPORTED = [
     "cs_mlp_set_weights", "cs_get_solver_info", "cs_set_proximities", "cs_detect_proximities",
     "cs_get_proximities", "cs_collision_step", "cs_mlp_moments", "cs_mlp_set_moments", "cs_mlp_gradient_device",
     "cs_mlp_apply_gradient", "cs_get_resident_blocks", "cs_set_handle_motions", "cs_tune",
-    "cs_mlp_train_step", "cs_mlp_energy_gradient",
+    "cs_mlp_train_step", "cs_mlp_energy_gradient", "cs_mlp_energy_begin", "cs_mlp_energy_gradient_device",
+    "cs_mlp_energy_end",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -198,6 +199,9 @@ def load_library() -> ctypes.CDLL:
         "cs_mlp_train_step": [vp, ctypes.POINTER(StepParams), ctypes.c_float, ctypes.c_int, ctypes.c_ulonglong,
                               ctypes.POINTER(StepStats), _fp],
         "cs_mlp_energy_gradient": [vp, ctypes.POINTER(StepParams), ctypes.c_int, ctypes.c_int, _fp, _fp],
+        "cs_mlp_energy_begin": [vp, ctypes.POINTER(StepParams)],
+        "cs_mlp_energy_gradient_device": [vp, ctypes.c_int, ctypes.c_int, vp, _fp],
+        "cs_mlp_energy_end": [vp, ctypes.POINTER(StepStats)],
         "cs_mlp_moments": [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_longlong)],
         "cs_mlp_set_moments": [vp, _dp, ctypes.c_longlong],
         "cs_mlp_gradient_device": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, _fp],
@@ -585,6 +589,23 @@ class Context:
         self.check(self.lib.cs_mlp_energy_gradient(self.h, ctypes.byref(params), s0, s1, g.ctypes.data_as(_fp),
                                                    ctypes.byref(loss)))
         return g, loss.value
+
+    def mlp_energy_begin(self, params: StepParams):
+        self.check(self.lib.cs_mlp_energy_begin(self.h, ctypes.byref(params)))
+
+    def mlp_energy_gradient_device(self, s0: int, s1: int, grad) -> float:
+        """The energy loss's gradient for sheets [s0, s1) into `grad` (a CUDA tensor of
+        MLP_TRAINED floats on this context's device); returns the minibatch loss."""
+        loss = ctypes.c_float(0.0)
+        self.check(self.lib.cs_mlp_energy_gradient_device(self.h, s0, s1, ctypes.c_void_p(grad.data_ptr()),
+                                                          ctypes.byref(loss)))
+        return loss.value
+
+    def mlp_energy_end(self, allow_unconverged: bool = False):
+        stats = StepStats()
+        st = self.lib.cs_mlp_energy_end(self.h, ctypes.byref(stats))
+        self.check(st, (CS_OK, CS_ERR_NOT_CONVERGED, CS_ERR_NON_SPD) if allow_unconverged else (CS_OK,))
+        return stats
 
     def mlp_gradient_device(self, slot: int, s0: int, s1: int, grad) -> float:
         """One minibatch's gradient into `grad`, a CUDA tensor of MLP_TRAINED floats on this

@@ -1,5 +1,8 @@
 """Training of the learned warm start: on one context, or data-parallel over ranks.
 
+`energy_step_data_parallel` is the data-parallel form of cs_mlp_train_step (energy-norm
+training along the solver's own trajectories), with the same minibatch order.
+
 cs_mlp_train runs Adam over minibatches of whole sheets of the recorded trajectories on one
 GPU.  `train_data_parallel` runs the same schedule on every rank of a process group, each rank
 on its own trajectories: the normalisation comes from the moments summed over ranks, and every
@@ -75,3 +78,32 @@ def train_data_parallel(ctx, n_slots: int, n_sheets: int, epochs: int, lr: float
             ctx.mlp_apply_gradient(grad, lr)
         losses.append(acc / max(len(batches), 1))
     return losses
+
+
+def energy_step_data_parallel(ctx, params, n_sheets: int, lr: float, sheets_per_batch: int, seed: int,
+                              allreduce_sum: Callable, world: int, grad=None, allow_unconverged: bool = True):
+    """One step of energy-norm training (cs_mlp_train_step) with gradients averaged over the
+    group: this rank's step is solved and updated as cs_mlp_train_step does it, and every
+    minibatch of cs_mlp_train_step's order (its seeded shuffle) takes the Adam step on the
+    gradient summed over the ranks and divided by their number.  Every rank has the same
+    number of sheets, so the collectives pair up.  Returns (step statistics, mean minibatch
+    loss of this rank)."""
+    import torch
+
+    from .native import MLP_TRAINED
+
+    if grad is None:
+        grad = torch.empty(MLP_TRAINED, dtype=torch.float32, device=ctx.torch_device)
+    ctx.mlp_energy_begin(params)
+    (batches,) = list(minibatch_schedule(1, n_sheets, sheets_per_batch, 1, seed))
+    acc = 0.0
+    for _, s0, s1 in batches:
+        acc += ctx.mlp_energy_gradient_device(s0, s1, grad)
+        if world > 1:
+            allreduce_sum(grad)
+            grad.mul_(1.0 / world)
+            if grad.is_cuda:
+                torch.cuda.current_stream(grad.device).synchronize()
+        ctx.mlp_apply_gradient(grad, lr)
+    stats = ctx.mlp_energy_end(allow_unconverged=allow_unconverged)
+    return stats, acc / max(len(batches), 1)

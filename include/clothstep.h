@@ -383,6 +383,16 @@ cs_status cs_mlp_train_step(cs_ctx* ctx, const cs_step_params* params, float lr,
                             unsigned long long seed, cs_step_stats* stats, float* loss);
 cs_status cs_mlp_energy_gradient(cs_ctx* ctx, const cs_step_params* params, int sheet_begin, int sheet_end,
                                  float* grad, float* loss);
+/* cs_mlp_train_step in parts, for data-parallel training across ranks (each on its own
+ * trajectories): cs_mlp_energy_begin (assembly, features, solve), then per minibatch of the
+ * common schedule cs_mlp_energy_gradient_device (the loss's gradient for sheets
+ * [sheet_begin, sheet_end) into a DEVICE buffer of CS_MLP_PARAMS - 38 floats, to all-reduce,
+ * and the minibatch's loss) and cs_mlp_apply_gradient, then cs_mlp_energy_end (the state
+ * update; stats as cs_step's).  With one rank and cs_mlp_train_step's minibatch order (its
+ * seeded shuffle of the minibatches) they give its weights bit for bit. */
+cs_status cs_mlp_energy_begin(cs_ctx* ctx, const cs_step_params* params);
+cs_status cs_mlp_energy_gradient_device(cs_ctx* ctx, int sheet_begin, int sheet_end, float* grad, float* loss);
+cs_status cs_mlp_energy_end(cs_ctx* ctx, cs_step_stats* stats);
 /* Data-parallel training across ranks (one context per GPU, each on its own trajectories):
  * cs_mlp_moments gives the normalisation's sums (38 doubles: 16 feature and 3 target sums, then
  * their 19 sums of squares) and node count for an all-reduce, cs_mlp_set_moments sets the

@@ -112,3 +112,25 @@ def test_two_ranks_same_data_equal_one_rank():
 def test_two_ranks_different_data_agree():
     w = run_two([31, 32])
     assert np.array_equal(w[0], w[1])
+
+
+def test_energy_single_rank_matches_train_step():
+    """The data-parallel energy step (cs_mlp_energy_begin / _gradient_device / apply / _end) with
+    one rank reproduces cs_mlp_train_step bit for bit: weights, state and losses."""
+    a, b = recorded_ctx(13), recorded_ctx(13)
+    for c in (a, b):
+        c.mlp_fit_normalization(SLOTS)
+    sc = scenes.windy_batch(SHEETS, NQ, seed=13)
+    p = native.step_params(sc.dt, sc.gravity, sc.handle_stiffness, tol=1e-7, max_iters=8000,
+                           warm_start=native.WARM_PREVIOUS)
+    for t in range(4):
+        _, la = a.mlp_train_step(p, lr=1e-3, sheets_per_batch=2, seed=40 + t)
+        _, lb = training.energy_step_data_parallel(b, p, SHEETS, 1e-3, 2, 40 + t, allreduce_sum=None, world=1,
+                                                   allow_unconverged=False)
+        assert abs(la - lb) <= 1e-6 * max(1.0, abs(la))
+    assert np.array_equal(a.mlp_get_weights(), b.mlp_get_weights())
+    xa, va = a.get_state()
+    xb, vb = b.get_state()
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+    a.close()
+    b.close()
