@@ -1,0 +1,310 @@
+// Coarse-space correction of the batched PCG loop (pcg.cu).  No reference counterpart: the
+// reference's GPU solve is Jacobi-PCG (Cloth.cu:766-809).
+//
+// Block-Jacobi PCG needs many iterations on a large sheet (1,700 on a 1,000 x 1,000 grid): the
+// smooth error spans the sheet and the diagonal blocks cannot move it.  Each sheet's nodes are
+// grouped into aggregates (its rest (u, v) coordinates binned into g x g cells, the non-empty
+// cells), and the preconditioner becomes additive two-level,
+//     z = D^-1 r + R^T A_c^-1 R r,
+// R summing a vector over each aggregate (one value per aggregate and component) and
+// A_c = R A R^T.  Per step: A_c is summed from per-pair contributor lists (a fixed order, so
+// the result is deterministic) and inverted by Gauss-Jordan in FP32 -- one CTA with the matrix
+// in shared memory up to CS_BC_SMALL_NC unknowns, else a cluster of CS_BC_CLUSTER CTAs with its
+// rows spread over their shared memory and each pivot row broadcast through distributed shared
+// memory -- then symmetrised.  A_c is SPD (A is), so no pivoting is needed; a pivot that is not
+// positive disables the correction of that sheet for the step.  Per CG trip, after the vector
+// update: R r (a warp per aggregate), e_c = A_c^-1 R r (a warp per coarse row), then
+// z += R^T e_c with the r.z and r.r partials recomputed (a warp per 32 rows in natural order,
+// as cs_vector_kernel lays them out).  Sheets solved cluster-resident (their own coarse
+// correction, resident.cu) and sheets with proximities (blocks outside the pattern) skip it.
+#include <cooperative_groups.h>
+
+#include "cs_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+template <class T>
+__device__ __forceinline__ T bc_warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// The sheet takes the correction this step (independent of its phase).
+__device__ __forceinline__ bool bc_sheet_on(const Batch& B, int s) {
+    if (!B.params->coarse || !B.bc_agg) return false;
+    if (B.sheets[s].bc_na <= 0) return false;
+    if (B.sheet_prox && B.sheet_prox[s]) return false;
+    return true;
+}
+
+// The sheet applies the correction in this trip: a CG iteration or a sweep start of the loop.
+__device__ __forceinline__ bool bc_trip_on(const Batch& B, int s) {
+    const int ph = B.inst[s].phase;
+    return (ph == PH_CG || ph == PH_INIT) && bc_sheet_on(B, s) && B.bc_ok[s];
+}
+
+}  // namespace
+
+// A_c of every sheet the loop solves: a warp per coarse pair (a, b) sums the 3x3 blocks of its
+// contributor slots (lane-strided, then a butterfly: a fixed order) into rows 3a..3a+2,
+// columns 3b..3b+2 of the sheet's dense coarse matrix (zeroed before).  Grid: x over pairs,
+// y over sheets.
+__global__ void __launch_bounds__(256) cs_bc_assemble_kernel(Batch B) {
+    const int s = blockIdx.y;
+    if (!bc_sheet_on(B, s) || B.inst[s].phase == PH_RESIDENT) return;
+    const SheetDesc& sh = B.sheets[s];
+    const int nc = 3 * sh.bc_na;
+    float* M = B.bc_mat + sh.bc_mat_off;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int q = blockIdx.x * wpb + (threadIdx.x >> 5); q < sh.bc_npair; q += gridDim.x * wpb) {
+        const int4 pr = B.bc_pair[sh.bc_pair_off + q];
+        float a[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) a[k] = 0.f;
+        for (int k = pr.z + lane; k < pr.w; k += 32) {
+            const int slot = B.bc_contrib[k];
+            const float* panel = B.A + (size_t)(sh.panel_off + (slot >> 5)) * CS_PANEL_FLOATS;
+            const int l = slot & 31;
+            const float4 a0 = reinterpret_cast<const float4*>(panel)[l];
+            const float4 a1 = reinterpret_cast<const float4*>(panel + 128)[l];
+            const float a8 = panel[256 + l];
+            a[0] += a0.x;
+            a[1] += a0.y;
+            a[2] += a0.z;
+            a[3] += a0.w;
+            a[4] += a1.x;
+            a[5] += a1.y;
+            a[6] += a1.z;
+            a[7] += a1.w;
+            a[8] += a8;
+        }
+#pragma unroll
+        for (int k = 0; k < 9; k++) a[k] = bc_warp_sum(a[k]);
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) M[(size_t)(3 * pr.x + k / 3) * nc + 3 * pr.y + k % 3] = a[k];
+        }
+    }
+}
+
+// Gauss-Jordan inversion in place of an SPD matrix held by one CTA in shared memory (nc <=
+// CS_BC_SMALL_NC), a block per sheet; the inverse is written symmetrised.
+__global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch B) {
+    extern __shared__ float bc_sm[];
+    __shared__ int bad;
+    const int s = blockIdx.x;
+    if (!bc_sheet_on(B, s) || B.inst[s].phase == PH_RESIDENT) return;
+    const SheetDesc& sh = B.sheets[s];
+    const int nc = 3 * sh.bc_na;
+    if (nc > CS_BC_SMALL_NC) return;
+    float* M = bc_sm;
+    float* rowb = bc_sm + nc * nc;
+    float* colb = rowb + nc;
+    const float* G = B.bc_mat + sh.bc_mat_off;
+    const int n2 = nc * nc;
+    for (int e = threadIdx.x; e < n2; e += blockDim.x) M[e] = G[e];
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    for (int k = 0; k < nc; k++) {
+        const float p = M[k * nc + k];
+        if (!(p > 0.f) || !isfinite(p)) {  // the same value in every thread: a uniform exit
+            if (threadIdx.x == 0) bad = 1;
+            break;
+        }
+        const float ip = 1.0f / p;
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+            rowb[j] = j == k ? ip : M[k * nc + j] * ip;
+            colb[j] = M[j * nc + k];
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < n2; e += blockDim.x) {
+            const int i = e / nc, j = e - i * nc;
+            float v;
+            if (i == k) v = rowb[j];
+            else if (j == k) v = -colb[i] * ip;
+            else v = __fmaf_rn(-colb[i], rowb[j], M[e]);
+            M[e] = v;
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    float* Inv = B.bc_inv + sh.bc_mat_off;
+    if (!bad)
+        for (int e = threadIdx.x; e < n2; e += blockDim.x) {
+            const int i = e / nc, j = e - i * nc;
+            Inv[e] = 0.5f * (M[e] + M[j * nc + i]);
+        }
+    if (threadIdx.x == 0) B.bc_ok[s] = bad ? 0 : 1;
+}
+
+// Gauss-Jordan inversion of a larger coarse matrix (CS_BC_SMALL_NC < nc <= CS_BC_MAX_NC) by a
+// cluster of CS_BC_CLUSTER CTAs, one cluster per sheet of B.bc_big: rank c holds rows
+// c, c + CS_BC_CLUSTER, ... in shared memory.  Per pivot k its owner writes the normalised row
+// (and a validity flag) into every CTA's pivot buffer (two buffers alternate), one cluster
+// barrier, then every CTA updates its rows.  A CTA reuses a buffer only after the barrier that
+// follows every CTA's last read of it, so one barrier per pivot suffices.  The raw inverse goes
+// back to bc_mat, then (after a barrier) each CTA writes its rows of the symmetrised inverse.
+__global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Batch B) {
+    extern __shared__ float bc_sm[];
+    __shared__ int bad;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int s = B.bc_big[blockIdx.x / CS_BC_CLUSTER];
+    // the same decision in every CTA of the cluster: all return, or none
+    if (!bc_sheet_on(B, s) || B.inst[s].phase == PH_RESIDENT) return;
+    const SheetDesc& sh = B.sheets[s];
+    const int nc = 3 * sh.bc_na;
+    if (nc <= CS_BC_SMALL_NC || nc > CS_BC_MAX_NC) return;
+    const int RM = (nc + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER;
+    const int R = (nc - rank + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER;  // rows rank + CS_BC_CLUSTER * li
+    float* M = bc_sm;                    // RM x nc
+    float* pbuf = bc_sm + RM * nc;       // 2 x (nc + 1): pivot row, then the validity flag
+    float* colb = pbuf + 2 * (nc + 1);   // RM
+    float* G = B.bc_mat + sh.bc_mat_off;
+    for (int e = threadIdx.x; e < R * nc; e += blockDim.x) {
+        const int li = e / nc, j = e - li * nc;
+        M[e] = G[(size_t)(rank + CS_BC_CLUSTER * li) * nc + j];
+    }
+    if (threadIdx.x == 0) bad = 0;
+    cluster.sync();  // every CTA has started and loaded its rows before remote writes
+    for (int k = 0; k < nc; k++) {
+        float* buf = pbuf + (k & 1) * (nc + 1);
+        if (rank == k % CS_BC_CLUSTER) {
+            const int lk = k / CS_BC_CLUSTER;
+            const float p = M[lk * nc + k];
+            const bool ok = p > 0.f && isfinite(p);
+            const float ip = ok ? 1.0f / p : 0.f;
+            for (int t = threadIdx.x; t < (nc + 1) * CS_BC_CLUSTER; t += blockDim.x) {
+                const int dst = t / (nc + 1), j = t - dst * (nc + 1);
+                const float v = j == nc ? (ok ? 1.f : 0.f) : (j == k ? ip : M[lk * nc + j] * ip);
+                float* rb = cluster.map_shared_rank(buf, dst);
+                rb[j] = v;
+            }
+        }
+        cluster.sync();
+        if (buf[nc] == 0.f) {  // the same flag in every CTA: a uniform exit
+            if (threadIdx.x == 0) bad = 1;
+            break;
+        }
+        const float ip = buf[k];
+        for (int li = threadIdx.x; li < R; li += blockDim.x) colb[li] = M[li * nc + k];
+        __syncthreads();
+        for (int e = threadIdx.x; e < R * nc; e += blockDim.x) {
+            const int li = e / nc, j = e - li * nc;
+            const int i = rank + CS_BC_CLUSTER * li;
+            float v;
+            if (i == k) v = buf[j];
+            else if (j == k) v = -colb[li] * ip;
+            else v = __fmaf_rn(-colb[li], buf[j], M[e]);
+            M[e] = v;
+        }
+        __syncthreads();
+    }
+    cluster.sync();
+    if (!bad)
+        for (int e = threadIdx.x; e < R * nc; e += blockDim.x) {
+            const int li = e / nc, j = e - li * nc;
+            G[(size_t)(rank + CS_BC_CLUSTER * li) * nc + j] = M[e];
+        }
+    __threadfence();
+    cluster.sync();
+    float* Inv = B.bc_inv + sh.bc_mat_off;
+    if (!bad)
+        for (int e = threadIdx.x; e < R * nc; e += blockDim.x) {
+            const int li = e / nc, j = e - li * nc;
+            const int i = rank + CS_BC_CLUSTER * li;
+            Inv[(size_t)i * nc + j] = 0.5f * (M[e] + __ldcg(&G[(size_t)j * nc + i]));
+        }
+    if (rank == 0 && threadIdx.x == 0) B.bc_ok[s] = bad ? 0 : 1;
+}
+
+// R r: a warp per aggregate sums r over its member nodes (ascending, lane-strided, then a
+// butterfly) in FP64, stored in FP32.
+__global__ void __launch_bounds__(256) cs_bc_restrict_kernel(Batch B) {
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (w >= B.bc_total_agg) return;
+    const int2 sa = B.bc_agg[w];
+    if (!bc_trip_on(B, sa.x)) return;
+    const SheetDesc& sh = B.sheets[sa.x];
+    const int m0 = B.bc_mptr[sh.bc_agg_off + sa.y], m1 = B.bc_mptr[sh.bc_agg_off + sa.y + 1];
+    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+    for (int m = m0 + lane; m < m1; m += 32) {
+        const int node = sh.node_off + B.bc_mem[sh.bc_mem_off + m];
+        r0 += (double)B.r[3 * node];
+        r1 += (double)B.r[3 * node + 1];
+        r2 += (double)B.r[3 * node + 2];
+    }
+    r0 = bc_warp_sum(r0);
+    r1 = bc_warp_sum(r1);
+    r2 = bc_warp_sum(r2);
+    if (lane == 0) {
+        float* rc = B.bc_rc + sh.bc_vec_off + 3 * sa.y;
+        rc[0] = (float)r0;
+        rc[1] = (float)r1;
+        rc[2] = (float)r2;
+    }
+}
+
+// e_c = A_c^-1 R r: a warp per coarse row (lane-strided columns, then a butterfly).
+__global__ void __launch_bounds__(256) cs_bc_apply_kernel(Batch B) {
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (w >= 3 * B.bc_total_agg) return;
+    const int2 sa = B.bc_agg[w / 3];
+    if (!bc_trip_on(B, sa.x)) return;
+    const SheetDesc& sh = B.sheets[sa.x];
+    const int nc = 3 * sh.bc_na, i = 3 * sa.y + w % 3;
+    const float* row = B.bc_inv + sh.bc_mat_off + (size_t)i * nc;
+    const float* rc = B.bc_rc + sh.bc_vec_off;
+    float acc = 0.f;
+    for (int j = lane; j < nc; j += 32) acc = __fmaf_rn(row[j], rc[j], acc);
+    acc = bc_warp_sum(acc);
+    if (lane == 0) B.bc_ec[sh.bc_vec_off + i] = acc;
+}
+
+// z += R^T e_c over the rows of the slice index's natural-order chunk (as cs_vector_kernel takes
+// them), and that chunk's r.z and r.r partials recomputed with the corrected z.
+__global__ void __launch_bounds__(128) cs_bc_finish_kernel(Batch B) {
+    const int slice = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (slice >= B.n_slices) return;
+    const SliceDesc sd = B.slices[slice];
+    if (!bc_trip_on(B, sd.sheet)) return;
+    const SheetDesc& sh = B.sheets[sd.sheet];
+    const bool mixed = B.params->mixed != 0;
+    const bool live = lane < sd.rows;
+    const int local = CS_SLICE * (slice - sh.slice_off) + lane;
+    double rz = 0.0, rr = 0.0;
+    float rzf = 0.f, rrf = 0.f;
+    if (live) {
+        const int row = sh.node_off + local;
+        const float* ec = B.bc_ec + sh.bc_vec_off + 3 * B.bc_node_agg[sh.bc_node_off + local];
+        float r[3], z[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            r[c] = B.r[3 * row + c];
+            z[c] = B.z[3 * row + c] + ec[c];
+            B.z[3 * row + c] = z[c];
+        }
+        if (mixed) {
+            rz = (double)r[0] * z[0] + (double)r[1] * z[1] + (double)r[2] * z[2];
+            rr = (double)r[0] * r[0] + (double)r[1] * r[1] + (double)r[2] * r[2];
+        } else {
+            rzf = r[0] * z[0] + r[1] * z[1] + r[2] * z[2];
+            rrf = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        }
+    }
+    if (mixed) {
+        rz = bc_warp_sum(rz);
+        rr = bc_warp_sum(rr);
+    } else {
+        rz = (double)bc_warp_sum(rzf);
+        rr = (double)bc_warp_sum(rrf);
+    }
+    if (lane == 0) {
+        B.part[2 * slice] = rz;
+        B.part[2 * slice + 1] = rr;
+    }
+}

@@ -57,6 +57,10 @@ struct SheetDesc {
     int resident;               // 1: solved by the cluster-resident kernel (resident.cu)
     int csr_ptr_off;            // this sheet's topology in tcsr_ptr (block CSR for slot lookups)
     int panel_off;              // first value panel: global slot = panel_off * 32 + topology slot
+    // coarse space of the batched loop: this sheet's topology in the aggregate arrays, its
+    // aggregates, its coarse unknowns' offset in the per-sheet vectors and its matrices' offset
+    int bc_node_off, bc_agg_off, bc_mem_off, bc_pair_off, bc_npair, bc_na, bc_vec_off;
+    long long bc_mat_off;
 };
 
 struct SliceDesc {
@@ -103,6 +107,16 @@ enum InstPhase : int {
 // the coarse space holds one constant per (segment, component).
 // threads of the per-instance reduction kernels of the batched loop
 #define CS_REDUCE_THREADS 256
+// coarse-space correction of the batched loop (coarse.cu): a sheet's nodes binned by their rest
+// (u, v) into g x g cells (g = round(sqrt(nodes / CS_BC_NODES_PER_AGG)), 1..CS_BC_MAX_G), the
+// non-empty cells its aggregates; coarse systems up to CS_BC_SMALL_NC unknowns are inverted by
+// one CTA in shared memory, larger ones by a cluster of CS_BC_CLUSTER CTAs
+#define CS_BC_NODES_PER_AGG 256
+#define CS_BC_MAX_G 16
+#define CS_BC_MAX_NC (3 * CS_BC_MAX_G * CS_BC_MAX_G)
+#define CS_BC_SMALL_NC 192
+#define CS_BC_CLUSTER 16
+#define CS_BC_THREADS 512
 #define CS_COARSE_MAX_K 8
 #define CS_COARSE_AGGS 54
 // Threads of the per-sheet set-up kernel that forms and inverts the coarse matrix.
@@ -185,6 +199,22 @@ struct ProxInst {
 
 struct Batch {
     int N = 0, F = 0, E = 0, S = 0;
+    // coarse-space correction of the batched loop (coarse.cu)
+    int bc_total_agg = 0;        // aggregates of all sheets (the per-aggregate kernels' work list)
+    int bc_max_npair = 0;        // largest coarse pair count of a sheet
+    int bc_n_big = 0;            // sheets whose coarse system exceeds CS_BC_SMALL_NC
+    int2* bc_agg = nullptr;      // per global aggregate: (sheet, local aggregate)
+    int* bc_big = nullptr;       // the sheets inverted by a cluster
+    int* bc_node_agg = nullptr;  // per topology node: its aggregate
+    int* bc_mptr = nullptr;      // per topology aggregate: member range (na + 1 per topology)
+    int* bc_mem = nullptr;       // per topology: member nodes, by aggregate, ascending
+    int4* bc_pair = nullptr;     // per topology coarse pair: (a, b, contributor begin, end)
+    int* bc_contrib = nullptr;   // topology slots (panel * 32 + lane) of the stored blocks of each pair
+    float* bc_mat = nullptr;     // per sheet nc x nc: the coarse matrix R A R^T (then GJ's work)
+    float* bc_inv = nullptr;     // per sheet nc x nc: its inverse, symmetrised
+    float* bc_rc = nullptr;      // per sheet nc: R r
+    float* bc_ec = nullptr;      // per sheet nc: A_c^-1 R r
+    int* bc_ok = nullptr;        // per sheet: the coarse inverse of this step is valid
     int n_slices = 0, n_panels = 0, n_tpanels = 0, n_tables = 0;
     // nodes
     float *x = nullptr, *v = nullptr, *dv = nullptr, *mass = nullptr;

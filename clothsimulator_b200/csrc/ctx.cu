@@ -51,6 +51,12 @@ static_assert(CS_SPMV_CANDIDATES == CS_TUNE_SPMV_SHAPES, "the tuner's result hol
 __global__ void cs_prox_kernel(Batch B);
 __global__ void cs_prox_row_kernel(Batch B);
 __global__ void cs_slice_bnorm_kernel(Batch B);
+__global__ void cs_bc_assemble_kernel(Batch B);
+__global__ void cs_bc_invert_small_kernel(Batch B);
+__global__ void cs_bc_invert_cluster_kernel(Batch B);
+__global__ void cs_bc_restrict_kernel(Batch B);
+__global__ void cs_bc_apply_kernel(Batch B);
+__global__ void cs_bc_finish_kernel(Batch B);
 __global__ void cs_scan_sums_kernel(const int* data, int n, int* partial);
 __global__ void cs_scan_partials_kernel(int* partial, int nb, int* total);
 __global__ void cs_scan_apply_kernel(int* data, int n, const int* partial);
@@ -601,6 +607,69 @@ void permuteLanesByAggregate(Topo& T, const std::vector<int>& agg) {
     T.tcontrib.swap(tcontrib);
 }
 
+// Coarse space of the batched loop for one topology (coarse.cu): the nodes binned by their rest
+// (u, v) into g x g cells of the bounding box (g = round(sqrt(nodes / CS_BC_NODES_PER_AGG)),
+// 1..gmax), the non-empty cells numbered in cell order as aggregates; members of each
+// aggregate ascending; per pair of aggregates, the stored blocks coupling them in slot order.
+struct BCPlan {
+    int na = 0;
+    std::vector<int> agg, mptr, mem, contrib;
+    std::vector<int4> pairs;
+};
+
+void batchedCoarsePlan(const Topo& T, int gmax, BCPlan& P) {
+    P = BCPlan();
+    const int n = T.n_nodes;
+    if (n <= 0 || (int)T.node_uv.size() < 2 * n) return;
+    int g = (int)std::lround(std::sqrt((double)n / CS_BC_NODES_PER_AGG));
+    g = std::max(1, std::min(g, gmax));
+    float u0 = T.node_uv[0], u1 = u0, v0 = T.node_uv[1], v1 = v0;
+    for (int i = 0; i < n; i++) {
+        u0 = std::min(u0, T.node_uv[2 * i]);
+        u1 = std::max(u1, T.node_uv[2 * i]);
+        v0 = std::min(v0, T.node_uv[2 * i + 1]);
+        v1 = std::max(v1, T.node_uv[2 * i + 1]);
+    }
+    const double du = u1 > u0 ? (double)(u1 - u0) : 1.0, dv = v1 > v0 ? (double)(v1 - v0) : 1.0;
+    std::vector<int> cell(n), id(g * g, -1);
+    for (int i = 0; i < n; i++) {
+        const int cu = std::min(g - 1, std::max(0, (int)((T.node_uv[2 * i] - u0) / du * g)));
+        const int cv = std::min(g - 1, std::max(0, (int)((T.node_uv[2 * i + 1] - v0) / dv * g)));
+        cell[i] = cu * g + cv;
+        id[cell[i]] = 0;
+    }
+    for (int k = 0; k < g * g; k++)
+        if (id[k] == 0) id[k] = P.na++;
+    P.agg.resize(n);
+    P.mptr.assign(P.na + 1, 0);
+    for (int i = 0; i < n; i++) {
+        P.agg[i] = id[cell[i]];
+        P.mptr[P.agg[i] + 1]++;
+    }
+    for (int a = 0; a < P.na; a++) P.mptr[a + 1] += P.mptr[a];
+    P.mem.resize(n);
+    std::vector<int> fill(P.mptr.begin(), P.mptr.end() - 1);
+    for (int i = 0; i < n; i++) P.mem[fill[P.agg[i]]++] = i;
+    // coarse pattern: every stored block (slots with contributors; padding has none)
+    std::vector<std::tuple<int, int, int>> blk;
+    for (int sl = 0; sl < T.n_slices; sl++)
+        for (int k = 0; k < T.slice_width[sl]; k++)
+            for (int l = 0; l < T.slice_rows[sl]; l++) {
+                const int slot = (T.slice_tpanel0[sl] + k) * CS_SLICE + l;
+                if (T.tcptr[slot + 1] == T.tcptr[slot]) continue;
+                blk.emplace_back(P.agg[T.rowmap[sl * CS_SLICE + l]], P.agg[T.tcol[slot]], slot);
+            }
+    std::sort(blk.begin(), blk.end());
+    for (size_t i = 0; i < blk.size();) {
+        size_t j = i;
+        while (j < blk.size() && std::get<0>(blk[j]) == std::get<0>(blk[i]) && std::get<1>(blk[j]) == std::get<1>(blk[i])) j++;
+        P.pairs.push_back(make_int4(std::get<0>(blk[i]), std::get<1>(blk[i]), (int)P.contrib.size(),
+                                    (int)(P.contrib.size() + (j - i))));
+        for (size_t q = i; q < j; q++) P.contrib.push_back(std::get<2>(blk[q]));
+        i = j;
+    }
+}
+
 // Coarse-space plan of one topology on a cluster of `ncta` CTAs: each CTA's strip of rows is cut
 // into K segments of equal row count along the principal axis of the rows' rest coordinates (a
 // strip of a grid sheet is a band of grid rows; its segments are blocks side by side), and the
@@ -808,6 +877,8 @@ struct cs_ctx {
     int spmvShape = CS_SPMV_DEFAULT;    // launch shape of the batched SpMV (cs_tune)
     int tunedDegree = 0, tunedCoarse = 0;  // fastest resident preconditioner found by cs_tune (0: not tuned)
     int tunedSolver = -1;                  // faster solve route found by cs_tune (-1: not tuned)
+    size_t bcSmemBig = 0;                  // dynamic shared memory of cs_bc_invert_cluster_kernel
+    long long bcMatFloats = 0;             // floats of the batched loop's coarse matrices
     bool energyBegun = false;              // cs_mlp_energy_begin ran; cs_mlp_energy_end not yet
     int energyLoopCap = 0;                 // the begun step's trip bound (its statistics)
     std::vector<int> handleNode;  // batch node of every handle, in load order (cs_set_handle_motions)
@@ -928,9 +999,48 @@ int launchAssembly(cs_ctx* c) {
     return n;
 }
 
+// The batched loop's coarse matrices of this step's systems, inverted (coarse.cu; the kernels
+// return at once for sheets the loop does not solve or when the step asks for no correction).
+int launchBatchedCoarseSetup(cs_ctx* c) {
+    Batch& B = c->B;
+    if (B.bc_total_agg <= 0) return 0;
+    cudaMemsetAsync(B.bc_mat, 0, (size_t)c->bcMatFloats * sizeof(float), c->stream);
+    const int gx = std::max(1, std::min(256, nblk(B.bc_max_npair, 8)));
+    cs_bc_assemble_kernel<<<dim3(gx, B.S), 256, 0, c->stream>>>(B);
+    cs_bc_invert_small_kernel<<<B.S, CS_BC_THREADS, (CS_BC_SMALL_NC * CS_BC_SMALL_NC + 2 * CS_BC_SMALL_NC) * sizeof(float),
+                                c->stream>>>(B);
+    int n = 2;
+    if (B.bc_n_big > 0) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = CS_BC_CLUSTER;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(CS_BC_CLUSTER * B.bc_n_big);
+        cfg.blockDim = dim3(CS_BC_THREADS);
+        cfg.dynamicSmemBytes = c->bcSmemBig;
+        cfg.stream = c->stream;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, cs_bc_invert_cluster_kernel, B);
+        n++;
+    }
+    return n;
+}
+
+// Kernels per step of the batched loop's coarse set-up, of the resident solve, and per loop trip
+// (the launch counters of cs_get_counters).
+int bcSetupKernels(const cs_ctx* c) { return c->B.bc_total_agg > 0 ? 2 + (c->B.bc_n_big > 0 ? 1 : 0) : 0; }
+int residentKernels(const cs_ctx* c) {
+    return c->resClusters > 0 ? 1 + (c->B.res_cnc > 0 && c->B.n_resident > 0 ? 1 : 0) : 0;
+}
+int tripKernels(const cs_ctx* c) { return 4 + (c->B.bc_total_agg > 0 ? 3 : 0); }
+
 void launchSolvePrologue(cs_ctx* c) {
     Batch& B = c->B;
     cs_solve_setup_kernel<<<B.S, 128, 0, c->stream>>>(B);
+    launchBatchedCoarseSetup(c);
     cs_solve_prologue_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B);
 }
 
@@ -986,6 +1096,12 @@ void launchTrip(cs_ctx* c, cudaGraphConditionalHandle h) {
     launchSpmvShape(B, c->spmvShape, c->stream);
     cs_reduce1_kernel<<<B.S, CS_REDUCE_THREADS, 0, c->stream>>>(B);
     cs_vector_kernel<<<g, 128, 0, c->stream>>>(B);
+    if (B.bc_total_agg > 0) {
+        // the coarse correction of z and the r.z, r.r partials it changes (coarse.cu)
+        cs_bc_restrict_kernel<<<nblk((long long)B.bc_total_agg * 32, 256), 256, 0, c->stream>>>(B);
+        cs_bc_apply_kernel<<<nblk((long long)B.bc_total_agg * 96, 256), 256, 0, c->stream>>>(B);
+        cs_bc_finish_kernel<<<g, 128, 0, c->stream>>>(B);
+    }
     cs_reduce2_kernel<<<B.S, CS_REDUCE_THREADS, 0, c->stream>>>(B, h);
 }
 
@@ -1315,6 +1431,56 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             hragg.insert(hragg.end(), topos[t]->n_nodes, -1);
         }
     }
+    // the batched loop's coarse spaces (after the lane moves above: the contributor slots refer
+    // to the final slot numbering); up to CS_BC_MAX_G^2 aggregates when 16-CTA clusters can run
+    // the larger inversions, else as many as one CTA inverts
+    int bcGmax = CS_BC_MAX_G;
+    {
+        const size_t smemBig = ((size_t)((CS_BC_MAX_NC + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER) * CS_BC_MAX_NC +
+                                2 * (CS_BC_MAX_NC + 1) + (CS_BC_MAX_NC + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER) * sizeof(float);
+        int nclusters = 0;
+        if (cudaFuncSetAttribute(cs_bc_invert_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBig) ==
+                cudaSuccess &&
+            cudaFuncSetAttribute(cs_bc_invert_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+                cudaSuccess) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = CS_BC_CLUSTER;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(CS_BC_CLUSTER);
+            cfg.blockDim = dim3(CS_BC_THREADS);
+            cfg.dynamicSmemBytes = smemBig;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, cs_bc_invert_cluster_kernel, &cfg) != cudaSuccess) nclusters = 0;
+        }
+        cudaGetLastError();
+        c->bcSmemBig = smemBig;
+        if (nclusters <= 0) bcGmax = 8;  // 64 aggregates, 192 unknowns: one CTA inverts them
+        CS_CUDA(cudaFuncSetAttribute(cs_bc_invert_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (CS_BC_SMALL_NC * CS_BC_SMALL_NC + 2 * CS_BC_SMALL_NC) * (int)sizeof(float)));
+    }
+    std::vector<BCPlan> bcplans(topos.size());
+    for (size_t t = 0; t < topos.size(); t++) batchedCoarsePlan(*topos[t], bcGmax, bcplans[t]);
+    std::vector<int> hbc_node_agg, hbc_mptr, hbc_mem, hbc_contrib;
+    std::vector<int4> hbc_pair;
+    std::vector<int> topoBcNode0(topos.size()), topoBcAgg0(topos.size()), topoBcMem0(topos.size()),
+        topoBcPair0(topos.size());
+    for (size_t t = 0; t < topos.size(); t++) {
+        const BCPlan& P = bcplans[t];
+        topoBcNode0[t] = (int)hbc_node_agg.size();
+        topoBcAgg0[t] = (int)hbc_mptr.size();
+        topoBcMem0[t] = (int)hbc_mem.size();
+        topoBcPair0[t] = (int)hbc_pair.size();
+        hbc_node_agg.insert(hbc_node_agg.end(), P.agg.begin(), P.agg.end());
+        hbc_mptr.insert(hbc_mptr.end(), P.mptr.begin(), P.mptr.end());
+        hbc_mem.insert(hbc_mem.end(), P.mem.begin(), P.mem.end());
+        const int c0 = (int)hbc_contrib.size();
+        for (const int4& q : P.pairs) hbc_pair.push_back(make_int4(q.x, q.y, q.z + c0, q.w + c0));
+        hbc_contrib.insert(hbc_contrib.end(), P.contrib.begin(), P.contrib.end());
+    }
     c->resCL = c->resThreads = c->resClusters = 0;
     c->resSmem = 0;
     B.res_cnc = B.res_ck = B.res_coff = 0;
@@ -1371,6 +1537,10 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     }
     int node_off = 0, face_off = 0, edge_off = 0, slice_off = 0, panel_off = 0;
     long long nnzb = 0;
+    int bcVec = 0, bcMaxPair = 0;
+    long long bcMat = 0;
+    std::vector<int2> hbc_agg;
+    std::vector<int> hbc_big;
     for (int s = 0; s < n_sheets; s++) {
         const cs_sheet_desc& d = sheets[s];
         const cs_material_desc& m = mats[d.material];
@@ -1392,6 +1562,23 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         sd.resident = topoResident[sheetTopoId[s]];
         sd.csr_ptr_off = topoCsrPtr0[sheetTopoId[s]];
         sd.panel_off = panel_off;
+        {
+            const int t = sheetTopoId[s];
+            const BCPlan& P = bcplans[t];
+            sd.bc_node_off = topoBcNode0[t];
+            sd.bc_agg_off = topoBcAgg0[t];
+            sd.bc_mem_off = topoBcMem0[t];
+            sd.bc_pair_off = topoBcPair0[t];
+            sd.bc_npair = (int)P.pairs.size();
+            sd.bc_na = P.na;
+            sd.bc_vec_off = bcVec;
+            sd.bc_mat_off = bcMat;
+            bcVec += 3 * P.na;
+            bcMat += (long long)(3 * P.na) * (3 * P.na);
+            for (int a = 0; a < P.na; a++) hbc_agg.push_back(make_int2(s, a));
+            if (3 * P.na > CS_BC_SMALL_NC) hbc_big.push_back(s);
+            bcMaxPair = std::max(bcMaxPair, (int)P.pairs.size());
+        }
         hnode_sheet.insert(hnode_sheet.end(), d.n_nodes, s);
         float bmult = m.bending_mult * m.thicken;
         for (int i = 0; i < 15; i++) sd.bending[i] = m.bending[i / 5][i % 5] * bmult;
@@ -1528,6 +1715,22 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     UP(nbr, hnbr);
     UP(node_sheet, hnode_sheet);
     UP(rowmap, hrowmap);
+    UP(bc_agg, hbc_agg);
+    UP(bc_big, hbc_big);
+    UP(bc_node_agg, hbc_node_agg);
+    UP(bc_mptr, hbc_mptr);
+    UP(bc_mem, hbc_mem);
+    UP(bc_pair, hbc_pair);
+    UP(bc_contrib, hbc_contrib);
+    if ((st = dalloc(c, &B.bc_mat, (size_t)std::max(1LL, bcMat))) != CS_OK) return st;
+    if ((st = dalloc(c, &B.bc_inv, (size_t)std::max(1LL, bcMat))) != CS_OK) return st;
+    if ((st = dalloc(c, &B.bc_rc, (size_t)std::max(1, bcVec))) != CS_OK) return st;
+    if ((st = dalloc(c, &B.bc_ec, (size_t)std::max(1, bcVec))) != CS_OK) return st;
+    UP(bc_ok, std::vector<int>(n_sheets, 0));
+    B.bc_total_agg = (int)hbc_agg.size();
+    B.bc_max_npair = bcMaxPair;
+    B.bc_n_big = (int)hbc_big.size();
+    c->bcMatFloats = bcMat;
     UP(row2slot, hrow2slot);
     UP(tcsr_ptr, htcsr_ptr);
     UP(tcsr_col, htcsr_col);
@@ -1938,6 +2141,25 @@ cs_status candidatePairs(cs_ctx* c, const int* sheetGroup, int& npairs) {
 }
 
 // Scratch of the collision step: node-sized arrays once per batch, impact-sized ones grown.
+// The found impacts [0, n) into K.sorted by (time, node ids, type, index): four stable radix
+// sorts over the key parts, least significant first (cs_impact_keys_kernel), then one gather;
+// *pin = the permutation buffer holding the order.
+cs_status sortImpacts(cs_ctx* c, int nFound, int* pin_out) {
+    Collide& K = c->coll;
+    int pin = 0;
+    for (int pass = 0; pass < 4; pass++) {
+        cs_impact_keys_kernel<<<nblk(nFound, 256), 256, 0, c->stream>>>(K, nFound, pass, K.sperm[pin], K.skey[0],
+                                                                       K.sperm[pin]);
+        size_t bytes = K.stmp_bytes;
+        CS_CUDA(cub::DeviceRadixSort::SortPairs(K.stmp, bytes, K.skey[0], K.skey[1], K.sperm[pin], K.sperm[pin ^ 1],
+                                                nFound, 0, pass == 0 ? 1 : pass == 2 ? 32 : 64, c->stream));
+        pin ^= 1;
+    }
+    cs_impact_gather_kernel<<<nblk(nFound, 256), 256, 0, c->stream>>>(K, nFound, K.sperm[pin]);
+    *pin_out = pin;
+    return CS_OK;
+}
+
 cs_status collideScratch(cs_ctx* c, int nFound, int nAll) {
     Batch& B = c->B;
     Collide& K = c->coll;
@@ -2125,18 +2347,9 @@ cs_status cs_collision_step(cs_ctx* c, const cs_collision_params* p, cs_collisio
             }
             if (nFound > K.found_cap) return fail(c, CS_ERR_STATE, "impact buffer overflow");
             if ((st = collideScratch(c, nFound, nAll + nFound)) != CS_OK) return st;
-            // the round's impacts in order (time, node ids, type, index): four stable radix
-            // sorts over the key parts, least significant first, then one gather
+            // the round's impacts in order (time, node ids, type, index)
             int pin = 0;
-            for (int pass = 0; pass < 4; pass++) {
-                cs_impact_keys_kernel<<<nblk(nFound, 256), 256, 0, c->stream>>>(K, nFound, pass, K.sperm[pin], K.skey[0],
-                                                                               K.sperm[pin]);
-                size_t bytes = K.stmp_bytes;
-                CS_CUDA(cub::DeviceRadixSort::SortPairs(K.stmp, bytes, K.skey[0], K.skey[1], K.sperm[pin], K.sperm[pin ^ 1],
-                                                        nFound, 0, pass == 0 ? 1 : pass == 2 ? 32 : 64, c->stream));
-                pin ^= 1;
-            }
-            cs_impact_gather_kernel<<<nblk(nFound, 256), 256, 0, c->stream>>>(K, nFound, K.sperm[pin]);
+            if ((st = sortImpacts(c, nFound, &pin)) != CS_OK) return st;
             // independent impacts: rounds of per-node minima until no impact is live
             const int g = nblk(nFound, 256);
             cs_select_init_kernel<<<nblk(nFound + 1, 256), 256, 0, c->stream>>>(K, nFound);
@@ -2341,7 +2554,7 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
         if ((st = buildGraph(c, learned)) != CS_OK) return st;
         CS_CUDA(cudaGraphLaunch(learned ? c->graphExecLearned : c->graphExec, c->stream));
     } else {
-        c->hostLaunches += launchAssembly(c) + 3 + (c->resClusters > 0 ? 1 : 0);
+        c->hostLaunches += launchAssembly(c) + 3 + bcSetupKernels(c) + residentKernels(c);
         if (learned) c->hostLaunches += launchMlpInference(c, c->B.warm);
         launchSolvePrologue(c);
         launchResident(c);
@@ -2363,8 +2576,7 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
     if (p->use_graph) {
         c->graphSteps++;
         c->graphLaunchesFixed += (c->B.F ? 1 : 0) + (c->B.E ? 1 : 0) + 1 + 3 + (learned ? 3 : 0) +
-                                 (c->resClusters > 0 ? 1 : 0) +
-                                 (c->B.n_pinst > 0 ? 3 : 0);
+                                 bcSetupKernels(c) + residentKernels(c) + (c->B.n_pinst > 0 ? 3 : 0);
     }
     if (!stats) return CS_OK;
     return fillStepStats(c, stats, d.loop_cap, true);
@@ -2738,6 +2950,37 @@ cs_status cs_tune(cs_ctx* c, const cs_step_params* p, int reps, cs_tune_result* 
     return CS_OK;
 }
 
+cs_status cs_impact_order(cs_ctx* c, const int32_t* nodes, const float* t, const int32_t* type, int n,
+                          int32_t* order) {
+    if (!c || n < 0 || (n > 0 && (!nodes || !t || !type || !order))) return CS_ERR_INVALID_ARG;
+    if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
+    if (n == 0) return CS_OK;
+    for (int i = 0; i < n; i++) {
+        if (!(t[i] >= 0.0f) || (type[i] != 0 && type[i] != 1))
+            return fail(c, CS_ERR_INVALID_ARG, "impact %d: time below 0 or bad type", i);
+        for (int k = 0; k < 4; k++)
+            if (nodes[4 * i + k] < 0) return fail(c, CS_ERR_INVALID_ARG, "impact %d: negative node id", i);
+    }
+    CS_CUDA(cudaSetDevice(c->device));
+    cs_status st = collideScratch(c, n, 1);
+    if (st != CS_OK) return st;
+    std::vector<ImpactRec> h(n);
+    for (int i = 0; i < n; i++) {
+        ImpactRec r{};
+        for (int k = 0; k < 4; k++) r.nodes[k] = nodes[4 * i + k];
+        r.t = t[i];
+        r.type = type[i];
+        h[i] = r;
+    }
+    Collide& K = c->coll;
+    CS_CUDA(cudaMemcpyAsync(K.found, h.data(), n * sizeof(ImpactRec), cudaMemcpyHostToDevice, c->stream));
+    int pin = 0;
+    if ((st = sortImpacts(c, n, &pin)) != CS_OK) return st;
+    CS_CUDA(cudaMemcpyAsync(order, K.sperm[pin], n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    return CS_OK;
+}
+
 cs_status cs_get_counters(cs_ctx* c, long long* out) {
     if (!c || !out) return CS_ERR_INVALID_ARG;
     if (!c->loaded) return fail(c, CS_ERR_STATE, "no batch loaded");
@@ -2747,8 +2990,8 @@ cs_status cs_get_counters(cs_ctx* c, long long* out) {
     long long trips = (long long)(unsigned)loopv[4];
     out[0] = c->steps;
     out[1] = trips;
-    // graph steps: fixed kernels plus four per loop trip; host-driven steps are counted directly
-    out[2] = c->hostLaunches + c->graphLaunchesFixed + 4 * trips;
+    // graph steps: fixed kernels plus those of every loop trip; host-driven steps are counted directly
+    out[2] = c->hostLaunches + c->graphLaunchesFixed + tripKernels(c) * trips;
     return CS_OK;
 }
 

@@ -41,7 +41,7 @@ EXPORTED = [
     "cs_get_proximities", "cs_collision_step", "cs_mlp_moments", "cs_mlp_set_moments", "cs_mlp_gradient_device",
     "cs_mlp_apply_gradient", "cs_get_resident_blocks", "cs_set_handle_motions", "cs_tune",
     "cs_mlp_train_step", "cs_mlp_energy_gradient", "cs_mlp_energy_begin", "cs_mlp_energy_gradient_device",
-    "cs_mlp_energy_end",
+    "cs_mlp_energy_end", "cs_impact_order",
 ]
 MLP_PARAMS = 14761
 MLP_TRAINED = 14723
@@ -202,6 +202,7 @@ def load_library() -> ctypes.CDLL:
         "cs_mlp_energy_begin": [vp, ctypes.POINTER(StepParams)],
         "cs_mlp_energy_gradient_device": [vp, ctypes.c_int, ctypes.c_int, vp, _fp],
         "cs_mlp_energy_end": [vp, ctypes.POINTER(StepStats)],
+        "cs_impact_order": [vp, _ip, _fp, _ip, ctypes.c_int, _ip],
         "cs_mlp_moments": [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_longlong)],
         "cs_mlp_set_moments": [vp, _dp, ctypes.c_longlong],
         "cs_mlp_gradient_device": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, _fp],
@@ -589,6 +590,17 @@ class Context:
         self.check(self.lib.cs_mlp_energy_gradient(self.h, ctypes.byref(params), s0, s1, g.ctypes.data_as(_fp),
                                                    ctypes.byref(loss)))
         return g, loss.value
+
+    def impact_order(self, nodes, t, types):
+        """cs_impact_order: the collision step's order of the given impacts (indices)."""
+        nd = _i32(np.asarray(nodes).reshape(-1, 4))
+        tt = _f32(t)
+        ty = _i32(types)
+        n = tt.shape[0]
+        out = np.zeros(n, np.int32)
+        self.check(self.lib.cs_impact_order(self.h, nd.ctypes.data_as(_ip), tt.ctypes.data_as(_fp),
+                                            ty.ctypes.data_as(_ip), n, out.ctypes.data_as(_ip)))
+        return out
 
     def mlp_energy_begin(self, params: StepParams):
         self.check(self.lib.cs_mlp_energy_begin(self.h, ctypes.byref(params)))

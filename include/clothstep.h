@@ -95,11 +95,16 @@ typedef struct cs_step_params {
                                  block-Jacobi inverse; an odd degree 3..CS_PRECOND_MAX_DEGREE a
                                  Chebyshev polynomial of that degree in the block-Jacobi-scaled
                                  matrix of each CTA's strip of rows (no exchange between CTAs).
-                                 The batched loop always uses block-Jacobi. */
-    int coarse;               /* cluster-resident solver with the Chebyshev preconditioner: 1 adds
-                                 a coarse-space correction (one constant per component on each of
-                                 a few geometric segments of every CTA's strip, the coarse matrix
-                                 inverted per sheet and step), 0 leaves it out */
+                                 The batched loop uses block-Jacobi (with the coarse
+                                 correction when `coarse`). */
+    int coarse;               /* 1 adds a coarse-space correction, 0 leaves it out.  Cluster-resident
+                                 solver with the Chebyshev preconditioner: one constant per
+                                 component on each of a few geometric segments of every CTA's
+                                 strip.  Batched loop: one per aggregate of about 256 nodes (the
+                                 rest (u, v) binned into at most 16 x 16 cells), added to
+                                 block-Jacobi; sheets with proximities keep block-Jacobi alone.
+                                 Either way the coarse matrix R A R^T is inverted per sheet and
+                                 step. */
     /* Cloth::physicsStep's `transformations` (Cloth.cuh:91-92): the motions' transformations at
      * this step (Simulator::updateTransformations, Simulator.cu:565-569), CS_TRANSFORM_FLOATS
      * floats each -- scaling, translation (3), rotation quaternion (s, x, y, z) -- as
@@ -338,6 +343,15 @@ cs_status cs_profile_kernels(cs_ctx* ctx, const cs_step_params* params, int reps
 cs_status cs_get_counters(cs_ctx* ctx, long long* counters);
 /* The cudaStream_t the context launches on (for callers that record events on it). */
 cs_status cs_get_stream(cs_ctx* ctx, void** stream);
+/* The order the collision step gives n impacts (node ids nodes[4 i .. 4 i + 3], time t[i] >= 0,
+ * type[i] 0 vertex-face / 1 edge-edge): by time (-0.0 as +0.0), then node ids, then type (the
+ * reference's std::sort in Simulator::independentImpacts, Simulator.cu:394-420, ordered by
+ * time; the rest makes the order total), then input index, computed by the same device sort
+ * (four stable radix passes).  order[k] = the index of the k-th impact.  For tests; the
+ * context must hold a batch (its collision scratch is used). */
+cs_status cs_impact_order(cs_ctx* ctx, const int32_t* nodes, const float* t, const int32_t* type, int n,
+                          int32_t* order);
+
 /* Check of the tcgen05 tile GEMM the learned warm start is built on (no reference counterpart):
  * D[128 x N] = A[128 x K] * B[N x K]^T with BF16 inputs (raw 16-bit patterns, row-major host
  * arrays) and FP32 accumulation in tensor memory; K and N multiples of 16 in [16, 128]. */

@@ -134,3 +134,25 @@ def test_coplanar_start_matches_oracle(ctx_factory):
     assert orounds == -1 and st == native.CS_ERR_NOT_CONVERGED
     assert oimpacts > 0 and impacts == oimpacts
     assert np.array_equal(x.reshape(-1, 3), ox.astype(np.float32))
+
+
+def test_impact_order_ties_and_signed_zero(ctx_factory):
+    """The collision step's device sort of a round's impacts (cs_impact_order: four stable radix
+    passes over type, (n2, n3), n1, (t, n0)) equals the oracle's order -- time with -0.0 equal
+    to +0.0 (impactBefore, oracle_collide.hpp), then node ids, then type -- with the input index
+    as the last key, on records built to tie: few distinct times, small node ids, both types,
+    exact duplicates."""
+    scene = scenes.hang(8)
+    ctx = ctx_factory(scene.sheets)
+    rng = np.random.default_rng(3)
+    n = 3000
+    t = rng.choice(np.array([0.0, -0.0, 0.25, 0.5, 0.5000001, 1.0], np.float32), n)
+    nodes = rng.integers(0, 5, size=(n, 4)).astype(np.int32)
+    types = rng.integers(0, 2, n).astype(np.int32)
+    nodes[100:110] = nodes[99]
+    t[100:110] = t[99]
+    types[100:110] = types[99]
+    order = ctx.impact_order(nodes, t, types)
+    ref = sorted(range(n), key=lambda i: (float(t[i]) + 0.0, *(int(v) for v in nodes[i]), int(types[i]), i))
+    assert np.array_equal(order, np.array(ref, np.int32))
+    assert np.any(np.signbit(t) & (t == 0)) and np.any(~np.signbit(t) & (t == 0))

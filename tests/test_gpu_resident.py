@@ -85,7 +85,8 @@ def test_resident_and_batched_agree(ctx_factory):
     res = {}
     for solver in (native.SOLVER_AUTO, native.SOLVER_BATCHED):
         ctx.set_state(x0, v0)
-        stats, _ = ctx.step(params_for(scene, solver=solver))
+        # the same preconditioner on both routes: block-Jacobi, no coarse correction
+        stats, _ = ctx.step(params_for(scene, solver=solver, coarse=0))
         it, rr, fl = ctx.instance_stats()
         res[solver] = (ctx.get_dv().copy(), it.copy(), rr.copy(), fl.copy(), stats.loop_trips)
     dva, ita, rra, fla, tripa = res[native.SOLVER_AUTO]
@@ -105,7 +106,8 @@ def test_resident_plain_fp32_matches_batched_plain(ctx_factory):
     res = {}
     for solver in (native.SOLVER_AUTO, native.SOLVER_BATCHED):
         ctx.set_state(x0, v0)
-        ctx.step(params_for(scene, tol=1e-6, precision=native.PREC_PLAIN_FP32, solver=solver), allow_unconverged=True)
+        ctx.step(params_for(scene, tol=1e-6, precision=native.PREC_PLAIN_FP32, solver=solver, coarse=0),
+                 allow_unconverged=True)
         res[solver] = ctx.instance_stats()
     ita, rra, fla = res[native.SOLVER_AUTO]
     itb, rrb, flb = res[native.SOLVER_BATCHED]
