@@ -10,10 +10,10 @@
 // A_c = R A R^T.  Per step: A_c is summed from per-pair contributor lists (a fixed order, so
 // the result is deterministic) and inverted by Gauss-Jordan in FP32 -- one CTA with the matrix
 // in shared memory up to CS_BC_SMALL_NC unknowns, else a cluster of CS_BC_CLUSTER CTAs with its
-// rows spread over their shared memory and each pivot row broadcast through distributed shared
+// rows spread over their shared memory and each pivot row read through distributed shared
 // memory -- then symmetrised.  A_c is SPD (A is), so no pivoting is needed; a pivot that is not
 // positive disables the correction of that sheet for the step.  Per CG trip, after the vector
-// update: R r (a warp per aggregate), e_c = A_c^-1 R r (a warp per coarse row), then
+// update: R r (a block per aggregate), e_c = A_c^-1 R r (a warp per coarse row), then
 // z += R^T e_c with the r.z and r.r partials recomputed (a warp per 32 rows in natural order,
 // as cs_vector_kernel lays them out).  Sheets solved cluster-resident (their own coarse
 // correction, resident.cu) and sheets with proximities (blocks outside the pattern) skip it.
@@ -92,7 +92,8 @@ __global__ void __launch_bounds__(256) cs_bc_assemble_kernel(Batch B) {
 }
 
 // Gauss-Jordan inversion in place of an SPD matrix held by one CTA in shared memory (nc <=
-// CS_BC_SMALL_NC), a block per sheet; the inverse is written symmetrised.
+// CS_BC_SMALL_NC), a block per sheet; the inverse is written symmetrised.  Thread t updates
+// column t % nc of rows t / nc, t / nc + blockDim / nc, ... (no division in the loops).
 __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch B) {
     extern __shared__ float bc_sm[];
     __shared__ int bad;
@@ -108,6 +109,9 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
     const int n2 = nc * nc;
     for (int e = threadIdx.x; e < n2; e += blockDim.x) M[e] = G[e];
     if (threadIdx.x == 0) bad = 0;
+    // this thread's column and first row, and the row stride of the threads sharing a column
+    const int rs = blockDim.x / nc, j = threadIdx.x % nc, i0 = threadIdx.x / nc;
+    const bool active = i0 < rs;  // threads beyond rs * nc idle in the update
     __syncthreads();
     for (int k = 0; k < nc; k++) {
         const float p = M[k * nc + k];
@@ -116,18 +120,20 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
             break;
         }
         const float ip = 1.0f / p;
-        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
-            rowb[j] = j == k ? ip : M[k * nc + j] * ip;
-            colb[j] = M[j * nc + k];
+        for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+            rowb[q] = q == k ? ip : M[k * nc + q] * ip;
+            colb[q] = M[q * nc + k];
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < n2; e += blockDim.x) {
-            const int i = e / nc, j = e - i * nc;
-            float v;
-            if (i == k) v = rowb[j];
-            else if (j == k) v = -colb[i] * ip;
-            else v = __fmaf_rn(-colb[i], rowb[j], M[e]);
-            M[e] = v;
+        if (active) {
+            const float rj = rowb[j];
+            for (int i = i0; i < nc; i += rs) {
+                float v;
+                if (i == k) v = rj;
+                else if (j == k) v = -colb[i] * ip;
+                else v = __fmaf_rn(-colb[i], rj, M[i * nc + j]);
+                M[i * nc + j] = v;
+            }
         }
         __syncthreads();
     }
@@ -135,8 +141,8 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
     float* Inv = B.bc_inv + sh.bc_mat_off;
     if (!bad)
         for (int e = threadIdx.x; e < n2; e += blockDim.x) {
-            const int i = e / nc, j = e - i * nc;
-            Inv[e] = 0.5f * (M[e] + M[j * nc + i]);
+            const int i = e / nc, jj = e - i * nc;
+            Inv[e] = 0.5f * (M[e] + M[jj * nc + i]);
         }
     if (threadIdx.x == 0) B.bc_ok[s] = bad ? 0 : 1;
 }
@@ -144,10 +150,12 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
 // Gauss-Jordan inversion of a larger coarse matrix (CS_BC_SMALL_NC < nc <= CS_BC_MAX_NC) by a
 // cluster of CS_BC_CLUSTER CTAs, one cluster per sheet of B.bc_big: rank c holds rows
 // c, c + CS_BC_CLUSTER, ... in shared memory.  Per pivot k its owner writes the normalised row
-// (and a validity flag) into every CTA's pivot buffer (two buffers alternate), one cluster
-// barrier, then every CTA updates its rows.  A CTA reuses a buffer only after the barrier that
-// follows every CTA's last read of it, so one barrier per pivot suffices.  The raw inverse goes
-// back to bc_mat, then (after a barrier) each CTA writes its rows of the symmetrised inverse.
+// and a validity flag into its own pivot buffer (two alternate), one cluster barrier, then every
+// CTA reads the row from the owner's shared memory (distributed shared memory loads: each
+// thread the entries of its columns) and updates its rows, thread t column t, t + blockDim, ...
+// An owner rewrites a buffer only after the barrier that follows every CTA's last read of it,
+// so one barrier per pivot suffices.  The raw inverse goes back to bc_mat, then (after a
+// barrier) each CTA writes its rows of the symmetrised inverse.
 __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Batch B) {
     extern __shared__ float bc_sm[];
     __shared__ int bad;
@@ -170,37 +178,36 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
         M[e] = G[(size_t)(rank + CS_BC_CLUSTER * li) * nc + j];
     }
     if (threadIdx.x == 0) bad = 0;
-    cluster.sync();  // every CTA has started and loaded its rows before remote writes
+    cluster.sync();  // every CTA has started and loaded its rows before remote reads
     for (int k = 0; k < nc; k++) {
-        float* buf = pbuf + (k & 1) * (nc + 1);
-        if (rank == k % CS_BC_CLUSTER) {
+        const int owner = k % CS_BC_CLUSTER;
+        float* mine = pbuf + (k & 1) * (nc + 1);
+        if (rank == owner) {
             const int lk = k / CS_BC_CLUSTER;
             const float p = M[lk * nc + k];
             const bool ok = p > 0.f && isfinite(p);
             const float ip = ok ? 1.0f / p : 0.f;
-            for (int t = threadIdx.x; t < (nc + 1) * CS_BC_CLUSTER; t += blockDim.x) {
-                const int dst = t / (nc + 1), j = t - dst * (nc + 1);
-                const float v = j == nc ? (ok ? 1.f : 0.f) : (j == k ? ip : M[lk * nc + j] * ip);
-                float* rb = cluster.map_shared_rank(buf, dst);
-                rb[j] = v;
-            }
+            for (int j = threadIdx.x; j <= nc; j += blockDim.x)
+                mine[j] = j == nc ? (ok ? 1.f : 0.f) : (j == k ? ip : M[lk * nc + j] * ip);
         }
+        for (int li = threadIdx.x; li < R; li += blockDim.x) colb[li] = M[li * nc + k];
         cluster.sync();
-        if (buf[nc] == 0.f) {  // the same flag in every CTA: a uniform exit
+        const float* ob = cluster.map_shared_rank(mine, owner);
+        if (ob[nc] == 0.f) {  // the same flag in every CTA: a uniform exit
             if (threadIdx.x == 0) bad = 1;
             break;
         }
-        const float ip = buf[k];
-        for (int li = threadIdx.x; li < R; li += blockDim.x) colb[li] = M[li * nc + k];
-        __syncthreads();
-        for (int e = threadIdx.x; e < R * nc; e += blockDim.x) {
-            const int li = e / nc, j = e - li * nc;
-            const int i = rank + CS_BC_CLUSTER * li;
-            float v;
-            if (i == k) v = buf[j];
-            else if (j == k) v = -colb[li] * ip;
-            else v = __fmaf_rn(-colb[li], buf[j], M[e]);
-            M[e] = v;
+        const float ip = ob[k];
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+            const float bj = ob[j];
+            for (int li = 0; li < R; li++) {
+                const int i = rank + CS_BC_CLUSTER * li;
+                float v;
+                if (i == k) v = bj;
+                else if (j == k) v = -colb[li] * ip;
+                else v = __fmaf_rn(-colb[li], bj, M[li * nc + j]);
+                M[li * nc + j] = v;
+            }
         }
         __syncthreads();
     }
@@ -222,17 +229,18 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
     if (rank == 0 && threadIdx.x == 0) B.bc_ok[s] = bad ? 0 : 1;
 }
 
-// R r: a warp per aggregate sums r over its member nodes (ascending, lane-strided, then a
-// butterfly) in FP64, stored in FP32.
+// R r: a block per aggregate sums r over its member nodes (thread-strided over the ascending
+// members, then a fixed-order block sum) in FP64, stored in FP32.
 __global__ void __launch_bounds__(256) cs_bc_restrict_kernel(Batch B) {
-    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    __shared__ double sh3[3 * 8];
+    const int w = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (w >= B.bc_total_agg) return;
     const int2 sa = B.bc_agg[w];
     if (!bc_trip_on(B, sa.x)) return;
     const SheetDesc& sh = B.sheets[sa.x];
     const int m0 = B.bc_mptr[sh.bc_agg_off + sa.y], m1 = B.bc_mptr[sh.bc_agg_off + sa.y + 1];
     double r0 = 0.0, r1 = 0.0, r2 = 0.0;
-    for (int m = m0 + lane; m < m1; m += 32) {
+    for (int m = m0 + (int)threadIdx.x; m < m1; m += blockDim.x) {
         const int node = sh.node_off + B.bc_mem[sh.bc_mem_off + m];
         r0 += (double)B.r[3 * node];
         r1 += (double)B.r[3 * node + 1];
@@ -242,10 +250,15 @@ __global__ void __launch_bounds__(256) cs_bc_restrict_kernel(Batch B) {
     r1 = bc_warp_sum(r1);
     r2 = bc_warp_sum(r2);
     if (lane == 0) {
-        float* rc = B.bc_rc + sh.bc_vec_off + 3 * sa.y;
-        rc[0] = (float)r0;
-        rc[1] = (float)r1;
-        rc[2] = (float)r2;
+        sh3[3 * wid] = r0;
+        sh3[3 * wid + 1] = r1;
+        sh3[3 * wid + 2] = r2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += sh3[3 * q + threadIdx.x];
+        B.bc_rc[sh.bc_vec_off + 3 * sa.y + threadIdx.x] = (float)t;
     }
 }
 

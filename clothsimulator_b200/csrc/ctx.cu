@@ -1098,7 +1098,7 @@ void launchTrip(cs_ctx* c, cudaGraphConditionalHandle h) {
     cs_vector_kernel<<<g, 128, 0, c->stream>>>(B);
     if (B.bc_total_agg > 0) {
         // the coarse correction of z and the r.z, r.r partials it changes (coarse.cu)
-        cs_bc_restrict_kernel<<<nblk((long long)B.bc_total_agg * 32, 256), 256, 0, c->stream>>>(B);
+        cs_bc_restrict_kernel<<<B.bc_total_agg, 256, 0, c->stream>>>(B);
         cs_bc_apply_kernel<<<nblk((long long)B.bc_total_agg * 96, 256), 256, 0, c->stream>>>(B);
         cs_bc_finish_kernel<<<g, 128, 0, c->stream>>>(B);
     }
@@ -2780,6 +2780,31 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
         }
         ms[7] = acc / reps;
         ms[8] = accSetup / reps;
+    }
+    // the batched loop's coarse correction (coarse.cu): its per-step set-up for the sheets the
+    // loop solves, and one trip's kernels (R r, A_c^-1 R r, z += R^T e_c with the partials)
+    ms[9] = ms[10] = 0.f;
+    if (B.bc_total_agg > 0 && p->coarse) {
+        cs_slice_bnorm_kernel<<<nblk((long long)B.n_slices * 32, 128), 128, 0, c->stream>>>(B);
+        cs_solve_setup_kernel<<<B.S, 128, 0, c->stream>>>(B);
+        float t = 0.f;
+        cudaEventRecord(c->ev0, c->stream);
+        for (int r = 0; r < reps; r++) launchBatchedCoarseSetup(c);
+        cudaEventRecord(c->ev1, c->stream);
+        cudaEventSynchronize(c->ev1);
+        cudaEventElapsedTime(&t, c->ev0, c->ev1);
+        ms[9] = t / reps;
+        cs_solve_prologue_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B);
+        cudaEventRecord(c->ev0, c->stream);
+        for (int r = 0; r < reps; r++) {
+            cs_bc_restrict_kernel<<<B.bc_total_agg, 256, 0, c->stream>>>(B);
+            cs_bc_apply_kernel<<<nblk((long long)B.bc_total_agg * 96, 256), 256, 0, c->stream>>>(B);
+            cs_bc_finish_kernel<<<g, 128, 0, c->stream>>>(B);
+        }
+        cudaEventRecord(c->ev1, c->stream);
+        cudaEventSynchronize(c->ev1);
+        cudaEventElapsedTime(&t, c->ev0, c->ev1);
+        ms[10] = t / reps;
     }
     CS_CUDA(cudaGetLastError());
     CS_CUDA(cudaStreamSynchronize(c->stream));

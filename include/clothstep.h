@@ -336,8 +336,11 @@ cs_status cs_device_pointers(cs_ctx* ctx, float** x, float** v, float** dv);
  * [3] SpMV of a CG iteration, [4] vector update of a CG iteration, [5] per-instance reduction,
  * [6] FP64 residual SpMV, [7] one cluster-resident solve of all resident sheets (0 if none;
  * when every sheet is resident, cs_get_instance_stats then reports that solve), [8] the set-up
- * of its coarse-space correction (forming and inverting the coarse matrices; 0 without it); ms
- * holds 9 floats.  Overwrites the solver's scratch vectors and dv64 (not x, v or dv). */
+ * of its coarse-space correction (forming and inverting the coarse matrices; 0 without it),
+ * [9] the batched loop's coarse set-up for the sheets the loop solves (forming and inverting
+ * their coarse matrices), [10] one loop trip's coarse-correction kernels (0 without the
+ * correction); ms holds 11 floats.  Overwrites the solver's scratch vectors and dv64 (not x, v
+ * or dv). */
 cs_status cs_profile_kernels(cs_ctx* ctx, const cs_step_params* params, int reps, float* ms);
 /* Cumulative counts since cs_load_batch: [0] steps, [1] solve-loop trips, [2] kernel launches. */
 cs_status cs_get_counters(cs_ctx* ctx, long long* counters);
