@@ -23,6 +23,8 @@
 
 namespace cg = cooperative_groups;
 
+static_assert(CS_BC_MAX_NC <= 2 * CS_BC_THREADS, "a thread of the cluster inversion updates at most two columns");
+
 namespace {
 
 template <class T>
@@ -192,14 +194,21 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
         }
         for (int li = threadIdx.x; li < R; li += blockDim.x) colb[li] = M[li * nc + k];
         cluster.sync();
+        // this thread's remote loads issued together: the flag, 1/p, the entries of its columns
+        // (at most two: nc <= CS_BC_MAX_NC <= 2 x CS_BC_THREADS)
         const float* ob = cluster.map_shared_rank(mine, owner);
-        if (ob[nc] == 0.f) {  // the same flag in every CTA: a uniform exit
+        const int j0 = threadIdx.x, j1 = threadIdx.x + blockDim.x;
+        const float flag = ob[nc], ip = ob[k];
+        const float b0 = j0 < nc ? ob[j0] : 0.f, b1 = j1 < nc ? ob[j1] : 0.f;
+        if (flag == 0.f) {  // the same flag in every CTA: a uniform exit
             if (threadIdx.x == 0) bad = 1;
             break;
         }
-        const float ip = ob[k];
-        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
-            const float bj = ob[j];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int j = h ? j1 : j0;
+            const float bj = h ? b1 : b0;
+            if (j >= nc) continue;
             for (int li = 0; li < R; li++) {
                 const int i = rank + CS_BC_CLUSTER * li;
                 float v;
