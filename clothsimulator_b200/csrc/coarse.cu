@@ -11,8 +11,9 @@
 // the result is deterministic) and inverted by Gauss-Jordan in FP32 -- one CTA with the matrix
 // in shared memory up to CS_BC_SMALL_NC unknowns, else a cluster of CS_BC_CLUSTER CTAs with its
 // rows spread over their shared memory and each pivot row read through distributed shared
-// memory -- then symmetrised.  A_c is SPD (A is), so no pivoting is needed; a pivot that is not
-// positive disables the correction of that sheet for the step.  Per CG trip, after the vector
+// memory -- then symmetrised.  A_c is SPD (A is), so no pivoting is needed; the pivots are the
+// aggregates' 3x3 diagonal blocks, and one that is not positive definite disables the sheet's
+// correction for the step.  Per CG trip, after the vector
 // update: R r (a block per aggregate), e_c = A_c^-1 R r (a warp per coarse row), then
 // z += R^T e_c with the r.z and r.r partials recomputed (a warp per 32 rows in natural order,
 // as cs_vector_kernel lays them out).  Sheets solved cluster-resident (their own coarse
@@ -93,9 +94,31 @@ __global__ void __launch_bounds__(256) cs_bc_assemble_kernel(Batch B) {
     }
 }
 
-// Gauss-Jordan inversion in place of an SPD matrix held by one CTA in shared memory (nc <=
-// CS_BC_SMALL_NC), a block per sheet; the inverse is written symmetrised.  Thread t updates
-// column t % nc of rows t / nc, t / nc + blockDim / nc, ... (no division in the loops).
+// Inverse of a 3x3 block (row-major) by its adjugate; false unless it is positive definite
+// enough to pivot on (positive leading entry and determinant, finite).
+__device__ __forceinline__ bool bc_inv3(const float (&a)[9], float (&r)[9]) {
+    const float c0 = a[4] * a[8] - a[5] * a[7], c1 = a[5] * a[6] - a[3] * a[8], c2 = a[3] * a[7] - a[4] * a[6];
+    const float det = a[0] * c0 + a[1] * c1 + a[2] * c2;
+    if (!(a[0] > 0.f) || !(det > 0.f) || !isfinite(det)) return false;
+    const float id = 1.0f / det;
+    r[0] = c0 * id;
+    r[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    r[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    r[3] = c1 * id;
+    r[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    r[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    r[6] = c2 * id;
+    r[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    r[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+    return true;
+}
+
+// Gauss-Jordan inversion in place with 3x3 pivot blocks (one per aggregate: a third of the
+// barriers of scalar pivots) of an SPD matrix held by one CTA in shared memory (nc <=
+// CS_BC_SMALL_NC), a block per sheet; the inverse is written symmetrised.  Per pivot block K:
+// U = D^-1 A[K, :] (D = A[K, K]), then every row i outside K gets A[i, :] -= A[i, K] U and
+// A[i, K] = -A[i, K] D^-1, and rows K become U.  Thread t updates column t % nc of rows
+// t / nc, t / nc + blockDim / nc, ... (no division in the loops).
 __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch B) {
     extern __shared__ float bc_sm[];
     __shared__ int bad;
@@ -105,35 +128,47 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
     const int nc = 3 * sh.bc_na;
     if (nc > CS_BC_SMALL_NC) return;
     float* M = bc_sm;
-    float* rowb = bc_sm + nc * nc;
-    float* colb = rowb + nc;
+    float* rowb = bc_sm + nc * nc;  // 3 x nc: U
+    float* colb = rowb + 3 * nc;    // 3 x nc: column t of K over all rows
     const float* G = B.bc_mat + sh.bc_mat_off;
     const int n2 = nc * nc;
     for (int e = threadIdx.x; e < n2; e += blockDim.x) M[e] = G[e];
     if (threadIdx.x == 0) bad = 0;
-    // this thread's column and first row, and the row stride of the threads sharing a column
     const int rs = blockDim.x / nc, j = threadIdx.x % nc, i0 = threadIdx.x / nc;
     const bool active = i0 < rs;  // threads beyond rs * nc idle in the update
     __syncthreads();
-    for (int k = 0; k < nc; k++) {
-        const float p = M[k * nc + k];
-        if (!(p > 0.f) || !isfinite(p)) {  // the same value in every thread: a uniform exit
+    for (int k0 = 0; k0 < nc; k0 += 3) {
+        float d[9], di[9];
+#pragma unroll
+        for (int q = 0; q < 9; q++) d[q] = M[(k0 + q / 3) * nc + k0 + q % 3];
+        if (!bc_inv3(d, di)) {  // the same values in every thread: a uniform exit
             if (threadIdx.x == 0) bad = 1;
             break;
         }
-        const float ip = 1.0f / p;
         for (int q = threadIdx.x; q < nc; q += blockDim.x) {
-            rowb[q] = q == k ? ip : M[k * nc + q] * ip;
-            colb[q] = M[q * nc + k];
+            const int c = q - k0;  // column of K, or outside 0..2
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const float dk = c == 0 ? di[3 * r] : c == 1 ? di[3 * r + 1] : di[3 * r + 2];
+                const float u = (c >= 0 && c < 3)
+                                    ? dk
+                                    : di[3 * r] * M[k0 * nc + q] + di[3 * r + 1] * M[(k0 + 1) * nc + q] +
+                                          di[3 * r + 2] * M[(k0 + 2) * nc + q];
+                rowb[r * nc + q] = u;
+                colb[r * nc + q] = M[q * nc + k0 + r];
+            }
         }
         __syncthreads();
         if (active) {
-            const float rj = rowb[j];
+            const float u0 = rowb[j], u1 = rowb[nc + j], u2 = rowb[2 * nc + j];
+            const bool jk = j >= k0 && j < k0 + 3;
             for (int i = i0; i < nc; i += rs) {
                 float v;
-                if (i == k) v = rj;
-                else if (j == k) v = -colb[i] * ip;
-                else v = __fmaf_rn(-colb[i], rj, M[i * nc + j]);
+                if (i >= k0 && i < k0 + 3) v = rowb[(i - k0) * nc + j];
+                else {
+                    const float t = colb[i] * u0 + colb[nc + i] * u1 + colb[2 * nc + i] * u2;
+                    v = jk ? -t : M[i * nc + j] - t;
+                }
                 M[i * nc + j] = v;
             }
         }
@@ -149,15 +184,15 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
     if (threadIdx.x == 0) B.bc_ok[s] = bad ? 0 : 1;
 }
 
-// Gauss-Jordan inversion of a larger coarse matrix (CS_BC_SMALL_NC < nc <= CS_BC_MAX_NC) by a
-// cluster of CS_BC_CLUSTER CTAs, one cluster per sheet of B.bc_big: rank c holds rows
-// c, c + CS_BC_CLUSTER, ... in shared memory.  Per pivot k its owner writes the normalised row
-// and a validity flag into its own pivot buffer (two alternate), one cluster barrier, then every
-// CTA reads the row from the owner's shared memory (distributed shared memory loads: each
-// thread the entries of its columns) and updates its rows, thread t column t, t + blockDim, ...
-// An owner rewrites a buffer only after the barrier that follows every CTA's last read of it,
-// so one barrier per pivot suffices.  The raw inverse goes back to bc_mat, then (after a
-// barrier) each CTA writes its rows of the symmetrised inverse.
+// The same inversion of a larger coarse matrix (CS_BC_SMALL_NC < nc <= CS_BC_MAX_NC) by a
+// cluster of CS_BC_CLUSTER CTAs, one cluster per sheet of B.bc_big: rank c holds the rows of
+// aggregates c, c + CS_BC_CLUSTER, ... in shared memory.  Per pivot block (aggregate) its owner
+// writes U = D^-1 A[K, :] and a validity flag into its own pivot buffer (two alternate), one
+// cluster barrier, then every CTA reads the entries of its columns from the owner's shared
+// memory (distributed shared memory loads, issued together) and updates its rows, thread t
+// columns t and t + blockDim.  An owner rewrites a buffer only after the barrier that follows
+// every CTA's last read of it, so one barrier per pivot block suffices.  The raw inverse goes
+// back to bc_mat, then (after a barrier) each CTA writes its rows of the symmetrised inverse.
 __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Batch B) {
     extern __shared__ float bc_sm[];
     __shared__ int bad;
@@ -167,39 +202,61 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
     // the same decision in every CTA of the cluster: all return, or none
     if (!bc_sheet_on(B, s) || B.inst[s].phase == PH_RESIDENT) return;
     const SheetDesc& sh = B.sheets[s];
-    const int nc = 3 * sh.bc_na;
+    const int na = sh.bc_na, nc = 3 * na;
     if (nc <= CS_BC_SMALL_NC || nc > CS_BC_MAX_NC) return;
-    const int RM = (nc + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER;
-    const int R = (nc - rank + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER;  // rows rank + CS_BC_CLUSTER * li
-    float* M = bc_sm;                    // RM x nc
-    float* pbuf = bc_sm + RM * nc;       // 2 x (nc + 1): pivot row, then the validity flag
-    float* colb = pbuf + 2 * (nc + 1);   // RM
+    const int RM = 3 * ((na + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER);
+    const int R = 3 * ((na - rank + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER);  // local row li: aggregate rank + 16 (li / 3)
+    float* M = bc_sm;                        // RM x nc
+    float* pbuf = bc_sm + RM * nc;           // 2 x (3 nc + 1): U, then the validity flag
+    float* colb = pbuf + 2 * (3 * nc + 1);   // 3 x RM
     float* G = B.bc_mat + sh.bc_mat_off;
+    auto grow = [&](int li) { return 3 * (rank + CS_BC_CLUSTER * (li / 3)) + li % 3; };
     for (int e = threadIdx.x; e < R * nc; e += blockDim.x) {
         const int li = e / nc, j = e - li * nc;
-        M[e] = G[(size_t)(rank + CS_BC_CLUSTER * li) * nc + j];
+        M[e] = G[(size_t)grow(li) * nc + j];
     }
     if (threadIdx.x == 0) bad = 0;
     cluster.sync();  // every CTA has started and loaded its rows before remote reads
-    for (int k = 0; k < nc; k++) {
-        const int owner = k % CS_BC_CLUSTER;
-        float* mine = pbuf + (k & 1) * (nc + 1);
+    for (int kb = 0; kb < na; kb++) {
+        const int owner = kb % CS_BC_CLUSTER, k0 = 3 * kb;
+        float* mine = pbuf + (kb & 1) * (3 * nc + 1);
         if (rank == owner) {
-            const int lk = k / CS_BC_CLUSTER;
-            const float p = M[lk * nc + k];
-            const bool ok = p > 0.f && isfinite(p);
-            const float ip = ok ? 1.0f / p : 0.f;
-            for (int j = threadIdx.x; j <= nc; j += blockDim.x)
-                mine[j] = j == nc ? (ok ? 1.f : 0.f) : (j == k ? ip : M[lk * nc + j] * ip);
+            const int l0 = 3 * (kb / CS_BC_CLUSTER);
+            float d[9], di[9];
+#pragma unroll
+            for (int q = 0; q < 9; q++) d[q] = M[(l0 + q / 3) * nc + k0 + q % 3];
+            const bool ok = bc_inv3(d, di);
+            for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+                const int c = q - k0;  // column of K, or outside 0..2
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    const float dk = c == 0 ? di[3 * r] : c == 1 ? di[3 * r + 1] : di[3 * r + 2];
+                    mine[r * nc + q] = !ok ? 0.f
+                                       : (c >= 0 && c < 3)
+                                           ? dk
+                                           : di[3 * r] * M[l0 * nc + q] + di[3 * r + 1] * M[(l0 + 1) * nc + q] +
+                                                 di[3 * r + 2] * M[(l0 + 2) * nc + q];
+                }
+            }
+            if (threadIdx.x == 0) mine[3 * nc] = ok ? 1.f : 0.f;
         }
-        for (int li = threadIdx.x; li < R; li += blockDim.x) colb[li] = M[li * nc + k];
+        for (int li = threadIdx.x; li < R; li += blockDim.x) {
+#pragma unroll
+            for (int r = 0; r < 3; r++) colb[r * RM + li] = M[li * nc + k0 + r];
+        }
         cluster.sync();
-        // this thread's remote loads issued together: the flag, 1/p, the entries of its columns
+        // this thread's remote loads issued together: the flag and U's entries of its columns
         // (at most two: nc <= CS_BC_MAX_NC <= 2 x CS_BC_THREADS)
         const float* ob = cluster.map_shared_rank(mine, owner);
         const int j0 = threadIdx.x, j1 = threadIdx.x + blockDim.x;
-        const float flag = ob[nc], ip = ob[k];
-        const float b0 = j0 < nc ? ob[j0] : 0.f, b1 = j1 < nc ? ob[j1] : 0.f;
+        const float flag = ob[3 * nc];
+        float u[2][3];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int j = h ? j1 : j0;
+#pragma unroll
+            for (int r = 0; r < 3; r++) u[h][r] = j < nc ? ob[r * nc + j] : 0.f;
+        }
         if (flag == 0.f) {  // the same flag in every CTA: a uniform exit
             if (threadIdx.x == 0) bad = 1;
             break;
@@ -207,14 +264,16 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int j = h ? j1 : j0;
-            const float bj = h ? b1 : b0;
             if (j >= nc) continue;
+            const bool jk = j >= k0 && j < k0 + 3;
             for (int li = 0; li < R; li++) {
-                const int i = rank + CS_BC_CLUSTER * li;
+                const int i = grow(li);
                 float v;
-                if (i == k) v = bj;
-                else if (j == k) v = -colb[li] * ip;
-                else v = __fmaf_rn(-colb[li], bj, M[li * nc + j]);
+                if (i >= k0 && i < k0 + 3) v = i == k0 ? u[h][0] : i == k0 + 1 ? u[h][1] : u[h][2];
+                else {
+                    const float t = colb[li] * u[h][0] + colb[RM + li] * u[h][1] + colb[2 * RM + li] * u[h][2];
+                    v = jk ? -t : M[li * nc + j] - t;
+                }
                 M[li * nc + j] = v;
             }
         }
@@ -224,7 +283,7 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
     if (!bad)
         for (int e = threadIdx.x; e < R * nc; e += blockDim.x) {
             const int li = e / nc, j = e - li * nc;
-            G[(size_t)(rank + CS_BC_CLUSTER * li) * nc + j] = M[e];
+            G[(size_t)grow(li) * nc + j] = M[e];
         }
     __threadfence();
     cluster.sync();
@@ -232,7 +291,7 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
     if (!bad)
         for (int e = threadIdx.x; e < R * nc; e += blockDim.x) {
             const int li = e / nc, j = e - li * nc;
-            const int i = rank + CS_BC_CLUSTER * li;
+            const int i = grow(li);
             Inv[(size_t)i * nc + j] = 0.5f * (M[e] + __ldcg(&G[(size_t)j * nc + i]));
         }
     if (rank == 0 && threadIdx.x == 0) B.bc_ok[s] = bad ? 0 : 1;
