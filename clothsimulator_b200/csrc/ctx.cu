@@ -855,9 +855,13 @@ struct cs_ctx {
     std::vector<SliceDesc> slices;
     std::vector<std::shared_ptr<Topo>> sheetTopo;
     long long nnzb_pattern = 0;
-    // graph
-    cudaGraphExec_t graphExec = nullptr;
-    cudaGraph_t graph = nullptr;
+    // graphs of the step, per [learned warm start][coarse-correction kernels in the loop trips]
+    cudaGraphExec_t gexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaGraph_t gph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    // launchTrip launches the batched coarse correction's kernels (the step asks for it); the
+    // launch counter's trips before the last change of this setting and their kernels
+    bool tripCoarse = true;
+    long long tripsBase = 0, tripLaunchBase = 0;
     DevParams hostParams{};
     bool lastStepValid = false;
     long long steps = 0, hostLaunches = 0, graphSteps = 0, graphLaunchesFixed = 0;
@@ -869,8 +873,6 @@ struct cs_ctx {
     int mlpGridL1 = 0, mlpGridL23 = 0;  // inference grids: resident CTAs per SM (TMEM: 512 columns per SM)
     long long adamStep = 0;
     float* mlpScratch = nullptr;  // per-epoch loss accumulators, gradient output
-    cudaGraphExec_t graphExecLearned = nullptr;
-    cudaGraph_t graphLearned = nullptr;
     // cluster-resident solver launch (resident.cu): CTAs per cluster, threads per CTA,
     // clusters in the persistent grid, dynamic shared memory per CTA
     int resCL = 0, resThreads = 0, resClusters = 0, resClustersMax = 0;
@@ -942,14 +944,15 @@ void freeBatch(cs_ctx* c) {
     c->tunedDegree = c->tunedCoarse = 0;
     c->handleNode.clear();
     c->maxHandleMotion = -1;
-    if (c->graphExec) cudaGraphExecDestroy(c->graphExec);
-    if (c->graph) cudaGraphDestroy(c->graph);
-    if (c->graphExecLearned) cudaGraphExecDestroy(c->graphExecLearned);
-    if (c->graphLearned) cudaGraphDestroy(c->graphLearned);
-    c->graphExec = nullptr;
-    c->graph = nullptr;
-    c->graphExecLearned = nullptr;
-    c->graphLearned = nullptr;
+    for (int l = 0; l < 2; l++)
+        for (int k = 0; k < 2; k++) {
+            if (c->gexec[l][k]) cudaGraphExecDestroy(c->gexec[l][k]);
+            if (c->gph[l][k]) cudaGraphDestroy(c->gph[l][k]);
+            c->gexec[l][k] = nullptr;
+            c->gph[l][k] = nullptr;
+        }
+    c->tripCoarse = true;
+    c->tripsBase = c->tripLaunchBase = 0;
     c->mlp = MlpDev();
     c->mlpInit = false;
     c->adamStep = 0;
@@ -1035,7 +1038,22 @@ int bcSetupKernels(const cs_ctx* c) { return c->B.bc_total_agg > 0 ? 2 + (c->B.b
 int residentKernels(const cs_ctx* c) {
     return c->resClusters > 0 ? 1 + (c->B.res_cnc > 0 && c->B.n_resident > 0 ? 1 : 0) : 0;
 }
-int tripKernels(const cs_ctx* c) { return 4 + (c->B.bc_total_agg > 0 ? 3 : 0); }
+int tripKernels(const cs_ctx* c) { return 4 + (c->B.bc_total_agg > 0 && c->tripCoarse ? 3 : 0); }
+
+// Whether the loop trips launch the batched coarse correction's kernels (only when the step asks
+// for the correction: without it they would only return); the launch counter folds the trips
+// so far at the old setting.
+cs_status setTripCoarse(cs_ctx* c, bool on) {
+    if (c->tripCoarse == on) return CS_OK;
+    int loopv[8];
+    CS_CUDA(cudaMemcpyAsync(loopv, c->B.loop, sizeof(loopv), cudaMemcpyDeviceToHost, c->stream));
+    CS_CUDA(cudaStreamSynchronize(c->stream));
+    const long long trips = (long long)(unsigned)loopv[4];
+    c->tripLaunchBase += (long long)tripKernels(c) * (trips - c->tripsBase);
+    c->tripsBase = trips;
+    c->tripCoarse = on;
+    return CS_OK;
+}
 
 void launchSolvePrologue(cs_ctx* c) {
     Batch& B = c->B;
@@ -1096,7 +1114,7 @@ void launchTrip(cs_ctx* c, cudaGraphConditionalHandle h) {
     launchSpmvShape(B, c->spmvShape, c->stream);
     cs_reduce1_kernel<<<B.S, CS_REDUCE_THREADS, 0, c->stream>>>(B);
     cs_vector_kernel<<<g, 128, 0, c->stream>>>(B);
-    if (B.bc_total_agg > 0) {
+    if (B.bc_total_agg > 0 && c->tripCoarse) {
         // the coarse correction of z and the r.z, r.r partials it changes (coarse.cu)
         cs_bc_restrict_kernel<<<B.bc_total_agg, 256, 0, c->stream>>>(B);
         cs_bc_apply_kernel<<<nblk((long long)B.bc_total_agg * 96, 256), 256, 0, c->stream>>>(B);
@@ -1106,11 +1124,11 @@ void launchTrip(cs_ctx* c, cudaGraphConditionalHandle h) {
 }
 
 cs_status buildGraph(cs_ctx* c, bool learned) {
-    cudaGraphExec_t& exec = learned ? c->graphExecLearned : c->graphExec;
+    cudaGraphExec_t& exec = c->gexec[learned][c->tripCoarse];
     if (exec) return CS_OK;
     cudaGraph_t graph;
     CS_CUDA(cudaGraphCreate(&graph, 0));
-    (learned ? c->graphLearned : c->graph) = graph;
+    c->gph[learned][c->tripCoarse] = graph;
     // prelude: assembly (+ learned warm start) + solve setup, captured into the graph
     CS_CUDA(cudaStreamBeginCaptureToGraph(c->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     launchAssembly(c);
@@ -1848,14 +1866,13 @@ cs_status cs_set_state(cs_ctx* c, const float* x, const float* v) {
 namespace {
 
 void destroyGraphs(cs_ctx* c) {
-    if (c->graphExec) cudaGraphExecDestroy(c->graphExec);
-    if (c->graph) cudaGraphDestroy(c->graph);
-    if (c->graphExecLearned) cudaGraphExecDestroy(c->graphExecLearned);
-    if (c->graphLearned) cudaGraphDestroy(c->graphLearned);
-    c->graphExec = nullptr;
-    c->graph = nullptr;
-    c->graphExecLearned = nullptr;
-    c->graphLearned = nullptr;
+    for (int l = 0; l < 2; l++)
+        for (int k = 0; k < 2; k++) {
+            if (c->gexec[l][k]) cudaGraphExecDestroy(c->gexec[l][k]);
+            if (c->gph[l][k]) cudaGraphDestroy(c->gph[l][k]);
+            c->gexec[l][k] = nullptr;
+            c->gph[l][k] = nullptr;
+        }
 }
 
 template <class T>
@@ -2548,11 +2565,12 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
     DevParams d = toDev(p);
     c->hostParams = d;
     CS_CUDA(cudaMemcpyAsync(c->B.params, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
+    if ((st = setTripCoarse(c, p->coarse != 0)) != CS_OK) return st;
     CS_CUDA(cudaEventRecord(c->ev0, c->stream));
     const bool learned = p->warm_start == CS_WARM_LEARNED;
     if (p->use_graph) {
         if ((st = buildGraph(c, learned)) != CS_OK) return st;
-        CS_CUDA(cudaGraphLaunch(learned ? c->graphExecLearned : c->graphExec, c->stream));
+        CS_CUDA(cudaGraphLaunch(c->gexec[learned][c->tripCoarse], c->stream));
     } else {
         c->hostLaunches += launchAssembly(c) + 3 + bcSetupKernels(c) + residentKernels(c);
         if (learned) c->hostLaunches += launchMlpInference(c, c->B.warm);
@@ -2757,30 +2775,6 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
     ms[5] = timeIt(5);
     cs_profile_setup_kernel<<<nblk(B.S, 128), 128, 0, c->stream>>>(B, PH_RES);
     ms[6] = timeIt(6);
-    // one whole cluster-resident solve of every resident sheet from the zero guess (or the
-    // warm start the parameters ask for); set-up launches untimed, the solve between events
-    ms[7] = ms[8] = 0.f;
-    if (c->resClusters > 0) {
-        float acc = 0.f, accSetup = 0.f;
-        for (int r = 0; r < reps; r++) {
-            launchSolvePrologueAgain(c);
-            cudaEventRecord(c->ev0, c->stream);
-            launchCoarseSetup(c);
-            cudaEventRecord(c->ev1, c->stream);
-            cudaEventSynchronize(c->ev1);
-            float t = 0.f;
-            cudaEventElapsedTime(&t, c->ev0, c->ev1);
-            accSetup += t;
-            cudaEventRecord(c->ev0, c->stream);
-            launchResident(c, false);
-            cudaEventRecord(c->ev1, c->stream);
-            cudaEventSynchronize(c->ev1);
-            cudaEventElapsedTime(&t, c->ev0, c->ev1);
-            acc += t;
-        }
-        ms[7] = acc / reps;
-        ms[8] = accSetup / reps;
-    }
     // the batched loop's coarse correction (coarse.cu): its per-step set-up for the sheets the
     // loop solves, and one trip's kernels (R r, A_c^-1 R r, z += R^T e_c with the partials)
     ms[9] = ms[10] = 0.f;
@@ -2806,6 +2800,31 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
         cudaEventElapsedTime(&t, c->ev0, c->ev1);
         ms[10] = t / reps;
     }
+    // one whole cluster-resident solve of every resident sheet from the zero guess (or the
+    // warm start the parameters ask for); set-up launches untimed, the solve between events
+    ms[7] = ms[8] = 0.f;
+    if (c->resClusters > 0) {
+        float acc = 0.f, accSetup = 0.f;
+        for (int r = 0; r < reps; r++) {
+            launchSolvePrologueAgain(c);
+            cudaEventRecord(c->ev0, c->stream);
+            launchCoarseSetup(c);
+            cudaEventRecord(c->ev1, c->stream);
+            cudaEventSynchronize(c->ev1);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, c->ev0, c->ev1);
+            accSetup += t;
+            cudaEventRecord(c->ev0, c->stream);
+            launchResident(c, false);
+            cudaEventRecord(c->ev1, c->stream);
+            cudaEventSynchronize(c->ev1);
+            cudaEventElapsedTime(&t, c->ev0, c->ev1);
+            acc += t;
+        }
+        ms[7] = acc / reps;
+        ms[8] = accSetup / reps;
+    }
+
     CS_CUDA(cudaGetLastError());
     CS_CUDA(cudaStreamSynchronize(c->stream));
     // the per-sheet statistics of the last timed resident solve stay readable when it solved
@@ -2835,6 +2854,7 @@ __global__ void cs_checksum_kernel(const uint32_t* __restrict__ w, long long n, 
 static float timeWholeSolve(cs_ctx* c, const cs_step_params& q) {
     Batch& B = c->B;
     DevParams d = toDev(&q);
+    if (setTripCoarse(c, q.coarse != 0) != CS_OK) return -1.f;
     if (cudaMemcpyAsync(B.params, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream) != cudaSuccess) return -1.f;
     launchSolvePrologueAgain(c);
     cudaEventRecord(c->ev0, c->stream);
@@ -3016,7 +3036,7 @@ cs_status cs_get_counters(cs_ctx* c, long long* out) {
     out[0] = c->steps;
     out[1] = trips;
     // graph steps: fixed kernels plus those of every loop trip; host-driven steps are counted directly
-    out[2] = c->hostLaunches + c->graphLaunchesFixed + tripKernels(c) * trips;
+    out[2] = c->hostLaunches + c->graphLaunchesFixed + c->tripLaunchBase + tripKernels(c) * (trips - c->tripsBase);
     return CS_OK;
 }
 
@@ -3096,6 +3116,7 @@ cs_status mlpEnergyPrepare(cs_ctx* c, const cs_step_params* p) {
     Batch& B = c->B;
     MlpDev& M = c->mlp;
     DevParams d = toDev(p);
+    if ((st = setTripCoarse(c, p->coarse != 0)) != CS_OK) return st;
     CS_CUDA(cudaMemcpyAsync(B.params, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
     launchAssembly(c);
     cs_mlp_features_kernel<<<nblk(B.N, 256), 256, 0, c->stream>>>(B, M, M.feat);
