@@ -188,9 +188,9 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
 // cluster of CS_BC_CLUSTER CTAs, one cluster per sheet of B.bc_big: rank c holds the rows of
 // aggregates c, c + CS_BC_CLUSTER, ... in shared memory.  Per pivot block (aggregate) its owner
 // writes U = D^-1 A[K, :] and a validity flag into its own pivot buffer (two alternate), one
-// cluster barrier, then every CTA reads the entries of its columns from the owner's shared
-// memory (distributed shared memory loads, issued together) and updates its rows, thread t
-// columns t and t + blockDim.  An owner rewrites a buffer only after the barrier that follows
+// cluster barrier, then every CTA copies it from the owner's shared memory into its own
+// (16-byte distributed shared memory loads) and updates its rows, thread t columns t and
+// t + blockDim.  An owner rewrites a buffer only after the barrier that follows
 // every CTA's last read of it, so one barrier per pivot block suffices.  The raw inverse goes
 // back to bc_mat, then (after a barrier) each CTA writes its rows of the symmetrised inverse.
 __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Batch B) {
@@ -206,9 +206,11 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
     if (nc <= CS_BC_SMALL_NC || nc > CS_BC_MAX_NC) return;
     const int RM = 3 * ((na + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER);
     const int R = 3 * ((na - rank + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER);  // local row li: aggregate rank + 16 (li / 3)
+    const int UB = (3 * nc + 1 + 3) & ~3;    // a pivot buffer: U, the validity flag, padded to 16 bytes
     float* M = bc_sm;                        // RM x nc
-    float* pbuf = bc_sm + RM * nc;           // 2 x (3 nc + 1): U, then the validity flag
-    float* colb = pbuf + 2 * (3 * nc + 1);   // 3 x RM
+    float* pbuf = bc_sm + ((RM * nc + 3) & ~3);  // 2 x UB, 16-byte aligned
+    float* lbuf = pbuf + 2 * UB;             // UB: this CTA's copy of the current pivot buffer
+    float* colb = lbuf + UB;                 // 3 x RM
     float* G = B.bc_mat + sh.bc_mat_off;
     auto grow = [&](int li) { return 3 * (rank + CS_BC_CLUSTER * (li / 3)) + li % 3; };
     for (int e = threadIdx.x; e < R * nc; e += blockDim.x) {
@@ -219,7 +221,7 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
     cluster.sync();  // every CTA has started and loaded its rows before remote reads
     for (int kb = 0; kb < na; kb++) {
         const int owner = kb % CS_BC_CLUSTER, k0 = 3 * kb;
-        float* mine = pbuf + (kb & 1) * (3 * nc + 1);
+        float* mine = pbuf + (kb & 1) * UB;
         if (rank == owner) {
             const int l0 = 3 * (kb / CS_BC_CLUSTER);
             float d[9], di[9];
@@ -245,17 +247,23 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
             for (int r = 0; r < 3; r++) colb[r * RM + li] = M[li * nc + k0 + r];
         }
         cluster.sync();
-        // this thread's remote loads issued together: the flag and U's entries of its columns
-        // (at most two: nc <= CS_BC_MAX_NC <= 2 x CS_BC_THREADS)
-        const float* ob = cluster.map_shared_rank(mine, owner);
+        // the owner's pivot buffer copied once into this CTA's shared memory (16-byte
+        // distributed shared memory loads), then read locally
+        {
+            const float4* ob4 = reinterpret_cast<const float4*>(cluster.map_shared_rank(mine, owner));
+            float4* lb4 = reinterpret_cast<float4*>(lbuf);
+            for (int q = threadIdx.x; q < UB / 4; q += blockDim.x) lb4[q] = ob4[q];
+        }
+        __syncthreads();
+        // this thread's columns (at most two: nc <= CS_BC_MAX_NC <= 2 x CS_BC_THREADS)
         const int j0 = threadIdx.x, j1 = threadIdx.x + blockDim.x;
-        const float flag = ob[3 * nc];
+        const float flag = lbuf[3 * nc];
         float u[2][3];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int j = h ? j1 : j0;
 #pragma unroll
-            for (int r = 0; r < 3; r++) u[h][r] = j < nc ? ob[r * nc + j] : 0.f;
+            for (int r = 0; r < 3; r++) u[h][r] = j < nc ? lbuf[r * nc + j] : 0.f;
         }
         if (flag == 0.f) {  // the same flag in every CTA: a uniform exit
             if (threadIdx.x == 0) bad = 1;

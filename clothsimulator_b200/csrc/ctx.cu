@@ -1455,7 +1455,8 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     int bcGmax = CS_BC_MAX_G;
     {
         const size_t rm = 3 * (((size_t)CS_BC_MAX_NC / 3 + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER);
-        const size_t smemBig = (rm * CS_BC_MAX_NC + 2 * (3 * (size_t)CS_BC_MAX_NC + 1) + 3 * rm) * sizeof(float);
+        const size_t ub = (3 * (size_t)CS_BC_MAX_NC + 1 + 3) & ~(size_t)3;
+        const size_t smemBig = (((rm * CS_BC_MAX_NC + 3) & ~(size_t)3) + 3 * ub + 3 * rm) * sizeof(float);
         int nclusters = 0;
         if (cudaFuncSetAttribute(cs_bc_invert_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBig) ==
                 cudaSuccess &&
