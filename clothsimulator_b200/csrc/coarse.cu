@@ -11,9 +11,9 @@
 // the result is deterministic) and inverted by Gauss-Jordan in FP32 -- one CTA with the matrix
 // in shared memory up to CS_BC_SMALL_NC unknowns, else a cluster of CS_BC_CLUSTER CTAs with its
 // rows spread over their shared memory and each pivot row read through distributed shared
-// memory -- then symmetrised.  A_c is SPD (A is), so no pivoting is needed; the pivots are the
-// aggregates' 3x3 diagonal blocks, and one that is not positive definite disables the sheet's
-// correction for the step.  Per CG trip, after the vector
+// memory -- then symmetrised.  A_c is SPD (A is), so no pivoting is needed; the pivots are
+// diagonal blocks of CS_BC_PB aggregates (CS_BC_KB rows, a twelfth of the barriers of scalar
+// pivots), and a non-positive pivot inside one disables the sheet's correction for the step.  Per CG trip, after the vector
 // update: R r (a block per aggregate), e_c = A_c^-1 R r (a warp per coarse row), then
 // z += R^T e_c with the r.z and r.r partials recomputed (a warp per 32 rows in natural order,
 // as cs_vector_kernel lays them out).  Sheets solved cluster-resident (their own coarse
@@ -94,31 +94,47 @@ __global__ void __launch_bounds__(256) cs_bc_assemble_kernel(Batch B) {
     }
 }
 
-// Inverse of a 3x3 block (row-major) by its adjugate; false unless it is positive definite
-// enough to pivot on (positive leading entry and determinant, finite).
-__device__ __forceinline__ bool bc_inv3(const float (&a)[9], float (&r)[9]) {
-    const float c0 = a[4] * a[8] - a[5] * a[7], c1 = a[5] * a[6] - a[3] * a[8], c2 = a[3] * a[7] - a[4] * a[6];
-    const float det = a[0] * c0 + a[1] * c1 + a[2] * c2;
-    if (!(a[0] > 0.f) || !(det > 0.f) || !isfinite(det)) return false;
-    const float id = 1.0f / det;
-    r[0] = c0 * id;
-    r[1] = (a[2] * a[7] - a[1] * a[8]) * id;
-    r[2] = (a[1] * a[5] - a[2] * a[4]) * id;
-    r[3] = c1 * id;
-    r[4] = (a[0] * a[8] - a[2] * a[6]) * id;
-    r[5] = (a[2] * a[3] - a[0] * a[5]) * id;
-    r[6] = c2 * id;
-    r[7] = (a[1] * a[6] - a[0] * a[7]) * id;
-    r[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+// In-place Gauss-Jordan inverse of a kn x kn SPD block (kn <= CS_BC_KB, row stride
+// CS_BC_KB) in shared memory by one warp; false (the same in every lane) if a pivot is not
+// positive.  Each lane reads its elements' old values before the warp writes the new ones.
+__device__ bool bc_warp_inverse(float* D, int kn) {
+    const int lane = threadIdx.x & 31;
+    constexpr int PER = (CS_BC_KB * CS_BC_KB + 31) / 32;
+    for (int p = 0; p < kn; p++) {
+        const float piv = D[p * CS_BC_KB + p];
+        if (!(piv > 0.f) || !isfinite(piv)) return false;
+        const float ip = 1.0f / piv;
+        float nv[PER];
+#pragma unroll
+        for (int m = 0; m < PER; m++) {
+            const int e = lane + 32 * m;
+            nv[m] = 0.f;
+            if (e < kn * kn) {
+                const int i = e / kn, j = e - i * kn;
+                const float a = D[i * CS_BC_KB + j], ci = D[i * CS_BC_KB + p], pj = D[p * CS_BC_KB + j];
+                nv[m] = i == p ? (j == p ? ip : pj * ip) : (j == p ? -ci * ip : a - ci * (pj * ip));
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < PER; m++) {
+            const int e = lane + 32 * m;
+            if (e < kn * kn) {
+                const int i = e / kn, j = e - i * kn;
+                D[i * CS_BC_KB + j] = nv[m];
+            }
+        }
+        __syncwarp();
+    }
     return true;
 }
 
-// Gauss-Jordan inversion in place with 3x3 pivot blocks (one per aggregate: a third of the
-// barriers of scalar pivots) of an SPD matrix held by one CTA in shared memory (nc <=
-// CS_BC_SMALL_NC), a block per sheet; the inverse is written symmetrised.  Per pivot block K:
-// U = D^-1 A[K, :] (D = A[K, K]), then every row i outside K gets A[i, :] -= A[i, K] U and
-// A[i, K] = -A[i, K] D^-1, and rows K become U.  Thread t updates column t % nc of rows
-// t / nc, t / nc + blockDim / nc, ... (no division in the loops).
+// Gauss-Jordan inversion in place with pivot blocks of CS_BC_PB aggregates (CS_BC_KB rows: a
+// twelfth of the barriers of scalar pivots) of an SPD matrix held by one CTA in shared memory
+// (nc <= CS_BC_SMALL_NC), a block per sheet; the inverse is written symmetrised.  Per pivot
+// block K (kn rows from k0): D = A[K, K] inverted by one warp, U = D^-1 A[K, :] with U[:, K] =
+// D^-1, then every row i outside K gets A[i, :] -= A[i, K] U (the K columns: -A[i, K] D^-1) and
+// rows K become U.  Thread t updates column t % nc of rows t / nc, t / nc + blockDim / nc, ...
 __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch B) {
     extern __shared__ float bc_sm[];
     __shared__ int bad;
@@ -128,8 +144,9 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
     const int nc = 3 * sh.bc_na;
     if (nc > CS_BC_SMALL_NC) return;
     float* M = bc_sm;
-    float* rowb = bc_sm + nc * nc;  // 3 x nc: U
-    float* colb = rowb + 3 * nc;    // 3 x nc: column t of K over all rows
+    float* U = bc_sm + nc * nc;            // CS_BC_KB x nc
+    float* colb = U + CS_BC_KB * nc;       // nc x CS_BC_KB: A[i, K]
+    float* D = colb + CS_BC_KB * nc;       // CS_BC_KB x CS_BC_KB
     const float* G = B.bc_mat + sh.bc_mat_off;
     const int n2 = nc * nc;
     for (int e = threadIdx.x; e < n2; e += blockDim.x) M[e] = G[e];
@@ -137,36 +154,48 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
     const int rs = blockDim.x / nc, j = threadIdx.x % nc, i0 = threadIdx.x / nc;
     const bool active = i0 < rs;  // threads beyond rs * nc idle in the update
     __syncthreads();
-    for (int k0 = 0; k0 < nc; k0 += 3) {
-        float d[9], di[9];
-#pragma unroll
-        for (int q = 0; q < 9; q++) d[q] = M[(k0 + q / 3) * nc + k0 + q % 3];
-        if (!bc_inv3(d, di)) {  // the same values in every thread: a uniform exit
-            if (threadIdx.x == 0) bad = 1;
-            break;
+    for (int k0 = 0; k0 < nc; k0 += CS_BC_KB) {
+        const int kn = min(CS_BC_KB, nc - k0);
+        for (int e = threadIdx.x; e < kn * kn; e += blockDim.x) {
+            const int a = e / kn, b = e - a * kn;
+            D[a * CS_BC_KB + b] = M[(k0 + a) * nc + k0 + b];
         }
+        for (int e = threadIdx.x; e < nc * kn; e += blockDim.x) {
+            const int i = e / kn, t = e - i * kn;
+            colb[i * CS_BC_KB + t] = M[i * nc + k0 + t];
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const bool ok = bc_warp_inverse(D, kn);
+            if (threadIdx.x == 0 && !ok) bad = 1;
+        }
+        __syncthreads();
+        if (bad) break;  // uniform: read after the barrier
         for (int q = threadIdx.x; q < nc; q += blockDim.x) {
-            const int c = q - k0;  // column of K, or outside 0..2
-#pragma unroll
-            for (int r = 0; r < 3; r++) {
-                const float dk = c == 0 ? di[3 * r] : c == 1 ? di[3 * r + 1] : di[3 * r + 2];
-                const float u = (c >= 0 && c < 3)
-                                    ? dk
-                                    : di[3 * r] * M[k0 * nc + q] + di[3 * r + 1] * M[(k0 + 1) * nc + q] +
-                                          di[3 * r + 2] * M[(k0 + 2) * nc + q];
-                rowb[r * nc + q] = u;
-                colb[r * nc + q] = M[q * nc + k0 + r];
+            const int c = q - k0;
+            for (int t = 0; t < kn; t++) {
+                float u;
+                if (c >= 0 && c < kn) u = D[t * CS_BC_KB + c];
+                else {
+                    u = 0.f;
+                    for (int v = 0; v < kn; v++) u = __fmaf_rn(D[t * CS_BC_KB + v], M[(k0 + v) * nc + q], u);
+                }
+                U[t * nc + q] = u;
             }
         }
         __syncthreads();
         if (active) {
-            const float u0 = rowb[j], u1 = rowb[nc + j], u2 = rowb[2 * nc + j];
-            const bool jk = j >= k0 && j < k0 + 3;
+            float uj[CS_BC_KB];
+#pragma unroll
+            for (int t = 0; t < CS_BC_KB; t++) uj[t] = t < kn ? U[t * nc + j] : 0.f;
+            const bool jk = j >= k0 && j < k0 + kn;
             for (int i = i0; i < nc; i += rs) {
                 float v;
-                if (i >= k0 && i < k0 + 3) v = rowb[(i - k0) * nc + j];
+                if (i >= k0 && i < k0 + kn) v = U[(i - k0) * nc + j];
                 else {
-                    const float t = colb[i] * u0 + colb[nc + i] * u1 + colb[2 * nc + i] * u2;
+                    float t = 0.f;
+#pragma unroll
+                    for (int q = 0; q < CS_BC_KB; q++) t = __fmaf_rn(colb[i * CS_BC_KB + q], uj[q], t);
                     v = jk ? -t : M[i * nc + j] - t;
                 }
                 M[i * nc + j] = v;
@@ -186,13 +215,14 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
 
 // The same inversion of a larger coarse matrix (CS_BC_SMALL_NC < nc <= CS_BC_MAX_NC) by a
 // cluster of CS_BC_CLUSTER CTAs, one cluster per sheet of B.bc_big: rank c holds the rows of
-// aggregates c, c + CS_BC_CLUSTER, ... in shared memory.  Per pivot block (aggregate) its owner
-// writes U = D^-1 A[K, :] and a validity flag into its own pivot buffer (two alternate), one
-// cluster barrier, then every CTA copies it from the owner's shared memory into its own
-// (16-byte distributed shared memory loads) and updates its rows, thread t columns t and
-// t + blockDim.  An owner rewrites a buffer only after the barrier that follows
-// every CTA's last read of it, so one barrier per pivot block suffices.  The raw inverse goes
-// back to bc_mat, then (after a barrier) each CTA writes its rows of the symmetrised inverse.
+// pivot blocks c, c + CS_BC_CLUSTER, ... in shared memory.  Per pivot block its owner inverts
+// D (one warp) and writes U and a validity flag into its buffer, one cluster barrier, then every
+// other CTA copies the buffer from the owner's shared memory into its own (16-byte distributed
+// shared memory loads) and all update their rows, thread t columns t and t + blockDim.  A CTA's
+// buffer is overwritten (by its own copy or its own U) only after the barrier that follows
+// every other CTA's copy from it, so one cluster barrier per pivot block suffices.  The raw
+// inverse goes back to bc_mat, then (after a barrier) each CTA writes its rows of the
+// symmetrised inverse.
 __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Batch B) {
     extern __shared__ float bc_sm[];
     __shared__ int bad;
@@ -202,70 +232,68 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
     // the same decision in every CTA of the cluster: all return, or none
     if (!bc_sheet_on(B, s) || B.inst[s].phase == PH_RESIDENT) return;
     const SheetDesc& sh = B.sheets[s];
-    const int na = sh.bc_na, nc = 3 * na;
+    const int nc = 3 * sh.bc_na;
     if (nc <= CS_BC_SMALL_NC || nc > CS_BC_MAX_NC) return;
-    const int RM = 3 * ((na + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER);
-    const int R = 3 * ((na - rank + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER);  // local row li: aggregate rank + 16 (li / 3)
-    const int UB = (3 * nc + 1 + 3) & ~3;    // a pivot buffer: U, the validity flag, padded to 16 bytes
-    float* M = bc_sm;                        // RM x nc
-    float* pbuf = bc_sm + ((RM * nc + 3) & ~3);  // 2 x UB, 16-byte aligned
-    float* lbuf = pbuf + 2 * UB;             // UB: this CTA's copy of the current pivot buffer
-    float* colb = lbuf + UB;                 // 3 x RM
+    const int nblk = (nc + CS_BC_KB - 1) / CS_BC_KB;              // only the last may be partial
+    const int RM = CS_BC_KB * ((nblk + CS_BC_CLUSTER - 1) / CS_BC_CLUSTER);
+    int R = 0;                                                     // this CTA's rows
+    for (int kb = rank; kb < nblk; kb += CS_BC_CLUSTER) R += min(CS_BC_KB, nc - CS_BC_KB * kb);
+    const int UB = (CS_BC_KB * nc + 1 + 3) & ~3;                   // U, the flag, padded to 16 bytes
+    float* M = bc_sm;                                              // RM x nc
+    float* lbuf = bc_sm + ((RM * nc + 3) & ~3);                    // UB
+    float* colb = lbuf + UB;                                       // RM x CS_BC_KB: A[i, K]
+    float* D = colb + RM * CS_BC_KB;                               // CS_BC_KB x CS_BC_KB
     float* G = B.bc_mat + sh.bc_mat_off;
-    auto grow = [&](int li) { return 3 * (rank + CS_BC_CLUSTER * (li / 3)) + li % 3; };
+    auto grow = [&](int li) { return CS_BC_KB * (rank + CS_BC_CLUSTER * (li / CS_BC_KB)) + li % CS_BC_KB; };
     for (int e = threadIdx.x; e < R * nc; e += blockDim.x) {
         const int li = e / nc, j = e - li * nc;
         M[e] = G[(size_t)grow(li) * nc + j];
     }
     if (threadIdx.x == 0) bad = 0;
     cluster.sync();  // every CTA has started and loaded its rows before remote reads
-    for (int kb = 0; kb < na; kb++) {
-        const int owner = kb % CS_BC_CLUSTER, k0 = 3 * kb;
-        float* mine = pbuf + (kb & 1) * UB;
+    const int j0 = threadIdx.x, j1 = threadIdx.x + blockDim.x;
+    for (int kb = 0; kb < nblk; kb++) {
+        const int owner = kb % CS_BC_CLUSTER, k0 = CS_BC_KB * kb, kn = min(CS_BC_KB, nc - k0);
+        for (int e = threadIdx.x; e < R * kn; e += blockDim.x) {
+            const int li = e / kn, t = e - li * kn;
+            colb[li * CS_BC_KB + t] = M[li * nc + k0 + t];
+        }
         if (rank == owner) {
-            const int l0 = 3 * (kb / CS_BC_CLUSTER);
-            float d[9], di[9];
-#pragma unroll
-            for (int q = 0; q < 9; q++) d[q] = M[(l0 + q / 3) * nc + k0 + q % 3];
-            const bool ok = bc_inv3(d, di);
+            const int l0 = CS_BC_KB * (kb / CS_BC_CLUSTER);
+            for (int e = threadIdx.x; e < kn * kn; e += blockDim.x) {
+                const int a = e / kn, b = e - a * kn;
+                D[a * CS_BC_KB + b] = M[(l0 + a) * nc + k0 + b];
+            }
+            __syncthreads();
+            __shared__ int okD;
+            if (threadIdx.x < 32) {
+                const bool ok = bc_warp_inverse(D, kn);
+                if (threadIdx.x == 0) okD = ok ? 1 : 0;
+            }
+            __syncthreads();
             for (int q = threadIdx.x; q < nc; q += blockDim.x) {
-                const int c = q - k0;  // column of K, or outside 0..2
-#pragma unroll
-                for (int r = 0; r < 3; r++) {
-                    const float dk = c == 0 ? di[3 * r] : c == 1 ? di[3 * r + 1] : di[3 * r + 2];
-                    mine[r * nc + q] = !ok ? 0.f
-                                       : (c >= 0 && c < 3)
-                                           ? dk
-                                           : di[3 * r] * M[l0 * nc + q] + di[3 * r + 1] * M[(l0 + 1) * nc + q] +
-                                                 di[3 * r + 2] * M[(l0 + 2) * nc + q];
+                const int c = q - k0;
+                for (int t = 0; t < kn; t++) {
+                    float u;
+                    if (!okD) u = 0.f;
+                    else if (c >= 0 && c < kn) u = D[t * CS_BC_KB + c];
+                    else {
+                        u = 0.f;
+                        for (int v = 0; v < kn; v++) u = __fmaf_rn(D[t * CS_BC_KB + v], M[(l0 + v) * nc + q], u);
+                    }
+                    lbuf[t * nc + q] = u;
                 }
             }
-            if (threadIdx.x == 0) mine[3 * nc] = ok ? 1.f : 0.f;
-        }
-        for (int li = threadIdx.x; li < R; li += blockDim.x) {
-#pragma unroll
-            for (int r = 0; r < 3; r++) colb[r * RM + li] = M[li * nc + k0 + r];
+            if (threadIdx.x == 0) lbuf[CS_BC_KB * nc] = okD ? 1.f : 0.f;
         }
         cluster.sync();
-        // the owner's pivot buffer copied once into this CTA's shared memory (16-byte
-        // distributed shared memory loads), then read locally
-        {
-            const float4* ob4 = reinterpret_cast<const float4*>(cluster.map_shared_rank(mine, owner));
+        if (rank != owner) {
+            const float4* ob4 = reinterpret_cast<const float4*>(cluster.map_shared_rank(lbuf, owner));
             float4* lb4 = reinterpret_cast<float4*>(lbuf);
             for (int q = threadIdx.x; q < UB / 4; q += blockDim.x) lb4[q] = ob4[q];
         }
         __syncthreads();
-        // this thread's columns (at most two: nc <= CS_BC_MAX_NC <= 2 x CS_BC_THREADS)
-        const int j0 = threadIdx.x, j1 = threadIdx.x + blockDim.x;
-        const float flag = lbuf[3 * nc];
-        float u[2][3];
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int j = h ? j1 : j0;
-#pragma unroll
-            for (int r = 0; r < 3; r++) u[h][r] = j < nc ? lbuf[r * nc + j] : 0.f;
-        }
-        if (flag == 0.f) {  // the same flag in every CTA: a uniform exit
+        if (lbuf[CS_BC_KB * nc] == 0.f) {  // the same flag in every CTA: a uniform exit
             if (threadIdx.x == 0) bad = 1;
             break;
         }
@@ -273,13 +301,18 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
         for (int h = 0; h < 2; h++) {
             const int j = h ? j1 : j0;
             if (j >= nc) continue;
-            const bool jk = j >= k0 && j < k0 + 3;
+            float uj[CS_BC_KB];
+#pragma unroll
+            for (int t = 0; t < CS_BC_KB; t++) uj[t] = t < kn ? lbuf[t * nc + j] : 0.f;
+            const bool jk = j >= k0 && j < k0 + kn;
             for (int li = 0; li < R; li++) {
                 const int i = grow(li);
                 float v;
-                if (i >= k0 && i < k0 + 3) v = i == k0 ? u[h][0] : i == k0 + 1 ? u[h][1] : u[h][2];
+                if (i >= k0 && i < k0 + kn) v = lbuf[(i - k0) * nc + j];
                 else {
-                    const float t = colb[li] * u[h][0] + colb[RM + li] * u[h][1] + colb[2 * RM + li] * u[h][2];
+                    float t = 0.f;
+#pragma unroll
+                    for (int q = 0; q < CS_BC_KB; q++) t = __fmaf_rn(colb[li * CS_BC_KB + q], uj[q], t);
                     v = jk ? -t : M[li * nc + j] - t;
                 }
                 M[li * nc + j] = v;

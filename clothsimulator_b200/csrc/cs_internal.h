@@ -117,6 +117,9 @@ enum InstPhase : int {
 #define CS_BC_SMALL_NC 192
 #define CS_BC_CLUSTER 16
 #define CS_BC_THREADS 512
+// Gauss-Jordan pivot blocks of the coarse inversion: CS_BC_PB aggregates, CS_BC_KB rows
+#define CS_BC_PB 4
+#define CS_BC_KB (3 * CS_BC_PB)
 #define CS_COARSE_MAX_K 8
 #define CS_COARSE_AGGS 54
 // Threads of the per-sheet set-up kernel that forms and inverts the coarse matrix.
