@@ -100,6 +100,13 @@ __global__ void __launch_bounds__(256) cs_bc_assemble_kernel(Batch B) {
 __device__ bool bc_warp_inverse(float* D, int kn) {
     const int lane = threadIdx.x & 31;
     constexpr int PER = (CS_BC_KB * CS_BC_KB + 31) / 32;
+    int ii[PER], jj[PER];
+#pragma unroll
+    for (int m = 0; m < PER; m++) {
+        const int e = lane + 32 * m;
+        ii[m] = e < kn * kn ? e / kn : -1;
+        jj[m] = e < kn * kn ? e - ii[m] * kn : 0;
+    }
     for (int p = 0; p < kn; p++) {
         const float piv = D[p * CS_BC_KB + p];
         if (!(piv > 0.f) || !isfinite(piv)) return false;
@@ -107,26 +114,72 @@ __device__ bool bc_warp_inverse(float* D, int kn) {
         float nv[PER];
 #pragma unroll
         for (int m = 0; m < PER; m++) {
-            const int e = lane + 32 * m;
+            const int i = ii[m], j = jj[m];
             nv[m] = 0.f;
-            if (e < kn * kn) {
-                const int i = e / kn, j = e - i * kn;
+            if (i >= 0) {
                 const float a = D[i * CS_BC_KB + j], ci = D[i * CS_BC_KB + p], pj = D[p * CS_BC_KB + j];
                 nv[m] = i == p ? (j == p ? ip : pj * ip) : (j == p ? -ci * ip : a - ci * (pj * ip));
             }
         }
         __syncwarp();
 #pragma unroll
-        for (int m = 0; m < PER; m++) {
-            const int e = lane + 32 * m;
-            if (e < kn * kn) {
-                const int i = e / kn, j = e - i * kn;
-                D[i * CS_BC_KB + j] = nv[m];
-            }
-        }
+        for (int m = 0; m < PER; m++)
+            if (ii[m] >= 0) D[ii[m] * CS_BC_KB + jj[m]] = nv[m];
         __syncwarp();
     }
     return true;
+}
+
+// t[r] = sum_q C[r][q] u[q] for four rows of 12 coefficients each (16-byte loads, the rows'
+// chains independent); C rows 48 bytes apart.
+__device__ __forceinline__ void bc_dot12x4(const float* C, const float (&u)[CS_BC_KB], float (&t)[4]) {
+    static_assert(CS_BC_KB == 12, "four-aggregate pivot blocks");
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const float4* c4 = reinterpret_cast<const float4*>(C + r * CS_BC_KB);
+        const float4 a = c4[0], b = c4[1], c = c4[2];
+        float x = a.x * u[0];
+        float y = a.y * u[1];
+        x = __fmaf_rn(a.z, u[2], x);
+        y = __fmaf_rn(a.w, u[3], y);
+        x = __fmaf_rn(b.x, u[4], x);
+        y = __fmaf_rn(b.y, u[5], y);
+        x = __fmaf_rn(b.z, u[6], x);
+        y = __fmaf_rn(b.w, u[7], y);
+        x = __fmaf_rn(c.x, u[8], x);
+        y = __fmaf_rn(c.y, u[9], y);
+        x = __fmaf_rn(c.z, u[10], x);
+        y = __fmaf_rn(c.w, u[11], y);
+        t[r] = x + y;
+    }
+}
+
+// out[t * ldo] = sum_v D[t][v] a[v * lda] for t < kn (one column of D^-1 A[K, :]); a full
+// block's sums unrolled with their loads issued together.
+__device__ __forceinline__ void bc_block_rows_times(const float* D, const float* a, int lda, int kn, float* out,
+                                                    int ldo) {
+    if (kn == CS_BC_KB) {
+        float av[CS_BC_KB];
+#pragma unroll
+        for (int v = 0; v < CS_BC_KB; v++) av[v] = a[(size_t)v * lda];
+#pragma unroll
+        for (int t = 0; t < CS_BC_KB; t++) {
+            const float* d = D + t * CS_BC_KB;
+            float x = d[0] * av[0], y = d[1] * av[1];
+#pragma unroll
+            for (int v = 2; v < CS_BC_KB; v += 2) {
+                x = __fmaf_rn(d[v], av[v], x);
+                y = __fmaf_rn(d[v + 1], av[v + 1], y);
+            }
+            out[(size_t)t * ldo] = x + y;
+        }
+        return;
+    }
+    for (int t = 0; t < kn; t++) {
+        float u = 0.f;
+        for (int v = 0; v < kn; v++) u = __fmaf_rn(D[t * CS_BC_KB + v], a[(size_t)v * lda], u);
+        out[(size_t)t * ldo] = u;
+    }
 }
 
 // Gauss-Jordan inversion in place with pivot blocks of CS_BC_PB aggregates (CS_BC_KB rows: a
@@ -144,9 +197,9 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
     const int nc = 3 * sh.bc_na;
     if (nc > CS_BC_SMALL_NC) return;
     float* M = bc_sm;
-    float* U = bc_sm + nc * nc;            // CS_BC_KB x nc
-    float* colb = U + CS_BC_KB * nc;       // nc x CS_BC_KB: A[i, K]
-    float* D = colb + CS_BC_KB * nc;       // CS_BC_KB x CS_BC_KB
+    float* colb = bc_sm + ((nc * nc + 3) & ~3);  // nc x CS_BC_KB: A[i, K], 16-byte aligned rows
+    float* U = colb + CS_BC_KB * nc;             // CS_BC_KB x nc
+    float* D = U + CS_BC_KB * nc;                // CS_BC_KB x CS_BC_KB
     const float* G = B.bc_mat + sh.bc_mat_off;
     const int n2 = nc * nc;
     for (int e = threadIdx.x; e < n2; e += blockDim.x) M[e] = G[e];
@@ -160,9 +213,9 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
             const int a = e / kn, b = e - a * kn;
             D[a * CS_BC_KB + b] = M[(k0 + a) * nc + k0 + b];
         }
-        for (int e = threadIdx.x; e < nc * kn; e += blockDim.x) {
-            const int i = e / kn, t = e - i * kn;
-            colb[i * CS_BC_KB + t] = M[i * nc + k0 + t];
+        for (int e = threadIdx.x; e < nc * CS_BC_KB; e += blockDim.x) {
+            const int i = e / CS_BC_KB, t = e - i * CS_BC_KB;
+            colb[e] = t < kn ? M[i * nc + k0 + t] : 0.f;
         }
         __syncthreads();
         if (threadIdx.x < 32) {
@@ -173,15 +226,11 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
         if (bad) break;  // uniform: read after the barrier
         for (int q = threadIdx.x; q < nc; q += blockDim.x) {
             const int c = q - k0;
-            for (int t = 0; t < kn; t++) {
-                float u;
-                if (c >= 0 && c < kn) u = D[t * CS_BC_KB + c];
-                else {
-                    u = 0.f;
-                    for (int v = 0; v < kn; v++) u = __fmaf_rn(D[t * CS_BC_KB + v], M[(k0 + v) * nc + q], u);
-                }
-                U[t * nc + q] = u;
+            if (c >= 0 && c < kn) {
+                for (int t = 0; t < kn; t++) U[t * nc + q] = D[t * CS_BC_KB + c];
+                continue;
             }
+            bc_block_rows_times(D, M + (size_t)k0 * nc + q, nc, kn, U + q, nc);
         }
         __syncthreads();
         if (active) {
@@ -193,9 +242,20 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_small_kernel(Batch
                 float v;
                 if (i >= k0 && i < k0 + kn) v = U[(i - k0) * nc + j];
                 else {
-                    float t = 0.f;
-#pragma unroll
-                    for (int q = 0; q < CS_BC_KB; q++) t = __fmaf_rn(colb[i * CS_BC_KB + q], uj[q], t);
+                    const float4* c4 = reinterpret_cast<const float4*>(colb + i * CS_BC_KB);
+                    const float4 a = c4[0], b = c4[1], c = c4[2];
+                    float x = a.x * uj[0], y = a.y * uj[1];
+                    x = __fmaf_rn(a.z, uj[2], x);
+                    y = __fmaf_rn(a.w, uj[3], y);
+                    x = __fmaf_rn(b.x, uj[4], x);
+                    y = __fmaf_rn(b.y, uj[5], y);
+                    x = __fmaf_rn(b.z, uj[6], x);
+                    y = __fmaf_rn(b.w, uj[7], y);
+                    x = __fmaf_rn(c.x, uj[8], x);
+                    y = __fmaf_rn(c.y, uj[9], y);
+                    x = __fmaf_rn(c.z, uj[10], x);
+                    y = __fmaf_rn(c.w, uj[11], y);
+                    const float t = x + y;
                     v = jk ? -t : M[i * nc + j] - t;
                 }
                 M[i * nc + j] = v;
@@ -254,9 +314,9 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
     const int j0 = threadIdx.x, j1 = threadIdx.x + blockDim.x;
     for (int kb = 0; kb < nblk; kb++) {
         const int owner = kb % CS_BC_CLUSTER, k0 = CS_BC_KB * kb, kn = min(CS_BC_KB, nc - k0);
-        for (int e = threadIdx.x; e < R * kn; e += blockDim.x) {
-            const int li = e / kn, t = e - li * kn;
-            colb[li * CS_BC_KB + t] = M[li * nc + k0 + t];
+        for (int e = threadIdx.x; e < RM * CS_BC_KB; e += blockDim.x) {
+            const int li = e / CS_BC_KB, t = e - li * CS_BC_KB;
+            colb[e] = (li < R && t < kn) ? M[li * nc + k0 + t] : 0.f;  // rows and columns past the data: 0
         }
         if (rank == owner) {
             const int l0 = CS_BC_KB * (kb / CS_BC_CLUSTER);
@@ -273,16 +333,11 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
             __syncthreads();
             for (int q = threadIdx.x; q < nc; q += blockDim.x) {
                 const int c = q - k0;
-                for (int t = 0; t < kn; t++) {
-                    float u;
-                    if (!okD) u = 0.f;
-                    else if (c >= 0 && c < kn) u = D[t * CS_BC_KB + c];
-                    else {
-                        u = 0.f;
-                        for (int v = 0; v < kn; v++) u = __fmaf_rn(D[t * CS_BC_KB + v], M[(l0 + v) * nc + q], u);
-                    }
-                    lbuf[t * nc + q] = u;
+                if (!okD || (c >= 0 && c < kn)) {
+                    for (int t = 0; t < kn; t++) lbuf[t * nc + q] = okD ? D[t * CS_BC_KB + c] : 0.f;
+                    continue;
                 }
+                bc_block_rows_times(D, M + (size_t)l0 * nc + q, nc, kn, lbuf + q, nc);
             }
             if (threadIdx.x == 0) lbuf[CS_BC_KB * nc] = okD ? 1.f : 0.f;
         }
@@ -297,6 +352,7 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
             if (threadIdx.x == 0) bad = 1;
             break;
         }
+        const int ownRow0 = rank == owner ? CS_BC_KB * (kb / CS_BC_CLUSTER) : -CS_BC_KB;  // this CTA's rows of K
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int j = h ? j1 : j0;
@@ -305,17 +361,18 @@ __global__ void __launch_bounds__(CS_BC_THREADS) cs_bc_invert_cluster_kernel(Bat
 #pragma unroll
             for (int t = 0; t < CS_BC_KB; t++) uj[t] = t < kn ? lbuf[t * nc + j] : 0.f;
             const bool jk = j >= k0 && j < k0 + kn;
-            for (int li = 0; li < R; li++) {
-                const int i = grow(li);
-                float v;
-                if (i >= k0 && i < k0 + kn) v = lbuf[(i - k0) * nc + j];
-                else {
-                    float t = 0.f;
+            for (int l4 = 0; l4 < R; l4 += 4) {  // RM is a multiple of 12: rows l4..l4+3 exist in colb
+                float t[4];
+                bc_dot12x4(colb + l4 * CS_BC_KB, uj, t);
 #pragma unroll
-                    for (int q = 0; q < CS_BC_KB; q++) t = __fmaf_rn(colb[li * CS_BC_KB + q], uj[q], t);
-                    v = jk ? -t : M[li * nc + j] - t;
+                for (int r = 0; r < 4; r++) {
+                    const int li = l4 + r;
+                    if (li >= R) break;
+                    float v;
+                    if (li >= ownRow0 && li < ownRow0 + kn) v = lbuf[(li - ownRow0) * nc + j];
+                    else v = jk ? -t[r] : M[li * nc + j] - t[r];
+                    M[li * nc + j] = v;
                 }
-                M[li * nc + j] = v;
             }
         }
         __syncthreads();

@@ -1010,7 +1010,7 @@ int launchBatchedCoarseSetup(cs_ctx* c) {
     cudaMemsetAsync(B.bc_mat, 0, (size_t)c->bcMatFloats * sizeof(float), c->stream);
     const int gx = std::max(1, std::min(256, nblk(B.bc_max_npair, 8)));
     cs_bc_assemble_kernel<<<dim3(gx, B.S), 256, 0, c->stream>>>(B);
-    cs_bc_invert_small_kernel<<<B.S, CS_BC_THREADS, (CS_BC_SMALL_NC * CS_BC_SMALL_NC + 2 * CS_BC_KB * CS_BC_SMALL_NC + CS_BC_KB * CS_BC_KB) * sizeof(float),
+    cs_bc_invert_small_kernel<<<B.S, CS_BC_THREADS, (CS_BC_SMALL_NC * CS_BC_SMALL_NC + 4 + 2 * CS_BC_KB * CS_BC_SMALL_NC + CS_BC_KB * CS_BC_KB) * sizeof(float),
                                 c->stream>>>(B);
     int n = 2;
     if (B.bc_n_big > 0) {
@@ -1481,7 +1481,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         c->bcSmemBig = smemBig;
         if (nclusters <= 0) bcGmax = 8;  // 64 aggregates, 192 unknowns: one CTA inverts them
         CS_CUDA(cudaFuncSetAttribute(cs_bc_invert_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (CS_BC_SMALL_NC * CS_BC_SMALL_NC + 2 * CS_BC_KB * CS_BC_SMALL_NC + CS_BC_KB * CS_BC_KB) * (int)sizeof(float)));
+                                     (CS_BC_SMALL_NC * CS_BC_SMALL_NC + 4 + 2 * CS_BC_KB * CS_BC_SMALL_NC + CS_BC_KB * CS_BC_KB) * (int)sizeof(float)));
     }
     std::vector<BCPlan> bcplans(topos.size());
     for (size_t t = 0; t < topos.size(); t++) batchedCoarsePlan(*topos[t], bcGmax, bcplans[t]);
