@@ -189,6 +189,87 @@ def test_data_parallel_training_two_gloo_ranks():
     assert count == 30 and np.allclose(sums, np.arange(38) * 3)
 
 
+class FakeEnergyContext(FakeTrainingContext):
+    """The energy-norm step's parts (cs_mlp_energy_begin / _gradient_device / _end) on a vector
+    of parameters: the gradient of minibatch [s0, s1) at step k is w - target, the target
+    depending on the rank, the step and s0; begin and end count the steps."""
+
+    def __init__(self, rank, n):
+        super().__init__(rank, n)
+        self.k = 0
+        self.open = False
+
+    def mlp_energy_begin(self, params):
+        assert not self.open
+        self.open = True
+
+    def mlp_energy_gradient_device(self, s0, s1, grad):
+        assert self.open
+        g = self.w - self.target(self.rank, self.k, s0)
+        grad.numpy()[:] = g
+        return float(0.5 * (g * g).sum())
+
+    def mlp_energy_end(self, allow_unconverged=False):
+        assert self.open
+        self.open = False
+        self.k += 1
+        return None
+
+
+def _energy_dp_rank(rank, world, port, out):
+    os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch.distributed as dist
+
+    from clothsimulator_b200 import native, training
+
+    dist.init_process_group("gloo", init_method="env://", timeout=datetime.timedelta(seconds=60))
+    ctx = FakeEnergyContext(rank, native.MLP_TRAINED)
+    for step in range(3):
+        training.energy_step_data_parallel(ctx, None, 5, 0.5, 2, 40 + step, allreduce_sum=dist.all_reduce,
+                                           world=world)
+    out[rank] = {"w": ctx.w.copy(), "steps": ctx.k}
+    dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+def test_energy_data_parallel_step_two_gloo_ranks():
+    """energy_step_data_parallel over two gloo ranks: identical parameters on both, equal to
+    serial descent on the gradients averaged over the ranks, in cs_mlp_train_step's minibatch
+    order (its seeded shuffle), each step opened and closed once."""
+    sys.path.insert(0, ROOT)
+    from clothsimulator_b200 import native, training
+
+    world = 2
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        ctx = mp.get_context("spawn")
+        procs = [ctx.Process(target=_energy_dp_rank, args=(r, world, port, out)) for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(150)
+        codes = [p.exitcode for p in procs]
+        for p in procs:
+            if p.is_alive():
+                p.kill()
+        assert codes == [0, 0], codes
+        res = dict(out)
+    assert np.array_equal(res[0]["w"], res[1]["w"]) and res[0]["steps"] == 3
+    ref = [FakeEnergyContext(r, native.MLP_TRAINED) for r in range(world)]
+    w = np.zeros(native.MLP_TRAINED, np.float32)
+    for step in range(3):
+        (batches,) = list(training.minibatch_schedule(1, 5, 2, 1, 40 + step))
+        for _, s0, s1 in batches:
+            g = sum((w - c.target(c.rank, step, s0)) for c in ref) * np.float32(1.0 / world)
+            w = (w - np.float32(0.5) * g.astype(np.float32)).astype(np.float32)
+    assert np.allclose(res[0]["w"], w, rtol=1e-6, atol=1e-7)
+
+
 # Strong scaling (one workload split across ranks): the sheet partition balanced by stored
 # blocks, and the per-sheet statistics gathered back in workload order with one all-gather.
 
