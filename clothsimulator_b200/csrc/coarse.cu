@@ -487,3 +487,188 @@ __global__ void __launch_bounds__(128) cs_bc_finish_kernel(Batch B) {
         B.part[2 * slice + 1] = rr;
     }
 }
+
+// ---------------------------------------------------------------------------------------
+// Coarse matrix of each resident sheet, for the coarse-space correction of the cluster-resident
+// solver (resident.cu): A_c = R A R^T, where R sums the rows of each aggregate (a segment of a
+// CTA's strip) per component, so block (a, b) of A_c is the sum of the stored blocks A_ij with
+// row i in aggregate a and column j in aggregate b.  The loader lists those blocks per pair
+// (a, b) in slot order; a warp sums a pair, lane l taking the blocks l, l + 32, ... in order,
+// and a butterfly combines the lanes (a fixed order: deterministic, no atomics).  A_c is SPD (A
+// is, and R has full row rank), so Gauss-Jordan elimination inverts it in place in shared memory
+// without pivoting, in FP32, with pivot blocks of CS_BC_KB rows.  Per block K (kn rows from k0):
+// D = A[K, K] is inverted by one warp (bc_warp_inverse); the rows K become U = D^-1 A[K, :] with
+// U[:, K] = D^-1, a thread per column in place; every row i outside K gets A[i, j] -= A[i, K]
+// U[:, j] on the columns outside K, and after a barrier A[i, K] = -A[i, K] D^-1 (a thread per
+// row).  Five barriers per block.  The inverse, symmetrised, is stored per work item for the
+// resident kernel, which applies its CTA's rows each CG iteration.  A non-positive or
+// non-finite pivot marks the work item's coarse matrix invalid and the solve runs without the
+// correction.  One CTA per resident work item; dynamic shared memory cs_coarse_setup_smem(nc).
+namespace {
+
+__device__ __forceinline__ void coarse_load_block(const Batch& B, const SheetDesc& sh, int slot, float (&a)[9]) {
+    const float* pk = B.A + (size_t)(sh.panel_off + slot / CS_SLICE) * CS_PANEL_FLOATS;
+    const int l = slot % CS_SLICE;
+    const float4 a0 = __ldg(reinterpret_cast<const float4*>(pk) + l);
+    const float4 a1 = __ldg(reinterpret_cast<const float4*>(pk + 128) + l);
+    a[0] = a0.x;
+    a[1] = a0.y;
+    a[2] = a0.z;
+    a[3] = a0.w;
+    a[4] = a1.x;
+    a[5] = a1.y;
+    a[6] = a1.z;
+    a[7] = a1.w;
+    a[8] = __ldg(pk + 256 + l);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(CS_COARSE_THREADS) cs_coarse_setup_kernel(Batch B) {
+    extern __shared__ __align__(16) float cs_coarse_sm[];
+    __shared__ int bad;
+    const DevParams& P = *B.params;
+    if (P.solver != CS_SOLVER_AUTO_DEV || P.cheb_degree < 3 || !P.coarse) return;  // uniform
+    const int idx = blockIdx.x;
+    if (idx >= B.n_resident) return;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+    const SheetDesc& sh = B.sheets[B.rlist[idx]];
+    const int4 ci = B.rcoarse[sh.topo];
+    const int nc = ci.x;
+    if (nc == 0 || nc > B.res_cnc) {
+        if (tid == 0) B.cvalid[idx] = 0;
+        return;
+    }
+    const int ld = cs_coarse_ld(nc);
+    float* M = cs_coarse_sm;             // nc x ld
+    float* D = M + (size_t)nc * ld;      // CS_BC_KB x CS_BC_KB
+    for (int i = tid; i < nc * ld; i += blockDim.x) M[i] = 0.f;
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    for (int q = ci.z + w; q < ci.w; q += nw) {
+        const int4 pr = B.cpair[q];
+        float acc[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int k = pr.z + lane;
+        // two of the lane's blocks in flight at a time, added in order
+        for (; k + 32 < pr.w; k += 64) {
+            float a0[9], a1[9];
+            coarse_load_block(B, sh, __ldg(&B.ccontrib[k]), a0);
+            coarse_load_block(B, sh, __ldg(&B.ccontrib[k + 32]), a1);
+#pragma unroll
+            for (int e = 0; e < 9; e++) acc[e] += a0[e];
+#pragma unroll
+            for (int e = 0; e < 9; e++) acc[e] += a1[e];
+        }
+        if (k < pr.w) {
+            float a0[9];
+            coarse_load_block(B, sh, __ldg(&B.ccontrib[k]), a0);
+#pragma unroll
+            for (int e = 0; e < 9; e++) acc[e] += a0[e];
+        }
+#pragma unroll
+        for (int e = 0; e < 9; e++) acc[e] = bc_warp_sum(acc[e]);
+        if (lane == 0) {
+#pragma unroll
+            for (int e = 0; e < 9; e++) M[(size_t)(3 * pr.x + e / 3) * ld + 3 * pr.y + e % 3] = acc[e];
+        }
+    }
+    __syncthreads();
+    const int rs = blockDim.x / nc;  // rows whose updates run together (nc <= blockDim)
+    const int j = tid % nc, i0 = tid / nc;
+    for (int k0 = 0; k0 < nc; k0 += CS_BC_KB) {
+        const int kn = min(CS_BC_KB, nc - k0);
+        for (int e = tid; e < kn * kn; e += blockDim.x) {
+            const int a = e / kn, b = e - a * kn;
+            D[a * CS_BC_KB + b] = M[(size_t)(k0 + a) * ld + k0 + b];
+        }
+        __syncthreads();
+        if (w == 0) {
+            const bool ok = bc_warp_inverse(D, kn);
+            if (lane == 0 && !ok) bad = 1;
+        }
+        __syncthreads();
+        if (bad) break;  // uniform: read after the barrier
+        // rows K become U = D^-1 A[K, :] (U[:, K] = D^-1), a thread per column, in place
+        for (int q = tid; q < nc; q += blockDim.x) {
+            float* col = M + (size_t)k0 * ld + q;
+            const int c = q - k0;
+            if (c >= 0 && c < kn) {
+                for (int t = 0; t < kn; t++) col[(size_t)t * ld] = D[t * CS_BC_KB + c];
+                continue;
+            }
+            float av[CS_BC_KB];
+#pragma unroll
+            for (int v = 0; v < CS_BC_KB; v++) av[v] = v < kn ? col[(size_t)v * ld] : 0.f;
+#pragma unroll
+            for (int t = 0; t < CS_BC_KB; t++) {
+                if (t >= kn) break;
+                float x = 0.f, y = 0.f;
+#pragma unroll
+                for (int v = 0; v < CS_BC_KB; v += 2) {
+                    if (v < kn) x = __fmaf_rn(D[t * CS_BC_KB + v], av[v], x);
+                    if (v + 1 < kn) y = __fmaf_rn(D[t * CS_BC_KB + v + 1], av[v + 1], y);
+                }
+                col[(size_t)t * ld] = x + y;
+            }
+        }
+        __syncthreads();
+        // rows outside K, columns outside K: A[i, j] -= A[i, K] U[:, j]
+        if (i0 < rs && !(j >= k0 && j < k0 + kn)) {
+            float uj[CS_BC_KB];
+#pragma unroll
+            for (int t = 0; t < CS_BC_KB; t++) uj[t] = t < kn ? M[(size_t)(k0 + t) * ld + j] : 0.f;
+#pragma unroll 2
+            for (int i = i0; i < nc; i += rs) {
+                if (i >= k0 && i < k0 + kn) continue;
+                const float* ai = M + (size_t)i * ld + k0;  // 16-byte aligned: ld and k0 are multiples of 4
+                float x, y;
+                if (kn == CS_BC_KB) {
+                    const float4* a4 = reinterpret_cast<const float4*>(ai);
+                    const float4 a = a4[0], b = a4[1], c = a4[2];
+                    x = a.x * uj[0];
+                    y = a.y * uj[1];
+                    x = __fmaf_rn(a.z, uj[2], x);
+                    y = __fmaf_rn(a.w, uj[3], y);
+                    x = __fmaf_rn(b.x, uj[4], x);
+                    y = __fmaf_rn(b.y, uj[5], y);
+                    x = __fmaf_rn(b.z, uj[6], x);
+                    y = __fmaf_rn(b.w, uj[7], y);
+                    x = __fmaf_rn(c.x, uj[8], x);
+                    y = __fmaf_rn(c.y, uj[9], y);
+                    x = __fmaf_rn(c.z, uj[10], x);
+                    y = __fmaf_rn(c.w, uj[11], y);
+                } else {
+                    x = 0.f;
+                    y = 0.f;
+                    for (int t = 0; t < kn; t++) x = __fmaf_rn(ai[t], uj[t], x);
+                }
+                M[(size_t)i * ld + j] -= x + y;
+            }
+        }
+        __syncthreads();
+        // rows outside K, columns K: A[i, K] = -A[i, K] D^-1, a thread per row
+        for (int i = tid; i < nc; i += blockDim.x) {
+            if (i >= k0 && i < k0 + kn) continue;
+            float* ai = M + (size_t)i * ld + k0;
+            float av[CS_BC_KB];
+#pragma unroll
+            for (int v = 0; v < CS_BC_KB; v++) av[v] = v < kn ? ai[v] : 0.f;
+#pragma unroll
+            for (int c = 0; c < CS_BC_KB; c++) {
+                if (c >= kn) break;
+                float x = 0.f;
+#pragma unroll
+                for (int v = 0; v < CS_BC_KB; v++)
+                    if (v < kn) x = __fmaf_rn(av[v], D[v * CS_BC_KB + c], x);
+                ai[c] = -x;
+            }
+        }
+        __syncthreads();
+    }
+    // written out symmetrised
+    float* out = B.cinv + (size_t)idx * B.res_cnc * B.res_cnc;
+    if (!bad)
+        for (int i = w; i < nc; i += nw)
+            for (int jj = lane; jj < nc; jj += 32) out[(size_t)i * nc + jj] = 0.5f * (M[(size_t)i * ld + jj] + M[(size_t)jj * ld + i]);
+    if (tid == 0) B.cvalid[idx] = bad ? 0 : 1;
+}

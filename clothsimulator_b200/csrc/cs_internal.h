@@ -4,18 +4,18 @@
 //   nodes   : x, v, dv as 3N floats (xyz interleaved), mass N, handle float4 N (xyz target,
 //             w = handle count), FP64 solution accumulator dv64 3N.
 //   faces   : int4 {n0, n1, n2, sheet} (global node ids), float4 inverse rest matrix
-//             (Face::inverse, Face.cu:16), rest area; one 384-byte element record per face.
+//             (Face::inverse, Face.cu:16), rest area.
 //   edges   : interior edges only (the reference skips boundary edges, Cloth.cu:142):
 //             int4 {n0, n1, opposite0, opposite1}, int meta (face-vertex rotations), sheet,
-//             float4 {area0 + area1, bias weight side 0, side 1, 0}; one 128-byte record.
+//             float4 {area0 + area1, bias weight side 0, side 1, 0}.
 //   system  : SELL-32 block layout.  A sheet's rows (nodes), sorted by block count within
 //             windows of sigma rows (sigma chosen per topology to minimise padding), are cut
 //             into slices of 32; slice s has `width` block slots per row (padded with zero
 //             blocks).  Slot (slice, k, lane) stores its 3x3 block in a "panel" of 32 lanes:
 //             entries 0-3 as float4[32], entries 4-7 as float4[32], entry 8 as float[32]
 //             (1152 bytes per panel, 128-bit coalesced loads).  Slot k = 0 is the diagonal.
-//             Column indices and the assembly contributor lists are per *topology* (shared
-//             by all sheets with identical connectivity) and hold sheet-local node ids.
+//             Column indices and the assembly's row lists are per *topology* (shared by all
+//             sheets with identical connectivity) and hold sheet-local ids.
 #ifndef CLOTHSTEP_CS_INTERNAL_H
 #define CLOTHSTEP_CS_INTERNAL_H
 
@@ -28,20 +28,15 @@
 #define CS_PANEL_FLOATS 288  // 32 lanes x 9 entries
 #define CS_TABLE_N 30
 #define CS_TABLE_ENTRIES (CS_TABLE_N * CS_TABLE_N * CS_TABLE_N)
-// Element records, laid out for 16-byte loads in the gather.  Face (120 floats): block
-// (a, b) of -dt^2 J at [12 (3a + b) + 3 kp + kq] (three float4, the last three floats zero);
-// dt (f + dt J v) of node a at [108 + 4a + kp]; wind force at [111], [115], [119].  Edge (32
-// floats): node i's (dtheta_i, coefficient) at [4i .. 4i + 3]; dt (f + dt J v) of node i at
-// [16 + 4i + c]; theta at [19].
-#define CS_FACE_REC 120
-#define CS_EDGE_REC 32
-
 // Contributor code: bit 31 = edge (1) / face (0); bits 4..30 = sheet-local element id;
 // bits 2..3 = local row corner a; bits 0..1 = local column corner b.
 #define CS_CODE_EDGE 0x80000000u
 __host__ __device__ inline uint32_t cs_code(int is_edge, int elem, int a, int b) {
     return (is_edge ? CS_CODE_EDGE : 0u) | ((uint32_t)elem << 4) | ((uint32_t)a << 2) | (uint32_t)b;
 }
+// Threads per CTA of the assembly gather (forces.cu); its slot accumulators take
+// 4 warps x gather_width x 1152 bytes of shared memory.
+#define CS_GATHER_THREADS 128
 
 struct SheetDesc {
     int node_off, n_nodes;
@@ -122,8 +117,13 @@ enum InstPhase : int {
 #define CS_BC_KB (3 * CS_BC_PB)
 #define CS_COARSE_MAX_K 8
 #define CS_COARSE_AGGS 54
-// Threads of the per-sheet set-up kernel that forms and inverts the coarse matrix.
+// Threads of the per-sheet set-up kernel that forms and inverts the coarse matrix, and its
+// dynamic shared memory: the nc x nc matrix with rows padded to 16 bytes, then one pivot block.
 #define CS_COARSE_THREADS 512
+__host__ __device__ inline int cs_coarse_ld(int nc) { return (nc + 3) & ~3; }
+__host__ __device__ inline size_t cs_coarse_setup_smem(int nc) {
+    return ((size_t)nc * cs_coarse_ld(nc) + CS_BC_KB * CS_BC_KB) * sizeof(float);
+}
 // Launch shapes of the batched SpMV that cs_tune times (pcg.cu, kSpmvShapes): threads per block,
 // slices per warp, block slots whose loads are issued together.
 struct SpmvShape {
@@ -230,20 +230,24 @@ struct Batch {
     int4* face_nodes = nullptr;
     float4* face_inv = nullptr;
     float* face_area = nullptr;
-    float* face_rec = nullptr;
     // edges
     int4* edge_nodes = nullptr;
     int* edge_meta = nullptr;
     int* edge_sheet = nullptr;
     float4* edge_par = nullptr;
-    float* edge_rec = nullptr;
     // sheets, materials, topology
     SheetDesc* sheets = nullptr;
     float4* tables = nullptr;
     SliceDesc* slices = nullptr;
     int* tcol = nullptr;         // per topology panel: 32 local column ids
-    int* tcptr = nullptr;        // per topology slot: contributor range start (n_tpanels*32 + 1)
-    uint32_t* tcontrib = nullptr;
+    // assembly row lists (forces.cu, cs_gather_kernel): per topology node (at row2slot_off),
+    // its (face << 2 | corner, slots of the face's corners) in face order and its (interior
+    // edge << 2 | corner, slots of the edge's four nodes) in edge order; slots 8 bits each
+    int* rface_ptr = nullptr;    // topology nodes of all topologies + 1
+    int2* rface = nullptr;
+    int* redge_ptr = nullptr;
+    int2* redge = nullptr;
+    int gather_width = 0;        // widest slice of the batch (the gather's accumulators per lane)
     int* nbr_ptr = nullptr;      // per topology: one-ring neighbour CSR (sheet-local ids)
     int* nbr = nullptr;
     int* node_sheet = nullptr;   // sheet of every node

@@ -33,8 +33,6 @@
 #include "mlp.h"
 
 // kernels (forces.cu, pcg.cu)
-__global__ void cs_face_kernel(Batch B);
-__global__ void cs_edge_kernel(Batch B);
 __global__ void cs_gather_kernel(Batch B);
 __global__ void cs_expand_kernel(Batch B, float* face_f, float* face_J, float* edge_f, float* edge_J);
 __global__ void cs_reduce1_kernel(Batch B);
@@ -206,6 +204,11 @@ struct Topo {
     // every edge (reference order): nodes, adjacent faces per side (-1: none); per face its
     // edges (v0 v1), (v1 v2), (v2 v0); per node its (face, corner) pairs in face order
     std::vector<int> e_nodes, e_faces, f_edges, nf_ptr, nf_code;
+    // assembly row lists: per node its (face << 2 | corner) in face order and its (interior
+    // edge << 2 | corner) in edge order, each with the slots (positions in the node's row) of
+    // the element's corners, 8 bits per corner
+    std::vector<int> rf_ptr, re_ptr;
+    std::vector<int2> rf, re;
     // rest (uv) coordinates of every node, from the first sheet of this connectivity: the
     // geometry the coarse-space segments of the cluster-resident solver are cut along
     std::vector<float> node_uv;
@@ -468,6 +471,48 @@ std::shared_ptr<Topo> buildTopo(const cs_sheet_desc& s, std::string& err) {
             }
     }
     t->tcptr[(size_t)tp * CS_SLICE] = (int)t->tcontrib.size();
+    // Row lists of the assembly gather.  Walking a row's faces, then its edges, in index order
+    // and adding each element's blocks onto the slots of its corners visits every block's
+    // contributors in the order of the lists above (faces by index, then edges, per element
+    // by corner).
+    {
+        auto slotIn = [&](int i, int j) {
+            const auto& cols = rowCols[i];
+            for (size_t k = 0; k < cols.size(); k++)
+                if (cols[k] == j) return (int)k;
+            return -1;
+        };
+        for (int i = 0; i < nn; i++)
+            if (rowCols[i].size() > 255) {
+                err = "a node couples to more than 255 nodes";
+                return nullptr;
+            }
+        t->rf_ptr.assign(nn + 1, 0);
+        t->rf.resize(3 * (size_t)nf);
+        for (int i = 0; i < nn; i++) {
+            t->rf_ptr[i + 1] = t->nf_ptr[i + 1];
+            for (int q = t->nf_ptr[i]; q < t->nf_ptr[i + 1]; q++) {
+                const int f = t->nf_code[q] >> 2;
+                int slots = 0;
+                for (int b = 0; b < 3; b++) slots |= slotIn(i, t->fx[3 * f + b]) << (8 * b);
+                t->rf[q] = make_int2(t->nf_code[q], slots);
+            }
+        }
+        std::vector<int> cntE(nn + 1, 0);
+        for (int e = 0; e < nie; e++)
+            for (int a = 0; a < 4; a++) cntE[t->ie_nodes[4 * e + a] + 1]++;
+        for (int i = 0; i < nn; i++) cntE[i + 1] += cntE[i];
+        t->re_ptr = cntE;
+        t->re.resize(4 * (size_t)nie);
+        std::vector<int> fillE(cntE.begin(), cntE.end() - 1);
+        for (int e = 0; e < nie; e++)
+            for (int a = 0; a < 4; a++) {
+                const int i = t->ie_nodes[4 * e + a];
+                int slots = 0;
+                for (int b = 0; b < 4; b++) slots |= slotIn(i, t->ie_nodes[4 * e + b]) << (8 * b);
+                t->re[fillE[i]++] = make_int2((e << 2) | a, slots);
+            }
+    }
     // block-CSR view
     t->csr_ptr.assign(nn + 1, 0);
     t->csr_col.clear();
@@ -866,6 +911,7 @@ struct cs_ctx {
     bool lastStepValid = false;
     long long steps = 0, hostLaunches = 0, graphSteps = 0, graphLaunchesFixed = 0;
     int gatherGrid = 1;  // persistent assembly gather: a few warps per SM walk the slices
+    size_t gatherSmem = 0;  // its dynamic shared memory (slot accumulators)
     // learned warm start
     MlpDev mlp;
     bool mlpInit = false;
@@ -988,9 +1034,7 @@ inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 int launchAssembly(cs_ctx* c) {
     Batch& B = c->B;
     int n = 1;
-    if (B.F) cs_face_kernel<<<nblk(B.F, 64), 64, 0, c->stream>>>(B), n++;
-    if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B), n++;
-    cs_gather_kernel<<<c->gatherGrid, 128, 0, c->stream>>>(B);
+    cs_gather_kernel<<<c->gatherGrid, CS_GATHER_THREADS, c->gatherSmem, c->stream>>>(B);
     if (B.n_pinst > 0) {
         // proximity terms after the handles (Cloth.cu:676-684): records, then per row the
         // blocks, right-hand side and block-Jacobi inverse, then the ||b|| partials
@@ -1075,8 +1119,7 @@ void launchSolvePrologueAgain(cs_ctx* c) {
 // kernel returns at once unless the step asks for the coarse correction).
 void launchCoarseSetup(cs_ctx* c) {
     if (c->resClusters > 0 && c->B.res_cnc > 0 && c->B.n_resident > 0)
-        cs_coarse_setup_kernel<<<c->B.n_resident, CS_COARSE_THREADS,
-                                 (size_t)(c->B.res_cnc + 4) * c->B.res_cnc * sizeof(float), c->stream>>>(c->B);
+        cs_coarse_setup_kernel<<<c->B.n_resident, CS_COARSE_THREADS, cs_coarse_setup_smem(c->B.res_cnc), c->stream>>>(c->B);
 }
 
 void launchResident(cs_ctx* c, bool setup = true) {
@@ -1312,8 +1355,9 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     std::vector<SheetDesc> hs(n_sheets);
     std::vector<SliceDesc> hslices;
     // per-topology arrays, concatenated
-    std::vector<int> htcol, htcptr;
-    std::vector<uint32_t> htcontrib;
+    std::vector<int> htcol, hrface_ptr, hredge_ptr;
+    std::vector<int2> hrface, hredge;
+    int gatherWidth = 1;
     std::vector<int> hnbr_ptr, hnbr, hnode_sheet, hrowmap, hrow2slot;
     std::vector<int> topoRow2Slot0(topos.size());
     std::vector<int> topoNbrPtr0(topos.size()), topoNbr0(topos.size());
@@ -1510,7 +1554,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         B.res_cnc = 3 * res.cl * res.ck;
         B.res_coff = (int)(res.smem - coarseSmemBytes(res.cl, res.ck));
         CS_CUDA(cudaFuncSetAttribute(cs_coarse_setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (B.res_cnc + 4) * B.res_cnc * (int)sizeof(float)));
+                                     (int)cs_coarse_setup_smem(B.res_cnc)));
     }
     if (res.clusters > 0) {
         // the launch attributes of the chosen plan (the evaluation set others)
@@ -1526,7 +1570,6 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             topoPanel0[t] = tp;
             topoSlice0[t] = ts;
             const Topo& T = *topos[t];
-            int cbase = (int)htcontrib.size();
             htcol.insert(htcol.end(), T.tcol.begin(), T.tcol.end());
             if (topoResident[t]) {
                 // halo slots follow the batch's own slots in every CTA's p array
@@ -1538,8 +1581,13 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             } else {
                 hrcode.insert(hrcode.end(), T.tcol.size(), 0);
             }
-            for (size_t i = 0; i + 1 < T.tcptr.size(); i++) htcptr.push_back(T.tcptr[i] + cbase);
-            htcontrib.insert(htcontrib.end(), T.tcontrib.begin(), T.tcontrib.end());
+            // the gather's row lists at the row2slot offsets (node-indexed; the next topology's
+            // first pointer ends this one's last row)
+            for (int i = 0; i < T.n_nodes; i++) hrface_ptr.push_back(T.rf_ptr[i] + (int)hrface.size());
+            for (int i = 0; i < T.n_nodes; i++) hredge_ptr.push_back(T.re_ptr[i] + (int)hredge.size());
+            hrface.insert(hrface.end(), T.rf.begin(), T.rf.end());
+            hredge.insert(hredge.end(), T.re.begin(), T.re.end());
+            for (int w : T.slice_width) gatherWidth = std::max(gatherWidth, w);
             hrowmap.insert(hrowmap.end(), T.rowmap.begin(), T.rowmap.end());
             topoRow2Slot0[t] = (int)hrow2slot.size();
             hrow2slot.insert(hrow2slot.end(), T.row2slot.begin(), T.row2slot.end());
@@ -1554,7 +1602,10 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
             tp += T.n_tpanels;
             ts += T.n_slices;
         }
-        htcptr.push_back((int)htcontrib.size());
+        hrface_ptr.push_back((int)hrface.size());
+        hredge_ptr.push_back((int)hredge.size());
+        if (hrface.empty()) hrface.push_back(make_int2(0, 0));
+        if (hredge.empty()) hredge.push_back(make_int2(0, 0));
     }
     int node_off = 0, face_off = 0, edge_off = 0, slice_off = 0, panel_off = 0;
     long long nnzb = 0;
@@ -1730,8 +1781,11 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     UP(tables, tables);
     UP(slices, hslices);
     UP(tcol, htcol);
-    UP(tcptr, htcptr);
-    UP(tcontrib, htcontrib);
+    UP(rface_ptr, hrface_ptr);
+    UP(redge_ptr, hredge_ptr);
+    UP(rface, hrface);
+    UP(redge, hredge);
+    B.gather_width = gatherWidth;
     UP(nbr_ptr, hnbr_ptr);
     UP(nbr, hnbr);
     UP(node_sheet, hnode_sheet);
@@ -1775,8 +1829,6 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     AL(x0, 3LL * B.N);
     AL(dv64, 3LL * B.N);
     AL(warm, 3LL * B.N);
-    AL(face_rec, (long long)B.F * CS_FACE_REC);
-    AL(edge_rec, (long long)std::max(B.E, 1) * CS_EDGE_REC);
     AL(A, (long long)B.n_panels * CS_PANEL_FLOATS);
     AL(b, 3LL * B.N);
     AL(Pinv, 9LL * B.N);
@@ -1803,11 +1855,17 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     {
         cudaDeviceProp prop;
         CS_CUDA(cudaGetDeviceProperties(&prop, c->device));
-        // persistent gather: CTAs per SM (CS_GATHER_CTAS_PER_SM, 1..16) bound the slices in
-        // flight, so the element records they read stay in L2
-        int perSM = 4;
-        if (const char* ev = std::getenv("CS_GATHER_CTAS_PER_SM")) perSM = std::min(16, std::max(1, std::atoi(ev)));
-        c->gatherGrid = std::max(1, std::min(nblk((long long)B.n_slices * 32, 128), perSM * prop.multiProcessorCount));
+        // persistent gather: as many CTAs per SM as its slot accumulators allow (at most
+        // CS_GATHER_CTAS_PER_SM, 1..16, when set)
+        c->gatherSmem = (size_t)(CS_GATHER_THREADS / 32) * B.gather_width * 9 * CS_SLICE * sizeof(float);
+        if (c->gatherSmem > (size_t)prop.sharedMemPerBlockOptin)
+            return fail(c, CS_ERR_INVALID_ARG, "slices of %d block slots exceed the assembly's shared memory", B.gather_width);
+        CS_CUDA(cudaFuncSetAttribute(cs_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->gatherSmem));
+        int perSM = 0;
+        CS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, cs_gather_kernel, CS_GATHER_THREADS, c->gatherSmem));
+        if (const char* ev = std::getenv("CS_GATHER_CTAS_PER_SM")) perSM = std::min(perSM, std::min(16, std::max(1, std::atoi(ev))));
+        perSM = std::max(perSM, 1);
+        c->gatherGrid = std::max(1, std::min(nblk((long long)B.n_slices * 32, CS_GATHER_THREADS), perSM * prop.multiProcessorCount));
     }
     c->loaded = true;
     return CS_OK;
@@ -2753,9 +2811,7 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
         cudaEventRecord(c->ev0, c->stream);
         for (int r = 0; r < reps; r++) {
             switch (which) {
-                case 0: if (B.F) cs_face_kernel<<<nblk(B.F, 64), 64, 0, c->stream>>>(B); break;
-                case 1: if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B); break;
-                case 2: cs_gather_kernel<<<c->gatherGrid, 128, 0, c->stream>>>(B); break;
+                case 2: cs_gather_kernel<<<c->gatherGrid, CS_GATHER_THREADS, c->gatherSmem, c->stream>>>(B); break;
                 case 3: launchSpmvShape(B, c->spmvShape, c->stream); break;
                 case 4: cs_vector_kernel<<<g, 128, 0, c->stream>>>(B); break;
                 case 5: cs_reduce1_kernel<<<B.S, CS_REDUCE_THREADS, 0, c->stream>>>(B); break;
@@ -2768,7 +2824,9 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
         cudaEventElapsedTime(&t, c->ev0, c->ev1);
         return t / reps;
     };
-    for (int k = 0; k < 3; k++) ms[k] = timeIt(k);
+    // the element terms are evaluated inside the gather: entries 0 and 1 stay 0
+    ms[0] = ms[1] = 0.f;
+    ms[2] = timeIt(2);
     // solver kernels with every instance held in one phase
     cs_solve_setup_kernel<<<B.S, 128, 0, c->stream>>>(B);
     cs_solve_prologue_kernel<<<nblk(3LL * B.N, 256), 256, 0, c->stream>>>(B);

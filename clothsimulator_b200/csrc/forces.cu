@@ -6,15 +6,15 @@
 // reference's CPU assembly entry by entry.
 //
 // Kernels:
-//   cs_face_kernel   one thread per face: normal, wind drag, stretching force, its 9x9
-//                    contribution -dt^2 J to A and the face's right-hand-side terms.
-//   cs_edge_kernel   one thread per interior edge: dihedral bending force, the rank-one
-//                    Jacobian factors (dtheta, coefficient) and the edge's right-hand side.
-//   cs_gather_kernel one warp per 32-row slice: every block (i, j) of A sums its
-//                    contributors in the reference's order (mass, faces by index, edges by
-//                    index, handles) from a precomputed per-topology list: no atomics, no
-//                    sort, bit-reproducible.  Diagonal slots also produce b, the 3x3
-//                    block-Jacobi inverse and the slice's ||b||^2.
+//   cs_gather_kernel one warp per 32-row slice, lane = row: the row's own rows of the
+//                    stretching terms of its faces and of the bending terms of its interior
+//                    edges, summed into every block (i, j) of A in the reference's order (mass,
+//                    faces by index, edges by index, handles) in shared memory: no atomics, no
+//                    sort, no element records, bit-reproducible.  Also b, the 3x3 block-Jacobi
+//                    inverse and the slice's ||b||^2.
+//   cs_expand_kernel the per-element f and J as the reference's force functions return them
+//                    (inspection).
+//   cs_prox_kernel, cs_prox_row_kernel  proximity terms on top of the assembled system.
 #include "cs_internal.h"
 
 namespace {
@@ -179,40 +179,25 @@ __device__ __forceinline__ float stretch_h(float fu_p, float fv_p, float fu_q, f
 
 }  // namespace
 
-// Face record (CS_FACE_REC = 120 floats, 16-byte aligned pieces for the gather's vector
-// loads): the face's 9x9 contribution to A, -dt*dt*J, as nine row-major 3x3 blocks (block
-// (a, b) at 12 (3a + b), three zero floats after each), dt*(f + dt*J*v) of the stretching
-// term for node a at 108 + 4a .. 108 + 4a + 2, and dt * wind force added to each node at
-// 111, 115, 119.
-//
-// face_eval evaluates one face exactly as Face::update (normal), the wind loop of
-// Cloth::addExternalForces and stretchingForce (PhysicsHelper.cu:264-291) do.  With
-// rec != nullptr it writes the face record; with fo/Jo it writes f and J as stretchingForce
-// returns them (the inspection path).
-__device__ __forceinline__ void face_eval(const Batch& B, int f, float* __restrict__ rec, float* __restrict__ fo,
-                                          float* __restrict__ Jo) {
-    const DevParams& P = *B.params;
-    const float dt = P.dt;
-    const float s = -dt * dt;
-    int4 fn = B.face_nodes[f];
+namespace {
+
+// One face's stretching terms: the state its rows share (stretchingForce's set-up,
+// PhysicsHelper.cu:264-281, with F from Face.cu:109-111), then one row p = 3a + kp at a time.
+struct FaceState {
+    float area;
+    float G00, G01, G11, gu, gv;
+    float4 k;
+    float D0[3], D1[3], fu[3], fv[3], vel[9];
+};
+
+__device__ __forceinline__ void face_setup(const Batch& B, int f, FaceState& S) {
+    const int4 fn = B.face_nodes[f];
     const SheetDesc& sh = B.sheets[fn.w];
-    f3 x0 = ld3(B.x, fn.x), x1 = ld3(B.x, fn.y), x2 = ld3(B.x, fn.z);
-    f3 v0 = ld3(B.v, fn.x), v1 = ld3(B.v, fn.y), v2 = ld3(B.v, fn.z);
-    float area = B.face_area[f];
-    float4 inv = B.face_inv[f];  // (00, 01, 10, 11)
-
-    // Face::update (Face.cu:124-127): normal from the current positions.
-    f3 e1 = sub(x1, x0), e2 = sub(x2, x0);
-    f3 n = normalized(cross(e1, e2));
-
-    // Wind drag (Cloth.cu:105-122), on the rest area of a free face.
-    f3 avg = dvd(add(add(v0, v1), v2), 3.0f);
-    f3 rel = sub(mk(sh.wind_v[0], sh.wind_v[1], sh.wind_v[2]), avg);
-    float vn = dot(n, rel);
-    f3 vt = sub(rel, scl(vn, n));
-    f3 force = dvd(scl(area, add(scl(sh.wind_density * absf_(vn) * vn, n), scl(sh.wind_drag, vt))), 3.0f);
-    f3 fw = scl(dt, force);
-
+    const f3 x0 = ld3(B.x, fn.x), x1 = ld3(B.x, fn.y), x2 = ld3(B.x, fn.z);
+    const f3 v0 = ld3(B.v, fn.x), v1 = ld3(B.v, fn.y), v2 = ld3(B.v, fn.z);
+    S.area = B.face_area[f];
+    const float4 inv = B.face_inv[f];  // (00, 01, 10, 11)
+    const f3 e1 = sub(x1, x0), e2 = sub(x2, x0);
     // F = [x1 - x0, x2 - x0] * inverse (Face.cu:109-111), G = (F^T F - I) / 2
     float F[3][2];
     {
@@ -234,79 +219,90 @@ __device__ __forceinline__ void face_eval(const Batch& B, int f, float* __restri
     FtF00 += F[2][0] * F[2][0];
     FtF01 += F[2][0] * F[2][1];
     FtF11 += F[2][1] * F[2][1];
-    float G00 = 0.5f * (FtF00 - 1.0f), G01 = 0.5f * (FtF01 - 0.0f), G11 = 0.5f * (FtF11 - 1.0f);
-    float4 k = stretch_stiffness(B.tables + (size_t)sh.table * CS_TABLE_ENTRIES, G00, G01, G11);
-    const float gu = maxf_(G00, 0.0f), gv = maxf_(G11, 0.0f);
+    S.G00 = 0.5f * (FtF00 - 1.0f);
+    S.G01 = 0.5f * (FtF01 - 0.0f);
+    S.G11 = 0.5f * (FtF11 - 1.0f);
+    S.k = stretch_stiffness(B.tables + (size_t)sh.table * CS_TABLE_ENTRIES, S.G00, S.G01, S.G11);
+    S.gu = maxf_(S.G00, 0.0f);
+    S.gv = maxf_(S.G11, 0.0f);
     // D = [-Y.row0 - Y.row1, Y.row0, Y.row1] as columns (PhysicsHelper.cu:268-271)
-    const float D0[3] = {-inv.x - inv.z, inv.x, inv.z};
-    const float D1[3] = {-inv.y - inv.w, inv.y, inv.w};
-    const float fu[3] = {F[0][0], F[1][0], F[2][0]};
-    const float fv[3] = {F[0][1], F[1][1], F[2][1]};
+    S.D0[0] = -inv.x - inv.z;
+    S.D0[1] = inv.x;
+    S.D0[2] = inv.z;
+    S.D1[0] = -inv.y - inv.w;
+    S.D1[1] = inv.y;
+    S.D1[2] = inv.w;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        S.fu[i] = F[i][0];
+        S.fv[i] = F[i][1];
+    }
     const float vel[9] = {v0.x, v0.y, v0.z, v1.x, v1.y, v1.z, v2.x, v2.y, v2.z};
 #pragma unroll
-    for (int p = 0; p < 9; p++) {
-        const int a = p / 3, kp = p % 3;
-        const float fuu = D0[a] * fu[kp], fvv = D1[a] * fv[kp], fuv = 0.5f * (D0[a] * fv[kp] + D1[a] * fu[kp]);
-        // grad with the expression order of PhysicsHelper.cu:282; f = -area * grad
-        float g = k.x * G00 * fuu;
-        g += k.z * G11 * fvv;
-        g += k.y * (G00 * fvv + G11 * fuu);
-        g += 2.0f * k.w * G01 * fuv;
-        const float fp = -area * g;
-        float jv = 0.0f;
-#pragma unroll
-        for (int q = 0; q < 9; q++) {
-            const int b = q / 3, kq = q % 3;
-            const float h = stretch_h(fu[kp], fv[kp], fu[kq], fv[kq], D0[a], D1[a], D0[b], D1[b], k.x, k.y, k.z, k.w,
-                                      gu, gv, kp == kq);
-            const float J = -area * h;
-            jv += (dt * J) * vel[q];
-            if (rec) rec[12 * (3 * a + b) + 3 * kp + kq] = s * J;  // block (a, b): three float4
-            if (Jo) Jo[9 * p + q] = J;
-        }
-        if (rec) rec[108 + 4 * a + kp] = dt * (fp + jv);
-        if (fo) fo[p] = fp;
-    }
-    if (rec) {
-#pragma unroll
-        for (int blk = 0; blk < 9; blk++) rec[12 * blk + 9] = rec[12 * blk + 10] = rec[12 * blk + 11] = 0.0f;
-        rec[111] = fw.x;
-        rec[115] = fw.y;
-        rec[119] = fw.z;
-    }
+    for (int i = 0; i < 9; i++) S.vel[i] = vel[i];
 }
 
-// One thread per face; the block's records are staged in shared memory (row stride 121 floats,
-// conflict-free) and written out as one contiguous, coalesced range.
-__global__ void __launch_bounds__(64) cs_face_kernel(Batch B) {
-    constexpr int kStride = CS_FACE_REC + 1;
-    __shared__ float stage[64 * kStride];
-    const int f0 = blockIdx.x * blockDim.x;
-    const int f = f0 + threadIdx.x;
-    if (f < B.F) face_eval(B, f, stage + threadIdx.x * kStride, nullptr, nullptr);
-    __syncthreads();
-    const int nf = min((int)blockDim.x, B.F - f0);
-    float* out = B.face_rec + (size_t)f0 * CS_FACE_REC;
-    for (int e = threadIdx.x; e < nf * CS_FACE_REC; e += blockDim.x)
-        out[e] = stage[(e / CS_FACE_REC) * kStride + e % CS_FACE_REC];
+// Row p = 3a + kp of the face's stretching terms: f_p (returned in fp) and, for each column
+// q, J(p, q) handed to emit(q, J) in column order; returns dt (f_p + dt sum_q J(p, q) v_q), the
+// row's right-hand-side term, with the reference's operation order (PhysicsHelper.cu:282-290).
+template <class Emit>
+__device__ __forceinline__ float face_row(const FaceState& S, int p, float dt, float& fp, Emit emit) {
+    const int a = p / 3, kp = p % 3;
+    // the row's corner and component by selects (no indexed local arrays)
+    const float D0a = a == 0 ? S.D0[0] : (a == 1 ? S.D0[1] : S.D0[2]);
+    const float D1a = a == 0 ? S.D1[0] : (a == 1 ? S.D1[1] : S.D1[2]);
+    const float fup = kp == 0 ? S.fu[0] : (kp == 1 ? S.fu[1] : S.fu[2]);
+    const float fvp = kp == 0 ? S.fv[0] : (kp == 1 ? S.fv[1] : S.fv[2]);
+    const float fuu = D0a * fup, fvv = D1a * fvp, fuv = 0.5f * (D0a * fvp + D1a * fup);
+    // grad with the expression order of PhysicsHelper.cu:282; f = -area * grad
+    float g = S.k.x * S.G00 * fuu;
+    g += S.k.z * S.G11 * fvv;
+    g += S.k.y * (S.G00 * fvv + S.G11 * fuu);
+    g += 2.0f * S.k.w * S.G01 * fuv;
+    fp = -S.area * g;
+    float jv = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+        const int b = q / 3, kq = q % 3;
+        const float h = stretch_h(fup, fvp, S.fu[kq], S.fv[kq], D0a, D1a, S.D0[b], S.D1[b], S.k.x, S.k.y, S.k.z, S.k.w, S.gu,
+                                  S.gv, kp == kq);
+        const float J = -S.area * h;
+        jv += (dt * J) * S.vel[q];
+        emit(q, J);
+    }
+    return dt * (fp + jv);
 }
 
-// Edge record (32 floats): node i's (dtheta_i, coefficient) at [4i .. 4i + 3], dt*(f + dt*J*v)
-// of the bending term for node i at [16 + 4i .. 16 + 4i + 2], theta at [19].
-__global__ void __launch_bounds__(128) cs_edge_kernel(Batch B) {
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= B.E) return;
-    const DevParams& P = *B.params;
-    const float dt = P.dt;
-    int4 en = B.edge_nodes[e];
-    int meta = B.edge_meta[e];
+// dt times the wind drag on each node of a face (Cloth.cu:105-122) on its rest area, from the
+// normal of the current positions (Face::update, Face.cu:124-127).
+__device__ __forceinline__ f3 face_wind(const Batch& B, int f, float dt) {
+    const int4 fn = B.face_nodes[f];
+    const SheetDesc& sh = B.sheets[fn.w];
+    const f3 x0 = ld3(B.x, fn.x), x1 = ld3(B.x, fn.y), x2 = ld3(B.x, fn.z);
+    const f3 v0 = ld3(B.v, fn.x), v1 = ld3(B.v, fn.y), v2 = ld3(B.v, fn.z);
+    const float area = B.face_area[f];
+    const f3 n = normalized(cross(sub(x1, x0), sub(x2, x0)));
+    const f3 avg = dvd(add(add(v0, v1), v2), 3.0f);
+    const f3 rel = sub(mk(sh.wind_v[0], sh.wind_v[1], sh.wind_v[2]), avg);
+    const float vn = dot(n, rel);
+    const f3 vt = sub(rel, scl(vn, n));
+    const f3 force = dvd(scl(area, add(scl(sh.wind_density * absf_(vn) * vn, n), scl(sh.wind_drag, vt))), 3.0f);
+    return scl(dt, force);
+}
+
+// Dihedral bending of one interior edge (bendingForce, PhysicsHelper.cu:327-353, with the
+// adjacent face normals of Face.cu:124-127 and the bending stiffness of Material.cu:126-156):
+// the gradient dtheta (4 nodes x 3), the coefficient of the rank-one Jacobian
+// coef dtheta dtheta^T and the angle theta; f = coef theta dtheta.
+__device__ __forceinline__ void edge_geom(const Batch& B, int e, float (&dth)[12], float& coef, float& angle) {
+    const int4 en = B.edge_nodes[e];
+    const int meta = B.edge_meta[e];
     const SheetDesc& sh = B.sheets[B.edge_sheet[e]];
-    float4 par = B.edge_par[e];
-    f3 x0 = ld3(B.x, en.x), x1 = ld3(B.x, en.y), x2 = ld3(B.x, en.z), x3 = ld3(B.x, en.w);
-
-    // Adjacent face normals with each face's own vertex order (Face.cu:124-127).
-    // Face 0's cyclic vertex order is a rotation of (x0, x1, opposite0), face 1's of
-    // (x1, x0, opposite1); meta holds the two rotations.
+    const float4 par = B.edge_par[e];
+    const f3 x0 = ld3(B.x, en.x), x1 = ld3(B.x, en.y), x2 = ld3(B.x, en.z), x3 = ld3(B.x, en.w);
+    // Adjacent face normals with each face's own vertex order (Face.cu:124-127).  Face 0's
+    // cyclic vertex order is a rotation of (x0, x1, opposite0), face 1's of (x1, x0,
+    // opposite1); meta holds the two rotations.
     f3 n0, n1;
     {
         int r = meta & 3;
@@ -320,18 +316,16 @@ __global__ void __launch_bounds__(128) cs_edge_kernel(Batch B) {
         c = r == 0 ? x3 : (r == 1 ? x1 : x0);
         n1 = normalized(cross(sub(b, a), sub(c, a)));
     }
-    // bendingForce (PhysicsHelper.cu:327-353)
-    float length = nrm(sub(x1, x0));
-    float angle;
+    const float length = nrm(sub(x1, x0));
     {
         f3 ee = normalized(sub(x0, x1));
         float sine = dot(ee, cross(n0, n1));
         float cosine = dot(n0, n1);
         angle = (float)atan2((double)sine, (double)cosine);
     }
-    float area = par.x;
-    f3 ed = sub(x1, x0);
-    float en2 = dot(ed, ed);
+    const float area = par.x;
+    const f3 ed = sub(x1, x0);
+    const float en2 = dot(ed, ed);
     float h0, h1, w00, w01, w10, w11;
     {
         f3 t = sub(x2, x0);
@@ -349,172 +343,156 @@ __global__ void __launch_bounds__(128) cs_edge_kernel(Batch B) {
         w10 = 1.0f - tt;
         w11 = tt;
     }
-    f3 a0 = sub(dvd(scl(-w00, n0), h0), dvd(scl(w10, n1), h1));
-    f3 a1 = sub(dvd(scl(-w01, n0), h0), dvd(scl(w11, n1), h1));
-    f3 a2 = dvd(n0, h0);
-    f3 a3 = dvd(n1, h1);
-    float dth[12] = {a0.x, a0.y, a0.z, a1.x, a1.y, a1.z, a2.x, a2.y, a2.z, a3.x, a3.y, a3.z};
-    float k0 = bend_stiffness(sh.bending, length, angle, area, par.y);
-    float k1 = bend_stiffness(sh.bending, length, angle, area, par.z);
-    float coef = -0.25f * minf_(k0, k1) * (length * length) / area;
-    float ca = coef * angle;
-
-    f3 v0 = ld3(B.v, en.x), v1 = ld3(B.v, en.y), v2 = ld3(B.v, en.z), v3 = ld3(B.v, en.w);
-    float vel[12] = {v0.x, v0.y, v0.z, v1.x, v1.y, v1.z, v2.x, v2.y, v2.z, v3.x, v3.y, v3.z};
-    float bb[12];
+    const f3 a0 = sub(dvd(scl(-w00, n0), h0), dvd(scl(w10, n1), h1));
+    const f3 a1 = sub(dvd(scl(-w01, n0), h0), dvd(scl(w11, n1), h1));
+    const f3 a2 = dvd(n0, h0);
+    const f3 a3 = dvd(n1, h1);
+    const float d[12] = {a0.x, a0.y, a0.z, a1.x, a1.y, a1.z, a2.x, a2.y, a2.z, a3.x, a3.y, a3.z};
 #pragma unroll
-    for (int p = 0; p < 12; p++) {
-        float jv = 0.0f;
-#pragma unroll
-        for (int q = 0; q < 12; q++) jv += (dt * (coef * (dth[p] * dth[q]))) * vel[q];
-        bb[p] = dt * (ca * dth[p] + jv);
-    }
-    float4* out = reinterpret_cast<float4*>(B.edge_rec + (size_t)e * CS_EDGE_REC);
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        out[i] = make_float4(dth[3 * i], dth[3 * i + 1], dth[3 * i + 2], coef);
-        out[4 + i] = make_float4(bb[3 * i], bb[3 * i + 1], bb[3 * i + 2], i == 0 ? angle : 0.0f);
-    }
+    for (int i = 0; i < 12; i++) dth[i] = d[i];
+    const float k0 = bend_stiffness(sh.bending, length, angle, area, par.y);
+    const float k1 = bend_stiffness(sh.bending, length, angle, area, par.z);
+    coef = -0.25f * minf_(k0, k1) * (length * length) / area;
 }
 
-// Assembly gather.  Warps walk the slices grid-stride (a persistent launch of a few warps per
-// SM), so the slices in flight at any moment cover a few sheets and their element records
-// stay in L2.  Lane = row.  For every block slot the contributors are summed in the
-// reference's order; their codes and record values are fetched four at a time so several
-// loads are in flight before the ordered additions.  Writes A's panels, and for the
-// diagonal slot b, the block-Jacobi inverse and the slice's ||b||^2 (part[2*slice]).
-__global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
+}  // namespace
+
+// Assembly.  Warps walk the slices grid-stride (a persistent launch); lane = row.  Each row
+// evaluates its own rows of the stretching terms of its faces and of the bending terms of its
+// interior edges (the element arithmetic of face_row and edge_geom, shared with the inspection
+// kernel below), and adds each block into the row's slot accumulators in shared memory:
+// faces in index order, then edges in index order, after the mass and before the handles, so
+// every block (i, j) sums its contributors in the reference's order (Cloth.cu:78-169) with no
+// atomics and no element records in memory.  b follows the reference's order too: gravity,
+// wind (faces), stretching (faces), bending (edges), handles (Cloth.cu:94-169).  A face is
+// evaluated by each of its three corner rows (a third of its rows each) and an edge's
+// gradient by each of its four nodes' rows.  Writes A's panels, b, the block-Jacobi inverse
+// of the diagonal block and the slice's ||b||^2 (part[2*slice]).
+//
+// Dynamic shared memory: per warp gather_width slots x 9 entries x 32 lanes, entry e of slot k
+// of a lane at [(9 k + e) * 32 + lane] (each lane touches only its own words: no conflicts).
+// Row lists (per topology node, at its sheet's row2slot_off): rface = {face << 2 | corner,
+// the row's slots of the face's corners 0..2, 8 bits each}, redge likewise for the interior
+// edges' corners 0..3.
+extern __shared__ float cs_gather_acc[];
+
+__global__ void __launch_bounds__(CS_GATHER_THREADS) cs_gather_kernel(Batch B) {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     const DevParams& P = *B.params;
     const float dt = P.dt;
     const float s = -dt * dt;
+    float* const acc = cs_gather_acc + (size_t)(threadIdx.x >> 5) * B.gather_width * 9 * CS_SLICE + lane;
     for (int slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; slice < B.n_slices; slice += warps) {
         const SliceDesc sd = B.slices[slice];
         const SheetDesc& sh = B.sheets[sd.sheet];
         const bool live = lane < sd.rows;
-        const int row = sd.row0 + (live ? B.rowmap[sd.topo_slice * CS_SLICE + lane] : 0);
-        const float* __restrict__ frec = B.face_rec + (size_t)sh.face_off * CS_FACE_REC;
-        const float* __restrict__ erec = B.edge_rec + (size_t)sh.edge_off * CS_EDGE_REC;
-        double bsq = 0.0;
-        for (int k = 0; k < sd.width; k++) {
-            const int tslot = (sd.tpanel0 + k) * CS_SLICE + lane;
-            float a[9];
+        const int lrow = live ? B.rowmap[sd.topo_slice * CS_SLICE + lane] : 0;
+        const int row = sd.row0 + lrow;
+        const float m = live ? B.mass[row] : 0.0f;
+        for (int k = 0; k < sd.width; k++)
 #pragma unroll
-            for (int t = 0; t < 9; t++) a[t] = 0.0f;
-            int c0 = 0, c1 = 0;
-            if (live) {
-                if (k == 0) {
-                    const float m = B.mass[row];
-                    a[0] = m; a[4] = m; a[8] = m;
+            for (int e = 0; e < 9; e++) acc[(9 * k + e) * CS_SLICE] = (k == 0 && (e & 3) == 0) ? m : 0.0f;
+        float b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;
+        if (live) {
+            const int base = sh.row2slot_off + lrow;
+            const int f0 = __ldg(&B.rface_ptr[base]), f1 = __ldg(&B.rface_ptr[base + 1]);
+            const int e0 = __ldg(&B.redge_ptr[base]), e1 = __ldg(&B.redge_ptr[base + 1]);
+            b0 += (dt * m) * P.gravity[0];
+            b1 += (dt * m) * P.gravity[1];
+            b2 += (dt * m) * P.gravity[2];
+            for (int t = f0; t < f1; t++) {
+                const f3 w = face_wind(B, sh.face_off + (__ldg(&B.rface[t].x) >> 2), dt);
+                b0 += w.x;
+                b1 += w.y;
+                b2 += w.z;
+            }
+            for (int t = f0; t < f1; t++) {
+                const int2 c = __ldg(&B.rface[t]);
+                FaceState S;
+                face_setup(B, sh.face_off + (c.x >> 2), S);
+                const int a = c.x & 3;
+                float r[3];
+#pragma unroll
+                for (int kp = 0; kp < 3; kp++) {
+                    float fp;
+                    r[kp] = face_row(S, 3 * a + kp, dt, fp, [&](int q, float J) {
+                        acc[(9 * ((c.y >> (8 * (q / 3))) & 0xff) + 3 * kp + q % 3) * CS_SLICE] += s * J;
+                    });
                 }
-                c0 = __ldg(&B.tcptr[tslot]);
-                c1 = __ldg(&B.tcptr[tslot + 1]);
-                for (int c = c0; c < c1; c += 4) {
-                    uint32_t code[4];
-                    float v[4][9];
+                b0 += r[0];
+                b1 += r[1];
+                b2 += r[2];
+            }
+            for (int t = e0; t < e1; t++) {
+                const int2 c = __ldg(&B.redge[t]);
+                const int e = sh.edge_off + (c.x >> 2), a = c.x & 3;
+                float dth[12], coef, angle;
+                edge_geom(B, e, dth, coef, angle);
+                // the row's node's gradient by selects (no indexed local arrays)
+                float da[3];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) code[j] = (c + j < c1) ? __ldg(&B.tcontrib[c + j]) : 0u;
+                for (int kk = 0; kk < 3; kk++)
+                    da[kk] = a == 0 ? dth[kk] : (a == 1 ? dth[3 + kk] : (a == 2 ? dth[6 + kk] : dth[9 + kk]));
+                // the row's rank-one blocks (a, b), b = 0..3, onto their slots
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        if (c + j >= c1) continue;
-                        const int elem = (int)((code[j] >> 4) & 0x7FFFFFFu);
-                        const int ca = (code[j] >> 2) & 3, cb = code[j] & 3;
-                        if (!(code[j] & CS_CODE_EDGE)) {
-                            const float4* r = reinterpret_cast<const float4*>(frec + (size_t)elem * CS_FACE_REC +
-                                                                              12 * (3 * ca + cb));
-                            const float4 q0 = __ldg(r), q1 = __ldg(r + 1), q2 = __ldg(r + 2);
-                            v[j][0] = q0.x; v[j][1] = q0.y; v[j][2] = q0.z; v[j][3] = q0.w;
-                            v[j][4] = q1.x; v[j][5] = q1.y; v[j][6] = q1.z; v[j][7] = q1.w;
-                            v[j][8] = q2.x;
-                        } else {
-                            const float4* r = reinterpret_cast<const float4*>(erec + (size_t)elem * CS_EDGE_REC);
-                            const float4 qa = __ldg(r + ca), qb = __ldg(r + cb);
-                            const float coef = qa.w;
-                            const float da[3] = {qa.x, qa.y, qa.z}, db[3] = {qb.x, qb.y, qb.z};
+                for (int bb = 0; bb < 4; bb++) {
+                    float* d = acc + 9 * ((c.y >> (8 * bb)) & 0xff) * CS_SLICE;
 #pragma unroll
-                            for (int kk = 0; kk < 3; kk++)
+                    for (int kk = 0; kk < 3; kk++)
 #pragma unroll
-                                for (int hh = 0; hh < 3; hh++) v[j][3 * kk + hh] = s * (coef * (da[kk] * db[hh]));
-                        }
-                    }
-#pragma unroll
-                    for (int j = 0; j < 4; j++)
-                        if (c + j < c1)
-#pragma unroll
-                            for (int e = 0; e < 9; e++) a[e] += v[j][e];
+                        for (int hh = 0; hh < 3; hh++) d[(3 * kk + hh) * CS_SLICE] += s * (coef * (da[kk] * dth[3 * bb + hh]));
                 }
-                if (k == 0) {
-                    const int hc = (int)B.handle[row].w;
-                    for (int t = 0; t < hc; t++) {
-                        const float add_ = dt * dt * P.handle_stiffness;
-                        a[0] += add_; a[4] += add_; a[8] += add_;
-                    }
+                // dt (f + dt J v) of the row's node (PhysicsHelper.cu:351-352)
+                const int4 en = B.edge_nodes[e];
+                const f3 v0 = ld3(B.v, en.x), v1 = ld3(B.v, en.y), v2 = ld3(B.v, en.z), v3 = ld3(B.v, en.w);
+                const float vel[12] = {v0.x, v0.y, v0.z, v1.x, v1.y, v1.z, v2.x, v2.y, v2.z, v3.x, v3.y, v3.z};
+                const float ca = coef * angle;
+                float r[3];
+#pragma unroll
+                for (int kk = 0; kk < 3; kk++) {
+                    float jv = 0.0f;
+#pragma unroll
+                    for (int q = 0; q < 12; q++) jv += (dt * (coef * (da[kk] * dth[q]))) * vel[q];
+                    r[kk] = dt * (ca * da[kk] + jv);
+                }
+                b0 += r[0];
+                b1 += r[1];
+                b2 += r[2];
+            }
+            const float4 hd = B.handle[row];
+            const int hc = (int)hd.w;
+            if (hc > 0) {
+                const float add_ = dt * dt * P.handle_stiffness;
+                for (int t = 0; t < hc; t++) {
+                    acc[0] += add_;
+                    acc[4 * CS_SLICE] += add_;
+                    acc[8 * CS_SLICE] += add_;
+                }
+                const f3 xr = ld3(B.x, row), vr = ld3(B.v, row);
+                // the target: the handle's position at load, or a motion's transformation of it
+                const int mo = B.handle_motion[row];
+                const f3 target = mo >= 0 ? transform_point(B.params->motion[mo], mk(hd.x, hd.y, hd.z))
+                                          : mk(hd.x, hd.y, hd.z);
+                const f3 fh = mulv(scl(dt, sub(sub(target, xr), scl(dt, vr))), P.handle_stiffness);
+                for (int t = 0; t < hc; t++) {
+                    b0 += fh.x;
+                    b1 += fh.y;
+                    b2 += fh.z;
                 }
             }
-            // streaming stores: A is read back from DRAM by the solvers, while the element
-            // records this kernel re-reads should keep their place in L2
+        }
+        // the panels, streamed (the solvers read A back from DRAM)
+        double bsq = 0.0;
+        for (int k = 0; k < sd.width; k++) {
+            float a[9];
+#pragma unroll
+            for (int e = 0; e < 9; e++) a[e] = acc[(9 * k + e) * CS_SLICE];
             float* panel = B.A + (size_t)(sd.panel0 + k) * CS_PANEL_FLOATS;
             __stcs(reinterpret_cast<float4*>(panel) + lane, make_float4(a[0], a[1], a[2], a[3]));
             __stcs(reinterpret_cast<float4*>(panel + 128) + lane, make_float4(a[4], a[5], a[6], a[7]));
             __stcs(panel + 256 + lane, a[8]);
-
             if (k == 0 && live) {
-                // Right-hand side in the reference's order: gravity, wind (faces), stretching
-                // (faces), bending (edges), handles (Cloth.cu:94-169).
-                const float m = B.mass[row];
-                const float g0 = (dt * m) * P.gravity[0], g1 = (dt * m) * P.gravity[1], g2 = (dt * m) * P.gravity[2];
-                float b0 = 0.0f + g0, b1 = 0.0f + g1, b2 = 0.0f + g2;
-                for (int pass = 0; pass < 3; pass++) {
-                    for (int c = c0; c < c1; c += 4) {
-                        float w[4][3];
-                        bool use[4];
-#pragma unroll
-                        for (int j = 0; j < 4; j++) {
-                            use[j] = false;
-                            if (c + j >= c1) continue;
-                            const uint32_t code = __ldg(&B.tcontrib[c + j]);
-                            const bool edge = (code & CS_CODE_EDGE) != 0;
-                            if (edge != (pass == 2)) continue;
-                            const int elem = (int)((code >> 4) & 0x7FFFFFFu);
-                            const int ca = (code >> 2) & 3;
-                            if (pass == 0) {
-                                const float* r = frec + (size_t)elem * CS_FACE_REC;
-                                w[j][0] = __ldg(r + 111);
-                                w[j][1] = __ldg(r + 115);
-                                w[j][2] = __ldg(r + 119);
-                            } else {
-                                const float4 q = __ldg(reinterpret_cast<const float4*>(
-                                    pass == 1 ? frec + (size_t)elem * CS_FACE_REC + 108 + 4 * ca
-                                              : erec + (size_t)elem * CS_EDGE_REC + 16 + 4 * ca));
-                                w[j][0] = q.x;
-                                w[j][1] = q.y;
-                                w[j][2] = q.z;
-                            }
-                            use[j] = true;
-                        }
-#pragma unroll
-                        for (int j = 0; j < 4; j++)
-                            if (use[j]) {
-                                b0 += w[j][0];
-                                b1 += w[j][1];
-                                b2 += w[j][2];
-                            }
-                    }
-                }
-                const float4 hd = B.handle[row];
-                const int hc = (int)hd.w;
-                if (hc > 0) {
-                    const f3 xr = ld3(B.x, row), vr = ld3(B.v, row);
-                    // the target: the handle's position at load, or a motion's transformation of it
-                    const int mo = B.handle_motion[row];
-                    const f3 target = mo >= 0 ? transform_point(B.params->motion[mo], mk(hd.x, hd.y, hd.z))
-                                              : mk(hd.x, hd.y, hd.z);
-                    const f3 fh = mulv(scl(dt, sub(sub(target, xr), scl(dt, vr))), P.handle_stiffness);
-                    for (int t = 0; t < hc; t++) {
-                        b0 += fh.x; b1 += fh.y; b2 += fh.z;
-                    }
-                }
                 B.b[3 * row] = b0;
                 B.b[3 * row + 1] = b1;
                 B.b[3 * row + 2] = b2;
@@ -528,20 +506,27 @@ __global__ void __launch_bounds__(128) cs_gather_kernel(Batch B) {
     }
 }
 
-// The reference's per-element outputs (f, J) for inspection: faces re-evaluated from the
-// current state as stretchingForce returns them (PhysicsHelper.cu:288-290), interior edges
-// expanded from the last assembly's records as bendingForce returns them
-// (PhysicsHelper.cu:351-352).
+// The reference's per-element outputs (f, J) for inspection, from the current state: faces
+// as stretchingForce returns them (PhysicsHelper.cu:288-290), interior edges as bendingForce
+// returns them (PhysicsHelper.cu:351-352).
 __global__ void __launch_bounds__(128) cs_expand_kernel(Batch B, float* face_f, float* face_J, float* edge_f,
                                                         float* edge_J) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < B.F) face_eval(B, i, nullptr, face_f + 9 * (size_t)i, face_J + 81 * (size_t)i);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float dt = B.params->dt;
+    if (i < B.F) {
+        FaceState S;
+        face_setup(B, i, S);
+        float* Jo = face_J + 81 * (size_t)i;
+        for (int p = 0; p < 9; p++) {
+            float fp;
+            face_row(S, p, dt, fp, [&](int q, float J) { Jo[9 * p + q] = J; });
+            face_f[9 * (size_t)i + p] = fp;
+        }
+    }
     if (i < B.E) {
-        const float* r = B.edge_rec + (size_t)i * CS_EDGE_REC;
-        const float coef = r[3], angle = r[19];
+        float d[12], coef, angle;
+        edge_geom(B, i, d, coef, angle);
         const float ca = coef * angle;
-        float d[12];
-        for (int p = 0; p < 12; p++) d[p] = r[4 * (p / 3) + p % 3];
         for (int p = 0; p < 12; p++) {
             edge_f[12 * (size_t)i + p] = ca * d[p];
             for (int q = 0; q < 12; q++) edge_J[144 * (size_t)i + 12 * p + q] = coef * (d[p] * d[q]);

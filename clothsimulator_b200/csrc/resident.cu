@@ -1053,110 +1053,3 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
 #undef WMASKS
     cl.sync();  // no CTA leaves while another may still address its shared memory
 }
-
-// Coarse matrix of each resident sheet for the coarse-space correction of the solve above:
-// A_c = R A R^T, where R sums the rows of each aggregate (a segment of a CTA's strip) per
-// component, so block (a, b) of A_c is the sum of the stored blocks A_ij with row i in
-// aggregate a and column j in aggregate b.  The loader lists those blocks per pair (a, b) in
-// slot order; a warp sums a pair, lane l taking the blocks l, l + 32, ... in order, and a
-// butterfly combines the lanes (a fixed order: deterministic, no atomics).  A_c is SPD (A is,
-// and R has full row rank), so Gauss-Jordan elimination inverts it in place in shared memory
-// without pivoting, in FP32: per pivot one FMA sweep over every entry with the pivot row and
-// column read from copies (two buffers), then the pivot row and column themselves.  The inverse, symmetrised,
-// is stored per work item for the resident kernel, which applies its CTA's rows each CG
-// iteration.  A non-positive or non-finite pivot marks the work item's coarse matrix invalid
-// and the solve runs without the correction.  One CTA per resident work item; dynamic shared
-// memory (nc + 4) x nc floats.
-static_assert(3 * CS_COARSE_AGGS <= 6 * 32, "the elimination's column loop covers at most 192 columns");
-
-__global__ void __launch_bounds__(CS_COARSE_THREADS) cs_coarse_setup_kernel(Batch B) {
-    const DevParams P = *B.params;
-    if (P.solver != CS_SOLVER_AUTO_DEV || P.cheb_degree < 3 || !P.coarse) return;  // uniform
-    const int idx = blockIdx.x;
-    if (idx >= B.n_resident) return;
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
-    const SheetDesc sh = B.sheets[B.rlist[idx]];
-    const int4 ci = B.rcoarse[sh.topo];
-    const int nc = ci.x;
-    if (nc == 0 || nc > B.res_cnc) {
-        if (tid == 0) B.cvalid[idx] = 0;
-        return;
-    }
-    float* M = reinterpret_cast<float*>(cs_res_smem);
-    float* colb = M + nc * nc;   // [2][nc] pivot columns
-    float* rowb = colb + 2 * nc;  // [2][nc] pivot rows
-    for (int i = tid; i < nc * nc; i += blockDim.x) M[i] = 0.f;
-    __syncthreads();
-    for (int q = ci.z + w; q < ci.w; q += nw) {
-        const int4 pr = B.cpair[q];
-        float acc[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        for (int k = pr.z + lane; k < pr.w; k += 32) {
-            const int slot = __ldg(&B.ccontrib[k]);
-            const float* pk = B.A + (size_t)(sh.panel_off + slot / CS_SLICE) * CS_PANEL_FLOATS;
-            const int l = slot % CS_SLICE;
-            const float4 a0 = __ldg(reinterpret_cast<const float4*>(pk) + l);
-            const float4 a1 = __ldg(reinterpret_cast<const float4*>(pk + 128) + l);
-            const float a8 = __ldg(pk + 256 + l);
-            acc[0] += a0.x; acc[1] += a0.y; acc[2] += a0.z;
-            acc[3] += a0.w; acc[4] += a1.x; acc[5] += a1.y;
-            acc[6] += a1.z; acc[7] += a1.w; acc[8] += a8;
-        }
-#pragma unroll
-        for (int i = 0; i < 9; i++) acc[i] = rwarp_sum(acc[i]);
-        if (lane == 0) {
-#pragma unroll
-            for (int i = 0; i < 3; i++)
-#pragma unroll
-                for (int j = 0; j < 3; j++) M[(3 * pr.x + i) * nc + 3 * pr.y + j] = acc[3 * i + j];
-        }
-    }
-    __syncthreads();
-    for (int i = tid; i < nc; i += blockDim.x) {
-        colb[i] = M[i * nc];
-        rowb[i] = M[i];
-    }
-    __syncthreads();
-    bool ok = true;
-    for (int k = 0; k < nc; k++) {
-        const float* cb = colb + (k & 1) * nc;
-        const float* rb = rowb + (k & 1) * nc;
-        float* cn = colb + ((k + 1) & 1) * nc;
-        float* rn = rowb + ((k + 1) & 1) * nc;
-        const float piv = rb[k];  // every thread reads the same value: a uniform decision
-        if (!(piv > 0.f) || !(piv < 3.0e38f)) {
-            ok = false;
-            break;
-        }
-        const float ip = 1.f / piv;
-        // a_ij <- a_ij - a_ik a_kj / p everywhere (one FMA per entry, no branches); then the
-        // pivot column (a_ik <- -a_ik / p) and row (a_kj <- a_kj / p, a_kk <- 1/p)
-        for (int i = w; i < nc; i += nw) {
-            const float c = cb[i];
-            float* Mi = M + i * nc;
-#pragma unroll
-            for (int n = 0; n < 6; n++) {
-                const int j = lane + 32 * n;
-                if (j < nc) Mi[j] = fmaf(-c, rb[j] * ip, Mi[j]);
-            }
-        }
-        __syncthreads();
-        for (int i = tid; i < nc; i += blockDim.x) {
-            M[i * nc + k] = i == k ? ip : -cb[i] * ip;
-            if (i != k) M[k * nc + i] = rb[i] * ip;
-        }
-        __syncthreads();
-        // the next step's pivot row and column
-        if (k + 1 < nc)
-            for (int i = tid; i < nc; i += blockDim.x) {
-                cn[i] = M[i * nc + k + 1];
-                rn[i] = M[(k + 1) * nc + i];
-            }
-        __syncthreads();
-    }
-    // written out symmetrised
-    float* out = B.cinv + (size_t)idx * B.res_cnc * B.res_cnc;
-    if (ok)
-        for (int i = w; i < nc; i += nw)
-            for (int j = lane; j < nc; j += 32) out[i * nc + j] = 0.5f * (M[i * nc + j] + M[j * nc + i]);
-    if (tid == 0) B.cvalid[idx] = ok ? 1 : 0;
-}
