@@ -7,7 +7,8 @@
 //             (Face::inverse, Face.cu:16), rest area.
 //   edges   : interior edges only (the reference skips boundary edges, Cloth.cu:142):
 //             int4 {n0, n1, opposite0, opposite1}, int meta (face-vertex rotations), sheet,
-//             float4 {area0 + area1, bias weight side 0, side 1, 0}.
+//             float4 {area0 + area1, bias weight side 0, side 1, 0}; per step a 64-byte
+//             record of its bending geometry (dtheta, coefficient, theta).
 //   system  : SELL-32 block layout.  A sheet's rows (nodes), sorted by block count within
 //             windows of sigma rows (sigma chosen per topology to minimise padding), are cut
 //             into slices of 32; slice s has `width` block slots per row (padded with zero
@@ -235,6 +236,7 @@ struct Batch {
     int* edge_meta = nullptr;
     int* edge_sheet = nullptr;
     float4* edge_par = nullptr;
+    float4* edge_geo = nullptr;  // per step: 4 per edge, dtheta (12), coefficient, theta (cs_edge_kernel)
     // sheets, materials, topology
     SheetDesc* sheets = nullptr;
     float4* tables = nullptr;

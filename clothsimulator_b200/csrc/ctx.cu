@@ -33,6 +33,7 @@
 #include "mlp.h"
 
 // kernels (forces.cu, pcg.cu)
+__global__ void cs_edge_kernel(Batch B);
 __global__ void cs_gather_kernel(Batch B);
 __global__ void cs_expand_kernel(Batch B, float* face_f, float* face_J, float* edge_f, float* edge_J);
 __global__ void cs_reduce1_kernel(Batch B);
@@ -891,6 +892,10 @@ struct cs_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // a second stream for the resident coarse set-up, forked after the assembly and joined before
+    // the resident solve (it overlaps the learned inference and the solve set-up)
+    cudaStream_t side = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
     std::string err;
     Batch B;
     bool loaded = false;
@@ -1034,6 +1039,7 @@ inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 int launchAssembly(cs_ctx* c) {
     Batch& B = c->B;
     int n = 1;
+    if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B), n++;
     cs_gather_kernel<<<c->gatherGrid, CS_GATHER_THREADS, c->gatherSmem, c->stream>>>(B);
     if (B.n_pinst > 0) {
         // proximity terms after the handles (Cloth.cu:676-684): records, then per row the
@@ -1078,6 +1084,8 @@ int launchBatchedCoarseSetup(cs_ctx* c) {
 
 // Kernels per step of the batched loop's coarse set-up, of the resident solve, and per loop trip
 // (the launch counters of cs_get_counters).
+// Kernels launchAssembly launches: the edge records, the gather, the proximity terms.
+int assemblyKernels(const cs_ctx* c) { return (c->B.E ? 1 : 0) + 1 + (c->B.n_pinst > 0 ? 3 : 0); }
 int bcSetupKernels(const cs_ctx* c) { return c->B.bc_total_agg > 0 ? 2 + (c->B.bc_n_big > 0 ? 1 : 0) : 0; }
 int residentKernels(const cs_ctx* c) {
     return c->resClusters > 0 ? 1 + (c->B.res_cnc > 0 && c->B.n_resident > 0 ? 1 : 0) : 0;
@@ -1140,6 +1148,26 @@ void launchResident(cs_ctx* c, bool setup = true) {
     cudaLaunchKernelEx(&cfg, cs_resident_pcg_kernel, c->B);
 }
 
+int launchMlpInference(cs_ctx* c, float* pred);
+
+// The step up to its solve loop: assembly; the resident sheets' coarse matrices on the side
+// stream while the learned inference (when asked) and the solve set-up run on the main stream;
+// the join; the cluster-resident solve.  Captured into the step graph, or launched directly.
+void launchPrelude(cs_ctx* c, bool learned) {
+    launchAssembly(c);
+    const bool fork = c->resClusters > 0 && c->B.res_cnc > 0 && c->B.n_resident > 0;
+    if (fork) {
+        cudaEventRecord(c->evFork, c->stream);
+        cudaStreamWaitEvent(c->side, c->evFork, 0);
+        cs_coarse_setup_kernel<<<c->B.n_resident, CS_COARSE_THREADS, cs_coarse_setup_smem(c->B.res_cnc), c->side>>>(c->B);
+        cudaEventRecord(c->evJoin, c->side);
+    }
+    if (learned) launchMlpInference(c, c->B.warm);
+    launchSolvePrologue(c);
+    if (fork) cudaStreamWaitEvent(c->stream, c->evJoin, 0);
+    launchResident(c, false);
+}
+
 // Learned warm start: features of the assembled system, layer 1, layers 2-3 + output; the
 // prediction replaces the previous dv in B.warm (the solve then starts from it).
 int launchMlpInference(cs_ctx* c, float* pred) {
@@ -1174,10 +1202,7 @@ cs_status buildGraph(cs_ctx* c, bool learned) {
     c->gph[learned][c->tripCoarse] = graph;
     // prelude: assembly (+ learned warm start) + solve setup, captured into the graph
     CS_CUDA(cudaStreamBeginCaptureToGraph(c->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    launchAssembly(c);
-    if (learned) launchMlpInference(c, c->B.warm);
-    launchSolvePrologue(c);
-    launchResident(c);
+    launchPrelude(c, learned);
     cudaStreamCaptureStatus cst;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
@@ -1245,7 +1270,10 @@ cs_status cs_create(cs_ctx** out, int device) {
     auto* c = new cs_ctx();
     c->device = device;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->evFork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess) {
         delete c;
         return CS_ERR_CUDA;
     }
@@ -1260,6 +1288,9 @@ cs_status cs_destroy(cs_ctx* c) {
     freeBatch(c);
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
+    cudaEventDestroy(c->evFork);
+    cudaEventDestroy(c->evJoin);
+    cudaStreamDestroy(c->side);
     cudaStreamDestroy(c->stream);
     delete c;
     return CS_OK;
@@ -1827,6 +1858,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     if ((st = dalloc(c, &B.field, (size_t)(n))) != CS_OK) return st;
     AL(dv, 3LL * B.N);
     AL(x0, 3LL * B.N);
+    AL(edge_geo, 4LL * std::max(B.E, 1));
     AL(dv64, 3LL * B.N);
     AL(warm, 3LL * B.N);
     AL(A, (long long)B.n_panels * CS_PANEL_FLOATS);
@@ -2633,10 +2665,8 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
         if ((st = buildGraph(c, learned)) != CS_OK) return st;
         CS_CUDA(cudaGraphLaunch(c->gexec[learned][c->tripCoarse], c->stream));
     } else {
-        c->hostLaunches += launchAssembly(c) + 3 + bcSetupKernels(c) + residentKernels(c);
-        if (learned) c->hostLaunches += launchMlpInference(c, c->B.warm);
-        launchSolvePrologue(c);
-        launchResident(c);
+        c->hostLaunches += assemblyKernels(c) + 3 + bcSetupKernels(c) + residentKernels(c) + (learned ? 3 : 0);
+        launchPrelude(c, learned);
         int go = 1;
         int trips = 0;
         while (go) {
@@ -2654,8 +2684,7 @@ cs_status cs_step(cs_ctx* c, const cs_step_params* p, cs_step_stats* stats) {
     c->steps++;
     if (p->use_graph) {
         c->graphSteps++;
-        c->graphLaunchesFixed += (c->B.F ? 1 : 0) + (c->B.E ? 1 : 0) + 1 + 3 + (learned ? 3 : 0) +
-                                 bcSetupKernels(c) + residentKernels(c) + (c->B.n_pinst > 0 ? 3 : 0);
+        c->graphLaunchesFixed += assemblyKernels(c) + 3 + (learned ? 3 : 0) + bcSetupKernels(c) + residentKernels(c);
     }
     if (!stats) return CS_OK;
     return fillStepStats(c, stats, d.loop_cap, true);
@@ -2811,6 +2840,7 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
         cudaEventRecord(c->ev0, c->stream);
         for (int r = 0; r < reps; r++) {
             switch (which) {
+                case 1: if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B); break;
                 case 2: cs_gather_kernel<<<c->gatherGrid, CS_GATHER_THREADS, c->gatherSmem, c->stream>>>(B); break;
                 case 3: launchSpmvShape(B, c->spmvShape, c->stream); break;
                 case 4: cs_vector_kernel<<<g, 128, 0, c->stream>>>(B); break;
@@ -2824,8 +2854,9 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
         cudaEventElapsedTime(&t, c->ev0, c->ev1);
         return t / reps;
     };
-    // the element terms are evaluated inside the gather: entries 0 and 1 stay 0
-    ms[0] = ms[1] = 0.f;
+    // the face terms are evaluated inside the gather: entry 0 stays 0
+    ms[0] = 0.f;
+    ms[1] = timeIt(1);
     ms[2] = timeIt(2);
     // solver kernels with every instance held in one phase
     cs_solve_setup_kernel<<<B.S, 128, 0, c->stream>>>(B);

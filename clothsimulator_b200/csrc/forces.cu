@@ -6,12 +6,14 @@
 // reference's CPU assembly entry by entry.
 //
 // Kernels:
+//   cs_edge_kernel   one thread per interior edge: dihedral bending geometry (dtheta, the
+//                    rank-one Jacobian's coefficient, theta) as a 64-byte record.
 //   cs_gather_kernel one warp per 32-row slice, lane = row: the row's own rows of the
-//                    stretching terms of its faces and of the bending terms of its interior
-//                    edges, summed into every block (i, j) of A in the reference's order (mass,
-//                    faces by index, edges by index, handles) in shared memory: no atomics, no
-//                    sort, no element records, bit-reproducible.  Also b, the 3x3 block-Jacobi
-//                    inverse and the slice's ||b||^2.
+//                    stretching terms of its faces (evaluated here) and of the bending terms of
+//                    its interior edges, summed into every block (i, j) of A in the reference's
+//                    order (mass, faces by index, edges by index, handles) in shared memory: no
+//                    atomics, no sort, bit-reproducible.  Also b, the 3x3 block-Jacobi inverse
+//                    and the slice's ||b||^2.
 //   cs_expand_kernel the per-element f and J as the reference's force functions return them
 //                    (inspection).
 //   cs_prox_kernel, cs_prox_row_kernel  proximity terms on top of the assembled system.
@@ -357,16 +359,32 @@ __device__ __forceinline__ void edge_geom(const Batch& B, int e, float (&dth)[12
 
 }  // namespace
 
+// One thread per interior edge: its bending geometry (edge_geom) once, as a 64-byte record
+// {dtheta 0-2, coef}, {dtheta 3-5, theta}, {dtheta 6-8, 0}, {dtheta 9-11, 0} that the
+// gather's four rows of the edge read (the records of the slices in flight stay in L2).
+__global__ void __launch_bounds__(128) cs_edge_kernel(Batch B) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= B.E) return;
+    float d[12], coef, angle;
+    edge_geom(B, e, d, coef, angle);
+    float4* out = B.edge_geo + 4 * (size_t)e;
+    out[0] = make_float4(d[0], d[1], d[2], coef);
+    out[1] = make_float4(d[3], d[4], d[5], angle);
+    out[2] = make_float4(d[6], d[7], d[8], 0.0f);
+    out[3] = make_float4(d[9], d[10], d[11], 0.0f);
+}
+
 // Assembly.  Warps walk the slices grid-stride (a persistent launch); lane = row.  Each row
-// evaluates its own rows of the stretching terms of its faces and of the bending terms of its
-// interior edges (the element arithmetic of face_row and edge_geom, shared with the inspection
-// kernel below), and adds each block into the row's slot accumulators in shared memory:
+// evaluates its own rows of the stretching terms of its faces (face_row, shared with the
+// inspection kernel below) and forms its rows of the bending terms of its interior edges from
+// their records (cs_edge_kernel), and adds each block into the row's slot accumulators in
+// shared memory:
 // faces in index order, then edges in index order, after the mass and before the handles, so
 // every block (i, j) sums its contributors in the reference's order (Cloth.cu:78-169) with no
-// atomics and no element records in memory.  b follows the reference's order too: gravity,
-// wind (faces), stretching (faces), bending (edges), handles (Cloth.cu:94-169).  A face is
-// evaluated by each of its three corner rows (a third of its rows each) and an edge's
-// gradient by each of its four nodes' rows.  Writes A's panels, b, the block-Jacobi inverse
+// atomics.  b follows the reference's order too: gravity, wind (faces), stretching (faces),
+// bending (edges), handles (Cloth.cu:94-169).  A face is evaluated by each of its three
+// corner rows (a third of its rows each); face records, nine 3x3 blocks per face, would be
+// read back through L2 by rows far apart in the slice order.  Writes A's panels, b, the block-Jacobi inverse
 // of the diagonal block and the slice's ||b||^2 (part[2*slice]).
 //
 // Dynamic shared memory: per warp gather_width slots x 9 entries x 32 lanes, entry e of slot k
@@ -428,7 +446,14 @@ __global__ void __launch_bounds__(CS_GATHER_THREADS) cs_gather_kernel(Batch B) {
                 const int2 c = __ldg(&B.redge[t]);
                 const int e = sh.edge_off + (c.x >> 2), a = c.x & 3;
                 float dth[12], coef, angle;
-                edge_geom(B, e, dth, coef, angle);
+                {
+                    const float4* rec = B.edge_geo + 4 * (size_t)e;
+                    const float4 q0 = __ldg(rec), q1 = __ldg(rec + 1), q2 = __ldg(rec + 2), q3 = __ldg(rec + 3);
+                    dth[0] = q0.x; dth[1] = q0.y; dth[2] = q0.z; coef = q0.w;
+                    dth[3] = q1.x; dth[4] = q1.y; dth[5] = q1.z; angle = q1.w;
+                    dth[6] = q2.x; dth[7] = q2.y; dth[8] = q2.z;
+                    dth[9] = q3.x; dth[10] = q3.y; dth[11] = q3.z;
+                }
                 // the row's node's gradient by selects (no indexed local arrays)
                 float da[3];
 #pragma unroll

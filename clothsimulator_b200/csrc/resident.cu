@@ -557,6 +557,13 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
         double gam = 0.0, gam_prev = 0.0, rr = 0.0, delta = 0.0, alpha_d = 0.0, res0 = bn, resnorm = -1.0,
                first_res = -1.0;
         bool cont = false;  // the next PH_INIT keeps the search direction (reliable update)
+        // dv64 and e are known to be zero (zero guess before its first CG step, or a rejected
+        // warm start just cleared): the next FP64 residual is b itself and needs no SpMV
+        bool dv_zero = !P.warm;
+        // the warm start was just scaled by affine_a: the next residual is the affine combination
+        // (1 - a) b + a r of b and the residual r of the unscaled start, no SpMV either
+        bool affine = false;
+        double affine_a = 0.0;
         // the warm start's scaling pass (warm_scale): its first residual gives d.b and d.r
         bool scale_pass = P.warm && P.warm_scale;
         // 1 / gam and 1 / (gam alpha), computed when gam and alpha are set, so that the next
@@ -675,7 +682,11 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
             }
             if (phase == PH_RES) {
                 // fold the FP32 correction into the FP64 solution; every CTA signals that its
-                // rows are written; then r = b - A dv64 in FP64 over global dv64
+                // rows are written; then r = b - A dv64 in FP64 over global dv64 (r = b when
+                // dv64 is known to be zero: no signal, no SpMV; the decision is uniform)
+                const bool zero = dv_zero, aff = affine;
+                dv_zero = false;
+                affine = false;
                 if (live) {
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
@@ -683,32 +694,51 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                         e[c] = 0.f;
                     }
                 }
-                __syncthreads();
-                if (tid == 0) {
-                    asm volatile("fence.acq_rel.cluster;" ::: "memory");
-                    for (int c = 0; c < ncta; c++) rbar_arrive_remote(mapa(sbar, c));
+                if (!zero && !aff) {
+                    __syncthreads();
+                    if (tid == 0) {
+                        asm volatile("fence.acq_rel.cluster;" ::: "memory");
+                        for (int c = 0; c < ncta; c++) rbar_arrive_remote(mapa(sbar, c));
+                    }
+                    ok = res_wait<true>(S, sbar, nres & 1u);
+                    nres++;
+                    if (!ok) break;
                 }
-                ok = res_wait<true>(S, sbar, nres & 1u);
-                nres++;
-                if (!ok) break;
                 double v[3] = {0.0, 0.0, 0.0};
                 if (live) {
                     const float* pn = in_smem ? sm_panels + (size_t)lp * CS_PANEL_FLOATS : B.A + (size_t)gp * CS_PANEL_FLOATS;
                     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-                    for (int k = 0; k < width; k++) {
-                        const int col = __ldg(&B.tcol[(tp + k) * CS_SLICE + lane]) + sh.node_off;
-                        const float* pk = pn + (size_t)k * CS_PANEL_FLOATS;
-                        const float4 a0 = reinterpret_cast<const float4*>(pk)[lane];
-                        const float4 a1 = reinterpret_cast<const float4*>(pk + 128)[lane];
-                        const float a8 = pk[256 + lane];
-                        const double d0 = __ldcg(&B.dv64[3 * col]), d1 = __ldcg(&B.dv64[3 * col + 1]),
-                                     d2 = __ldcg(&B.dv64[3 * col + 2]);
-                        y0 += (double)a0.x * d0 + (double)a0.y * d1 + (double)a0.z * d2;
-                        y1 += (double)a0.w * d0 + (double)a1.x * d1 + (double)a1.y * d2;
-                        y2 += (double)a1.z * d0 + (double)a1.w * d1 + (double)a8 * d2;
+                    // four slots' column and dv64 loads in flight at a time; sums in slot order
+#pragma unroll
+                    for (int k0 = 0; k0 < CS_RES_MAX_WIDTH; k0 += 4) {
+                        if (zero || aff || k0 >= width) break;
+                        int col[4];
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            col[j] = k0 + j < width ? __ldg(&B.tcol[(tp + k0 + j) * CS_SLICE + lane]) + sh.node_off : g;
+                        double d[4][3];
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+#pragma unroll
+                            for (int c = 0; c < 3; c++) d[j][c] = __ldcg(&B.dv64[3 * col[j] + c]);
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            if (k0 + j >= width) break;
+                            const float* pk = pn + (size_t)(k0 + j) * CS_PANEL_FLOATS;
+                            const float4 a0 = reinterpret_cast<const float4*>(pk)[lane];
+                            const float4 a1 = reinterpret_cast<const float4*>(pk + 128)[lane];
+                            const float a8 = pk[256 + lane];
+                            y0 += (double)a0.x * d[j][0] + (double)a0.y * d[j][1] + (double)a0.z * d[j][2];
+                            y1 += (double)a0.w * d[j][0] + (double)a1.x * d[j][1] + (double)a1.y * d[j][2];
+                            y2 += (double)a1.z * d[j][0] + (double)a1.w * d[j][1] + (double)a8 * d[j][2];
+                        }
                     }
-                    const double r0 = (double)B.b[3 * g] - y0, r1 = (double)B.b[3 * g + 1] - y1,
-                                 r2 = (double)B.b[3 * g + 2] - y2;
+                    double r0 = (double)B.b[3 * g] - y0, r1 = (double)B.b[3 * g + 1] - y1, r2 = (double)B.b[3 * g + 2] - y2;
+                    if (aff) {
+                        r0 = (1.0 - affine_a) * (double)B.b[3 * g] + affine_a * (double)r[0];
+                        r1 = (1.0 - affine_a) * (double)B.b[3 * g + 1] + affine_a * (double)r[1];
+                        r2 = (1.0 - affine_a) * (double)B.b[3 * g + 2] + affine_a * (double)r[2];
+                    }
                     // drift of the recursive residual it replaces
                     const double q0 = r0 - (double)r[0], q1 = r1 - (double)r[1], q2 = r2 - (double)r[2];
                     r[0] = (float)r0;
@@ -748,7 +778,9 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
 #pragma unroll
                             for (int c = 0; c < 3; c++) B.dv64[3 * g + c] *= a;
                         }
-                        continue;  // phase stays PH_RES
+                        affine = true;  // b - A (a d) = (1 - a) b + a (b - A d)
+                        affine_a = a;
+                        continue;       // phase stays PH_RES
                     }
                     flags |= CS_IF_WARM_REJECTED;
                     sweeps = 1;
@@ -759,6 +791,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
 #pragma unroll
                             for (int c = 0; c < 3; c++) B.dv64[3 * g + c] = 0.0;
                         }
+                        dv_zero = true;
                         phase = PH_RES;
                     }
                     continue;
@@ -779,12 +812,17 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
 #pragma unroll
                                 for (int c = 0; c < 3; c++) B.dv64[3 * g + c] = 0.0;
                             }
+                            dv_zero = true;
                             phase = PH_RES;
                         }
                         continue;
                     }
                 }
-                if (res <= P.tol * bn || bn == 0.0) {
+                if ((res <= P.tol * bn && aff) || (aff && bn == 0.0)) {
+                    // converged by the affine residual (built from an FP32 copy of r): confirmed
+                    // by a residual of the scaled start before the solve ends
+                    phase = PH_RES;
+                } else if (res <= P.tol * bn || bn == 0.0) {
                     flags |= CS_IF_CONVERGED;
                     phase = PH_FINISH;
                 } else if (iters >= P.max_iters) {
@@ -814,6 +852,7 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                 }
             }
             if (phase == PH_CG) {
+                dv_zero = false;  // e (folded into dv64 by the next residual) leaves zero here
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     e[c] = __fmaf_rn(alpha, p[c], e[c]);

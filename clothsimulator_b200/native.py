@@ -516,9 +516,9 @@ class Context:
         self.check(self.lib.cs_device_pointers(self.h, ctypes.byref(x), ctypes.byref(v), ctypes.byref(dv)))
         return x.value, v.value, dv.value
 
-    # cs_profile_kernels' entries; the first two (separate face and edge kernels) stay 0 since the
-    # assembly gather evaluates the element terms itself, and are left out
-    KERNELS = [None, None, "gather", "spmv", "vector", "reduce", "spmv_fp64", "resident_solve", "coarse_setup",
+    # cs_profile_kernels' entries; the first (a separate face kernel) stays 0 since the assembly
+    # gather evaluates the face terms itself, and is left out
+    KERNELS = [None, "edge", "gather", "spmv", "vector", "reduce", "spmv_fp64", "resident_solve", "coarse_setup",
                "batched_coarse_setup", "batched_coarse_trip"]
 
     def profile_kernels(self, params: StepParams, reps: int = 20) -> dict:

@@ -332,8 +332,8 @@ cs_status cs_device_pointers(cs_ctx* ctx, float** x, float** v, float** dv);
  * (Simulator.cu:845-855); these time on the device instead. */
 
 /* Times each kernel of the step in isolation with CUDA events on the context's stream, `reps`
- * launches each, on the current batch: ms[0] and [1] 0 (the face and edge terms are evaluated
- * inside the assembly gather), [2] gather (assembly with the element terms),
+ * launches each, on the current batch: ms[0] 0 (the face terms are evaluated inside the
+ * assembly gather), [1] edge (bending geometry), [2] gather (assembly),
  * [3] SpMV of a CG iteration, [4] vector update of a CG iteration, [5] per-instance reduction,
  * [6] FP64 residual SpMV, [7] one cluster-resident solve of all resident sheets (0 if none;
  * when every sheet is resident, cs_get_instance_stats then reports that solve), [8] the set-up
