@@ -3251,10 +3251,10 @@ cs_status cs_mlp_init(cs_ctx* c, int slots, unsigned long long seed) {
     cudaDeviceProp prop;
     CS_CUDA(cudaGetDeviceProperties(&prop, c->device));
     c->mlpGridTile = 2 * prop.multiProcessorCount;
-    // layer 1: 64 TMEM columns per CTA (8 per SM); layers 2-3: 128 columns and 75 KB of shared
-    // memory per CTA (3 per SM)
+    // layer 1: 64 TMEM columns per CTA (8 per SM); layers 2-3: 128 columns and 51 KB of shared
+    // memory per CTA (4 per SM: the SM's 512 TMEM columns)
     c->mlpGridL1 = 8 * prop.multiProcessorCount;
-    c->mlpGridL23 = 3 * prop.multiProcessorCount;
+    c->mlpGridL23 = 4 * prop.multiProcessorCount;
     c->mlpGridTrain = prop.multiProcessorCount;
     CS_CUDA(cudaFuncSetAttribute(cs_mlp_l1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_SMEM_L1));
     CS_CUDA(cudaFuncSetAttribute(cs_mlp_l23_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_SMEM_L23));

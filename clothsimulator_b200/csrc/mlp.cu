@@ -274,20 +274,21 @@ __global__ void __launch_bounds__(128) cs_mlp_l1_kernel(Batch B, MlpDev M, const
 
 // Layers 2, 3 and the output over nodes [n0, n1).  Inference (z2 == nullptr): the prediction
 // previous dv + sigma_y y + mu_y is written to pred (may alias B.warm).  Training: z2, z3, y.
-__global__ void __launch_bounds__(128) cs_mlp_l23_kernel(Batch B, MlpDev M, int n0, int n1, float* __restrict__ z2,
+__global__ void __launch_bounds__(128, 4) cs_mlp_l23_kernel(Batch B, MlpDev M, int n0, int n1, float* __restrict__ z2,
                                                        float* __restrict__ z3, float* __restrict__ yout,
                                                        float* pred) {
+    // 51 KB, so that four CTAs (4 x 128 TMEM columns) share an SM: the u2 tile is free once
+    // layer 2's MMA is done, and then holds h2 and layer 3's weights
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* sA = smem;                  // 128 x 128 bf16: 32 KB
+    unsigned char* sH = smem;                  // after layer 2's MMA: 128 x 64, 16 KB
+    unsigned char* sW3 = smem + 16384;         // after layer 2's MMA: 64 x 64, 8 KB
     unsigned char* sW2 = smem + 32768;         // 64 x 128: 16 KB
-    unsigned char* sH = smem + 49152;          // 128 x 64: 16 KB
-    unsigned char* sW3 = smem + 65536;         // 64 x 64: 8 KB
-    float* sf = reinterpret_cast<float*>(smem + 73728);  // W4 (192), b2 (64), b3 (64), b4 (3), mu_y, sigma_y
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 73728 + 2048);
+    float* sf = reinterpret_cast<float*>(smem + 49152);  // W4 (192), b2 (64), b3 (64), b4 (3), mu_y, sigma_y
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 49152 + 2048);
     uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 1);
     const int t = threadIdx.x, warp = t >> 5;
     load_weight_tile(M.wb + MLP_W2, 64, 128, false, sW2);
-    load_weight_tile(M.wb + MLP_W3, 64, 64, false, sW3);
     for (int e = t; e < 192; e += 128) sf[e] = __bfloat162float(M.wb[MLP_W4 + e]);
     for (int e = t; e < 64; e += 128) {
         sf[192 + e] = M.w[MLP_B2 + e];
@@ -380,6 +381,19 @@ __global__ void __launch_bounds__(128) cs_mlp_l23_kernel(Batch B, MlpDev M, int 
         phase ^= 1;
         tc::fence_after_sync();
         if (!ok) break;
+        // the u2 tile is free: layer 3's weights (row-major 64 x 64, this thread's 16 pairs, all
+        // loads issued before the stores) into its second quarter; h2 goes into its first half
+        {
+            const uint32_t* w3g = reinterpret_cast<const uint32_t*>(M.wb + MLP_W3);
+            uint32_t w3r[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) w3r[i] = __ldg(w3g + t + 128 * i);
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const int e = 2 * (t + 128 * i), r = e >> 6, k = e & 63;
+                *reinterpret_cast<uint32_t*>(sW3 + tc::kmajor_offset(64, r, k)) = w3r[i];
+            }
+        }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             float zz[16];

@@ -60,7 +60,7 @@ __global__ void cs_mlp_energy_loss_kernel(MlpDev M, int s0, int s1, float* acc);
 
 // dynamic shared memory of the tile kernels (bytes)
 #define MLP_SMEM_L1 12816
-#define MLP_SMEM_L23 75792
+#define MLP_SMEM_L23 51216
 #define MLP_SMEM_BWD23 145232
 #define MLP_SMEM_BWD1 50304
 

@@ -818,9 +818,10 @@ __global__ void __launch_bounds__(CS_RES_MAX_WARPS * 32, 1) cs_resident_pcg_kern
                         continue;
                     }
                 }
-                if ((res <= P.tol * bn && aff) || (aff && bn == 0.0)) {
-                    // converged by the affine residual (built from an FP32 copy of r): confirmed
-                    // by a residual of the scaled start before the solve ends
+                if (aff && (res <= P.tol * bn || bn == 0.0 || iters >= P.max_iters)) {
+                    // the solve would end on the affine residual (built from an FP32 copy of r):
+                    // an FP64 residual of the scaled start decides instead, so the residual a
+                    // finished sheet reports is always an FP64 one
                     phase = PH_RES;
                 } else if (res <= P.tol * bn || bn == 0.0) {
                     flags |= CS_IF_CONVERGED;

@@ -361,3 +361,32 @@ def test_galerkin_scaled_warm_start(ctx_factory, route):
             else:
                 assert not np.any(fl & 2)
                 assert np.all(it <= 0.5 * it_zero), (it, it_zero)
+
+
+def test_converged_warm_start_reports_an_fp64_residual(ctx_factory):
+    """A warm start of twice the solution, Galerkin-scaled (factor 1/2), meets a loose tolerance
+    with no CG iteration.  The resident solver forms the scaled start's residual as (1 - a) b + a r
+    from the scale pass's residual r without an SpMV; a solve that would end on that residual
+    takes an FP64 residual of the scaled start first.  So the residual it reports is an FP64 one:
+    it agrees with the batched loop's, which always computes the scaled start's FP64 residual,
+    to 1e-4 relative (an affine residual built from the FP32 copy of r would miss by percents:
+    the scaled residual is the size of the solution's FP32 rounding)."""
+    scene = scenes.windy_batch(4, 24, seed=73)
+    ctx = ctx_factory(scene.sheets)
+    x0, v0 = initial_state(scene)
+    ctx.set_state(x0, v0)
+    ctx.step(params_for(scene, tol=1e-12, precond_degree=3, coarse=1))
+    exact = ctx.get_dv().copy()
+    rr = {}
+    for route, kw in (("resident_coarse", dict(precond_degree=3, coarse=1)),
+                      ("resident_jacobi", dict(precond_degree=1, coarse=0)),
+                      ("batched", dict(solver=native.SOLVER_BATCHED))):
+        ctx.set_state(x0, v0)
+        ctx.set_warm_start(2.0 * exact)
+        st, _ = ctx.step(params_for(scene, tol=1e-3, warm_start=native.WARM_PREVIOUS, warm_scale=1, **kw))
+        it, res, fl = ctx.instance_stats()
+        assert st.converged == 4 and np.all(it == 0) and not np.any(fl & 2), (route, it, fl)
+        assert rel(ctx.get_dv(), exact) < 1e-5, route
+        rr[route] = res.copy()
+    for route in ("resident_coarse", "resident_jacobi"):
+        assert np.all(np.abs(rr[route] - rr["batched"]) <= 1e-4 * rr["batched"]), (route, rr[route], rr["batched"])
