@@ -1036,6 +1036,18 @@ void freeBatch(cs_ctx* c) {
 
 inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
+// Raises a kernel's limit on dynamic shared memory to at least `bytes`, never lowering it.  The
+// limit belongs to the function (on the current device), not to a context: every context of
+// the process shares it, and batches of different sizes need different amounts, so a context
+// loaded later must not take away what an earlier one launches with.
+cudaError_t raiseDynSmem(const void* kernel, size_t bytes) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+    if (e != cudaSuccess) return e;
+    if ((size_t)a.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 int launchAssembly(cs_ctx* c) {
     Batch& B = c->B;
     int n = 1;
@@ -1451,7 +1463,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         R.cap = (int)std::min<size_t>((size_t)R.panels, budget / (CS_PANEL_FLOATS * sizeof(float)));
         R.smem = (size_t)R.cap * CS_PANEL_FLOATS * sizeof(float) + pbytes;
         if (budget > 0) {
-            cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R.smem);
+            raiseDynSmem((const void*)cs_resident_pcg_kernel, R.smem);
             if (cl > 8) cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
             cudaLaunchConfig_t cfg = {};
             cudaLaunchAttribute at[1];
@@ -1584,12 +1596,11 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         B.res_ck = res.ck;
         B.res_cnc = 3 * res.cl * res.ck;
         B.res_coff = (int)(res.smem - coarseSmemBytes(res.cl, res.ck));
-        CS_CUDA(cudaFuncSetAttribute(cs_coarse_setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)cs_coarse_setup_smem(B.res_cnc)));
+        CS_CUDA(raiseDynSmem((const void*)cs_coarse_setup_kernel, cs_coarse_setup_smem(B.res_cnc)));
     }
     if (res.clusters > 0) {
         // the launch attributes of the chosen plan (the evaluation set others)
-        CS_CUDA(cudaFuncSetAttribute(cs_resident_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)res.smem));
+        CS_CUDA(raiseDynSmem((const void*)cs_resident_pcg_kernel, res.smem));
         c->resCL = res.cl;
         c->resThreads = resW * CS_SLICE;
         c->resClusters = res.clusters;
@@ -1892,7 +1903,7 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
         c->gatherSmem = (size_t)(CS_GATHER_THREADS / 32) * B.gather_width * 9 * CS_SLICE * sizeof(float);
         if (c->gatherSmem > (size_t)prop.sharedMemPerBlockOptin)
             return fail(c, CS_ERR_INVALID_ARG, "slices of %d block slots exceed the assembly's shared memory", B.gather_width);
-        CS_CUDA(cudaFuncSetAttribute(cs_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->gatherSmem));
+        CS_CUDA(raiseDynSmem((const void*)cs_gather_kernel, c->gatherSmem));
         int perSM = 0;
         CS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, cs_gather_kernel, CS_GATHER_THREADS, c->gatherSmem));
         if (const char* ev = std::getenv("CS_GATHER_CTAS_PER_SM")) perSM = std::min(perSM, std::min(16, std::max(1, std::atoi(ev))));
