@@ -35,9 +35,10 @@
 __host__ __device__ inline uint32_t cs_code(int is_edge, int elem, int a, int b) {
     return (is_edge ? CS_CODE_EDGE : 0u) | ((uint32_t)elem << 4) | ((uint32_t)a << 2) | (uint32_t)b;
 }
-// Threads per CTA of the assembly gather (forces.cu); its slot accumulators take
-// 4 warps x gather_width x 1152 bytes of shared memory.  (One-warp CTAs, 15 warps per SM
-// instead of 12, measured slower on the windy batch: 3.82 against 3.35 ms.)
+// Threads per CTA of the assembly gather (forces.cu) at most; its slot accumulators take
+// gather_width x 1152 bytes of shared memory per warp, and a batch whose widest slice would not
+// fit four warps in a CTA's shared memory gets fewer.  (One-warp CTAs, 15 warps per SM instead
+// of 12, measured slower on the windy batch: 3.82 against 3.35 ms.)
 #define CS_GATHER_THREADS 128
 
 struct SheetDesc {

@@ -917,6 +917,7 @@ struct cs_ctx {
     long long steps = 0, hostLaunches = 0, graphSteps = 0, graphLaunchesFixed = 0;
     int gatherGrid = 1;  // persistent assembly gather: a few warps per SM walk the slices
     size_t gatherSmem = 0;  // its dynamic shared memory (slot accumulators)
+    int gatherWarps = 1;    // its warps per CTA
     // learned warm start
     MlpDev mlp;
     bool mlpInit = false;
@@ -1052,7 +1053,7 @@ int launchAssembly(cs_ctx* c) {
     Batch& B = c->B;
     int n = 1;
     if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B), n++;
-    cs_gather_kernel<<<c->gatherGrid, CS_GATHER_THREADS, c->gatherSmem, c->stream>>>(B);
+    cs_gather_kernel<<<c->gatherGrid, 32 * c->gatherWarps, c->gatherSmem, c->stream>>>(B);
     if (B.n_pinst > 0) {
         // proximity terms after the handles (Cloth.cu:676-684): records, then per row the
         // blocks, right-hand side and block-Jacobi inverse, then the ||b|| partials
@@ -1898,17 +1899,22 @@ cs_status cs_load_batch(cs_ctx* c, const cs_material_desc* mats, int n_mats, con
     {
         cudaDeviceProp prop;
         CS_CUDA(cudaGetDeviceProperties(&prop, c->device));
-        // persistent gather: as many CTAs per SM as its slot accumulators allow (at most
-        // CS_GATHER_CTAS_PER_SM, 1..16, when set)
-        c->gatherSmem = (size_t)(CS_GATHER_THREADS / 32) * B.gather_width * 9 * CS_SLICE * sizeof(float);
-        if (c->gatherSmem > (size_t)prop.sharedMemPerBlockOptin)
+        // persistent gather: CTAs of up to CS_GATHER_THREADS / 32 warps, fewer when a warp's
+        // slot accumulators (the widest slice's slots x 1,152 bytes) would not fit four times in
+        // a CTA's shared memory (meshes with high-valence nodes); as many CTAs per SM as the
+        // accumulators allow (at most CS_GATHER_CTAS_PER_SM, 1..16, when set)
+        const size_t perWarp = (size_t)B.gather_width * 9 * CS_SLICE * sizeof(float);
+        c->gatherWarps = (int)std::min<size_t>(CS_GATHER_THREADS / 32, (size_t)prop.sharedMemPerBlockOptin / perWarp);
+        if (c->gatherWarps < 1)
             return fail(c, CS_ERR_INVALID_ARG, "slices of %d block slots exceed the assembly's shared memory", B.gather_width);
+        c->gatherSmem = (size_t)c->gatherWarps * perWarp;
         CS_CUDA(raiseDynSmem((const void*)cs_gather_kernel, c->gatherSmem));
+        const int threads = 32 * c->gatherWarps;
         int perSM = 0;
-        CS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, cs_gather_kernel, CS_GATHER_THREADS, c->gatherSmem));
+        CS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, cs_gather_kernel, threads, c->gatherSmem));
         if (const char* ev = std::getenv("CS_GATHER_CTAS_PER_SM")) perSM = std::min(perSM, std::min(16, std::max(1, std::atoi(ev))));
         perSM = std::max(perSM, 1);
-        c->gatherGrid = std::max(1, std::min(nblk((long long)B.n_slices * 32, CS_GATHER_THREADS), perSM * prop.multiProcessorCount));
+        c->gatherGrid = std::max(1, std::min(nblk((long long)B.n_slices * 32, threads), perSM * prop.multiProcessorCount));
     }
     c->loaded = true;
     return CS_OK;
@@ -2852,7 +2858,7 @@ cs_status cs_profile_kernels(cs_ctx* c, const cs_step_params* p, int reps, float
         for (int r = 0; r < reps; r++) {
             switch (which) {
                 case 1: if (B.E) cs_edge_kernel<<<nblk(B.E, 128), 128, 0, c->stream>>>(B); break;
-                case 2: cs_gather_kernel<<<c->gatherGrid, CS_GATHER_THREADS, c->gatherSmem, c->stream>>>(B); break;
+                case 2: cs_gather_kernel<<<c->gatherGrid, 32 * c->gatherWarps, c->gatherSmem, c->stream>>>(B); break;
                 case 3: launchSpmvShape(B, c->spmvShape, c->stream); break;
                 case 4: cs_vector_kernel<<<g, 128, 0, c->stream>>>(B); break;
                 case 5: cs_reduce1_kernel<<<B.S, CS_REDUCE_THREADS, 0, c->stream>>>(B); break;
